@@ -1,0 +1,354 @@
+/*
+ * wadjet_gpu.h — C ABI of libwadjetgpu.so, the B200 (sm_100a) filter → hash-join →
+ * hash-aggregate pipeline that drops in under Wadjet's operator contract
+ * (internal/engine/exec/operators.go:10-108).
+ *
+ * Every entry point is plain C: opaque handles, raw pointers and sizes, an int
+ * status. A Go cgo wrapper implements exec.UnaryOperator / exec.Sink /
+ * exec.MergeableSink on top of these calls (the binding is shown in
+ * INTEGRATION.md). The reference interface each function replaces is cited
+ * beside it as path:line within the Wadjet source tree.
+ *
+ * Conventions
+ *  - Status: 0 = WG_OK; WG_E_NOMEM maps to memory.ErrMemoryExceeded
+ *    (internal/engine/memory/tracker.go:15). wg_last_error() returns a
+ *    thread-local message for the most recent failing call on this thread.
+ *  - Host pointers passed in are read only during the call (the cgo rule that C
+ *    must not retain Go pointers). Device memory belongs to the handle and is
+ *    released by the matching *_destroy.
+ *  - A handle is not re-entrant; callers serialise calls per handle (the Go
+ *    wrapper holds a mutex the way HashAggregate.Consume does,
+ *    exec/aggregate.go:1076). The context is thread-safe.
+ *  - "_device" variants take descriptors whose data/valid/sel pointers are
+ *    device addresses on the context's GPU; the others take host memory and
+ *    stage it through the context's pinned buffers.
+ */
+#ifndef WADJET_GPU_H
+#define WADJET_GPU_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define WG_API __attribute__((visibility("default")))
+#else
+#define WG_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+typedef int32_t wg_status;
+#define WG_OK             0
+#define WG_E_NOMEM        1  /* HBM ledger refused a reservation (memory.ErrMemoryExceeded) */
+#define WG_E_INVALID      2  /* bad argument / schema mismatch                              */
+#define WG_E_TIMEOUT      3  /* a bounded device-side wait ran out                           */
+#define WG_E_CUDA         4  /* a CUDA runtime call failed                                   */
+#define WG_E_UNSUPPORTED  5  /* shape the GPU path does not cover (e.g. string keys)          */
+#define WG_E_STATE        6  /* call out of order (consume after finalize, ...)               */
+
+/* ---- type ids: values of parquet.TypeID (internal/storage/parquet/schema.go:13-34) ---- */
+#define WG_TYPE_BOOL       0
+#define WG_TYPE_INT32      1
+#define WG_TYPE_INT64      2
+#define WG_TYPE_FLOAT32    3
+#define WG_TYPE_FLOAT64    4
+#define WG_TYPE_STRING     5
+#define WG_TYPE_BYTES      6
+#define WG_TYPE_TIMESTAMP  7
+#define WG_TYPE_IPV4       8   /* stored in Int64Data (kernel/compare.go:158) */
+#define WG_TYPE_IPV6       9
+#define WG_TYPE_CIDR      10
+#define WG_TYPE_MAC       11
+#define WG_TYPE_PORT      12
+#define WG_TYPE_PROTOCOL  13
+#define WG_TYPE_DURATION  14
+#define WG_TYPE_UUID      15
+#define WG_TYPE_DATE      16
+#define WG_TYPE_DECIMAL   17   /* element = wg_int128 */
+
+/* ---- compare ops: kernel.CompareOp (internal/engine/exec/kernel/compare.go:16-23) ---- */
+#define WG_OP_EQ 0
+#define WG_OP_NE 1
+#define WG_OP_LT 2
+#define WG_OP_LE 3
+#define WG_OP_GT 4
+#define WG_OP_GE 5
+
+/* kind of a filter constant (the Go `any` value handed to ResolveFilterKernel,
+ * kernel/compare.go:145). It is converted to the column's type exactly as
+ * toInt64 / toFloat64 do (kernel/compare.go:580-640). */
+#define WG_CONST_INT   0
+#define WG_CONST_FLOAT 1
+
+/* ---- aggregate functions: exec.AggFunc (internal/engine/exec/aggregate.go:27-31) ---- */
+#define WG_AGG_SUM   0
+#define WG_AGG_COUNT 1   /* input_col = -1 is COUNT(*) */
+#define WG_AGG_MIN   2
+#define WG_AGG_MAX   3
+#define WG_AGG_AVG   4
+
+/* ---- join types: exec.JoinType (internal/engine/exec/join.go:20-30) ---- */
+#define WG_JOIN_INNER 0
+
+/* Int128 DECIMAL element. Field order is Go's batch.Int128{Hi int64; Lo uint64}
+ * (internal/engine/batch/decimal.go:11), i.e. the opposite of a little-endian
+ * __int128. */
+typedef struct wg_int128 {
+  int64_t  hi;
+  uint64_t lo;
+} wg_int128;
+
+/* One column vector (batch.Vector, internal/engine/batch/vector.go:302).
+ * valid_words: NULL = no nulls; otherwise bit i of word i/64 is 1 when row i is
+ * valid, LSB first (batch.Bitmap, internal/engine/batch/bitmap.go:7,84). */
+typedef struct wg_column {
+  int32_t         type_id;
+  int32_t         scale;       /* DECIMAL scale, else 0 */
+  const void*     data;
+  const uint64_t* valid_words;
+  int64_t         len;
+} wg_column;
+
+/* One record batch (batch.RecordBatch, internal/engine/batch/batch.go:9).
+ * sel: NULL = all rows active, else sel_len ascending row indices (batch.go:13). */
+typedef struct wg_batch_desc {
+  int32_t          ncols;
+  int32_t          _pad;
+  const wg_column* cols;
+  int64_t          len;
+  const uint32_t*  sel;
+  int64_t          sel_len;
+} wg_batch_desc;
+
+/* One aggregate (exec.AggColumn, internal/engine/exec/aggregate.go:73).
+ * out_type: WG_TYPE_FLOAT64 / WG_TYPE_INT64 as the planner declares it
+ * (planner/physical/plan.go:9954); 0 picks the planner default: COUNT → INT64,
+ * SUM/AVG → FLOAT64, MIN/MAX → their input's class (exec/aggregate.go:4611). */
+typedef struct wg_agg_spec {
+  int32_t func;
+  int32_t input_col;
+  int32_t out_type;
+  int32_t _pad;
+} wg_agg_spec;
+
+/* One filter predicate `col OP const` (exec.KernelFilter, exec/filter.go:347). */
+typedef struct wg_predicate {
+  int32_t col;
+  int32_t op;
+  int32_t const_kind;
+  int32_t _pad;
+  int64_t const_i64;
+  double  const_f64;
+} wg_predicate;
+
+/* A projection expression in postfix form (exec.Project over expr.BinOpNumeric,
+ * internal/engine/expr/binop_numeric.go). Integer arithmetic wraps like Go
+ * int64; float arithmetic is IEEE binary64 with no contraction; a DECIMAL input
+ * read as float goes through Int128.ToFloat64 (expr/expr.go:225,257). */
+#define WG_EXPR_COL      0   /* push column `arg` */
+#define WG_EXPR_CONST_I  1   /* push imm_i64 */
+#define WG_EXPR_CONST_F  2   /* push imm_f64 */
+#define WG_EXPR_ADD      3
+#define WG_EXPR_SUB      4
+#define WG_EXPR_MUL      5
+#define WG_EXPR_DIV      6   /* float only */
+#define WG_EXPR_SHR      7   /* int only: arithmetic shift right by imm_i64 (top of stack) */
+#define WG_EXPR_AND      8   /* int only */
+#define WG_EXPR_MAX_OPS 12
+typedef struct wg_expr_op {
+  int32_t opcode;
+  int32_t arg;
+  int64_t imm_i64;
+  double  imm_f64;
+} wg_expr_op;
+typedef struct wg_expr {
+  int32_t    result_type;      /* WG_TYPE_INT64 or WG_TYPE_FLOAT64 */
+  int32_t    n_ops;
+  wg_expr_op ops[WG_EXPR_MAX_OPS];
+} wg_expr;
+
+/* Raw per-group aggregate state, the SoA accumulators of exec.flatAccumArrays
+ * (internal/engine/exec/agg_scatter.go:16). Arrays are caller-allocated with
+ * n_groups entries per key column / aggregate, laid out [k * n_groups + g].
+ * Any pointer may be NULL to skip that field. */
+typedef struct wg_group_export {
+  int64_t*   keys;       /* group key widened to int64 (packed keys unpacked per column) */
+  uint8_t*   key_valid;  /* 0 = the NULL group for that key column */
+  int64_t*   count;      /* non-null input rows per aggregate (COUNT(*) = all rows) */
+  int64_t*   i64;        /* sumI64 / minI64 / maxI64 */
+  double*    f64;        /* sumF64 / minF64 / maxF64 */
+  wg_int128* dec;        /* sumDec / minDec / maxDec */
+  uint8_t*   has;        /* hasMin / hasMax; for SUM/COUNT/AVG: count > 0 */
+} wg_group_export;
+
+typedef struct wg_ctx    wg_ctx;
+typedef struct wg_filter wg_filter;
+typedef struct wg_join   wg_join;
+typedef struct wg_agg    wg_agg;
+
+/* ======================================================================== */
+/* Context, HBM ledger                                                       */
+/* ======================================================================== */
+
+/* Thread-local message of the last failing call on this thread ("" if none). */
+WG_API const char* wg_last_error(void);
+
+/* Library version string. */
+WG_API const char* wg_version(void);
+
+/* Create a context on `device`: one CUDA stream, a pinned staging area and an
+ * HBM ledger with `hbm_budget_bytes` (0 = free device memory at creation)
+ * (memory.NewTracker, internal/engine/memory/tracker.go:36). pinned_spill_bytes
+ * caps the pinned host memory used for aggregate spill partitions. */
+WG_API wg_status wg_ctx_create(int32_t device, int64_t hbm_budget_bytes,
+                        int64_t pinned_spill_bytes, wg_ctx** out);
+WG_API wg_status wg_ctx_destroy(wg_ctx* ctx);
+/* Wait until all work queued on the context's stream is done. */
+WG_API wg_status wg_ctx_synchronize(wg_ctx* ctx);
+/* Ledger counters (Tracker.Used / Peak / Budget, tracker.go:129,151,134). */
+WG_API wg_status wg_ledger_stats(wg_ctx* ctx, int64_t* used, int64_t* peak, int64_t* budget);
+/* Explicit reservations against the ledger (Tracker.Reserve/Release,
+ * tracker.go:53,73); WG_E_NOMEM when over budget, nothing reserved then. */
+WG_API wg_status wg_ledger_reserve(wg_ctx* ctx, int64_t bytes);
+WG_API wg_status wg_ledger_release(wg_ctx* ctx, int64_t bytes);
+/* The CUDA stream (cudaStream_t) the context launches on, for callers that
+ * order their own work against it. */
+WG_API void*     wg_ctx_stream(wg_ctx* ctx);
+/* Number of kernels this context has launched since creation. */
+WG_API int64_t   wg_ctx_launch_count(wg_ctx* ctx);
+
+/* ======================================================================== */
+/* Filter: exec.KernelFilter (internal/engine/exec/filter.go:347-425) with    */
+/* kernel.ResolveFilterKernel / compareFilterImpl (kernel/compare.go:47,145)  */
+/* ======================================================================== */
+
+/* Bind a predicate on column `col_idx`; the typed kernel is resolved on the
+ * first execute from that column's type (KernelFilter.Execute, filter.go:373). */
+WG_API wg_status wg_filter_create(wg_ctx* ctx, int32_t col_idx, int32_t op,
+                           int32_t const_kind, int64_t const_i64, double const_f64,
+                           wg_filter** out);
+/* Host batch in, ascending selection out (out_sel must hold in->sel_len rows if
+ * in->sel, else in->len). *out_n = 0 means "fully filtered": the Go wrapper
+ * returns a nil batch (filter.go:420). Nulls never match (compare.go:53-60). */
+WG_API wg_status wg_filter_execute(wg_filter* f, const wg_batch_desc* in,
+                            uint32_t* out_sel, int64_t* out_n);
+/* Device batch in, device selection out; *out_n is read back to the host. */
+WG_API wg_status wg_filter_execute_device(wg_filter* f, const wg_batch_desc* in,
+                                   uint32_t* out_sel_dev, int64_t* out_n);
+WG_API wg_status wg_filter_destroy(wg_filter* f);
+
+/* ======================================================================== */
+/* Hash join: exec.HashJoin / HashJoinProbe (internal/engine/exec/join.go)   */
+/* ======================================================================== */
+
+/* Inner equi-join on one integer-class key column (tryEnableIntKey,
+ * join.go:520). build_key_col indexes the build batches; probe_key_col the
+ * probe batches; payload_cols are build columns carried to the output.
+ * build_row_hint pre-sizes the build buffers (HashJoin.BuildRowHint). */
+WG_API wg_status wg_join_create(wg_ctx* ctx, int32_t join_type, int32_t build_key_col,
+                         int32_t probe_key_col, int32_t n_payload,
+                         const int32_t* payload_cols, int64_t build_row_hint,
+                         wg_join** out);
+/* Append one build batch (the per-batch arenaAppendInt loop, join.go:551). */
+WG_API wg_status wg_join_build_append(wg_join* j, const wg_batch_desc* build);
+WG_API wg_status wg_join_build_append_device(wg_join* j, const wg_batch_desc* build);
+/* Build the device hash index over everything appended (end of
+ * HashJoin.Build, join.go:771). Null keys never join. */
+WG_API wg_status wg_join_build_finish(wg_join* j);
+/* Number of build rows stored and number of distinct keys indexed. */
+WG_API wg_status wg_join_build_stats(wg_join* j, int64_t* build_rows, int64_t* distinct_keys);
+/* HashJoinProbe.Execute → inlineIntProbe (join.go:2306,2670), bounded output
+ * (BoundedOutputOperator, operators.go:86): emits at most `cap` match pairs
+ * (probe_row, build_row) ordered by probe position, starting at probe position
+ * *cursor (0 on the first call). On return *cursor is the next position to
+ * resume from (== active rows when done) and *out_n the number of pairs. */
+WG_API wg_status wg_join_probe(wg_join* j, const wg_batch_desc* probe,
+                        uint32_t* out_probe_rows, int64_t* out_build_rows,
+                        int64_t cap, int64_t* cursor, int64_t* out_n);
+/* Gather build payload column `payload_idx` for `n` build rows
+ * (gatherVector, exec/sort.go:611). out/out_valid are host buffers
+ * (out_valid may be NULL; it receives one byte per row, 1 = valid). */
+WG_API wg_status wg_join_gather(wg_join* j, int32_t payload_idx, const int64_t* build_rows,
+                         int64_t n, void* out, uint8_t* out_valid);
+/* Forget the build side so the handle can build again (a fresh HashJoin for the
+ * next query over the same plan); device buffers are kept for reuse. */
+WG_API wg_status wg_join_reset(wg_join* j);
+WG_API wg_status wg_join_destroy(wg_join* j);
+
+/* ======================================================================== */
+/* Hash aggregate: exec.HashAggregate (internal/engine/exec/aggregate.go)     */
+/* ======================================================================== */
+
+/* GROUP BY key_cols with aggs (NewHashAggregate, aggregate.go:1023). One
+ * integer-class key column takes the int-key path (aggregate.go:1544); 2-4
+ * integer-class columns of at most 16 bytes take the packed path
+ * (aggregate.go:1596, packed_hash.go:386). group_ndv_hint pre-sizes the device
+ * table (HashAggregate.GroupNDVHint); 0 = grow on demand. */
+WG_API wg_status wg_agg_create(wg_ctx* ctx, int32_t n_keys, const int32_t* key_cols,
+                        int32_t n_aggs, const wg_agg_spec* aggs,
+                        int64_t group_ndv_hint, wg_agg** out);
+/* HashAggregate.Consume (aggregate.go:1075) of a host / device batch. */
+WG_API wg_status wg_agg_consume(wg_agg* a, const wg_batch_desc* in);
+WG_API wg_status wg_agg_consume_device(wg_agg* a, const wg_batch_desc* in);
+/* CloneSink / MergeSink (aggregate.go:4646,4682): a fresh handle of the same
+ * shape, and folding src's groups into dst (src is left untouched). */
+WG_API wg_status wg_agg_clone(wg_agg* a, wg_agg** out);
+WG_API wg_status wg_agg_merge(wg_agg* dst, wg_agg* src);
+/* Finalize (aggregate.go:3855): no more input; *n_groups = output rows. */
+WG_API wg_status wg_agg_finalize(wg_agg* a, int64_t* n_groups);
+/* Next (aggregate.go:4202): finalized rows [start, start+max_rows) into host
+ * columns out_cols[0..n_keys+n_aggs) — keys in their input types, then one
+ * column per aggregate in its output type. out_cols[i].data / valid_words
+ * point at caller buffers (valid_words may be NULL when the caller does not
+ * want null bits; bit layout as batch.Bitmap). *n_out = rows written. */
+WG_API wg_status wg_agg_emit(wg_agg* a, int64_t start, int64_t max_rows,
+                      wg_column* out_cols, int64_t* n_out);
+/* Raw accumulator state of every group, for bit-exact checks. */
+WG_API wg_status wg_agg_export(wg_agg* a, const wg_group_export* out);
+/* Forget all groups and input (the state after wg_agg_create). */
+WG_API wg_status wg_agg_reset(wg_agg* a);
+WG_API wg_status wg_agg_destroy(wg_agg* a);
+
+/* ======================================================================== */
+/* Fused pipeline: Pipeline.Run (exec/pipeline.go:81) over                    */
+/* KernelFilter* → HashJoinProbe → Project → HashAggregate in one kernel      */
+/* ======================================================================== */
+
+/* Virtual schema seen by the aggregate: input columns [0, ncols), then the
+ * join's payload columns, then one column per expression. Filters apply to
+ * input columns before the probe (the planner's pushdown order, plan.go:5750). */
+typedef struct wg_pipeline_desc {
+  const wg_batch_desc* input;
+  int32_t              n_filters;
+  int32_t              n_exprs;
+  const wg_predicate*  filters;
+  wg_join*             join;       /* NULL = no join; probe key = join's probe_key_col */
+  const wg_expr*       exprs;
+  wg_agg*              agg;        /* sink; must not be finalized */
+} wg_pipeline_desc;
+
+/* Run one pass of the pipeline over a host-resident input (staged to HBM in
+ * chunks that overlap copies with the kernel) or a device-resident input. */
+WG_API wg_status wg_pipeline_run(wg_ctx* ctx, const wg_pipeline_desc* p);
+WG_API wg_status wg_pipeline_run_device(wg_ctx* ctx, const wg_pipeline_desc* p);
+
+/* ======================================================================== */
+/* Synthetic benchmark tables, generated in HBM (include/wadjet_synth.h).    */
+/* No counterpart in the reference, whose benchmarks fill batches with       */
+/* SetValue loops (internal/engine/exec/bench_test.go). Rows [row0, row0+n)  */
+/* of each column are written to device pointers; NULL skips a column.       */
+/* ======================================================================== */
+WG_API wg_status wg_synth_starjoin_fact(wg_ctx* ctx, uint64_t seed, int64_t row0, int64_t n, int32_t* fk,
+                                        int32_t* qty, wg_int128* price, double* disc);
+WG_API wg_status wg_synth_starjoin_dim(wg_ctx* ctx, uint64_t seed, int64_t n, int32_t* key, int32_t* grp);
+WG_API wg_status wg_synth_groupby(wg_ctx* ctx, uint64_t seed, int64_t row0, int64_t n, int64_t ngroups,
+                                  int64_t* k, int64_t* v, double* f, int32_t* flag);
+WG_API wg_status wg_synth_highcard(wg_ctx* ctx, uint64_t seed, int64_t row0, int64_t n, int32_t* a, int64_t* b,
+                                   wg_int128* amt, double* x);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* WADJET_GPU_H */

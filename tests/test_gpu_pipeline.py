@@ -1,0 +1,155 @@
+"""The fused filter → probe → project → aggregate kernel against the oracle's
+Pipeline.Run on the benchmark workloads, plus size-independent properties at
+the full 2^28-row star-join size."""
+import numpy as np
+import pytest
+
+from oracle import binding as ob
+from tests.helpers import DEC_DTYPE, assert_groups_equal
+
+pytestmark = pytest.mark.gpu
+
+I32, I64, F64, DEC = 1, 2, 4, 17
+
+
+def to_host_dec(t):
+    return t.cpu().numpy().reshape(-1).view(DEC_DTYPE)
+
+
+def starjoin_plan(wg):
+    expr = wg.Expr(F64, [wg.Expr.col(2), wg.Expr.const_f(1.0), wg.Expr.col(3), "-", "*"])
+    aggs = [wg.AggColumn(wg.AGG_SUM, 5), wg.AggColumn(wg.AGG_SUM, 2)]
+    return expr, aggs
+
+
+def test_device_generator_matches_host_generator(ctx):
+    from wadjet_b200 import synth
+    n, row0 = 100_000, 12_345
+    fk, qty, price, disc = synth.starjoin_fact(ctx, n, row0=row0)
+    hfk, hqty, hprice, hdisc = ob.gen_starjoin_fact(n, row0=row0)
+    np.testing.assert_array_equal(fk.cpu().numpy(), hfk)
+    np.testing.assert_array_equal(qty.cpu().numpy(), hqty)
+    np.testing.assert_array_equal(to_host_dec(price), hprice)
+    np.testing.assert_array_equal(disc.cpu().numpy().view(np.uint64), hdisc.view(np.uint64))
+    key, grp = synth.starjoin_dim(ctx)
+    hkey, hgrp = ob.gen_starjoin_dim()
+    np.testing.assert_array_equal(key.cpu().numpy(), hkey)
+    np.testing.assert_array_equal(grp.cpu().numpy(), hgrp)
+    a, b, amt, x = synth.highcard(ctx, n, row0=row0)
+    ha, hb, hamt, hx = ob.gen_highcard(n, row0=row0)
+    np.testing.assert_array_equal(a.cpu().numpy(), ha)
+    np.testing.assert_array_equal(b.cpu().numpy(), hb)
+    np.testing.assert_array_equal(to_host_dec(amt), hamt)
+    np.testing.assert_array_equal(x.cpu().numpy().view(np.uint64), hx.view(np.uint64))
+    k, v, f, flag = synth.groupby(ctx, n, row0=row0)
+    hk, hv, hf, hflag = ob.gen_groupby(n, row0=row0)
+    for g, h in ((k, hk), (v, hv), (flag, hflag)):
+        np.testing.assert_array_equal(g.cpu().numpy(), h)
+    np.testing.assert_array_equal(f.cpu().numpy().view(np.uint64), hf.view(np.uint64))
+
+
+def test_groupby_workload_matches_oracle(ctx):
+    """SELECT k, SUM(v), COUNT(*), MIN(f), MAX(f) FROM t WHERE flag < 7 GROUP BY k, 2^20 rows."""
+    import wadjet_b200 as wg
+    from wadjet_b200 import synth
+    n = 1 << 20
+    k, v, f, flag = synth.groupby(ctx, n)
+    aggs = [wg.AggColumn(wg.AGG_SUM, 1), wg.AggColumn(wg.AGG_COUNT, -1), wg.AggColumn(wg.AGG_MIN, 2),
+            wg.AggColumn(wg.AGG_MAX, 2)]
+    g = wg.HashAggregate(ctx, [0], aggs, ndv_hint=4096)
+    batch = wg.Batch([wg.Column(I64, k), wg.Column(I64, v), wg.Column(F64, f), wg.Column(I32, flag)])
+    wg.run_pipeline(ctx, batch, g, filters=[(3, wg.OP_LT, 7)], device=True)
+    g.finalize()
+    hk, hv, hf, hflag = (t.cpu().numpy() for t in (k, v, f, flag))
+    o = ob.Agg([0], [(0, 1, 0), (1, -1, 0), (2, 2, 0), (3, 2, 0)])
+    ob.pipeline(ob.HostBatch([(I64, hk, None, 0), (I64, hv, None, 0), (F64, hf, None, 0), (I32, hflag, None, 0)]),
+                o, filters=[(3, wg.OP_LT, 7)], threads=8)
+    assert_groups_equal(g.export(), o.export(), ["sum_i", "count", "min_f", "max_f"])
+    g.close()
+
+
+@pytest.mark.parametrize("host_input", [False, True])
+def test_starjoin_workload_matches_oracle(ctx, host_input):
+    """Star join + aggregate, 2^22 fact rows against the full 2^22-row dimension."""
+    import wadjet_b200 as wg
+    from wadjet_b200 import synth
+    n = 1 << 22
+    fk, qty, price, disc = synth.starjoin_fact(ctx, n)
+    key, grp = synth.starjoin_dim(ctx)
+    j = wg.HashJoin(ctx, 0, 0, payload=[1], build_row_hint=1 << 22)
+    j.build([wg.Batch([wg.Column(I32, key), wg.Column(I32, grp)])], device=True)
+    expr, aggs = starjoin_plan(wg)
+    g = wg.HashAggregate(ctx, [4], aggs, ndv_hint=1000)
+    hfk, hqty, hprice, hdisc = fk.cpu().numpy(), qty.cpu().numpy(), to_host_dec(price), disc.cpu().numpy()
+    if host_input:
+        batch = wg.Batch([wg.Column(I32, hfk), wg.Column(I32, hqty), wg.Column(DEC, hprice, scale=2),
+                          wg.Column(F64, hdisc)])
+    else:
+        batch = wg.Batch([wg.Column(I32, fk), wg.Column(I32, qty), wg.Column(DEC, price, scale=2),
+                          wg.Column(F64, disc)])
+    wg.run_pipeline(ctx, batch, g, filters=[(1, wg.OP_GT, 10)], join=j, exprs=[expr], device=not host_input)
+    g.finalize()
+    hkey, hgrp = key.cpu().numpy(), grp.cpu().numpy()
+    oj = ob.Join(1 << 22)
+    oj.append(I32, hkey)
+    o = ob.Agg([4], [(0, 5, 0), (0, 2, 0)])
+    ob.pipeline(ob.HostBatch([(I32, hfk, None, 0), (I32, hqty, None, 0), (DEC, hprice, None, 2), (F64, hdisc, None, 0)]),
+                o, filters=[(1, wg.OP_GT, 10)], join=oj, probe_key=0,
+                build=ob.HostBatch([(I32, hkey, None, 0), (I32, hgrp, None, 0)]), payload=[1],
+                exprs=[ob.expr(F64, [("col", 2), ("cf", 1.0), ("col", 3), "-", "*"])], threads=8)
+    assert_groups_equal(g.export(), o.export(), ["sum_f", "sum_d"])
+    g.close()
+    j.close()
+
+
+def test_highcard_workload_matches_oracle(ctx):
+    """GROUP BY (a int32, b int64) packed key, 2^22 rows (~3.9M groups)."""
+    import wadjet_b200 as wg
+    from wadjet_b200 import synth
+    n = 1 << 22
+    a, b, amt, x = synth.highcard(ctx, n)
+    aggs = [wg.AggColumn(wg.AGG_SUM, 2), wg.AggColumn(wg.AGG_COUNT, -1), wg.AggColumn(wg.AGG_MIN, 3),
+            wg.AggColumn(wg.AGG_MAX, 3)]
+    g = wg.HashAggregate(ctx, [0, 1], aggs, ndv_hint=1 << 22)
+    batch = wg.Batch([wg.Column(I32, a), wg.Column(I64, b), wg.Column(DEC, amt, scale=2), wg.Column(F64, x)])
+    wg.run_pipeline(ctx, batch, g, device=True)
+    g.finalize()
+    ha, hb, hamt, hx = a.cpu().numpy(), b.cpu().numpy(), to_host_dec(amt), x.cpu().numpy()
+    o = ob.Agg([0, 1], [(0, 2, 0), (1, -1, 0), (2, 3, 0), (3, 3, 0)])
+    ob.pipeline(ob.HostBatch([(I32, ha, None, 0), (I64, hb, None, 0), (DEC, hamt, None, 2), (F64, hx, None, 0)]),
+                o, threads=8)
+    assert_groups_equal(g.export(), o.export(), ["sum_d", "count", "min_f", "max_f"])
+    g.close()
+
+
+def test_starjoin_full_size_properties(ctx):
+    """2^28 fact rows: per-group COUNT sums to the filtered row count and the exact
+    DECIMAL SUM(price) over all groups equals the sum over the filtered rows."""
+    import torch
+    import wadjet_b200 as wg
+    from wadjet_b200 import synth
+    n = 1 << 28
+    fk, qty, price, disc = synth.starjoin_fact(ctx, n)
+    key, grp = synth.starjoin_dim(ctx)
+    j = wg.HashJoin(ctx, 0, 0, payload=[1], build_row_hint=1 << 22)
+    j.build([wg.Batch([wg.Column(I32, key), wg.Column(I32, grp)])], device=True)
+    expr, aggs = starjoin_plan(wg)
+    aggs = aggs + [wg.AggColumn(wg.AGG_COUNT, -1)]
+    g = wg.HashAggregate(ctx, [4], aggs, ndv_hint=1000)
+    batch = wg.Batch([wg.Column(I32, fk), wg.Column(I32, qty), wg.Column(DEC, price, scale=2), wg.Column(F64, disc)])
+    wg.run_pipeline(ctx, batch, g, filters=[(1, wg.OP_GT, 10)], join=j, exprs=[expr], device=True)
+    g.finalize()
+    e = g.export()
+    keep = qty > 10
+    want_rows = int(keep.sum().item())
+    want_price = int(price[:, 1][keep].sum().item())  # every price fits int64 and so does the total
+    assert int(e["count"][2].sum()) == want_rows
+    assert e["keys"].shape[1] == 1000
+    dec = e["dec"][1]
+    assert (dec["hi"] == 0).all()
+    assert int(dec["lo"].astype(object).sum()) == want_price
+    assert np.all(e["f64"][0] > 0)
+    del fk, qty, price, disc
+    torch.cuda.empty_cache()
+    g.close()
+    j.close()

@@ -1,0 +1,476 @@
+"""wadjet_b200 — Wadjet's filter → hash-join → hash-aggregate path on the B200.
+
+A host-side mirror of the reference's operator contract
+(internal/engine/exec/operators.go) over the C ABI of libwadjetgpu.so:
+
+- ``KernelFilter``  — exec.KernelFilter (exec/filter.go:347): typed ``col OP const``
+  that compacts the selection vector; ``None`` means "fully filtered".
+- ``HashJoin``      — exec.HashJoin inner int-key join (exec/join.go:42): build,
+  then bounded-output probe returning (probe_row, build_row) pairs.
+- ``HashAggregate`` — exec.HashAggregate (exec/aggregate.go:98): consume batches,
+  CloneSink / MergeSink, Finalize, then ``next()`` pages of 2048 rows.
+- ``run_pipeline``  — Pipeline.Run (exec/pipeline.go:81) fused into one kernel.
+
+Columns are numpy arrays (host) or torch CUDA tensors (device). DECIMAL values
+use ``DEC_DTYPE`` = (hi int64, lo uint64), Go's batch.Int128 field order.
+Every compute call runs on the GPU through the shared library; there is no CPU
+fallback, and a missing library raises at import.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import Iterable, Optional, Sequence
+
+import numpy as np
+
+from . import _abi as abi
+from ._abi import (AGG_AVG, AGG_COUNT, AGG_MAX, AGG_MIN, AGG_SUM, CONST_FLOAT, CONST_INT, OP_EQ, OP_GE, OP_GT,
+                   OP_LE, OP_LT, OP_NE, TYPE_DATE, TYPE_DECIMAL, TYPE_DURATION, TYPE_FLOAT32, TYPE_FLOAT64,
+                   TYPE_INT32, TYPE_INT64, TYPE_IPV4, TYPE_MAC, TYPE_PORT, TYPE_PROTOCOL, TYPE_TIMESTAMP)
+
+__all__ = [
+    "Context", "Column", "Batch", "KernelFilter", "HashJoin", "HashAggregate", "AggColumn", "Expr", "run_pipeline",
+    "WadjetGPUError", "MemoryExceeded", "DEC_DTYPE", "lib",
+]
+
+DEC_DTYPE = np.dtype([("hi", "<i8"), ("lo", "<u8")])
+BATCH_SIZE = 2048  # batch.DefaultBatchSize (internal/engine/batch/batch.go:6)
+
+class _Lib:
+    """The loaded libwadjetgpu.so, opened on first use (so `python -m wadjet_b200.build`
+    can run before the library exists). A missing library raises; nothing falls back."""
+
+    def __getattr__(self, name):
+        return getattr(abi.load(), name)
+
+
+lib = _Lib()
+
+_ELEM = {TYPE_INT32: 4, TYPE_PORT: 4, TYPE_PROTOCOL: 4, TYPE_DATE: 4, TYPE_FLOAT32: 4, TYPE_INT64: 8,
+         TYPE_TIMESTAMP: 8, TYPE_IPV4: 8, TYPE_MAC: 8, TYPE_DURATION: 8, TYPE_FLOAT64: 8, TYPE_DECIMAL: 16}
+_NP = {TYPE_INT32: np.int32, TYPE_PORT: np.int32, TYPE_PROTOCOL: np.int32, TYPE_DATE: np.int32,
+       TYPE_FLOAT32: np.float32, TYPE_INT64: np.int64, TYPE_TIMESTAMP: np.int64, TYPE_IPV4: np.int64,
+       TYPE_MAC: np.int64, TYPE_DURATION: np.int64, TYPE_FLOAT64: np.float64, TYPE_DECIMAL: DEC_DTYPE}
+
+
+class WadjetGPUError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"wadjet-gpu status {status}: {msg}")
+        self.status = status
+
+
+class MemoryExceeded(WadjetGPUError):
+    """memory.ErrMemoryExceeded (internal/engine/memory/tracker.go:15)."""
+
+
+def _check(status: int) -> None:
+    if status != abi.WG_OK:
+        msg = (lib.wg_last_error() or b"").decode()
+        if status == abi.WG_E_NOMEM:
+            raise MemoryExceeded(status, msg)
+        raise WadjetGPUError(status, msg)
+
+
+def pack_validity(valid: np.ndarray) -> np.ndarray:
+    """bool per row (True = valid) → batch.Bitmap words (bit 1 = valid, LSB first)."""
+    valid = np.asarray(valid, dtype=bool)
+    b = np.packbits(valid, bitorder="little")
+    pad = (-len(b)) % 8
+    if pad:
+        b = np.concatenate([b, np.zeros(pad, np.uint8)])
+    return b.view(np.uint64).copy()
+
+
+def unpack_validity(words: np.ndarray, n: int) -> np.ndarray:
+    return np.unpackbits(np.asarray(words, np.uint64).view(np.uint8), bitorder="little")[:n].astype(bool)
+
+
+def _is_torch(x) -> bool:
+    return type(x).__module__.startswith("torch")
+
+
+@dataclass
+class Column:
+    """One batch.Vector: typed data plus optional validity (True = valid)."""
+    type_id: int
+    data: object                      # numpy array or torch tensor
+    valid: Optional[object] = None    # numpy bool array / torch uint64 words on device
+    scale: int = 0
+
+    def __len__(self) -> int:
+        return int(self.data.shape[0])
+
+    def _desc(self, keep: list) -> abi.wg_column:
+        if _is_torch(self.data):
+            ptr = self.data.data_ptr()
+            vptr = self.valid.data_ptr() if self.valid is not None else None
+        else:
+            arr = np.ascontiguousarray(self.data)
+            keep.append(arr)
+            ptr = arr.ctypes.data
+            vptr = None
+            if self.valid is not None:
+                w = pack_validity(self.valid) if np.asarray(self.valid).dtype == bool else np.asarray(self.valid, np.uint64)
+                keep.append(w)
+                vptr = w.ctypes.data
+        return abi.wg_column(self.type_id, self.scale, ptr, vptr, len(self))
+
+
+class Batch:
+    """batch.RecordBatch: columns plus an optional selection vector (ascending row ids)."""
+
+    def __init__(self, cols: Sequence[Column], sel=None, length: Optional[int] = None):
+        self.cols = list(cols)
+        self.sel = sel
+        self.len = length if length is not None else (len(self.cols[0]) if self.cols else 0)
+
+    def desc(self) -> tuple[abi.wg_batch_desc, list]:
+        keep: list = []
+        arr = (abi.wg_column * max(1, len(self.cols)))(*[c._desc(keep) for c in self.cols])
+        keep.append(arr)
+        sel_ptr, sel_len = None, 0
+        if self.sel is not None:
+            if _is_torch(self.sel):
+                sel_ptr, sel_len = self.sel.data_ptr(), int(self.sel.shape[0])
+            else:
+                s = np.ascontiguousarray(self.sel, dtype=np.uint32)
+                keep.append(s)
+                sel_ptr, sel_len = s.ctypes.data, len(s)
+        d = abi.wg_batch_desc(len(self.cols), 0, arr, self.len, sel_ptr, sel_len)
+        keep.append(d)
+        return d, keep
+
+
+class Context:
+    """Device, stream and HBM ledger (memory.Tracker over device bytes)."""
+
+    def __init__(self, device: int = 0, hbm_budget: int = 0, pinned_spill: int = 0):
+        h = C.c_void_p()
+        _check(lib.wg_ctx_create(device, hbm_budget, pinned_spill, C.byref(h)))
+        self.h = h
+
+    def close(self) -> None:
+        if self.h:
+            lib.wg_ctx_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def synchronize(self) -> None:
+        _check(lib.wg_ctx_synchronize(self.h))
+
+    def ledger(self) -> dict:
+        u, p, b = C.c_int64(), C.c_int64(), C.c_int64()
+        _check(lib.wg_ledger_stats(self.h, C.byref(u), C.byref(p), C.byref(b)))
+        return {"used": u.value, "peak": p.value, "budget": b.value}
+
+    def reserve(self, n: int) -> None:
+        _check(lib.wg_ledger_reserve(self.h, n))
+
+    def release(self, n: int) -> None:
+        _check(lib.wg_ledger_release(self.h, n))
+
+    @property
+    def stream(self) -> int:
+        return lib.wg_ctx_stream(self.h) or 0
+
+    @property
+    def launches(self) -> int:
+        return int(lib.wg_ctx_launch_count(self.h))
+
+
+def _const(value) -> tuple[int, int, float]:
+    if isinstance(value, (float, np.floating)):
+        return CONST_FLOAT, 0, float(value)
+    return CONST_INT, int(value), 0.0
+
+
+class KernelFilter:
+    """exec.KernelFilter: `batch.cols[col] OP value`; returns the compacted selection."""
+
+    def __init__(self, ctx: Context, col: int, op: int, value):
+        self.ctx = ctx
+        kind, i, f = _const(value)
+        h = C.c_void_p()
+        _check(lib.wg_filter_create(ctx.h, col, op, kind, i, f, C.byref(h)))
+        self.h = h
+
+    def execute(self, batch: Batch) -> Optional[np.ndarray]:
+        d, keep = batch.desc()
+        n_items = len(batch.sel) if batch.sel is not None else batch.len
+        out = np.empty(max(1, n_items), np.uint32)
+        n = C.c_int64()
+        _check(lib.wg_filter_execute(self.h, C.byref(d), out.ctypes.data, C.byref(n)))
+        return None if n.value == 0 else out[: n.value].copy()
+
+    def execute_device(self, batch: Batch, out_sel) -> int:
+        d, keep = batch.desc()
+        n = C.c_int64()
+        _check(lib.wg_filter_execute_device(self.h, C.byref(d), out_sel.data_ptr(), C.byref(n)))
+        return n.value
+
+    def close(self) -> None:
+        if self.h:
+            lib.wg_filter_destroy(self.h)
+            self.h = None
+
+
+class HashJoin:
+    """exec.HashJoin (inner, one integer-class key) + HashJoinProbe."""
+
+    def __init__(self, ctx: Context, build_key: int, probe_key: int, payload: Sequence[int] = (),
+                 build_row_hint: int = 0):
+        self.ctx = ctx
+        self.payload = list(payload)
+        self.payload_types: list[int] = []
+        pay = (C.c_int32 * max(1, len(payload)))(*payload)
+        h = C.c_void_p()
+        _check(lib.wg_join_create(ctx.h, abi.JOIN_INNER, build_key, probe_key, len(payload), pay, build_row_hint,
+                                  C.byref(h)))
+        self.h = h
+
+    def build(self, batches: Iterable[Batch], device: bool = False) -> None:
+        for b in batches:
+            if not self.payload_types:
+                self.payload_types = [b.cols[p].type_id for p in self.payload]
+            d, keep = b.desc()
+            fn = lib.wg_join_build_append_device if device else lib.wg_join_build_append
+            _check(fn(self.h, C.byref(d)))
+        _check(lib.wg_join_build_finish(self.h))
+
+    def reset(self) -> None:
+        """Forget the build side (device buffers are kept for the next build)."""
+        _check(lib.wg_join_reset(self.h))
+
+    def stats(self) -> tuple[int, int]:
+        r, k = C.c_int64(), C.c_int64()
+        _check(lib.wg_join_build_stats(self.h, C.byref(r), C.byref(k)))
+        return r.value, k.value
+
+    def probe(self, batch: Batch, cap: int = 16 * BATCH_SIZE):
+        """Yield (probe_rows uint32, build_rows int64) chunks of at most `cap` pairs."""
+        d, keep = batch.desc()
+        cursor = C.c_int64(0)
+        while True:
+            pr = np.empty(max(1, cap), np.uint32)
+            br = np.empty(max(1, cap), np.int64)
+            n = C.c_int64()
+            _check(lib.wg_join_probe(self.h, C.byref(d), pr.ctypes.data, br.ctypes.data, cap, C.byref(cursor),
+                                     C.byref(n)))
+            if n.value > 0:
+                yield pr[: n.value].copy(), br[: n.value].copy()
+            if n.value < cap:
+                return
+
+    def gather(self, payload_idx: int, build_rows: np.ndarray, dtype) -> tuple[np.ndarray, np.ndarray]:
+        rows = np.ascontiguousarray(build_rows, np.int64)
+        out = np.empty(max(1, len(rows)), dtype)
+        valid = np.empty(max(1, len(rows)), np.uint8)
+        _check(lib.wg_join_gather(self.h, payload_idx, rows.ctypes.data, len(rows), out.ctypes.data,
+                                  valid.ctypes.data))
+        return out[: len(rows)], valid[: len(rows)].astype(bool)
+
+    def close(self) -> None:
+        if self.h:
+            lib.wg_join_destroy(self.h)
+            self.h = None
+
+
+@dataclass
+class AggColumn:
+    """exec.AggColumn: func, input column (-1 = COUNT(*)), declared output type (0 = default)."""
+    func: int
+    input_col: int = -1
+    out_type: int = 0
+
+
+class HashAggregate:
+    """exec.HashAggregate over the device hash table."""
+
+    def __init__(self, ctx: Context, group_by: Sequence[int], aggs: Sequence[AggColumn], ndv_hint: int = 0,
+                 _handle=None):
+        self.ctx = ctx
+        self.group_by = list(group_by)
+        self.aggs = list(aggs)
+        self.ndv_hint = ndv_hint
+        self._key_types: Optional[list[int]] = None
+        if _handle is not None:
+            self.h = _handle
+            return
+        keys = (C.c_int32 * max(1, len(group_by)))(*group_by)
+        specs = (abi.wg_agg_spec * max(1, len(aggs)))(*[abi.wg_agg_spec(a.func, a.input_col, a.out_type, 0)
+                                                        for a in aggs])
+        h = C.c_void_p()
+        _check(lib.wg_agg_create(ctx.h, len(group_by), keys, len(aggs), specs, ndv_hint, C.byref(h)))
+        self.h = h
+        self._out_pos = 0
+        self._n_groups = None
+
+    def consume(self, batch: Batch, device: bool = False) -> None:
+        if self._key_types is None:
+            self._key_types = [batch.cols[k].type_id for k in self.group_by]
+            self._in_types = [batch.cols[a.input_col].type_id if a.input_col >= 0 else None for a in self.aggs]
+        d, keep = batch.desc()
+        _check((lib.wg_agg_consume_device if device else lib.wg_agg_consume)(self.h, C.byref(d)))
+
+    def clone_sink(self) -> "HashAggregate":
+        h = C.c_void_p()
+        _check(lib.wg_agg_clone(self.h, C.byref(h)))
+        c = HashAggregate(self.ctx, self.group_by, self.aggs, self.ndv_hint, _handle=h)
+        c._out_pos, c._n_groups = 0, None
+        return c
+
+    def merge_sink(self, other: "HashAggregate") -> None:
+        _check(lib.wg_agg_merge(self.h, other.h))
+        if self._key_types is None and other._key_types is not None:
+            self._key_types, self._in_types = other._key_types, other._in_types
+
+    def finalize(self) -> int:
+        n = C.c_int64()
+        _check(lib.wg_agg_finalize(self.h, C.byref(n)))
+        self._n_groups = n.value
+        self._out_pos = 0
+        return n.value
+
+    def reset(self) -> None:
+        _check(lib.wg_agg_reset(self.h))
+        self._n_groups = None
+        self._out_pos = 0
+
+    def export(self) -> dict:
+        """Raw accumulator state of every group (keys widened to int64)."""
+        n = self._n_groups if self._n_groups is not None else self.finalize()
+        nk, na = len(self.group_by), len(self.aggs)
+        r = {"keys": np.zeros((nk, n), np.int64), "key_valid": np.zeros((nk, n), np.uint8),
+             "count": np.zeros((na, n), np.int64), "i64": np.zeros((na, n), np.int64),
+             "f64": np.zeros((na, n), np.float64), "dec": np.zeros((na, n), DEC_DTYPE),
+             "has": np.zeros((na, n), np.uint8)}
+        if n == 0:
+            return r
+        e = abi.wg_group_export(*[r[k].ctypes.data if r[k].size else None
+                                  for k in ("keys", "key_valid", "count", "i64", "f64", "dec", "has")])
+        _check(lib.wg_agg_export(self.h, C.byref(e)))
+        return r
+
+    def output_types(self) -> list[int]:
+        key_types = self._key_types or [TYPE_INT64] * len(self.group_by)
+        outs = []
+        for i, a in enumerate(self.aggs):
+            if a.out_type:
+                outs.append(a.out_type)
+            elif a.func == AGG_COUNT:
+                outs.append(TYPE_INT64)
+            elif a.func in (AGG_SUM, AGG_AVG):
+                outs.append(TYPE_FLOAT64)
+            else:
+                t = self._in_types[i] if self._key_types is not None else None
+                outs.append(TYPE_FLOAT64 if t in (TYPE_FLOAT32, TYPE_FLOAT64, TYPE_DECIMAL, None) else TYPE_INT64)
+        return [t if _ELEM.get(t) == 4 else (TYPE_INT64 if t != TYPE_FLOAT64 else t) for t in key_types] + outs
+
+    def next(self, max_rows: int = BATCH_SIZE) -> Optional[list[tuple[np.ndarray, np.ndarray]]]:
+        """HashAggregate.Next: the next page of finalized rows as (values, valid) per column, or None."""
+        if self._n_groups is None:
+            self.finalize()
+        if self._out_pos >= self._n_groups:
+            return None
+        m = min(max_rows, self._n_groups - self._out_pos)
+        types = self.output_types()
+        bufs, words = [], []
+        cols = (abi.wg_column * len(types))()
+        for i, t in enumerate(types):
+            b = np.zeros(m, np.int32 if _ELEM.get(t) == 4 else (np.float64 if t == TYPE_FLOAT64 else np.int64))
+            w = np.zeros((m + 63) // 64, np.uint64)
+            bufs.append(b)
+            words.append(w)
+            cols[i] = abi.wg_column(t, 0, b.ctypes.data, w.ctypes.data, m)
+        n = C.c_int64()
+        _check(lib.wg_agg_emit(self.h, self._out_pos, m, cols, C.byref(n)))
+        self._out_pos += n.value
+        return [(b[: n.value], unpack_validity(w, n.value)) for b, w in zip(bufs, words)]
+
+    def collect(self) -> list[tuple[np.ndarray, np.ndarray]]:
+        """Every finalized row (all pages of next() concatenated)."""
+        pages = []
+        while True:
+            p = self.next(1 << 20)
+            if p is None:
+                break
+            pages.append(p)
+        if not pages:
+            types = self.output_types()
+            return [(np.zeros(0, np.int32 if _ELEM.get(t) == 4 else (np.float64 if t == TYPE_FLOAT64 else np.int64)),
+                     np.zeros(0, bool)) for t in types]
+        return [(np.concatenate([p[i][0] for p in pages]), np.concatenate([p[i][1] for p in pages]))
+                for i in range(len(pages[0]))]
+
+    def close(self) -> None:
+        if self.h:
+            lib.wg_agg_destroy(self.h)
+            self.h = None
+
+
+class Expr:
+    """Postfix projection program: Expr.float_([Expr.col(3), Expr.const_f(1.0), Expr.col(4), "-", "*"])."""
+
+    _OPS = {"+": abi.EXPR_ADD, "-": abi.EXPR_SUB, "*": abi.EXPR_MUL, "/": abi.EXPR_DIV, ">>": abi.EXPR_SHR,
+            "&": abi.EXPR_AND}
+
+    def __init__(self, result_type: int, program: Sequence):
+        self.result_type = result_type
+        self.program = list(program)
+
+    @staticmethod
+    def col(i: int):
+        return ("col", i)
+
+    @staticmethod
+    def const_i(v: int):
+        return ("ci", v)
+
+    @staticmethod
+    def const_f(v: float):
+        return ("cf", v)
+
+    def to_c(self) -> abi.wg_expr:
+        e = abi.wg_expr()
+        e.result_type = self.result_type
+        e.n_ops = len(self.program)
+        for k, op in enumerate(self.program):
+            if isinstance(op, str):
+                e.ops[k] = abi.wg_expr_op(self._OPS[op], 0, 0, 0.0)
+            elif op[0] == "col":
+                e.ops[k] = abi.wg_expr_op(abi.EXPR_COL, op[1], 0, 0.0)
+            elif op[0] == "ci":
+                e.ops[k] = abi.wg_expr_op(abi.EXPR_CONST_I, 0, int(op[1]), 0.0)
+            else:
+                e.ops[k] = abi.wg_expr_op(abi.EXPR_CONST_F, 0, 0, float(op[1]))
+        return e
+
+
+def predicate(col: int, op: int, value) -> abi.wg_predicate:
+    kind, i, f = _const(value)
+    return abi.wg_predicate(col, op, kind, 0, i, f)
+
+
+def run_pipeline(ctx: Context, batch: Batch, agg: HashAggregate, filters: Sequence = (),
+                 join: Optional[HashJoin] = None, exprs: Sequence[Expr] = (), device: bool = False) -> None:
+    """Pipeline.Run: KernelFilter* → HashJoinProbe → Project → HashAggregate in one kernel per window.
+
+    `filters` are (col, op, value) triples on input columns. The aggregate sees
+    the virtual schema [input columns, join payload columns, expressions].
+    """
+    d, keep = batch.desc()
+    preds = (abi.wg_predicate * max(1, len(filters)))(*[predicate(*f) for f in filters])
+    ex = (abi.wg_expr * max(1, len(exprs)))(*[e.to_c() for e in exprs])
+    if agg._key_types is None:
+        pay_types = getattr(join, "payload_types", [])
+        vtypes = [c.type_id for c in batch.cols] + list(pay_types) + [e.result_type for e in exprs]
+        agg._key_types = [vtypes[k] for k in agg.group_by]
+        agg._in_types = [vtypes[a.input_col] if a.input_col >= 0 else None for a in agg.aggs]
+    p = abi.wg_pipeline_desc(C.pointer(d), len(filters), len(exprs), preds, join.h if join else None, ex, agg.h)
+    _check((lib.wg_pipeline_run_device if device else lib.wg_pipeline_run)(ctx.h, C.byref(p)))

@@ -1,0 +1,138 @@
+"""ctypes declarations of include/wadjet_gpu.h (the C ABI of libwadjetgpu.so)."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libwadjetgpu.so")
+
+# status codes
+WG_OK, WG_E_NOMEM, WG_E_INVALID, WG_E_TIMEOUT, WG_E_CUDA, WG_E_UNSUPPORTED, WG_E_STATE = range(7)
+
+# parquet.TypeID values (internal/storage/parquet/schema.go:13-34)
+TYPE_BOOL, TYPE_INT32, TYPE_INT64, TYPE_FLOAT32, TYPE_FLOAT64 = 0, 1, 2, 3, 4
+TYPE_STRING, TYPE_BYTES, TYPE_TIMESTAMP, TYPE_IPV4, TYPE_IPV6, TYPE_CIDR = 5, 6, 7, 8, 9, 10
+TYPE_MAC, TYPE_PORT, TYPE_PROTOCOL, TYPE_DURATION, TYPE_UUID, TYPE_DATE, TYPE_DECIMAL = 11, 12, 13, 14, 15, 16, 17
+
+# kernel.CompareOp
+OP_EQ, OP_NE, OP_LT, OP_LE, OP_GT, OP_GE = range(6)
+CONST_INT, CONST_FLOAT = 0, 1
+# exec.AggFunc
+AGG_SUM, AGG_COUNT, AGG_MIN, AGG_MAX, AGG_AVG = range(5)
+JOIN_INNER = 0
+# expression opcodes
+EXPR_COL, EXPR_CONST_I, EXPR_CONST_F, EXPR_ADD, EXPR_SUB, EXPR_MUL, EXPR_DIV, EXPR_SHR, EXPR_AND = range(9)
+EXPR_MAX_OPS = 12
+
+
+class wg_int128(C.Structure):
+    _fields_ = [("hi", C.c_int64), ("lo", C.c_uint64)]
+
+
+class wg_column(C.Structure):
+    _fields_ = [("type_id", C.c_int32), ("scale", C.c_int32), ("data", C.c_void_p),
+                ("valid_words", C.c_void_p), ("len", C.c_int64)]
+
+
+class wg_batch_desc(C.Structure):
+    _fields_ = [("ncols", C.c_int32), ("_pad", C.c_int32), ("cols", C.POINTER(wg_column)),
+                ("len", C.c_int64), ("sel", C.c_void_p), ("sel_len", C.c_int64)]
+
+
+class wg_agg_spec(C.Structure):
+    _fields_ = [("func", C.c_int32), ("input_col", C.c_int32), ("out_type", C.c_int32), ("_pad", C.c_int32)]
+
+
+class wg_predicate(C.Structure):
+    _fields_ = [("col", C.c_int32), ("op", C.c_int32), ("const_kind", C.c_int32), ("_pad", C.c_int32),
+                ("const_i64", C.c_int64), ("const_f64", C.c_double)]
+
+
+class wg_expr_op(C.Structure):
+    _fields_ = [("opcode", C.c_int32), ("arg", C.c_int32), ("imm_i64", C.c_int64), ("imm_f64", C.c_double)]
+
+
+class wg_expr(C.Structure):
+    _fields_ = [("result_type", C.c_int32), ("n_ops", C.c_int32), ("ops", wg_expr_op * EXPR_MAX_OPS)]
+
+
+class wg_group_export(C.Structure):
+    _fields_ = [("keys", C.c_void_p), ("key_valid", C.c_void_p), ("count", C.c_void_p), ("i64", C.c_void_p),
+                ("f64", C.c_void_p), ("dec", C.c_void_p), ("has", C.c_void_p)]
+
+
+class wg_pipeline_desc(C.Structure):
+    _fields_ = [("input", C.POINTER(wg_batch_desc)), ("n_filters", C.c_int32), ("n_exprs", C.c_int32),
+                ("filters", C.POINTER(wg_predicate)), ("join", C.c_void_p), ("exprs", C.POINTER(wg_expr)),
+                ("agg", C.c_void_p)]
+
+
+P = C.c_void_p
+PP = C.POINTER(C.c_void_p)
+I32, I64, F64 = C.c_int32, C.c_int64, C.c_double
+PI64 = C.POINTER(C.c_int64)
+
+# name -> (restype, argtypes); every symbol include/wadjet_gpu.h declares
+SIGNATURES = {
+    "wg_last_error": (C.c_char_p, []),
+    "wg_version": (C.c_char_p, []),
+    "wg_ctx_create": (I32, [I32, I64, I64, PP]),
+    "wg_ctx_destroy": (I32, [P]),
+    "wg_ctx_synchronize": (I32, [P]),
+    "wg_ledger_stats": (I32, [P, PI64, PI64, PI64]),
+    "wg_ledger_reserve": (I32, [P, I64]),
+    "wg_ledger_release": (I32, [P, I64]),
+    "wg_ctx_stream": (P, [P]),
+    "wg_ctx_launch_count": (I64, [P]),
+    "wg_filter_create": (I32, [P, I32, I32, I32, I64, F64, PP]),
+    "wg_filter_execute": (I32, [P, C.POINTER(wg_batch_desc), P, PI64]),
+    "wg_filter_execute_device": (I32, [P, C.POINTER(wg_batch_desc), P, PI64]),
+    "wg_filter_destroy": (I32, [P]),
+    "wg_join_create": (I32, [P, I32, I32, I32, I32, C.POINTER(C.c_int32), I64, PP]),
+    "wg_join_build_append": (I32, [P, C.POINTER(wg_batch_desc)]),
+    "wg_join_build_append_device": (I32, [P, C.POINTER(wg_batch_desc)]),
+    "wg_join_build_finish": (I32, [P]),
+    "wg_join_build_stats": (I32, [P, PI64, PI64]),
+    "wg_join_probe": (I32, [P, C.POINTER(wg_batch_desc), P, P, I64, PI64, PI64]),
+    "wg_join_gather": (I32, [P, I32, P, I64, P, P]),
+    "wg_join_reset": (I32, [P]),
+    "wg_join_destroy": (I32, [P]),
+    "wg_agg_create": (I32, [P, I32, C.POINTER(C.c_int32), I32, C.POINTER(wg_agg_spec), I64, PP]),
+    "wg_agg_consume": (I32, [P, C.POINTER(wg_batch_desc)]),
+    "wg_agg_consume_device": (I32, [P, C.POINTER(wg_batch_desc)]),
+    "wg_agg_clone": (I32, [P, PP]),
+    "wg_agg_merge": (I32, [P, P]),
+    "wg_agg_finalize": (I32, [P, PI64]),
+    "wg_agg_emit": (I32, [P, I64, I64, C.POINTER(wg_column), PI64]),
+    "wg_agg_export": (I32, [P, C.POINTER(wg_group_export)]),
+    "wg_agg_reset": (I32, [P]),
+    "wg_agg_destroy": (I32, [P]),
+    "wg_pipeline_run": (I32, [P, C.POINTER(wg_pipeline_desc)]),
+    "wg_pipeline_run_device": (I32, [P, C.POINTER(wg_pipeline_desc)]),
+    "wg_synth_starjoin_fact": (I32, [P, C.c_uint64, I64, I64, P, P, P, P]),
+    "wg_synth_starjoin_dim": (I32, [P, C.c_uint64, I64, P, P]),
+    "wg_synth_groupby": (I32, [P, C.c_uint64, I64, I64, I64, P, P, P, P]),
+    "wg_synth_highcard": (I32, [P, C.c_uint64, I64, I64, P, P, P, P]),
+}
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Load libwadjetgpu.so from the package directory (built by wadjet_b200.build).
+
+    There is no fallback: without the library the GPU operators do not exist.
+    """
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m wadjet_b200.build`")
+    lib = C.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib

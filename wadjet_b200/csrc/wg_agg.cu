@@ -1,0 +1,1033 @@
+// wg_agg.cu — exec.HashAggregate and the fused pipeline on the GPU.
+//
+// Host policy around the device table (see wg_agg.cuh for the slot layout):
+//  - The table is an open-addressing array of (cap + 2) slots, cap a power of
+//    two, at most 75% of cap regular groups (inserts beyond are refused and
+//    flagged, never silently dropped).
+//  - A launch that provably cannot reach the limit (groups known so far + rows
+//    in the launch) runs straight through. Otherwise a small table is
+//    snapshotted, the launch runs, and on an overflow the snapshot is restored,
+//    the table grown 4x and the launch replayed; a large table is fed in chunks
+//    that each fit, growing between chunks. Either way every row is applied
+//    exactly once.
+//  - Low-cardinality int keys use a CTA-private shared-memory table flushed to
+//    the global table at the end of the kernel.
+#include "wg_internal.h"
+#include "wg_agg_kernels.cuh"
+
+#include <algorithm>
+#include <cstdlib>
+
+namespace wg {
+wg_status resolve_pred(const wg_predicate& p, int32_t type_id, wgd::Pred* out);
+wg_status join_view(wg_join* j, wgd::JoinView* v);
+int32_t join_probe_key_col(wg_join* j);
+int32_t join_n_payload(wg_join* j);
+int32_t join_payload_type(wg_join* j, int i);
+int32_t join_payload_scale(wg_join* j, int i);
+bool join_payload_nullable(wg_join* j, int i);
+int64_t join_max_fanout(wg_join* j);
+}  // namespace wg
+
+using namespace wgd;
+
+namespace {
+
+constexpr int kAggBlock = 512;
+constexpr int64_t kSnapshotMaxBytes = 256LL << 20;
+constexpr double kMaxLoad = 0.75;
+
+__global__ void init_table_kernel(unsigned long long* slots, int64_t words, int sw, Layout L) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < words; i += (int64_t)gridDim.x * blockDim.x)
+    slots[i] = L.init[i % sw];
+}
+
+__device__ __forceinline__ bool slot_used(const Layout& L, const unsigned long long* s, uint64_t idx, uint64_t cap) {
+  if (L.key_words == 0) return idx == 0;
+  if (idx >= cap) return s[L.key_words] != 0;  // special slots: any rows
+  if (L.key_words == 1) return s[0] != WG_EMPTY_KEY;
+  return !(s[0] == ~0ULL && s[1] == ~0ULL);
+}
+
+// Fold every group of table (Ls, Ts) into (Ld, Td): MergeSink, table growth and
+// layout upgrades are all this one kernel.
+template <int NA>
+__global__ void fold_kernel(Layout Ls, Table Ts, Layout Ld, Table Td, int32_t* err) {
+  const uint64_t cap = Ts.mask + 1;
+  const uint64_t n = Ls.key_words == 0 ? 1 : cap + 2;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    const unsigned long long* s = Ts.slots + i * Ls.slot_words;
+    if (!slot_used(Ls, s, i, cap)) continue;
+    unsigned long long k0 = 0, k1 = 0;
+    bool knull = false;
+    if (Ls.key_words >= 1) {
+      if (i == cap + 1) knull = true;
+      else if (i == cap) { k0 = Ls.key_words == 1 ? WG_EMPTY_KEY : ~0ULL; k1 = ~0ULL; }
+      else { k0 = s[0]; if (Ls.key_words == 2) k1 = s[1]; }
+    }
+    unsigned long long* d = find_global(Ld, Td, k0, k1, knull, err);
+    if (!d) continue;
+    Contrib<NA> c;
+    slot_contrib<NA>(Ls, s, c);
+    apply<NA>(Ld, d, c, s[Ls.key_words]);
+  }
+}
+
+__global__ void compact_kernel(Layout L, Table T, int64_t* list, unsigned long long* count) {
+  const uint64_t cap = T.mask + 1;
+  const uint64_t n = L.key_words == 0 ? 1 : cap + 2;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < n; base += stride) {
+    const uint64_t i = base + threadIdx.x;
+    const bool used = i < n && slot_used(L, T.slots + i * L.slot_words, i, cap);
+    const unsigned m = __ballot_sync(WG_FULL_MASK, used);
+    if (m == 0) continue;
+    const int lane = threadIdx.x & 31;
+    unsigned long long off = 0;
+    if (lane == 0) off = atomicAdd(count, (unsigned long long)__popc(m));
+    off = __shfl_sync(WG_FULL_MASK, off, 0);
+    if (used) list[off + __popc(m & ((1u << lane) - 1))] = (int64_t)i;
+  }
+}
+
+struct FinalArgs {
+  Layout L;
+  Table T;
+  const int64_t* list;
+  int64_t start, n;
+  int32_t key_cls[WG_MAX_KEYS];
+  int32_t agg_func[WG_MAX_AGGS];
+  int32_t agg_out[WG_MAX_AGGS];   // 0 = int64 out, 1 = float64 out
+  int32_t agg_scale[WG_MAX_AGGS];
+  // export (raw)
+  int64_t* keys; uint8_t* key_valid; int64_t* count; int64_t* i64; double* f64; wg_int128* dec; uint8_t* has;
+  int64_t stride;                 // n_groups (rows per key / aggregate block)
+  // emit (finalized)
+  void* out[WG_MAX_KEYS + WG_MAX_AGGS];
+  uint8_t* out_valid[WG_MAX_KEYS + WG_MAX_AGGS];
+};
+
+__device__ __forceinline__ void slot_agg_state(const Layout& L, const unsigned long long* s, int a, int64_t& cnt,
+                                               int64_t& iv, double& fv, unsigned long long& dlo,
+                                               unsigned long long& dhi, bool& has) {
+  const AggD g = L.agg[a];
+  const unsigned long long rows = s[L.key_words];
+  const unsigned long long nulls = g.null_off >= 0 ? s[g.null_off] : 0;
+  cnt = (int64_t)(rows - nulls);
+  has = cnt > 0;
+  iv = 0; fv = 0.0; dlo = 0; dhi = 0;
+  switch (g.kind) {
+    case K_SUM_I64: case K_MIN_I64: case K_MAX_I64: iv = (int64_t)s[g.off]; break;
+    case K_SUM_F64: fv = as_f(s[g.off]); break;
+    case K_MIN_F64: case K_MAX_F64: fv = ord_to_f64(s[g.off]); break;
+    case K_SUM_DEC: case K_MIN_DEC: case K_MAX_DEC: dlo = s[g.off]; dhi = s[g.off + 1]; break;
+    default: break;
+  }
+  if (!has && g.kind >= K_MIN_I64) { iv = 0; fv = 0.0; dlo = 0; dhi = 0; }
+}
+
+__device__ __forceinline__ int64_t slot_key(const Layout& L, const unsigned long long* s, int k) {
+  if (L.key_words == 1) return (int64_t)s[0];
+  const unsigned long long w = s[L.key_word[k]];
+  return L.key_i32[k] ? (int64_t)(int32_t)(uint32_t)(w >> L.key_shift[k]) : (int64_t)w;
+}
+
+__global__ void export_kernel(FinalArgs A) {
+  const Layout& L = A.L;
+  const uint64_t cap = A.T.mask + 1;
+  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < A.n; g += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t idx = (uint64_t)A.list[A.start + g];
+    const unsigned long long* s = A.T.slots + idx * L.slot_words;
+    const int64_t o = g;
+    for (int k = 0; k < L.n_keys; ++k) {
+      const bool valid = !(L.key_words >= 1 && idx == cap + 1);
+      if (A.keys) A.keys[k * A.stride + o] = valid ? slot_key(L, s, k) : 0;
+      if (A.key_valid) A.key_valid[k * A.stride + o] = valid ? 1 : 0;
+    }
+    for (int a = 0; a < L.n_aggs; ++a) {
+      int64_t cnt, iv; double fv; unsigned long long dlo, dhi; bool has;
+      slot_agg_state(L, s, a, cnt, iv, fv, dlo, dhi, has);
+      if (A.count) A.count[a * A.stride + o] = cnt;
+      if (A.i64) A.i64[a * A.stride + o] = iv;
+      if (A.f64) A.f64[a * A.stride + o] = fv;
+      if (A.dec) { wg_int128 d; d.hi = (int64_t)dhi; d.lo = dlo; A.dec[a * A.stride + o] = d; }
+      if (A.has) A.has[a * A.stride + o] = has ? 1 : 0;
+    }
+  }
+}
+
+// writeAccToColumn (internal/engine/exec/aggregate_partial_spill.go:1855-1960)
+__global__ void emit_kernel(FinalArgs A) {
+  const Layout& L = A.L;
+  const uint64_t cap = A.T.mask + 1;
+  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < A.n; g += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t idx = (uint64_t)A.list[A.start + g];
+    const unsigned long long* s = A.T.slots + idx * L.slot_words;
+    for (int k = 0; k < L.n_keys; ++k) {
+      const bool valid = !(L.key_words >= 1 && idx == cap + 1);
+      const int64_t v = valid ? slot_key(L, s, k) : 0;
+      if (A.key_cls[k] == WG_CLS_I32) ((int32_t*)A.out[k])[g] = (int32_t)v;
+      else ((int64_t*)A.out[k])[g] = v;
+      A.out_valid[k][g] = valid ? 1 : 0;
+    }
+    for (int a = 0; a < L.n_aggs; ++a) {
+      int64_t cnt, iv; double fv; unsigned long long dlo, dhi; bool has;
+      slot_agg_state(L, s, a, cnt, iv, fv, dlo, dhi, has);
+      const int kind = L.agg[a].kind;
+      const int func = A.agg_func[a];
+      const bool dec = kind == K_SUM_DEC || kind == K_MIN_DEC || kind == K_MAX_DEC;
+      const bool flt = kind == K_SUM_F64 || kind == K_MIN_F64 || kind == K_MAX_F64;
+      bool valid = true;
+      double f = 0.0;
+      int64_t i = 0;
+      if (func == WG_AGG_COUNT) {
+        i = cnt; f = __ll2double_rn(cnt);
+      } else if (func == WG_AGG_SUM || func == WG_AGG_AVG) {
+        if (cnt == 0) valid = false;
+        else {
+          f = dec ? dec_to_f64((int64_t)dhi, dlo, A.agg_scale[a]) : flt ? fv : __ll2double_rn(iv);
+          if (func == WG_AGG_AVG) f = __ddiv_rn(f, __ll2double_rn(cnt));
+          i = iv;
+        }
+      } else {  // MIN / MAX
+        if (!has) valid = false;
+        else {
+          f = dec ? dec_to_f64((int64_t)dhi, dlo, A.agg_scale[a]) : flt ? fv : __ll2double_rn(iv);
+          i = dec ? (int64_t)dlo : flt ? (int64_t)fv : iv;
+        }
+      }
+      const int c = L.n_keys + a;
+      if (A.agg_out[a] == 0) ((int64_t*)A.out[c])[g] = valid ? i : 0;
+      else ((double*)A.out[c])[g] = valid ? f : 0.0;
+      A.out_valid[c][g] = valid ? 1 : 0;
+    }
+  }
+}
+
+template <int NA>
+void launch_fold(const Layout& Ls, const Table& Ts, const Layout& Ld, const Table& Td, int32_t* err, unsigned grid,
+                 cudaStream_t st) {
+  fold_kernel<NA><<<grid, 256, 0, st>>>(Ls, Ts, Ld, Td, err);
+}
+
+unsigned grid_cap(wg::Ctx* ctx, int64_t n, int block, int per_sm = 16) {
+  int64_t b = (n + block - 1) / block;
+  b = std::min<int64_t>(b, (int64_t)ctx->sm_count * per_sm);
+  return (unsigned)std::max<int64_t>(b, 1);
+}
+
+int env_int(const char* name, int dflt) {
+  const char* v = std::getenv(name);
+  return v && *v ? std::atoi(v) : dflt;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// host aggregate object
+// ---------------------------------------------------------------------------
+struct wg_agg {
+  wg::Ctx* ctx;
+  std::vector<int32_t> key_cols;
+  std::vector<wg_agg_spec> specs;
+  int64_t hint = 0;
+  bool resolved = false;
+  bool finalized = false;
+  // resolved schema (from the first batch's virtual schema)
+  std::vector<int32_t> key_types;
+  std::vector<int32_t> in_cls, in_scale, out_type, kind;
+  std::vector<bool> nullable;
+  wgd::Layout L{};
+  // table
+  wg::DevBuf table, backup, ctr;   // ctr: [0] n_groups, [1] overflow flag
+  uint64_t cap = 0;
+  int shift = 0;
+  int64_t known_groups = 0;        // regular groups, exact as of the last read-back
+  int64_t upper_groups = 0;        // upper bound since then
+  // finalize
+  wg::DevBuf list, cnt;
+  int64_t n_out = 0;
+  std::vector<wg::DevBuf> emit_bufs, emit_valid;
+  bool emitted = false;
+};
+
+namespace wg {
+
+static wgd::Table table_view(wg_agg* a) {
+  wgd::Table T;
+  T.slots = a->table.as<unsigned long long>();
+  T.n_groups = a->ctr.as<unsigned long long>();
+  T.overflow = (int32_t*)(a->ctr.as<unsigned long long>() + 1);
+  T.shift = a->shift;
+  T._pad = 0;
+  T.mask = a->cap - 1;
+  T.limit = (unsigned long long)((double)a->cap * kMaxLoad);
+  return T;
+}
+
+static int64_t table_words(const wg_agg* a, uint64_t cap) {
+  return a->L.key_words == 0 ? a->L.slot_words : (int64_t)(cap + 2) * a->L.slot_words;
+}
+
+// Build the slot layout from kinds/nullability.
+static void build_layout(wg_agg* a) {
+  wgd::Layout& L = a->L;
+  const int nk = (int)a->key_cols.size();
+  int w = L.key_words;
+  const int rows_at = w++;
+  bool need_even = L.key_words == 2;
+  for (size_t i = 0; i < a->specs.size(); ++i) {
+    wgd::AggD& g = L.agg[i];
+    g.kind = a->kind[i];
+    const int kw = wgd::kind_words(g.kind);
+    if (g.kind == wgd::K_MIN_DEC || g.kind == wgd::K_MAX_DEC) { if (w & 1) ++w; need_even = true; }
+    g.off = kw > 0 ? w : -1;
+    w += kw;
+    g.null_off = (a->nullable[i] && a->specs[i].input_col >= 0) ? w++ : -1;
+    g.vcol = a->specs[i].input_col;
+  }
+  if (need_even && (w & 1)) ++w;
+  L.slot_words = w;
+  L.n_keys = nk;
+  L.n_aggs = (int)a->specs.size();
+  for (int i = 0; i < WG_MAX_SLOT_WORDS; ++i) L.init[i] = 0;
+  if (L.key_words == 1) L.init[0] = WG_EMPTY_KEY;
+  if (L.key_words == 2) { L.init[0] = ~0ULL; L.init[1] = ~0ULL; }
+  L.init[rows_at] = 0;
+  for (size_t i = 0; i < a->specs.size(); ++i) {
+    const wgd::AggD& g = L.agg[i];
+    switch (g.kind) {
+      case wgd::K_MIN_I64: L.init[g.off] = 0x7FFFFFFFFFFFFFFFULL; break;
+      case wgd::K_MAX_I64: L.init[g.off] = 0x8000000000000000ULL; break;
+      case wgd::K_MIN_F64: L.init[g.off] = ~0ULL; break;
+      case wgd::K_MAX_F64: L.init[g.off] = 0ULL; break;
+      case wgd::K_MIN_DEC: L.init[g.off] = ~0ULL; L.init[g.off + 1] = 0x7FFFFFFFFFFFFFFFULL; break;
+      case wgd::K_MAX_DEC: L.init[g.off] = 0ULL; L.init[g.off + 1] = 0x8000000000000000ULL; break;
+      default: break;
+    }
+  }
+}
+
+static wg_status init_table(wg_agg* a, DevBuf& buf, uint64_t cap) {
+  Ctx* ctx = a->ctx;
+  const int64_t words = table_words(a, cap);
+  WG_TRY(buf.alloc(ctx, words * 8));
+  init_table_kernel<<<grid_cap(ctx, words, 256), 256, 0, ctx->stream>>>(buf.as<unsigned long long>(), words,
+                                                                       a->L.slot_words, a->L);
+  ctx->count_launch();
+  WG_CUDA_TRY(cudaGetLastError());
+  return WG_OK;
+}
+
+static uint64_t cap_for(int64_t groups) {
+  uint64_t cap = 1024;
+  while ((double)cap * kMaxLoad < (double)groups * 1.34) cap <<= 1;  // target ~56% load
+  return cap;
+}
+
+static int log2u(uint64_t v) { int l = 0; while ((1ULL << l) < v) ++l; return l; }
+
+static void run_fold(wg_agg* a, const wgd::Layout& Ls, const wgd::Table& Ts, const wgd::Layout& Ld, const wgd::Table& Td) {
+  Ctx* ctx = a->ctx;
+  const int64_t n = Ls.key_words == 0 ? 1 : (int64_t)(Ts.mask + 3);
+  const unsigned grid = grid_cap(ctx, n, 256);
+  if (Ls.n_aggs <= 4) launch_fold<4>(Ls, Ts, Ld, Td, ctx->dev_error, grid, ctx->stream);
+  else launch_fold<8>(Ls, Ts, Ld, Td, ctx->dev_error, grid, ctx->stream);
+  ctx->count_launch();
+}
+
+// Re-create the table with capacity new_cap and/or a new layout, folding every
+// group across.
+static wg_status rebuild_table(wg_agg* a, uint64_t new_cap, const wgd::Layout& new_layout) {
+  Ctx* ctx = a->ctx;
+  const wgd::Layout old_L = a->L;
+  const wgd::Table old_T = table_view(a);
+  DevBuf old_table = std::move(a->table);
+  DevBuf old_ctr = std::move(a->ctr);
+  a->L = new_layout;
+  a->cap = a->L.key_words == 0 ? 1 : new_cap;
+  a->shift = 64 - log2u(a->cap);
+  WG_TRY(init_table(a, a->table, a->cap));
+  WG_TRY(a->ctr.alloc(ctx, 64));
+  WG_CUDA_TRY(cudaMemsetAsync(a->ctr.get(), 0, 64, ctx->stream));
+  wgd::Table old_view = old_T;
+  old_view.slots = old_table.as<unsigned long long>();
+  old_view.n_groups = old_ctr.as<unsigned long long>();
+  old_view.overflow = (int32_t*)(old_ctr.as<unsigned long long>() + 1);
+  run_fold(a, old_L, old_view, a->L, table_view(a));
+  WG_CUDA_TRY(cudaGetLastError());
+  WG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  a->backup.reset();
+  return WG_OK;
+}
+
+static int agg_kind(int func, int cls) {
+  switch (func) {
+    case WG_AGG_COUNT: return wgd::K_COUNT;
+    case WG_AGG_SUM: case WG_AGG_AVG:  // initFlatAccums, aggregate.go:6060-6090
+      if (cls == WG_CLS_F32 || cls == WG_CLS_F64) return wgd::K_SUM_F64;
+      if (cls == WG_CLS_DEC) return wgd::K_SUM_DEC;
+      if (cls == WG_CLS_I64 && func == WG_AGG_AVG) return wgd::K_SUM_F64;
+      return wgd::K_SUM_I64;
+    case WG_AGG_MIN:
+      return (cls == WG_CLS_F32 || cls == WG_CLS_F64) ? wgd::K_MIN_F64 : cls == WG_CLS_DEC ? wgd::K_MIN_DEC : wgd::K_MIN_I64;
+    case WG_AGG_MAX:
+      return (cls == WG_CLS_F32 || cls == WG_CLS_F64) ? wgd::K_MAX_F64 : cls == WG_CLS_DEC ? wgd::K_MAX_DEC : wgd::K_MAX_I64;
+  }
+  return -1;
+}
+
+// Virtual schema of one launch: type, scale and nullability per virtual column.
+struct VSchema {
+  std::vector<int32_t> type, scale;
+  std::vector<bool> nullable;
+};
+
+// resolveIndices (aggregate.go:1296): fix the path and the accumulators from the
+// first batch's schema.
+static wg_status agg_resolve(wg_agg* a, const VSchema& vs) {
+  const int nk = (int)a->key_cols.size();
+  a->key_types.clear();
+  for (int k = 0; k < nk; ++k) {
+    const int kc = a->key_cols[k];
+    if (kc < 0 || kc >= (int)vs.type.size()) return fail(WG_E_INVALID, "group column out of range");
+    const int cls = class_of(vs.type[kc]);
+    if (cls != WG_CLS_I32 && cls != WG_CLS_I64)
+      return fail(WG_E_UNSUPPORTED, "GROUP BY key is not an integer-class column (string keys are not on the GPU path)");
+    a->key_types.push_back(vs.type[kc]);
+  }
+  std::memset(&a->L, 0, sizeof(a->L));
+  if (nk == 0) a->L.key_words = 0;
+  else if (nk == 1) a->L.key_words = 1;
+  else {
+    // buildPackedLayout (packed_hash.go:386): widest-first into two 64-bit words
+    int total = 0;
+    for (int k = 0; k < nk; ++k) total += class_of(a->key_types[k]) == WG_CLS_I32 ? 4 : 8;
+    if (nk > WG_MAX_KEYS || total > 16) return fail(WG_E_UNSUPPORTED, "composite key does not pack into 128 bits");
+    a->L.key_words = 2;
+    int next_wide = 0;
+    for (int k = 0; k < nk; ++k)
+      if (class_of(a->key_types[k]) == WG_CLS_I64) { a->L.key_word[k] = next_wide++; a->L.key_shift[k] = 0; a->L.key_i32[k] = 0; }
+    std::vector<std::pair<int, int>> slots;
+    for (int w = next_wide; w < 2; ++w) { slots.push_back({w, 0}); slots.push_back({w, 32}); }
+    size_t nn = 0;
+    for (int k = 0; k < nk; ++k)
+      if (class_of(a->key_types[k]) == WG_CLS_I32) {
+        a->L.key_word[k] = slots[nn].first; a->L.key_shift[k] = slots[nn].second; a->L.key_i32[k] = 1; ++nn;
+      }
+  }
+  for (int k = 0; k < nk; ++k) a->L.key_vcol[k] = a->key_cols[k];
+  const size_t na = a->specs.size();
+  a->in_cls.assign(na, WG_CLS_BAD); a->in_scale.assign(na, 0); a->out_type.assign(na, 0); a->kind.assign(na, 0);
+  a->nullable.assign(na, false);
+  for (size_t i = 0; i < na; ++i) {
+    const wg_agg_spec& s = a->specs[i];
+    if (s.func < WG_AGG_SUM || s.func > WG_AGG_AVG) return fail(WG_E_UNSUPPORTED, "aggregate function is not on the GPU path");
+    if (s.input_col < 0) {
+      if (s.func != WG_AGG_COUNT) return fail(WG_E_INVALID, "only COUNT may omit its input column");
+    } else {
+      if (s.input_col >= (int)vs.type.size()) return fail(WG_E_INVALID, "aggregate column out of range");
+      a->in_cls[i] = class_of(vs.type[s.input_col]);
+      a->in_scale[i] = vs.scale[s.input_col];
+      if (a->in_cls[i] == WG_CLS_BAD) return fail(WG_E_UNSUPPORTED, "aggregate input type is not on the GPU path");
+      a->nullable[i] = vs.nullable[s.input_col];
+    }
+    a->kind[i] = agg_kind(s.func, a->in_cls[i]);
+    int ot = s.out_type;
+    if (ot == 0) {  // aggOutputType (plan.go:9968) / minMaxOutputType (aggregate.go:4611)
+      if (s.func == WG_AGG_COUNT) ot = WG_TYPE_INT64;
+      else if (s.func == WG_AGG_SUM || s.func == WG_AGG_AVG) ot = WG_TYPE_FLOAT64;
+      else ot = (a->in_cls[i] == WG_CLS_I32 || a->in_cls[i] == WG_CLS_I64) ? WG_TYPE_INT64 : WG_TYPE_FLOAT64;
+    }
+    if (ot != WG_TYPE_INT64 && ot != WG_TYPE_FLOAT64) return fail(WG_E_UNSUPPORTED, "aggregate output type must be INT64 or FLOAT64");
+    a->out_type[i] = ot;
+  }
+  if (na > WG_MAX_AGGS) return fail(WG_E_UNSUPPORTED, "more than 8 aggregates");
+  build_layout(a);
+  if (a->L.slot_words > WG_MAX_SLOT_WORDS) return fail(WG_E_UNSUPPORTED, "aggregate state too wide");
+  a->cap = a->L.key_words == 0 ? 1 : cap_for(std::max<int64_t>(a->hint, 1024));
+  a->shift = 64 - log2u(a->cap);
+  WG_TRY(init_table(a, a->table, a->cap));
+  WG_TRY(a->ctr.alloc(a->ctx, 64));
+  WG_CUDA_TRY(cudaMemsetAsync(a->ctr.get(), 0, 64, a->ctx->stream));
+  a->known_groups = 0;
+  a->upper_groups = 0;
+  a->resolved = true;
+  return WG_OK;
+}
+
+// Upgrade the layout when a batch brings NULLs to an aggregate whose state has
+// no null counter yet.
+static wg_status agg_check_nullable(wg_agg* a, const VSchema& vs) {
+  bool need = false;
+  std::vector<bool> nn = a->nullable;
+  for (size_t i = 0; i < a->specs.size(); ++i) {
+    const int c = a->specs[i].input_col;
+    if (c >= 0 && vs.nullable[c] && !nn[i]) { nn[i] = true; need = true; }
+  }
+  if (!need) return WG_OK;
+  wg_agg tmp;  // compute the new layout on a scratch copy of the shape
+  tmp.key_cols = a->key_cols; tmp.specs = a->specs; tmp.kind = a->kind; tmp.nullable = nn;
+  tmp.L = a->L;
+  build_layout(&tmp);
+  for (int k = 0; k < WG_MAX_KEYS; ++k) tmp.L.key_vcol[k] = a->L.key_vcol[k];
+  if (tmp.L.slot_words > WG_MAX_SLOT_WORDS) return fail(WG_E_UNSUPPORTED, "aggregate state too wide");
+  a->nullable = nn;
+  return rebuild_table(a, a->cap, tmp.L);
+}
+
+static wg_status refresh_groups(wg_agg* a) {
+  int64_t v[2];
+  WG_TRY(read_back_i64(a->ctx, (const int64_t*)a->ctr.get(), v, 2));
+  a->known_groups = v[0];
+  a->upper_groups = v[0];
+  return WG_OK;
+}
+
+// One launch description (device input already resident).
+struct LaunchSpec {
+  wgd::Plan P;
+  bool smem = false;
+  int block = kAggBlock;
+  unsigned grid = 1;
+  size_t smem_bytes = 0;
+};
+
+template <int NA>
+static void launch_pipeline_t(const LaunchSpec& ls, cudaStream_t st) {
+  if (ls.smem) {
+    cudaFuncSetAttribute(wgd::pipeline_kernel<NA, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ls.smem_bytes);
+    wgd::pipeline_kernel<NA, true><<<ls.grid, ls.block, ls.smem_bytes, st>>>(ls.P);
+  } else {
+    wgd::pipeline_kernel<NA, false><<<ls.grid, ls.block, 0, st>>>(ls.P);
+  }
+}
+
+static wg_status launch_pipeline(wg_agg* a, const LaunchSpec& ls, int64_t n_items) {
+  Ctx* ctx = a->ctx;
+  LaunchSpec l2 = ls;
+  wgd::Plan& P = l2.P;
+  P.T = table_view(a);
+  // the table's layout, with this launch's compact column numbering
+  wgd::Layout L = a->L;
+  for (int k = 0; k < WG_MAX_KEYS; ++k) L.key_vcol[k] = ls.P.L.key_vcol[k];
+  for (int i = 0; i < WG_MAX_AGGS; ++i) L.agg[i].vcol = ls.P.L.agg[i].vcol;
+  P.L = L;
+  P.n_items = n_items;
+  if (a->L.n_aggs <= 4) launch_pipeline_t<4>(l2, ctx->stream);
+  else launch_pipeline_t<8>(l2, ctx->stream);
+  ctx->count_launch();
+  WG_CUDA_TRY(cudaGetLastError());
+  return WG_OK;
+}
+
+}  // namespace wg
+
+// Everything the fused pipeline needs to run one device-resident input.
+struct PipelineRun {
+  wg_agg* agg;
+  const wg_batch_desc* in;      // device descriptors
+  int32_t n_filters;
+  const wg_predicate* filters;
+  wg_join* join;
+  int32_t n_exprs;
+  const wg_expr* exprs;
+};
+
+namespace wg {
+
+// Column rebasing for a row window without a selection vector: the kernel sees
+// rows [0, n); data pointers move by row0 (row0 is a multiple of 64 so the
+// validity bitmap moves by whole words).
+static void rebase_cols(wgd::Plan& P, int64_t row0) {
+  for (int j = 0; j < P.n_in; ++j) {
+    const int64_t es = P.in[j].cls == WG_CLS_I32 || P.in[j].cls == WG_CLS_F32 ? 4 : P.in[j].cls == WG_CLS_DEC ? 16 : 8;
+    P.in[j].data = (const char*)P.in[j].data + row0 * es;
+    if (P.in[j].valid) P.in[j].valid += row0 >> 6;
+  }
+}
+
+static wg_status build_plan(const PipelineRun& r, wgd::Plan& P, VSchema& vs, std::vector<int>& in_map) {
+  std::memset(&P, 0, sizeof(P));
+  const wg_batch_desc* in = r.in;
+  const int ncols = in->ncols;
+  const int npay = r.join ? join_n_payload(r.join) : 0;
+  // virtual schema in caller numbering
+  vs.type.clear(); vs.scale.clear(); vs.nullable.clear();
+  for (int c = 0; c < ncols; ++c) {
+    vs.type.push_back(in->cols[c].type_id); vs.scale.push_back(in->cols[c].scale);
+    vs.nullable.push_back(in->cols[c].valid_words != nullptr);
+  }
+  for (int p = 0; p < npay; ++p) {
+    vs.type.push_back(join_payload_type(r.join, p)); vs.scale.push_back(join_payload_scale(r.join, p));
+    vs.nullable.push_back(join_payload_nullable(r.join, p));
+  }
+  if (r.n_exprs < 0 || r.n_exprs > WG_MAX_EXPRS) return fail(WG_E_UNSUPPORTED, "at most 2 projection expressions");
+  for (int e = 0; e < r.n_exprs; ++e) {
+    const wg_expr& x = r.exprs[e];
+    if (x.result_type != WG_TYPE_INT64 && x.result_type != WG_TYPE_FLOAT64) return fail(WG_E_INVALID, "expression result type must be INT64 or FLOAT64");
+    bool nul = false;
+    for (int k = 0; k < x.n_ops && k < WG_EXPR_MAX_OPS; ++k)
+      if (x.ops[k].opcode == WG_EXPR_COL) {
+        if (x.ops[k].arg < 0 || x.ops[k].arg >= ncols + npay) return fail(WG_E_INVALID, "expression column out of range");
+        nul = nul || vs.nullable[x.ops[k].arg];
+      }
+    vs.type.push_back(x.result_type); vs.scale.push_back(0); vs.nullable.push_back(nul);
+  }
+  // referenced input columns → compact indices
+  in_map.assign(ncols, -1);
+  std::vector<int> order;
+  auto use = [&](int c) -> wg_status {
+    if (c < 0) return WG_OK;
+    if (c >= ncols) return WG_OK;
+    if (in_map[c] < 0) {
+      if ((int)order.size() >= WG_MAX_IN) return fail(WG_E_UNSUPPORTED, "more than 8 input columns referenced");
+      in_map[c] = (int)order.size();
+      order.push_back(c);
+    }
+    return WG_OK;
+  };
+  if (r.n_filters < 0 || r.n_filters > WG_MAX_FILTERS) return fail(WG_E_UNSUPPORTED, "at most 4 filter predicates");
+  for (int f = 0; f < r.n_filters; ++f) {
+    if (r.filters[f].col < 0 || r.filters[f].col >= ncols)
+      return fail(WG_E_INVALID, "filter column " + std::to_string(r.filters[f].col) + " does not exist in the input schema");
+    WG_TRY(use(r.filters[f].col));
+  }
+  if (r.join) {
+    const int pk = join_probe_key_col(r.join);
+    if (pk < 0 || pk >= ncols) return fail(WG_E_INVALID, "probe key column out of range");
+    const int pcls = class_of(in->cols[pk].type_id);
+    if (pcls != WG_CLS_I32 && pcls != WG_CLS_I64) return fail(WG_E_UNSUPPORTED, "probe key is not an integer-class column");
+    WG_TRY(use(pk));
+  }
+  for (int e = 0; e < r.n_exprs; ++e)
+    for (int k = 0; k < r.exprs[e].n_ops && k < WG_EXPR_MAX_OPS; ++k)
+      if (r.exprs[e].ops[k].opcode == WG_EXPR_COL) WG_TRY(use(r.exprs[e].ops[k].arg));
+  for (int32_t kc : r.agg->key_cols) WG_TRY(use(kc));
+  for (const wg_agg_spec& s : r.agg->specs) WG_TRY(use(s.input_col));
+  const int nin = (int)order.size();
+  auto vmap = [&](int c) -> int {  // caller vcol → compact vcol
+    if (c < 0) return -1;
+    if (c < ncols) return in_map[c];
+    return nin + (c - ncols);
+  };
+  P.n_in = nin;
+  for (int j = 0; j < nin; ++j) {
+    const wg_column& c = in->cols[order[j]];
+    const int cls = class_of(c.type_id);
+    if (cls == WG_CLS_BAD) return fail(WG_E_UNSUPPORTED, "input column type is not on the GPU path");
+    P.in[j] = wgd::DCol{c.data, c.valid_words, cls, c.scale};
+    P.vcls[j] = cls; P.vscale[j] = c.scale;
+  }
+  P.n_filters = r.n_filters;
+  for (int f = 0; f < r.n_filters; ++f) {
+    WG_TRY(resolve_pred(r.filters[f], in->cols[r.filters[f].col].type_id, &P.filt[f]));
+    P.filt[f].col = in_map[r.filters[f].col];
+  }
+  if (r.join) {
+    P.has_join = 1;
+    WG_TRY(join_view(r.join, &P.join));
+    P.probe_col = in_map[join_probe_key_col(r.join)];
+    for (int p = 0; p < npay; ++p) { P.vcls[nin + p] = class_of(vs.type[ncols + p]); P.vscale[nin + p] = vs.scale[ncols + p]; }
+  } else {
+    P.join.n_pay = 0;
+  }
+  P.n_exprs = r.n_exprs;
+  for (int e = 0; e < r.n_exprs; ++e) {
+    const wg_expr& x = r.exprs[e];
+    wgd::ExprD& d = P.expr[e];
+    if (x.n_ops < 1 || x.n_ops > WG_EXPR_MAX_OPS) return fail(WG_E_INVALID, "expression needs 1..12 operations");
+    d.n_ops = x.n_ops;
+    d.result_cls = x.result_type == WG_TYPE_INT64 ? WG_CLS_I64 : WG_CLS_F64;
+    int depth = 0;
+    for (int k = 0; k < x.n_ops; ++k) {
+      const wg_expr_op& o = x.ops[k];
+      d.opc[k] = o.opcode;
+      d.arg[k] = o.opcode == WG_EXPR_COL ? vmap(o.arg) : 0;
+      if (o.opcode == WG_EXPR_CONST_F) std::memcpy(&d.imm[k], &o.imm_f64, 8);
+      else d.imm[k] = o.imm_i64;
+      if (o.opcode <= WG_EXPR_CONST_F) ++depth;
+      else if (o.opcode <= WG_EXPR_AND) { if (depth < 2) return fail(WG_E_INVALID, "expression stack underflow"); --depth; }
+      else return fail(WG_E_INVALID, "unknown expression opcode");
+      if (depth > 4) return fail(WG_E_UNSUPPORTED, "expression deeper than 4 stack entries");
+    }
+    if (depth != 1) return fail(WG_E_INVALID, "expression must leave exactly one value");
+    P.vcls[nin + npay + e] = d.result_cls;
+    P.vscale[nin + npay + e] = 0;
+  }
+  for (int k = 0; k < (int)r.agg->key_cols.size(); ++k) P.L.key_vcol[k] = vmap(r.agg->key_cols[k]);
+  for (size_t i = 0; i < r.agg->specs.size(); ++i) P.L.agg[i].vcol = vmap(r.agg->specs[i].input_col);
+  P.sel = in->sel;
+  P.n_items = in->sel ? in->sel_len : in->len;
+  return WG_OK;
+}
+
+// Run the fused kernel over a device-resident input with the overflow policy.
+static wg_status run_device(const PipelineRun& r) {
+  wg_agg* a = r.agg;
+  Ctx* ctx = a->ctx;
+  if (a->finalized) return fail(WG_E_STATE, "aggregate already finalized");
+  LaunchSpec ls;
+  VSchema vs;
+  std::vector<int> in_map;
+  WG_TRY(build_plan(r, ls.P, vs, in_map));
+  if (!a->resolved) WG_TRY(agg_resolve(a, vs));
+  else WG_TRY(agg_check_nullable(a, vs));
+  ls.P.err = ctx->dev_error;
+  const int64_t n_items = ls.P.n_items;
+  if (n_items == 0) return WG_OK;
+  const int64_t fan = r.join ? std::max<int64_t>(1, join_max_fanout(r.join)) : 1;
+
+  // kernel shape: shared-memory table for low-cardinality single int keys
+  bool any_null_words = false, any_dec_minmax = false;
+  for (int i = 0; i < a->L.n_aggs; ++i) {
+    any_null_words |= a->L.agg[i].null_off >= 0;
+    any_dec_minmax |= a->L.agg[i].kind == wgd::K_MIN_DEC || a->L.agg[i].kind == wgd::K_MAX_DEC;
+  }
+  const int blocks_per_sm = std::max(1, env_int("WG_AGG_BLOCKS_PER_SM", 2));
+  ls.block = kAggBlock;
+  const int64_t smem_budget = (int64_t)ctx->max_smem_optin / blocks_per_sm - 2048;
+  const int S = (int)std::min<int64_t>(smem_budget / (a->L.slot_words * 8), 16384);
+  const int64_t expect = std::max<int64_t>(a->hint, a->known_groups);
+  ls.smem = env_int("WG_AGG_SMEM", 1) != 0 && a->L.key_words == 1 && !any_null_words && !any_dec_minmax && S >= 256 &&
+            expect > 0 && expect * 2 <= S;
+  ls.P.smem_slots = ls.smem ? S : 0;
+  ls.smem_bytes = ls.smem ? (size_t)S * a->L.slot_words * 8 : 0;
+  ls.grid = (unsigned)(ctx->sm_count * blocks_per_sm);
+  if (!ls.smem) ls.grid = (unsigned)std::min<int64_t>((int64_t)ctx->sm_count * 4, (n_items + 1023) / 1024 + 1);
+
+  const wgd::Plan base = ls.P;
+  auto limit = [&]() { return (int64_t)((double)a->cap * kMaxLoad); };
+
+  // 1) provably safe: one launch
+  if (a->L.key_words == 0 || a->upper_groups + n_items * fan <= limit()) {
+    WG_TRY(launch_pipeline(a, ls, n_items));
+    a->upper_groups += a->L.key_words == 0 ? 0 : n_items * fan;
+    return check_device_error(ctx);
+  }
+  // 2) small table: snapshot, run, replay on overflow
+  const int64_t tbytes = table_words(a, a->cap) * 8;
+  if (tbytes <= kSnapshotMaxBytes) {
+    for (int attempt = 0; attempt < 16; ++attempt) {
+      const int64_t tb = table_words(a, a->cap) * 8;
+      WG_TRY(a->backup.ensure(ctx, tb + 64));
+      WG_CUDA_TRY(cudaMemcpyAsync(a->backup.get(), a->table.get(), (size_t)tb, cudaMemcpyDeviceToDevice, ctx->stream));
+      WG_CUDA_TRY(cudaMemcpyAsync(a->backup.as<char>() + tb, a->ctr.get(), 64, cudaMemcpyDeviceToDevice, ctx->stream));
+      WG_TRY(launch_pipeline(a, ls, n_items));
+      int64_t v[2];
+      WG_TRY(read_back_i64(ctx, (const int64_t*)a->ctr.get(), v, 2));
+      WG_TRY(check_device_error(ctx));
+      if ((int32_t)v[1] == 0) {
+        a->known_groups = a->upper_groups = v[0];
+        return WG_OK;
+      }
+      // overflow: restore, grow 4x, replay
+      WG_CUDA_TRY(cudaMemcpyAsync(a->table.get(), a->backup.get(), (size_t)tb, cudaMemcpyDeviceToDevice, ctx->stream));
+      WG_CUDA_TRY(cudaMemcpyAsync(a->ctr.get(), a->backup.as<char>() + tb, 64, cudaMemcpyDeviceToDevice, ctx->stream));
+      WG_TRY(rebuild_table(a, a->cap * 4, a->L));
+      WG_TRY(refresh_groups(a));
+      const int64_t expect2 = std::max<int64_t>(a->hint, a->known_groups);
+      if (ls.smem && expect2 * 2 > S) { ls.smem = false; ls.P.smem_slots = 0; ls.smem_bytes = 0; }
+      if (table_words(a, a->cap) * 8 > kSnapshotMaxBytes) break;
+    }
+  }
+  // 3) large table: chunks that each fit, growing between chunks
+  WG_TRY(refresh_groups(a));
+  if (ls.smem) { ls.smem = false; ls.P.smem_slots = 0; ls.smem_bytes = 0; ls.grid = (unsigned)(ctx->sm_count * 4); }
+  int64_t done = 0;
+  const int64_t min_chunk = 1 << 20;
+  while (done < n_items) {
+    int64_t room = (limit() - a->known_groups) / fan;
+    if (room < min_chunk && room < n_items - done) {
+      WG_TRY(rebuild_table(a, cap_for(a->known_groups + std::min<int64_t>(n_items - done, 64LL << 20) * fan), a->L));
+      WG_TRY(refresh_groups(a));
+      room = (limit() - a->known_groups) / fan;
+    }
+    int64_t m = std::min<int64_t>(room, n_items - done);
+    if (!ls.P.sel) m = std::max<int64_t>(64, m & ~int64_t(63));
+    m = std::min<int64_t>(m, n_items - done);
+    LaunchSpec lc = ls;
+    lc.P = base;
+    if (lc.P.sel) lc.P.sel = base.sel + done;
+    else rebase_cols(lc.P, done);
+    WG_TRY(launch_pipeline(a, lc, m));
+    WG_TRY(refresh_groups(a));
+    WG_TRY(check_device_error(ctx));
+    int64_t v[2];
+    WG_TRY(read_back_i64(ctx, (const int64_t*)a->ctr.get(), v, 2));
+    if ((int32_t)v[1] != 0) return fail(WG_E_NOMEM, "aggregate table overflow on a checked chunk");
+    done += m;
+  }
+  return WG_OK;
+}
+
+// Compact the occupied slots once; the list drives export and emit.
+static wg_status agg_compact(wg_agg* a) {
+  Ctx* ctx = a->ctx;
+  const int64_t n = a->L.key_words == 0 ? 1 : (int64_t)a->cap + 2;
+  WG_TRY(a->list.ensure(ctx, n * 8));
+  WG_TRY(a->cnt.ensure(ctx, 64));
+  WG_CUDA_TRY(cudaMemsetAsync(a->cnt.get(), 0, 8, ctx->stream));
+  compact_kernel<<<grid_cap(ctx, n, 256), 256, 0, ctx->stream>>>(a->L, table_view(a), a->list.as<int64_t>(),
+                                                                  a->cnt.as<unsigned long long>());
+  ctx->count_launch();
+  WG_CUDA_TRY(cudaGetLastError());
+  int64_t c = 0;
+  WG_TRY(read_back_i64(ctx, a->cnt.as<int64_t>(), &c, 1));
+  a->n_out = c;
+  return WG_OK;
+}
+
+static void fill_final_args(wg_agg* a, FinalArgs& A) {
+  std::memset(&A, 0, sizeof(A));
+  A.L = a->L;
+  A.T = table_view(a);
+  A.list = a->list.as<int64_t>();
+  for (size_t k = 0; k < a->key_types.size(); ++k) A.key_cls[k] = class_of(a->key_types[k]);
+  for (size_t i = 0; i < a->specs.size(); ++i) {
+    A.agg_func[i] = a->specs[i].func;
+    A.agg_out[i] = a->out_type[i] == WG_TYPE_INT64 ? 0 : 1;
+    A.agg_scale[i] = a->in_scale[i];
+  }
+}
+
+}  // namespace wg
+
+using namespace wg;
+
+namespace wg {
+// Access for the pipeline entry points (wg_pipeline.cu).
+wg_status agg_run_device(wg_agg* a, const wg_batch_desc* in, int32_t nf, const wg_predicate* f, wg_join* j, int32_t ne,
+                         const wg_expr* e) {
+  PipelineRun r{a, in, nf, f, j, ne, e};
+  return run_device(r);
+}
+Ctx* agg_ctx(wg_agg* a) { return a->ctx; }
+std::vector<int32_t> agg_input_cols(wg_agg* a) {
+  std::vector<int32_t> r = a->key_cols;
+  for (const wg_agg_spec& s : a->specs) r.push_back(s.input_col);
+  return r;
+}
+}  // namespace wg
+
+extern "C" {
+
+wg_status wg_agg_create(wg_ctx* ctx, int32_t n_keys, const int32_t* key_cols, int32_t n_aggs, const wg_agg_spec* aggs,
+                        int64_t group_ndv_hint, wg_agg** out) {
+  if (!ctx || !out || n_keys < 0 || n_aggs < 0 || (n_keys > 0 && !key_cols) || (n_aggs > 0 && !aggs))
+    return fail(WG_E_INVALID, "bad aggregate arguments");
+  if (n_keys > WG_MAX_KEYS) return fail(WG_E_UNSUPPORTED, "more than 4 GROUP BY columns");
+  if (n_aggs > WG_MAX_AGGS) return fail(WG_E_UNSUPPORTED, "more than 8 aggregates");
+  wg_agg* a = new wg_agg();
+  a->ctx = ctx;
+  a->key_cols.assign(key_cols, key_cols + n_keys);
+  a->specs.assign(aggs, aggs + n_aggs);
+  a->hint = group_ndv_hint;
+  *out = a;
+  return WG_OK;
+}
+
+wg_status wg_agg_consume_device(wg_agg* a, const wg_batch_desc* in) {
+  if (!a || !in) return fail(WG_E_INVALID, "NULL argument");
+  WG_TRY(ensure_device(a->ctx));
+  PipelineRun r{a, in, 0, nullptr, nullptr, 0, nullptr};
+  return run_device(r);
+}
+
+wg_status wg_agg_consume(wg_agg* a, const wg_batch_desc* in) {
+  if (!a || !in) return fail(WG_E_INVALID, "NULL argument");
+  WG_TRY(ensure_device(a->ctx));
+  StagedBatch sb;
+  WG_TRY(stage_batch(a->ctx, in, &sb));
+  PipelineRun r{a, &sb.desc, 0, nullptr, nullptr, 0, nullptr};
+  WG_TRY(run_device(r));
+  WG_CUDA_TRY(cudaStreamSynchronize(a->ctx->stream));
+  return WG_OK;
+}
+
+wg_status wg_agg_clone(wg_agg* a, wg_agg** out) {
+  if (!a || !out) return fail(WG_E_INVALID, "NULL argument");
+  return wg_agg_create(static_cast<wg_ctx*>(a->ctx), (int32_t)a->key_cols.size(), a->key_cols.data(), (int32_t)a->specs.size(),
+                       a->specs.data(), a->hint, out);
+}
+
+wg_status wg_agg_merge(wg_agg* d, wg_agg* s) {
+  if (!d || !s) return fail(WG_E_INVALID, "NULL argument");
+  if (d->ctx != s->ctx) return fail(WG_E_INVALID, "aggregates belong to different contexts");
+  if (d->key_cols != s->key_cols || d->specs.size() != s->specs.size()) return fail(WG_E_INVALID, "aggregate shapes differ");
+  WG_TRY(ensure_device(d->ctx));
+  if (d->finalized) return fail(WG_E_STATE, "aggregate already finalized");
+  if (!s->resolved) return WG_OK;
+  Ctx* ctx = d->ctx;
+  if (!d->resolved) {
+    // adopt the source's resolved schema (mergeSinkState inherits it, aggregate.go:4722)
+    d->key_types = s->key_types; d->in_cls = s->in_cls; d->in_scale = s->in_scale; d->out_type = s->out_type;
+    d->kind = s->kind; d->nullable = s->nullable; d->L = s->L;
+    d->cap = d->L.key_words == 0 ? 1 : cap_for(std::max<int64_t>(d->hint, 1024));
+    d->shift = 64 - log2u(d->cap);
+    WG_TRY(init_table(d, d->table, d->cap));
+    WG_TRY(d->ctr.alloc(ctx, 64));
+    WG_CUDA_TRY(cudaMemsetAsync(d->ctr.get(), 0, 64, ctx->stream));
+    d->resolved = true;
+  }
+  if (d->kind != s->kind) return fail(WG_E_INVALID, "aggregate input types differ");
+  // destination must carry every null counter the source has
+  bool upgrade = false;
+  std::vector<bool> nn = d->nullable;
+  for (size_t i = 0; i < nn.size(); ++i) if (s->nullable[i] && !nn[i]) { nn[i] = true; upgrade = true; }
+  if (upgrade) {
+    wg_agg tmp;
+    tmp.key_cols = d->key_cols; tmp.specs = d->specs; tmp.kind = d->kind; tmp.nullable = nn; tmp.L = d->L;
+    build_layout(&tmp);
+    for (int k = 0; k < WG_MAX_KEYS; ++k) tmp.L.key_vcol[k] = d->L.key_vcol[k];
+    d->nullable = nn;
+    WG_TRY(rebuild_table(d, d->cap, tmp.L));
+  }
+  WG_TRY(refresh_groups(d));
+  WG_TRY(refresh_groups(s));
+  const int64_t need = d->known_groups + s->known_groups;
+  if (d->L.key_words != 0 && need > (int64_t)((double)d->cap * kMaxLoad)) WG_TRY(rebuild_table(d, cap_for(need), d->L));
+  run_fold(d, s->L, table_view(s), d->L, table_view(d));
+  WG_CUDA_TRY(cudaGetLastError());
+  WG_TRY(refresh_groups(d));
+  return check_device_error(ctx);
+}
+
+wg_status wg_agg_finalize(wg_agg* a, int64_t* n_groups) {
+  if (!a) return fail(WG_E_INVALID, "NULL argument");
+  WG_TRY(ensure_device(a->ctx));
+  if (!a->resolved) {
+    // never fed: a scalar aggregate still emits its one identity row (aggregate.go:4270)
+    a->finalized = true;
+    a->n_out = a->key_cols.empty() ? 1 : 0;
+    if (n_groups) *n_groups = a->n_out;
+    return WG_OK;
+  }
+  if (!a->finalized) {
+    WG_TRY(agg_compact(a));
+    a->finalized = true;
+  }
+  if (n_groups) *n_groups = a->n_out;
+  return check_device_error(a->ctx);
+}
+
+wg_status wg_agg_export(wg_agg* a, const wg_group_export* o) {
+  if (!a || !o) return fail(WG_E_INVALID, "NULL argument");
+  if (!a->finalized) return fail(WG_E_STATE, "aggregate not finalized");
+  Ctx* ctx = a->ctx;
+  WG_TRY(ensure_device(ctx));
+  if (!a->resolved || a->n_out == 0) return WG_OK;
+  const int64_t n = a->n_out;
+  const int nk = (int)a->key_cols.size(), na = (int)a->specs.size();
+  DevBuf keys, kv, cnt, i64, f64, dec, has;
+  FinalArgs A;
+  fill_final_args(a, A);
+  A.start = 0; A.n = n; A.stride = n;
+  if (o->keys && nk) { WG_TRY(keys.alloc(ctx, nk * n * 8)); A.keys = keys.as<int64_t>(); }
+  if (o->key_valid && nk) { WG_TRY(kv.alloc(ctx, nk * n)); A.key_valid = kv.as<uint8_t>(); }
+  if (o->count && na) { WG_TRY(cnt.alloc(ctx, na * n * 8)); A.count = cnt.as<int64_t>(); }
+  if (o->i64 && na) { WG_TRY(i64.alloc(ctx, na * n * 8)); A.i64 = i64.as<int64_t>(); }
+  if (o->f64 && na) { WG_TRY(f64.alloc(ctx, na * n * 8)); A.f64 = f64.as<double>(); }
+  if (o->dec && na) { WG_TRY(dec.alloc(ctx, na * n * 16)); A.dec = dec.as<wg_int128>(); }
+  if (o->has && na) { WG_TRY(has.alloc(ctx, na * n)); A.has = has.as<uint8_t>(); }
+  export_kernel<<<grid_cap(ctx, n, 256), 256, 0, ctx->stream>>>(A);
+  ctx->count_launch();
+  WG_CUDA_TRY(cudaGetLastError());
+  auto back = [&](void* dst, DevBuf& src, int64_t bytes) -> wg_status {
+    if (dst && src.get() && bytes > 0) WG_CUDA_TRY(cudaMemcpyAsync(dst, src.get(), (size_t)bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    return WG_OK;
+  };
+  WG_TRY(back(o->keys, keys, nk * n * 8));
+  WG_TRY(back(o->key_valid, kv, nk * n));
+  WG_TRY(back(o->count, cnt, na * n * 8));
+  WG_TRY(back(o->i64, i64, na * n * 8));
+  WG_TRY(back(o->f64, f64, na * n * 8));
+  WG_TRY(back(o->dec, dec, na * n * 16));
+  WG_TRY(back(o->has, has, na * n));
+  WG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return check_device_error(ctx);
+}
+
+wg_status wg_agg_emit(wg_agg* a, int64_t start, int64_t max_rows, wg_column* out_cols, int64_t* n_out) {
+  if (!a || !n_out || (max_rows > 0 && !out_cols)) return fail(WG_E_INVALID, "NULL argument");
+  if (!a->finalized) return fail(WG_E_STATE, "aggregate not finalized");
+  Ctx* ctx = a->ctx;
+  WG_TRY(ensure_device(ctx));
+  const int nk = (int)a->key_cols.size(), na = (int)a->specs.size();
+  *n_out = 0;
+  if (start < 0 || start >= a->n_out || max_rows <= 0) return WG_OK;
+  const int64_t m = std::min<int64_t>(max_rows, a->n_out - start);
+  if (!a->resolved) {  // scalar aggregate over no input: COUNT 0, everything else NULL
+    for (int i = 0; i < na; ++i) {
+      wg_column& c = out_cols[i];
+      const bool is_count = a->specs[i].func == WG_AGG_COUNT;
+      int ot = a->specs[i].out_type ? a->specs[i].out_type : (is_count ? WG_TYPE_INT64 : WG_TYPE_FLOAT64);
+      if (ot == WG_TYPE_INT64) ((int64_t*)c.data)[0] = 0; else ((double*)c.data)[0] = 0.0;
+      if (c.valid_words) {
+        uint64_t* w = (uint64_t*)c.valid_words;
+        w[0] = is_count ? (w[0] | 1ULL) : (w[0] & ~1ULL);
+      }
+    }
+    *n_out = 1;
+    return WG_OK;
+  }
+  FinalArgs A;
+  fill_final_args(a, A);
+  A.start = start; A.n = m;
+  std::vector<DevBuf> bufs((size_t)(nk + na)), vals((size_t)(nk + na));
+  std::vector<int64_t> es((size_t)(nk + na));
+  for (int c = 0; c < nk + na; ++c) {
+    es[c] = c < nk ? (class_of(a->key_types[c]) == WG_CLS_I32 ? 4 : 8) : 8;
+    WG_TRY(bufs[c].alloc(ctx, m * es[c]));
+    WG_TRY(vals[c].alloc(ctx, m));
+    A.out[c] = bufs[c].get();
+    A.out_valid[c] = vals[c].as<uint8_t>();
+  }
+  emit_kernel<<<grid_cap(ctx, m, 256), 256, 0, ctx->stream>>>(A);
+  ctx->count_launch();
+  WG_CUDA_TRY(cudaGetLastError());
+  std::vector<std::vector<uint8_t>> hv((size_t)(nk + na), std::vector<uint8_t>((size_t)m));
+  for (int c = 0; c < nk + na; ++c) {
+    WG_CUDA_TRY(cudaMemcpyAsync((void*)out_cols[c].data, bufs[c].get(), (size_t)(m * es[c]), cudaMemcpyDeviceToHost, ctx->stream));
+    WG_CUDA_TRY(cudaMemcpyAsync(hv[c].data(), vals[c].get(), (size_t)m, cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  WG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  for (int c = 0; c < nk + na; ++c) {
+    uint64_t* w = (uint64_t*)out_cols[c].valid_words;
+    if (!w) continue;
+    for (int64_t i = 0; i < m; ++i) {
+      if (hv[c][i]) w[i >> 6] |= 1ULL << (i & 63);
+      else w[i >> 6] &= ~(1ULL << (i & 63));
+    }
+  }
+  *n_out = m;
+  return check_device_error(ctx);
+}
+
+wg_status wg_agg_reset(wg_agg* a) {
+  if (!a) return fail(WG_E_INVALID, "NULL argument");
+  WG_TRY(ensure_device(a->ctx));
+  a->finalized = false;
+  a->n_out = 0;
+  if (!a->resolved) return WG_OK;
+  Ctx* ctx = a->ctx;
+  const int64_t words = table_words(a, a->cap);
+  init_table_kernel<<<grid_cap(ctx, words, 256), 256, 0, ctx->stream>>>(a->table.as<unsigned long long>(), words,
+                                                                       a->L.slot_words, a->L);
+  ctx->count_launch();
+  WG_CUDA_TRY(cudaGetLastError());
+  WG_CUDA_TRY(cudaMemsetAsync(a->ctr.get(), 0, 64, ctx->stream));
+  a->known_groups = 0;
+  a->upper_groups = 0;
+  return WG_OK;
+}
+
+wg_status wg_agg_destroy(wg_agg* a) {
+  if (!a) return WG_OK;
+  ensure_device(a->ctx);
+  cudaStreamSynchronize(a->ctx->stream);
+  delete a;
+  return WG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,97 @@
+// wg_agg.cuh — device structures of the hash aggregate and the fused pipeline.
+//
+// The aggregate restates exec.HashAggregate's state (internal/engine/exec/
+// aggregate.go:1296-2613, agg_scatter.go) as one open-addressing table in HBM
+// whose slots hold the key and every accumulator inline (array-of-structs, so a
+// row touches one or two 32-byte sectors):
+//
+//   slot = [key words (0 scalar | 1 int key | 2 packed key)] [rows]
+//          [per aggregate: state words (0..2)] [per nullable aggregate: nulls]
+//
+// The per-aggregate non-NULL count is `rows - nulls`, so COUNT needs no state
+// and columns without NULLs cost no count traffic. Two extra slots follow the
+// table: [cap] holds the group whose key equals the empty sentinel, [cap+1]
+// the NULL key (single-key path, processRow's NULL group, aggregate.go:3422).
+#pragma once
+
+#include "wg_join.cuh"
+#include "wg_pred.cuh"
+
+#define WG_MAX_KEYS 4
+#define WG_MAX_AGGS 8
+#define WG_MAX_IN 8
+#define WG_MAX_EXPRS 2
+#define WG_MAX_FILTERS 4
+#define WG_MAX_SLOT_WORDS 32
+#define WG_EXPR_OPS 12
+
+#define WG_EMPTY_KEY 0x8000000000000001ULL   // -0x7FFFFFFFFFFFFFFF, intHashEmpty (int_hash.go:42)
+
+namespace wgd {
+
+enum Kind : int32_t {
+  K_COUNT = 0,
+  K_SUM_I64, K_SUM_F64, K_SUM_DEC,
+  K_MIN_I64, K_MAX_I64, K_MIN_F64, K_MAX_F64, K_MIN_DEC, K_MAX_DEC
+};
+
+__host__ __device__ __forceinline__ int kind_words(int k) {
+  return (k == K_COUNT) ? 0 : (k == K_SUM_DEC || k == K_MIN_DEC || k == K_MAX_DEC) ? 2 : 1;
+}
+
+struct AggD {
+  int32_t kind;
+  int32_t off;        // first state word, -1 when none
+  int32_t null_off;   // null-count word, -1 when the input has no NULLs
+  int32_t vcol;       // virtual input column, -1 = COUNT(*)
+};
+
+struct Layout {
+  int32_t key_words;
+  int32_t slot_words;
+  int32_t n_keys;
+  int32_t n_aggs;
+  int32_t key_vcol[WG_MAX_KEYS];
+  int32_t key_i32[WG_MAX_KEYS];    // packed field is 4 bytes wide
+  int32_t key_word[WG_MAX_KEYS];
+  int32_t key_shift[WG_MAX_KEYS];
+  AggD agg[WG_MAX_AGGS];
+  unsigned long long init[WG_MAX_SLOT_WORDS];   // empty-slot pattern
+};
+
+struct Table {
+  unsigned long long* slots;     // (cap + 2) * slot_words words
+  unsigned long long* n_groups;  // regular slots taken (reservations)
+  int32_t* overflow;             // set when an insert was refused at the limit
+  int32_t shift;
+  int32_t _pad;
+  uint64_t mask;                 // cap - 1
+  unsigned long long limit;      // max regular groups before inserts are refused
+};
+
+struct ExprD {
+  int32_t n_ops;
+  int32_t result_cls;            // WG_CLS_I64 or WG_CLS_F64
+  int32_t opc[WG_EXPR_OPS];
+  int32_t arg[WG_EXPR_OPS];
+  long long imm[WG_EXPR_OPS];    // int immediate, or the bits of a float immediate
+};
+
+struct Plan {
+  int64_t n_items;
+  const uint32_t* sel;           // nullptr = rows [0, n_items)
+  int32_t n_in, n_filters, has_join, n_exprs;
+  int32_t probe_col;
+  int32_t smem_slots;            // >0: CTA-private shared-memory table of this many slots
+  DCol in[WG_MAX_IN];
+  Pred filt[WG_MAX_FILTERS];
+  JoinView join;
+  ExprD expr[WG_MAX_EXPRS];
+  int32_t vcls[WG_MAX_IN + WG_MAX_PAYLOAD + WG_MAX_EXPRS];
+  int32_t vscale[WG_MAX_IN + WG_MAX_PAYLOAD + WG_MAX_EXPRS];
+  Layout L;
+  Table T;
+  int32_t* err;
+};
+
+}  // namespace wgd

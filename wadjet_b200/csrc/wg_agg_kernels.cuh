@@ -1,0 +1,434 @@
+// wg_agg_kernels.cuh — device code of the hash aggregate and the fused
+// filter → probe → project → aggregate kernel.
+#pragma once
+
+#include "wg_agg.cuh"
+
+namespace wgd {
+
+struct Val {
+  unsigned long long lo, hi;
+  bool null;
+};
+
+__device__ __forceinline__ Val load_val(const DCol& c, int64_t i) {
+  Val v;
+  v.hi = 0;
+  v.null = is_null(c, i);
+  switch (c.cls) {
+    case WG_CLS_I32: v.lo = (unsigned long long)(long long)__ldg((const int32_t*)c.data + i); break;
+    case WG_CLS_I64: v.lo = (unsigned long long)__ldg((const long long*)c.data + i); break;
+    case WG_CLS_F32: v.lo = (unsigned long long)__double_as_longlong((double)__ldg((const float*)c.data + i)); break;
+    case WG_CLS_F64: v.lo = (unsigned long long)__double_as_longlong(__ldg((const double*)c.data + i)); break;
+    case WG_CLS_DEC: {
+      const longlong2 d = __ldg((const longlong2*)c.data + i);
+      v.lo = (unsigned long long)d.y;
+      v.hi = (unsigned long long)d.x;
+      break;
+    }
+    default: v.lo = 0;
+  }
+  return v;
+}
+
+__device__ __forceinline__ Val fetch_base(const Plan& P, int j, int64_t row, int32_t brow) {
+  if (j < P.n_in) return load_val(P.in[j], row);
+  return load_val(P.join.pay[j - P.n_in], brow);
+}
+
+__device__ __forceinline__ double as_f(unsigned long long w) { return __longlong_as_double((long long)w); }
+__device__ __forceinline__ unsigned long long as_w(double d) { return (unsigned long long)__double_as_longlong(d); }
+
+// Postfix evaluation of a projection (expr.BinOpNumeric): integer ops wrap,
+// float ops are single IEEE operations (no contraction), DECIMAL operands read
+// as Int128.ToFloat64, a NULL operand makes the result NULL. The four-entry
+// stack is addressed through selects so it stays in registers.
+__device__ __forceinline__ Val eval_expr(const Plan& P, const ExprD& e, int64_t row, int32_t brow) {
+  unsigned long long s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+  unsigned fl = 0;  // bit i: stack entry i holds a float
+  int sp = 0;
+  bool null = false;
+  for (int k = 0; k < WG_EXPR_OPS; ++k) {
+    if (k >= e.n_ops) break;
+    const int opc = e.opc[k];
+    unsigned long long w = 0;
+    bool isf = false;
+    if (opc == 0) {  // WG_EXPR_COL
+      const int j = e.arg[k];
+      Val v = fetch_base(P, j, row, brow);
+      null |= v.null;
+      const int cls = P.vcls[j];
+      if (cls == WG_CLS_I32 || cls == WG_CLS_I64) { w = v.lo; isf = false; }
+      else if (cls == WG_CLS_DEC) { w = as_w(dec_to_f64((int64_t)v.hi, v.lo, P.vscale[j])); isf = true; }
+      else { w = v.lo; isf = true; }
+    } else if (opc == 1) {
+      w = (unsigned long long)e.imm[k]; isf = false;
+    } else if (opc == 2) {
+      w = (unsigned long long)e.imm[k]; isf = true;
+    } else {
+      if (sp < 2) { set_error(P.err, WG_DERR_STACK); Val r; r.lo = 0; r.hi = 0; r.null = true; return r; }
+      const unsigned long long b = sp == 1 ? s0 : sp == 2 ? s1 : sp == 3 ? s2 : s3;
+      const unsigned long long a = sp == 2 ? s0 : sp == 3 ? s1 : s2;
+      const bool bf = (fl >> (sp - 1)) & 1, af = (fl >> (sp - 2)) & 1;
+      sp -= 2;
+      if (opc == 7 || opc == 8) {  // SHR, AND (integers)
+        w = opc == 7 ? (unsigned long long)((long long)a >> (b & 63)) : (a & b);
+        isf = false;
+      } else if (!af && !bf && opc != 6) {
+        w = opc == 3 ? a + b : opc == 4 ? a - b : a * b;
+        isf = false;
+      } else {
+        const double x = af ? as_f(a) : __ll2double_rn((long long)a);
+        const double y = bf ? as_f(b) : __ll2double_rn((long long)b);
+        double r = 0.0;
+        switch (opc) {
+          case 3: r = __dadd_rn(x, y); break;
+          case 4: r = __dsub_rn(x, y); break;
+          case 5: r = __dmul_rn(x, y); break;
+          case 6: r = __ddiv_rn(x, y); break;
+        }
+        w = as_w(r);
+        isf = true;
+      }
+    }
+    if (sp >= 4) { set_error(P.err, WG_DERR_STACK); Val r; r.lo = 0; r.hi = 0; r.null = true; return r; }
+    if (sp == 0) s0 = w; else if (sp == 1) s1 = w; else if (sp == 2) s2 = w; else s3 = w;
+    fl = isf ? (fl | (1u << sp)) : (fl & ~(1u << sp));
+    ++sp;
+  }
+  Val r;
+  r.hi = 0;
+  r.null = null;
+  const unsigned long long top = sp == 1 ? s0 : sp == 2 ? s1 : sp == 3 ? s2 : s3;
+  const bool tf = sp > 0 && ((fl >> (sp - 1)) & 1);
+  if (e.result_cls == WG_CLS_F64 && !tf) r.lo = as_w(__ll2double_rn((long long)top));
+  else r.lo = top;
+  return r;
+}
+
+__device__ __forceinline__ Val fetch(const Plan& P, int j, int64_t row, int32_t brow) {
+  const int nb = P.n_in + P.join.n_pay;
+  if (j < nb) return fetch_base(P, j, row, brow);
+  return eval_expr(P, P.expr[j - nb], row, brow);
+}
+
+template <int NA>
+struct Contrib {
+  unsigned long long w0[NA], w1[NA];
+  int nul[NA];
+};
+
+// One row's contribution to each aggregate (the scatter kernels' per-row
+// update, internal/engine/exec/agg_scatter.go:178-510), as combinable words.
+template <int NA>
+__device__ __forceinline__ void make_contrib(const Plan& P, int64_t row, int32_t brow, Contrib<NA>& c) {
+  const Layout& L = P.L;
+#pragma unroll
+  for (int a = 0; a < NA; ++a) {
+    c.w0[a] = 0; c.w1[a] = 0; c.nul[a] = 0;
+    if (a >= L.n_aggs) continue;
+    const AggD g = L.agg[a];
+    if (g.vcol < 0 || g.kind == K_COUNT) {
+      if (g.vcol >= 0) c.nul[a] = fetch(P, g.vcol, row, brow).null ? 1 : 0;
+      continue;
+    }
+    const Val v = fetch(P, g.vcol, row, brow);
+    if (v.null) {
+      c.nul[a] = 1;
+      c.w0[a] = L.init[g.off];
+      if (kind_words(g.kind) == 2) c.w1[a] = L.init[g.off + 1];
+      continue;
+    }
+    const int cls = P.vcls[g.vcol];
+    switch (g.kind) {
+      case K_SUM_I64: case K_MIN_I64: case K_MAX_I64: c.w0[a] = v.lo; break;
+      case K_SUM_F64:
+        c.w0[a] = (cls == WG_CLS_I32 || cls == WG_CLS_I64) ? as_w(__ll2double_rn((long long)v.lo)) : v.lo;
+        break;
+      case K_MIN_F64: case K_MAX_F64: c.w0[a] = f64_to_ord(as_f(v.lo)); break;
+      default: c.w0[a] = v.lo; c.w1[a] = v.hi; break;  // DECIMAL kinds
+    }
+  }
+}
+
+__device__ __forceinline__ void combine(int kind, unsigned long long& a0, unsigned long long& a1, unsigned long long b0,
+                                        unsigned long long b1) {
+  switch (kind) {
+    case K_SUM_I64: a0 += b0; break;
+    case K_SUM_F64: a0 = as_w(__dadd_rn(as_f(a0), as_f(b0))); break;
+    case K_SUM_DEC: add128(a0, a1, b0, b1); break;
+    case K_MIN_I64: if ((long long)b0 < (long long)a0) a0 = b0; break;
+    case K_MAX_I64: if ((long long)b0 > (long long)a0) a0 = b0; break;
+    case K_MIN_F64: if (b0 < a0) a0 = b0; break;
+    case K_MAX_F64: if (b0 > a0) a0 = b0; break;
+    case K_MIN_DEC: if (less128(b0, b1, a0, a1)) { a0 = b0; a1 = b1; } break;
+    case K_MAX_DEC: if (less128(a0, a1, b0, b1)) { a0 = b0; a1 = b1; } break;
+    default: break;
+  }
+}
+
+// Fold a combined contribution into a slot (HBM or shared memory) with atomics.
+template <int NA>
+__device__ __forceinline__ void apply(const Layout& L, unsigned long long* s, const Contrib<NA>& c,
+                                      unsigned long long rows) {
+  atomicAdd(s + L.key_words, rows);
+#pragma unroll
+  for (int a = 0; a < NA; ++a) {
+    if (a >= L.n_aggs) continue;
+    const AggD g = L.agg[a];
+    const unsigned long long w0 = c.w0[a], w1 = c.w1[a];
+    switch (g.kind) {
+      case K_SUM_I64: if (w0) atomicAdd(s + g.off, w0); break;
+      case K_SUM_F64: { const double d = as_f(w0); if (d != 0.0) atomicAdd((double*)(s + g.off), d); } break;
+      case K_SUM_DEC: atomic_add128(s + g.off, w0, w1); break;
+      case K_MIN_I64: if (w0 != 0x7FFFFFFFFFFFFFFFULL) atomicMin((long long*)(s + g.off), (long long)w0); break;
+      case K_MAX_I64: if (w0 != 0x8000000000000000ULL) atomicMax((long long*)(s + g.off), (long long)w0); break;
+      case K_MIN_F64: if (w0 != ~0ULL) atomicMin(s + g.off, w0); break;
+      case K_MAX_F64: if (w0 != 0ULL) atomicMax(s + g.off, w0); break;
+      case K_MIN_DEC: atomic_min128((U128*)(s + g.off), w0, w1); break;
+      case K_MAX_DEC: atomic_max128((U128*)(s + g.off), w0, w1); break;
+      default: break;
+    }
+    if (g.null_off >= 0 && c.nul[a]) atomicAdd(s + g.null_off, (unsigned long long)c.nul[a]);
+  }
+}
+
+// Contribution held by a whole slot (shared-memory flush, merge, migration).
+template <int NA>
+__device__ __forceinline__ void slot_contrib(const Layout& L, const unsigned long long* s, Contrib<NA>& c) {
+#pragma unroll
+  for (int a = 0; a < NA; ++a) {
+    c.w0[a] = 0; c.w1[a] = 0; c.nul[a] = 0;
+    if (a >= L.n_aggs) continue;
+    const AggD g = L.agg[a];
+    if (g.off >= 0) { c.w0[a] = s[g.off]; if (kind_words(g.kind) == 2) c.w1[a] = s[g.off + 1]; }
+    if (g.null_off >= 0) c.nul[a] = (int)s[g.null_off];
+  }
+}
+
+// Find or insert the global slot of a key. Inserting claims a group
+// reservation first; past T.limit the insert is refused and the overflow flag
+// raised (the host then replays the launch on a larger table).
+__device__ __forceinline__ unsigned long long* find_global(const Layout& L, const Table& T, unsigned long long k0,
+                                                           unsigned long long k1, bool keynull, int32_t* err) {
+  const int sw = L.slot_words;
+  if (L.key_words == 0) return T.slots;
+  const uint64_t cap = T.mask + 1;
+  if (keynull) return T.slots + (cap + 1) * sw;
+  if (L.key_words == 1) {
+    if (k0 == WG_EMPTY_KEY) return T.slots + cap * sw;
+    uint64_t h = fib_slot(k0, T.shift);
+    for (uint64_t probe = 0; probe <= T.mask; ++probe) {
+      unsigned long long* s = T.slots + h * sw;
+      unsigned long long cur = *((volatile unsigned long long*)s);
+      if (cur == k0) return s;
+      if (cur == WG_EMPTY_KEY) {
+        unsigned long long r = atomicAdd(T.n_groups, 1ULL);
+        if (r >= T.limit) {
+          atomicAdd(T.n_groups, ~0ULL);
+          *T.overflow = 1;
+          return nullptr;
+        }
+        unsigned long long old = atomicCAS(s, WG_EMPTY_KEY, k0);
+        if (old == WG_EMPTY_KEY) return s;
+        atomicAdd(T.n_groups, ~0ULL);
+        if (old == k0) return s;
+      }
+      h = (h + 1) & T.mask;
+    }
+  } else {
+    if (k0 == ~0ULL && k1 == ~0ULL) return T.slots + cap * sw;
+    uint64_t h = packed_slot(k0, k1, T.shift);
+    for (uint64_t probe = 0; probe <= T.mask; ++probe) {
+      unsigned long long* s = T.slots + h * sw;
+      // A slot's key words change once, from {~0,~0} to the key. A read with
+      // neither word ~0 is therefore the complete key; anything else is settled
+      // by the 128-bit CAS below.
+      const U128 cur = read128(s);
+      if (cur.lo != ~0ULL && cur.hi != ~0ULL) {
+        if (cur.lo == k0 && cur.hi == k1) return s;
+      } else {
+        unsigned long long r = atomicAdd(T.n_groups, 1ULL);
+        if (r >= T.limit) {
+          atomicAdd(T.n_groups, ~0ULL);
+          *T.overflow = 1;
+          return nullptr;
+        }
+        U128 e; e.lo = ~0ULL; e.hi = ~0ULL;
+        U128 k; k.lo = k0; k.hi = k1;
+        U128 old = cas128((U128*)s, e, k);
+        if (old.lo == e.lo && old.hi == e.hi) return s;
+        atomicAdd(T.n_groups, ~0ULL);
+        if (old.lo == k0 && old.hi == k1) return s;
+      }
+      h = (h + 1) & T.mask;
+    }
+  }
+  set_error(err, WG_DERR_TABLE_FULL);
+  return nullptr;
+}
+
+// CTA-private shared-memory table (single int64 key, no NULL words). Returns
+// nullptr when the key is absent and the table has reached its fill limit.
+__device__ __forceinline__ unsigned long long* find_smem(unsigned long long* sm, int S, int sw,
+                                                         unsigned long long k0, int* s_groups, int s_limit) {
+  if (k0 == WG_EMPTY_KEY) return nullptr;
+  uint32_t h = (uint32_t)__umul64hi(k0 * 0x9E3779B97F4A7C15ULL, (unsigned long long)S);
+  for (int p = 0; p < S; ++p) {
+    unsigned long long* s = sm + (size_t)h * sw;
+    unsigned long long cur = *((volatile unsigned long long*)s);
+    if (cur == k0) return s;
+    if (cur == WG_EMPTY_KEY) {
+      if (*((volatile int*)s_groups) >= s_limit) return nullptr;
+      unsigned long long old = atomicCAS(s, WG_EMPTY_KEY, k0);
+      if (old == WG_EMPTY_KEY) { atomicAdd(s_groups, 1); return s; }
+      if (old == k0) return s;
+    }
+    h = (h + 1 == (uint32_t)S) ? 0u : h + 1;
+  }
+  return nullptr;
+}
+
+// Warp-cooperative update: lanes holding the same key pre-combine their
+// contributions (__match_any_sync) and only the group's lowest lane touches the
+// table, so hot keys cost one set of atomics per warp instead of one per row.
+template <int NA, bool SMEM>
+__device__ __forceinline__ void warp_update(const Plan& P, bool cur, unsigned long long k0, unsigned long long k1,
+                                            bool knull, Contrib<NA>& c, unsigned long long* sm, int* s_groups,
+                                            int s_limit) {
+  const Layout& L = P.L;
+  const unsigned am = __ballot_sync(WG_FULL_MASK, cur);
+  if (am == 0) return;
+  const int lane = threadIdx.x & 31;
+  unsigned peers = __match_any_sync(WG_FULL_MASK, k0);
+  if (L.key_words == 2) peers &= __match_any_sync(WG_FULL_MASK, k1);
+  peers &= __match_any_sync(WG_FULL_MASK, knull ? 1u : 0u);
+  peers &= am;
+  const int mysz = cur ? __popc(peers) : 0;
+  const bool leader = cur && (__ffs(peers) - 1) == lane;
+  const int maxsz = (int)__reduce_max_sync(WG_FULL_MASK, (unsigned)mysz);
+  for (int i = 1; i < maxsz; ++i) {
+    const bool take = leader && i < mysz;
+    const int src = take ? (int)__fns(peers, 0, i + 1) : lane;
+#pragma unroll
+    for (int a = 0; a < NA; ++a) {
+      if (a >= L.n_aggs) continue;
+      const AggD g = L.agg[a];
+      const int kw = kind_words(g.kind);
+      unsigned long long b0 = 0, b1 = 0;
+      int bn = 0;
+      if (kw >= 1) b0 = __shfl_sync(WG_FULL_MASK, c.w0[a], src);
+      if (kw == 2) b1 = __shfl_sync(WG_FULL_MASK, c.w1[a], src);
+      if (g.null_off >= 0) bn = __shfl_sync(WG_FULL_MASK, c.nul[a], src);
+      if (take) {
+        combine(g.kind, c.w0[a], c.w1[a], b0, b1);
+        c.nul[a] += bn;
+      }
+    }
+  }
+  if (leader) {
+    unsigned long long* s = nullptr;
+    if (SMEM && !knull) s = find_smem(sm, P.smem_slots, L.slot_words, k0, s_groups, s_limit);
+    if (s == nullptr) s = find_global(L, P.T, k0, k1, knull, P.err);
+    if (s != nullptr) apply<NA>(L, s, c, (unsigned long long)mysz);
+  }
+}
+
+// Group key of one (row, build row): the int-key path widens to int64
+// (consumeBatchIntGroup, aggregate.go:1908); the packed path places each column
+// by buildPackedLayout (packed_hash.go:386) as packedKeyAt does (:456).
+__device__ __forceinline__ bool make_key(const Plan& P, int64_t row, int32_t brow, unsigned long long& k0,
+                                         unsigned long long& k1, bool& knull) {
+  const Layout& L = P.L;
+  k0 = 0; k1 = 0; knull = false;
+  if (L.key_words == 0) return true;
+  if (L.key_words == 1) {
+    Val v = fetch(P, L.key_vcol[0], row, brow);
+    knull = v.null;
+    k0 = v.null ? 0 : v.lo;
+    return true;
+  }
+  for (int k = 0; k < WG_MAX_KEYS; ++k) {
+    if (k >= L.n_keys) break;
+    Val v = fetch(P, L.key_vcol[k], row, brow);
+    if (v.null) { set_error(P.err, WG_DERR_NULL_PACKED); return false; }
+    const unsigned long long w = L.key_i32[k] ? ((unsigned long long)(uint32_t)(int32_t)v.lo) << L.key_shift[k] : v.lo;
+    if (L.key_word[k] == 0) k0 |= w; else k1 |= w;
+  }
+  return true;
+}
+
+// The fused pipeline: KernelFilter chain → HashJoinProbe → Project →
+// HashAggregate.Consume for every input row, one warp per 32 consecutive rows.
+template <int NA, bool SMEM>
+__global__ void __launch_bounds__(512) pipeline_kernel(const __grid_constant__ Plan P) {
+  extern __shared__ unsigned long long sm[];
+  __shared__ int s_groups;
+  const Layout& L = P.L;
+  const int S = P.smem_slots;
+  const int s_limit = (S * 7) / 8;
+  if (SMEM) {
+    const int sw = L.slot_words;
+    for (int i = threadIdx.x; i < S * sw; i += blockDim.x) sm[i] = L.init[i % sw];
+    if (threadIdx.x == 0) s_groups = 0;
+    __syncthreads();
+  }
+  const int lane = threadIdx.x & 31;
+  const int64_t wpb = blockDim.x >> 5;
+  const int64_t total_warps = (int64_t)gridDim.x * wpb;
+  for (int64_t base = ((int64_t)blockIdx.x * wpb + (threadIdx.x >> 5)) * 32; base < P.n_items;
+       base += total_warps * 32) {
+    const int64_t item = base + lane;
+    bool act = item < P.n_items;
+    int64_t row = 0;
+    if (act) row = P.sel ? (int64_t)__ldg(P.sel + item) : item;
+    for (int f = 0; f < WG_MAX_FILTERS; ++f) {
+      if (f >= P.n_filters) break;
+      if (act) act = pred_row(P.filt[f], P.in[P.filt[f].col], row);
+    }
+    int32_t brow = -1;
+    if (P.has_join && act) {
+      const Val kv = load_val(P.in[P.probe_col], row);
+      if (kv.null) act = false;
+      else {
+        brow = join_head(P.join, (int64_t)kv.lo, P.err);
+        act = brow >= 0;
+      }
+    }
+    for (;;) {
+      if (!__any_sync(WG_FULL_MASK, act)) break;
+      unsigned long long k0 = 0, k1 = 0;
+      bool knull = false;
+      Contrib<NA> c;
+      bool cur = act;
+      if (cur) {
+        cur = make_key(P, row, brow, k0, k1, knull);
+        make_contrib<NA>(P, row, brow, c);
+      } else {
+#pragma unroll
+        for (int a = 0; a < NA; ++a) { c.w0[a] = 0; c.w1[a] = 0; c.nul[a] = 0; }
+      }
+      warp_update<NA, SMEM>(P, cur, k0, k1, knull, c, sm, &s_groups, s_limit);
+      if (!P.has_join) break;
+      if (act) {
+        brow = __ldg(P.join.next + brow);
+        act = brow >= 0;
+      }
+    }
+  }
+  if (SMEM) {
+    __syncthreads();
+    const int sw = L.slot_words;
+    for (int i = threadIdx.x; i < S; i += blockDim.x) {
+      const unsigned long long* s = sm + (size_t)i * sw;
+      if (s[0] == WG_EMPTY_KEY) continue;
+      unsigned long long* g = find_global(L, P.T, s[0], 0, false, P.err);
+      if (g == nullptr) continue;
+      Contrib<NA> c;
+      slot_contrib<NA>(L, s, c);
+      apply<NA>(L, g, c, s[L.key_words]);
+    }
+  }
+}
+
+}  // namespace wgd

@@ -1,0 +1,324 @@
+// wg_filter.cu — exec.KernelFilter on the GPU (internal/engine/exec/filter.go:347-425).
+//
+// One pass over the column: each thread evaluates 4 × V rows with 128-bit
+// vector loads (V = 16 / element size), every row's verdict becomes a bit of a
+// warp ballot-style count, a block-wide scan orders the survivors, and the
+// tile's position in the output comes from a decoupled look-back over the
+// preceding tiles (Merrill & Garland, "Single-pass Parallel Prefix Scan with
+// Decoupled Look-back", NVIDIA TR 2016). Output is the ascending selection
+// vector the reference's compaction produces, so the result is bit-exact.
+// Every wait on a predecessor tile is bounded; on expiry the kernel records
+// WG_DERR_TIMEOUT and publishes its own state so no successor waits forever.
+#include "wg_internal.h"
+#include "wg_pred.cuh"
+
+namespace wg {
+
+// Resolve a predicate constant against the column type (ResolveFilterKernel,
+// internal/engine/exec/kernel/compare.go:145-182; toInt64/toFloat64/toDateInt32 :580-640).
+wg_status resolve_pred(const wg_predicate& p, int32_t type_id, wgd::Pred* out) {
+  if (p.op < WG_OP_EQ || p.op > WG_OP_GE) return fail(WG_E_INVALID, "unknown compare op");
+  auto to_i64 = [&]() -> long long {
+    if (p.const_kind == WG_CONST_FLOAT) {
+      double f = p.const_f64;  // Go float64→int64 on amd64: out of range gives MinInt64
+      if (!(f >= -9223372036854775808.0 && f < 9223372036854775808.0)) return INT64_MIN;
+      return (long long)f;
+    }
+    return p.const_i64;
+  };
+  auto to_f64 = [&]() -> double { return p.const_kind == WG_CONST_FLOAT ? p.const_f64 : (double)p.const_i64; };
+  out->col = p.col;
+  out->op = p.op;
+  out->_pad = 0;
+  out->ci = 0;
+  out->cf = 0;
+  switch (type_id) {
+    case WG_TYPE_INT64: case WG_TYPE_TIMESTAMP: case WG_TYPE_DURATION: case WG_TYPE_IPV4: case WG_TYPE_MAC:
+      out->cls = WG_CLS_I64; out->ci = to_i64(); return WG_OK;
+    case WG_TYPE_INT32: case WG_TYPE_PORT: case WG_TYPE_PROTOCOL:
+      out->cls = WG_CLS_I32; out->ci = (int32_t)to_i64(); return WG_OK;
+    case WG_TYPE_DATE:
+      out->cls = WG_CLS_I32; out->ci = p.const_kind == WG_CONST_FLOAT ? 0 : (int32_t)p.const_i64; return WG_OK;
+    case WG_TYPE_FLOAT64:
+      out->cls = WG_CLS_F64; out->cf = to_f64(); return WG_OK;
+    case WG_TYPE_FLOAT32:
+      out->cls = WG_CLS_F32; out->cf = (double)(float)to_f64(); return WG_OK;
+    default:
+      return fail(WG_E_UNSUPPORTED, "filter on this column type is not on the GPU path");
+  }
+}
+
+}  // namespace wg
+
+namespace {
+
+using namespace wgd;
+
+constexpr int kBlock = 256;
+constexpr int kRows = 4;
+constexpr unsigned long long kFlagAgg = 1ULL << 62;
+constexpr unsigned long long kFlagInc = 2ULL << 62;
+constexpr unsigned long long kValMask = (1ULL << 62) - 1;
+constexpr long long kSpinLimit = 1LL << 22;
+
+struct FilterArgs {
+  DCol col;
+  Pred p;
+  const uint32_t* sel;   // nullptr = rows 0..n-1
+  int64_t n;             // items: rows, or selection entries
+  uint32_t* out;
+  unsigned long long* status;
+  int* tile_counter;
+  int64_t* out_n;
+  int32_t* err;
+  int64_t num_tiles;
+};
+
+template <typename T> struct VecOf;
+template <> struct VecOf<int32_t> { using type = int4; };
+template <> struct VecOf<float> { using type = float4; };
+template <> struct VecOf<long long> { using type = longlong2; };
+template <> struct VecOf<double> { using type = double2; };
+
+template <int CLS> struct ClsT;
+template <> struct ClsT<WG_CLS_I32> { using T = int32_t; };
+template <> struct ClsT<WG_CLS_I64> { using T = long long; };
+template <> struct ClsT<WG_CLS_F32> { using T = float; };
+template <> struct ClsT<WG_CLS_F64> { using T = double; };
+
+template <int CLS, bool VEC>
+__global__ void __launch_bounds__(kBlock) filter_compact_kernel(const FilterArgs a) {
+  using T = typename ClsT<CLS>::T;
+  constexpr int V = VEC ? (int)(16 / sizeof(T)) : 1;
+  constexpr int64_t kTile = (int64_t)kBlock * V * kRows;
+  __shared__ int s_tile;
+  __shared__ int s_warp[kRows][kBlock / 32];
+  __shared__ int s_total;
+  __shared__ long long s_prefix;
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) s_tile = atomicAdd(a.tile_counter, 1);
+  __syncthreads();
+  const int64_t tile = s_tile;
+  const int64_t tile_base = tile * kTile;
+  const T cval = (CLS == WG_CLS_F32 || CLS == WG_CLS_F64) ? (T)a.p.cf : (T)a.p.ci;
+
+  unsigned bits[kRows];
+  int excl[kRows];
+#pragma unroll
+  for (int r = 0; r < kRows; ++r) {
+    const int64_t i0 = tile_base + ((int64_t)r * kBlock + tid) * V;
+    unsigned b = 0;
+    if (a.sel == nullptr && VEC && i0 + V <= a.n) {
+      typename VecOf<T>::type v = __ldg(reinterpret_cast<const typename VecOf<T>::type*>((const T*)a.col.data + i0));
+      const T* e = reinterpret_cast<const T*>(&v);
+#pragma unroll
+      for (int k = 0; k < V; ++k)
+        if (cmp_op<T>(e[k], cval, a.p.op) && !is_null(a.col, i0 + k)) b |= 1u << k;
+    } else {
+#pragma unroll
+      for (int k = 0; k < V; ++k) {
+        const int64_t it = i0 + k;
+        if (it < a.n) {
+          const int64_t row = a.sel ? (int64_t)__ldg(a.sel + it) : it;
+          if (!is_null(a.col, row) && cmp_op<T>(__ldg((const T*)a.col.data + row), cval, a.p.op)) b |= 1u << k;
+        }
+      }
+    }
+    bits[r] = b;
+    // warp inclusive scan of this thread's survivor count
+    int c = __popc(b), incl = c;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      int y = __shfl_up_sync(WG_FULL_MASK, incl, d);
+      if (lane >= d) incl += y;
+    }
+    excl[r] = incl - c;
+    if (lane == 31) s_warp[r][warp] = incl;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    int run = 0;
+    for (int r = 0; r < kRows; ++r)
+      for (int w = 0; w < kBlock / 32; ++w) { int t = s_warp[r][w]; s_warp[r][w] = run; run += t; }
+    s_total = run;
+    // decoupled look-back
+    long long prefix = 0;
+    if (tile == 0) {
+      atomicExch(a.status, kFlagInc | (unsigned long long)run);
+    } else {
+      atomicExch(a.status + tile, kFlagAgg | (unsigned long long)run);
+      int64_t pred = tile - 1;
+      long long spins = 0;
+      while (pred >= 0) {
+        unsigned long long s = *((volatile unsigned long long*)(a.status + pred));
+        unsigned long long flag = s & ~kValMask;
+        if (flag == 0) {
+          if (++spins > kSpinLimit) { set_error(a.err, WG_DERR_TIMEOUT); break; }
+          __nanosleep(64);
+          continue;
+        }
+        prefix += (long long)(s & kValMask);
+        if (flag == kFlagInc) break;
+        --pred;
+      }
+      atomicExch(a.status + tile, kFlagInc | (unsigned long long)(prefix + run));
+    }
+    s_prefix = prefix;
+    if (tile == a.num_tiles - 1) *a.out_n = prefix + run;
+  }
+  __syncthreads();
+  const long long prefix = s_prefix;
+#pragma unroll
+  for (int r = 0; r < kRows; ++r) {
+    unsigned b = bits[r];
+    if (!b) continue;
+    long long pos = prefix + s_warp[r][warp] + excl[r];
+    const int64_t i0 = tile_base + ((int64_t)r * kBlock + tid) * V;
+#pragma unroll
+    for (int k = 0; k < V; ++k)
+      if (b & (1u << k)) a.out[pos++] = a.sel ? __ldg(a.sel + i0 + k) : (uint32_t)(i0 + k);
+  }
+}
+
+template <int CLS>
+void launch_cls(bool vec, const FilterArgs& a, dim3 grid, cudaStream_t s) {
+  if (vec) filter_compact_kernel<CLS, true><<<grid, kBlock, 0, s>>>(a);
+  else filter_compact_kernel<CLS, false><<<grid, kBlock, 0, s>>>(a);
+}
+
+}  // namespace
+
+struct wg_filter {
+  wg::Ctx* ctx;
+  wg_predicate pred;
+  bool resolved = false;
+  int32_t type_id = -1;
+  wgd::Pred dp{};
+  wg::DevBuf status, counter, out_sel, out_n;
+  wg::StagedBatch staged;
+};
+
+namespace wg {
+
+// Run the compaction over a device-resident column; *n_out is left on the device.
+wg_status filter_launch(Ctx* ctx, const wgd::Pred& p, const wg_column& col, const uint32_t* sel, int64_t n_items,
+                        uint32_t* out, int64_t* n_out_dev, DevBuf& status, DevBuf& counter) {
+  const int cls = class_of(col.type_id);
+  const int64_t es = elem_size(col.type_id);
+  const bool vec = sel == nullptr && ((uintptr_t)col.data % 16 == 0);
+  const int64_t V = vec ? 16 / es : 1;
+  const int64_t tile = (int64_t)kBlock * V * kRows;
+  const int64_t tiles = (n_items + tile - 1) / tile;
+  if (tiles == 0) {
+    WG_CUDA_TRY(cudaMemsetAsync(n_out_dev, 0, sizeof(int64_t), ctx->stream));
+    return WG_OK;
+  }
+  if (tiles > (1LL << 31) - 1) return fail(WG_E_INVALID, "batch too large");
+  WG_TRY(status.ensure(ctx, tiles * 8));
+  WG_TRY(counter.ensure(ctx, 16));
+  WG_CUDA_TRY(cudaMemsetAsync(status.get(), 0, (size_t)(tiles * 8), ctx->stream));
+  WG_CUDA_TRY(cudaMemsetAsync(counter.get(), 0, sizeof(int), ctx->stream));
+  FilterArgs a;
+  a.col = wgd::DCol{col.data, col.valid_words, cls, col.scale};
+  a.p = p;
+  a.sel = sel;
+  a.n = n_items;
+  a.out = out;
+  a.status = status.as<unsigned long long>();
+  a.tile_counter = counter.as<int>();
+  a.out_n = n_out_dev;
+  a.err = ctx->dev_error;
+  a.num_tiles = tiles;
+  dim3 grid((unsigned)tiles);
+  switch (cls) {
+    case WG_CLS_I32: launch_cls<WG_CLS_I32>(vec, a, grid, ctx->stream); break;
+    case WG_CLS_I64: launch_cls<WG_CLS_I64>(vec, a, grid, ctx->stream); break;
+    case WG_CLS_F32: launch_cls<WG_CLS_F32>(vec, a, grid, ctx->stream); break;
+    case WG_CLS_F64: launch_cls<WG_CLS_F64>(vec, a, grid, ctx->stream); break;
+    default: return fail(WG_E_UNSUPPORTED, "filter on this column type is not on the GPU path");
+  }
+  ctx->count_launch();
+  WG_CUDA_TRY(cudaGetLastError());
+  return WG_OK;
+}
+
+}  // namespace wg
+
+using namespace wg;
+
+static wg_status filter_resolve(wg_filter* f, const wg_batch_desc* in) {
+  if (!in) return fail(WG_E_INVALID, "batch is NULL");
+  if (f->pred.col < 0 || f->pred.col >= in->ncols)
+    return fail(WG_E_INVALID, "filter column " + std::to_string(f->pred.col) + " does not exist in the input schema");
+  const int32_t t = in->cols[f->pred.col].type_id;
+  if (!f->resolved) {
+    WG_TRY(resolve_pred(f->pred, t, &f->dp));
+    f->type_id = t;
+    f->resolved = true;
+  } else if (t != f->type_id) {
+    return fail(WG_E_INVALID, "filter column changed type after the kernel was resolved");
+  }
+  return WG_OK;
+}
+
+extern "C" {
+
+wg_status wg_filter_create(wg_ctx* ctx, int32_t col_idx, int32_t op, int32_t const_kind, int64_t const_i64,
+                           double const_f64, wg_filter** out) {
+  if (!ctx || !out) return fail(WG_E_INVALID, "NULL argument");
+  if (op < WG_OP_EQ || op > WG_OP_GE) return fail(WG_E_INVALID, "unknown compare op");
+  if (const_kind != WG_CONST_INT && const_kind != WG_CONST_FLOAT) return fail(WG_E_INVALID, "unknown constant kind");
+  wg_filter* f = new wg_filter();
+  f->ctx = ctx;
+  f->pred = wg_predicate{col_idx, op, const_kind, 0, const_i64, const_f64};
+  *out = f;
+  return WG_OK;
+}
+
+wg_status wg_filter_execute_device(wg_filter* f, const wg_batch_desc* in, uint32_t* out_sel_dev, int64_t* out_n) {
+  if (!f || !out_n) return fail(WG_E_INVALID, "NULL argument");
+  WG_TRY(ensure_device(f->ctx));
+  WG_TRY(filter_resolve(f, in));
+  Ctx* ctx = f->ctx;
+  const int64_t n_items = in->sel ? in->sel_len : in->len;
+  WG_TRY(f->out_n.ensure(ctx, 16));
+  WG_TRY(filter_launch(ctx, f->dp, in->cols[f->pred.col], in->sel, n_items, out_sel_dev, f->out_n.as<int64_t>(),
+                       f->status, f->counter));
+  WG_TRY(read_back_i64(ctx, f->out_n.as<int64_t>(), out_n, 1));
+  return check_device_error(ctx);
+}
+
+wg_status wg_filter_execute(wg_filter* f, const wg_batch_desc* in, uint32_t* out_sel, int64_t* out_n) {
+  if (!f || !out_n || !out_sel) return fail(WG_E_INVALID, "NULL argument");
+  WG_TRY(ensure_device(f->ctx));
+  WG_TRY(filter_resolve(f, in));
+  Ctx* ctx = f->ctx;
+  // stage only the filtered column (and the selection vector)
+  wg_column only = in->cols[f->pred.col];
+  wg_batch_desc one{1, 0, &only, in->len, in->sel, in->sel_len};
+  WG_TRY(stage_batch(ctx, &one, &f->staged));
+  const int64_t n_items = in->sel ? in->sel_len : in->len;
+  WG_TRY(f->out_sel.ensure(ctx, std::max<int64_t>(n_items * 4, 16)));
+  WG_TRY(f->out_n.ensure(ctx, 16));
+  wgd::Pred p = f->dp;
+  WG_TRY(filter_launch(ctx, p, f->staged.cols[0], f->staged.desc.sel, n_items, f->out_sel.as<uint32_t>(),
+                       f->out_n.as<int64_t>(), f->status, f->counter));
+  WG_TRY(read_back_i64(ctx, f->out_n.as<int64_t>(), out_n, 1));
+  WG_TRY(check_device_error(ctx));
+  if (*out_n > 0) {
+    WG_CUDA_TRY(cudaMemcpyAsync(out_sel, f->out_sel.get(), (size_t)(*out_n * 4), cudaMemcpyDeviceToHost, ctx->stream));
+    WG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  }
+  return WG_OK;
+}
+
+wg_status wg_filter_destroy(wg_filter* f) {
+  if (!f) return WG_OK;
+  ensure_device(f->ctx);
+  cudaStreamSynchronize(f->ctx->stream);
+  delete f;
+  return WG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,539 @@
+// wg_join.cu — exec.HashJoin (inner, int key) on the GPU.
+//
+// Build (HashJoin.Build, internal/engine/exec/join.go:771 → arenaAppendInt :551):
+// build batches are appended to device-resident key/payload columns; finish
+// sizes an open-addressing table at <= 50% load and inserts every non-NULL key
+// with one thread per build row. A 64-bit (or 128-bit) atomicCAS swaps the
+// slot's head to the inserting row and the replaced head becomes next[row] —
+// the chained arena of the reference, built in parallel. Chains hold the same
+// rows as the reference's; their order among equal keys is the order the
+// atomics landed in, which a canonical sort of the join output makes moot.
+//
+// Probe (HashJoinProbe.Execute → inlineIntProbe, join.go:2306,2670) with the
+// bounded-output protocol (operators.go:86): pairs are counted per probe row,
+// scanned, and the window [cursor, cursor + cap) of the ordered pair list is
+// written.
+#include "wg_internal.h"
+#include "wg_join.cuh"
+
+#include <cub/cub.cuh>
+
+namespace {
+
+using namespace wgd;
+
+constexpr long long kCasLimit = 1LL << 24;
+
+struct BuildArgs {
+  DCol key;
+  int64_t n;
+  int32_t flavor;
+  int32_t shift;
+  uint64_t mask;
+  void* slots;
+  int32_t* next;
+  unsigned long long* distinct;
+  int32_t* dup;
+  int32_t* err;
+};
+
+__global__ void join_build_kernel(const BuildArgs a) {
+  for (int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < a.n;
+       row += (int64_t)gridDim.x * blockDim.x) {
+    if (is_null(a.key, row)) continue;
+    const int64_t key = ld_i64(a.key, row);
+    uint64_t h = fib_slot((uint64_t)key, a.shift);
+    uint64_t probes = 0;
+    long long spins = 0;
+    bool done = false;
+    if (a.flavor == 0) {
+      unsigned long long* s = (unsigned long long*)a.slots;
+      const unsigned long long mine = ((unsigned long long)(uint32_t)row << 32) | (uint32_t)(int32_t)key;
+      unsigned long long cur = *((volatile unsigned long long*)(s + h));
+      while (!done) {
+        if (++spins > kCasLimit) { set_error(a.err, WG_DERR_TIMEOUT); break; }
+        const int32_t head = (int32_t)(cur >> 32);
+        if (head == -1 || (uint32_t)cur == (uint32_t)(int32_t)key) {
+          unsigned long long old = atomicCAS(s + h, cur, mine);
+          if (old == cur) {
+            a.next[row] = head;
+            if (head == -1) atomicAdd(a.distinct, 1ULL); else *a.dup = 1;
+            done = true;
+          } else {
+            cur = old;  // lost a race on this slot: re-examine it
+          }
+        } else {
+          if (++probes > a.mask) { set_error(a.err, WG_DERR_TABLE_FULL); break; }
+          h = (h + 1) & a.mask;
+          cur = *((volatile unsigned long long*)(s + h));
+        }
+      }
+    } else {
+      U128* s = (U128*)a.slots;
+      U128 mine;
+      mine.lo = (unsigned long long)key;
+      mine.hi = (unsigned long long)(uint32_t)row;
+      U128 cur = read128(s + h);  // may be torn; every decision is confirmed by a CAS
+      while (!done) {
+        if (++spins > kCasLimit) { set_error(a.err, WG_DERR_TIMEOUT); break; }
+        const int32_t head = (int32_t)(uint32_t)cur.hi;
+        if (head == -1 || (int64_t)cur.lo == key) {
+          U128 old = cas128(s + h, cur, mine);
+          if (old.lo == cur.lo && old.hi == cur.hi) {
+            a.next[row] = head;
+            if (head == -1) atomicAdd(a.distinct, 1ULL); else *a.dup = 1;
+            done = true;
+          } else {
+            cur = old;
+          }
+        } else {
+          const U128 chk = cas128(s + h, cur, cur);  // the slot really holds another key?
+          if (chk.lo != cur.lo || chk.hi != cur.hi) { cur = chk; continue; }
+          if (++probes > a.mask) { set_error(a.err, WG_DERR_TABLE_FULL); break; }
+          h = (h + 1) & a.mask;
+          cur = read128(s + h);
+        }
+      }
+    }
+  }
+}
+
+struct ProbeArgs {
+  JoinView j;
+  DCol key;
+  const uint32_t* sel;
+  int64_t n;
+  int64_t* counts;
+  const int64_t* offs;
+  int64_t cursor;
+  int64_t cap;
+  uint32_t* out_probe;
+  int64_t* out_build;
+  int32_t* err;
+};
+
+__global__ void join_probe_count_kernel(const ProbeArgs a) {
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < a.n; p += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t row = a.sel ? (int64_t)a.sel[p] : p;
+    int64_t c = 0;
+    if (!is_null(a.key, row)) {
+      for (int32_t ref = join_head(a.j, ld_i64(a.key, row), a.err); ref >= 0; ref = __ldg(a.j.next + ref)) ++c;
+    }
+    a.counts[p] = c;
+  }
+}
+
+__global__ void join_probe_emit_kernel(const ProbeArgs a) {
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < a.n; p += (int64_t)gridDim.x * blockDim.x) {
+    if (a.counts[p] == 0) continue;
+    int64_t j = a.offs[p];
+    if (j >= a.cursor + a.cap || j + a.counts[p] <= a.cursor) continue;
+    const int64_t row = a.sel ? (int64_t)a.sel[p] : p;
+    for (int32_t ref = join_head(a.j, ld_i64(a.key, row), a.err); ref >= 0 && j < a.cursor + a.cap;
+         ref = __ldg(a.j.next + ref), ++j) {
+      if (j >= a.cursor) {
+        a.out_probe[j - a.cursor] = (uint32_t)row;
+        a.out_build[j - a.cursor] = ref;
+      }
+    }
+  }
+}
+
+// Longest chain (max build rows sharing one key): the join's worst fan-out.
+__global__ void join_fanout_kernel(JoinView j, unsigned long long* max_len) {
+  const uint64_t cap = j.mask + 1;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cap; i += (uint64_t)gridDim.x * blockDim.x) {
+    int32_t head;
+    if (j.flavor == 0) head = (int32_t)(((const unsigned long long*)j.slots)[i] >> 32);
+    else head = (int32_t)(uint32_t)((const longlong2*)j.slots)[i].y;
+    if (head < 0) continue;
+    unsigned long long c = 0;
+    for (int32_t r = head; r >= 0; r = j.next[r]) ++c;
+    atomicMax(max_len, c);
+  }
+}
+
+__global__ void gather_kernel(const char* src, int64_t es, const uint64_t* valid, const int64_t* rows, int64_t n,
+                              char* dst, uint8_t* dst_valid) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = rows[i];
+    for (int64_t b = 0; b < es; ++b) dst[i * es + b] = src[r * es + b];
+    if (dst_valid) dst_valid[i] = valid ? (uint8_t)((valid[r >> 6] >> (r & 63)) & 1ULL) : (uint8_t)1;
+  }
+}
+
+// Clear the bits of NULL rows of src into dst (all-ones initialised) at bit offset off.
+__global__ void append_valid_kernel(uint32_t* dst, int64_t off, const uint64_t* src, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    if (((src[i >> 6] >> (i & 63)) & 1ULL) == 0) {
+      const int64_t b = off + i;
+      atomicAnd(dst + (b >> 5), ~(1u << (b & 31)));
+    }
+  }
+}
+
+unsigned grid_for(wg::Ctx* ctx, int64_t n, int block) {
+  int64_t blocks = (n + block - 1) / block;
+  int64_t cap = (int64_t)ctx->sm_count * 16;
+  if (blocks > cap) blocks = cap;
+  if (blocks < 1) blocks = 1;
+  return (unsigned)blocks;
+}
+
+}  // namespace
+
+// A growable device column of the build side.
+struct BuildCol {
+  int32_t type_id = 0, scale = 0;
+  int64_t es = 0;
+  wg::DevBuf data, valid;   // valid allocated lazily, all ones = valid
+  int64_t cap_rows = 0;
+  bool has_valid = false;
+};
+
+struct wg_join {
+  wg::Ctx* ctx;
+  int32_t build_key_col, probe_key_col;
+  std::vector<int32_t> payload_cols;
+  int64_t hint;
+  int64_t rows = 0;
+  BuildCol key;
+  std::vector<BuildCol> pay;
+  bool finished = false;
+  bool schema_set = false;
+  // index
+  int32_t flavor = 0;
+  int32_t shift = 0;
+  uint64_t capacity = 0;
+  wg::DevBuf slots, next, scratch, counts, offs, outp, outb, rows_dev, gath, gath_valid;
+  int64_t distinct = 0;
+  bool unique = true;
+  int64_t max_fanout = 1;
+  wg::StagedBatch staged;
+};
+
+namespace wg {
+
+static wg_status grow_col(Ctx* ctx, BuildCol& c, int64_t need_rows, int64_t used_rows) {
+  if (need_rows <= c.cap_rows) return WG_OK;
+  int64_t cap = std::max<int64_t>(need_rows, std::max<int64_t>(c.cap_rows * 2, 1024));
+  DevBuf nd;
+  WG_TRY(nd.alloc(ctx, cap * c.es));
+  if (used_rows > 0)
+    WG_CUDA_TRY(cudaMemcpyAsync(nd.get(), c.data.get(), (size_t)(used_rows * c.es), cudaMemcpyDeviceToDevice, ctx->stream));
+  if (c.has_valid) {
+    DevBuf nv;
+    int64_t words = (cap + 63) / 64;
+    WG_TRY(nv.alloc(ctx, words * 8));
+    WG_CUDA_TRY(cudaMemsetAsync(nv.get(), 0xFF, (size_t)(words * 8), ctx->stream));
+    if (used_rows > 0)
+      WG_CUDA_TRY(cudaMemcpyAsync(nv.get(), c.valid.get(), (size_t)(((used_rows + 63) / 64) * 8), cudaMemcpyDeviceToDevice,
+                                  ctx->stream));
+    WG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    c.valid = std::move(nv);
+  }
+  WG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  c.data = std::move(nd);
+  c.cap_rows = cap;
+  return WG_OK;
+}
+
+static wg_status append_col(Ctx* ctx, BuildCol& c, const wg_column& src, int64_t n, int64_t at) {
+  WG_TRY(grow_col(ctx, c, at + n, at));
+  if (n > 0)
+    WG_CUDA_TRY(cudaMemcpyAsync((char*)c.data.get() + at * c.es, src.data, (size_t)(n * c.es), cudaMemcpyDefault,
+                                ctx->stream));
+  if (src.valid_words) {
+    if (!c.has_valid) {
+      int64_t words = (c.cap_rows + 63) / 64;
+      WG_TRY(c.valid.alloc(ctx, words * 8));
+      WG_CUDA_TRY(cudaMemsetAsync(c.valid.get(), 0xFF, (size_t)(words * 8), ctx->stream));
+      c.has_valid = true;
+    }
+    // src bitmap may live on the host: bring it over first
+    DevBuf tmp;
+    const uint64_t* sv = src.valid_words;
+    cudaPointerAttributes attr;
+    if (cudaPointerGetAttributes(&attr, sv) != cudaSuccess || attr.type != cudaMemoryTypeDevice) {
+      cudaGetLastError();
+      int64_t words = (n + 63) / 64;
+      WG_TRY(tmp.alloc(ctx, std::max<int64_t>(words * 8, 16)));
+      WG_CUDA_TRY(cudaMemcpyAsync(tmp.get(), sv, (size_t)(words * 8), cudaMemcpyHostToDevice, ctx->stream));
+      sv = tmp.as<uint64_t>();
+    }
+    if (n > 0) {
+      append_valid_kernel<<<grid_for(ctx, n, 256), 256, 0, ctx->stream>>>(c.valid.as<uint32_t>(), at, sv, n);
+      ctx->count_launch();
+      WG_CUDA_TRY(cudaGetLastError());
+    }
+    WG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  }
+  return WG_OK;
+}
+
+static wg_status join_append(wg_join* j, const wg_batch_desc* b) {
+  Ctx* ctx = j->ctx;
+  if (j->finished) return fail(WG_E_STATE, "join build already finished");
+  if (!b || j->build_key_col < 0 || j->build_key_col >= b->ncols) return fail(WG_E_INVALID, "build key column out of range");
+  if (b->sel) return fail(WG_E_INVALID, "build batches must be flattened (no selection vector)");
+  const wg_column& kc = b->cols[j->build_key_col];
+  int kcls = class_of(kc.type_id);
+  if (kcls != WG_CLS_I32 && kcls != WG_CLS_I64) return fail(WG_E_UNSUPPORTED, "join key is not an integer-class column");
+  if (!j->schema_set) {
+    j->key.type_id = kc.type_id; j->key.es = elem_size(kc.type_id);
+    j->pay.resize(j->payload_cols.size());
+    for (size_t i = 0; i < j->payload_cols.size(); ++i) {
+      int pc = j->payload_cols[i];
+      if (pc < 0 || pc >= b->ncols) return fail(WG_E_INVALID, "payload column out of range");
+      const wg_column& c = b->cols[pc];
+      if (elem_size(c.type_id) == 0) return fail(WG_E_UNSUPPORTED, "payload column type is not on the GPU path");
+      j->pay[i].type_id = c.type_id; j->pay[i].scale = c.scale; j->pay[i].es = elem_size(c.type_id);
+    }
+    j->flavor = kcls == WG_CLS_I32 ? 0 : 1;
+    j->schema_set = true;
+  } else if (kc.type_id != j->key.type_id) {
+    return fail(WG_E_INVALID, "build key type changed between batches");
+  }
+  const int64_t n = b->len;
+  int64_t hint = std::max<int64_t>(j->hint, j->rows + n);
+  WG_TRY(grow_col(ctx, j->key, hint, j->rows));
+  WG_TRY(append_col(ctx, j->key, kc, n, j->rows));
+  for (size_t i = 0; i < j->pay.size(); ++i) {
+    const wg_column& c = b->cols[j->payload_cols[i]];
+    if (c.type_id != j->pay[i].type_id) return fail(WG_E_INVALID, "payload type changed between batches");
+    WG_TRY(grow_col(ctx, j->pay[i], hint, j->rows));
+    WG_TRY(append_col(ctx, j->pay[i], c, n, j->rows));
+  }
+  j->rows += n;
+  WG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return WG_OK;
+}
+
+// Device view for the fused pipeline and the probe kernels.
+wg_status join_view(wg_join* j, wgd::JoinView* v) {
+  if (!j->finished) return fail(WG_E_STATE, "join build not finished");
+  v->flavor = j->flavor;
+  v->shift = j->shift;
+  v->mask = j->capacity - 1;
+  v->slots = j->slots.get();
+  v->next = j->next.as<int32_t>();
+  v->n_pay = (int32_t)j->pay.size();
+  v->_pad = 0;
+  for (size_t i = 0; i < j->pay.size() && i < WG_MAX_PAYLOAD; ++i)
+    v->pay[i] = wgd::DCol{j->pay[i].data.get(), j->pay[i].has_valid ? j->pay[i].valid.as<uint64_t>() : nullptr,
+                          class_of(j->pay[i].type_id), j->pay[i].scale};
+  return WG_OK;
+}
+int32_t join_probe_key_col(wg_join* j) { return j->probe_key_col; }
+int32_t join_n_payload(wg_join* j) { return (int32_t)j->pay.size(); }
+int32_t join_payload_type(wg_join* j, int i) { return j->pay[i].type_id; }
+int32_t join_payload_scale(wg_join* j, int i) { return j->pay[i].scale; }
+bool join_payload_nullable(wg_join* j, int i) { return j->pay[i].has_valid; }
+bool join_unique(wg_join* j) { return j->unique; }
+int64_t join_max_fanout(wg_join* j) { return j->max_fanout; }
+
+}  // namespace wg
+
+using namespace wg;
+
+extern "C" {
+
+wg_status wg_join_create(wg_ctx* ctx, int32_t join_type, int32_t build_key_col, int32_t probe_key_col,
+                         int32_t n_payload, const int32_t* payload_cols, int64_t build_row_hint, wg_join** out) {
+  if (!ctx || !out) return fail(WG_E_INVALID, "NULL argument");
+  if (join_type != WG_JOIN_INNER) return fail(WG_E_UNSUPPORTED, "only inner joins are on the GPU path");
+  if (n_payload < 0 || n_payload > WG_MAX_PAYLOAD || (n_payload > 0 && !payload_cols))
+    return fail(WG_E_INVALID, "at most 4 payload columns");
+  wg_join* j = new wg_join();
+  j->ctx = ctx;
+  j->build_key_col = build_key_col;
+  j->probe_key_col = probe_key_col;
+  j->payload_cols.assign(payload_cols, payload_cols + n_payload);
+  j->hint = build_row_hint > 0 ? build_row_hint : 1024;
+  *out = j;
+  return WG_OK;
+}
+
+wg_status wg_join_build_append(wg_join* j, const wg_batch_desc* b) {
+  if (!j) return fail(WG_E_INVALID, "join is NULL");
+  WG_TRY(ensure_device(j->ctx));
+  return join_append(j, b);
+}
+
+wg_status wg_join_build_append_device(wg_join* j, const wg_batch_desc* b) {
+  if (!j) return fail(WG_E_INVALID, "join is NULL");
+  WG_TRY(ensure_device(j->ctx));
+  return join_append(j, b);
+}
+
+wg_status wg_join_build_finish(wg_join* j) {
+  if (!j) return fail(WG_E_INVALID, "join is NULL");
+  if (j->finished) return WG_OK;
+  Ctx* ctx = j->ctx;
+  WG_TRY(ensure_device(ctx));
+  if (!j->schema_set) { j->flavor = 0; j->key.type_id = WG_TYPE_INT32; j->key.es = 4; }
+  uint64_t cap = 1024;
+  while (cap < (uint64_t)std::max<int64_t>(2 * j->rows, 1)) cap <<= 1;
+  int log2 = 0;
+  while ((1ULL << log2) < cap) ++log2;
+  j->capacity = cap;
+  j->shift = 64 - log2;
+  const int64_t slot_bytes = j->flavor == 0 ? 8 : 16;
+  WG_TRY(j->slots.ensure(ctx, (int64_t)cap * slot_bytes));
+  WG_TRY(j->next.ensure(ctx, std::max<int64_t>(j->rows, 1) * 4));
+  WG_TRY(j->scratch.ensure(ctx, 64));
+  WG_CUDA_TRY(cudaMemsetAsync(j->slots.get(), 0xFF, (size_t)(cap * slot_bytes), ctx->stream));
+  WG_CUDA_TRY(cudaMemsetAsync(j->scratch.get(), 0, 64, ctx->stream));
+  if (j->rows > 0) {
+    BuildArgs a;
+    a.key = wgd::DCol{j->key.data.get(), j->key.has_valid ? j->key.valid.as<uint64_t>() : nullptr,
+                      class_of(j->key.type_id), 0};
+    a.n = j->rows;
+    a.flavor = j->flavor;
+    a.shift = j->shift;
+    a.mask = cap - 1;
+    a.slots = j->slots.get();
+    a.next = j->next.as<int32_t>();
+    a.distinct = j->scratch.as<unsigned long long>();
+    a.dup = (int32_t*)(j->scratch.as<char>() + 8);
+    a.err = ctx->dev_error;
+    join_build_kernel<<<grid_for(ctx, j->rows, 256), 256, 0, ctx->stream>>>(a);
+    ctx->count_launch();
+    WG_CUDA_TRY(cudaGetLastError());
+  }
+  int64_t back[2] = {0, 0};
+  WG_TRY(read_back_i64(ctx, j->scratch.as<int64_t>(), back, 2));
+  WG_TRY(check_device_error(ctx));
+  j->distinct = back[0];
+  j->unique = (int32_t)back[1] == 0;
+  j->finished = true;
+  j->max_fanout = 1;
+  if (!j->unique) {
+    wgd::JoinView v;
+    WG_TRY(join_view(j, &v));
+    WG_CUDA_TRY(cudaMemsetAsync(j->scratch.get(), 0, 8, ctx->stream));
+    join_fanout_kernel<<<grid_for(ctx, (int64_t)cap, 256), 256, 0, ctx->stream>>>(v, j->scratch.as<unsigned long long>());
+    ctx->count_launch();
+    WG_CUDA_TRY(cudaGetLastError());
+    int64_t mf = 1;
+    WG_TRY(read_back_i64(ctx, j->scratch.as<int64_t>(), &mf, 1));
+    j->max_fanout = std::max<int64_t>(1, mf);
+  }
+  return WG_OK;
+}
+
+wg_status wg_join_build_stats(wg_join* j, int64_t* build_rows, int64_t* distinct_keys) {
+  if (!j) return fail(WG_E_INVALID, "join is NULL");
+  if (build_rows) *build_rows = j->rows;
+  if (distinct_keys) *distinct_keys = j->distinct;
+  return WG_OK;
+}
+
+wg_status wg_join_probe(wg_join* j, const wg_batch_desc* probe, uint32_t* out_probe_rows, int64_t* out_build_rows,
+                        int64_t cap, int64_t* cursor, int64_t* out_n) {
+  if (!j || !probe || !cursor || !out_n || cap < 0) return fail(WG_E_INVALID, "NULL argument");
+  Ctx* ctx = j->ctx;
+  WG_TRY(ensure_device(ctx));
+  if (!j->finished) return fail(WG_E_STATE, "join build not finished");
+  if (j->probe_key_col < 0 || j->probe_key_col >= probe->ncols) return fail(WG_E_INVALID, "probe key column out of range");
+  const wg_column& kc = probe->cols[j->probe_key_col];
+  if (class_of(kc.type_id) != WG_CLS_I32 && class_of(kc.type_id) != WG_CLS_I64)
+    return fail(WG_E_UNSUPPORTED, "probe key is not an integer-class column");
+  wg_column only = kc;
+  wg_batch_desc one{1, 0, &only, probe->len, probe->sel, probe->sel_len};
+  WG_TRY(stage_batch(ctx, &one, &j->staged));
+  const int64_t n = probe->sel ? probe->sel_len : probe->len;
+  *out_n = 0;
+  if (n == 0) return WG_OK;
+  WG_TRY(j->counts.ensure(ctx, n * 8));
+  WG_TRY(j->offs.ensure(ctx, n * 8));
+  ProbeArgs a;
+  WG_TRY(join_view(j, &a.j));
+  a.key = wgd::DCol{j->staged.cols[0].data, j->staged.cols[0].valid_words, class_of(kc.type_id), 0};
+  a.sel = j->staged.desc.sel;
+  a.n = n;
+  a.counts = j->counts.as<int64_t>();
+  a.offs = j->offs.as<int64_t>();
+  a.cursor = *cursor;
+  a.cap = cap;
+  a.err = ctx->dev_error;
+  join_probe_count_kernel<<<grid_for(ctx, n, 256), 256, 0, ctx->stream>>>(a);
+  ctx->count_launch();
+  WG_CUDA_TRY(cudaGetLastError());
+  size_t tmp_bytes = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, a.counts, j->offs.as<int64_t>(), (int)n, ctx->stream);
+  WG_TRY(j->scratch.ensure(ctx, std::max<int64_t>((int64_t)tmp_bytes, 64)));
+  cub::DeviceScan::ExclusiveSum(j->scratch.get(), tmp_bytes, a.counts, j->offs.as<int64_t>(), (int)n, ctx->stream);
+  ctx->count_launch();
+  int64_t last[2] = {0, 0};
+  WG_TRY(read_back_i64(ctx, j->offs.as<int64_t>() + (n - 1), &last[0], 1));
+  WG_TRY(read_back_i64(ctx, j->counts.as<int64_t>() + (n - 1), &last[1], 1));
+  const int64_t total = last[0] + last[1];
+  const int64_t m = std::max<int64_t>(0, std::min<int64_t>(cap, total - *cursor));
+  if (m > 0) {
+    WG_TRY(j->outp.ensure(ctx, m * 4));
+    WG_TRY(j->outb.ensure(ctx, m * 8));
+    a.out_probe = j->outp.as<uint32_t>();
+    a.out_build = j->outb.as<int64_t>();
+    join_probe_emit_kernel<<<grid_for(ctx, n, 256), 256, 0, ctx->stream>>>(a);
+    ctx->count_launch();
+    WG_CUDA_TRY(cudaGetLastError());
+    WG_CUDA_TRY(cudaMemcpyAsync(out_probe_rows, j->outp.get(), (size_t)(m * 4), cudaMemcpyDeviceToHost, ctx->stream));
+    WG_CUDA_TRY(cudaMemcpyAsync(out_build_rows, j->outb.get(), (size_t)(m * 8), cudaMemcpyDeviceToHost, ctx->stream));
+    WG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  }
+  WG_TRY(check_device_error(ctx));
+  *cursor += m;
+  *out_n = m;
+  return WG_OK;
+}
+
+wg_status wg_join_gather(wg_join* j, int32_t payload_idx, const int64_t* build_rows, int64_t n, void* out,
+                         uint8_t* out_valid) {
+  if (!j || (n > 0 && (!build_rows || !out))) return fail(WG_E_INVALID, "NULL argument");
+  if (payload_idx < 0 || payload_idx >= (int32_t)j->pay.size()) return fail(WG_E_INVALID, "payload index out of range");
+  Ctx* ctx = j->ctx;
+  WG_TRY(ensure_device(ctx));
+  if (n == 0) return WG_OK;
+  for (int64_t i = 0; i < n; ++i)
+    if (build_rows[i] < 0 || build_rows[i] >= j->rows) return fail(WG_E_INVALID, "build row out of range");
+  BuildCol& c = j->pay[payload_idx];
+  WG_TRY(j->rows_dev.ensure(ctx, n * 8));
+  WG_TRY(j->gath.ensure(ctx, n * c.es));
+  WG_TRY(j->gath_valid.ensure(ctx, n));
+  WG_CUDA_TRY(cudaMemcpyAsync(j->rows_dev.get(), build_rows, (size_t)(n * 8), cudaMemcpyHostToDevice, ctx->stream));
+  gather_kernel<<<grid_for(ctx, n, 256), 256, 0, ctx->stream>>>(
+      c.data.as<char>(), c.es, c.has_valid ? c.valid.as<uint64_t>() : nullptr, j->rows_dev.as<int64_t>(), n,
+      j->gath.as<char>(), j->gath_valid.as<uint8_t>());
+  ctx->count_launch();
+  WG_CUDA_TRY(cudaGetLastError());
+  WG_CUDA_TRY(cudaMemcpyAsync(out, j->gath.get(), (size_t)(n * c.es), cudaMemcpyDeviceToHost, ctx->stream));
+  if (out_valid) WG_CUDA_TRY(cudaMemcpyAsync(out_valid, j->gath_valid.get(), (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
+  WG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return WG_OK;
+}
+
+wg_status wg_join_reset(wg_join* j) {
+  if (!j) return fail(WG_E_INVALID, "join is NULL");
+  WG_TRY(ensure_device(j->ctx));
+  WG_CUDA_TRY(cudaStreamSynchronize(j->ctx->stream));
+  j->rows = 0;
+  j->finished = false;
+  j->key.has_valid = false;
+  j->key.valid.reset();
+  for (BuildCol& c : j->pay) { c.has_valid = false; c.valid.reset(); }
+  j->distinct = 0;
+  j->unique = true;
+  j->max_fanout = 1;
+  return WG_OK;
+}
+
+wg_status wg_join_destroy(wg_join* j) {
+  if (!j) return WG_OK;
+  ensure_device(j->ctx);
+  cudaStreamSynchronize(j->ctx->stream);
+  delete j;
+  return WG_OK;
+}
+
+}  // extern "C"

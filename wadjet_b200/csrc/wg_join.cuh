@@ -1,0 +1,63 @@
+// wg_join.cuh — device view of a built hash-join index, shared by the
+// standalone probe and the fused filter → probe → aggregate kernel.
+//
+// The index restates HashJoin's int-key build (internal/engine/exec/join.go:
+// 520-575): an open-addressing table maps each distinct key to the most
+// recently inserted build row (the chain head) and `next[row]` links each build
+// row to the previous row with the same key (arenaNext). Keys are widened to
+// int64 as intKeyFromVector does (join.go:504). NULL keys are never indexed.
+//
+// Two slot flavours, picked from the build key's storage class:
+//  - int32-class keys: one 8-byte word {key32 (low), head32 (high)}, so a
+//    single 64-bit atomicCAS installs key and head together;
+//  - int64-class keys: 16 bytes {key64, head32, pad32}, installed with the
+//    sm_90+ 16-byte atomicCAS.
+// A slot is empty when its head is -1 (every occupied slot has head >= 0).
+#pragma once
+
+#include "wg_device.cuh"
+
+#define WG_MAX_PAYLOAD 4
+
+namespace wgd {
+
+struct JoinView {
+  int32_t flavor;          // 0 = 8-byte slots (int32 keys), 1 = 16-byte slots (int64 keys)
+  int32_t shift;           // 64 - log2(capacity)
+  uint64_t mask;           // capacity - 1
+  const void* slots;
+  const int32_t* next;
+  int32_t n_pay;
+  int32_t _pad;
+  DCol pay[WG_MAX_PAYLOAD];
+};
+
+// Chain head of `key`, or -1 when absent (HashJoinProbe's idx.Get, join.go:2700).
+__device__ __forceinline__ int32_t join_head(const JoinView& j, int64_t key, int32_t* err) {
+  uint64_t h = fib_slot((uint64_t)key, j.shift);
+  if (j.flavor == 0) {
+    if (key < INT32_MIN || key > INT32_MAX) return -1;
+    const unsigned long long* s = (const unsigned long long*)j.slots;
+    const uint32_t k32 = (uint32_t)(int32_t)key;
+    for (uint64_t probe = 0; probe <= j.mask; ++probe) {
+      unsigned long long v = __ldg(s + h);
+      int32_t head = (int32_t)(v >> 32);
+      if (head == -1) return -1;
+      if ((uint32_t)v == k32) return head;
+      h = (h + 1) & j.mask;
+    }
+  } else {
+    const longlong2* s = (const longlong2*)j.slots;
+    for (uint64_t probe = 0; probe <= j.mask; ++probe) {
+      longlong2 v = __ldg(s + h);
+      int32_t head = (int32_t)(uint32_t)v.y;
+      if (head == -1) return -1;
+      if (v.x == key) return head;
+      h = (h + 1) & j.mask;
+    }
+  }
+  set_error(err, WG_DERR_TABLE_FULL);
+  return -1;
+}
+
+}  // namespace wgd

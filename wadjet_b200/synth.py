@@ -1,0 +1,57 @@
+"""Benchmark tables generated in HBM (include/wadjet_synth.h) as torch CUDA tensors.
+
+- ``starjoin(n)``  : fact fk int32 Zipf(1.1) over 2^22 keys, qty int32 U[1,50],
+  price DECIMAL(15,2) as Int128, disc float64 U[0,0.1); dim of 2^22 unique keys with grp U[0,1000).
+- ``groupby(n)``   : k int64 U[0,4096), v int64 U[0,1e6), f float64 U[0,1), flag int32 U[0,10).
+- ``highcard(n)``  : a int32, b int64 (~2^26 distinct (a,b)), amt DECIMAL(18,2), x float64 ~N(0,1).
+"""
+from __future__ import annotations
+
+import torch
+
+from . import _check, lib
+
+SEED = 42
+DIM_ROWS = 1 << 22
+
+
+def _p(t):
+    return t.data_ptr() if t is not None else None
+
+
+def starjoin_fact(ctx, n: int, seed: int = SEED, row0: int = 0, device: int = 0):
+    dev = torch.device("cuda", device)
+    fk = torch.empty(n, dtype=torch.int32, device=dev)
+    qty = torch.empty(n, dtype=torch.int32, device=dev)
+    price = torch.empty((n, 2), dtype=torch.int64, device=dev)   # (hi, lo) per row
+    disc = torch.empty(n, dtype=torch.float64, device=dev)
+    _check(lib.wg_synth_starjoin_fact(ctx.h, seed, row0, n, _p(fk), _p(qty), _p(price), _p(disc)))
+    return fk, qty, price, disc
+
+
+def starjoin_dim(ctx, n: int = DIM_ROWS, seed: int = SEED, device: int = 0):
+    dev = torch.device("cuda", device)
+    key = torch.empty(n, dtype=torch.int32, device=dev)
+    grp = torch.empty(n, dtype=torch.int32, device=dev)
+    _check(lib.wg_synth_starjoin_dim(ctx.h, seed, n, _p(key), _p(grp)))
+    return key, grp
+
+
+def groupby(ctx, n: int, ngroups: int = 4096, seed: int = SEED, row0: int = 0, device: int = 0):
+    dev = torch.device("cuda", device)
+    k = torch.empty(n, dtype=torch.int64, device=dev)
+    v = torch.empty(n, dtype=torch.int64, device=dev)
+    f = torch.empty(n, dtype=torch.float64, device=dev)
+    flag = torch.empty(n, dtype=torch.int32, device=dev)
+    _check(lib.wg_synth_groupby(ctx.h, seed, row0, n, ngroups, _p(k), _p(v), _p(f), _p(flag)))
+    return k, v, f, flag
+
+
+def highcard(ctx, n: int, seed: int = SEED, row0: int = 0, device: int = 0):
+    dev = torch.device("cuda", device)
+    a = torch.empty(n, dtype=torch.int32, device=dev)
+    b = torch.empty(n, dtype=torch.int64, device=dev)
+    amt = torch.empty((n, 2), dtype=torch.int64, device=dev)
+    x = torch.empty(n, dtype=torch.float64, device=dev)
+    _check(lib.wg_synth_highcard(ctx.h, seed, row0, n, _p(a), _p(b), _p(amt), _p(x)))
+    return a, b, amt, x
