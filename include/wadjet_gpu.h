@@ -335,6 +335,47 @@ WG_API wg_status wg_pipeline_run(wg_ctx* ctx, const wg_pipeline_desc* p);
 WG_API wg_status wg_pipeline_run_device(wg_ctx* ctx, const wg_pipeline_desc* p);
 
 /* ======================================================================== */
+/* Batched mode: many small, independent filter + GROUP BY queries in one    */
+/* persistent launch, replayed from a CUDA graph. No counterpart in the      */
+/* reference, which runs each query's Pipeline.Run separately                */
+/* (exec/pipeline.go:81); every query keeps that operator contract's result. */
+/* ======================================================================== */
+typedef struct wg_batched wg_batched;
+
+typedef struct wg_batched_query {
+  const wg_batch_desc* input;    /* device-resident columns, no selection vector */
+  int32_t              n_filters;
+  int32_t              n_aggs;
+  const wg_predicate*  filters;  /* AND chain on input columns */
+  const int32_t*       key_cols; /* n_keys group columns */
+  int32_t              n_keys;
+  int32_t              _pad;
+  const wg_agg_spec*   aggs;
+  int64_t              ndv_hint; /* expected groups; sizes the query's table */
+} wg_batched_query;
+
+/* Launch shape and table sizing (picked per workload by the autotuner,
+ * wadjet_b200/autotune.py); a zero field takes the built-in default. */
+typedef struct wg_tune_params {
+  int32_t tile_rows;        /* rows per work item */
+  int32_t block;            /* threads per CTA */
+  int32_t ctas_per_sm;
+  int32_t smem_max_groups;  /* queries expecting at most this many groups pre-combine each
+                               work item in a shared-memory table */
+  double  max_load;         /* table load the hint is sized for */
+} wg_tune_params;
+
+WG_API wg_status wg_batched_create(wg_ctx* ctx, int32_t n_queries, const wg_batched_query* queries,
+                                   const wg_tune_params* params, wg_batched** out);
+/* Run every query once (one graph launch) and wait; n_groups[q] receives each
+ * query's group count (may be NULL). Queries whose table overflowed its hint are
+ * re-run on a grown table before returning. */
+WG_API wg_status wg_batched_run(wg_batched* b, int64_t* n_groups);
+/* Raw state of query q's groups (as wg_agg_export) after a run. */
+WG_API wg_status wg_batched_export(wg_batched* b, int32_t q, const wg_group_export* out);
+WG_API wg_status wg_batched_destroy(wg_batched* b);
+
+/* ======================================================================== */
 /* Synthetic benchmark tables, generated in HBM (include/wadjet_synth.h).    */
 /* No counterpart in the reference, whose benchmarks fill batches with       */
 /* SetValue loops (internal/engine/exec/bench_test.go). Rows [row0, row0+n)  */
@@ -347,6 +388,11 @@ WG_API wg_status wg_synth_groupby(wg_ctx* ctx, uint64_t seed, int64_t row0, int6
                                   int64_t* k, int64_t* v, double* f, int32_t* flag);
 WG_API wg_status wg_synth_highcard(wg_ctx* ctx, uint64_t seed, int64_t row0, int64_t n, int32_t* a, int64_t* b,
                                    wg_int128* amt, double* x);
+/* Batched workload, query q: its row count, key cardinality and filter
+ * threshold (host), and its columns (device; vi for even q, vf for odd q). */
+WG_API wg_status wg_synth_batched_params(uint64_t seed, int32_t q, int64_t* rows, int64_t* card, int32_t* threshold);
+WG_API wg_status wg_synth_batched(wg_ctx* ctx, uint64_t seed, int32_t q, int64_t n, int64_t card, int64_t* key,
+                                  int64_t* vi, double* vf, int32_t* filt);
 
 #ifdef __cplusplus
 }

@@ -160,12 +160,42 @@ WG_SYN_HD double wg_syn_hc_x(uint64_t seed, uint64_t row) {
   return s - 6.0;
 }
 
+/* ---- batched workload: query q of a batch ----
+ * rows N_q = round(exp(U[ln 1e4, ln 1e7])), key cardinality C_q =
+ * round(exp(U[ln 16, ln 1e6])), selectivity s_q ~ U[0.1, 0.9] → filter
+ * `f < round(1000 s_q)` on f int32 U[0,1000); value int64 U[0,1e6) for even q,
+ * float64 U[0,1) for odd q; key int64 U[0, C_q). Rows use seed + q. */
+#define WG_SYN_BQ_KEY   40
+#define WG_SYN_BQ_VI    41
+#define WG_SYN_BQ_VF    42
+#define WG_SYN_BQ_FILT  43
+#define WG_SYN_BQ_PARAM 44
+
+WG_SYN_HD int64_t wg_syn_bq_key(uint64_t seed, uint64_t row, int64_t card) {
+  return wg_syn_int(seed, WG_SYN_BQ_KEY, row, 0, card - 1);
+}
+WG_SYN_HD int64_t wg_syn_bq_vi(uint64_t seed, uint64_t row) { return wg_syn_int(seed, WG_SYN_BQ_VI, row, 0, 999999); }
+WG_SYN_HD double wg_syn_bq_vf(uint64_t seed, uint64_t row) { return wg_syn_u01(seed, WG_SYN_BQ_VF, row); }
+WG_SYN_HD int32_t wg_syn_bq_filt(uint64_t seed, uint64_t row) {
+  return (int32_t)wg_syn_int(seed, WG_SYN_BQ_FILT, row, 0, 999);
+}
+
 #include <math.h>
 #if defined(__CUDACC__)
 #define WG_SYN_HOST __host__ static inline
 #else
 #define WG_SYN_HOST static inline
 #endif
+
+/* Parameters of query q (host only: uses exp/log once per query). */
+WG_SYN_HOST void wg_syn_bq_params(uint64_t seed, uint32_t q, int64_t* rows, int64_t* card, int32_t* threshold) {
+  const double u0 = wg_syn_u01(seed, WG_SYN_BQ_PARAM, 3ULL * q);
+  const double u1 = wg_syn_u01(seed, WG_SYN_BQ_PARAM, 3ULL * q + 1);
+  const double u2 = wg_syn_u01(seed, WG_SYN_BQ_PARAM, 3ULL * q + 2);
+  *rows = (int64_t)llround(exp(log(1e4) + u0 * (log(1e7) - log(1e4))));
+  *card = (int64_t)llround(exp(log(16.0) + u1 * (log(1e6) - log(16.0))));
+  *threshold = (int32_t)llround(1000.0 * (0.1 + 0.8 * u2));
+}
 /* Zipf(s) inverse-CDF table over n ranks: cdf[i] = sum_{r<=i} (r+1)^-s / total,
  * summed in rank order, last entry forced to exactly 1.0. Built once on the
  * host and shared by every consumer so all of them sample identical keys. */

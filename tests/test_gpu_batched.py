@@ -1,0 +1,71 @@
+"""Batched mode (many queries in one persistent graph-replayed launch) against the
+oracle run query by query: each query's groups must be what its own
+Pipeline.Run produces."""
+import numpy as np
+import pytest
+
+from oracle import binding as ob
+from tests.helpers import assert_groups_equal
+
+pytestmark = pytest.mark.gpu
+
+I32, I64, F64 = 1, 2, 4
+
+
+def make_queries(ctx, nq, max_rows, hint_scale=1.0):
+    import wadjet_b200 as wg
+    from wadjet_b200 import synth
+    qs, host = [], []
+    for q in range(nq):
+        n, card, thr = synth.batched_params(q)
+        n = min(n, max_rows)
+        key, val, filt, card, thr = synth.batched_query(ctx, q, rows=n)
+        vt = I64 if q % 2 == 0 else F64
+        batch = wg.Batch([wg.Column(I64, key), wg.Column(vt, val), wg.Column(I32, filt)])
+        aggs = [wg.AggColumn(wg.AGG_SUM, 1), wg.AggColumn(wg.AGG_COUNT, -1), wg.AggColumn(wg.AGG_MIN, 1),
+                wg.AggColumn(wg.AGG_MAX, 1)]
+        qs.append({"batch": batch, "group_by": [0], "aggs": aggs, "filters": [(2, wg.OP_LT, thr)],
+                   "ndv_hint": max(1, int(card * hint_scale)), "_keep": (key, val, filt)})
+        host.append((key.cpu().numpy(), val.cpu().numpy(), filt.cpu().numpy(), vt, thr))
+    return qs, host
+
+
+def oracle_query(key, val, filt, vt, thr):
+    o = ob.Agg([0], [(0, 1, 0), (1, -1, 0), (2, 1, 0), (3, 1, 0)])
+    ob.pipeline(ob.HostBatch([(I64, key, None, 0), (vt, val, None, 0), (I32, filt, None, 0)]), o,
+                filters=[(2, 2, thr)], threads=4)
+    return o.export()
+
+
+def kinds(vt):
+    return ["sum_i", "count", "min_i", "max_i"] if vt == I64 else ["sum_f", "count", "min_f", "max_f"]
+
+
+@pytest.mark.parametrize("params", [None, "nosmem", "small_tiles"])
+def test_batched_matches_oracle(ctx, params):
+    import wadjet_b200 as wg
+    tp = {None: None, "nosmem": wg.TuneParams(smem_max_groups=-1),
+          "small_tiles": wg.TuneParams(tile_rows=4096, block=256, ctas_per_sm=4)}[params]
+    qs, host = make_queries(ctx, 24, 300_000)
+    b = wg.BatchedQueries(ctx, qs, tp)
+    for _ in range(2):  # the graph is replayed: the second run must reset state
+        counts = b.run()
+    for q, (key, val, filt, vt, thr) in enumerate(host):
+        want = oracle_query(key, val, filt, vt, thr)
+        assert counts[q] == want["keys"].shape[1]
+        assert_groups_equal(b.export(q, int(counts[q])), want, kinds(vt))
+    b.close()
+
+
+def test_batched_hint_too_small_is_rerun(ctx):
+    """A query whose real group count overflows its hinted table is re-run on a
+    grown table; results stay exact and the next replay uses the new table."""
+    import wadjet_b200 as wg
+    qs, host = make_queries(ctx, 6, 200_000, hint_scale=0.01)
+    b = wg.BatchedQueries(ctx, qs, wg.TuneParams(max_load=0.75))
+    for _ in range(2):
+        counts = b.run()
+        for q, (key, val, filt, vt, thr) in enumerate(host):
+            want = oracle_query(key, val, filt, vt, thr)
+            assert_groups_equal(b.export(q, int(counts[q])), want, kinds(vt))
+    b.close()

@@ -68,11 +68,22 @@ def test_groupby_workload_matches_oracle(ctx):
     g.close()
 
 
+KNOBS = [  # (WG_TILE, WG_JOIN_DIRECT, WG_AGG_SMEM): every GPU lever on, off, and mixed
+    ("1", "1", "1"), ("0", "0", "0"), ("1", "0", "1"), ("0", "1", "0"), ("1", "1", "0")]
+
+
+@pytest.mark.parametrize("knobs", KNOBS, ids=lambda k: "tile%s-direct%s-smem%s" % k)
 @pytest.mark.parametrize("host_input", [False, True])
-def test_starjoin_workload_matches_oracle(ctx, host_input):
-    """Star join + aggregate, 2^22 fact rows against the full 2^22-row dimension."""
+def test_starjoin_workload_matches_oracle(ctx, host_input, knobs, monkeypatch):
+    """Star join + aggregate, 2^22 fact rows against the full 2^22-row dimension, with
+    each GPU lever switched off in turn (the reference's optimisation-invariance
+    oracle, internal/optswitch): every combination must give the same groups."""
     import wadjet_b200 as wg
     from wadjet_b200 import synth
+    if host_input and knobs != KNOBS[0]:
+        pytest.skip("host staging is lever-independent; covered with all levers on")
+    for name, val in zip(("WG_TILE", "WG_JOIN_DIRECT", "WG_AGG_SMEM"), knobs):
+        monkeypatch.setenv(name, val)
     n = 1 << 22
     fk, qty, price, disc = synth.starjoin_fact(ctx, n)
     key, grp = synth.starjoin_dim(ctx)
@@ -102,10 +113,12 @@ def test_starjoin_workload_matches_oracle(ctx, host_input):
     j.close()
 
 
-def test_highcard_workload_matches_oracle(ctx):
+@pytest.mark.parametrize("tile", ["1", "0"])
+def test_highcard_workload_matches_oracle(ctx, tile, monkeypatch):
     """GROUP BY (a int32, b int64) packed key, 2^22 rows (~3.9M groups)."""
     import wadjet_b200 as wg
     from wadjet_b200 import synth
+    monkeypatch.setenv("WG_TILE", tile)
     n = 1 << 22
     a, b, amt, x = synth.highcard(ctx, n)
     aggs = [wg.AggColumn(wg.AGG_SUM, 2), wg.AggColumn(wg.AGG_COUNT, -1), wg.AggColumn(wg.AGG_MIN, 3),

@@ -452,6 +452,72 @@ class Expr:
         return e
 
 
+def _export_arrays(nk: int, na: int, n: int) -> dict:
+    return {"keys": np.zeros((nk, n), np.int64), "key_valid": np.zeros((nk, n), np.uint8),
+            "count": np.zeros((na, n), np.int64), "i64": np.zeros((na, n), np.int64),
+            "f64": np.zeros((na, n), np.float64), "dec": np.zeros((na, n), DEC_DTYPE),
+            "has": np.zeros((na, n), np.uint8)}
+
+
+@dataclass
+class TuneParams:
+    """Launch shape / table sizing of the batched mode (wg_tune_params); 0 = default."""
+    tile_rows: int = 0
+    block: int = 0
+    ctas_per_sm: int = 0
+    smem_max_groups: int = 0
+    max_load: float = 0.0
+
+
+class BatchedQueries:
+    """Many independent filter + GROUP BY queries run by one persistent launch
+    replayed from a CUDA graph. queries: list of dicts with keys
+    batch (device Batch), group_by, aggs (AggColumn), filters [(col, op, value)], ndv_hint."""
+
+    def __init__(self, ctx: Context, queries: Sequence[dict], params: Optional[TuneParams] = None):
+        self.ctx = ctx
+        self._keep: list = []
+        self.shapes = []
+        arr = (abi.wg_batched_query * len(queries))()
+        for i, q in enumerate(queries):
+            d, keep = q["batch"].desc()
+            self._keep += [d, keep]
+            f = (abi.wg_predicate * max(1, len(q.get("filters", ()))))(*[predicate(*x) for x in q.get("filters", ())])
+            keys = (C.c_int32 * max(1, len(q["group_by"])))(*q["group_by"])
+            specs = (abi.wg_agg_spec * max(1, len(q["aggs"])))(*[abi.wg_agg_spec(a.func, a.input_col, a.out_type, 0)
+                                                                 for a in q["aggs"]])
+            self._keep += [f, keys, specs]
+            arr[i] = abi.wg_batched_query(C.pointer(d), len(q.get("filters", ())), len(q["aggs"]), f, keys,
+                                          len(q["group_by"]), 0, specs, int(q.get("ndv_hint", 0)))
+            self.shapes.append((len(q["group_by"]), len(q["aggs"])))
+        self._keep.append(arr)
+        tp = params or TuneParams()
+        ctp = abi.wg_tune_params(tp.tile_rows, tp.block, tp.ctas_per_sm, tp.smem_max_groups, tp.max_load)
+        h = C.c_void_p()
+        _check(lib.wg_batched_create(ctx.h, len(queries), arr, C.byref(ctp), C.byref(h)))
+        self.h = h
+        self.n = len(queries)
+
+    def run(self) -> np.ndarray:
+        out = np.zeros(self.n, np.int64)
+        _check(lib.wg_batched_run(self.h, out.ctypes.data_as(C.POINTER(C.c_int64))))
+        return out
+
+    def export(self, q: int, n_groups: int) -> dict:
+        nk, na = self.shapes[q]
+        r = _export_arrays(nk, na, n_groups)
+        if n_groups:
+            e = abi.wg_group_export(*[r[k].ctypes.data if r[k].size else None
+                                      for k in ("keys", "key_valid", "count", "i64", "f64", "dec", "has")])
+            _check(lib.wg_batched_export(self.h, q, C.byref(e)))
+        return r
+
+    def close(self) -> None:
+        if self.h:
+            lib.wg_batched_destroy(self.h)
+            self.h = None
+
+
 def predicate(col: int, op: int, value) -> abi.wg_predicate:
     kind, i, f = _const(value)
     return abi.wg_predicate(col, op, kind, 0, i, f)

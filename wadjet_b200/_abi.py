@@ -68,6 +68,17 @@ class wg_pipeline_desc(C.Structure):
                 ("agg", C.c_void_p)]
 
 
+class wg_batched_query(C.Structure):
+    _fields_ = [("input", C.POINTER(wg_batch_desc)), ("n_filters", C.c_int32), ("n_aggs", C.c_int32),
+                ("filters", C.POINTER(wg_predicate)), ("key_cols", C.POINTER(C.c_int32)), ("n_keys", C.c_int32),
+                ("_pad", C.c_int32), ("aggs", C.POINTER(wg_agg_spec)), ("ndv_hint", C.c_int64)]
+
+
+class wg_tune_params(C.Structure):
+    _fields_ = [("tile_rows", C.c_int32), ("block", C.c_int32), ("ctas_per_sm", C.c_int32),
+                ("smem_max_groups", C.c_int32), ("max_load", C.c_double)]
+
+
 P = C.c_void_p
 PP = C.POINTER(C.c_void_p)
 I32, I64, F64 = C.c_int32, C.c_int64, C.c_double
@@ -110,10 +121,16 @@ SIGNATURES = {
     "wg_agg_destroy": (I32, [P]),
     "wg_pipeline_run": (I32, [P, C.POINTER(wg_pipeline_desc)]),
     "wg_pipeline_run_device": (I32, [P, C.POINTER(wg_pipeline_desc)]),
+    "wg_batched_create": (I32, [P, I32, C.POINTER(wg_batched_query), C.POINTER(wg_tune_params), PP]),
+    "wg_batched_run": (I32, [P, PI64]),
+    "wg_batched_export": (I32, [P, I32, C.POINTER(wg_group_export)]),
+    "wg_batched_destroy": (I32, [P]),
     "wg_synth_starjoin_fact": (I32, [P, C.c_uint64, I64, I64, P, P, P, P]),
     "wg_synth_starjoin_dim": (I32, [P, C.c_uint64, I64, P, P]),
     "wg_synth_groupby": (I32, [P, C.c_uint64, I64, I64, I64, P, P, P, P]),
     "wg_synth_highcard": (I32, [P, C.c_uint64, I64, I64, P, P, P, P]),
+    "wg_synth_batched_params": (I32, [C.c_uint64, I32, PI64, PI64, C.POINTER(C.c_int32)]),
+    "wg_synth_batched": (I32, [P, C.c_uint64, I32, I64, I64, P, P, P, P]),
 }
 
 _lib = None

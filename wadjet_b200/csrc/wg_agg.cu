@@ -20,7 +20,7 @@
 
 namespace wg {
 wg_status resolve_pred(const wg_predicate& p, int32_t type_id, wgd::Pred* out);
-wg_status join_view(wg_join* j, wgd::JoinView* v);
+wg_status join_view_fused(wg_join* j, wgd::JoinView* v);
 int32_t join_probe_key_col(wg_join* j);
 int32_t join_n_payload(wg_join* j);
 int32_t join_payload_type(wg_join* j, int i);
@@ -491,10 +491,24 @@ struct LaunchSpec {
   int block = kAggBlock;
   unsigned grid = 1;
   size_t smem_bytes = 0;
+  bool tile = false;          // TMA-staged tile kernel
+  wgd::TileCfg cfg{};
 };
 
 template <int NA>
 static void launch_pipeline_t(const LaunchSpec& ls, cudaStream_t st) {
+  if (ls.tile) {
+    const size_t dyn = (size_t)ls.cfg.table_off + (ls.smem ? (size_t)ls.P.smem_slots * ls.P.L.slot_words * 8 : 0);
+    const unsigned threads = 32u * (1u + (unsigned)ls.cfg.consumers);
+    if (ls.smem) {
+      cudaFuncSetAttribute(wgd::tile_pipeline_kernel<NA, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+      wgd::tile_pipeline_kernel<NA, true><<<ls.grid, threads, dyn, st>>>(ls.P, ls.cfg);
+    } else {
+      cudaFuncSetAttribute(wgd::tile_pipeline_kernel<NA, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+      wgd::tile_pipeline_kernel<NA, false><<<ls.grid, threads, dyn, st>>>(ls.P, ls.cfg);
+    }
+    return;
+  }
   if (ls.smem) {
     cudaFuncSetAttribute(wgd::pipeline_kernel<NA, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ls.smem_bytes);
     wgd::pipeline_kernel<NA, true><<<ls.grid, ls.block, ls.smem_bytes, st>>>(ls.P);
@@ -514,6 +528,7 @@ static wg_status launch_pipeline(wg_agg* a, const LaunchSpec& ls, int64_t n_item
   for (int i = 0; i < WG_MAX_AGGS; ++i) L.agg[i].vcol = ls.P.L.agg[i].vcol;
   P.L = L;
   P.n_items = n_items;
+  if (l2.tile) l2.cfg.n_tiles = (n_items + l2.cfg.rows - 1) / l2.cfg.rows;
   if (a->L.n_aggs <= 4) launch_pipeline_t<4>(l2, ctx->stream);
   else launch_pipeline_t<8>(l2, ctx->stream);
   ctx->count_launch();
@@ -626,7 +641,7 @@ static wg_status build_plan(const PipelineRun& r, wgd::Plan& P, VSchema& vs, std
   }
   if (r.join) {
     P.has_join = 1;
-    WG_TRY(join_view(r.join, &P.join));
+    WG_TRY(join_view_fused(r.join, &P.join));
     P.probe_col = in_map[join_probe_key_col(r.join)];
     for (int p = 0; p < npay; ++p) { P.vcls[nin + p] = class_of(vs.type[ncols + p]); P.vscale[nin + p] = vs.scale[ncols + p]; }
   } else {
@@ -696,6 +711,49 @@ static wg_status run_device(const PipelineRun& r) {
   ls.grid = (unsigned)(ctx->sm_count * blocks_per_sm);
   if (!ls.smem) ls.grid = (unsigned)std::min<int64_t>((int64_t)ctx->sm_count * 4, (n_items + 1023) / 1024 + 1);
 
+  // TMA-staged tile kernel: contiguous input (no selection vector) whose columns
+  // start on 16-byte boundaries; one persistent CTA per SM.
+  bool aligned = ls.P.sel == nullptr && ls.P.n_in > 0;
+  for (int j = 0; j < ls.P.n_in; ++j) aligned = aligned && ((uintptr_t)ls.P.in[j].data % 16 == 0);
+  if (aligned && env_int("WG_TILE", 1) != 0 && n_items >= 4096) {
+    wgd::TileCfg& c = ls.cfg;
+    std::memset(&c, 0, sizeof(c));
+    c.consumers = std::max(1, std::min(31, env_int("WG_TILE_CONSUMERS", 16)));
+    c.stages = std::max(2, std::min(8, env_int("WG_TILE_STAGES", 2)));
+    const int64_t budget = (int64_t)ctx->max_smem_optin - 1024;
+    const int64_t table_bytes = ls.smem ? (int64_t)S * a->L.slot_words * 8 : 0;
+    for (int rows = std::max(64, env_int("WG_TILE_ROWS", 2048) & ~63); rows >= 64; rows /= 2) {
+      int64_t off = 0;
+      for (int j = 0; j < ls.P.n_in; ++j) {
+        const int cls = ls.P.in[j].cls;
+        c.es[j] = cls == WG_CLS_I32 || cls == WG_CLS_F32 ? 4 : cls == WG_CLS_DEC ? 16 : 8;
+        c.col_off[j] = (int32_t)off;
+        off += ((int64_t)rows * c.es[j] + 15) & ~int64_t(15);
+      }
+      // the shared-memory aggregate table shrinks to what the stages leave over
+      int64_t tb = table_bytes;
+      if (ls.smem && off * c.stages + tb > budget) {
+        const int64_t s2 = (budget - off * c.stages) / (a->L.slot_words * 8);
+        if (s2 >= 256 && expect * 2 <= s2) { ls.P.smem_slots = (int)s2; tb = s2 * a->L.slot_words * 8; }
+      }
+      if (off * c.stages + tb <= budget) {
+        c.rows = rows;
+        c.stage_bytes = (int32_t)off;
+        c.table_off = (int32_t)(off * c.stages);
+        ls.tile = true;
+        if (ls.smem && tb != table_bytes) ls.smem_bytes = (size_t)tb;
+        break;
+      }
+    }
+    if (ls.tile) {
+      if (ls.smem && (int64_t)c.table_off + (int64_t)ls.P.smem_slots * a->L.slot_words * 8 > budget) {
+        ls.smem = false;
+        ls.P.smem_slots = 0;
+      }
+      ls.grid = (unsigned)ctx->sm_count;
+    }
+  }
+
   const wgd::Plan base = ls.P;
   auto limit = [&]() { return (int64_t)((double)a->cap * kMaxLoad); };
 
@@ -733,7 +791,7 @@ static wg_status run_device(const PipelineRun& r) {
   }
   // 3) large table: chunks that each fit, growing between chunks
   WG_TRY(refresh_groups(a));
-  if (ls.smem) { ls.smem = false; ls.P.smem_slots = 0; ls.smem_bytes = 0; ls.grid = (unsigned)(ctx->sm_count * 4); }
+  if (ls.smem) { ls.smem = false; ls.P.smem_slots = 0; ls.smem_bytes = 0; if (!ls.tile) ls.grid = (unsigned)(ctx->sm_count * 4); }
   int64_t done = 0;
   const int64_t min_chunk = 1 << 20;
   while (done < n_items) {
@@ -1027,6 +1085,331 @@ wg_status wg_agg_destroy(wg_agg* a) {
   ensure_device(a->ctx);
   cudaStreamSynchronize(a->ctx->stream);
   delete a;
+  return WG_OK;
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Batched mode: many small filter + GROUP BY queries in one persistent launch.
+//
+// Every query keeps its own aggregate (table, layout, launch plan); a work list
+// of (query, row window) items is drained by persistent CTAs through an atomic
+// cursor. Queries expecting few groups pre-combine each work item in a
+// shared-memory table flushed to their HBM table at the end of the item. The
+// whole run — table resets, the kernel, the group counts and their copy to the
+// host — is captured once in a CUDA graph and replayed.
+// ===========================================================================
+namespace {
+
+struct BatchItem {
+  int32_t q;
+  int32_t rows;
+  int64_t row0;
+};
+
+struct ResetDesc {
+  unsigned long long* slots;
+  int64_t words;
+  int32_t sw;
+  int32_t key_words;
+  unsigned long long* ctr;
+  uint64_t cap;
+  unsigned long long init[WG_MAX_SLOT_WORDS];
+};
+
+__global__ void batched_reset_kernel(const ResetDesc* rd, int n) {
+  for (int q = blockIdx.x; q < n; q += gridDim.x) {
+    const ResetDesc& r = rd[q];
+    for (int64_t i = threadIdx.x; i < r.words; i += blockDim.x) r.slots[i] = r.init[i % r.sw];
+    if (threadIdx.x < 8) r.ctr[threadIdx.x] = 0;
+  }
+}
+
+// groups per query: regular slots taken + the two special slots when used; -1 on overflow
+__global__ void batched_count_kernel(const ResetDesc* rd, int n, long long* out) {
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+    const ResetDesc& r = rd[q];
+    if (((const int32_t*)(r.ctr + 1))[0] != 0) { out[q] = -1; continue; }
+    if (r.key_words == 0) { out[q] = 1; continue; }
+    long long g = (long long)r.ctr[0];
+    g += r.slots[r.cap * r.sw + r.key_words] != 0;
+    g += r.slots[(r.cap + 1) * r.sw + r.key_words] != 0;
+    out[q] = g;
+  }
+}
+
+template <int NA>
+__global__ void __launch_bounds__(512) batched_kernel(const Plan* plans, const BatchItem* items, int64_t n_items,
+                                                      unsigned long long* cursor) {
+  extern __shared__ unsigned long long sm[];
+  __shared__ int s_groups;
+  __shared__ long long s_item;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (;;) {
+    if (threadIdx.x == 0) s_item = (long long)atomicAdd(cursor, 1ULL);
+    __syncthreads();
+    const long long it = s_item;
+    if (it >= n_items) break;
+    const BatchItem w = items[it];
+    const Plan& P = plans[w.q];
+    const int S = P.smem_slots;
+    if (S > 0) {
+      smem_table_init<NA>(P.L, sm, S, &s_groups);
+      __syncthreads();
+      const int s_limit = (S * 7) / 8;
+      for (int base = warp * 32; base < w.rows; base += nw * 32) {
+        const int i = base + lane;
+        SrcGlobal src{w.row0 + (i < w.rows ? i : 0)};
+        process_rows<NA, true>(P, src, i < w.rows, sm, &s_groups, s_limit);
+      }
+      __syncthreads();
+      smem_table_flush<NA>(P, sm, S);
+    } else {
+      for (int base = warp * 32; base < w.rows; base += nw * 32) {
+        const int i = base + lane;
+        SrcGlobal src{w.row0 + (i < w.rows ? i : 0)};
+        process_rows<NA, false>(P, src, i < w.rows, sm, &s_groups, 0);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace
+
+struct wg_batched {
+  wg::Ctx* ctx;
+  std::vector<wg_agg*> aggs;
+  std::vector<wg_batch_desc> inputs;
+  std::vector<std::vector<wg_column>> cols;
+  std::vector<std::vector<wg_predicate>> filters;
+  wg_tune_params tp{};
+  int max_na = 4;
+  size_t dyn_smem = 0;
+  std::vector<wgd::Plan> plans_h;
+  std::vector<BatchItem> items_h;
+  std::vector<ResetDesc> reset_h;
+  wg::DevBuf plans, items, resets, cursor, counts;
+  long long* counts_host = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+namespace wg {
+
+static wg_status batched_plan(wg_batched* b) {
+  Ctx* ctx = b->ctx;
+  const int n = (int)b->aggs.size();
+  b->plans_h.assign((size_t)n, wgd::Plan{});
+  b->reset_h.assign((size_t)n, ResetDesc{});
+  b->max_na = 4;
+  int64_t max_smem_words = 0;
+  for (int q = 0; q < n; ++q) {
+    wg_agg* a = b->aggs[q];
+    PipelineRun r{a, &b->inputs[q], (int32_t)b->filters[q].size(), b->filters[q].data(), nullptr, 0, nullptr};
+    LaunchSpec ls;
+    VSchema vs;
+    std::vector<int> in_map;
+    WG_TRY(build_plan(r, ls.P, vs, in_map));
+    if (ls.P.sel) return fail(WG_E_INVALID, "batched inputs must not carry a selection vector");
+    wgd::Plan& P = b->plans_h[q];
+    P = ls.P;
+    P.T = table_view(a);
+    wgd::Layout L = a->L;
+    for (int k = 0; k < WG_MAX_KEYS; ++k) L.key_vcol[k] = ls.P.L.key_vcol[k];
+    for (int i = 0; i < WG_MAX_AGGS; ++i) L.agg[i].vcol = ls.P.L.agg[i].vcol;
+    P.L = L;
+    P.err = ctx->dev_error;
+    bool plain = a->L.key_words == 1;
+    for (int i = 0; i < a->L.n_aggs; ++i)
+      plain = plain && a->L.agg[i].null_off < 0 && a->L.agg[i].kind != wgd::K_MIN_DEC && a->L.agg[i].kind != wgd::K_MAX_DEC;
+    const int64_t smax = b->tp.smem_max_groups;
+    int S = 0;
+    if (plain && a->hint > 0 && a->hint <= smax) {
+      S = (int)std::max<int64_t>(256, std::min<int64_t>(16384, a->hint * 2));
+      max_smem_words = std::max<int64_t>(max_smem_words, (int64_t)S * a->L.slot_words);
+    }
+    P.smem_slots = S;
+    if (a->L.n_aggs > 4) b->max_na = 8;
+    ResetDesc& rd = b->reset_h[q];
+    rd.slots = a->table.as<unsigned long long>();
+    rd.words = table_words(a, a->cap);
+    rd.sw = a->L.slot_words;
+    rd.key_words = a->L.key_words;
+    rd.ctr = a->ctr.as<unsigned long long>();
+    rd.cap = a->cap;
+    for (int i = 0; i < WG_MAX_SLOT_WORDS; ++i) rd.init[i] = a->L.init[i];
+  }
+  b->dyn_smem = (size_t)max_smem_words * 8;
+  if ((int64_t)b->dyn_smem > (int64_t)ctx->max_smem_optin - 1024) return fail(WG_E_INVALID, "shared-memory table too large");
+  WG_TRY(b->plans.ensure(ctx, (int64_t)sizeof(wgd::Plan) * n));
+  WG_TRY(b->resets.ensure(ctx, (int64_t)sizeof(ResetDesc) * n));
+  WG_CUDA_TRY(cudaMemcpy(b->plans.get(), b->plans_h.data(), sizeof(wgd::Plan) * n, cudaMemcpyHostToDevice));
+  WG_CUDA_TRY(cudaMemcpy(b->resets.get(), b->reset_h.data(), sizeof(ResetDesc) * n, cudaMemcpyHostToDevice));
+  // work items: tile_rows-row windows of every query, largest queries first
+  std::vector<int> order((size_t)n);
+  for (int q = 0; q < n; ++q) order[q] = q;
+  std::sort(order.begin(), order.end(), [&](int x, int y) { return b->inputs[x].len > b->inputs[y].len; });
+  b->items_h.clear();
+  for (int q : order)
+    for (int64_t r0 = 0; r0 < b->inputs[q].len; r0 += b->tp.tile_rows)
+      b->items_h.push_back(BatchItem{q, (int32_t)std::min<int64_t>(b->tp.tile_rows, b->inputs[q].len - r0), r0});
+  WG_TRY(b->items.ensure(ctx, (int64_t)(sizeof(BatchItem) * std::max<size_t>(1, b->items_h.size()))));
+  if (!b->items_h.empty())
+    WG_CUDA_TRY(cudaMemcpy(b->items.get(), b->items_h.data(), sizeof(BatchItem) * b->items_h.size(), cudaMemcpyHostToDevice));
+  WG_TRY(b->cursor.ensure(ctx, 64));
+  WG_TRY(b->counts.ensure(ctx, 8 * (int64_t)std::max(1, n)));
+  return WG_OK;
+}
+
+static void batched_enqueue(wg_batched* b, cudaStream_t st) {
+  Ctx* ctx = b->ctx;
+  const int n = (int)b->aggs.size();
+  batched_reset_kernel<<<std::min(n, ctx->sm_count * 8), 256, 0, st>>>(b->resets.as<ResetDesc>(), n);
+  cudaMemsetAsync(b->cursor.get(), 0, 8, st);
+  const unsigned grid = (unsigned)(ctx->sm_count * std::max(1, b->tp.ctas_per_sm));
+  if (b->max_na <= 4) {
+    batched_kernel<4><<<grid, b->tp.block, b->dyn_smem, st>>>(b->plans.as<wgd::Plan>(), b->items.as<BatchItem>(),
+                                                             (int64_t)b->items_h.size(),
+                                                             b->cursor.as<unsigned long long>());
+  } else {
+    batched_kernel<8><<<grid, b->tp.block, b->dyn_smem, st>>>(b->plans.as<wgd::Plan>(), b->items.as<BatchItem>(),
+                                                             (int64_t)b->items_h.size(),
+                                                             b->cursor.as<unsigned long long>());
+  }
+  batched_count_kernel<<<(n + 255) / 256, 256, 0, st>>>(b->resets.as<ResetDesc>(), n, b->counts.as<long long>());
+  cudaMemcpyAsync(b->counts_host, b->counts.get(), 8 * (size_t)n, cudaMemcpyDeviceToHost, st);
+}
+
+static wg_status batched_capture(wg_batched* b) {
+  Ctx* ctx = b->ctx;
+  if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
+  if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
+  WG_CUDA_TRY(cudaFuncSetAttribute(batched_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->dyn_smem));
+  WG_CUDA_TRY(cudaFuncSetAttribute(batched_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->dyn_smem));
+  WG_CUDA_TRY(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+  batched_enqueue(b, ctx->stream);
+  WG_CUDA_TRY(cudaStreamEndCapture(ctx->stream, &b->graph));
+  WG_CUDA_TRY(cudaGraphInstantiate(&b->exec, b->graph, 0));
+  return WG_OK;
+}
+
+}  // namespace wg
+
+extern "C" {
+
+wg_status wg_batched_create(wg_ctx* ctx, int32_t n, const wg_batched_query* qs, const wg_tune_params* params,
+                            wg_batched** out) {
+  if (!ctx || !out || n < 1 || !qs) return fail(WG_E_INVALID, "bad batched arguments");
+  WG_TRY(ensure_device(ctx));
+  wg_batched* b = new wg_batched();
+  b->ctx = ctx;
+  wg_tune_params tp{};
+  if (params) tp = *params;
+  if (tp.tile_rows <= 0) tp.tile_rows = 1 << 15;
+  tp.tile_rows = std::max(64, tp.tile_rows & ~63);
+  if (tp.block <= 0) tp.block = 512;
+  tp.block = std::max(64, std::min(512, tp.block & ~31));
+  if (tp.ctas_per_sm <= 0) tp.ctas_per_sm = 2;
+  if (tp.smem_max_groups == 0) tp.smem_max_groups = 2048;  // negative: never use shared memory
+  if (tp.smem_max_groups < 0) tp.smem_max_groups = 0;
+  if (tp.max_load <= 0.0 || tp.max_load > kMaxLoad) tp.max_load = 0.5;
+  b->tp = tp;
+  b->aggs.resize((size_t)n, nullptr);
+  b->inputs.resize((size_t)n);
+  b->cols.resize((size_t)n);
+  b->filters.resize((size_t)n);
+  auto cleanup = [&](wg_status s) { wg_batched_destroy(b); return s; };
+  for (int q = 0; q < n; ++q) {
+    const wg_batched_query& x = qs[q];
+    if (!x.input || x.input->sel || x.n_filters < 0 || x.n_filters > WG_MAX_FILTERS)
+      return cleanup(fail(WG_E_INVALID, "batched query " + std::to_string(q) + ": bad input or filters"));
+    b->cols[q].assign(x.input->cols, x.input->cols + x.input->ncols);
+    b->inputs[q] = *x.input;
+    b->inputs[q].cols = b->cols[q].data();
+    b->filters[q].assign(x.filters, x.filters + x.n_filters);
+    wg_status s = wg_agg_create(ctx, x.n_keys, x.key_cols, x.n_aggs, x.aggs, x.ndv_hint, &b->aggs[q]);
+    if (s != WG_OK) return cleanup(s);
+    wg_agg* a = b->aggs[q];
+    // resolve the aggregate against the query's schema, sized for its hint
+    PipelineRun r{a, &b->inputs[q], (int32_t)b->filters[q].size(), b->filters[q].data(), nullptr, 0, nullptr};
+    LaunchSpec ls;
+    VSchema vs;
+    std::vector<int> in_map;
+    s = build_plan(r, ls.P, vs, in_map);
+    if (s == WG_OK) s = agg_resolve(a, vs);
+    if (s == WG_OK && a->L.key_words != 0) {
+      uint64_t cap = 1024;
+      while ((double)cap * tp.max_load < (double)std::max<int64_t>(1, x.ndv_hint)) cap <<= 1;
+      if (cap != a->cap) s = rebuild_table(a, cap, a->L);
+    }
+    if (s != WG_OK) return cleanup(s);
+  }
+  if (cudaMallocHost((void**)&b->counts_host, 8 * (size_t)n) != cudaSuccess)
+    return cleanup(fail(WG_E_CUDA, "pinned counts"));
+  wg_status s = batched_plan(b);
+  if (s == WG_OK) s = batched_capture(b);
+  if (s != WG_OK) return cleanup(s);
+  *out = b;
+  return WG_OK;
+}
+
+wg_status wg_batched_run(wg_batched* b, int64_t* n_groups) {
+  if (!b) return fail(WG_E_INVALID, "batched is NULL");
+  Ctx* ctx = b->ctx;
+  WG_TRY(ensure_device(ctx));
+  WG_CUDA_TRY(cudaGraphLaunch(b->exec, ctx->stream));
+  ctx->count_launch(4);
+  WG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  WG_TRY(check_device_error(ctx));
+  const int n = (int)b->aggs.size();
+  bool replan = false;
+  for (int q = 0; q < n; ++q) {
+    wg_agg* a = b->aggs[q];
+    a->finalized = false;
+    if (b->counts_host[q] >= 0) continue;
+    // this query outgrew its hint: rerun it alone on a 4x table
+    WG_TRY(rebuild_table(a, a->cap * 4, a->L));
+    WG_TRY(wg_agg_reset(a));
+    PipelineRun r{a, &b->inputs[q], (int32_t)b->filters[q].size(), b->filters[q].data(), nullptr, 0, nullptr};
+    WG_TRY(run_device(r));
+    int64_t g = 0;
+    WG_TRY(wg_agg_finalize(a, &g));
+    a->finalized = false;
+    b->counts_host[q] = g;
+    replan = true;
+  }
+  if (n_groups)
+    for (int q = 0; q < n; ++q) n_groups[q] = b->counts_host[q];
+  if (replan) {  // tables moved: the graph must point at the new ones
+    WG_TRY(batched_plan(b));
+    WG_TRY(batched_capture(b));
+  }
+  return WG_OK;
+}
+
+wg_status wg_batched_export(wg_batched* b, int32_t q, const wg_group_export* out) {
+  if (!b || q < 0 || q >= (int32_t)b->aggs.size()) return fail(WG_E_INVALID, "bad query index");
+  wg_agg* a = b->aggs[q];
+  a->finalized = false;
+  int64_t g = 0;
+  WG_TRY(wg_agg_finalize(a, &g));
+  wg_status s = wg_agg_export(a, out);
+  a->finalized = false;
+  return s;
+}
+
+wg_status wg_batched_destroy(wg_batched* b) {
+  if (!b) return WG_OK;
+  ensure_device(b->ctx);
+  cudaStreamSynchronize(b->ctx->stream);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  if (b->counts_host) cudaFreeHost(b->counts_host);
+  for (wg_agg* a : b->aggs)
+    if (a) wg_agg_destroy(a);
+  delete b;
   return WG_OK;
 }
 

@@ -3,6 +3,7 @@
 #pragma once
 
 #include "wg_agg.cuh"
+#include "wg_tma.cuh"
 
 namespace wgd {
 
@@ -31,8 +32,25 @@ __device__ __forceinline__ Val load_val(const DCol& c, int64_t i) {
   return v;
 }
 
-__device__ __forceinline__ Val fetch_base(const Plan& P, int j, int64_t row, int32_t brow) {
-  if (j < P.n_in) return load_val(P.in[j], row);
+// Row sources: where one row's input columns are read from. SrcGlobal reads
+// HBM directly; the tile kernel's source reads its TMA-staged shared-memory tile.
+struct SrcGlobal {
+  int64_t row;
+  __device__ __forceinline__ Val in(const Plan& P, int j) const { return load_val(P.in[j], row); }
+};
+
+template <class Src>
+__device__ __forceinline__ Val fetch_base(const Plan& P, const Src& src, int j, int32_t brow) {
+  if (j < P.n_in) return src.in(P, j);
+  if (P.join.direct) {  // brow already holds the payload's 32 bits
+    Val v;
+    v.hi = 0;
+    v.null = false;
+    v.lo = P.join.pay[0].cls == WG_CLS_F32
+               ? (unsigned long long)__double_as_longlong((double)__int_as_float(brow))
+               : (unsigned long long)(long long)brow;
+    return v;
+  }
   return load_val(P.join.pay[j - P.n_in], brow);
 }
 
@@ -43,7 +61,8 @@ __device__ __forceinline__ unsigned long long as_w(double d) { return (unsigned 
 // float ops are single IEEE operations (no contraction), DECIMAL operands read
 // as Int128.ToFloat64, a NULL operand makes the result NULL. The four-entry
 // stack is addressed through selects so it stays in registers.
-__device__ __forceinline__ Val eval_expr(const Plan& P, const ExprD& e, int64_t row, int32_t brow) {
+template <class Src>
+__device__ __forceinline__ Val eval_expr(const Plan& P, const ExprD& e, const Src& src, int32_t brow) {
   unsigned long long s0 = 0, s1 = 0, s2 = 0, s3 = 0;
   unsigned fl = 0;  // bit i: stack entry i holds a float
   int sp = 0;
@@ -55,7 +74,7 @@ __device__ __forceinline__ Val eval_expr(const Plan& P, const ExprD& e, int64_t 
     bool isf = false;
     if (opc == 0) {  // WG_EXPR_COL
       const int j = e.arg[k];
-      Val v = fetch_base(P, j, row, brow);
+      Val v = fetch_base(P, src, j, brow);
       null |= v.null;
       const int cls = P.vcls[j];
       if (cls == WG_CLS_I32 || cls == WG_CLS_I64) { w = v.lo; isf = false; }
@@ -106,10 +125,11 @@ __device__ __forceinline__ Val eval_expr(const Plan& P, const ExprD& e, int64_t 
   return r;
 }
 
-__device__ __forceinline__ Val fetch(const Plan& P, int j, int64_t row, int32_t brow) {
+template <class Src>
+__device__ __forceinline__ Val fetch(const Plan& P, const Src& src, int j, int32_t brow) {
   const int nb = P.n_in + P.join.n_pay;
-  if (j < nb) return fetch_base(P, j, row, brow);
-  return eval_expr(P, P.expr[j - nb], row, brow);
+  if (j < nb) return fetch_base(P, src, j, brow);
+  return eval_expr(P, P.expr[j - nb], src, brow);
 }
 
 template <int NA>
@@ -120,8 +140,8 @@ struct Contrib {
 
 // One row's contribution to each aggregate (the scatter kernels' per-row
 // update, internal/engine/exec/agg_scatter.go:178-510), as combinable words.
-template <int NA>
-__device__ __forceinline__ void make_contrib(const Plan& P, int64_t row, int32_t brow, Contrib<NA>& c) {
+template <int NA, class Src>
+__device__ __forceinline__ void make_contrib(const Plan& P, const Src& src, int32_t brow, Contrib<NA>& c) {
   const Layout& L = P.L;
 #pragma unroll
   for (int a = 0; a < NA; ++a) {
@@ -129,10 +149,10 @@ __device__ __forceinline__ void make_contrib(const Plan& P, int64_t row, int32_t
     if (a >= L.n_aggs) continue;
     const AggD g = L.agg[a];
     if (g.vcol < 0 || g.kind == K_COUNT) {
-      if (g.vcol >= 0) c.nul[a] = fetch(P, g.vcol, row, brow).null ? 1 : 0;
+      if (g.vcol >= 0) c.nul[a] = fetch(P, src, g.vcol, brow).null ? 1 : 0;
       continue;
     }
-    const Val v = fetch(P, g.vcol, row, brow);
+    const Val v = fetch(P, src, g.vcol, brow);
     if (v.null) {
       c.nul[a] = 1;
       c.w0[a] = L.init[g.off];
@@ -337,20 +357,21 @@ __device__ __forceinline__ void warp_update(const Plan& P, bool cur, unsigned lo
 // Group key of one (row, build row): the int-key path widens to int64
 // (consumeBatchIntGroup, aggregate.go:1908); the packed path places each column
 // by buildPackedLayout (packed_hash.go:386) as packedKeyAt does (:456).
-__device__ __forceinline__ bool make_key(const Plan& P, int64_t row, int32_t brow, unsigned long long& k0,
+template <class Src>
+__device__ __forceinline__ bool make_key(const Plan& P, const Src& src, int32_t brow, unsigned long long& k0,
                                          unsigned long long& k1, bool& knull) {
   const Layout& L = P.L;
   k0 = 0; k1 = 0; knull = false;
   if (L.key_words == 0) return true;
   if (L.key_words == 1) {
-    Val v = fetch(P, L.key_vcol[0], row, brow);
+    Val v = fetch(P, src, L.key_vcol[0], brow);
     knull = v.null;
     k0 = v.null ? 0 : v.lo;
     return true;
   }
   for (int k = 0; k < WG_MAX_KEYS; ++k) {
     if (k >= L.n_keys) break;
-    Val v = fetch(P, L.key_vcol[k], row, brow);
+    Val v = fetch(P, src, L.key_vcol[k], brow);
     if (v.null) { set_error(P.err, WG_DERR_NULL_PACKED); return false; }
     const unsigned long long w = L.key_i32[k] ? ((unsigned long long)(uint32_t)(int32_t)v.lo) << L.key_shift[k] : v.lo;
     if (L.key_word[k] == 0) k0 |= w; else k1 |= w;
@@ -358,19 +379,91 @@ __device__ __forceinline__ bool make_key(const Plan& P, int64_t row, int32_t bro
   return true;
 }
 
-// The fused pipeline: KernelFilter chain → HashJoinProbe → Project →
-// HashAggregate.Consume for every input row, one warp per 32 consecutive rows.
+// `col OP const` on an already loaded value (compareFilterImpl, compare.go:47).
+__device__ __forceinline__ bool pred_val(const Pred& p, const Val& v) {
+  if (v.null) return false;
+  switch (p.cls) {
+    case WG_CLS_I32: return cmp_op<int32_t>((int32_t)(long long)v.lo, (int32_t)p.ci, p.op);
+    case WG_CLS_I64: return cmp_op<long long>((long long)v.lo, p.ci, p.op);
+    case WG_CLS_F32: return cmp_op<double>(as_f(v.lo), (double)(float)p.cf, p.op);  // both exact in binary64
+    case WG_CLS_F64: return cmp_op<double>(as_f(v.lo), p.cf, p.op);
+    default: return false;
+  }
+}
+
+// One row per lane of a warp: KernelFilter chain → HashJoinProbe → Project →
+// HashAggregate.Consume. All 32 lanes call it together (act = row present).
+template <int NA, bool SMEM, class Src>
+__device__ __forceinline__ void process_rows(const Plan& P, const Src& src, bool act, unsigned long long* sm,
+                                             int* s_groups, int s_limit) {
+  for (int f = 0; f < WG_MAX_FILTERS; ++f) {
+    if (f >= P.n_filters) break;
+    if (act) act = pred_val(P.filt[f], src.in(P, P.filt[f].col));
+  }
+  int32_t brow = -1;
+  if (P.has_join && act) {
+    const Val kv = src.in(P, P.probe_col);
+    if (kv.null) act = false;
+    else if (P.join.direct) act = join_direct(P.join, (int64_t)kv.lo, brow, P.err);
+    else {
+      brow = join_head(P.join, (int64_t)kv.lo, P.err);
+      act = brow >= 0;
+    }
+  }
+  for (;;) {
+    if (!__any_sync(WG_FULL_MASK, act)) break;
+    unsigned long long k0 = 0, k1 = 0;
+    bool knull = false;
+    Contrib<NA> c;
+    bool cur = act;
+    if (cur) {
+      cur = make_key(P, src, brow, k0, k1, knull);
+      make_contrib<NA>(P, src, brow, c);
+    } else {
+#pragma unroll
+      for (int a = 0; a < NA; ++a) { c.w0[a] = 0; c.w1[a] = 0; c.nul[a] = 0; }
+    }
+    warp_update<NA, SMEM>(P, cur, k0, k1, knull, c, sm, s_groups, s_limit);
+    if (!P.has_join || P.join.direct) break;  // unique keys: at most one match
+    if (act) {
+      brow = __ldg(P.join.next + brow);       // arenaNext chain (join.go:2700)
+      act = brow >= 0;
+    }
+  }
+}
+
+template <int NA>
+__device__ __forceinline__ void smem_table_init(const Layout& L, unsigned long long* sm, int S, int* s_groups) {
+  const int sw = L.slot_words;
+  for (int i = threadIdx.x; i < S * sw; i += blockDim.x) sm[i] = L.init[i % sw];
+  if (threadIdx.x == 0) *s_groups = 0;
+}
+
+template <int NA>
+__device__ __forceinline__ void smem_table_flush(const Plan& P, const unsigned long long* sm, int S) {
+  const Layout& L = P.L;
+  const int sw = L.slot_words;
+  for (int i = threadIdx.x; i < S; i += blockDim.x) {
+    const unsigned long long* s = sm + (size_t)i * sw;
+    if (s[0] == WG_EMPTY_KEY) continue;
+    unsigned long long* g = find_global(L, P.T, s[0], 0, false, P.err);
+    if (g == nullptr) continue;
+    Contrib<NA> c;
+    slot_contrib<NA>(L, s, c);
+    apply<NA>(L, g, c, s[L.key_words]);
+  }
+}
+
+// The fused pipeline reading HBM directly: one warp per 32 consecutive rows
+// (or selection-vector entries), grid-stride.
 template <int NA, bool SMEM>
 __global__ void __launch_bounds__(512) pipeline_kernel(const __grid_constant__ Plan P) {
   extern __shared__ unsigned long long sm[];
   __shared__ int s_groups;
-  const Layout& L = P.L;
   const int S = P.smem_slots;
   const int s_limit = (S * 7) / 8;
   if (SMEM) {
-    const int sw = L.slot_words;
-    for (int i = threadIdx.x; i < S * sw; i += blockDim.x) sm[i] = L.init[i % sw];
-    if (threadIdx.x == 0) s_groups = 0;
+    smem_table_init<NA>(P.L, sm, S, &s_groups);
     __syncthreads();
   }
   const int lane = threadIdx.x & 31;
@@ -379,56 +472,130 @@ __global__ void __launch_bounds__(512) pipeline_kernel(const __grid_constant__ P
   for (int64_t base = ((int64_t)blockIdx.x * wpb + (threadIdx.x >> 5)) * 32; base < P.n_items;
        base += total_warps * 32) {
     const int64_t item = base + lane;
-    bool act = item < P.n_items;
-    int64_t row = 0;
-    if (act) row = P.sel ? (int64_t)__ldg(P.sel + item) : item;
-    for (int f = 0; f < WG_MAX_FILTERS; ++f) {
-      if (f >= P.n_filters) break;
-      if (act) act = pred_row(P.filt[f], P.in[P.filt[f].col], row);
-    }
-    int32_t brow = -1;
-    if (P.has_join && act) {
-      const Val kv = load_val(P.in[P.probe_col], row);
-      if (kv.null) act = false;
-      else {
-        brow = join_head(P.join, (int64_t)kv.lo, P.err);
-        act = brow >= 0;
-      }
-    }
-    for (;;) {
-      if (!__any_sync(WG_FULL_MASK, act)) break;
-      unsigned long long k0 = 0, k1 = 0;
-      bool knull = false;
-      Contrib<NA> c;
-      bool cur = act;
-      if (cur) {
-        cur = make_key(P, row, brow, k0, k1, knull);
-        make_contrib<NA>(P, row, brow, c);
-      } else {
-#pragma unroll
-        for (int a = 0; a < NA; ++a) { c.w0[a] = 0; c.w1[a] = 0; c.nul[a] = 0; }
-      }
-      warp_update<NA, SMEM>(P, cur, k0, k1, knull, c, sm, &s_groups, s_limit);
-      if (!P.has_join) break;
-      if (act) {
-        brow = __ldg(P.join.next + brow);
-        act = brow >= 0;
-      }
-    }
+    const bool act = item < P.n_items;
+    SrcGlobal src{act ? (P.sel ? (int64_t)__ldg(P.sel + item) : item) : 0};
+    process_rows<NA, SMEM>(P, src, act, sm, &s_groups, s_limit);
   }
   if (SMEM) {
     __syncthreads();
-    const int sw = L.slot_words;
-    for (int i = threadIdx.x; i < S; i += blockDim.x) {
-      const unsigned long long* s = sm + (size_t)i * sw;
-      if (s[0] == WG_EMPTY_KEY) continue;
-      unsigned long long* g = find_global(L, P.T, s[0], 0, false, P.err);
-      if (g == nullptr) continue;
-      Contrib<NA> c;
-      slot_contrib<NA>(L, s, c);
-      apply<NA>(L, g, c, s[L.key_words]);
+    smem_table_flush<NA>(P, sm, S);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Tile-staged variant: a producer warp streams each tile's input columns into
+// shared memory with bulk asynchronous copies (cp.async.bulk, completing on an
+// mbarrier), STAGES tiles ahead; consumer warps evaluate the rows out of shared
+// memory. HBM streaming then no longer waits on the probe's dependent loads.
+// ---------------------------------------------------------------------------
+struct TileCfg {
+  int32_t rows;                // T: rows per tile (multiple of 64)
+  int32_t stages;
+  int32_t stage_bytes;
+  int32_t consumers;           // consumer warps
+  int32_t col_off[WG_MAX_IN];  // byte offset of column j inside a stage
+  int32_t es[WG_MAX_IN];       // element size of column j
+  int32_t table_off;           // byte offset of the shared-memory aggregate table
+  int32_t _pad;
+  int64_t n_tiles;
+};
+
+// Row i of the current tile: staged bytes come from shared memory, the ragged
+// tail past the last whole 16-byte chunk from HBM.
+struct SrcTile {
+  const char* stage;
+  int64_t row0;
+  int32_t i;
+  int32_t m;
+  const TileCfg* C;
+  __device__ __forceinline__ Val in(const Plan& P, int j) const {
+    const DCol& c = P.in[j];
+    const int es = C->es[j];
+    const int staged = ((m * es) & ~15) / es;
+    const int64_t row = row0 + i;
+    const char* p = i < staged ? stage + C->col_off[j] + (size_t)i * es : (const char*)c.data + row * es;
+    Val v;
+    v.hi = 0;
+    v.null = is_null(c, row);
+    switch (c.cls) {
+      case WG_CLS_I32: v.lo = (unsigned long long)(long long)*(const int32_t*)p; break;
+      case WG_CLS_I64: v.lo = *(const unsigned long long*)p; break;
+      case WG_CLS_F32: v.lo = (unsigned long long)__double_as_longlong((double)*(const float*)p); break;
+      case WG_CLS_F64: v.lo = *(const unsigned long long*)p; break;
+      case WG_CLS_DEC: v.hi = ((const unsigned long long*)p)[0]; v.lo = ((const unsigned long long*)p)[1]; break;
+      default: v.lo = 0;
+    }
+    return v;
+  }
+};
+
+template <int NA, bool SMEM>
+__global__ void __launch_bounds__(544, 1) tile_pipeline_kernel(const __grid_constant__ Plan P,
+                                                               const __grid_constant__ TileCfg C) {
+  extern __shared__ __align__(128) unsigned char tsm[];
+  __shared__ int s_groups;
+  __shared__ __align__(8) unsigned long long bars[16];  // full[0..7], empty[8..15]
+  unsigned long long* full = bars;
+  unsigned long long* empty = bars + 8;
+  unsigned long long* table = (unsigned long long*)(tsm + C.table_off);
+  const int S = P.smem_slots;
+  const int s_limit = (S * 7) / 8;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < C.stages; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], C.consumers);
+    }
+    mbar_init_fence();
+  }
+  if (SMEM) smem_table_init<NA>(P.L, table, S, &s_groups);
+  __syncthreads();
+
+  if (warp == 0) {
+    // producer: one lane issues every copy
+    if (lane == 0) {
+      int64_t it = 0;
+      bool ok = true;
+      for (int64_t tile = blockIdx.x; tile < C.n_tiles; tile += gridDim.x, ++it) {
+        const int s = (int)(it % C.stages);
+        if (it >= C.stages && !mbar_wait(&empty[s], (uint32_t)(((it / C.stages) - 1) & 1), P.err)) { ok = false; break; }
+        const int64_t row0 = tile * C.rows;
+        const int m = (int)min((int64_t)C.rows, P.n_items - row0);
+        uint32_t total = 0;
+        for (int j = 0; j < P.n_in; ++j) total += (uint32_t)((m * C.es[j]) & ~15);
+        mbar_arrive_expect_tx(&full[s], total);
+        unsigned char* st = tsm + (size_t)s * C.stage_bytes;
+        for (int j = 0; j < P.n_in; ++j) {
+          const uint32_t bytes = (uint32_t)((m * C.es[j]) & ~15);
+          if (bytes) bulk_g2s(st + C.col_off[j], (const char*)P.in[j].data + row0 * C.es[j], bytes, &full[s]);
+        }
+      }
+      // never leave with copies in flight: wait for the last issued tiles to land
+      const int64_t issued = it;
+      for (int64_t k = issued > C.stages ? issued - C.stages : 0; k < issued; ++k)
+        mbar_wait(&full[k % C.stages], (uint32_t)((k / C.stages) & 1), P.err);
+      (void)ok;
+    }
+  } else {
+    const int cw = warp - 1;
+    int64_t it = 0;
+    for (int64_t tile = blockIdx.x; tile < C.n_tiles; tile += gridDim.x, ++it) {
+      const int s = (int)(it % C.stages);
+      if (!mbar_wait(&full[s], (uint32_t)((it / C.stages) & 1), P.err)) break;
+      const int64_t row0 = tile * C.rows;
+      const int m = (int)min((int64_t)C.rows, P.n_items - row0);
+      const unsigned char* st = tsm + (size_t)s * C.stage_bytes;
+      for (int base = cw * 32; base < m; base += C.consumers * 32) {
+        const int i = base + lane;
+        SrcTile src{(const char*)st, row0, i < m ? i : 0, m, &C};
+        process_rows<NA, SMEM>(P, src, i < m, table, &s_groups, s_limit);
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[s]);
     }
   }
+  __syncthreads();
+  if (SMEM) smem_table_flush<NA>(P, table, S);
 }
 
 }  // namespace wgd

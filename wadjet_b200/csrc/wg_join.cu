@@ -18,6 +18,9 @@
 
 #include <cub/cub.cuh>
 
+#include <climits>
+#include <cstdlib>
+
 namespace {
 
 using namespace wgd;
@@ -139,6 +142,30 @@ __global__ void join_probe_emit_kernel(const ProbeArgs a) {
   }
 }
 
+// Smallest and largest non-NULL build key (to pick a sentinel that is not a key).
+__global__ void key_range_kernel(DCol key, int64_t n, long long* mn, long long* mx) {
+  long long lo = LLONG_MAX, hi = LLONG_MIN;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    if (is_null(key, i)) continue;
+    const long long k = ld_i64(key, i);
+    lo = k < lo ? k : lo;
+    hi = k > hi ? k : hi;
+  }
+  atomicMin(mn, lo);
+  atomicMax(mx, hi);
+}
+
+// Rewrite a unique-key table as {key32, payload32} slots (empty = sentinel key).
+__global__ void direct_table_kernel(const unsigned long long* slots, uint64_t cap, const uint32_t* pay,
+                                    int32_t sentinel, unsigned long long* out) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cap; i += (uint64_t)gridDim.x * blockDim.x) {
+    const unsigned long long v = slots[i];
+    const int32_t head = (int32_t)(v >> 32);
+    out[i] = head < 0 ? (unsigned long long)(uint32_t)sentinel
+                      : ((unsigned long long)pay[head] << 32) | (uint32_t)v;
+  }
+}
+
 // Longest chain (max build rows sharing one key): the join's worst fan-out.
 __global__ void join_fanout_kernel(JoinView j, unsigned long long* max_len) {
   const uint64_t cap = j.mask + 1;
@@ -209,6 +236,10 @@ struct wg_join {
   int64_t distinct = 0;
   bool unique = true;
   int64_t max_fanout = 1;
+  // direct-payload copy of the table for the fused kernel (see JoinView)
+  wg::DevBuf dslots;
+  bool direct = false;
+  int32_t sentinel = 0;
   wg::StagedBatch staged;
 };
 
@@ -318,10 +349,23 @@ wg_status join_view(wg_join* j, wgd::JoinView* v) {
   v->slots = j->slots.get();
   v->next = j->next.as<int32_t>();
   v->n_pay = (int32_t)j->pay.size();
+  v->direct = 0;
+  v->sentinel = 0;
   v->_pad = 0;
   for (size_t i = 0; i < j->pay.size() && i < WG_MAX_PAYLOAD; ++i)
     v->pay[i] = wgd::DCol{j->pay[i].data.get(), j->pay[i].has_valid ? j->pay[i].valid.as<uint64_t>() : nullptr,
                           class_of(j->pay[i].type_id), j->pay[i].scale};
+  return WG_OK;
+}
+
+// The view the fused pipeline probes: the direct-payload table when one was built.
+wg_status join_view_fused(wg_join* j, wgd::JoinView* v) {
+  WG_TRY(join_view(j, v));
+  if (j->direct) {
+    v->slots = j->dslots.get();
+    v->direct = 1;
+    v->sentinel = j->sentinel;
+  }
   return WG_OK;
 }
 int32_t join_probe_key_col(wg_join* j) { return j->probe_key_col; }
@@ -419,7 +463,36 @@ wg_status wg_join_build_finish(wg_join* j) {
     WG_TRY(read_back_i64(ctx, j->scratch.as<int64_t>(), &mf, 1));
     j->max_fanout = std::max<int64_t>(1, mf);
   }
-  return WG_OK;
+  // Direct-payload table for the fused probe: unique int32 keys, exactly one
+  // 4-byte payload column without NULLs, and an int32 value that is no key.
+  j->direct = false;
+  const char* dsw = std::getenv("WG_JOIN_DIRECT");
+  if ((!dsw || std::atoi(dsw) != 0) && j->unique && j->flavor == 0 && j->pay.size() == 1 && j->pay[0].es == 4 &&
+      !j->pay[0].has_valid && j->rows > 0) {
+    long long* mm = (long long*)(j->scratch.as<char>() + 16);
+    const long long init[2] = {LLONG_MAX, LLONG_MIN};
+    WG_CUDA_TRY(cudaMemcpyAsync(mm, init, 16, cudaMemcpyHostToDevice, ctx->stream));
+    wgd::DCol kd{j->key.data.get(), j->key.has_valid ? j->key.valid.as<uint64_t>() : nullptr, class_of(j->key.type_id), 0};
+    key_range_kernel<<<grid_for(ctx, j->rows, 256), 256, 0, ctx->stream>>>(kd, j->rows, mm, mm + 1);
+    ctx->count_launch();
+    WG_CUDA_TRY(cudaGetLastError());
+    int64_t r[2];
+    WG_TRY(read_back_i64(ctx, (const int64_t*)mm, r, 2));
+    bool ok = true;
+    if (r[0] > INT32_MIN) j->sentinel = (int32_t)(r[0] - 1);
+    else if (r[1] < INT32_MAX) j->sentinel = (int32_t)(r[1] + 1);
+    else ok = false;
+    if (ok) {
+      WG_TRY(j->dslots.ensure(ctx, (int64_t)cap * 8));
+      direct_table_kernel<<<grid_for(ctx, (int64_t)cap, 256), 256, 0, ctx->stream>>>(
+          j->slots.as<unsigned long long>(), cap, j->pay[0].data.as<uint32_t>(), j->sentinel,
+          j->dslots.as<unsigned long long>());
+      ctx->count_launch();
+      WG_CUDA_TRY(cudaGetLastError());
+      j->direct = true;
+    }
+  }
+  return check_device_error(ctx);
 }
 
 wg_status wg_join_build_stats(wg_join* j, int64_t* build_rows, int64_t* distinct_keys) {

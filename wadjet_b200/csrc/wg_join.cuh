@@ -28,9 +28,31 @@ struct JoinView {
   const void* slots;
   const int32_t* next;
   int32_t n_pay;
+  // Direct-payload table (unique int32 keys, one 4-byte payload without NULLs):
+  // each slot holds {key32, payload32} instead of {key32, head32}, so a probe
+  // returns the payload with one load; empty slots hold `sentinel`, an int32
+  // that is not a build key.
+  int32_t direct;
+  int32_t sentinel;
   int32_t _pad;
   DCol pay[WG_MAX_PAYLOAD];
 };
+
+// Direct-payload lookup: the payload's raw 32 bits of `key`, or false.
+__device__ __forceinline__ bool join_direct(const JoinView& j, int64_t key, int32_t& out, int32_t* err) {
+  if (key < INT32_MIN || key > INT32_MAX || key == (int64_t)j.sentinel) return false;
+  const unsigned long long* s = (const unsigned long long*)j.slots;
+  const uint32_t k32 = (uint32_t)(int32_t)key;
+  uint64_t h = fib_slot((uint64_t)key, j.shift);
+  for (uint64_t probe = 0; probe <= j.mask; ++probe) {
+    const unsigned long long v = __ldg(s + h);
+    if ((uint32_t)v == k32) { out = (int32_t)(v >> 32); return true; }
+    if ((int32_t)(uint32_t)v == j.sentinel) return false;
+    h = (h + 1) & j.mask;
+  }
+  set_error(err, WG_DERR_TABLE_FULL);
+  return false;
+}
 
 // Chain head of `key`, or -1 when absent (HashJoinProbe's idx.Get, join.go:2700).
 __device__ __forceinline__ int32_t join_head(const JoinView& j, int64_t key, int32_t* err) {

@@ -46,6 +46,16 @@ __global__ void highcard_kernel(uint64_t seed, int64_t row0, int64_t n, int32_t*
   }
 }
 
+__global__ void batched_query_kernel(uint64_t seed, int64_t n, int64_t card, int64_t* key, int64_t* vi, double* vf,
+                                     int32_t* filt) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    if (key) key[i] = wg_syn_bq_key(seed, (uint64_t)i, card);
+    if (vi) vi[i] = wg_syn_bq_vi(seed, (uint64_t)i);
+    if (vf) vf[i] = wg_syn_bq_vf(seed, (uint64_t)i);
+    if (filt) filt[i] = wg_syn_bq_filt(seed, (uint64_t)i);
+  }
+}
+
 unsigned synth_grid(wg::Ctx* ctx, int64_t n) {
   int64_t b = (n + 255) / 256;
   return (unsigned)std::max<int64_t>(1, std::min<int64_t>(b, (int64_t)ctx->sm_count * 32));
@@ -125,6 +135,24 @@ wg_status wg_synth_highcard(wg_ctx* ctx, uint64_t seed, int64_t row0, int64_t n,
   WG_TRY(ensure_device(ctx));
   if (n == 0) return WG_OK;
   highcard_kernel<<<synth_grid(ctx, n), 256, 0, ctx->stream>>>(seed, row0, n, a, b, amt, x);
+  ctx->count_launch();
+  WG_CUDA_TRY(cudaGetLastError());
+  WG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return WG_OK;
+}
+
+wg_status wg_synth_batched_params(uint64_t seed, int32_t q, int64_t* rows, int64_t* card, int32_t* threshold) {
+  if (!rows || !card || !threshold || q < 0) return fail(WG_E_INVALID, "bad generator arguments");
+  wg_syn_bq_params(seed, (uint32_t)q, rows, card, threshold);
+  return WG_OK;
+}
+
+wg_status wg_synth_batched(wg_ctx* ctx, uint64_t seed, int32_t q, int64_t n, int64_t card, int64_t* key, int64_t* vi,
+                           double* vf, int32_t* filt) {
+  if (!ctx || n < 0 || card < 1 || q < 0) return fail(WG_E_INVALID, "bad generator arguments");
+  WG_TRY(ensure_device(ctx));
+  if (n == 0) return WG_OK;
+  batched_query_kernel<<<synth_grid(ctx, n), 256, 0, ctx->stream>>>(seed + (uint64_t)q, n, card, key, vi, vf, filt);
   ctx->count_launch();
   WG_CUDA_TRY(cudaGetLastError());
   WG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));

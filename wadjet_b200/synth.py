@@ -55,3 +55,28 @@ def highcard(ctx, n: int, seed: int = SEED, row0: int = 0, device: int = 0):
     x = torch.empty(n, dtype=torch.float64, device=dev)
     _check(lib.wg_synth_highcard(ctx.h, seed, row0, n, _p(a), _p(b), _p(amt), _p(x)))
     return a, b, amt, x
+
+
+def batched_params(q: int, seed: int = SEED) -> tuple[int, int, int]:
+    """(rows, key cardinality, filter threshold) of query q of the batched workload."""
+    import ctypes as C
+    r, c, t = C.c_int64(), C.c_int64(), C.c_int32()
+    _check(lib.wg_synth_batched_params(seed, q, C.byref(r), C.byref(c), C.byref(t)))
+    return r.value, c.value, t.value
+
+
+def batched_query(ctx, q: int, seed: int = SEED, device: int = 0, rows: int | None = None):
+    """Columns (key int64, value int64 for even q / float64 for odd q, filt int32) of query q."""
+    n, card, thr = batched_params(q, seed)
+    if rows is not None:
+        n = rows
+    dev = torch.device("cuda", device)
+    key = torch.empty(n, dtype=torch.int64, device=dev)
+    filt = torch.empty(n, dtype=torch.int32, device=dev)
+    if q % 2 == 0:
+        val = torch.empty(n, dtype=torch.int64, device=dev)
+        _check(lib.wg_synth_batched(ctx.h, seed, q, n, card, _p(key), _p(val), None, _p(filt)))
+    else:
+        val = torch.empty(n, dtype=torch.float64, device=dev)
+        _check(lib.wg_synth_batched(ctx.h, seed, q, n, card, _p(key), None, _p(val), _p(filt)))
+    return key, val, filt, card, thr
