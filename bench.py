@@ -55,6 +55,12 @@ def parse_args():
     p.add_argument("--rows", type=int, default=FACT_ROWS)
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--workload", choices=["starjoin", "groupby", "highcard", "batched", "serving"],
+                   default="starjoin", help="starjoin is the headline; the others print their own lines")
+    p.add_argument("--queries", type=int, default=512, help="batched: queries per batch")
+    p.add_argument("--qps", type=float, default=2000.0, help="serving: Poisson arrival rate")
+    p.add_argument("--seconds", type=float, default=3.0, help="serving: arrival window")
+    p.add_argument("--slots", type=int, default=8, help="serving: concurrent request slots")
     return p.parse_args()
 
 
@@ -338,6 +344,244 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         dist.destroy_process_group()
 
 
+# ------------------------------------------------------- other workloads --
+def _timed_ms(stream, fn, steps, warmup):
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def run_groupby(args):
+    """SELECT k, SUM(v), COUNT(*), MIN(f), MAX(f) FROM t WHERE flag < 7 GROUP BY k (4096 groups)."""
+    import torch
+    import wadjet_b200 as wg
+    from wadjet_b200 import synth
+    ctx = wg.Context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    peak, kind = measured_peak_hbm()
+    for n in (1 << 20, 1 << 28):
+        k, v, f, flag = synth.groupby(ctx, n)
+        batch = wg.Batch([wg.Column(wg.TYPE_INT64, k), wg.Column(wg.TYPE_INT64, v), wg.Column(wg.TYPE_FLOAT64, f),
+                          wg.Column(wg.TYPE_INT32, flag)])
+        agg = wg.HashAggregate(ctx, [0], [wg.AggColumn(wg.AGG_SUM, 1), wg.AggColumn(wg.AGG_COUNT, -1),
+                                          wg.AggColumn(wg.AGG_MIN, 2), wg.AggColumn(wg.AGG_MAX, 2)], ndv_hint=4096)
+
+        def step():
+            agg.reset()
+            wg.run_pipeline(ctx, batch, agg, filters=[(3, wg.OP_LT, 7)], device=True)
+            assert agg.finalize() == 4096
+
+        ms = _timed_ms(stream, step, args.steps, args.warmup)
+        alg = n * 28 + 4096 * 40
+        print(json.dumps({"workload": "groupby", "metric": "rows/s", "rows": n, "value": n / (ms / 1e3),
+                          "unit": "rows/s", "ms_per_step": ms, "hbm_gbs": alg / (ms / 1e3) / 1e9,
+                          "frac_of_peak": alg / (ms / 1e3) / 1e9 / peak, "peak_kind": peak_kind_note(kind)}),
+              flush=True)
+        agg.close()
+        del k, v, f, flag
+        torch.cuda.empty_cache()
+    ctx.close()
+
+
+def peak_kind_note(kind):
+    return f"of {kind} hbm_gbs"
+
+
+def run_highcard(args):
+    """GROUP BY (a int32, b int64) over 2^28 rows (~65.9M groups): SUM(amount) Int128, COUNT(*), MIN(x), MAX(x)."""
+    import torch
+    import wadjet_b200 as wg
+    from wadjet_b200 import synth
+    ctx = wg.Context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    n = args.rows
+    a, b, amt, x = synth.highcard(ctx, n)
+    batch = wg.Batch([wg.Column(wg.TYPE_INT32, a), wg.Column(wg.TYPE_INT64, b),
+                      wg.Column(wg.TYPE_DECIMAL, amt, scale=2), wg.Column(wg.TYPE_FLOAT64, x)])
+    agg = wg.HashAggregate(ctx, [0, 1], [wg.AggColumn(wg.AGG_SUM, 2), wg.AggColumn(wg.AGG_COUNT, -1),
+                                         wg.AggColumn(wg.AGG_MIN, 3), wg.AggColumn(wg.AGG_MAX, 3)],
+                           ndv_hint=1 << 26)
+    groups = [0]
+
+    def step():
+        agg.reset()
+        wg.run_pipeline(ctx, batch, agg, device=True)
+        groups[0] = agg.finalize()
+
+    ms = _timed_ms(stream, step, args.steps, max(1, args.warmup))
+    peak, kind = measured_peak_hbm()
+    alg = n * 36 + groups[0] * (16 + 16 + 8 + 8 + 8)
+    print(json.dumps({"workload": "highcard", "metric": "rows/s", "rows": n, "groups": groups[0],
+                      "value": n / (ms / 1e3), "unit": "rows/s", "ms_per_step": ms,
+                      "hbm_gbs": alg / (ms / 1e3) / 1e9, "frac_of_peak": alg / (ms / 1e3) / 1e9 / peak,
+                      "peak_kind": peak_kind_note(kind), "ledger_peak_bytes": ctx.ledger()["peak"]}), flush=True)
+    agg.close()
+    ctx.close()
+
+
+def run_batched(args):
+    """512 filter + GROUP BY queries (rows log-uniform 1e4..1e7, cardinality 16..1e6): one graph-replayed
+    persistent launch against the plain per-query path (one pipeline call per query)."""
+    import numpy as np
+    import torch
+    import wadjet_b200 as wg
+    from wadjet_b200 import autotune, synth
+    ctx = wg.Context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    qs, rows = [], 0
+    for q in range(args.queries):
+        key, val, filt, card, thr = synth.batched_query(ctx, q)
+        vt = wg.TYPE_INT64 if q % 2 == 0 else wg.TYPE_FLOAT64
+        qs.append({"batch": wg.Batch([wg.Column(wg.TYPE_INT64, key), wg.Column(vt, val),
+                                      wg.Column(wg.TYPE_INT32, filt)]),
+                   "group_by": [0], "aggs": [wg.AggColumn(wg.AGG_SUM, 1), wg.AggColumn(wg.AGG_COUNT, -1),
+                                             wg.AggColumn(wg.AGG_MIN, 1), wg.AggColumn(wg.AGG_MAX, 1)],
+                   "filters": [(2, wg.OP_LT, thr)], "ndv_hint": card, "_keep": (key, val, filt)})
+        rows += key.shape[0]
+    params = autotune.load_tuned()
+    bq = wg.BatchedQueries(ctx, qs, params)
+    ms_batched = _timed_ms(stream, bq.run, args.steps, args.warmup)
+    bq.close()
+    # plain path: one aggregate and one pipeline call per query, run back to back
+    aggs = [wg.HashAggregate(ctx, q["group_by"], q["aggs"], ndv_hint=q["ndv_hint"]) for q in qs]
+    done_ms = []
+
+    def plain():
+        t0 = time.perf_counter()
+        done_ms.clear()
+        for q, agg in zip(qs, aggs):
+            agg.reset()
+            wg.run_pipeline(ctx, q["batch"], agg, filters=q["filters"], device=True)
+            agg.finalize()
+            done_ms.append(1e3 * (time.perf_counter() - t0))
+
+    ms_plain = _timed_ms(stream, plain, max(1, args.steps // 2), 1)
+    for a in aggs:
+        a.close()
+    peak, kind = measured_peak_hbm()
+    print(json.dumps({
+        "workload": "batched", "metric": "queries/s", "queries": args.queries, "rows": rows,
+        "value": args.queries / (ms_batched / 1e3), "unit": "queries/s", "ms_per_batch": ms_batched,
+        "plain_queries_per_s": args.queries / (ms_plain / 1e3), "plain_ms_per_batch": ms_plain,
+        "speedup_vs_plain": ms_plain / ms_batched,
+        "p50_ms": {"batched": ms_batched, "plain": float(np.percentile(done_ms, 50))},
+        "p99_ms": {"batched": ms_batched, "plain": float(np.percentile(done_ms, 99))},
+        "hbm_gbs": rows * 20 / (ms_batched / 1e3) / 1e9, "peak": peak, "peak_kind": kind,
+        "tuned": params.__dict__ if params else None}), flush=True)
+    ctx.close()
+
+
+def run_serving(args):
+    """Poisson arrivals over three templates (GROUP BY, star join + agg, IPv4 /24 GROUP BY) on resident
+    tables, request sizes log-uniform in [1e5, 1e8] rows (prefixes of 1e8-row resident tables)."""
+    import threading
+    import numpy as np
+    import torch
+    import wadjet_b200 as wg
+    from wadjet_b200 import synth
+    I32, I64, F64, DEC = wg.TYPE_INT32, wg.TYPE_INT64, wg.TYPE_FLOAT64, wg.TYPE_DECIMAL
+    ctx = wg.Context(0)
+    nmax = 100_000_000
+    gb = synth.groupby(ctx, nmax)
+    fk, qty, price, disc = synth.starjoin_fact(ctx, nmax)
+    key, grp = synth.starjoin_dim(ctx)
+    join = wg.HashJoin(ctx, 0, 0, payload=[1], build_row_hint=DIM_ROWS)
+    join.build([wg.Batch([wg.Column(I32, key), wg.Column(I32, grp)])], device=True)
+    rng = np.random.default_rng(2000)
+    addr = torch.from_numpy((np.int64(10 << 24) + rng.integers(0, 1 << 24, nmax)).astype(np.int64)).cuda()
+    nbytes = torch.from_numpy(np.round(rng.lognormal(8.0, 2.0, nmax)).astype(np.int64)).cuda()
+    expr_join = wg.Expr(F64, [wg.Expr.col(2), wg.Expr.const_f(1.0), wg.Expr.col(3), "-", "*"])
+    expr_ip = wg.Expr(I64, [wg.Expr.col(0), wg.Expr.const_i(8), ">>"])
+
+    def request(t, n):
+        if t == 0:
+            return dict(batch=wg.Batch([wg.Column(I64, gb[0][:n]), wg.Column(I64, gb[1][:n]),
+                                        wg.Column(F64, gb[2][:n]), wg.Column(I32, gb[3][:n])]), group_by=[0],
+                        aggs=[wg.AggColumn(wg.AGG_SUM, 1), wg.AggColumn(wg.AGG_COUNT, -1),
+                              wg.AggColumn(wg.AGG_MIN, 2), wg.AggColumn(wg.AGG_MAX, 2)],
+                        filters=[(3, wg.OP_LT, 7)], ndv_hint=4096)
+        if t == 1:
+            return dict(batch=wg.Batch([wg.Column(I32, fk[:n]), wg.Column(I32, qty[:n]),
+                                        wg.Column(DEC, price[:n], scale=2), wg.Column(F64, disc[:n])]),
+                        group_by=[4], aggs=[wg.AggColumn(wg.AGG_SUM, 5), wg.AggColumn(wg.AGG_SUM, 2)],
+                        filters=[(1, wg.OP_GT, 10)], join=join, exprs=[expr_join], ndv_hint=1000)
+        return dict(batch=wg.Batch([wg.Column(I64, addr[:n]), wg.Column(I64, nbytes[:n])]), group_by=[2],
+                    aggs=[wg.AggColumn(wg.AGG_SUM, 1), wg.AggColumn(wg.AGG_COUNT, -1)], exprs=[expr_ip],
+                    ndv_hint=1 << 16)
+
+    prng = np.random.default_rng(42)
+    n_req = int(args.qps * args.seconds)
+    gaps = prng.exponential(1.0 / args.qps, n_req)
+    kinds = prng.integers(0, 3, n_req)
+    sizes = (np.exp(prng.uniform(np.log(1e5), np.log(1e8), n_req)) // 64 * 64).astype(np.int64)
+    specs = [request(int(t), int(n)) for t, n in zip(kinds, sizes)]
+
+    def drive(slots):
+        srv = wg.Server(ctx, slots)
+        for i in range(min(24, n_req)):  # warm the per-slot pools
+            tk = srv.submit(**specs[i])
+            srv.wait(tk)
+            srv.release(tk)
+        srv.reset_stats()
+        tickets = []
+        lock = threading.Lock()
+        done = threading.Event()
+
+        def completer():
+            i = 0
+            while True:
+                with lock:
+                    if i < len(tickets):
+                        tk = tickets[i]
+                    elif done.is_set():
+                        return
+                    else:
+                        tk = None
+                if tk is None:
+                    time.sleep(0.0002)
+                    continue
+                srv.wait(tk)
+                srv.release(tk)
+                i += 1
+
+        th = threading.Thread(target=completer)
+        th.start()
+        t0 = time.perf_counter()
+        due = t0
+        for gap, spec in zip(gaps, specs):
+            due += gap
+            while time.perf_counter() < due:
+                pass
+            tk = srv.submit(**spec)
+            with lock:
+                tickets.append(tk)
+        done.set()
+        th.join()
+        st = srv.stats()
+        srv.close()
+        return st
+
+    cont = drive(args.slots)
+    plain = drive(1)
+    print(json.dumps({
+        "workload": "serving", "metric": "queries/s", "offered_qps": args.qps, "requests": n_req,
+        "value": cont["qps"], "unit": "queries/s", "slots": args.slots,
+        "p50_ms": 1e3 * cont["p50_s"], "p99_ms": 1e3 * cont["p99_s"],
+        "plain": {"qps": plain["qps"], "p50_ms": 1e3 * plain["p50_s"], "p99_ms": 1e3 * plain["p99_s"]},
+        "mean_rows_per_request": float(sizes.mean()), "templates": ["groupby", "join+agg", "ipv4 /24"]}),
+        flush=True)
+    join.close()
+    ctx.close()
+
+
 def main():
     args = parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -345,6 +589,10 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.workload != "starjoin":
+        {"groupby": run_groupby, "highcard": run_highcard, "batched": run_batched,
+         "serving": run_serving}[args.workload](args)
         return
     run_ours(args, rank, world, local_rank)
 

@@ -204,6 +204,11 @@ WG_API const char* wg_version(void);
  * caps the pinned host memory used for aggregate spill partitions. */
 WG_API wg_status wg_ctx_create(int32_t device, int64_t hbm_budget_bytes,
                         int64_t pinned_spill_bytes, wg_ctx** out);
+/* A context on the parent's device with its own streams and a child ledger
+ * that shares the parent's budget (Tracker.Child, memory/tracker.go:44):
+ * concurrent queries each get one, and every reservation also counts against
+ * the parent. The parent must outlive its children. */
+WG_API wg_status wg_ctx_create_child(wg_ctx* parent, wg_ctx** out);
 WG_API wg_status wg_ctx_destroy(wg_ctx* ctx);
 /* Wait until all work queued on the context's stream is done. */
 WG_API wg_status wg_ctx_synchronize(wg_ctx* ctx);
@@ -374,6 +379,45 @@ WG_API wg_status wg_batched_run(wg_batched* b, int64_t* n_groups);
 /* Raw state of query q's groups (as wg_agg_export) after a run. */
 WG_API wg_status wg_batched_export(wg_batched* b, int32_t q, const wg_group_export* out);
 WG_API wg_status wg_batched_destroy(wg_batched* b);
+
+/* ======================================================================== */
+/* Serving: a continuous-batching request loop. Requests are admitted into   */
+/* free slots (each with its own child context and stream) as slots and HBM  */
+/* (the shared ledger) free up, so requests that arrive while others run     */
+/* overlap on the device. Tables and join indexes stay resident across       */
+/* requests. No counterpart in the reference (its server runs each query's   */
+/* Pipeline.Run on goroutines, internal/server/grpc.go:120).                  */
+/* ======================================================================== */
+typedef struct wg_server wg_server;
+
+typedef struct wg_serve_request {
+  const wg_pipeline_desc* plan;  /* device-resident input; plan->agg is ignored */
+  const int32_t*          key_cols;
+  const wg_agg_spec*      aggs;
+  int32_t                 n_keys;
+  int32_t                 n_aggs;
+  int64_t                 ndv_hint;
+  int64_t                 est_bytes;  /* HBM held for admission; 0 = estimated from the hint */
+} wg_serve_request;
+
+typedef struct wg_serve_stats {
+  int64_t submitted, completed, failed, in_flight, queued;
+  double  p50_s, p99_s, mean_s, max_s;   /* latency = completion - submission */
+  double  qps;                           /* completed / (last completion - first submission) */
+} wg_serve_stats;
+
+WG_API wg_status wg_server_create(wg_ctx* ctx, int32_t n_slots, wg_server** out);
+/* Queue a request (copied); thread-safe. */
+WG_API wg_status wg_server_submit(wg_server* s, const wg_serve_request* r, int64_t* ticket);
+/* Wait for a request (timeout_s < 0: forever); its status is returned. */
+WG_API wg_status wg_server_wait(wg_server* s, int64_t ticket, double timeout_s, int64_t* n_groups, double* latency_s);
+WG_API wg_status wg_server_export(wg_server* s, int64_t ticket, const wg_group_export* out);
+/* Free a finished request's result and its HBM. */
+WG_API wg_status wg_server_release(wg_server* s, int64_t ticket);
+WG_API wg_status wg_server_stats(wg_server* s, wg_serve_stats* out);
+/* Forget latency statistics (e.g. after a warm-up). */
+WG_API wg_status wg_server_reset_stats(wg_server* s);
+WG_API wg_status wg_server_destroy(wg_server* s);
 
 /* ======================================================================== */
 /* Synthetic benchmark tables, generated in HBM (include/wadjet_synth.h).    */

@@ -141,12 +141,13 @@ class HostBatch:
 
 
 def filter_(t, data, valid, op, value, sel=None) -> np.ndarray:
-    col = HostBatch([(t, data, valid, 0)]).arr
+    hb = HostBatch([(t, data, valid, 0)])  # keeps the column and its packed validity alive for the call
     kind, i, f = (1, 0, float(value)) if isinstance(value, float) else (0, int(value), 0.0)
     p = Predicate(0, op, kind, 0, i, f)
     s = None if sel is None else np.ascontiguousarray(sel, np.uint32)
     out = np.empty(max(1, len(data) if s is None else len(s)), np.uint32)
-    n = lib().or_filter(C.byref(col[0]), len(data), _ptr(s), 0 if s is None else len(s), C.byref(p), out.ctypes.data)
+    n = lib().or_filter(C.byref(hb.arr[0]), len(data), _ptr(s), 0 if s is None else len(s), C.byref(p),
+                        out.ctypes.data)
     if n < 0:
         raise RuntimeError(_err())
     return out[:n].copy()

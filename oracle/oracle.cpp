@@ -761,8 +761,8 @@ int or_join_append(void* jp, const wg_column* key, int64_t base_row) {  // arena
     j->arena.push_back(base_row + i);
     auto r = j->index->put(k, idx);
     j->arena_next.push_back(r.second ? r.first : -1);
+    j->index->check_grow();  // per insert: a batch may hold more keys than the table has free slots
   }
-  j->index->check_grow();
   j->rows_seen += key->len;
   return 0;
 }

@@ -73,7 +73,7 @@ def test_join_matches_oracle(ctx, kt, dups, nulls):
     dt = np.int32 if kt == I32 else np.int64
     bkeys = (rng.integers(0, 5_000 if dups else 1 << 30, nb) if dups else rng.permutation(1 << 20)[:nb]).astype(dt)
     if kt == I64:
-        bkeys = bkeys * np.int64(1 << 33) - 7
+        bkeys = bkeys * np.int64(0x100000001) - 7  # spans the full int64 range
     pkeys = bkeys[rng.integers(0, nb, npr)].copy()
     pkeys[::7] = (pkeys[::7] + 1)  # some misses
     bvalid = random_valid(rng, nb, nulls)

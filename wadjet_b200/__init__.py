@@ -518,6 +518,68 @@ class BatchedQueries:
             self.h = None
 
 
+class Server:
+    """Continuous-batching request loop over device-resident tables (wg_server_*).
+
+    submit(batch, group_by, aggs, filters=(), join=None, exprs=(), ndv_hint=0) → ticket;
+    wait(ticket) → (n_groups, latency_s); export(ticket, n_groups) → raw group state;
+    release(ticket) frees the result (its aggregate returns to the slot's pool)."""
+
+    def __init__(self, ctx: Context, slots: int):
+        self.ctx = ctx
+        h = C.c_void_p()
+        _check(lib.wg_server_create(ctx.h, slots, C.byref(h)))
+        self.h = h
+        self._shapes: dict[int, tuple[int, int]] = {}
+
+    def submit(self, batch: Batch, group_by: Sequence[int], aggs: Sequence[AggColumn], filters: Sequence = (),
+               join: Optional["HashJoin"] = None, exprs: Sequence[Expr] = (), ndv_hint: int = 0,
+               est_bytes: int = 0) -> int:
+        d, keep = batch.desc()
+        preds = (abi.wg_predicate * max(1, len(filters)))(*[predicate(*f) for f in filters])
+        ex = (abi.wg_expr * max(1, len(exprs)))(*[e.to_c() for e in exprs])
+        p = abi.wg_pipeline_desc(C.pointer(d), len(filters), len(exprs), preds, join.h if join else None, ex, None)
+        keys = (C.c_int32 * max(1, len(group_by)))(*group_by)
+        specs = (abi.wg_agg_spec * max(1, len(aggs)))(*[abi.wg_agg_spec(a.func, a.input_col, a.out_type, 0)
+                                                        for a in aggs])
+        r = abi.wg_serve_request(C.pointer(p), keys, specs, len(group_by), len(aggs), ndv_hint, est_bytes)
+        t = C.c_int64()
+        _check(lib.wg_server_submit(self.h, C.byref(r), C.byref(t)))
+        self._shapes[t.value] = (len(group_by), len(aggs))
+        return t.value
+
+    def wait(self, ticket: int, timeout: float = -1.0) -> tuple[int, float]:
+        n, lat = C.c_int64(), C.c_double()
+        _check(lib.wg_server_wait(self.h, ticket, timeout, C.byref(n), C.byref(lat)))
+        return n.value, lat.value
+
+    def export(self, ticket: int, n_groups: int) -> dict:
+        nk, na = self._shapes[ticket]
+        r = _export_arrays(nk, na, n_groups)
+        if n_groups:
+            e = abi.wg_group_export(*[r[k].ctypes.data if r[k].size else None
+                                      for k in ("keys", "key_valid", "count", "i64", "f64", "dec", "has")])
+            _check(lib.wg_server_export(self.h, ticket, C.byref(e)))
+        return r
+
+    def release(self, ticket: int) -> None:
+        _check(lib.wg_server_release(self.h, ticket))
+        self._shapes.pop(ticket, None)
+
+    def stats(self) -> dict:
+        s = abi.wg_serve_stats()
+        _check(lib.wg_server_stats(self.h, C.byref(s)))
+        return {f: getattr(s, f) for f, _ in abi.wg_serve_stats._fields_}
+
+    def reset_stats(self) -> None:
+        _check(lib.wg_server_reset_stats(self.h))
+
+    def close(self) -> None:
+        if self.h:
+            lib.wg_server_destroy(self.h)
+            self.h = None
+
+
 def predicate(col: int, op: int, value) -> abi.wg_predicate:
     kind, i, f = _const(value)
     return abi.wg_predicate(col, op, kind, 0, i, f)

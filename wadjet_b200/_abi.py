@@ -79,6 +79,18 @@ class wg_tune_params(C.Structure):
                 ("smem_max_groups", C.c_int32), ("max_load", C.c_double)]
 
 
+class wg_serve_request(C.Structure):
+    _fields_ = [("plan", C.POINTER(wg_pipeline_desc)), ("key_cols", C.POINTER(C.c_int32)),
+                ("aggs", C.POINTER(wg_agg_spec)), ("n_keys", C.c_int32), ("n_aggs", C.c_int32),
+                ("ndv_hint", C.c_int64), ("est_bytes", C.c_int64)]
+
+
+class wg_serve_stats(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("failed", C.c_int64),
+                ("in_flight", C.c_int64), ("queued", C.c_int64), ("p50_s", C.c_double), ("p99_s", C.c_double),
+                ("mean_s", C.c_double), ("max_s", C.c_double), ("qps", C.c_double)]
+
+
 P = C.c_void_p
 PP = C.POINTER(C.c_void_p)
 I32, I64, F64 = C.c_int32, C.c_int64, C.c_double
@@ -89,6 +101,7 @@ SIGNATURES = {
     "wg_last_error": (C.c_char_p, []),
     "wg_version": (C.c_char_p, []),
     "wg_ctx_create": (I32, [I32, I64, I64, PP]),
+    "wg_ctx_create_child": (I32, [P, PP]),
     "wg_ctx_destroy": (I32, [P]),
     "wg_ctx_synchronize": (I32, [P]),
     "wg_ledger_stats": (I32, [P, PI64, PI64, PI64]),
@@ -125,6 +138,14 @@ SIGNATURES = {
     "wg_batched_run": (I32, [P, PI64]),
     "wg_batched_export": (I32, [P, I32, C.POINTER(wg_group_export)]),
     "wg_batched_destroy": (I32, [P]),
+    "wg_server_create": (I32, [P, I32, PP]),
+    "wg_server_submit": (I32, [P, C.POINTER(wg_serve_request), PI64]),
+    "wg_server_wait": (I32, [P, I64, F64, PI64, C.POINTER(C.c_double)]),
+    "wg_server_export": (I32, [P, I64, C.POINTER(wg_group_export)]),
+    "wg_server_release": (I32, [P, I64]),
+    "wg_server_stats": (I32, [P, C.POINTER(wg_serve_stats)]),
+    "wg_server_reset_stats": (I32, [P]),
+    "wg_server_destroy": (I32, [P]),
     "wg_synth_starjoin_fact": (I32, [P, C.c_uint64, I64, I64, P, P, P, P]),
     "wg_synth_starjoin_dim": (I32, [P, C.c_uint64, I64, P, P]),
     "wg_synth_groupby": (I32, [P, C.c_uint64, I64, I64, I64, P, P, P, P]),

@@ -144,20 +144,9 @@ const char* wg_last_error(void) { return wg::t_err.c_str(); }
 
 const char* wg_version(void) { return "wadjet-b200 0.1.0 (sm_100a)"; }
 
-wg_status wg_ctx_create(int32_t device, int64_t hbm_budget_bytes, int64_t pinned_spill_bytes, wg_ctx** out) {
-  if (!out) return fail(WG_E_INVALID, "out is NULL");
-  *out = nullptr;
-  int ndev = 0;
-  WG_CUDA_TRY(cudaGetDeviceCount(&ndev));
-  if (device < 0 || device >= ndev) return fail(WG_E_INVALID, "no such CUDA device");
-  WG_CUDA_TRY(cudaSetDevice(device));
-  int64_t budget = hbm_budget_bytes;
-  if (budget <= 0) {
-    size_t free_b = 0, total_b = 0;
-    WG_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
-    budget = (int64_t)free_b;
-  }
-  wg_ctx* c = new wg_ctx(budget);
+static wg_status ctx_make(int32_t device, int64_t budget, wg::Ledger* parent, int64_t pinned_spill_bytes,
+                          wg_ctx** out) {
+  wg_ctx* c = new wg_ctx(budget, parent);
   c->device = device;
   c->pinned_spill_bytes = pinned_spill_bytes;
   cudaDeviceProp prop;
@@ -183,6 +172,29 @@ wg_status wg_ctx_create(int32_t device, int64_t hbm_budget_bytes, int64_t pinned
   cudaDeviceSynchronize();
   *out = c;
   return WG_OK;
+}
+
+wg_status wg_ctx_create(int32_t device, int64_t hbm_budget_bytes, int64_t pinned_spill_bytes, wg_ctx** out) {
+  if (!out) return fail(WG_E_INVALID, "out is NULL");
+  *out = nullptr;
+  int ndev = 0;
+  WG_CUDA_TRY(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev) return fail(WG_E_INVALID, "no such CUDA device");
+  WG_CUDA_TRY(cudaSetDevice(device));
+  int64_t budget = hbm_budget_bytes;
+  if (budget <= 0) {
+    size_t free_b = 0, total_b = 0;
+    WG_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+    budget = (int64_t)free_b;
+  }
+  return ctx_make(device, budget, nullptr, pinned_spill_bytes, out);
+}
+
+wg_status wg_ctx_create_child(wg_ctx* parent, wg_ctx** out) {
+  if (!parent || !out) return fail(WG_E_INVALID, "NULL argument");
+  *out = nullptr;
+  WG_TRY(ensure_device(parent));
+  return ctx_make(parent->device, parent->ledger.budget(), &parent->ledger, parent->pinned_spill_bytes, out);
 }
 
 wg_status wg_ctx_destroy(wg_ctx* c) {

@@ -59,7 +59,7 @@ constexpr int kRows = 4;
 constexpr unsigned long long kFlagAgg = 1ULL << 62;
 constexpr unsigned long long kFlagInc = 2ULL << 62;
 constexpr unsigned long long kValMask = (1ULL << 62) - 1;
-constexpr long long kSpinLimit = 1LL << 22;
+constexpr long long kSpinLimit = 1LL << 20;
 
 struct FilterArgs {
   DCol col;

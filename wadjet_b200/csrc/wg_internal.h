@@ -34,20 +34,30 @@ wg_status fail(wg_status code, const std::string& msg);
   } while (0)
 
 // ---- HBM ledger (memory.Tracker, internal/engine/memory/tracker.go:19-160) ----
-// Lock-free Reserve with rollback; Peak is the high-water mark of Used.
+// Lock-free Reserve with rollback; Peak is the high-water mark of Used. A child
+// ledger (Tracker.Child, tracker.go:44) shares its parent's budget: a
+// reservation must fit both, and releases bubble up.
 class Ledger {
  public:
-  explicit Ledger(int64_t budget) : budget_(budget) {}
+  explicit Ledger(int64_t budget, Ledger* parent = nullptr) : budget_(budget), parent_(parent) {}
   bool reserve(int64_t n) {
     int64_t now = used_.fetch_add(n) + n;
     if (budget_ > 0 && now > budget_) {
       used_.fetch_sub(n);
       return false;
     }
+    if (parent_ && !parent_->reserve(n)) {
+      used_.fetch_sub(n);
+      return false;
+    }
     bump_peak(now);
     return true;
   }
-  void release(int64_t n) { used_.fetch_sub(n); }
+  void release(int64_t n) {
+    used_.fetch_sub(n);
+    if (parent_) parent_->release(n);
+  }
+  Ledger* parent() const { return parent_; }
   int64_t used() const { return used_.load(); }
   int64_t peak() const { return peak_.load(); }
   int64_t budget() const { return budget_; }
@@ -58,6 +68,7 @@ class Ledger {
     while (v > p && !peak_.compare_exchange_weak(p, v)) {}
   }
   int64_t budget_;
+  Ledger* parent_;
   std::atomic<int64_t> used_{0};
   std::atomic<int64_t> peak_{0};
 };
@@ -115,7 +126,7 @@ struct Ctx {
   int32_t* dev_error = nullptr;
   std::mutex mu;                    // serialises scalar read-backs
 
-  explicit Ctx(int64_t budget) : ledger(budget) {}
+  explicit Ctx(int64_t budget, Ledger* parent = nullptr) : ledger(budget, parent) {}
   void count_launch(int n = 1) { launches.fetch_add(n); }
 };
 
@@ -140,5 +151,5 @@ wg_status stage_batch(Ctx* ctx, const wg_batch_desc* in, StagedBatch* out);
 
 // Opaque handle bodies live in their .cu files; only the context is shared.
 struct wg_ctx : wg::Ctx {
-  explicit wg_ctx(int64_t budget) : wg::Ctx(budget) {}
+  explicit wg_ctx(int64_t budget, wg::Ledger* parent = nullptr) : wg::Ctx(budget, parent) {}
 };
