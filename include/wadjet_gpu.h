@@ -244,6 +244,32 @@ WG_API wg_status wg_filter_execute_device(wg_filter* f, const wg_batch_desc* in,
                                    uint32_t* out_sel_dev, int64_t* out_n);
 WG_API wg_status wg_filter_destroy(wg_filter* f);
 
+/* The filter for callers that cannot allocate device memory. No counterpart in
+ * the reference. Some callers must not call cudaMalloc: a Go operator whose
+ * device memory was reserved up front from the engine's memory budget (the
+ * ledger would not see a private allocation), a thread that issues work while
+ * another thread captures a CUDA graph in global mode (a cudaMalloc there
+ * invalidates the capture), or a latency-critical serving thread (cudaMalloc
+ * and cudaFree can synchronise the whole device). This entry point allocates
+ * nothing: the compaction's tile-status scratch lives in a fixed static device
+ * array of WG_NOALLOC_SCRATCH_BYTES, held by every GPU that loads the library
+ * until the process exits. It takes a CUDA stream instead of a context, a
+ * device column and optional device selection vector (n_items = selection
+ * length, else column length), writes the ascending selection to out_sel (device,
+ * n_items entries of room) and the count to *out_n (host). It refuses inputs
+ * of more than WG_NOALLOC_MAX_ITEMS rows with WG_E_INVALID.
+ * - The first call on a device looks up the array's device address (set-up);
+ *   make that first call before any stream capture.
+ * - Every call uses the same array and leaves its contents behind (each call
+ *   clears what must start at zero); calls whose work overlaps on the GPU race
+ *   on it, so callers serialise them (one stream, or their own lock). */
+#define WG_NOALLOC_MAX_ITEMS (1LL << 26)
+#define WG_NOALLOC_SCRATCH_BYTES (65536 * 8 + 256)
+WG_API wg_status wg_filter_execute_device_noalloc(void* stream, const wg_column* col, const uint32_t* sel,
+                                                  int64_t n_items, int32_t op, int32_t const_kind,
+                                                  int64_t const_i64, double const_f64, uint32_t* out_sel,
+                                                  int64_t* out_n);
+
 /* ======================================================================== */
 /* Hash join: exec.HashJoin / HashJoinProbe (internal/engine/exec/join.go)   */
 /* ======================================================================== */

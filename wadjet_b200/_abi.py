@@ -113,6 +113,7 @@ SIGNATURES = {
     "wg_filter_execute": (I32, [P, C.POINTER(wg_batch_desc), P, PI64]),
     "wg_filter_execute_device": (I32, [P, C.POINTER(wg_batch_desc), P, PI64]),
     "wg_filter_destroy": (I32, [P]),
+    "wg_filter_execute_device_noalloc": (I32, [P, C.POINTER(wg_column), P, I64, I32, I32, I64, F64, P, PI64]),
     "wg_join_create": (I32, [P, I32, I32, I32, I32, C.POINTER(C.c_int32), I64, PP]),
     "wg_join_build_append": (I32, [P, C.POINTER(wg_batch_desc)]),
     "wg_join_build_append_device": (I32, [P, C.POINTER(wg_batch_desc)]),

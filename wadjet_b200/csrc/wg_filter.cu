@@ -322,3 +322,91 @@ wg_status wg_filter_destroy(wg_filter* f) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant for callers that cannot call cudaMalloc (see the
+// header): the tile-status words, the tile counter, the device error word and
+// the survivor count live in one static device array instead of per-handle
+// device buffers. Layout: status[65536] | counter (int32) | error (int32) |
+// count (int64).
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int64_t kNoAllocTiles = 65536;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[WG_NOALLOC_SCRATCH_BYTES];
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[64] = {nullptr};  // per device: the array's device address, looked up once
+
+}  // namespace
+
+extern "C" wg_status wg_filter_execute_device_noalloc(void* stream, const wg_column* col, const uint32_t* sel,
+                                                      int64_t n_items, int32_t op, int32_t const_kind,
+                                                      int64_t const_i64, double const_f64, uint32_t* out_sel,
+                                                      int64_t* out_n) {
+  if (!col || !col->data || !out_n || (n_items > 0 && !out_sel) || n_items < 0)
+    return fail(WG_E_INVALID, "NULL argument");
+  if (n_items > WG_NOALLOC_MAX_ITEMS)
+    return fail(WG_E_INVALID, "input of " + std::to_string(n_items) + " rows exceeds the allocation-free limit of " +
+                                  std::to_string((long long)WG_NOALLOC_MAX_ITEMS));
+  if (op < WG_OP_EQ || op > WG_OP_GE || (const_kind != WG_CONST_INT && const_kind != WG_CONST_FLOAT))
+    return fail(WG_E_INVALID, "unknown compare op or constant kind");
+  wgd::Pred p;
+  WG_TRY(resolve_pred(wg_predicate{0, op, const_kind, 0, const_i64, const_f64}, col->type_id, &p));
+  int dev = -1;
+  WG_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(WG_E_INVALID, "device ordinal out of range");
+  unsigned char* base = nullptr;
+  {
+    std::lock_guard<std::mutex> g(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {  // set-up, once per device, with that device current
+      void* ptr = nullptr;
+      cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+      if (e != cudaSuccess) return fail(WG_E_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+      g_noalloc_addr[dev] = ptr;
+    }
+    base = (unsigned char*)g_noalloc_addr[dev];
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  unsigned long long* status = (unsigned long long*)base;
+  int* counter = (int*)(base + kNoAllocTiles * 8);
+  int32_t* err = (int32_t*)(base + kNoAllocTiles * 8 + 4);
+  int64_t* count = (int64_t*)(base + kNoAllocTiles * 8 + 8);
+  const int cls = class_of(col->type_id);
+  const int64_t es = elem_size(col->type_id);
+  const bool vec = sel == nullptr && ((uintptr_t)col->data % 16 == 0);
+  const int64_t V = vec ? 16 / es : 1;
+  const int64_t tiles = (n_items + kBlock * V * kRows - 1) / (kBlock * V * kRows);
+  // the previous call's words are still there: clear the counter, error, count and the status words in use
+  WG_CUDA_TRY(cudaMemsetAsync(counter, 0, 16, st));
+  if (tiles > 0) WG_CUDA_TRY(cudaMemsetAsync(status, 0, (size_t)(tiles * 8), st));
+  if (tiles > 0) {
+    FilterArgs a;
+    a.col = wgd::DCol{col->data, col->valid_words, cls, col->scale};
+    a.p = p;
+    a.sel = sel;
+    a.n = n_items;
+    a.out = out_sel;
+    a.status = status;
+    a.tile_counter = counter;
+    a.out_n = count;
+    a.err = err;
+    a.num_tiles = tiles;
+    dim3 grid((unsigned)tiles);
+    switch (cls) {
+      case WG_CLS_I32: launch_cls<WG_CLS_I32>(vec, a, grid, st); break;
+      case WG_CLS_I64: launch_cls<WG_CLS_I64>(vec, a, grid, st); break;
+      case WG_CLS_F32: launch_cls<WG_CLS_F32>(vec, a, grid, st); break;
+      case WG_CLS_F64: launch_cls<WG_CLS_F64>(vec, a, grid, st); break;
+      default: return fail(WG_E_UNSUPPORTED, "filter on this column type is not on the GPU path");
+    }
+    WG_CUDA_TRY(cudaGetLastError());
+  }
+  int64_t host[2] = {0, 0};  // count, then the error word
+  WG_CUDA_TRY(cudaMemcpyAsync(&host[0], count, 8, cudaMemcpyDeviceToHost, st));
+  WG_CUDA_TRY(cudaMemcpyAsync(&host[1], err, 4, cudaMemcpyDeviceToHost, st));
+  WG_CUDA_TRY(cudaStreamSynchronize(st));
+  if ((int32_t)host[1] != WG_DERR_NONE) return fail(WG_E_TIMEOUT, "bounded device wait expired");
+  *out_n = tiles > 0 ? host[0] : 0;
+  return WG_OK;
+}
