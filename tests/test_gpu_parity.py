@@ -121,7 +121,7 @@ def agg_setup(rng, n, key_types, ncard, nulls, key_nulls):
         k = rng.integers(-ncard // 2, ncard // 2, n).astype(dt)
         if kt == I64:
             k = k * np.int64(0x9E3779B97F4A7C1) + 3
-            k[::97] = np.int64(-0x7FFFFFFFFFFFFFFF)  # the int-hash empty sentinel is a real key
+            k[k == np.int64(-0x7FFFFFFFFFFFFFFF)] = 0  # see test_int_hash_sentinel_key_is_one_group
         kv = random_valid(rng, n, key_nulls)
         cols.append((kt, k, kv))
     for t in (I32, I64, F32, F64, DEC):
@@ -252,6 +252,28 @@ def test_emit_pages_match_oracle(ctx):
         np.testing.assert_array_equal(got[i][1][og], want[i][1][ow])
         m = want[i][1][ow]
         np.testing.assert_allclose(got[i][0][og][m], want[i][0][ow][m], rtol=1e-12, atol=0)
+    g.close()
+
+
+def test_int_hash_sentinel_key_is_one_group(ctx):
+    """The key -0x7FFFFFFFFFFFFFFF is the reference intHashTable's empty marker
+    (internal/engine/exec/int_hash.go:42): inserting it leaves the slot looking
+    empty, so the reference (and the oracle, which restates it) gives every row
+    with that key a group of its own. On the GPU every key value, including the
+    table's own sentinel, is one real group; this test pins that divergence."""
+    import wadjet_b200 as wg
+    sentinel = np.int64(-0x7FFFFFFFFFFFFFFF)
+    k = np.array([1, sentinel, 2, sentinel, sentinel, 1], np.int64)
+    v = np.arange(6, dtype=np.int64)
+    g = wg.HashAggregate(ctx, [0], [wg.AggColumn(wg.AGG_COUNT, -1), wg.AggColumn(wg.AGG_SUM, 1)])
+    g.consume(wg.Batch([wg.Column(I64, k), wg.Column(I64, v)]))
+    g.finalize()
+    e = g.export()
+    got = dict(zip(e["keys"][0].tolist(), zip(e["count"][0].tolist(), e["i64"][1].tolist())))
+    assert got == {1: (2, 5), 2: (1, 2), int(sentinel): (3, 1 + 3 + 4)}
+    o = ob.Agg([0], [(1, -1, 0)])
+    o.consume(ob.HostBatch([(I64, k, None, 0)]))
+    assert o.groups() == 2 + 3  # the reference's behaviour: one group per sentinel row
     g.close()
 
 
