@@ -340,6 +340,11 @@ WG_API wg_status wg_agg_emit(wg_agg* a, int64_t start, int64_t max_rows,
 WG_API wg_status wg_agg_export(wg_agg* a, const wg_group_export* out);
 /* Forget all groups and input (the state after wg_agg_create). */
 WG_API wg_status wg_agg_reset(wg_agg* a);
+/* Diagnostic, no counterpart in the reference: the compiled query shape the
+ * last fused launch into `a` ran on (1..6: a kernel built for exactly that
+ * query shape; 0: the generic kernel; -1: no fused launch yet). Results never
+ * depend on it. */
+WG_API int32_t wg_agg_kernel_shape(const wg_agg* a);
 WG_API wg_status wg_agg_destroy(wg_agg* a);
 
 /* ======================================================================== */

@@ -41,10 +41,12 @@ def kinds(vt):
     return ["sum_i", "count", "min_i", "max_i"] if vt == I64 else ["sum_f", "count", "min_f", "max_f"]
 
 
-@pytest.mark.parametrize("params", [None, "nosmem", "small_tiles"])
-def test_batched_matches_oracle(ctx, params):
+@pytest.mark.parametrize("params", [None, "nosmem", "small_tiles", "generic"])
+def test_batched_matches_oracle(ctx, params, monkeypatch):
     import wadjet_b200 as wg
-    tp = {None: None, "nosmem": wg.TuneParams(smem_max_groups=-1),
+    # "generic": the kernel that reads the query shape at run time instead of the compiled shapes
+    monkeypatch.setenv("WG_SPECIALIZE", "0" if params == "generic" else "1")
+    tp = {None: None, "generic": None, "nosmem": wg.TuneParams(smem_max_groups=-1),
           "small_tiles": wg.TuneParams(tile_rows=4096, block=256, ctas_per_sm=4)}[params]
     qs, host = make_queries(ctx, 24, 300_000)
     b = wg.BatchedQueries(ctx, qs, tp)

@@ -48,10 +48,17 @@ def test_device_generator_matches_host_generator(ctx):
     np.testing.assert_array_equal(f.cpu().numpy().view(np.uint64), hf.view(np.uint64))
 
 
-def test_groupby_workload_matches_oracle(ctx):
-    """SELECT k, SUM(v), COUNT(*), MIN(f), MAX(f) FROM t WHERE flag < 7 GROUP BY k, 2^20 rows."""
+# compiled query shapes (wg_agg_kernel_shape): 0 is the generic kernel
+SHAPE_STARJOIN, SHAPE_GROUPBY, SHAPE_HIGHCARD = 1, 2, 3
+
+
+@pytest.mark.parametrize("spec", ["1", "0"])
+def test_groupby_workload_matches_oracle(ctx, spec, monkeypatch):
+    """SELECT k, SUM(v), COUNT(*), MIN(f), MAX(f) FROM t WHERE flag < 7 GROUP BY k, 2^20 rows,
+    on the kernel compiled for this query shape and on the generic kernel."""
     import wadjet_b200 as wg
     from wadjet_b200 import synth
+    monkeypatch.setenv("WG_SPECIALIZE", spec)
     n = 1 << 20
     k, v, f, flag = synth.groupby(ctx, n)
     aggs = [wg.AggColumn(wg.AGG_SUM, 1), wg.AggColumn(wg.AGG_COUNT, -1), wg.AggColumn(wg.AGG_MIN, 2),
@@ -59,6 +66,7 @@ def test_groupby_workload_matches_oracle(ctx):
     g = wg.HashAggregate(ctx, [0], aggs, ndv_hint=4096)
     batch = wg.Batch([wg.Column(I64, k), wg.Column(I64, v), wg.Column(F64, f), wg.Column(I32, flag)])
     wg.run_pipeline(ctx, batch, g, filters=[(3, wg.OP_LT, 7)], device=True)
+    assert g.kernel_shape == (SHAPE_GROUPBY if spec == "1" else 0)
     g.finalize()
     hk, hv, hf, hflag = (t.cpu().numpy() for t in (k, v, f, flag))
     o = ob.Agg([0], [(0, 1, 0), (1, -1, 0), (2, 2, 0), (3, 2, 0)])
@@ -68,11 +76,13 @@ def test_groupby_workload_matches_oracle(ctx):
     g.close()
 
 
-KNOBS = [  # (WG_TILE, WG_JOIN_DIRECT, WG_AGG_SMEM): every GPU lever on, off, and mixed
-    ("1", "1", "1"), ("0", "0", "0"), ("1", "0", "1"), ("0", "1", "0"), ("1", "1", "0")]
+KNOB_NAMES = ("WG_TILE", "WG_JOIN_DIRECT", "WG_AGG_SMEM", "WG_SPECIALIZE")
+KNOBS = [  # every GPU lever on, off, and mixed
+    ("1", "1", "1", "1"), ("0", "0", "0", "0"), ("1", "0", "1", "1"), ("0", "1", "0", "1"), ("1", "1", "0", "1"),
+    ("1", "1", "1", "0"), ("0", "1", "1", "1")]
 
 
-@pytest.mark.parametrize("knobs", KNOBS, ids=lambda k: "tile%s-direct%s-smem%s" % k)
+@pytest.mark.parametrize("knobs", KNOBS, ids=lambda k: "tile%s-direct%s-smem%s-spec%s" % k)
 @pytest.mark.parametrize("host_input", [False, True])
 def test_starjoin_workload_matches_oracle(ctx, host_input, knobs, monkeypatch):
     """Star join + aggregate, 2^22 fact rows against the full 2^22-row dimension, with
@@ -82,7 +92,7 @@ def test_starjoin_workload_matches_oracle(ctx, host_input, knobs, monkeypatch):
     from wadjet_b200 import synth
     if host_input and knobs != KNOBS[0]:
         pytest.skip("host staging is lever-independent; covered with all levers on")
-    for name, val in zip(("WG_TILE", "WG_JOIN_DIRECT", "WG_AGG_SMEM"), knobs):
+    for name, val in zip(KNOB_NAMES, knobs):
         monkeypatch.setenv(name, val)
     n = 1 << 22
     fk, qty, price, disc = synth.starjoin_fact(ctx, n)
@@ -99,6 +109,8 @@ def test_starjoin_workload_matches_oracle(ctx, host_input, knobs, monkeypatch):
         batch = wg.Batch([wg.Column(I32, fk), wg.Column(I32, qty), wg.Column(DEC, price, scale=2),
                           wg.Column(F64, disc)])
     wg.run_pipeline(ctx, batch, g, filters=[(1, wg.OP_GT, 10)], join=j, exprs=[expr], device=not host_input)
+    # the compiled star-join shape needs the direct-payload join table
+    assert g.kernel_shape == (SHAPE_STARJOIN if knobs[1] == "1" and knobs[3] == "1" else 0)
     g.finalize()
     hkey, hgrp = key.cpu().numpy(), grp.cpu().numpy()
     oj = ob.Join(1 << 22)
@@ -113,12 +125,13 @@ def test_starjoin_workload_matches_oracle(ctx, host_input, knobs, monkeypatch):
     j.close()
 
 
-@pytest.mark.parametrize("tile", ["1", "0"])
-def test_highcard_workload_matches_oracle(ctx, tile, monkeypatch):
+@pytest.mark.parametrize("tile,spec", [("1", "1"), ("0", "1"), ("1", "0")])
+def test_highcard_workload_matches_oracle(ctx, tile, spec, monkeypatch):
     """GROUP BY (a int32, b int64) packed key, 2^22 rows (~3.9M groups)."""
     import wadjet_b200 as wg
     from wadjet_b200 import synth
     monkeypatch.setenv("WG_TILE", tile)
+    monkeypatch.setenv("WG_SPECIALIZE", spec)
     n = 1 << 22
     a, b, amt, x = synth.highcard(ctx, n)
     aggs = [wg.AggColumn(wg.AGG_SUM, 2), wg.AggColumn(wg.AGG_COUNT, -1), wg.AggColumn(wg.AGG_MIN, 3),
@@ -126,6 +139,7 @@ def test_highcard_workload_matches_oracle(ctx, tile, monkeypatch):
     g = wg.HashAggregate(ctx, [0, 1], aggs, ndv_hint=1 << 22)
     batch = wg.Batch([wg.Column(I32, a), wg.Column(I64, b), wg.Column(DEC, amt, scale=2), wg.Column(F64, x)])
     wg.run_pipeline(ctx, batch, g, device=True)
+    assert g.kernel_shape == (SHAPE_HIGHCARD if spec == "1" else 0)
     g.finalize()
     ha, hb, hamt, hx = a.cpu().numpy(), b.cpu().numpy(), to_host_dec(amt), x.cpu().numpy()
     o = ob.Agg([0, 1], [(0, 2, 0), (1, -1, 0), (2, 3, 0), (3, 3, 0)])
@@ -166,3 +180,26 @@ def test_starjoin_full_size_properties(ctx):
     torch.cuda.empty_cache()
     g.close()
     j.close()
+
+
+@pytest.mark.parametrize("spec", ["1", "0"])
+def test_ipv4_prefix_workload_matches_oracle(ctx, spec, monkeypatch):
+    """SELECT addr >> 8, SUM(bytes), COUNT(*) GROUP BY 1 over 2^21 rows (a projection as the group key)."""
+    import torch
+    import wadjet_b200 as wg
+    monkeypatch.setenv("WG_SPECIALIZE", spec)
+    rng = np.random.default_rng(2000)
+    n = 1 << 21
+    haddr = (np.int64(10 << 24) + rng.integers(0, 1 << 24, n)).astype(np.int64)
+    hbytes = np.round(rng.lognormal(8.0, 2.0, n)).astype(np.int64)
+    addr, nbytes = torch.from_numpy(haddr).cuda(), torch.from_numpy(hbytes).cuda()
+    g = wg.HashAggregate(ctx, [2], [wg.AggColumn(wg.AGG_SUM, 1), wg.AggColumn(wg.AGG_COUNT, -1)], ndv_hint=1 << 16)
+    expr = wg.Expr(I64, [wg.Expr.col(0), wg.Expr.const_i(8), ">>"])
+    wg.run_pipeline(ctx, wg.Batch([wg.Column(I64, addr), wg.Column(I64, nbytes)]), g, exprs=[expr], device=True)
+    assert g.kernel_shape == (6 if spec == "1" else 0)
+    g.finalize()
+    o = ob.Agg([2], [(0, 1, 0), (1, -1, 0)])
+    ob.pipeline(ob.HostBatch([(I64, haddr, None, 0), (I64, hbytes, None, 0)]), o,
+                exprs=[ob.expr(I64, [("col", 0), ("ci", 8), ">>"])], threads=4)
+    assert_groups_equal(g.export(), o.export(), ["sum_i", "count"])
+    g.close()

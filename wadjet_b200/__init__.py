@@ -342,6 +342,11 @@ class HashAggregate:
         self._n_groups = None
         self._out_pos = 0
 
+    @property
+    def kernel_shape(self) -> int:
+        """Compiled query shape of the last fused launch (0 generic, -1 none yet); a diagnostic only."""
+        return int(lib.wg_agg_kernel_shape(self.h))
+
     def export(self) -> dict:
         """Raw accumulator state of every group (keys widened to int64)."""
         n = self._n_groups if self._n_groups is not None else self.finalize()

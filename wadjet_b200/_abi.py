@@ -132,6 +132,7 @@ SIGNATURES = {
     "wg_agg_emit": (I32, [P, I64, I64, C.POINTER(wg_column), PI64]),
     "wg_agg_export": (I32, [P, C.POINTER(wg_group_export)]),
     "wg_agg_reset": (I32, [P]),
+    "wg_agg_kernel_shape": (I32, [P]),
     "wg_agg_destroy": (I32, [P]),
     "wg_pipeline_run": (I32, [P, C.POINTER(wg_pipeline_desc)]),
     "wg_pipeline_run_device": (I32, [P, C.POINTER(wg_pipeline_desc)]),

@@ -13,7 +13,7 @@
 //  - Low-cardinality int keys use a CTA-private shared-memory table flushed to
 //    the global table at the end of the kernel.
 #include "wg_internal.h"
-#include "wg_agg_kernels.cuh"
+#include "wg_shapes.cuh"
 
 #include <algorithm>
 #include <cstdlib>
@@ -65,11 +65,12 @@ __global__ void fold_kernel(Layout Ls, Table Ts, Layout Ld, Table Td, int32_t* e
       else if (i == cap) { k0 = Ls.key_words == 1 ? WG_EMPTY_KEY : ~0ULL; k1 = ~0ULL; }
       else { k0 = s[0]; if (Ls.key_words == 2) k1 = s[1]; }
     }
-    unsigned long long* d = find_global(Ld, Td, k0, k1, knull, err);
+    const LayoutAcc ls{Ls}, ld{Ld};
+    unsigned long long* d = find_global(ld, Td, k0, k1, knull, err);
     if (!d) continue;
     Contrib<NA> c;
-    slot_contrib<NA>(Ls, s, c);
-    apply<NA>(Ld, d, c, s[Ls.key_words]);
+    slot_contrib<NA>(ls, s, c);
+    apply<NA>(ld, d, c, s[Ls.key_words]);
   }
 }
 
@@ -249,6 +250,7 @@ struct wg_agg {
   int64_t n_out = 0;
   std::vector<wg::DevBuf> emit_bufs, emit_valid;
   bool emitted = false;
+  int32_t last_shape = -1;         // compiled shape of the last fused launch
 };
 
 namespace wg {
@@ -495,26 +497,56 @@ struct LaunchSpec {
   wgd::TileCfg cfg{};
 };
 
-template <int NA>
+template <int NA, class Sh>
 static void launch_pipeline_t(const LaunchSpec& ls, cudaStream_t st) {
+  const bool smem = Sh::smem_ok && ls.smem;
   if (ls.tile) {
-    const size_t dyn = (size_t)ls.cfg.table_off + (ls.smem ? (size_t)ls.P.smem_slots * ls.P.L.slot_words * 8 : 0);
+    const size_t dyn = (size_t)ls.cfg.table_off + (smem ? (size_t)ls.P.smem_slots * ls.P.L.slot_words * 8 : 0);
     const unsigned threads = 32u * (1u + (unsigned)ls.cfg.consumers);
-    if (ls.smem) {
-      cudaFuncSetAttribute(wgd::tile_pipeline_kernel<NA, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
-      wgd::tile_pipeline_kernel<NA, true><<<ls.grid, threads, dyn, st>>>(ls.P, ls.cfg);
-    } else {
-      cudaFuncSetAttribute(wgd::tile_pipeline_kernel<NA, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
-      wgd::tile_pipeline_kernel<NA, false><<<ls.grid, threads, dyn, st>>>(ls.P, ls.cfg);
+    if constexpr (Sh::smem_ok) {
+      if (smem) {
+        cudaFuncSetAttribute(wgd::tile_pipeline_kernel<NA, true, Sh>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)dyn);
+        wgd::tile_pipeline_kernel<NA, true, Sh><<<ls.grid, threads, dyn, st>>>(ls.P, ls.cfg);
+        return;
+      }
     }
+    cudaFuncSetAttribute(wgd::tile_pipeline_kernel<NA, false, Sh>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+    wgd::tile_pipeline_kernel<NA, false, Sh><<<ls.grid, threads, dyn, st>>>(ls.P, ls.cfg);
     return;
   }
-  if (ls.smem) {
-    cudaFuncSetAttribute(wgd::pipeline_kernel<NA, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ls.smem_bytes);
-    wgd::pipeline_kernel<NA, true><<<ls.grid, ls.block, ls.smem_bytes, st>>>(ls.P);
-  } else {
-    wgd::pipeline_kernel<NA, false><<<ls.grid, ls.block, 0, st>>>(ls.P);
+  if constexpr (Sh::smem_ok) {
+    if (smem) {
+      cudaFuncSetAttribute(wgd::pipeline_kernel<NA, true, Sh>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)ls.smem_bytes);
+      wgd::pipeline_kernel<NA, true, Sh><<<ls.grid, ls.block, ls.smem_bytes, st>>>(ls.P);
+      return;
+    }
   }
+  wgd::pipeline_kernel<NA, false, Sh><<<ls.grid, ls.block, 0, st>>>(ls.P);
+}
+
+// Launch on the compiled shape of the plan (ls.P.shape), or the generic kernel.
+static void launch_pipeline_shape(const LaunchSpec& ls, cudaStream_t st) {
+  using namespace wgd;
+  switch (ls.P.shape) {
+    case SHAPE_STARJOIN: launch_pipeline_t<ShapeStarJoin::n_aggs, StatShape<ShapeStarJoin>>(ls, st); return;
+    case SHAPE_GROUPBY: launch_pipeline_t<ShapeGroupBy::n_aggs, StatShape<ShapeGroupBy>>(ls, st); return;
+    case SHAPE_HIGHCARD: launch_pipeline_t<ShapeHighCard::n_aggs, StatShape<ShapeHighCard>>(ls, st); return;
+    case SHAPE_BATCH_I64: launch_pipeline_t<ShapeBatchI64::n_aggs, StatShape<ShapeBatchI64>>(ls, st); return;
+    case SHAPE_BATCH_F64: launch_pipeline_t<ShapeBatchF64::n_aggs, StatShape<ShapeBatchF64>>(ls, st); return;
+    case SHAPE_IPV4: launch_pipeline_t<ShapeIPv4::n_aggs, StatShape<ShapeIPv4>>(ls, st); return;
+    default: break;
+  }
+  if (ls.P.L.n_aggs <= 4) launch_pipeline_t<4, DynShape>(ls, st);
+  else launch_pipeline_t<8, DynShape>(ls, st);
+}
+
+// The compiled shape to launch a finished plan with; WG_SPECIALIZE=0 forces
+// the generic kernel.
+static int32_t pick_shape(const wgd::Plan& P) {
+  if (env_int("WG_SPECIALIZE", 1) == 0) return wgd::SHAPE_GENERIC;
+  return wgd::shape_of(P);
 }
 
 static wg_status launch_pipeline(wg_agg* a, const LaunchSpec& ls, int64_t n_items) {
@@ -529,8 +561,9 @@ static wg_status launch_pipeline(wg_agg* a, const LaunchSpec& ls, int64_t n_item
   P.L = L;
   P.n_items = n_items;
   if (l2.tile) l2.cfg.n_tiles = (n_items + l2.cfg.rows - 1) / l2.cfg.rows;
-  if (a->L.n_aggs <= 4) launch_pipeline_t<4>(l2, ctx->stream);
-  else launch_pipeline_t<8>(l2, ctx->stream);
+  P.shape = pick_shape(P);
+  a->last_shape = P.shape;
+  launch_pipeline_shape(l2, ctx->stream);
   ctx->count_launch();
   WG_CUDA_TRY(cudaGetLastError());
   return WG_OK;
@@ -1080,6 +1113,8 @@ wg_status wg_agg_reset(wg_agg* a) {
   return WG_OK;
 }
 
+int32_t wg_agg_kernel_shape(const wg_agg* a) { return a ? a->last_shape : -1; }
+
 wg_status wg_agg_destroy(wg_agg* a) {
   if (!a) return WG_OK;
   ensure_device(a->ctx);
@@ -1139,13 +1174,39 @@ __global__ void batched_count_kernel(const ResetDesc* rd, int n, long long* out)
   }
 }
 
+// One work item (a window of one query's rows) on shape Sh.
+template <int NA, class Sh>
+__device__ __forceinline__ void batched_item(const Plan& P, const BatchItem& w, unsigned long long* sm,
+                                             int* s_groups) {
+  const Sh sh{P};
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int S = P.smem_slots;
+  if (Sh::smem_ok && S > 0) {
+    smem_table_init(P.L, sm, S, s_groups);
+    __syncthreads();
+    const int s_limit = (S * 7) / 8;
+    for (int base = warp * 32; base < w.rows; base += nw * 32) {
+      const int i = base + lane;
+      SrcGlobal src{w.row0 + (i < w.rows ? i : 0)};
+      process_rows<NA, Sh::smem_ok>(P, sh, src, i < w.rows, sm, s_groups, s_limit);
+    }
+    __syncthreads();
+    smem_table_flush<NA>(P, sm, S);
+  } else {
+    for (int base = warp * 32; base < w.rows; base += nw * 32) {
+      const int i = base + lane;
+      SrcGlobal src{w.row0 + (i < w.rows ? i : 0)};
+      process_rows<NA, false>(P, sh, src, i < w.rows, sm, s_groups, 0);
+    }
+  }
+}
+
 template <int NA>
 __global__ void __launch_bounds__(512) batched_kernel(const Plan* plans, const BatchItem* items, int64_t n_items,
                                                       unsigned long long* cursor) {
   extern __shared__ unsigned long long sm[];
   __shared__ int s_groups;
   __shared__ long long s_item;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   for (;;) {
     if (threadIdx.x == 0) s_item = (long long)atomicAdd(cursor, 1ULL);
     __syncthreads();
@@ -1153,24 +1214,10 @@ __global__ void __launch_bounds__(512) batched_kernel(const Plan* plans, const B
     if (it >= n_items) break;
     const BatchItem w = items[it];
     const Plan& P = plans[w.q];
-    const int S = P.smem_slots;
-    if (S > 0) {
-      smem_table_init<NA>(P.L, sm, S, &s_groups);
-      __syncthreads();
-      const int s_limit = (S * 7) / 8;
-      for (int base = warp * 32; base < w.rows; base += nw * 32) {
-        const int i = base + lane;
-        SrcGlobal src{w.row0 + (i < w.rows ? i : 0)};
-        process_rows<NA, true>(P, src, i < w.rows, sm, &s_groups, s_limit);
-      }
-      __syncthreads();
-      smem_table_flush<NA>(P, sm, S);
-    } else {
-      for (int base = warp * 32; base < w.rows; base += nw * 32) {
-        const int i = base + lane;
-        SrcGlobal src{w.row0 + (i < w.rows ? i : 0)};
-        process_rows<NA, false>(P, src, i < w.rows, sm, &s_groups, 0);
-      }
+    switch (P.shape) {
+      case SHAPE_BATCH_I64: batched_item<ShapeBatchI64::n_aggs, StatShape<ShapeBatchI64>>(P, w, sm, &s_groups); break;
+      case SHAPE_BATCH_F64: batched_item<ShapeBatchF64::n_aggs, StatShape<ShapeBatchF64>>(P, w, sm, &s_groups); break;
+      default: batched_item<NA, DynShape>(P, w, sm, &s_groups); break;
     }
     __syncthreads();
   }
@@ -1231,6 +1278,9 @@ static wg_status batched_plan(wg_batched* b) {
       max_smem_words = std::max<int64_t>(max_smem_words, (int64_t)S * a->L.slot_words);
     }
     P.smem_slots = S;
+    P.shape = pick_shape(P);
+    if (P.shape != wgd::SHAPE_BATCH_I64 && P.shape != wgd::SHAPE_BATCH_F64) P.shape = wgd::SHAPE_GENERIC;
+    a->last_shape = P.shape;
     if (a->L.n_aggs > 4) b->max_na = 8;
     ResetDesc& rd = b->reset_h[q];
     rd.slots = a->table.as<unsigned long long>();

@@ -1,5 +1,14 @@
 // wg_agg_kernels.cuh — device code of the hash aggregate and the fused
 // filter → probe → project → aggregate kernel.
+//
+// Every decision about the query's shape (column types, filter operators, the
+// projection program, the slot layout, the aggregate kinds) goes through a
+// shape accessor. DynShape reads those facts from the launch plan at run time,
+// so one kernel serves any plan. StatShape<C> answers from the compile-time
+// constants of C: after unrolling, every switch on a type or kind folds away
+// and the kernel is straight-line code for that query shape. The host launches
+// a StatShape instantiation when the plan matches one exactly (shape_matches,
+// wg_shapes.cuh) and the DynShape one otherwise; results are identical.
 #pragma once
 
 #include "wg_agg.cuh"
@@ -12,17 +21,21 @@ struct Val {
   bool null;
 };
 
-__device__ __forceinline__ Val load_val(const DCol& c, int64_t i) {
+__device__ __forceinline__ double as_f(unsigned long long w) { return __longlong_as_double((long long)w); }
+__device__ __forceinline__ unsigned long long as_w(double d) { return (unsigned long long)__double_as_longlong(d); }
+
+// One value of storage class `cls` at element i of `data` (read-only path).
+__device__ __forceinline__ Val load_typed(const void* data, int cls, int64_t i) {
   Val v;
   v.hi = 0;
-  v.null = is_null(c, i);
-  switch (c.cls) {
-    case WG_CLS_I32: v.lo = (unsigned long long)(long long)__ldg((const int32_t*)c.data + i); break;
-    case WG_CLS_I64: v.lo = (unsigned long long)__ldg((const long long*)c.data + i); break;
-    case WG_CLS_F32: v.lo = (unsigned long long)__double_as_longlong((double)__ldg((const float*)c.data + i)); break;
-    case WG_CLS_F64: v.lo = (unsigned long long)__double_as_longlong(__ldg((const double*)c.data + i)); break;
+  v.null = false;
+  switch (cls) {
+    case WG_CLS_I32: v.lo = (unsigned long long)(long long)__ldg((const int32_t*)data + i); break;
+    case WG_CLS_I64: v.lo = (unsigned long long)__ldg((const long long*)data + i); break;
+    case WG_CLS_F32: v.lo = as_w((double)__ldg((const float*)data + i)); break;
+    case WG_CLS_F64: v.lo = (unsigned long long)__ldg((const long long*)data + i); break;
     case WG_CLS_DEC: {
-      const longlong2 d = __ldg((const longlong2*)c.data + i);
+      const longlong2 d = __ldg((const longlong2*)data + i);  // .x = hi, .y = lo
       v.lo = (unsigned long long)d.y;
       v.hi = (unsigned long long)d.x;
       break;
@@ -32,58 +45,180 @@ __device__ __forceinline__ Val load_val(const DCol& c, int64_t i) {
   return v;
 }
 
-// Row sources: where one row's input columns are read from. SrcGlobal reads
-// HBM directly; the tile kernel's source reads its TMA-staged shared-memory tile.
-struct SrcGlobal {
-  int64_t row;
-  __device__ __forceinline__ Val in(const Plan& P, int j) const { return load_val(P.in[j], row); }
+// The same from memory that may be shared (generic loads).
+__device__ __forceinline__ Val load_generic(const char* p, int cls) {
+  Val v;
+  v.hi = 0;
+  v.null = false;
+  switch (cls) {
+    case WG_CLS_I32: v.lo = (unsigned long long)(long long)*(const int32_t*)p; break;
+    case WG_CLS_I64: case WG_CLS_F64: v.lo = *(const unsigned long long*)p; break;
+    case WG_CLS_F32: v.lo = as_w((double)*(const float*)p); break;
+    case WG_CLS_DEC: v.hi = ((const unsigned long long*)p)[0]; v.lo = ((const unsigned long long*)p)[1]; break;
+    default: v.lo = 0;
+  }
+  return v;
+}
+
+__device__ __forceinline__ int cls_bytes(int cls) {
+  return cls == WG_CLS_I32 || cls == WG_CLS_F32 ? 4 : cls == WG_CLS_DEC ? 16 : 8;
+}
+
+// Identity of an accumulator word (the empty-slot value the layout starts from).
+__device__ __forceinline__ unsigned long long ident_word(int kind, int w) {
+  switch (kind) {
+    case K_MIN_I64: return 0x7FFFFFFFFFFFFFFFULL;
+    case K_MAX_I64: return 0x8000000000000000ULL;
+    case K_MIN_F64: return ~0ULL;
+    case K_MAX_F64: return 0ULL;
+    case K_MIN_DEC: return w == 0 ? ~0ULL : 0x7FFFFFFFFFFFFFFFULL;
+    case K_MAX_DEC: return w == 0 ? 0ULL : 0x8000000000000000ULL;
+    default: return 0ULL;
+  }
+}
+
+// ---- shape accessors --------------------------------------------------------
+
+// Layout facts of a table (folds, flushes, growth): always run time.
+struct LayoutAcc {
+  const Layout& L;
+  __device__ __forceinline__ int key_words() const { return L.key_words; }
+  __device__ __forceinline__ int slot_words() const { return L.slot_words; }
+  __device__ __forceinline__ int n_aggs() const { return L.n_aggs; }
+  __device__ __forceinline__ int agg_kind(int a) const { return L.agg[a].kind; }
+  __device__ __forceinline__ int agg_off(int a) const { return L.agg[a].off; }
+  __device__ __forceinline__ int agg_null_off(int a) const { return L.agg[a].null_off; }
 };
 
-template <class Src>
-__device__ __forceinline__ Val fetch_base(const Plan& P, const Src& src, int j, int32_t brow) {
-  if (j < P.n_in) return src.in(P, j);
-  if (P.join.direct) {  // brow already holds the payload's 32 bits
+// Everything from the plan at run time.
+struct DynShape {
+  static constexpr bool smem_ok = true;
+  const Plan& P;
+  __device__ __forceinline__ int n_in() const { return P.n_in; }
+  __device__ __forceinline__ int in_cls(int j) const { return P.in[j].cls; }
+  __device__ __forceinline__ int n_filters() const { return P.n_filters; }
+  __device__ __forceinline__ int filt_col(int f) const { return P.filt[f].col; }
+  __device__ __forceinline__ int filt_cls(int f) const { return P.filt[f].cls; }
+  __device__ __forceinline__ int filt_op(int f) const { return P.filt[f].op; }
+  __device__ __forceinline__ int has_join() const { return P.has_join; }
+  __device__ __forceinline__ int direct() const { return P.join.direct; }
+  __device__ __forceinline__ int probe_col() const { return P.probe_col; }
+  __device__ __forceinline__ int n_pay() const { return P.join.n_pay; }
+  __device__ __forceinline__ int pay_cls(int i) const { return P.join.pay[i].cls; }
+  __device__ __forceinline__ int n_exprs() const { return P.n_exprs; }
+  __device__ __forceinline__ int expr_nops(int e) const { return P.expr[e].n_ops; }
+  __device__ __forceinline__ int expr_opc(int e, int k) const { return P.expr[e].opc[k]; }
+  __device__ __forceinline__ int expr_arg(int e, int k) const { return P.expr[e].arg[k]; }
+  __device__ __forceinline__ int expr_cls(int e) const { return P.expr[e].result_cls; }
+  __device__ __forceinline__ int vcls(int j) const { return P.vcls[j]; }
+  __device__ __forceinline__ int key_words() const { return P.L.key_words; }
+  __device__ __forceinline__ int slot_words() const { return P.L.slot_words; }
+  __device__ __forceinline__ int n_keys() const { return P.L.n_keys; }
+  __device__ __forceinline__ int key_vcol(int k) const { return P.L.key_vcol[k]; }
+  __device__ __forceinline__ int key_i32(int k) const { return P.L.key_i32[k]; }
+  __device__ __forceinline__ int key_word(int k) const { return P.L.key_word[k]; }
+  __device__ __forceinline__ int key_shift(int k) const { return P.L.key_shift[k]; }
+  __device__ __forceinline__ int n_aggs() const { return P.L.n_aggs; }
+  __device__ __forceinline__ int agg_kind(int a) const { return P.L.agg[a].kind; }
+  __device__ __forceinline__ int agg_off(int a) const { return P.L.agg[a].off; }
+  __device__ __forceinline__ int agg_null_off(int a) const { return P.L.agg[a].null_off; }
+  __device__ __forceinline__ int agg_vcol(int a) const { return P.L.agg[a].vcol; }
+};
+
+// Everything from compile-time constants (see wg_shapes.cuh for the C structs).
+template <class C>
+struct StatShape {
+  static constexpr bool smem_ok = C::smem_ok;
+  const Plan& P;
+  __device__ __forceinline__ constexpr int n_in() const { return C::n_in; }
+  __device__ __forceinline__ constexpr int in_cls(int j) const { return C::in_cls(j); }
+  __device__ __forceinline__ constexpr int n_filters() const { return C::n_filters; }
+  __device__ __forceinline__ constexpr int filt_col(int f) const { return C::filt_col(f); }
+  __device__ __forceinline__ constexpr int filt_cls(int f) const { return C::filt_cls(f); }
+  __device__ __forceinline__ constexpr int filt_op(int f) const { return C::filt_op(f); }
+  __device__ __forceinline__ constexpr int has_join() const { return C::has_join; }
+  __device__ __forceinline__ constexpr int direct() const { return C::direct; }
+  __device__ __forceinline__ constexpr int probe_col() const { return C::probe_col; }
+  __device__ __forceinline__ constexpr int n_pay() const { return C::n_pay; }
+  __device__ __forceinline__ constexpr int pay_cls(int i) const { return C::pay_cls(i); }
+  __device__ __forceinline__ constexpr int n_exprs() const { return C::n_exprs; }
+  __device__ __forceinline__ constexpr int expr_nops(int e) const { return C::expr_nops(e, 0); }
+  __device__ __forceinline__ constexpr int expr_opc(int e, int k) const { return C::expr_opc(e, k); }
+  __device__ __forceinline__ constexpr int expr_arg(int e, int k) const { return C::expr_arg(e, k); }
+  __device__ __forceinline__ constexpr int expr_cls(int e) const { return C::expr_cls(e); }
+  __device__ __forceinline__ constexpr int vcls(int j) const { return C::vcls(j); }
+  __device__ __forceinline__ constexpr int key_words() const { return C::key_words; }
+  __device__ __forceinline__ constexpr int slot_words() const { return C::slot_words; }
+  __device__ __forceinline__ constexpr int n_keys() const { return C::n_keys; }
+  __device__ __forceinline__ constexpr int key_vcol(int k) const { return C::key_vcol(k); }
+  __device__ __forceinline__ constexpr int key_i32(int k) const { return C::key_i32(k); }
+  __device__ __forceinline__ constexpr int key_word(int k) const { return C::key_word(k); }
+  __device__ __forceinline__ constexpr int key_shift(int k) const { return C::key_shift(k); }
+  __device__ __forceinline__ constexpr int n_aggs() const { return C::n_aggs; }
+  __device__ __forceinline__ constexpr int agg_kind(int a) const { return C::agg_kind(a); }
+  __device__ __forceinline__ constexpr int agg_off(int a) const { return C::agg_off(a); }
+  __device__ __forceinline__ constexpr int agg_null_off(int a) const { return C::agg_null_off(a); }
+  __device__ __forceinline__ constexpr int agg_vcol(int a) const { return C::agg_vcol(a); }
+};
+
+// ---- row sources --------------------------------------------------------------
+
+// Input column j of one row, straight from HBM.
+struct SrcGlobal {
+  int64_t row;
+  template <class Sh>
+  __device__ __forceinline__ Val in(const Plan& P, const Sh& sh, int j) const {
+    Val v = load_typed(P.in[j].data, sh.in_cls(j), row);
+    v.null = is_null(P.in[j], row);
+    return v;
+  }
+};
+
+template <class Sh, class Src>
+__device__ __forceinline__ Val fetch_base(const Plan& P, const Sh& sh, const Src& src, int j, int32_t brow) {
+  if (j < sh.n_in()) return src.in(P, sh, j);
+  if (sh.direct()) {  // brow already holds the payload's 32 bits
     Val v;
     v.hi = 0;
     v.null = false;
-    v.lo = P.join.pay[0].cls == WG_CLS_F32
-               ? (unsigned long long)__double_as_longlong((double)__int_as_float(brow))
-               : (unsigned long long)(long long)brow;
+    v.lo = sh.pay_cls(0) == WG_CLS_F32 ? as_w((double)__int_as_float(brow)) : (unsigned long long)(long long)brow;
     return v;
   }
-  return load_val(P.join.pay[j - P.n_in], brow);
+  const int p = j - sh.n_in();
+  Val v = load_typed(P.join.pay[p].data, sh.pay_cls(p), brow);
+  v.null = is_null(P.join.pay[p], brow);
+  return v;
 }
-
-__device__ __forceinline__ double as_f(unsigned long long w) { return __longlong_as_double((long long)w); }
-__device__ __forceinline__ unsigned long long as_w(double d) { return (unsigned long long)__double_as_longlong(d); }
 
 // Postfix evaluation of a projection (expr.BinOpNumeric): integer ops wrap,
 // float ops are single IEEE operations (no contraction), DECIMAL operands read
 // as Int128.ToFloat64, a NULL operand makes the result NULL. The four-entry
-// stack is addressed through selects so it stays in registers.
-template <class Src>
-__device__ __forceinline__ Val eval_expr(const Plan& P, const ExprD& e, const Src& src, int32_t brow) {
+// stack is addressed through selects so it stays in registers (and, for a
+// static shape, folds to straight-line code).
+template <class Sh, class Src>
+__device__ __forceinline__ Val eval_expr(const Plan& P, const Sh& sh, int e, const Src& src, int32_t brow) {
   unsigned long long s0 = 0, s1 = 0, s2 = 0, s3 = 0;
   unsigned fl = 0;  // bit i: stack entry i holds a float
   int sp = 0;
   bool null = false;
+#pragma unroll
   for (int k = 0; k < WG_EXPR_OPS; ++k) {
-    if (k >= e.n_ops) break;
-    const int opc = e.opc[k];
+    if (k >= sh.expr_nops(e)) break;
+    const int opc = sh.expr_opc(e, k);
     unsigned long long w = 0;
     bool isf = false;
     if (opc == 0) {  // WG_EXPR_COL
-      const int j = e.arg[k];
-      Val v = fetch_base(P, src, j, brow);
+      const int j = sh.expr_arg(e, k);
+      Val v = fetch_base(P, sh, src, j, brow);
       null |= v.null;
-      const int cls = P.vcls[j];
+      const int cls = sh.vcls(j);
       if (cls == WG_CLS_I32 || cls == WG_CLS_I64) { w = v.lo; isf = false; }
       else if (cls == WG_CLS_DEC) { w = as_w(dec_to_f64((int64_t)v.hi, v.lo, P.vscale[j])); isf = true; }
       else { w = v.lo; isf = true; }
     } else if (opc == 1) {
-      w = (unsigned long long)e.imm[k]; isf = false;
+      w = (unsigned long long)P.expr[e].imm[k]; isf = false;
     } else if (opc == 2) {
-      w = (unsigned long long)e.imm[k]; isf = true;
+      w = (unsigned long long)P.expr[e].imm[k]; isf = true;
     } else {
       if (sp < 2) { set_error(P.err, WG_DERR_STACK); Val r; r.lo = 0; r.hi = 0; r.null = true; return r; }
       const unsigned long long b = sp == 1 ? s0 : sp == 2 ? s1 : sp == 3 ? s2 : s3;
@@ -120,16 +255,32 @@ __device__ __forceinline__ Val eval_expr(const Plan& P, const ExprD& e, const Sr
   r.null = null;
   const unsigned long long top = sp == 1 ? s0 : sp == 2 ? s1 : sp == 3 ? s2 : s3;
   const bool tf = sp > 0 && ((fl >> (sp - 1)) & 1);
-  if (e.result_cls == WG_CLS_F64 && !tf) r.lo = as_w(__ll2double_rn((long long)top));
+  if (sh.expr_cls(e) == WG_CLS_F64 && !tf) r.lo = as_w(__ll2double_rn((long long)top));
   else r.lo = top;
   return r;
 }
 
-template <class Src>
-__device__ __forceinline__ Val fetch(const Plan& P, const Src& src, int j, int32_t brow) {
-  const int nb = P.n_in + P.join.n_pay;
-  if (j < nb) return fetch_base(P, src, j, brow);
-  return eval_expr(P, P.expr[j - nb], src, brow);
+// The projected columns of one (row, build row), evaluated once and then read
+// by every key and aggregate that refers to them.
+struct ExprVals {
+  Val v[WG_MAX_EXPRS];
+};
+
+template <class Sh, class Src>
+__device__ __forceinline__ void eval_exprs(const Plan& P, const Sh& sh, const Src& src, int32_t brow, ExprVals& ev) {
+#pragma unroll
+  for (int e = 0; e < WG_MAX_EXPRS; ++e) {
+    if (e < sh.n_exprs()) ev.v[e] = eval_expr(P, sh, e, src, brow);
+    else { ev.v[e].lo = 0; ev.v[e].hi = 0; ev.v[e].null = true; }
+  }
+}
+
+template <class Sh, class Src>
+__device__ __forceinline__ Val fetch(const Plan& P, const Sh& sh, const Src& src, int j, int32_t brow,
+                                     const ExprVals& ev) {
+  const int nb = sh.n_in() + (sh.has_join() ? sh.n_pay() : 0);
+  if (j < nb) return fetch_base(P, sh, src, j, brow);
+  return j == nb ? ev.v[0] : ev.v[1];
 }
 
 template <int NA>
@@ -140,27 +291,27 @@ struct Contrib {
 
 // One row's contribution to each aggregate (the scatter kernels' per-row
 // update, internal/engine/exec/agg_scatter.go:178-510), as combinable words.
-template <int NA, class Src>
-__device__ __forceinline__ void make_contrib(const Plan& P, const Src& src, int32_t brow, Contrib<NA>& c) {
-  const Layout& L = P.L;
+template <int NA, class Sh, class Src>
+__device__ __forceinline__ void make_contrib(const Plan& P, const Sh& sh, const Src& src, int32_t brow,
+                                             const ExprVals& ev, Contrib<NA>& c) {
 #pragma unroll
   for (int a = 0; a < NA; ++a) {
     c.w0[a] = 0; c.w1[a] = 0; c.nul[a] = 0;
-    if (a >= L.n_aggs) continue;
-    const AggD g = L.agg[a];
-    if (g.vcol < 0 || g.kind == K_COUNT) {
-      if (g.vcol >= 0) c.nul[a] = fetch(P, src, g.vcol, brow).null ? 1 : 0;
+    if (a >= sh.n_aggs()) continue;
+    const int kind = sh.agg_kind(a), vcol = sh.agg_vcol(a);
+    if (vcol < 0 || kind == K_COUNT) {
+      if (vcol >= 0) c.nul[a] = fetch(P, sh, src, vcol, brow, ev).null ? 1 : 0;
       continue;
     }
-    const Val v = fetch(P, src, g.vcol, brow);
+    const Val v = fetch(P, sh, src, vcol, brow, ev);
     if (v.null) {
       c.nul[a] = 1;
-      c.w0[a] = L.init[g.off];
-      if (kind_words(g.kind) == 2) c.w1[a] = L.init[g.off + 1];
+      c.w0[a] = ident_word(kind, 0);
+      c.w1[a] = ident_word(kind, 1);
       continue;
     }
-    const int cls = P.vcls[g.vcol];
-    switch (g.kind) {
+    const int cls = sh.vcls(vcol);
+    switch (kind) {
       case K_SUM_I64: case K_MIN_I64: case K_MAX_I64: c.w0[a] = v.lo; break;
       case K_SUM_F64:
         c.w0[a] = (cls == WG_CLS_I32 || cls == WG_CLS_I64) ? as_w(__ll2double_rn((long long)v.lo)) : v.lo;
@@ -188,54 +339,55 @@ __device__ __forceinline__ void combine(int kind, unsigned long long& a0, unsign
 }
 
 // Fold a combined contribution into a slot (HBM or shared memory) with atomics.
-template <int NA>
-__device__ __forceinline__ void apply(const Layout& L, unsigned long long* s, const Contrib<NA>& c,
+template <int NA, class Lay>
+__device__ __forceinline__ void apply(const Lay& ly, unsigned long long* s, const Contrib<NA>& c,
                                       unsigned long long rows) {
-  atomicAdd(s + L.key_words, rows);
+  atomicAdd(s + ly.key_words(), rows);
 #pragma unroll
   for (int a = 0; a < NA; ++a) {
-    if (a >= L.n_aggs) continue;
-    const AggD g = L.agg[a];
+    if (a >= ly.n_aggs()) continue;
+    const int kind = ly.agg_kind(a), off = ly.agg_off(a), noff = ly.agg_null_off(a);
     const unsigned long long w0 = c.w0[a], w1 = c.w1[a];
-    switch (g.kind) {
-      case K_SUM_I64: if (w0) atomicAdd(s + g.off, w0); break;
-      case K_SUM_F64: { const double d = as_f(w0); if (d != 0.0) atomicAdd((double*)(s + g.off), d); } break;
-      case K_SUM_DEC: atomic_add128(s + g.off, w0, w1); break;
-      case K_MIN_I64: if (w0 != 0x7FFFFFFFFFFFFFFFULL) atomicMin((long long*)(s + g.off), (long long)w0); break;
-      case K_MAX_I64: if (w0 != 0x8000000000000000ULL) atomicMax((long long*)(s + g.off), (long long)w0); break;
-      case K_MIN_F64: if (w0 != ~0ULL) atomicMin(s + g.off, w0); break;
-      case K_MAX_F64: if (w0 != 0ULL) atomicMax(s + g.off, w0); break;
-      case K_MIN_DEC: atomic_min128((U128*)(s + g.off), w0, w1); break;
-      case K_MAX_DEC: atomic_max128((U128*)(s + g.off), w0, w1); break;
+    switch (kind) {
+      case K_SUM_I64: if (w0) atomicAdd(s + off, w0); break;
+      case K_SUM_F64: { const double d = as_f(w0); if (d != 0.0) atomicAdd((double*)(s + off), d); } break;
+      case K_SUM_DEC: atomic_add128(s + off, w0, w1); break;
+      case K_MIN_I64: if (w0 != 0x7FFFFFFFFFFFFFFFULL) atomicMin((long long*)(s + off), (long long)w0); break;
+      case K_MAX_I64: if (w0 != 0x8000000000000000ULL) atomicMax((long long*)(s + off), (long long)w0); break;
+      case K_MIN_F64: if (w0 != ~0ULL) atomicMin(s + off, w0); break;
+      case K_MAX_F64: if (w0 != 0ULL) atomicMax(s + off, w0); break;
+      case K_MIN_DEC: atomic_min128((U128*)(s + off), w0, w1); break;
+      case K_MAX_DEC: atomic_max128((U128*)(s + off), w0, w1); break;
       default: break;
     }
-    if (g.null_off >= 0 && c.nul[a]) atomicAdd(s + g.null_off, (unsigned long long)c.nul[a]);
+    if (noff >= 0 && c.nul[a]) atomicAdd(s + noff, (unsigned long long)c.nul[a]);
   }
 }
 
 // Contribution held by a whole slot (shared-memory flush, merge, migration).
-template <int NA>
-__device__ __forceinline__ void slot_contrib(const Layout& L, const unsigned long long* s, Contrib<NA>& c) {
+template <int NA, class Lay>
+__device__ __forceinline__ void slot_contrib(const Lay& ly, const unsigned long long* s, Contrib<NA>& c) {
 #pragma unroll
   for (int a = 0; a < NA; ++a) {
     c.w0[a] = 0; c.w1[a] = 0; c.nul[a] = 0;
-    if (a >= L.n_aggs) continue;
-    const AggD g = L.agg[a];
-    if (g.off >= 0) { c.w0[a] = s[g.off]; if (kind_words(g.kind) == 2) c.w1[a] = s[g.off + 1]; }
-    if (g.null_off >= 0) c.nul[a] = (int)s[g.null_off];
+    if (a >= ly.n_aggs()) continue;
+    const int off = ly.agg_off(a), noff = ly.agg_null_off(a);
+    if (off >= 0) { c.w0[a] = s[off]; if (kind_words(ly.agg_kind(a)) == 2) c.w1[a] = s[off + 1]; }
+    if (noff >= 0) c.nul[a] = (int)s[noff];
   }
 }
 
 // Find or insert the global slot of a key. Inserting claims a group
 // reservation first; past T.limit the insert is refused and the overflow flag
 // raised (the host then replays the launch on a larger table).
-__device__ __forceinline__ unsigned long long* find_global(const Layout& L, const Table& T, unsigned long long k0,
+template <class Lay>
+__device__ __forceinline__ unsigned long long* find_global(const Lay& ly, const Table& T, unsigned long long k0,
                                                            unsigned long long k1, bool keynull, int32_t* err) {
-  const int sw = L.slot_words;
-  if (L.key_words == 0) return T.slots;
+  const int sw = ly.slot_words();
+  if (ly.key_words() == 0) return T.slots;
   const uint64_t cap = T.mask + 1;
   if (keynull) return T.slots + (cap + 1) * sw;
-  if (L.key_words == 1) {
+  if (ly.key_words() == 1) {
     if (k0 == WG_EMPTY_KEY) return T.slots + cap * sw;
     uint64_t h = fib_slot(k0, T.shift);
     for (uint64_t probe = 0; probe <= T.mask; ++probe) {
@@ -312,16 +464,15 @@ __device__ __forceinline__ unsigned long long* find_smem(unsigned long long* sm,
 // Warp-cooperative update: lanes holding the same key pre-combine their
 // contributions (__match_any_sync) and only the group's lowest lane touches the
 // table, so hot keys cost one set of atomics per warp instead of one per row.
-template <int NA, bool SMEM>
-__device__ __forceinline__ void warp_update(const Plan& P, bool cur, unsigned long long k0, unsigned long long k1,
-                                            bool knull, Contrib<NA>& c, unsigned long long* sm, int* s_groups,
-                                            int s_limit) {
-  const Layout& L = P.L;
+template <int NA, bool SMEM, class Sh>
+__device__ __forceinline__ void warp_update(const Plan& P, const Sh& sh, bool cur, unsigned long long k0,
+                                            unsigned long long k1, bool knull, Contrib<NA>& c,
+                                            unsigned long long* sm, int* s_groups, int s_limit) {
   const unsigned am = __ballot_sync(WG_FULL_MASK, cur);
   if (am == 0) return;
   const int lane = threadIdx.x & 31;
   unsigned peers = __match_any_sync(WG_FULL_MASK, k0);
-  if (L.key_words == 2) peers &= __match_any_sync(WG_FULL_MASK, k1);
+  if (sh.key_words() == 2) peers &= __match_any_sync(WG_FULL_MASK, k1);
   peers &= __match_any_sync(WG_FULL_MASK, knull ? 1u : 0u);
   peers &= am;
   const int mysz = cur ? __popc(peers) : 0;
@@ -332,79 +483,84 @@ __device__ __forceinline__ void warp_update(const Plan& P, bool cur, unsigned lo
     const int src = take ? (int)__fns(peers, 0, i + 1) : lane;
 #pragma unroll
     for (int a = 0; a < NA; ++a) {
-      if (a >= L.n_aggs) continue;
-      const AggD g = L.agg[a];
-      const int kw = kind_words(g.kind);
+      if (a >= sh.n_aggs()) continue;
+      const int kind = sh.agg_kind(a);
+      const int kw = kind_words(kind);
       unsigned long long b0 = 0, b1 = 0;
       int bn = 0;
       if (kw >= 1) b0 = __shfl_sync(WG_FULL_MASK, c.w0[a], src);
       if (kw == 2) b1 = __shfl_sync(WG_FULL_MASK, c.w1[a], src);
-      if (g.null_off >= 0) bn = __shfl_sync(WG_FULL_MASK, c.nul[a], src);
+      if (sh.agg_null_off(a) >= 0) bn = __shfl_sync(WG_FULL_MASK, c.nul[a], src);
       if (take) {
-        combine(g.kind, c.w0[a], c.w1[a], b0, b1);
+        combine(kind, c.w0[a], c.w1[a], b0, b1);
         c.nul[a] += bn;
       }
     }
   }
   if (leader) {
     unsigned long long* s = nullptr;
-    if (SMEM && !knull) s = find_smem(sm, P.smem_slots, L.slot_words, k0, s_groups, s_limit);
-    if (s == nullptr) s = find_global(L, P.T, k0, k1, knull, P.err);
-    if (s != nullptr) apply<NA>(L, s, c, (unsigned long long)mysz);
+    if (SMEM && !knull) s = find_smem(sm, P.smem_slots, sh.slot_words(), k0, s_groups, s_limit);
+    if (s == nullptr) s = find_global(sh, P.T, k0, k1, knull, P.err);
+    if (s != nullptr) apply<NA>(sh, s, c, (unsigned long long)mysz);
   }
 }
 
 // Group key of one (row, build row): the int-key path widens to int64
 // (consumeBatchIntGroup, aggregate.go:1908); the packed path places each column
 // by buildPackedLayout (packed_hash.go:386) as packedKeyAt does (:456).
-template <class Src>
-__device__ __forceinline__ bool make_key(const Plan& P, const Src& src, int32_t brow, unsigned long long& k0,
-                                         unsigned long long& k1, bool& knull) {
-  const Layout& L = P.L;
+template <class Sh, class Src>
+__device__ __forceinline__ bool make_key(const Plan& P, const Sh& sh, const Src& src, int32_t brow,
+                                         const ExprVals& ev, unsigned long long& k0, unsigned long long& k1,
+                                         bool& knull) {
   k0 = 0; k1 = 0; knull = false;
-  if (L.key_words == 0) return true;
-  if (L.key_words == 1) {
-    Val v = fetch(P, src, L.key_vcol[0], brow);
+  if (sh.key_words() == 0) return true;
+  if (sh.key_words() == 1) {
+    Val v = fetch(P, sh, src, sh.key_vcol(0), brow, ev);
     knull = v.null;
     k0 = v.null ? 0 : v.lo;
     return true;
   }
+#pragma unroll
   for (int k = 0; k < WG_MAX_KEYS; ++k) {
-    if (k >= L.n_keys) break;
-    Val v = fetch(P, src, L.key_vcol[k], brow);
+    if (k >= sh.n_keys()) break;
+    Val v = fetch(P, sh, src, sh.key_vcol(k), brow, ev);
     if (v.null) { set_error(P.err, WG_DERR_NULL_PACKED); return false; }
-    const unsigned long long w = L.key_i32[k] ? ((unsigned long long)(uint32_t)(int32_t)v.lo) << L.key_shift[k] : v.lo;
-    if (L.key_word[k] == 0) k0 |= w; else k1 |= w;
+    const unsigned long long w =
+        sh.key_i32(k) ? ((unsigned long long)(uint32_t)(int32_t)v.lo) << sh.key_shift(k) : v.lo;
+    if (sh.key_word(k) == 0) k0 |= w; else k1 |= w;
   }
   return true;
 }
 
 // `col OP const` on an already loaded value (compareFilterImpl, compare.go:47).
-__device__ __forceinline__ bool pred_val(const Pred& p, const Val& v) {
+template <class Sh>
+__device__ __forceinline__ bool pred_val(const Plan& P, const Sh& sh, int f, const Val& v) {
   if (v.null) return false;
-  switch (p.cls) {
-    case WG_CLS_I32: return cmp_op<int32_t>((int32_t)(long long)v.lo, (int32_t)p.ci, p.op);
-    case WG_CLS_I64: return cmp_op<long long>((long long)v.lo, p.ci, p.op);
-    case WG_CLS_F32: return cmp_op<double>(as_f(v.lo), (double)(float)p.cf, p.op);  // both exact in binary64
-    case WG_CLS_F64: return cmp_op<double>(as_f(v.lo), p.cf, p.op);
+  const int op = sh.filt_op(f);
+  switch (sh.filt_cls(f)) {
+    case WG_CLS_I32: return cmp_op<int32_t>((int32_t)(long long)v.lo, (int32_t)P.filt[f].ci, op);
+    case WG_CLS_I64: return cmp_op<long long>((long long)v.lo, P.filt[f].ci, op);
+    case WG_CLS_F32: return cmp_op<double>(as_f(v.lo), (double)(float)P.filt[f].cf, op);  // both exact in binary64
+    case WG_CLS_F64: return cmp_op<double>(as_f(v.lo), P.filt[f].cf, op);
     default: return false;
   }
 }
 
 // One row per lane of a warp: KernelFilter chain → HashJoinProbe → Project →
 // HashAggregate.Consume. All 32 lanes call it together (act = row present).
-template <int NA, bool SMEM, class Src>
-__device__ __forceinline__ void process_rows(const Plan& P, const Src& src, bool act, unsigned long long* sm,
-                                             int* s_groups, int s_limit) {
+template <int NA, bool SMEM, class Sh, class Src>
+__device__ __forceinline__ void process_rows(const Plan& P, const Sh& sh, const Src& src, bool act,
+                                             unsigned long long* sm, int* s_groups, int s_limit) {
+#pragma unroll
   for (int f = 0; f < WG_MAX_FILTERS; ++f) {
-    if (f >= P.n_filters) break;
-    if (act) act = pred_val(P.filt[f], src.in(P, P.filt[f].col));
+    if (f >= sh.n_filters()) break;
+    if (act) act = pred_val(P, sh, f, src.in(P, sh, sh.filt_col(f)));
   }
   int32_t brow = -1;
-  if (P.has_join && act) {
-    const Val kv = src.in(P, P.probe_col);
+  if (sh.has_join() && act) {
+    const Val kv = src.in(P, sh, sh.probe_col());
     if (kv.null) act = false;
-    else if (P.join.direct) act = join_direct(P.join, (int64_t)kv.lo, brow, P.err);
+    else if (sh.direct()) act = join_direct(P.join, (int64_t)kv.lo, brow, P.err);
     else {
       brow = join_head(P.join, (int64_t)kv.lo, P.err);
       act = brow >= 0;
@@ -417,22 +573,23 @@ __device__ __forceinline__ void process_rows(const Plan& P, const Src& src, bool
     Contrib<NA> c;
     bool cur = act;
     if (cur) {
-      cur = make_key(P, src, brow, k0, k1, knull);
-      make_contrib<NA>(P, src, brow, c);
+      ExprVals ev;
+      eval_exprs(P, sh, src, brow, ev);
+      cur = make_key(P, sh, src, brow, ev, k0, k1, knull);
+      make_contrib<NA>(P, sh, src, brow, ev, c);
     } else {
 #pragma unroll
       for (int a = 0; a < NA; ++a) { c.w0[a] = 0; c.w1[a] = 0; c.nul[a] = 0; }
     }
-    warp_update<NA, SMEM>(P, cur, k0, k1, knull, c, sm, s_groups, s_limit);
-    if (!P.has_join || P.join.direct) break;  // unique keys: at most one match
+    warp_update<NA, SMEM>(P, sh, cur, k0, k1, knull, c, sm, s_groups, s_limit);
+    if (!sh.has_join() || sh.direct()) break;  // unique keys: at most one match
     if (act) {
-      brow = __ldg(P.join.next + brow);       // arenaNext chain (join.go:2700)
+      brow = __ldg(P.join.next + brow);         // arenaNext chain (join.go:2700)
       act = brow >= 0;
     }
   }
 }
 
-template <int NA>
 __device__ __forceinline__ void smem_table_init(const Layout& L, unsigned long long* sm, int S, int* s_groups) {
   const int sw = L.slot_words;
   for (int i = threadIdx.x; i < S * sw; i += blockDim.x) sm[i] = L.init[i % sw];
@@ -441,29 +598,30 @@ __device__ __forceinline__ void smem_table_init(const Layout& L, unsigned long l
 
 template <int NA>
 __device__ __forceinline__ void smem_table_flush(const Plan& P, const unsigned long long* sm, int S) {
-  const Layout& L = P.L;
-  const int sw = L.slot_words;
+  const LayoutAcc ly{P.L};
+  const int sw = P.L.slot_words;
   for (int i = threadIdx.x; i < S; i += blockDim.x) {
     const unsigned long long* s = sm + (size_t)i * sw;
     if (s[0] == WG_EMPTY_KEY) continue;
-    unsigned long long* g = find_global(L, P.T, s[0], 0, false, P.err);
+    unsigned long long* g = find_global(ly, P.T, s[0], 0, false, P.err);
     if (g == nullptr) continue;
     Contrib<NA> c;
-    slot_contrib<NA>(L, s, c);
-    apply<NA>(L, g, c, s[L.key_words]);
+    slot_contrib<NA>(ly, s, c);
+    apply<NA>(ly, g, c, s[P.L.key_words]);
   }
 }
 
 // The fused pipeline reading HBM directly: one warp per 32 consecutive rows
 // (or selection-vector entries), grid-stride.
-template <int NA, bool SMEM>
+template <int NA, bool SMEM, class Sh>
 __global__ void __launch_bounds__(512) pipeline_kernel(const __grid_constant__ Plan P) {
   extern __shared__ unsigned long long sm[];
   __shared__ int s_groups;
+  const Sh sh{P};
   const int S = P.smem_slots;
   const int s_limit = (S * 7) / 8;
   if (SMEM) {
-    smem_table_init<NA>(P.L, sm, S, &s_groups);
+    smem_table_init(P.L, sm, S, &s_groups);
     __syncthreads();
   }
   const int lane = threadIdx.x & 31;
@@ -474,7 +632,7 @@ __global__ void __launch_bounds__(512) pipeline_kernel(const __grid_constant__ P
     const int64_t item = base + lane;
     const bool act = item < P.n_items;
     SrcGlobal src{act ? (P.sel ? (int64_t)__ldg(P.sel + item) : item) : 0};
-    process_rows<NA, SMEM>(P, src, act, sm, &s_groups, s_limit);
+    process_rows<NA, SMEM>(P, sh, src, act, sm, &s_groups, s_limit);
   }
   if (SMEM) {
     __syncthreads();
@@ -508,28 +666,21 @@ struct SrcTile {
   int32_t i;
   int32_t m;
   const TileCfg* C;
-  __device__ __forceinline__ Val in(const Plan& P, int j) const {
+  template <class Sh>
+  __device__ __forceinline__ Val in(const Plan& P, const Sh& sh, int j) const {
     const DCol& c = P.in[j];
-    const int es = C->es[j];
+    const int cls = sh.in_cls(j);
+    const int es = cls_bytes(cls);
     const int staged = ((m * es) & ~15) / es;
     const int64_t row = row0 + i;
     const char* p = i < staged ? stage + C->col_off[j] + (size_t)i * es : (const char*)c.data + row * es;
-    Val v;
-    v.hi = 0;
+    Val v = load_generic(p, cls);
     v.null = is_null(c, row);
-    switch (c.cls) {
-      case WG_CLS_I32: v.lo = (unsigned long long)(long long)*(const int32_t*)p; break;
-      case WG_CLS_I64: v.lo = *(const unsigned long long*)p; break;
-      case WG_CLS_F32: v.lo = (unsigned long long)__double_as_longlong((double)*(const float*)p); break;
-      case WG_CLS_F64: v.lo = *(const unsigned long long*)p; break;
-      case WG_CLS_DEC: v.hi = ((const unsigned long long*)p)[0]; v.lo = ((const unsigned long long*)p)[1]; break;
-      default: v.lo = 0;
-    }
     return v;
   }
 };
 
-template <int NA, bool SMEM>
+template <int NA, bool SMEM, class Sh>
 __global__ void __launch_bounds__(544, 1) tile_pipeline_kernel(const __grid_constant__ Plan P,
                                                                const __grid_constant__ TileCfg C) {
   extern __shared__ __align__(128) unsigned char tsm[];
@@ -538,6 +689,7 @@ __global__ void __launch_bounds__(544, 1) tile_pipeline_kernel(const __grid_cons
   unsigned long long* full = bars;
   unsigned long long* empty = bars + 8;
   unsigned long long* table = (unsigned long long*)(tsm + C.table_off);
+  const Sh sh{P};
   const int S = P.smem_slots;
   const int s_limit = (S * 7) / 8;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -548,17 +700,16 @@ __global__ void __launch_bounds__(544, 1) tile_pipeline_kernel(const __grid_cons
     }
     mbar_init_fence();
   }
-  if (SMEM) smem_table_init<NA>(P.L, table, S, &s_groups);
+  if (SMEM) smem_table_init(P.L, table, S, &s_groups);
   __syncthreads();
 
   if (warp == 0) {
     // producer: one lane issues every copy
     if (lane == 0) {
       int64_t it = 0;
-      bool ok = true;
       for (int64_t tile = blockIdx.x; tile < C.n_tiles; tile += gridDim.x, ++it) {
         const int s = (int)(it % C.stages);
-        if (it >= C.stages && !mbar_wait(&empty[s], (uint32_t)(((it / C.stages) - 1) & 1), P.err)) { ok = false; break; }
+        if (it >= C.stages && !mbar_wait(&empty[s], (uint32_t)(((it / C.stages) - 1) & 1), P.err)) break;
         const int64_t row0 = tile * C.rows;
         const int m = (int)min((int64_t)C.rows, P.n_items - row0);
         uint32_t total = 0;
@@ -574,7 +725,6 @@ __global__ void __launch_bounds__(544, 1) tile_pipeline_kernel(const __grid_cons
       const int64_t issued = it;
       for (int64_t k = issued > C.stages ? issued - C.stages : 0; k < issued; ++k)
         mbar_wait(&full[k % C.stages], (uint32_t)((k / C.stages) & 1), P.err);
-      (void)ok;
     }
   } else {
     const int cw = warp - 1;
@@ -588,7 +738,7 @@ __global__ void __launch_bounds__(544, 1) tile_pipeline_kernel(const __grid_cons
       for (int base = cw * 32; base < m; base += C.consumers * 32) {
         const int i = base + lane;
         SrcTile src{(const char*)st, row0, i < m ? i : 0, m, &C};
-        process_rows<NA, SMEM>(P, src, i < m, table, &s_groups, s_limit);
+        process_rows<NA, SMEM>(P, sh, src, i < m, table, &s_groups, s_limit);
       }
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[s]);
