@@ -20,17 +20,22 @@ def canonical_order(exp: dict) -> np.ndarray:
     return np.lexsort(cols)
 
 
-def assert_groups_equal(got: dict, want: dict, kinds: list[str], rel: float = FLOAT_REL_TOL) -> None:
+def assert_groups_equal(got: dict, want: dict, kinds: list[str], rel: float = FLOAT_REL_TOL,
+                        magnitude: dict | None = None) -> None:
     """Compare two exported group tables after canonical sort.
 
     kinds[a] in {"count", "sum_i", "sum_f", "sum_d", "min_i", "max_i", "min_f", "max_f", "min_d", "max_d",
-    "avg_i", "avg_f", "avg_d"}: integer / DECIMAL state must match bit for bit, float sums within `rel`
-    relative error, float MIN/MAX exactly.
+    "avg_i", "avg_f", "avg_d"}: integer / DECIMAL state must match bit for bit, float MIN/MAX exactly, and
+    float sums within `rel` of their magnitude. A float sum taken in another order differs by rounding
+    error proportional to sum(|x|), not to |sum(x)|, so when the inputs have mixed signs the caller
+    passes `magnitude`: an export over the same groups whose float aggregate a holds sum(|x|) (mean(|x|)
+    for AVG), and the bound becomes rel * max(|want|, magnitude).
     """
     ng, nw = got["count"].shape[1] if got["count"].size else got["keys"].shape[1], \
         want["count"].shape[1] if want["count"].size else want["keys"].shape[1]
     assert ng == nw, f"group count {ng} != {nw}"
     og, ow = canonical_order(got), canonical_order(want)
+    om = canonical_order(magnitude) if magnitude is not None else None
     np.testing.assert_array_equal(got["key_valid"][:, og], want["key_valid"][:, ow])
     kvalid = want["key_valid"][:, ow].astype(bool)
     np.testing.assert_array_equal(np.where(kvalid, got["keys"][:, og], 0), np.where(kvalid, want["keys"][:, ow], 0))
@@ -45,7 +50,12 @@ def assert_groups_equal(got: dict, want: dict, kinds: list[str], rel: float = FL
             np.testing.assert_array_equal(got["dec"][a, og][has], want["dec"][a, ow][has], err_msg=f"agg {a} dec")
         elif kind in ("sum_f", "avg_f"):
             g, w = got["f64"][a, og][has], want["f64"][a, ow][has]
-            np.testing.assert_allclose(g, w, rtol=rel, atol=0, err_msg=f"agg {a} f64 sum")
+            scale = np.abs(w)
+            if magnitude is not None:
+                scale = np.maximum(scale, np.abs(magnitude["f64"][a, om][has]))
+            bad = ~(np.abs(g - w) <= rel * scale)
+            assert not bad.any(), (f"agg {a} f64 sum: {int(bad.sum())} of {bad.size} groups differ by more than "
+                                   f"{rel} of their magnitude; got {g[bad][:3]} want {w[bad][:3]}")
         elif kind in ("min_f", "max_f"):
             np.testing.assert_array_equal(got["f64"][a, og][has], want["f64"][a, ow][has], err_msg=f"agg {a} f64")
 

@@ -138,6 +138,19 @@ def make_aggs(nk):
     return specs, kinds
 
 
+def oracle_magnitude(cols, key_idx, specs):
+    """The oracle's per-group sum(|x|) (mean(|x|) for AVG) of every float aggregate: the scale that the
+    rounding error of a float sum taken in another order is proportional to."""
+    acols, idx = list(cols), {}
+    for i, (t, d, v) in enumerate(cols):
+        if t in (F32, F64):
+            idx[i] = len(acols)
+            acols.append((t, np.abs(d), v))
+    om = ob.Agg(key_idx, [(f, idx.get(c, c), 0) for f, c in specs])
+    om.consume(ob.HostBatch([(t, d, v, 2 if t == DEC else 0) for t, d, v in acols]))
+    return om.export()
+
+
 def run_both(ctx, cols, key_idx, specs, hint=0, batches=3, device=False):
     import torch
     import wadjet_b200 as wg
@@ -163,7 +176,7 @@ def run_both(ctx, cols, key_idx, specs, hint=0, batches=3, device=False):
                 g.consume(wg.Batch([wg.Column(t, d, v, 2 if t == DEC else 0) for t, d, v in sl]))
             o.consume(ob.HostBatch([(t, d, v, 2 if t == DEC else 0) for t, d, v in sl]))
         g.finalize()
-        results.append((g.export(), o.export(), g, o))
+        results.append((g.export(), o.export(), g, o, oracle_magnitude(cols, key_idx, part)))
     return results
 
 
@@ -176,8 +189,8 @@ def test_aggregate_matches_oracle(ctx, key_types, ncard, nulls, key_nulls):
     cols = agg_setup(rng, 60_000, key_types, ncard, nulls, key_nulls)
     specs, kinds = make_aggs(len(key_types))
     res = run_both(ctx, cols, list(range(len(key_types))), specs)
-    assert_groups_equal(res[0][0], res[0][1], kinds[:6])
-    assert_groups_equal(res[1][0], res[1][1], kinds[6:])
+    assert_groups_equal(res[0][0], res[0][1], kinds[:6], magnitude=res[0][4])
+    assert_groups_equal(res[1][0], res[1][1], kinds[6:], magnitude=res[1][4])
     for g in (res[0][2], res[1][2]):
         g.close()
 
@@ -189,8 +202,8 @@ def test_aggregate_device_batches_and_growth(ctx):
     cols = agg_setup(rng, 200_000, [I64], 150_000, 0.0, 0.0)
     specs, kinds = make_aggs(1)
     res = run_both(ctx, cols, [0], specs, hint=16, batches=4, device=True)
-    assert_groups_equal(res[0][0], res[0][1], kinds[:6])
-    assert_groups_equal(res[1][0], res[1][1], kinds[6:])
+    assert_groups_equal(res[0][0], res[0][1], kinds[:6], magnitude=res[0][4])
+    assert_groups_equal(res[1][0], res[1][1], kinds[6:], magnitude=res[1][4])
 
 
 def test_aggregate_low_cardinality_smem(ctx):
@@ -198,8 +211,8 @@ def test_aggregate_low_cardinality_smem(ctx):
     cols = agg_setup(rng, 300_000, [I64], 900, 0.0, 0.0)
     specs, kinds = make_aggs(1)
     res = run_both(ctx, cols, [0], specs, hint=1000, batches=2)
-    assert_groups_equal(res[0][0], res[0][1], kinds[:6])
-    assert_groups_equal(res[1][0], res[1][1], kinds[6:])
+    assert_groups_equal(res[0][0], res[0][1], kinds[:6], magnitude=res[0][4])
+    assert_groups_equal(res[1][0], res[1][1], kinds[6:], magnitude=res[1][4])
 
 
 def test_clone_and_merge(ctx):
@@ -220,7 +233,7 @@ def test_clone_and_merge(ctx):
         primary.merge_sink(w)
         w.close()
     primary.finalize()
-    assert_groups_equal(primary.export(), o.export(), kinds)
+    assert_groups_equal(primary.export(), o.export(), kinds, magnitude=oracle_magnitude(cols, [0], specs))
     primary.close()
 
 

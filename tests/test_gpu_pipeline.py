@@ -203,3 +203,30 @@ def test_ipv4_prefix_workload_matches_oracle(ctx, spec, monkeypatch):
                 exprs=[ob.expr(I64, [("col", 0), ("ci", 8), ">>"])], threads=4)
     assert_groups_equal(g.export(), o.export(), ["sum_i", "count"])
     g.close()
+
+
+@pytest.mark.parametrize("scale", [0, 2, 9, 18, 27, 38])
+def test_decimal_to_float_conversion_is_bit_exact(ctx, scale):
+    """Int128.ToFloat64 of every row, through a projection and MIN over one-row groups: values in the
+    64-bit fast path and beyond it, at several scales, must equal the oracle bit for bit."""
+    import torch
+    import wadjet_b200 as wg
+    rng = np.random.default_rng(scale)
+    n = 1 << 18
+    dec = np.zeros(n, DEC_DTYPE)
+    small = rng.random(n) < 0.6
+    lo = rng.integers(0, 2**63, n, dtype=np.int64).astype(np.uint64) >> rng.integers(0, 60, n).astype(np.uint64)
+    neg = rng.random(n) < 0.5
+    dec["lo"] = np.where(small & neg, (~lo) + np.uint64(1), lo)
+    dec["hi"] = np.where(small, np.where(neg, -1, 0), rng.integers(-(2**40), 2**40, n))
+    ids = np.arange(n, dtype=np.int64)
+    g = wg.HashAggregate(ctx, [0], [wg.AggColumn(wg.AGG_MIN, 2)], ndv_hint=n)
+    batch = wg.Batch([wg.Column(I64, torch.from_numpy(ids).cuda()),
+                      wg.Column(DEC, torch.from_numpy(dec.view(np.int64).reshape(-1, 2)).cuda(), scale=scale)])
+    wg.run_pipeline(ctx, batch, g, exprs=[wg.Expr(F64, [wg.Expr.col(1)])], device=True)
+    g.finalize()
+    o = ob.Agg([0], [(2, 2, 0)])
+    ob.pipeline(ob.HostBatch([(I64, ids, None, 0), (DEC, dec, None, scale)]), o,
+                exprs=[ob.expr(F64, [("col", 1)])], threads=4)
+    assert_groups_equal(g.export(), o.export(), ["min_f"])
+    g.close()

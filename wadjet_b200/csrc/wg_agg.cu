@@ -549,16 +549,20 @@ static int32_t pick_shape(const wgd::Plan& P) {
   return wgd::shape_of(P);
 }
 
+// The table's layout with a plan's compact column numbering.
+static wgd::Layout launch_layout(const wg_agg* a, const wgd::Plan& P) {
+  wgd::Layout L = a->L;
+  for (int k = 0; k < WG_MAX_KEYS; ++k) L.key_vcol[k] = P.L.key_vcol[k];
+  for (int i = 0; i < WG_MAX_AGGS; ++i) L.agg[i].vcol = P.L.agg[i].vcol;
+  return L;
+}
+
 static wg_status launch_pipeline(wg_agg* a, const LaunchSpec& ls, int64_t n_items) {
   Ctx* ctx = a->ctx;
   LaunchSpec l2 = ls;
   wgd::Plan& P = l2.P;
   P.T = table_view(a);
-  // the table's layout, with this launch's compact column numbering
-  wgd::Layout L = a->L;
-  for (int k = 0; k < WG_MAX_KEYS; ++k) L.key_vcol[k] = ls.P.L.key_vcol[k];
-  for (int i = 0; i < WG_MAX_AGGS; ++i) L.agg[i].vcol = ls.P.L.agg[i].vcol;
-  P.L = L;
+  P.L = launch_layout(a, ls.P);
   P.n_items = n_items;
   if (l2.tile) l2.cfg.n_tiles = (n_items + l2.cfg.rows - 1) / l2.cfg.rows;
   P.shape = pick_shape(P);
@@ -732,23 +736,30 @@ static wg_status run_device(const PipelineRun& r) {
     any_null_words |= a->L.agg[i].null_off >= 0;
     any_dec_minmax |= a->L.agg[i].kind == wgd::K_MIN_DEC || a->L.agg[i].kind == wgd::K_MAX_DEC;
   }
+  // a kernel compiled for this query shape runs 768-thread CTAs (48 warps per
+  // SM), the generic one 512-thread CTAs
+  wgd::Plan probe = ls.P;
+  probe.L = launch_layout(a, ls.P);
+  const bool stat = pick_shape(probe) != wgd::SHAPE_GENERIC;
   const int blocks_per_sm = std::max(1, env_int("WG_AGG_BLOCKS_PER_SM", 2));
-  ls.block = kAggBlock;
+  ls.block = stat ? wgd::StatShape<wgd::ShapeStarJoin>::kBlock : wgd::DynShape::kBlock;
   const int64_t smem_budget = (int64_t)ctx->max_smem_optin / blocks_per_sm - 2048;
   const int S = (int)std::min<int64_t>(smem_budget / (a->L.slot_words * 8), 16384);
   const int64_t expect = std::max<int64_t>(a->hint, a->known_groups);
+  // the shared table runs at most 5/8 full for the expected groups
   ls.smem = env_int("WG_AGG_SMEM", 1) != 0 && a->L.key_words == 1 && !any_null_words && !any_dec_minmax && S >= 256 &&
-            expect > 0 && expect * 2 <= S;
+            expect > 0 && expect * 8 <= (int64_t)S * 5;
   ls.P.smem_slots = ls.smem ? S : 0;
   ls.smem_bytes = ls.smem ? (size_t)S * a->L.slot_words * 8 : 0;
-  ls.grid = (unsigned)(ctx->sm_count * blocks_per_sm);
-  if (!ls.smem) ls.grid = (unsigned)std::min<int64_t>((int64_t)ctx->sm_count * 4, (n_items + 1023) / 1024 + 1);
+  const int64_t want_ctas = (n_items + ls.block - 1) / ls.block + 1;
+  ls.grid = (unsigned)std::min<int64_t>((int64_t)ctx->sm_count * blocks_per_sm, want_ctas);
+  if (!ls.smem && !stat) ls.grid = (unsigned)std::min<int64_t>((int64_t)ctx->sm_count * 4, (n_items + 1023) / 1024 + 1);
 
   // TMA-staged tile kernel: contiguous input (no selection vector) whose columns
   // start on 16-byte boundaries; one persistent CTA per SM.
   bool aligned = ls.P.sel == nullptr && ls.P.n_in > 0;
   for (int j = 0; j < ls.P.n_in; ++j) aligned = aligned && ((uintptr_t)ls.P.in[j].data % 16 == 0);
-  if (aligned && env_int("WG_TILE", 1) != 0 && n_items >= 4096) {
+  if (aligned && env_int("WG_TILE", 0) != 0 && n_items >= 4096) {
     wgd::TileCfg& c = ls.cfg;
     std::memset(&c, 0, sizeof(c));
     c.consumers = std::max(1, std::min(31, env_int("WG_TILE_CONSUMERS", 16)));
@@ -767,7 +778,7 @@ static wg_status run_device(const PipelineRun& r) {
       int64_t tb = table_bytes;
       if (ls.smem && off * c.stages + tb > budget) {
         const int64_t s2 = (budget - off * c.stages) / (a->L.slot_words * 8);
-        if (s2 >= 256 && expect * 2 <= s2) { ls.P.smem_slots = (int)s2; tb = s2 * a->L.slot_words * 8; }
+        if (s2 >= 256 && expect * 8 <= s2 * 5) { ls.P.smem_slots = (int)s2; tb = s2 * a->L.slot_words * 8; }
       }
       if (off * c.stages + tb <= budget) {
         c.rows = rows;
@@ -818,7 +829,7 @@ static wg_status run_device(const PipelineRun& r) {
       WG_TRY(rebuild_table(a, a->cap * 4, a->L));
       WG_TRY(refresh_groups(a));
       const int64_t expect2 = std::max<int64_t>(a->hint, a->known_groups);
-      if (ls.smem && expect2 * 2 > S) { ls.smem = false; ls.P.smem_slots = 0; ls.smem_bytes = 0; }
+      if (ls.smem && expect2 * 8 > (int64_t)S * 5) { ls.smem = false; ls.P.smem_slots = 0; ls.smem_bytes = 0; }
       if (table_words(a, a->cap) * 8 > kSnapshotMaxBytes) break;
     }
   }

@@ -93,6 +93,7 @@ struct LayoutAcc {
 // Everything from the plan at run time.
 struct DynShape {
   static constexpr bool smem_ok = true;
+  static constexpr int kBlock = 512, kMinBlocks = 2;  // launch shape of the plain fused kernel
   const Plan& P;
   __device__ __forceinline__ int n_in() const { return P.n_in; }
   __device__ __forceinline__ int in_cls(int j) const { return P.in[j].cls; }
@@ -129,6 +130,8 @@ struct DynShape {
 template <class C>
 struct StatShape {
   static constexpr bool smem_ok = C::smem_ok;
+  // straight-line code fits 40 registers: two 768-thread CTAs per SM (48 warps)
+  static constexpr int kBlock = 768, kMinBlocks = 2;
   const Plan& P;
   __device__ __forceinline__ constexpr int n_in() const { return C::n_in; }
   __device__ __forceinline__ constexpr int in_cls(int j) const { return C::in_cls(j); }
@@ -461,13 +464,24 @@ __device__ __forceinline__ unsigned long long* find_smem(unsigned long long* sm,
   return nullptr;
 }
 
-// Warp-cooperative update: lanes holding the same key pre-combine their
-// contributions (__match_any_sync) and only the group's lowest lane touches the
-// table, so hot keys cost one set of atomics per warp instead of one per row.
+// Update of one row per lane. With a CTA-private shared-memory table each lane
+// applies its own row there with shared-memory atomics (cheaper than combining
+// first). Rows bound for the HBM table (no shared table, a NULL key, or a
+// shared table at its fill limit) are combined first: lanes holding the same
+// key pre-combine their contributions (__match_any_sync) and only the group's
+// lowest lane touches the table, so a hot key costs one set of global atomics
+// per warp instead of one per row.
 template <int NA, bool SMEM, class Sh>
 __device__ __forceinline__ void warp_update(const Plan& P, const Sh& sh, bool cur, unsigned long long k0,
                                             unsigned long long k1, bool knull, Contrib<NA>& c,
                                             unsigned long long* sm, int* s_groups, int s_limit) {
+  if (SMEM && cur && !knull) {
+    unsigned long long* s = find_smem(sm, P.smem_slots, sh.slot_words(), k0, s_groups, s_limit);
+    if (s != nullptr) {
+      apply<NA>(sh, s, c, 1ULL);
+      cur = false;
+    }
+  }
   const unsigned am = __ballot_sync(WG_FULL_MASK, cur);
   if (am == 0) return;
   const int lane = threadIdx.x & 31;
@@ -498,9 +512,7 @@ __device__ __forceinline__ void warp_update(const Plan& P, const Sh& sh, bool cu
     }
   }
   if (leader) {
-    unsigned long long* s = nullptr;
-    if (SMEM && !knull) s = find_smem(sm, P.smem_slots, sh.slot_words(), k0, s_groups, s_limit);
-    if (s == nullptr) s = find_global(sh, P.T, k0, k1, knull, P.err);
+    unsigned long long* s = find_global(sh, P.T, k0, k1, knull, P.err);
     if (s != nullptr) apply<NA>(sh, s, c, (unsigned long long)mysz);
   }
 }
@@ -614,7 +626,7 @@ __device__ __forceinline__ void smem_table_flush(const Plan& P, const unsigned l
 // The fused pipeline reading HBM directly: one warp per 32 consecutive rows
 // (or selection-vector entries), grid-stride.
 template <int NA, bool SMEM, class Sh>
-__global__ void __launch_bounds__(512) pipeline_kernel(const __grid_constant__ Plan P) {
+__global__ void __launch_bounds__(Sh::kBlock, Sh::kMinBlocks) pipeline_kernel(const __grid_constant__ Plan P) {
   extern __shared__ unsigned long long sm[];
   __shared__ int s_groups;
   const Sh sh{P};
