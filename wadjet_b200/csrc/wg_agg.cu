@@ -70,7 +70,7 @@ __global__ void fold_kernel(Layout Ls, Table Ts, Layout Ld, Table Td, int32_t* e
     if (!d) continue;
     Contrib<NA> c;
     slot_contrib<NA>(ls, s, c);
-    apply<NA>(ld, d, c, s[Ls.key_words]);
+    apply<NA, false>(ld, d, c, s[Ls.key_words]);
   }
 }
 
@@ -798,6 +798,12 @@ static wg_status run_device(const PipelineRun& r) {
     }
   }
 
+  // shared-table row counters are 32-bit: a CTA's share of the rows stays below 2^31
+  if (ls.smem && n_items / std::max<int64_t>(1, ls.grid) >= (int64_t(1) << 31)) {
+    ls.smem = false;
+    ls.P.smem_slots = 0;
+    ls.smem_bytes = 0;
+  }
   const wgd::Plan base = ls.P;
   auto limit = [&]() { return (int64_t)((double)a->cap * kMaxLoad); };
 

@@ -341,26 +341,68 @@ __device__ __forceinline__ void combine(int kind, unsigned long long& a0, unsign
   }
 }
 
-// Fold a combined contribution into a slot (HBM or shared memory) with atomics.
-template <int NA, class Lay>
+// Add a two's-complement integer of `nlimbs` 32-bit limbs (lo, hi words) to the
+// limbs at L with native 32-bit shared-memory atomics: each limb's carry out is
+// read from the value its atomic replaced and added to the next limb, so the
+// words end up holding the exact sum mod 2^(32*nlimbs) in any interleaving.
+// (64-bit shared-memory atomic adds are compare-and-swap loops that replay
+// while lanes of a warp hit the same hot group; 32-bit adds are not.)
+__device__ __forceinline__ void smem_add_limbs(unsigned* L, int nlimbs, unsigned long long lo, unsigned long long hi) {
+  const unsigned x[4] = {(unsigned)lo, (unsigned)(lo >> 32), (unsigned)hi, (unsigned)(hi >> 32)};
+  unsigned carry = 0;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    if (i >= nlimbs) break;
+    const unsigned long long t = (unsigned long long)x[i] + carry;
+    if (t == 0) { carry = 0; continue; }
+    if (t == (1ULL << 32)) { carry = 1; continue; }  // adds 0 here, carries 1
+    const unsigned a = (unsigned)t;
+    const unsigned old = atomicAdd(L + i, a);
+    carry = (unsigned)(old + a) < old ? 1u : 0u;
+  }
+}
+
+// Fold a combined contribution into a slot with atomics. SH: the slot is in a
+// CTA-private shared-memory table, where the row count is a 32-bit counter in
+// the low half of its word (a CTA applies fewer than 2^32 rows), integer and
+// DECIMAL sums go limb by limb, and MIN/MAX skip the atomic when the slot
+// already holds a value at least as good (slot values only ever improve).
+template <int NA, bool SH, class Lay>
 __device__ __forceinline__ void apply(const Lay& ly, unsigned long long* s, const Contrib<NA>& c,
                                       unsigned long long rows) {
-  atomicAdd(s + ly.key_words(), rows);
+  if (SH) atomicAdd((unsigned*)(s + ly.key_words()), (unsigned)rows);
+  else atomicAdd(s + ly.key_words(), rows);
 #pragma unroll
   for (int a = 0; a < NA; ++a) {
     if (a >= ly.n_aggs()) continue;
     const int kind = ly.agg_kind(a), off = ly.agg_off(a), noff = ly.agg_null_off(a);
     const unsigned long long w0 = c.w0[a], w1 = c.w1[a];
+    unsigned long long* t = s + off;
     switch (kind) {
-      case K_SUM_I64: if (w0) atomicAdd(s + off, w0); break;
-      case K_SUM_F64: { const double d = as_f(w0); if (d != 0.0) atomicAdd((double*)(s + off), d); } break;
-      case K_SUM_DEC: atomic_add128(s + off, w0, w1); break;
-      case K_MIN_I64: if (w0 != 0x7FFFFFFFFFFFFFFFULL) atomicMin((long long*)(s + off), (long long)w0); break;
-      case K_MAX_I64: if (w0 != 0x8000000000000000ULL) atomicMax((long long*)(s + off), (long long)w0); break;
-      case K_MIN_F64: if (w0 != ~0ULL) atomicMin(s + off, w0); break;
-      case K_MAX_F64: if (w0 != 0ULL) atomicMax(s + off, w0); break;
-      case K_MIN_DEC: atomic_min128((U128*)(s + off), w0, w1); break;
-      case K_MAX_DEC: atomic_max128((U128*)(s + off), w0, w1); break;
+      case K_SUM_I64:
+        if (w0) { if (SH) smem_add_limbs((unsigned*)t, 2, w0, 0); else atomicAdd(t, w0); }
+        break;
+      case K_SUM_F64: { const double d = as_f(w0); if (d != 0.0) atomicAdd((double*)t, d); } break;
+      case K_SUM_DEC:
+        if (SH) smem_add_limbs((unsigned*)t, 4, w0, w1);
+        else atomic_add128(t, w0, w1);
+        break;
+      case K_MIN_I64:
+        if (w0 != 0x7FFFFFFFFFFFFFFFULL && (!SH || (long long)w0 < *(volatile long long*)t))
+          atomicMin((long long*)t, (long long)w0);
+        break;
+      case K_MAX_I64:
+        if (w0 != 0x8000000000000000ULL && (!SH || (long long)w0 > *(volatile long long*)t))
+          atomicMax((long long*)t, (long long)w0);
+        break;
+      case K_MIN_F64:
+        if (w0 != ~0ULL && (!SH || w0 < *(volatile unsigned long long*)t)) atomicMin(t, w0);
+        break;
+      case K_MAX_F64:
+        if (w0 != 0ULL && (!SH || w0 > *(volatile unsigned long long*)t)) atomicMax(t, w0);
+        break;
+      case K_MIN_DEC: atomic_min128((U128*)t, w0, w1); break;
+      case K_MAX_DEC: atomic_max128((U128*)t, w0, w1); break;
       default: break;
     }
     if (noff >= 0 && c.nul[a]) atomicAdd(s + noff, (unsigned long long)c.nul[a]);
@@ -478,7 +520,7 @@ __device__ __forceinline__ void warp_update(const Plan& P, const Sh& sh, bool cu
   if (SMEM && cur && !knull) {
     unsigned long long* s = find_smem(sm, P.smem_slots, sh.slot_words(), k0, s_groups, s_limit);
     if (s != nullptr) {
-      apply<NA>(sh, s, c, 1ULL);
+      apply<NA, true>(sh, s, c, 1ULL);
       cur = false;
     }
   }
@@ -513,7 +555,7 @@ __device__ __forceinline__ void warp_update(const Plan& P, const Sh& sh, bool cu
   }
   if (leader) {
     unsigned long long* s = find_global(sh, P.T, k0, k1, knull, P.err);
-    if (s != nullptr) apply<NA>(sh, s, c, (unsigned long long)mysz);
+    if (s != nullptr) apply<NA, false>(sh, s, c, (unsigned long long)mysz);
   }
 }
 
@@ -619,7 +661,7 @@ __device__ __forceinline__ void smem_table_flush(const Plan& P, const unsigned l
     if (g == nullptr) continue;
     Contrib<NA> c;
     slot_contrib<NA>(ly, s, c);
-    apply<NA>(ly, g, c, s[P.L.key_words]);
+    apply<NA, false>(ly, g, c, s[P.L.key_words]);
   }
 }
 
