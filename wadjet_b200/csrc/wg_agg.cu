@@ -741,16 +741,30 @@ static wg_status run_device(const PipelineRun& r) {
   wgd::Plan probe = ls.P;
   probe.L = launch_layout(a, ls.P);
   const bool stat = pick_shape(probe) != wgd::SHAPE_GENERIC;
-  const int blocks_per_sm = std::max(1, env_int("WG_AGG_BLOCKS_PER_SM", 2));
+  const int env_bps = env_int("WG_AGG_BLOCKS_PER_SM", 0);
+  int blocks_per_sm = env_bps > 0 ? env_bps : 2;
   ls.block = stat ? wgd::StatShape<wgd::ShapeStarJoin>::kBlock : wgd::DynShape::kBlock;
-  const int64_t smem_budget = (int64_t)ctx->max_smem_optin / blocks_per_sm - 2048;
-  const int S = (int)std::min<int64_t>(smem_budget / (a->L.slot_words * 8), 16384);
+  auto slots_for = [&](int bps) {
+    return (int)std::min<int64_t>(((int64_t)ctx->max_smem_optin / bps - 2048) / (a->L.slot_words * 8), 16384);
+  };
+  // a shared table runs at most 5/8 full for the expected groups, 3/4 when it
+  // fills a whole SM (one CTA per SM)
+  auto fits = [&](int64_t groups, int slots) {
+    return slots >= 256 && groups * (blocks_per_sm == 1 ? 4 : 8) <= (int64_t)slots * (blocks_per_sm == 1 ? 3 : 5);
+  };
+  int S = slots_for(blocks_per_sm);
   const int64_t expect = std::max<int64_t>(a->hint, a->known_groups);
-  // the shared table runs at most 5/8 full for the expected groups
-  ls.smem = env_int("WG_AGG_SMEM", 1) != 0 && a->L.key_words == 1 && !any_null_words && !any_dec_minmax && S >= 256 &&
-            expect > 0 && expect * 8 <= (int64_t)S * 5;
+  const bool smem_ok = env_int("WG_AGG_SMEM", 1) != 0 && a->L.key_words == 1 && !any_null_words && !any_dec_minmax &&
+                       expect > 0;
+  if (smem_ok && env_bps == 0 && !fits(expect, S)) {
+    blocks_per_sm = 1;
+    S = slots_for(1);
+    if (!fits(expect, S)) { blocks_per_sm = 2; S = slots_for(2); }
+  }
+  ls.smem = smem_ok && fits(expect, S);
   ls.P.smem_slots = ls.smem ? S : 0;
   ls.smem_bytes = ls.smem ? (size_t)S * a->L.slot_words * 8 : 0;
+  ls.P.prefetch = std::max(0, env_int("WG_PREFETCH", 2));
   const int64_t want_ctas = (n_items + ls.block - 1) / ls.block + 1;
   ls.grid = (unsigned)std::min<int64_t>((int64_t)ctx->sm_count * blocks_per_sm, want_ctas);
   if (!ls.smem && !stat) ls.grid = (unsigned)std::min<int64_t>((int64_t)ctx->sm_count * 4, (n_items + 1023) / 1024 + 1);
@@ -778,7 +792,7 @@ static wg_status run_device(const PipelineRun& r) {
       int64_t tb = table_bytes;
       if (ls.smem && off * c.stages + tb > budget) {
         const int64_t s2 = (budget - off * c.stages) / (a->L.slot_words * 8);
-        if (s2 >= 256 && expect * 8 <= s2 * 5) { ls.P.smem_slots = (int)s2; tb = s2 * a->L.slot_words * 8; }
+        if (fits(expect, (int)s2)) { ls.P.smem_slots = (int)s2; tb = s2 * a->L.slot_words * 8; }
       }
       if (off * c.stages + tb <= budget) {
         c.rows = rows;
@@ -835,7 +849,7 @@ static wg_status run_device(const PipelineRun& r) {
       WG_TRY(rebuild_table(a, a->cap * 4, a->L));
       WG_TRY(refresh_groups(a));
       const int64_t expect2 = std::max<int64_t>(a->hint, a->known_groups);
-      if (ls.smem && expect2 * 8 > (int64_t)S * 5) { ls.smem = false; ls.P.smem_slots = 0; ls.smem_bytes = 0; }
+      if (ls.smem && !fits(expect2, S)) { ls.smem = false; ls.P.smem_slots = 0; ls.smem_bytes = 0; }
       if (table_words(a, a->cap) * 8 > kSnapshotMaxBytes) break;
     }
   }

@@ -84,7 +84,7 @@ struct Plan {
   int32_t probe_col;
   int32_t smem_slots;            // >0: CTA-private shared-memory table of this many slots
   int32_t shape;                 // compiled query shape (wg_shapes.cuh), 0 = generic
-  int32_t _pad0;
+  int32_t prefetch;              // grid-stride iterations of input prefetched into L2 ahead (0 = off)
   DCol in[WG_MAX_IN];
   Pred filt[WG_MAX_FILTERS];
   JoinView join;

@@ -665,6 +665,30 @@ __device__ __forceinline__ void smem_table_flush(const Plan& P, const unsigned l
   }
 }
 
+// Ask L2 for the input lines of the 32 rows starting at row0 (the grid-stride
+// chunk this warp reaches `prefetch` iterations later), one 128-byte line per
+// lane, so the column loads of that iteration find their lines in L2 instead
+// of waiting for HBM. Only lines inside the columns are touched.
+template <class Sh>
+__device__ __forceinline__ void prefetch_rows(const Plan& P, const Sh& sh, int64_t row0, int lane) {
+  if (row0 >= P.n_items) return;
+  int first = 0;
+#pragma unroll
+  for (int j = 0; j < WG_MAX_IN; ++j) {
+    if (j >= sh.n_in()) break;
+    const int es = cls_bytes(sh.in_cls(j));
+    const int lines = es / 4;  // 32 rows x es bytes / 128
+    if (lane >= first && lane < first + lines) {
+      const int64_t row = row0 + (int64_t)(lane - first) * (128 / es);
+      if (row < P.n_items) {
+        const char* p = (const char*)P.in[j].data + row * es;
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+      }
+    }
+    first += lines;
+  }
+}
+
 // The fused pipeline reading HBM directly: one warp per 32 consecutive rows
 // (or selection-vector entries), grid-stride.
 template <int NA, bool SMEM, class Sh>
@@ -681,8 +705,10 @@ __global__ void __launch_bounds__(Sh::kBlock, Sh::kMinBlocks) pipeline_kernel(co
   const int lane = threadIdx.x & 31;
   const int64_t wpb = blockDim.x >> 5;
   const int64_t total_warps = (int64_t)gridDim.x * wpb;
+  const int64_t ahead = (int64_t)P.prefetch * total_warps * 32;
   for (int64_t base = ((int64_t)blockIdx.x * wpb + (threadIdx.x >> 5)) * 32; base < P.n_items;
        base += total_warps * 32) {
+    if (ahead > 0 && P.sel == nullptr) prefetch_rows(P, sh, base + ahead, lane);
     const int64_t item = base + lane;
     const bool act = item < P.n_items;
     SrcGlobal src{act ? (P.sel ? (int64_t)__ldg(P.sel + item) : item) : 0};
