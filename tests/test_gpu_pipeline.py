@@ -76,13 +76,14 @@ def test_groupby_workload_matches_oracle(ctx, spec, monkeypatch):
     g.close()
 
 
-KNOB_NAMES = ("WG_TILE", "WG_JOIN_DIRECT", "WG_AGG_SMEM", "WG_SPECIALIZE")
-KNOBS = [  # every GPU lever on, off, and mixed
-    ("1", "1", "1", "1"), ("0", "0", "0", "0"), ("1", "0", "1", "1"), ("0", "1", "0", "1"), ("1", "1", "0", "1"),
-    ("1", "1", "1", "0"), ("0", "1", "1", "1")]
+KNOB_NAMES = ("WG_TILE", "WG_JOIN_DIRECT", "WG_AGG_SMEM", "WG_SPECIALIZE", "WG_JOIN_DENSE", "WG_SMEM_REPLICAS")
+KNOBS = [  # the defaults first, then every GPU lever off, on and mixed
+    ("0", "1", "1", "1", "1", "4"), ("0", "0", "0", "0", "0", "1"), ("1", "1", "1", "1", "1", "4"),
+    ("1", "0", "1", "1", "1", "1"), ("0", "1", "0", "1", "1", "4"), ("1", "1", "0", "1", "0", "4"),
+    ("0", "1", "1", "0", "1", "2"), ("0", "1", "1", "1", "0", "1"), ("0", "1", "1", "1", "1", "8")]
 
 
-@pytest.mark.parametrize("knobs", KNOBS, ids=lambda k: "tile%s-direct%s-smem%s-spec%s" % k)
+@pytest.mark.parametrize("knobs", KNOBS, ids=lambda k: "tile%s-direct%s-smem%s-spec%s-dense%s-rep%s" % k)
 @pytest.mark.parametrize("host_input", [False, True])
 def test_starjoin_workload_matches_oracle(ctx, host_input, knobs, monkeypatch):
     """Star join + aggregate, 2^22 fact rows against the full 2^22-row dimension, with
@@ -114,6 +115,46 @@ def test_starjoin_workload_matches_oracle(ctx, host_input, knobs, monkeypatch):
     g.finalize()
     hkey, hgrp = key.cpu().numpy(), grp.cpu().numpy()
     oj = ob.Join(1 << 22)
+    oj.append(I32, hkey)
+    o = ob.Agg([4], [(0, 5, 0), (0, 2, 0)])
+    ob.pipeline(ob.HostBatch([(I32, hfk, None, 0), (I32, hqty, None, 0), (DEC, hprice, None, 2), (F64, hdisc, None, 0)]),
+                o, filters=[(1, wg.OP_GT, 10)], join=oj, probe_key=0,
+                build=ob.HostBatch([(I32, hkey, None, 0), (I32, hgrp, None, 0)]), payload=[1],
+                exprs=[ob.expr(F64, [("col", 2), ("cf", 1.0), ("col", 3), "-", "*"])], threads=8)
+    assert_groups_equal(g.export(), o.export(), ["sum_f", "sum_d"])
+    g.close()
+    j.close()
+
+
+@pytest.mark.parametrize("dense", ["1", "0"])
+def test_starjoin_with_missing_and_out_of_range_keys(ctx, dense, monkeypatch):
+    """A dimension whose keys are the even numbers of [1000, 1000 + 2^17) (so half the
+    slots of a dense index are empty) probed by fact keys spread over [0, 2^18): keys
+    below the smallest, above the largest and between build keys must all miss."""
+    import torch
+    import wadjet_b200 as wg
+    from tests.helpers import dec_array
+    monkeypatch.setenv("WG_JOIN_DENSE", dense)
+    rng = np.random.default_rng(11)
+    nd, nf = 1 << 16, 1 << 20
+    hkey = (1000 + 2 * rng.permutation(nd)).astype(np.int32)
+    hgrp = rng.integers(0, 700, nd).astype(np.int32)
+    hfk = rng.integers(0, 1 << 18, nf).astype(np.int32)
+    hqty = rng.integers(1, 51, nf).astype(np.int32)
+    hprice = dec_array(rng.integers(100, 10**7, nf))
+    hdisc = np.round(rng.random(nf) * 0.1, 2)
+    j = wg.HashJoin(ctx, 0, 0, payload=[1], build_row_hint=nd)
+    j.build([wg.Batch([wg.Column(I32, torch.from_numpy(hkey).cuda()), wg.Column(I32, torch.from_numpy(hgrp).cuda())])],
+            device=True)
+    expr, aggs = starjoin_plan(wg)
+    g = wg.HashAggregate(ctx, [4], aggs, ndv_hint=700)
+    batch = wg.Batch([wg.Column(I32, torch.from_numpy(hfk).cuda()), wg.Column(I32, torch.from_numpy(hqty).cuda()),
+                      wg.Column(DEC, torch.from_numpy(hprice.view(np.int64).reshape(-1, 2)).cuda(), scale=2),
+                      wg.Column(F64, torch.from_numpy(hdisc).cuda())])
+    wg.run_pipeline(ctx, batch, g, filters=[(1, wg.OP_GT, 10)], join=j, exprs=[expr], device=True)
+    assert g.kernel_shape == SHAPE_STARJOIN
+    g.finalize()
+    oj = ob.Join(nd)
     oj.append(I32, hkey)
     o = ob.Agg([4], [(0, 5, 0), (0, 2, 0)])
     ob.pipeline(ob.HostBatch([(I32, hfk, None, 0), (I32, hqty, None, 0), (DEC, hprice, None, 2), (F64, hdisc, None, 0)]),

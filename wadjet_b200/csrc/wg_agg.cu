@@ -744,26 +744,40 @@ static wg_status run_device(const PipelineRun& r) {
   const int env_bps = env_int("WG_AGG_BLOCKS_PER_SM", 0);
   int blocks_per_sm = env_bps > 0 ? env_bps : 2;
   ls.block = stat ? wgd::StatShape<wgd::ShapeStarJoin>::kBlock : wgd::DynShape::kBlock;
-  auto slots_for = [&](int bps) {
-    return (int)std::min<int64_t>(((int64_t)ctx->max_smem_optin / bps - 2048) / (a->L.slot_words * 8), 16384);
+  // copies of each float SUM per shared slot (lane-striped, see apply)
+  int n_fsum = 0;
+  for (int i = 0; i < a->L.n_aggs; ++i) n_fsum += a->L.agg[i].kind == wgd::K_SUM_F64;
+  const int max_rep = n_fsum > 0 ? std::max(1, std::min(8, env_int("WG_SMEM_REPLICAS", 4))) : 1;
+  auto stride_for = [&](int rep) { return a->L.slot_words + n_fsum * (rep - 1); };
+  auto slots_for = [&](int bps, int rep) {
+    return (int)std::min<int64_t>(((int64_t)ctx->max_smem_optin / bps - 2048) / (stride_for(rep) * 8), 16384);
   };
   // a shared table runs at most 5/8 full for the expected groups, 3/4 when it
   // fills a whole SM (one CTA per SM)
   auto fits = [&](int64_t groups, int slots) {
     return slots >= 256 && groups * (blocks_per_sm == 1 ? 4 : 8) <= (int64_t)slots * (blocks_per_sm == 1 ? 3 : 5);
   };
-  int S = slots_for(blocks_per_sm);
   const int64_t expect = std::max<int64_t>(a->hint, a->known_groups);
   const bool smem_ok = env_int("WG_AGG_SMEM", 1) != 0 && a->L.key_words == 1 && !any_null_words && !any_dec_minmax &&
                        expect > 0;
-  if (smem_ok && env_bps == 0 && !fits(expect, S)) {
-    blocks_per_sm = 1;
-    S = slots_for(1);
-    if (!fits(expect, S)) { blocks_per_sm = 2; S = slots_for(2); }
+  // prefer two CTAs per SM, then as many float-SUM copies as still fit
+  int S = 0, rep = 1;
+  bool found = false;
+  for (int bps = 2; bps >= 1 && smem_ok && !found; --bps) {
+    if (env_bps > 0 && bps != env_bps) continue;
+    blocks_per_sm = bps;
+    for (int r = max_rep; r >= 1 && !found; r /= 2)
+      if (fits(expect, slots_for(bps, r))) { S = slots_for(bps, r); rep = r; found = true; }
   }
-  ls.smem = smem_ok && fits(expect, S);
+  if (!found) {
+    blocks_per_sm = env_bps > 0 ? env_bps : 2;
+    S = slots_for(blocks_per_sm, 1);
+  }
+  ls.smem = found;
   ls.P.smem_slots = ls.smem ? S : 0;
-  ls.smem_bytes = ls.smem ? (size_t)S * a->L.slot_words * 8 : 0;
+  ls.P.smem_rep = rep;
+  ls.P.smem_sw = stride_for(rep);
+  ls.smem_bytes = ls.smem ? (size_t)S * ls.P.smem_sw * 8 : 0;
   ls.P.prefetch = std::max(0, env_int("WG_PREFETCH", 2));
   const int64_t want_ctas = (n_items + ls.block - 1) / ls.block + 1;
   ls.grid = (unsigned)std::min<int64_t>((int64_t)ctx->sm_count * blocks_per_sm, want_ctas);
@@ -779,6 +793,9 @@ static wg_status run_device(const PipelineRun& r) {
     c.consumers = std::max(1, std::min(31, env_int("WG_TILE_CONSUMERS", 16)));
     c.stages = std::max(2, std::min(8, env_int("WG_TILE_STAGES", 2)));
     const int64_t budget = (int64_t)ctx->max_smem_optin - 1024;
+    // the tile kernel's shared table keeps one copy of each float SUM
+    ls.P.smem_rep = 1;
+    ls.P.smem_sw = a->L.slot_words;
     const int64_t table_bytes = ls.smem ? (int64_t)S * a->L.slot_words * 8 : 0;
     for (int rows = std::max(64, env_int("WG_TILE_ROWS", 2048) & ~63); rows >= 64; rows /= 2) {
       int64_t off = 0;
@@ -1213,7 +1230,7 @@ __device__ __forceinline__ void batched_item(const Plan& P, const BatchItem& w, 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int S = P.smem_slots;
   if (Sh::smem_ok && S > 0) {
-    smem_table_init(P.L, sm, S, s_groups);
+    smem_table_init(P, sm, S, s_groups);
     __syncthreads();
     const int s_limit = (S * 7) / 8;
     for (int base = warp * 32; base < w.rows; base += nw * 32) {

@@ -85,6 +85,8 @@ struct Plan {
   int32_t smem_slots;            // >0: CTA-private shared-memory table of this many slots
   int32_t shape;                 // compiled query shape (wg_shapes.cuh), 0 = generic
   int32_t prefetch;              // grid-stride iterations of input prefetched into L2 ahead (0 = off)
+  int32_t smem_sw;               // words per shared-table slot (0 = the layout's slot_words)
+  int32_t smem_rep;              // copies of each float SUM in a shared slot (0 or 1 = one)
   DCol in[WG_MAX_IN];
   Pred filt[WG_MAX_FILTERS];
   JoinView join;

@@ -45,6 +45,28 @@ __device__ __forceinline__ Val load_typed(const void* data, int cls, int64_t i) 
   return v;
 }
 
+// The same for input columns read once: streaming loads (evict first), so the
+// stream does not push the join index and the tables out of L2.
+__device__ __forceinline__ Val load_stream(const void* data, int cls, int64_t i) {
+  Val v;
+  v.hi = 0;
+  v.null = false;
+  switch (cls) {
+    case WG_CLS_I32: v.lo = (unsigned long long)(long long)__ldcs((const int32_t*)data + i); break;
+    case WG_CLS_I64: v.lo = (unsigned long long)__ldcs((const long long*)data + i); break;
+    case WG_CLS_F32: v.lo = as_w((double)__ldcs((const float*)data + i)); break;
+    case WG_CLS_F64: v.lo = (unsigned long long)__ldcs((const long long*)data + i); break;
+    case WG_CLS_DEC: {
+      const longlong2 d = __ldcs((const longlong2*)data + i);  // .x = hi, .y = lo
+      v.lo = (unsigned long long)d.y;
+      v.hi = (unsigned long long)d.x;
+      break;
+    }
+    default: v.lo = 0;
+  }
+  return v;
+}
+
 // The same from memory that may be shared (generic loads).
 __device__ __forceinline__ Val load_generic(const char* p, int cls) {
   Val v;
@@ -171,7 +193,7 @@ struct SrcGlobal {
   int64_t row;
   template <class Sh>
   __device__ __forceinline__ Val in(const Plan& P, const Sh& sh, int j) const {
-    Val v = load_typed(P.in[j].data, sh.in_cls(j), row);
+    Val v = load_stream(P.in[j].data, sh.in_cls(j), row);
     v.null = is_null(P.in[j], row);
     return v;
   }
@@ -367,17 +389,28 @@ __device__ __forceinline__ void smem_add_limbs(unsigned* L, int nlimbs, unsigned
 // the low half of its word (a CTA applies fewer than 2^32 rows), integer and
 // DECIMAL sums go limb by limb, and MIN/MAX skip the atomic when the slot
 // already holds a value at least as good (slot values only ever improve).
+// A float SUM has no native shared-memory atomic (it is a compare-and-swap
+// loop that replays while lanes of a warp hit the same hot group), so a shared
+// slot may hold `rep` copies of each float SUM: lane l adds into copy l % rep
+// (copy 0 is the layout's word, copies 1.. follow the slot's regular words),
+// which divides those replays by about `rep`; the flush adds the copies.
 template <int NA, bool SH, class Lay>
 __device__ __forceinline__ void apply(const Lay& ly, unsigned long long* s, const Contrib<NA>& c,
-                                      unsigned long long rows) {
+                                      unsigned long long rows, int rep = 1) {
   if (SH) atomicAdd((unsigned*)(s + ly.key_words()), (unsigned)rows);
   else atomicAdd(s + ly.key_words(), rows);
+  const int copy = SH && rep > 1 ? (int)(threadIdx.x & 31) & (rep - 1) : 0;
+  int nf = 0;  // float SUMs before aggregate a
 #pragma unroll
   for (int a = 0; a < NA; ++a) {
     if (a >= ly.n_aggs()) continue;
     const int kind = ly.agg_kind(a), off = ly.agg_off(a), noff = ly.agg_null_off(a);
     const unsigned long long w0 = c.w0[a], w1 = c.w1[a];
     unsigned long long* t = s + off;
+    if (SH && kind == K_SUM_F64) {
+      if (copy > 0) t = s + ly.slot_words() + nf * (rep - 1) + (copy - 1);
+      ++nf;
+    }
     switch (kind) {
       case K_SUM_I64:
         if (w0) { if (SH) smem_add_limbs((unsigned*)t, 2, w0, 0); else atomicAdd(t, w0); }
@@ -485,6 +518,10 @@ __device__ __forceinline__ unsigned long long* find_global(const Lay& ly, const 
   return nullptr;
 }
 
+// Words per shared slot and copies of each float SUM in it.
+__device__ __forceinline__ int smem_stride(const Plan& P) { return P.smem_sw > 0 ? P.smem_sw : P.L.slot_words; }
+__device__ __forceinline__ int smem_copies(const Plan& P) { return P.smem_rep > 1 ? P.smem_rep : 1; }
+
 // CTA-private shared-memory table (single int64 key, no NULL words). Returns
 // nullptr when the key is absent and the table has reached its fill limit.
 __device__ __forceinline__ unsigned long long* find_smem(unsigned long long* sm, int S, int sw,
@@ -518,9 +555,9 @@ __device__ __forceinline__ void warp_update(const Plan& P, const Sh& sh, bool cu
                                             unsigned long long k1, bool knull, Contrib<NA>& c,
                                             unsigned long long* sm, int* s_groups, int s_limit) {
   if (SMEM && cur && !knull) {
-    unsigned long long* s = find_smem(sm, P.smem_slots, sh.slot_words(), k0, s_groups, s_limit);
+    unsigned long long* s = find_smem(sm, P.smem_slots, smem_stride(P), k0, s_groups, s_limit);
     if (s != nullptr) {
-      apply<NA, true>(sh, s, c, 1ULL);
+      apply<NA, true>(sh, s, c, 1ULL, smem_copies(P));
       cur = false;
     }
   }
@@ -644,23 +681,37 @@ __device__ __forceinline__ void process_rows(const Plan& P, const Sh& sh, const 
   }
 }
 
-__device__ __forceinline__ void smem_table_init(const Layout& L, unsigned long long* sm, int S, int* s_groups) {
-  const int sw = L.slot_words;
-  for (int i = threadIdx.x; i < S * sw; i += blockDim.x) sm[i] = L.init[i % sw];
+// Shared slot of P.smem_sw words: the layout's slot words (empty pattern),
+// then the extra float-SUM copies (+0.0).
+__device__ __forceinline__ void smem_table_init(const Plan& P, unsigned long long* sm, int S, int* s_groups) {
+  const int sw = P.L.slot_words, ssw = smem_stride(P);
+  for (int i = threadIdx.x; i < S * ssw; i += blockDim.x) {
+    const int w = i % ssw;
+    sm[i] = w < sw ? P.L.init[w] : 0ULL;
+  }
   if (threadIdx.x == 0) *s_groups = 0;
 }
 
 template <int NA>
 __device__ __forceinline__ void smem_table_flush(const Plan& P, const unsigned long long* sm, int S) {
   const LayoutAcc ly{P.L};
-  const int sw = P.L.slot_words;
+  const int sw = P.L.slot_words, ssw = smem_stride(P), rep = smem_copies(P);
   for (int i = threadIdx.x; i < S; i += blockDim.x) {
-    const unsigned long long* s = sm + (size_t)i * sw;
+    const unsigned long long* s = sm + (size_t)i * ssw;
     if (s[0] == WG_EMPTY_KEY) continue;
     unsigned long long* g = find_global(ly, P.T, s[0], 0, false, P.err);
     if (g == nullptr) continue;
     Contrib<NA> c;
     slot_contrib<NA>(ly, s, c);
+    int nf = 0;
+#pragma unroll
+    for (int a = 0; a < NA; ++a) {
+      if (a >= P.L.n_aggs || P.L.agg[a].kind != K_SUM_F64) continue;
+      double d = as_f(c.w0[a]);
+      for (int r = 1; r < rep; ++r) d = __dadd_rn(d, as_f(s[sw + nf * (rep - 1) + (r - 1)]));
+      c.w0[a] = as_w(d);
+      ++nf;
+    }
     apply<NA, false>(ly, g, c, s[P.L.key_words]);
   }
 }
@@ -699,7 +750,7 @@ __global__ void __launch_bounds__(Sh::kBlock, Sh::kMinBlocks) pipeline_kernel(co
   const int S = P.smem_slots;
   const int s_limit = (S * 7) / 8;
   if (SMEM) {
-    smem_table_init(P.L, sm, S, &s_groups);
+    smem_table_init(P, sm, S, &s_groups);
     __syncthreads();
   }
   const int lane = threadIdx.x & 31;
@@ -780,7 +831,7 @@ __global__ void __launch_bounds__(544, 1) tile_pipeline_kernel(const __grid_cons
     }
     mbar_init_fence();
   }
-  if (SMEM) smem_table_init(P.L, table, S, &s_groups);
+  if (SMEM) smem_table_init(P, table, S, &s_groups);
   __syncthreads();
 
   if (warp == 0) {

@@ -166,6 +166,22 @@ __global__ void direct_table_kernel(const unsigned long long* slots, uint64_t ca
   }
 }
 
+// Dense direct table: slot (key - base) = {key32, payload32}; slots without a
+// key keep {sentinel, 0} from the fill before this kernel.
+__global__ void dense_table_kernel(DCol key, int64_t n, const uint32_t* pay, long long base,
+                                   unsigned long long* out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    if (is_null(key, i)) continue;
+    const long long k = ld_i64(key, i);
+    out[k - base] = ((unsigned long long)pay[i] << 32) | (uint32_t)(int32_t)k;
+  }
+}
+
+__global__ void fill_u64_kernel(unsigned long long* out, int64_t n, unsigned long long v) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = v;
+}
+
 // Longest chain (max build rows sharing one key): the join's worst fan-out.
 __global__ void join_fanout_kernel(JoinView j, unsigned long long* max_len) {
   const uint64_t cap = j.mask + 1;
@@ -240,6 +256,9 @@ struct wg_join {
   wg::DevBuf dslots;
   bool direct = false;
   int32_t sentinel = 0;
+  bool dense = false;
+  long long dense_base = 0;
+  int64_t dense_slots = 0;
   wg::StagedBatch staged;
 };
 
@@ -351,7 +370,8 @@ wg_status join_view(wg_join* j, wgd::JoinView* v) {
   v->n_pay = (int32_t)j->pay.size();
   v->direct = 0;
   v->sentinel = 0;
-  v->_pad = 0;
+  v->dense = 0;
+  v->base = 0;
   for (size_t i = 0; i < j->pay.size() && i < WG_MAX_PAYLOAD; ++i)
     v->pay[i] = wgd::DCol{j->pay[i].data.get(), j->pay[i].has_valid ? j->pay[i].valid.as<uint64_t>() : nullptr,
                           class_of(j->pay[i].type_id), j->pay[i].scale};
@@ -365,6 +385,11 @@ wg_status join_view_fused(wg_join* j, wgd::JoinView* v) {
     v->slots = j->dslots.get();
     v->direct = 1;
     v->sentinel = j->sentinel;
+    if (j->dense) {
+      v->dense = 1;
+      v->base = j->dense_base;
+      v->mask = (uint64_t)j->dense_slots;
+    }
   }
   return WG_OK;
 }
@@ -466,6 +491,7 @@ wg_status wg_join_build_finish(wg_join* j) {
   // Direct-payload table for the fused probe: unique int32 keys, exactly one
   // 4-byte payload column without NULLs, and an int32 value that is no key.
   j->direct = false;
+  j->dense = false;
   const char* dsw = std::getenv("WG_JOIN_DIRECT");
   if ((!dsw || std::atoi(dsw) != 0) && j->unique && j->flavor == 0 && j->pay.size() == 1 && j->pay[0].es == 4 &&
       !j->pay[0].has_valid && j->rows > 0) {
@@ -482,7 +508,24 @@ wg_status wg_join_build_finish(wg_join* j) {
     if (r[0] > INT32_MIN) j->sentinel = (int32_t)(r[0] - 1);
     else if (r[1] < INT32_MAX) j->sentinel = (int32_t)(r[1] + 1);
     else ok = false;
-    if (ok) {
+    // keys spanning at most 4x the build rows: index by key - min instead of hashing
+    const char* dns = std::getenv("WG_JOIN_DENSE");
+    const int64_t span = r[1] - r[0] + 1;
+    if (ok && (!dns || std::atoi(dns) != 0) && span > 0 && span <= std::max<int64_t>(4 * j->rows, 1024) &&
+        span <= (int64_t(1) << 30)) {
+      WG_TRY(j->dslots.ensure(ctx, span * 8));
+      fill_u64_kernel<<<grid_for(ctx, span, 256), 256, 0, ctx->stream>>>(j->dslots.as<unsigned long long>(), span,
+                                                                          (unsigned long long)(uint32_t)j->sentinel);
+      ctx->count_launch();
+      dense_table_kernel<<<grid_for(ctx, j->rows, 256), 256, 0, ctx->stream>>>(
+          kd, j->rows, j->pay[0].data.as<uint32_t>(), r[0], j->dslots.as<unsigned long long>());
+      ctx->count_launch();
+      WG_CUDA_TRY(cudaGetLastError());
+      j->direct = true;
+      j->dense = true;
+      j->dense_base = r[0];
+      j->dense_slots = span;
+    } else if (ok) {
       WG_TRY(j->dslots.ensure(ctx, (int64_t)cap * 8));
       direct_table_kernel<<<grid_for(ctx, (int64_t)cap, 256), 256, 0, ctx->stream>>>(
           j->slots.as<unsigned long long>(), cap, j->pay[0].data.as<uint32_t>(), j->sentinel,

@@ -34,14 +34,26 @@ struct JoinView {
   // that is not a build key.
   int32_t direct;
   int32_t sentinel;
-  int32_t _pad;
+  // Dense direct table (unique keys spanning a range at most a few times the
+  // build size): slot i holds key base+i, so a probe is one load with no hash
+  // and no probing; `mask` then holds the number of slots.
+  int32_t dense;
+  long long base;
   DCol pay[WG_MAX_PAYLOAD];
 };
 
 // Direct-payload lookup: the payload's raw 32 bits of `key`, or false.
 __device__ __forceinline__ bool join_direct(const JoinView& j, int64_t key, int32_t& out, int32_t* err) {
-  if (key < INT32_MIN || key > INT32_MAX || key == (int64_t)j.sentinel) return false;
   const unsigned long long* s = (const unsigned long long*)j.slots;
+  if (j.dense) {
+    const unsigned long long i = (unsigned long long)(key - j.base);
+    if (i >= j.mask) return false;
+    const unsigned long long v = __ldg(s + i);
+    if ((uint32_t)v != (uint32_t)(int32_t)key) return false;  // an empty slot holds the sentinel key
+    out = (int32_t)(v >> 32);
+    return true;
+  }
+  if (key < INT32_MIN || key > INT32_MAX || key == (int64_t)j.sentinel) return false;
   const uint32_t k32 = (uint32_t)(int32_t)key;
   uint64_t h = fib_slot((uint64_t)key, j.shift);
   for (uint64_t probe = 0; probe <= j.mask; ++probe) {
