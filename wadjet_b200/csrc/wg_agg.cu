@@ -13,7 +13,7 @@
 //  - Low-cardinality int keys use a CTA-private shared-memory table flushed to
 //    the global table at the end of the kernel.
 #include "wg_internal.h"
-#include "wg_shapes.cuh"
+#include "wg_launch.cuh"
 
 #include <algorithm>
 #include <cstdlib>
@@ -33,7 +33,6 @@ using namespace wgd;
 
 namespace {
 
-constexpr int kAggBlock = 512;
 constexpr int64_t kSnapshotMaxBytes = 256LL << 20;
 constexpr double kMaxLoad = 0.75;
 
@@ -486,60 +485,14 @@ static wg_status refresh_groups(wg_agg* a) {
   return WG_OK;
 }
 
-// One launch description (device input already resident).
-struct LaunchSpec {
-  wgd::Plan P;
-  bool smem = false;
-  int block = kAggBlock;
-  unsigned grid = 1;
-  size_t smem_bytes = 0;
-  bool tile = false;          // TMA-staged tile kernel
-  wgd::TileCfg cfg{};
-};
-
-template <int NA, class Sh>
-static void launch_pipeline_t(const LaunchSpec& ls, cudaStream_t st) {
-  const bool smem = Sh::smem_ok && ls.smem;
-  if (ls.tile) {
-    const size_t dyn = (size_t)ls.cfg.table_off + (smem ? (size_t)ls.P.smem_slots * ls.P.L.slot_words * 8 : 0);
-    const unsigned threads = 32u * (1u + (unsigned)ls.cfg.consumers);
-    if constexpr (Sh::smem_ok) {
-      if (smem) {
-        cudaFuncSetAttribute(wgd::tile_pipeline_kernel<NA, true, Sh>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)dyn);
-        wgd::tile_pipeline_kernel<NA, true, Sh><<<ls.grid, threads, dyn, st>>>(ls.P, ls.cfg);
-        return;
-      }
-    }
-    cudaFuncSetAttribute(wgd::tile_pipeline_kernel<NA, false, Sh>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
-    wgd::tile_pipeline_kernel<NA, false, Sh><<<ls.grid, threads, dyn, st>>>(ls.P, ls.cfg);
-    return;
-  }
-  if constexpr (Sh::smem_ok) {
-    if (smem) {
-      cudaFuncSetAttribute(wgd::pipeline_kernel<NA, true, Sh>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)ls.smem_bytes);
-      wgd::pipeline_kernel<NA, true, Sh><<<ls.grid, ls.block, ls.smem_bytes, st>>>(ls.P);
-      return;
-    }
-  }
-  wgd::pipeline_kernel<NA, false, Sh><<<ls.grid, ls.block, 0, st>>>(ls.P);
-}
-
 // Launch on the compiled shape of the plan (ls.P.shape), or the generic kernel.
 static void launch_pipeline_shape(const LaunchSpec& ls, cudaStream_t st) {
-  using namespace wgd;
-  switch (ls.P.shape) {
-    case SHAPE_STARJOIN: launch_pipeline_t<ShapeStarJoin::n_aggs, StatShape<ShapeStarJoin>>(ls, st); return;
-    case SHAPE_GROUPBY: launch_pipeline_t<ShapeGroupBy::n_aggs, StatShape<ShapeGroupBy>>(ls, st); return;
-    case SHAPE_HIGHCARD: launch_pipeline_t<ShapeHighCard::n_aggs, StatShape<ShapeHighCard>>(ls, st); return;
-    case SHAPE_BATCH_I64: launch_pipeline_t<ShapeBatchI64::n_aggs, StatShape<ShapeBatchI64>>(ls, st); return;
-    case SHAPE_BATCH_F64: launch_pipeline_t<ShapeBatchF64::n_aggs, StatShape<ShapeBatchF64>>(ls, st); return;
-    case SHAPE_IPV4: launch_pipeline_t<ShapeIPv4::n_aggs, StatShape<ShapeIPv4>>(ls, st); return;
-    default: break;
+  if (ls.P.shape != wgd::SHAPE_GENERIC) {
+    launch_static_shape(ls, st);
+    return;
   }
-  if (ls.P.L.n_aggs <= 4) launch_pipeline_t<4, DynShape>(ls, st);
-  else launch_pipeline_t<8, DynShape>(ls, st);
+  if (ls.P.L.n_aggs <= 4) launch_pipeline_t<4, wgd::DynShape>(ls, st);
+  else launch_pipeline_t<8, wgd::DynShape>(ls, st);
 }
 
 // The compiled shape to launch a finished plan with; WG_SPECIALIZE=0 forces
@@ -741,9 +694,17 @@ static wg_status run_device(const PipelineRun& r) {
   wgd::Plan probe = ls.P;
   probe.L = launch_layout(a, ls.P);
   const bool stat = pick_shape(probe) != wgd::SHAPE_GENERIC;
+  // vector kernel (U rows per lane): compiled shapes over contiguous input whose
+  // columns start on 16-byte boundaries, no join or the direct-payload one
+  bool vec_ok = stat && ls.P.sel == nullptr && ls.P.n_in > 0 && (!ls.P.has_join || ls.P.join.direct);
+  for (int j = 0; j < ls.P.n_in; ++j) vec_ok = vec_ok && ((uintptr_t)ls.P.in[j].data % 16 == 0);
+  const int vec_env = env_int("WG_VEC", 2);
+  ls.vec = vec_ok && (vec_env == 2 || vec_env == 4) ? vec_env : 0;
+  ls.vec_ctas = env_int("WG_VEC_CTAS", 2) == 3 ? 3 : 2;
   const int env_bps = env_int("WG_AGG_BLOCKS_PER_SM", 0);
-  int blocks_per_sm = env_bps > 0 ? env_bps : 2;
-  ls.block = stat ? wgd::StatShape<wgd::ShapeStarJoin>::kBlock : wgd::DynShape::kBlock;
+  const int pref_bps = env_bps > 0 ? env_bps : ls.vec ? ls.vec_ctas : 2;
+  int blocks_per_sm = pref_bps;
+  ls.block = ls.vec ? 512 : stat ? wgd::StatShape<wgd::ShapeStarJoin>::kBlock : wgd::DynShape::kBlock;
   // copies of each float SUM per shared slot (lane-striped, see apply)
   int n_fsum = 0;
   for (int i = 0; i < a->L.n_aggs; ++i) n_fsum += a->L.agg[i].kind == wgd::K_SUM_F64;
@@ -760,17 +721,19 @@ static wg_status run_device(const PipelineRun& r) {
   const int64_t expect = std::max<int64_t>(a->hint, a->known_groups);
   const bool smem_ok = env_int("WG_AGG_SMEM", 1) != 0 && a->L.key_words == 1 && !any_null_words && !any_dec_minmax &&
                        expect > 0;
-  // prefer two CTAs per SM, then as many float-SUM copies as still fit
+  // prefer the kernel's CTAs per SM, then as many float-SUM copies as still
+  // fit; a table too large for that takes a whole SM (one CTA)
   int S = 0, rep = 1;
   bool found = false;
-  for (int bps = 2; bps >= 1 && smem_ok && !found; --bps) {
-    if (env_bps > 0 && bps != env_bps) continue;
-    blocks_per_sm = bps;
+  const int bps_try[2] = {pref_bps, 1};
+  for (int t = 0; t < 2 && smem_ok && !found; ++t) {
+    if (t == 1 && (env_bps > 0 || pref_bps == 1)) break;
+    blocks_per_sm = bps_try[t];
     for (int r = max_rep; r >= 1 && !found; r /= 2)
-      if (fits(expect, slots_for(bps, r))) { S = slots_for(bps, r); rep = r; found = true; }
+      if (fits(expect, slots_for(blocks_per_sm, r))) { S = slots_for(blocks_per_sm, r); rep = r; found = true; }
   }
   if (!found) {
-    blocks_per_sm = env_bps > 0 ? env_bps : 2;
+    blocks_per_sm = pref_bps;
     S = slots_for(blocks_per_sm, 1);
   }
   ls.smem = found;
@@ -779,7 +742,8 @@ static wg_status run_device(const PipelineRun& r) {
   ls.P.smem_sw = stride_for(rep);
   ls.smem_bytes = ls.smem ? (size_t)S * ls.P.smem_sw * 8 : 0;
   ls.P.prefetch = std::max(0, env_int("WG_PREFETCH", 2));
-  const int64_t want_ctas = (n_items + ls.block - 1) / ls.block + 1;
+  const int64_t rows_per_cta = (int64_t)ls.block * (ls.vec ? ls.vec : 1);
+  const int64_t want_ctas = (n_items + rows_per_cta - 1) / rows_per_cta + 1;
   ls.grid = (unsigned)std::min<int64_t>((int64_t)ctx->sm_count * blocks_per_sm, want_ctas);
   if (!ls.smem && !stat) ls.grid = (unsigned)std::min<int64_t>((int64_t)ctx->sm_count * 4, (n_items + 1023) / 1024 + 1);
 

@@ -720,7 +720,7 @@ __device__ __forceinline__ void smem_table_flush(const Plan& P, const unsigned l
 // chunk this warp reaches `prefetch` iterations later), one 128-byte line per
 // lane, so the column loads of that iteration find their lines in L2 instead
 // of waiting for HBM. Only lines inside the columns are touched.
-template <class Sh>
+template <int ROWS = 32, class Sh>
 __device__ __forceinline__ void prefetch_rows(const Plan& P, const Sh& sh, int64_t row0, int lane) {
   if (row0 >= P.n_items) return;
   int first = 0;
@@ -728,15 +728,16 @@ __device__ __forceinline__ void prefetch_rows(const Plan& P, const Sh& sh, int64
   for (int j = 0; j < WG_MAX_IN; ++j) {
     if (j >= sh.n_in()) break;
     const int es = cls_bytes(sh.in_cls(j));
-    const int lines = es / 4;  // 32 rows x es bytes / 128
-    if (lane >= first && lane < first + lines) {
-      const int64_t row = row0 + (int64_t)(lane - first) * (128 / es);
+    const int lines = ROWS * es / 128;
+    for (int l = lane - first; l < lines; l += 32) {
+      if (l < 0) continue;
+      const int64_t row = row0 + (int64_t)l * (128 / es);
       if (row < P.n_items) {
         const char* p = (const char*)P.in[j].data + row * es;
         asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
       }
     }
-    first += lines;
+    first = (first + lines) & 31;
   }
 }
 
@@ -764,6 +765,150 @@ __global__ void __launch_bounds__(Sh::kBlock, Sh::kMinBlocks) pipeline_kernel(co
     const bool act = item < P.n_items;
     SrcGlobal src{act ? (P.sel ? (int64_t)__ldg(P.sel + item) : item) : 0};
     process_rows<NA, SMEM>(P, sh, src, act, sm, &s_groups, s_limit);
+  }
+  if (SMEM) {
+    __syncthreads();
+    smem_table_flush<NA>(P, sm, S);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Vector variant for compiled shapes: each lane takes U consecutive rows, loads
+// each column's U values with 16-byte (or 8-byte) loads, evaluates all U
+// filters and issues all U join lookups before the first aggregate update, so
+// a warp keeps U times the bytes and lookups in flight of the one-row form.
+// ---------------------------------------------------------------------------
+
+// The input values of one row, held in registers.
+struct SrcRow {
+  Val v[WG_MAX_IN];
+  template <class Sh>
+  __device__ __forceinline__ Val in(const Plan&, const Sh&, int j) const { return v[j]; }
+};
+
+// Rows r0 .. r0+U-1 (r0 a multiple of U, column starts 16-byte aligned): one
+// vector load per 16 bytes when all U rows exist, row by row at the end.
+template <int U, class Sh>
+__device__ __forceinline__ void load_rows(const Plan& P, const Sh& sh, int64_t r0, SrcRow (&rw)[U]) {
+  const bool full = r0 + U <= P.n_items;
+#pragma unroll
+  for (int j = 0; j < WG_MAX_IN; ++j) {
+    if (j >= sh.n_in()) break;
+    const int cls = sh.in_cls(j);
+    const int es = cls_bytes(cls);
+    if (full) {
+      const char* p = (const char*)P.in[j].data + r0 * es;
+      unsigned long long w[2 * U];  // U*es bytes as 64-bit words (es <= 16)
+      const int nbytes = U * es;
+      if (nbytes == 4) {
+        w[0] = (unsigned long long)(uint32_t)__ldcs((const int32_t*)p);
+      } else if (nbytes == 8) {
+        w[0] = (unsigned long long)__ldcs((const long long*)p);
+      } else {
+#pragma unroll
+        for (int q = 0; q < 2 * U; q += 2) {
+          if (q * 8 >= nbytes) break;
+          const longlong2 d = __ldcs((const longlong2*)p + q / 2);
+          w[q] = (unsigned long long)d.x;
+          w[q + 1] = (unsigned long long)d.y;
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        Val& v = rw[u].v[j];
+        v.hi = 0;
+        if (cls == WG_CLS_I32 || cls == WG_CLS_F32) {
+          const uint32_t b = (uint32_t)(w[u >> 1] >> ((u & 1) * 32));
+          v.lo = cls == WG_CLS_I32 ? (unsigned long long)(long long)(int32_t)b : as_w((double)__uint_as_float(b));
+        } else if (cls == WG_CLS_DEC) {
+          v.hi = w[2 * u];      // {int64 hi; uint64 lo}
+          v.lo = w[2 * u + 1];
+        } else {
+          v.lo = w[u];
+        }
+        v.null = is_null(P.in[j], r0 + u);
+      }
+    } else {
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int64_t row = r0 + u;
+        if (row < P.n_items) {
+          rw[u].v[j] = load_stream(P.in[j].data, cls, row);
+          rw[u].v[j].null = is_null(P.in[j], row);
+        } else {
+          rw[u].v[j].lo = 0; rw[u].v[j].hi = 0; rw[u].v[j].null = true;
+        }
+      }
+    }
+  }
+}
+
+// U rows per lane (no join, or the direct-payload join): filters and lookups
+// for all rows first, then one warp-wide update per row.
+template <int NA, bool SMEM, int U, class Sh>
+__device__ __forceinline__ void process_rows_vec(const Plan& P, const Sh& sh, int64_t r0, unsigned long long* sm,
+                                                 int* s_groups, int s_limit) {
+  SrcRow rw[U];
+  load_rows<U>(P, sh, r0, rw);
+  bool act[U];
+  int32_t brow[U];
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    act[u] = r0 + u < P.n_items;
+    brow[u] = -1;
+#pragma unroll
+    for (int f = 0; f < WG_MAX_FILTERS; ++f) {
+      if (f >= sh.n_filters()) break;
+      if (act[u]) act[u] = pred_val(P, sh, f, rw[u].v[sh.filt_col(f)]);
+    }
+  }
+  if (sh.has_join()) {
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const Val kv = rw[u].v[sh.probe_col()];
+      if (act[u]) act[u] = !kv.null && join_direct(P.join, (int64_t)kv.lo, brow[u], P.err);
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    if (!__any_sync(WG_FULL_MASK, act[u])) continue;
+    unsigned long long k0 = 0, k1 = 0;
+    bool knull = false;
+    Contrib<NA> c;
+    bool cur = act[u];
+    if (cur) {
+      ExprVals ev;
+      eval_exprs(P, sh, rw[u], brow[u], ev);
+      cur = make_key(P, sh, rw[u], brow[u], ev, k0, k1, knull);
+      make_contrib<NA>(P, sh, rw[u], brow[u], ev, c);
+    } else {
+#pragma unroll
+      for (int a = 0; a < NA; ++a) { c.w0[a] = 0; c.w1[a] = 0; c.nul[a] = 0; }
+    }
+    warp_update<NA, SMEM>(P, sh, cur, k0, k1, knull, c, sm, s_groups, s_limit);
+  }
+}
+
+// Grid-stride over chunks of 32*U rows; MB CTAs of 512 threads per SM.
+template <int NA, bool SMEM, class Sh, int U, int MB>
+__global__ void __launch_bounds__(512, MB) pipeline_vec_kernel(const __grid_constant__ Plan P) {
+  static_assert(U == 2 || U == 4, "rows per lane");
+  extern __shared__ unsigned long long sm[];
+  __shared__ int s_groups;
+  const Sh sh{P};
+  const int S = P.smem_slots;
+  const int s_limit = (S * 7) / 8;
+  if (SMEM) {
+    smem_table_init(P, sm, S, &s_groups);
+    __syncthreads();
+  }
+  const int lane = threadIdx.x & 31;
+  const int64_t wpb = blockDim.x >> 5;
+  const int64_t step = (int64_t)gridDim.x * wpb * 32 * U;
+  const int64_t ahead = (int64_t)P.prefetch * step;
+  for (int64_t base = ((int64_t)blockIdx.x * wpb + (threadIdx.x >> 5)) * 32 * U; base < P.n_items; base += step) {
+    if (ahead > 0) prefetch_rows<32 * U>(P, sh, base + ahead, lane);
+    process_rows_vec<NA, SMEM, U>(P, sh, base + (int64_t)lane * U, sm, &s_groups, s_limit);
   }
   if (SMEM) {
     __syncthreads();
