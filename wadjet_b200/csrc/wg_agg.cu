@@ -26,6 +26,7 @@ int32_t join_n_payload(wg_join* j);
 int32_t join_payload_type(wg_join* j, int i);
 int32_t join_payload_scale(wg_join* j, int i);
 bool join_payload_nullable(wg_join* j, int i);
+bool join_payload_range(wg_join* j, int i, long long* lo, long long* hi);
 int64_t join_max_fanout(wg_join* j);
 }  // namespace wg
 
@@ -709,7 +710,9 @@ static wg_status run_device(const PipelineRun& r) {
   int n_fsum = 0;
   for (int i = 0; i < a->L.n_aggs; ++i) n_fsum += a->L.agg[i].kind == wgd::K_SUM_F64;
   const int max_rep = n_fsum > 0 ? std::max(1, std::min(8, env_int("WG_SMEM_REPLICAS", 4))) : 1;
-  auto stride_for = [&](int rep) { return a->L.slot_words + n_fsum * (rep - 1); };
+  // an odd number of 8-byte words per shared slot spreads the slots over all
+  // 16 bank pairs (an even stride maps them onto a few)
+  auto stride_for = [&](int rep) { return (a->L.slot_words + n_fsum * (rep - 1)) | 1; };
   auto slots_for = [&](int bps, int rep) {
     return (int)std::min<int64_t>(((int64_t)ctx->max_smem_optin / bps - 2048) / (stride_for(rep) * 8), 16384);
   };
@@ -736,12 +739,42 @@ static wg_status run_device(const PipelineRun& r) {
     blocks_per_sm = pref_bps;
     S = slots_for(blocks_per_sm, 1);
   }
+  // dense GROUP BY: the key is a join payload column whose value range is known
+  // and small, so the shared table is indexed by key - min (no hashing, no key
+  // compare, no insert) and holds exactly one slot per possible key
+  {
+    long long glo = 0, ghi = -1;
+    const int kv = ls.P.L.key_vcol[0];
+    const int npay = r.join ? join_n_payload(r.join) : 0;
+    const bool cand = smem_ok && env_int("WG_GROUP_DENSE", 1) != 0 && a->L.n_keys == 1 && r.join != nullptr &&
+                      kv >= ls.P.n_in && kv < ls.P.n_in + npay &&
+                      join_payload_range(r.join, kv - ls.P.n_in, &glo, &ghi) && ghi >= glo && ghi - glo < 16384;
+    bool placed = false;
+    for (int t = 0; t < 2 && cand && !placed; ++t) {
+      if (t == 1 && (env_bps > 0 || pref_bps == 1)) break;
+      const int bps = bps_try[t];
+      const int64_t budget = (int64_t)ctx->max_smem_optin / bps - 2048;
+      for (int r2 = max_rep; r2 >= 1 && !placed; r2 /= 2)
+        if ((ghi - glo + 1) * stride_for(r2) * 8 <= budget) {
+          blocks_per_sm = bps;
+          rep = r2;
+          S = (int)(ghi - glo + 1);
+          placed = true;
+        }
+    }
+    if (placed) {
+      found = true;
+      ls.P.gdense = 1;
+      ls.P.gmin = glo;
+    }
+  }
   ls.smem = found;
   ls.P.smem_slots = ls.smem ? S : 0;
   ls.P.smem_rep = rep;
   ls.P.smem_sw = stride_for(rep);
   ls.smem_bytes = ls.smem ? (size_t)S * ls.P.smem_sw * 8 : 0;
   ls.P.prefetch = std::max(0, env_int("WG_PREFETCH", 2));
+  ls.P.smem_combine = env_int("WG_SMEM_COMBINE", 0) != 0;
   const int64_t rows_per_cta = (int64_t)ls.block * (ls.vec ? ls.vec : 1);
   const int64_t want_ctas = (n_items + rows_per_cta - 1) / rows_per_cta + 1;
   ls.grid = (unsigned)std::min<int64_t>((int64_t)ctx->sm_count * blocks_per_sm, want_ctas);
@@ -757,8 +790,13 @@ static wg_status run_device(const PipelineRun& r) {
     c.consumers = std::max(1, std::min(31, env_int("WG_TILE_CONSUMERS", 16)));
     c.stages = std::max(2, std::min(8, env_int("WG_TILE_STAGES", 2)));
     const int64_t budget = (int64_t)ctx->max_smem_optin - 1024;
-    // the tile kernel's shared table keeps one copy of each float SUM
+    // the tile kernel's shared table keeps one copy of each float SUM and hashes
     ls.P.smem_rep = 1;
+    if (ls.P.gdense) {
+      ls.P.gdense = 0;
+      ls.smem = smem_ok && fits(expect, S);
+      ls.P.smem_slots = ls.smem ? S : 0;
+    }
     ls.P.smem_sw = a->L.slot_words;
     const int64_t table_bytes = ls.smem ? (int64_t)S * a->L.slot_words * 8 : 0;
     for (int rows = std::max(64, env_int("WG_TILE_ROWS", 2048) & ~63); rows >= 64; rows /= 2) {
@@ -830,7 +868,7 @@ static wg_status run_device(const PipelineRun& r) {
       WG_TRY(rebuild_table(a, a->cap * 4, a->L));
       WG_TRY(refresh_groups(a));
       const int64_t expect2 = std::max<int64_t>(a->hint, a->known_groups);
-      if (ls.smem && !fits(expect2, S)) { ls.smem = false; ls.P.smem_slots = 0; ls.smem_bytes = 0; }
+      if (ls.smem && !ls.P.gdense && !fits(expect2, S)) { ls.smem = false; ls.P.smem_slots = 0; ls.smem_bytes = 0; }
       if (table_words(a, a->cap) * 8 > kSnapshotMaxBytes) break;
     }
   }

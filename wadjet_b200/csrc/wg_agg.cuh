@@ -87,6 +87,10 @@ struct Plan {
   int32_t prefetch;              // grid-stride iterations of input prefetched into L2 ahead (0 = off)
   int32_t smem_sw;               // words per shared-table slot (0 = the layout's slot_words)
   int32_t smem_rep;              // copies of each float SUM in a shared slot (0 or 1 = one)
+  int32_t smem_combine;          // 1: lanes of a warp combine rows of one group before the shared atomics
+  int32_t gdense;                // 1: the shared table is indexed by key - gmin (keys known to lie in
+                                 //    [gmin, gmin + smem_slots)), no hashing and no key words
+  long long gmin;
   DCol in[WG_MAX_IN];
   Pred filt[WG_MAX_FILTERS];
   JoinView join;

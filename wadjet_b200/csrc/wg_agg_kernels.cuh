@@ -543,19 +543,32 @@ __device__ __forceinline__ unsigned long long* find_smem(unsigned long long* sm,
   return nullptr;
 }
 
-// Update of one row per lane. With a CTA-private shared-memory table each lane
-// applies its own row there with shared-memory atomics (cheaper than combining
-// first). Rows bound for the HBM table (no shared table, a NULL key, or a
-// shared table at its fill limit) are combined first: lanes holding the same
-// key pre-combine their contributions (__match_any_sync) and only the group's
-// lowest lane touches the table, so a hot key costs one set of global atomics
-// per warp instead of one per row.
+// The shared slot of key k0: direct (k0 - gmin) when the keys' range is known
+// and fits the table, else the hashed table.
+__device__ __forceinline__ unsigned long long* find_shared(const Plan& P, unsigned long long* sm, unsigned long long k0,
+                                                           int* s_groups, int s_limit) {
+  if (P.gdense) {
+    const unsigned long long d = k0 - (unsigned long long)P.gmin;
+    return d < (unsigned long long)P.smem_slots ? sm + d * smem_stride(P) : nullptr;
+  }
+  return find_smem(sm, P.smem_slots, smem_stride(P), k0, s_groups, s_limit);
+}
+
+// Update of one row per lane. Rows bound for the HBM table (no shared table, a
+// NULL key, or a shared table at its fill limit) are combined first: lanes
+// holding the same key pre-combine their contributions (__match_any_sync) and
+// only the group's lowest lane touches the table, so a hot key costs one set
+// of global atomics per warp instead of one per row. With a CTA-private
+// shared-memory table each lane applies its own row there with shared-memory
+// atomics, or, when P.smem_combine is set, the lanes combine first there too
+// (fewer atomics on a hot group's words at the price of the shuffles).
 template <int NA, bool SMEM, class Sh>
 __device__ __forceinline__ void warp_update(const Plan& P, const Sh& sh, bool cur, unsigned long long k0,
                                             unsigned long long k1, bool knull, Contrib<NA>& c,
                                             unsigned long long* sm, int* s_groups, int s_limit) {
-  if (SMEM && cur && !knull) {
-    unsigned long long* s = find_smem(sm, P.smem_slots, smem_stride(P), k0, s_groups, s_limit);
+  const bool combine_first = SMEM && P.smem_combine != 0;
+  if (SMEM && !combine_first && cur && !knull) {
+    unsigned long long* s = find_shared(P, sm, k0, s_groups, s_limit);
     if (s != nullptr) {
       apply<NA, true>(sh, s, c, 1ULL, smem_copies(P));
       cur = false;
@@ -591,6 +604,13 @@ __device__ __forceinline__ void warp_update(const Plan& P, const Sh& sh, bool cu
     }
   }
   if (leader) {
+    if (combine_first && !knull) {
+      unsigned long long* s = find_shared(P, sm, k0, s_groups, s_limit);
+      if (s != nullptr) {
+        apply<NA, true>(sh, s, c, (unsigned long long)mysz, smem_copies(P));
+        return;
+      }
+    }
     unsigned long long* s = find_global(sh, P.T, k0, k1, knull, P.err);
     if (s != nullptr) apply<NA, false>(sh, s, c, (unsigned long long)mysz);
   }
@@ -698,8 +718,14 @@ __device__ __forceinline__ void smem_table_flush(const Plan& P, const unsigned l
   const int sw = P.L.slot_words, ssw = smem_stride(P), rep = smem_copies(P);
   for (int i = threadIdx.x; i < S; i += blockDim.x) {
     const unsigned long long* s = sm + (size_t)i * ssw;
-    if (s[0] == WG_EMPTY_KEY) continue;
-    unsigned long long* g = find_global(ly, P.T, s[0], 0, false, P.err);
+    unsigned long long key = s[0];
+    if (P.gdense) {  // a direct slot is in use once it counted a row
+      if (s[P.L.key_words] == 0) continue;
+      key = (unsigned long long)P.gmin + (unsigned long long)i;
+    } else if (key == WG_EMPTY_KEY) {
+      continue;
+    }
+    unsigned long long* g = find_global(ly, P.T, key, 0, false, P.err);
     if (g == nullptr) continue;
     Contrib<NA> c;
     slot_contrib<NA>(ly, s, c);

@@ -259,6 +259,9 @@ struct wg_join {
   bool dense = false;
   long long dense_base = 0;
   int64_t dense_slots = 0;
+  // value range of each integer payload column without NULLs (for dense GROUP BY)
+  std::vector<long long> pay_lo, pay_hi;
+  std::vector<bool> pay_range;
   wg::StagedBatch staged;
 };
 
@@ -398,6 +401,12 @@ int32_t join_n_payload(wg_join* j) { return (int32_t)j->pay.size(); }
 int32_t join_payload_type(wg_join* j, int i) { return j->pay[i].type_id; }
 int32_t join_payload_scale(wg_join* j, int i) { return j->pay[i].scale; }
 bool join_payload_nullable(wg_join* j, int i) { return j->pay[i].has_valid; }
+bool join_payload_range(wg_join* j, int i, long long* lo, long long* hi) {
+  if (i < 0 || i >= (int)j->pay_range.size() || !j->pay_range[i]) return false;
+  *lo = j->pay_lo[i];
+  *hi = j->pay_hi[i];
+  return true;
+}
 bool join_unique(wg_join* j) { return j->unique; }
 int64_t join_max_fanout(wg_join* j) { return j->max_fanout; }
 
@@ -487,6 +496,26 @@ wg_status wg_join_build_finish(wg_join* j) {
     int64_t mf = 1;
     WG_TRY(read_back_i64(ctx, j->scratch.as<int64_t>(), &mf, 1));
     j->max_fanout = std::max<int64_t>(1, mf);
+  }
+  // value range of the integer payload columns without NULLs
+  j->pay_lo.assign(j->pay.size(), 0);
+  j->pay_hi.assign(j->pay.size(), 0);
+  j->pay_range.assign(j->pay.size(), false);
+  for (size_t p = 0; p < j->pay.size() && j->rows > 0; ++p) {
+    const int cls = class_of(j->pay[p].type_id);
+    if (j->pay[p].has_valid || (cls != WG_CLS_I32 && cls != WG_CLS_I64)) continue;
+    long long* mm = (long long*)(j->scratch.as<char>() + 32);
+    const long long init[2] = {LLONG_MAX, LLONG_MIN};
+    WG_CUDA_TRY(cudaMemcpyAsync(mm, init, 16, cudaMemcpyHostToDevice, ctx->stream));
+    wgd::DCol pd{j->pay[p].data.get(), nullptr, cls, 0};
+    key_range_kernel<<<grid_for(ctx, j->rows, 256), 256, 0, ctx->stream>>>(pd, j->rows, mm, mm + 1);
+    ctx->count_launch();
+    WG_CUDA_TRY(cudaGetLastError());
+    int64_t r[2];
+    WG_TRY(read_back_i64(ctx, (const int64_t*)mm, r, 2));
+    j->pay_lo[p] = r[0];
+    j->pay_hi[p] = r[1];
+    j->pay_range[p] = true;
   }
   // Direct-payload table for the fused probe: unique int32 keys, exactly one
   // 4-byte payload column without NULLs, and an int32 value that is no key.
