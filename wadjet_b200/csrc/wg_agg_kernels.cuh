@@ -742,30 +742,36 @@ __device__ __forceinline__ void smem_table_flush(const Plan& P, const unsigned l
   }
 }
 
-// Ask L2 for the input lines of the 32 rows starting at row0 (the grid-stride
-// chunk this warp reaches `prefetch` iterations later), one 128-byte line per
-// lane, so the column loads of that iteration find their lines in L2 instead
-// of waiting for HBM. Only lines inside the columns are touched.
-template <int ROWS = 32, class Sh>
-__device__ __forceinline__ void prefetch_rows(const Plan& P, const Sh& sh, int64_t row0, int lane) {
-  if (row0 >= P.n_items) return;
-  int first = 0;
+// One lane's share of the L2 prefetch of a grid-stride loop over chunks of
+// ROWS rows: the lane's 128-byte line of one column, fixed for the whole loop
+// (set up once, then one compare, one add and one prefetch per iteration).
+template <int ROWS>
+struct Prefetcher {
+  const char* p = nullptr;   // next line to prefetch (nullptr: this lane has none)
+  const char* end = nullptr;
+  int64_t step = 0;          // bytes between this lane's lines in consecutive iterations
+  template <class Sh>
+  __device__ __forceinline__ void init(const Plan& P, const Sh& sh, int64_t first_row, int64_t rows_per_iter,
+                                       int lane) {
+    int first = 0;
 #pragma unroll
-  for (int j = 0; j < WG_MAX_IN; ++j) {
-    if (j >= sh.n_in()) break;
-    const int es = cls_bytes(sh.in_cls(j));
-    const int lines = ROWS * es / 128;
-    for (int l = lane - first; l < lines; l += 32) {
-      if (l < 0) continue;
-      const int64_t row = row0 + (int64_t)l * (128 / es);
-      if (row < P.n_items) {
-        const char* p = (const char*)P.in[j].data + row * es;
-        asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+    for (int j = 0; j < WG_MAX_IN; ++j) {
+      if (j >= sh.n_in()) break;
+      const int es = cls_bytes(sh.in_cls(j));
+      const int lines = ROWS * es / 128;
+      if (lane >= first && lane < first + lines) {
+        p = (const char*)P.in[j].data + first_row * es + (int64_t)(lane - first) * 128;
+        end = (const char*)P.in[j].data + P.n_items * es;
+        step = rows_per_iter * es;
       }
+      first += lines;
     }
-    first = (first + lines) & 31;
   }
-}
+  __device__ __forceinline__ void next() {
+    if (p != nullptr && p < end) asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+    p += step;
+  }
+};
 
 // The fused pipeline reading HBM directly: one warp per 32 consecutive rows
 // (or selection-vector entries), grid-stride.
@@ -784,9 +790,11 @@ __global__ void __launch_bounds__(Sh::kBlock, Sh::kMinBlocks) pipeline_kernel(co
   const int64_t wpb = blockDim.x >> 5;
   const int64_t total_warps = (int64_t)gridDim.x * wpb;
   const int64_t ahead = (int64_t)P.prefetch * total_warps * 32;
-  for (int64_t base = ((int64_t)blockIdx.x * wpb + (threadIdx.x >> 5)) * 32; base < P.n_items;
-       base += total_warps * 32) {
-    if (ahead > 0 && P.sel == nullptr) prefetch_rows(P, sh, base + ahead, lane);
+  const int64_t base0 = ((int64_t)blockIdx.x * wpb + (threadIdx.x >> 5)) * 32;
+  Prefetcher<32> pf;
+  if (ahead > 0 && P.sel == nullptr) pf.init(P, sh, base0 + ahead, total_warps * 32, lane);
+  for (int64_t base = base0; base < P.n_items; base += total_warps * 32) {
+    pf.next();
     const int64_t item = base + lane;
     const bool act = item < P.n_items;
     SrcGlobal src{act ? (P.sel ? (int64_t)__ldg(P.sel + item) : item) : 0};
@@ -932,8 +940,11 @@ __global__ void __launch_bounds__(512, MB) pipeline_vec_kernel(const __grid_cons
   const int64_t wpb = blockDim.x >> 5;
   const int64_t step = (int64_t)gridDim.x * wpb * 32 * U;
   const int64_t ahead = (int64_t)P.prefetch * step;
-  for (int64_t base = ((int64_t)blockIdx.x * wpb + (threadIdx.x >> 5)) * 32 * U; base < P.n_items; base += step) {
-    if (ahead > 0) prefetch_rows<32 * U>(P, sh, base + ahead, lane);
+  const int64_t base0 = ((int64_t)blockIdx.x * wpb + (threadIdx.x >> 5)) * 32 * U;
+  Prefetcher<32 * U> pf;
+  if (ahead > 0) pf.init(P, sh, base0 + ahead, step, lane);
+  for (int64_t base = base0; base < P.n_items; base += step) {
+    pf.next();
     process_rows_vec<NA, SMEM, U>(P, sh, base + (int64_t)lane * U, sm, &s_groups, s_limit);
   }
   if (SMEM) {

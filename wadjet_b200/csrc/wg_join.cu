@@ -142,7 +142,9 @@ __global__ void join_probe_emit_kernel(const ProbeArgs a) {
   }
 }
 
-// Smallest and largest non-NULL build key (to pick a sentinel that is not a key).
+// Smallest and largest non-NULL value of an integer column (the build key's,
+// to pick a sentinel that is not a key; a payload's, for dense GROUP BY).
+// Reduced per warp and per CTA, then one atomic pair per CTA.
 __global__ void key_range_kernel(DCol key, int64_t n, long long* mn, long long* mx) {
   long long lo = LLONG_MAX, hi = LLONG_MIN;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -151,8 +153,28 @@ __global__ void key_range_kernel(DCol key, int64_t n, long long* mn, long long* 
     lo = k < lo ? k : lo;
     hi = k > hi ? k : hi;
   }
-  atomicMin(mn, lo);
-  atomicMax(mx, hi);
+  for (int o = 16; o > 0; o >>= 1) {
+    const long long l2 = __shfl_down_sync(WG_FULL_MASK, lo, o), h2 = __shfl_down_sync(WG_FULL_MASK, hi, o);
+    lo = l2 < lo ? l2 : lo;
+    hi = h2 > hi ? h2 : hi;
+  }
+  __shared__ long long s_lo[32], s_hi[32];
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = (blockDim.x + 31) >> 5;
+  if (l == 0) { s_lo[w] = lo; s_hi[w] = hi; }
+  __syncthreads();
+  if (w == 0) {
+    lo = l < nw ? s_lo[l] : LLONG_MAX;
+    hi = l < nw ? s_hi[l] : LLONG_MIN;
+    for (int o = 16; o > 0; o >>= 1) {
+      const long long l2 = __shfl_down_sync(WG_FULL_MASK, lo, o), h2 = __shfl_down_sync(WG_FULL_MASK, hi, o);
+      lo = l2 < lo ? l2 : lo;
+      hi = h2 > hi ? h2 : hi;
+    }
+    if (l == 0) {
+      atomicMin(mn, lo);
+      atomicMax(mx, hi);
+    }
+  }
 }
 
 // Rewrite a unique-key table as {key32, payload32} slots (empty = sentinel key).
