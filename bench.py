@@ -42,6 +42,10 @@ FACT_BYTES_PER_ROW = 4 + 4 + 16 + 8      # fk, qty, price (Int128), disc
 DIM_BYTES_PER_ROW = 4 + 4                # key, grp
 GROUP_STATE_BYTES = 8 + 8 + 16 + 8       # key, rows, SUM f64, SUM Int128
 CPU_SAMPLE_ROWS = 1 << 24
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one fused-kernel launch per fact row,
+# from an ncu capture of the 2^24-row case (600.5 MB / 2^24 rows), scaled by the rows of a launch:
+# profiles/pipeline_vec_kernel_starjoin_2p24.md
+NCU_TRAFFIC_BYTES_PER_FACT_ROW = 600.49e6 / (1 << 24)
 METRIC = "rows/s (filter+join+hash-agg, star join 2^28 fact rows)"
 
 
@@ -330,7 +334,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                        "parallelism": f"dp{world}" if world > 1 else "single",
                        "l2": "inputs (8.6 GB/rank) larger than L2; no flush"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": (achieved / peak) if achieved else None, "traffic": None,
+                         "frac": (achieved / peak) if achieved else None,
+                         "traffic": NCU_TRAFFIC_BYTES_PER_FACT_ROW * n,
+                         "traffic_source": "ncu capture at 2^24 fact rows scaled to this launch's rows",
                          "kernel": "pipeline_kernel", "kernel_ms": k_ms, "algorithmic_bytes": alg_bytes,
                          "peak_kind": peak_kind},
             "cpu_baseline": cpu,
