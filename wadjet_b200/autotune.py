@@ -87,7 +87,11 @@ def tune(ctx, nq: int, max_rows: int, grid=None, log=print) -> dict:
     names = list(grid)
     for combo in itertools.product(*[grid[k] for k in names]):
         p = dict(zip(names, combo))
-        ms = time_params(ctx, qs, wg.TuneParams(**p))
+        try:
+            ms = time_params(ctx, qs, wg.TuneParams(**p))
+        except wg.WadjetGPUError as e:  # a shape this device cannot launch: skip it
+            log(json.dumps({"params": p, "skipped": str(e)}))
+            continue
         results.append({"params": p, "ms": ms})
         log(json.dumps(results[-1]))
     best = min(results, key=lambda r: r["ms"])

@@ -1324,7 +1324,11 @@ static wg_status batched_plan(wg_batched* b) {
     const int64_t smax = b->tp.smem_max_groups;
     int S = 0;
     if (plain && a->hint > 0 && a->hint <= smax) {
-      S = (int)std::max<int64_t>(256, std::min<int64_t>(16384, a->hint * 2));
+      // at most the shared memory one CTA may take; a table that would then run
+      // more than 3/4 full stays in HBM
+      const int64_t fit = ((int64_t)ctx->max_smem_optin - 1024) / (a->L.slot_words * 8);
+      S = (int)std::min<int64_t>(fit, std::max<int64_t>(256, std::min<int64_t>(16384, a->hint * 2)));
+      if ((int64_t)S * 3 < a->hint * 4) S = 0;
       max_smem_words = std::max<int64_t>(max_smem_words, (int64_t)S * a->L.slot_words);
     }
     P.smem_slots = S;
