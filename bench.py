@@ -591,7 +591,9 @@ def run_serving(args):
         "workload": "serving", "metric": "queries/s", "offered_qps": args.qps, "requests": n_req,
         "value": cont["qps"], "unit": "queries/s", "slots": args.slots,
         "p50_ms": 1e3 * cont["p50_s"], "p99_ms": 1e3 * cont["p99_s"],
-        "plain": {"qps": plain["qps"], "p50_ms": 1e3 * plain["p50_s"], "p99_ms": 1e3 * plain["p99_s"]},
+        "mean_service_ms": 1e3 * cont["mean_service_s"], "mean_queue_ms": 1e3 * cont["mean_queue_s"],
+        "plain": {"qps": plain["qps"], "p50_ms": 1e3 * plain["p50_s"], "p99_ms": 1e3 * plain["p99_s"],
+                  "mean_service_ms": 1e3 * plain["mean_service_s"]},
         "mean_rows_per_request": float(sizes.mean()), "templates": ["groupby", "join+agg", "ipv4 /24"]}),
         flush=True)
     join.close()

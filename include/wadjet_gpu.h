@@ -435,6 +435,8 @@ typedef struct wg_serve_stats {
   int64_t submitted, completed, failed, in_flight, queued;
   double  p50_s, p99_s, mean_s, max_s;   /* latency = completion - submission */
   double  qps;                           /* completed / (last completion - first submission) */
+  double  mean_queue_s;                  /* mean time from submission to a slot starting the request */
+  double  mean_service_s;                /* mean time a slot spent on a request (run + finalize) */
 } wg_serve_stats;
 
 WG_API wg_status wg_server_create(wg_ctx* ctx, int32_t n_slots, wg_server** out);

@@ -88,7 +88,8 @@ class wg_serve_request(C.Structure):
 class wg_serve_stats(C.Structure):
     _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("failed", C.c_int64),
                 ("in_flight", C.c_int64), ("queued", C.c_int64), ("p50_s", C.c_double), ("p99_s", C.c_double),
-                ("mean_s", C.c_double), ("max_s", C.c_double), ("qps", C.c_double)]
+                ("mean_s", C.c_double), ("max_s", C.c_double), ("qps", C.c_double),
+                ("mean_queue_s", C.c_double), ("mean_service_s", C.c_double)]
 
 
 P = C.c_void_p

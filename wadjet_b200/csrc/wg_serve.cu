@@ -81,6 +81,7 @@ struct wg_server {
   bool stop = false;
   int64_t submitted = 0, completed = 0, failed = 0, running = 0;
   std::vector<double> lat;
+  double queue_sum = 0, service_sum = 0;
   double t_first = -1, t_last = 0;
 };
 
@@ -161,6 +162,8 @@ void worker_main(wg_server* s, int slot_idx) {
       if (r->status == WG_OK) {
         ++s->completed;
         s->lat.push_back(r->t_done - r->t_submit);
+        s->queue_sum += r->t_start - r->t_submit;
+        s->service_sum += r->t_done - r->t_start;
         s->t_last = std::max(s->t_last, r->t_done);
       } else {
         ++s->failed;
@@ -308,6 +311,8 @@ wg_status wg_server_stats(wg_server* s, wg_serve_stats* o) {
   o->mean_s = s->lat.empty() ? 0.0 : sum / (double)s->lat.size();
   o->max_s = mx;
   o->qps = (s->completed > 0 && s->t_last > s->t_first) ? (double)s->completed / (s->t_last - s->t_first) : 0.0;
+  o->mean_queue_s = s->lat.empty() ? 0.0 : s->queue_sum / (double)s->lat.size();
+  o->mean_service_s = s->lat.empty() ? 0.0 : s->service_sum / (double)s->lat.size();
   return WG_OK;
 }
 
@@ -315,6 +320,7 @@ wg_status wg_server_reset_stats(wg_server* s) {
   if (!s) return fail(WG_E_INVALID, "server is NULL");
   std::lock_guard<std::mutex> lk(s->mu);
   s->lat.clear();
+  s->queue_sum = s->service_sum = 0;
   s->completed = s->failed = s->submitted = 0;
   s->t_first = -1;
   s->t_last = 0;
