@@ -536,10 +536,14 @@ def run_serving(args):
 
     def drive(slots):
         srv = wg.Server(ctx, slots)
-        for i in range(min(24, n_req)):  # warm the per-slot pools
-            tk = srv.submit(**specs[i])
-            srv.wait(tk)
-            srv.release(tk)
+        # warm the per-slot pools: waves of requests held together, so each slot keeps
+        # several finished aggregates of every template for reuse
+        for wave in range(4):
+            held = [srv.submit(**specs[(wave * 3 * slots + i) % n_req]) for i in range(3 * slots)]
+            for tk in held:
+                srv.wait(tk)
+            for tk in held:
+                srv.release(tk)
         srv.reset_stats()
         tickets = []
         lock = threading.Lock()

@@ -284,7 +284,9 @@ wg_status wg_server_release(wg_server* s, int64_t ticket) {
     if (!it->second->done) return fail(WG_E_STATE, "request still running");
     r = it->second;
     s->reqs.erase(it);
-    if (r->agg && r->status == WG_OK && s->pool.size() < 4 * s->slots.size()) {
+    // keep enough finished aggregates that a slot rarely has to allocate a new
+    // one while the previous result of the same shape is still held
+    if (r->agg && r->status == WG_OK && s->pool.size() < 16 * s->slots.size()) {
       s->pool.push_back(Pooled{r->agg, r->slot, r->keys, r->aggs, r->hint});
       r->agg = nullptr;
     }
