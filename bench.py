@@ -534,7 +534,7 @@ def run_serving(args):
     sizes = (np.exp(prng.uniform(np.log(1e5), np.log(1e8), n_req)) // 64 * 64).astype(np.int64)
     specs = [request(int(t), int(n)) for t, n in zip(kinds, sizes)]
 
-    def drive(slots):
+    def drive(slots, gaps):
         srv = wg.Server(ctx, slots)
         # warm the per-slot pools: waves of requests held together, so each slot keeps
         # several finished aggregates of every template for reuse
@@ -589,8 +589,12 @@ def run_serving(args):
         return st
 
     sys.setswitchinterval(2e-4)  # the submitting and completing threads hand over quickly
-    cont = drive(args.slots)
-    plain = drive(1)
+    cont = drive(args.slots, gaps)
+    plain = drive(1, gaps)
+    # capacity: the same requests all queued at once (the server runs saturated)
+    burst = np.zeros(min(n_req, 4000))
+    cont_sat = drive(args.slots, burst)
+    plain_sat = drive(1, burst)
     print(json.dumps({
         "workload": "serving", "metric": "queries/s", "offered_qps": args.qps, "requests": n_req,
         "value": cont["qps"], "unit": "queries/s", "slots": args.slots,
@@ -598,6 +602,9 @@ def run_serving(args):
         "mean_service_ms": 1e3 * cont["mean_service_s"], "mean_queue_ms": 1e3 * cont["mean_queue_s"],
         "plain": {"qps": plain["qps"], "p50_ms": 1e3 * plain["p50_s"], "p99_ms": 1e3 * plain["p99_s"],
                   "mean_service_ms": 1e3 * plain["mean_service_s"]},
+        "capacity_qps": {"served": cont_sat["qps"], "plain": plain_sat["qps"],
+                         "served_mean_service_ms": 1e3 * cont_sat["mean_service_s"],
+                         "plain_mean_service_ms": 1e3 * plain_sat["mean_service_s"]},
         "mean_rows_per_request": float(sizes.mean()), "templates": ["groupby", "join+agg", "ipv4 /24"]}),
         flush=True)
     join.close()
