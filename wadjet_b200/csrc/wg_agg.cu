@@ -538,6 +538,7 @@ struct PipelineRun {
   wg_join* join;
   int32_t n_exprs;
   const wg_expr* exprs;
+  bool no_partition = false;    // set on the reordered copy (hash partitioning runs once)
 };
 
 namespace wg {
@@ -668,6 +669,9 @@ static wg_status build_plan(const PipelineRun& r, wgd::Plan& P, VSchema& vs, std
   return WG_OK;
 }
 
+static wg_status run_partitioned(const PipelineRun& r, const wgd::Plan& P0, const std::vector<int>& in_map,
+                                 bool* done);
+
 // Run the fused kernel over a device-resident input with the overflow policy.
 static wg_status run_device(const PipelineRun& r) {
   wg_agg* a = r.agg;
@@ -683,6 +687,11 @@ static wg_status run_device(const PipelineRun& r) {
   const int64_t n_items = ls.P.n_items;
   if (n_items == 0) return WG_OK;
   const int64_t fan = r.join ? std::max<int64_t>(1, join_max_fanout(r.join)) : 1;
+  if (!r.no_partition) {
+    bool done = false;
+    WG_TRY(run_partitioned(r, ls.P, in_map, &done));
+    if (done) return WG_OK;
+  }
 
   // kernel shape: shared-memory table for low-cardinality single int keys
   bool any_null_words = false, any_dec_minmax = false;
@@ -899,6 +908,80 @@ static wg_status run_device(const PipelineRun& r) {
     if ((int32_t)v[1] != 0) return fail(WG_E_NOMEM, "aggregate table overflow on a checked chunk");
     done += m;
   }
+  return WG_OK;
+}
+
+// Large tables: reorder the input by the top bits of the group key's table hash
+// (part_count_kernel / part_scatter_kernel) and aggregate the reordered copy in
+// order, so the atomics of any stretch of the run land in one L2-sized region
+// of the table instead of all over HBM. Applies to inputs of at least 2^22
+// rows, without a join, selection vector or NULL bitmaps, whose table is at
+// least 64 MB; WG_AGG_PARTITION=0 turns it off. *done says whether it ran.
+static wg_status run_partitioned(const PipelineRun& r, const wgd::Plan& P0, const std::vector<int>& in_map,
+                                 bool* done) {
+  *done = false;
+  wg_agg* a = r.agg;
+  Ctx* ctx = a->ctx;
+  const int64_t n = P0.n_items;
+  if (env_int("WG_AGG_PARTITION", 1) == 0 || r.join || P0.sel || a->L.key_words == 0 || n < (int64_t(1) << 22))
+    return WG_OK;
+  for (int j = 0; j < P0.n_in; ++j)
+    if (P0.in[j].valid) return WG_OK;
+  const int64_t expect = std::max<int64_t>(a->hint, a->known_groups);
+  const int64_t tbytes = std::max<int64_t>(table_words(a, a->cap), (int64_t)cap_for(expect) * a->L.slot_words) * 8;
+  if (tbytes < (int64_t(64) << 20)) return WG_OK;
+  int pbits = 1;
+  while (pbits < 10 && (tbytes >> pbits) > (int64_t(32) << 20)) ++pbits;
+  const int np = 1 << pbits;
+  wgd::Plan P = P0;
+  P.L = launch_layout(a, P0);
+  P.err = ctx->dev_error;
+  const unsigned grid = (unsigned)(ctx->sm_count * 2);
+  DevBuf counts, offs;
+  WG_TRY(counts.ensure(ctx, (int64_t)np * grid * 4));
+  WG_TRY(offs.ensure(ctx, (int64_t)np * grid * 8));
+  wgd::part_count_kernel<<<grid, 256, (size_t)np * 4, ctx->stream>>>(P, pbits, counts.as<uint32_t>());
+  ctx->count_launch();
+  WG_CUDA_TRY(cudaGetLastError());
+  std::vector<uint32_t> hc((size_t)np * grid);
+  std::vector<unsigned long long> ho((size_t)np * grid);
+  WG_CUDA_TRY(cudaMemcpyAsync(hc.data(), counts.get(), hc.size() * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  WG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  unsigned long long acc = 0;
+  for (size_t i = 0; i < hc.size(); ++i) { ho[i] = acc; acc += hc[i]; }  // partition-major, then CTA
+  if ((int64_t)acc != n) return fail(WG_E_CUDA, "partition counts do not add up to the input rows");
+  WG_CUDA_TRY(cudaMemcpyAsync(offs.get(), ho.data(), ho.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
+  std::vector<DevBuf> bufs((size_t)P.n_in);
+  wgd::PartOut po{};
+  for (int j = 0; j < P.n_in; ++j) {
+    const int cls = P.in[j].cls;
+    const int es = cls == WG_CLS_I32 || cls == WG_CLS_F32 ? 4 : cls == WG_CLS_DEC ? 16 : 8;
+    WG_TRY(bufs[(size_t)j].alloc(ctx, n * es));
+    po.data[j] = bufs[(size_t)j].as<char>();
+    po.es[j] = es;
+  }
+  wgd::part_scatter_kernel<<<grid, 256, (size_t)np * 12, ctx->stream>>>(P, pbits, offs.as<unsigned long long>(), po);
+  ctx->count_launch();
+  WG_CUDA_TRY(cudaGetLastError());
+  // the caller's batch with its referenced columns replaced by the reordered copy
+  wg_batch_desc d2 = *r.in;
+  std::vector<wg_column> c2(r.in->cols, r.in->cols + r.in->ncols);
+  for (int c = 0; c < r.in->ncols; ++c)
+    if (in_map[(size_t)c] >= 0) {
+      c2[(size_t)c].data = bufs[(size_t)in_map[(size_t)c]].get();
+      c2[(size_t)c].valid_words = nullptr;
+      c2[(size_t)c].len = n;
+    }
+  d2.cols = c2.data();
+  d2.len = n;
+  d2.sel = nullptr;
+  d2.sel_len = 0;
+  PipelineRun r2 = r;
+  r2.in = &d2;
+  r2.no_partition = true;
+  WG_TRY(run_device(r2));
+  WG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));  // the copy is freed on return
+  *done = true;
   return WG_OK;
 }
 

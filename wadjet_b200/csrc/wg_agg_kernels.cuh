@@ -807,6 +807,85 @@ __global__ void __launch_bounds__(Sh::kBlock, Sh::kMinBlocks) pipeline_kernel(co
 }
 
 // ---------------------------------------------------------------------------
+// Hash partitioning of the input for large tables. The table's slot is the top
+// bits of a 64-bit key hash, so rows grouped by the top `pbits` bits of that
+// hash touch one 1/2^pbits region of the table. Rows reordered that way and
+// fed in order keep the aggregate's working set to an L2-sized region at any
+// time. The order is a pure permutation of the input: every row is kept
+// (filters still run in the aggregation pass) and NULL keys go to region 0.
+// ---------------------------------------------------------------------------
+template <class Sh>
+__device__ __forceinline__ uint32_t row_partition(const Plan& P, const Sh& sh, int64_t row, int pbits) {
+  const SrcGlobal src{row};
+  ExprVals ev;
+  eval_exprs(P, sh, src, -1, ev);
+  const int shift = 64 - pbits;
+  if (sh.key_words() == 1) {
+    const Val v = fetch(P, sh, src, sh.key_vcol(0), -1, ev);
+    return v.null ? 0u : (uint32_t)fib_slot(v.lo, shift);
+  }
+  unsigned long long k0 = 0, k1 = 0;
+#pragma unroll
+  for (int k = 0; k < WG_MAX_KEYS; ++k) {
+    if (k >= sh.n_keys()) break;
+    const Val v = fetch(P, sh, src, sh.key_vcol(k), -1, ev);
+    if (v.null) return 0u;
+    const unsigned long long w =
+        sh.key_i32(k) ? ((unsigned long long)(uint32_t)(int32_t)v.lo) << sh.key_shift(k) : v.lo;
+    if (sh.key_word(k) == 0) k0 |= w; else k1 |= w;
+  }
+  return (uint32_t)packed_slot(k0, k1, shift);
+}
+
+// Rows per partition seen by each CTA (counts[p * gridDim.x + cta]).
+static __global__ void __launch_bounds__(256) part_count_kernel(const __grid_constant__ Plan P, int pbits, uint32_t* counts) {
+  extern __shared__ uint32_t hist[];
+  const int np = 1 << pbits;
+  for (int i = threadIdx.x; i < np; i += blockDim.x) hist[i] = 0;
+  __syncthreads();
+  const DynShape sh{P};
+  for (int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < P.n_items;
+       row += (int64_t)gridDim.x * blockDim.x)
+    atomicAdd(&hist[row_partition(P, sh, row, pbits)], 1u);
+  __syncthreads();
+  for (int i = threadIdx.x; i < np; i += blockDim.x) counts[(size_t)i * gridDim.x + blockIdx.x] = hist[i];
+}
+
+// Output columns of the reordered copy (one per input column of the plan).
+struct PartOut {
+  char* data[WG_MAX_IN];
+  int32_t es[WG_MAX_IN];
+};
+
+// Same grid and row order as part_count_kernel: each CTA writes its rows of
+// partition p from offs[p * gridDim.x + cta] on.
+static __global__ void __launch_bounds__(256) part_scatter_kernel(const __grid_constant__ Plan P, int pbits,
+                                                           const unsigned long long* offs, PartOut out) {
+  extern __shared__ unsigned long long base[];  // np bases, then np 32-bit cursors
+  const int np = 1 << pbits;
+  uint32_t* cur = (uint32_t*)(base + np);
+  for (int i = threadIdx.x; i < np; i += blockDim.x) {
+    base[i] = offs[(size_t)i * gridDim.x + blockIdx.x];
+    cur[i] = 0;
+  }
+  __syncthreads();
+  const DynShape sh{P};
+  for (int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < P.n_items;
+       row += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t p = row_partition(P, sh, row, pbits);
+    const unsigned long long dst = base[p] + atomicAdd(&cur[p], 1u);
+    for (int j = 0; j < P.n_in; ++j) {
+      const int es = out.es[j];
+      const char* src = (const char*)P.in[j].data + row * es;
+      char* d = out.data[j] + dst * es;
+      if (es == 4) *(uint32_t*)d = __ldcs((const uint32_t*)src);
+      else if (es == 8) *(unsigned long long*)d = __ldcs((const unsigned long long*)src);
+      else *(longlong2*)d = __ldcs((const longlong2*)src);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Vector variant for compiled shapes: each lane takes U consecutive rows, loads
 // each column's U values with 16-byte (or 8-byte) loads, evaluates all U
 // filters and issues all U join lookups before the first aggregate update, so
