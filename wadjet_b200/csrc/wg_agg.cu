@@ -74,6 +74,20 @@ __global__ void fold_kernel(Layout Ls, Table Ts, Layout Ld, Table Td, int32_t* e
   }
 }
 
+// out[i] = the slot list[i] of a table (slot_words words each): one partition's
+// groups appended to a spilled aggregate's compact result.
+__global__ void gather_slots_kernel(const unsigned long long* slots, int sw, const int64_t* list, int64_t n,
+                                    unsigned long long* out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n * sw; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t g = i / sw;
+    out[i] = slots[list[g] * sw + (i - g * sw)];
+  }
+}
+
+__global__ void iota_kernel(int64_t* out, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) out[i] = i;
+}
+
 __global__ void compact_kernel(Layout L, Table T, int64_t* list, unsigned long long* count) {
   const uint64_t cap = T.mask + 1;
   const uint64_t n = L.key_words == 0 ? 1 : cap + 2;
@@ -251,6 +265,33 @@ struct wg_agg {
   std::vector<wg::DevBuf> emit_bufs, emit_valid;
   bool emitted = false;
   int32_t last_shape = -1;         // compiled shape of the last fused launch
+  // Spill (the table for the expected groups does not fit the HBM ledger): the
+  // consume calls partition their rows by the key hash's top bits into runs in
+  // pinned host memory; finalize aggregates one partition at a time into a
+  // small table and appends its groups to a compact result, which then stands
+  // in for the table (`spilled`).
+  bool spill = false;
+  bool spilled = false;
+  int spill_pbits = 0;
+  uint64_t small_cap = 0;
+  struct SpillRun {
+    int64_t rows = 0;
+    std::vector<int64_t> off;        // start of each partition in the run (np + 1)
+    std::vector<char*> col;          // pinned host copy of each plan input column
+  };
+  std::vector<SpillRun> runs;
+  std::vector<std::pair<char*, int64_t>> host_blocks;  // pinned arena (kept for the next query)
+  size_t block_idx = 0;
+  int64_t block_used = 0, host_bytes = 0;
+  // the spilled consume calls' shape, replayed per partition at finalize
+  std::vector<wg_column> sp_cols;
+  std::vector<int> sp_map, sp_es;    // caller column -> plan input, plan input element size
+  std::vector<wg_predicate> sp_filters;
+  std::vector<wg_expr> sp_exprs;
+  std::vector<wg::DevBuf> sp_dev;    // device staging per plan input column
+  ~wg_agg() {
+    for (auto& b : host_blocks) cudaFreeHost(b.first);
+  }
 };
 
 namespace wg {
@@ -449,7 +490,22 @@ static wg_status agg_resolve(wg_agg* a, const VSchema& vs) {
   if (a->L.slot_words > WG_MAX_SLOT_WORDS) return fail(WG_E_UNSUPPORTED, "aggregate state too wide");
   a->cap = a->L.key_words == 0 ? 1 : cap_for(std::max<int64_t>(a->hint, 1024));
   a->shift = 64 - log2u(a->cap);
-  WG_TRY(init_table(a, a->table, a->cap));
+  wg_status st = init_table(a, a->table, a->cap);
+  if (st == WG_E_NOMEM && a->L.key_words >= 1 && a->ctx->pinned_spill_bytes > 0 && env_int("WG_AGG_SPILL", 1) != 0) {
+    // spill: one small table per hash partition, each holding about 1/16 of
+    // what the ledger has left
+    const int64_t left = a->ctx->ledger.budget() > 0 ? a->ctx->ledger.budget() - a->ctx->ledger.used() : (int64_t(1) << 40);
+    const int64_t full = (int64_t)a->cap * a->L.slot_words * 8;
+    int pbits = 1;
+    while (pbits < 10 && (full >> pbits) > left / 16) ++pbits;
+    a->spill = true;
+    a->spill_pbits = pbits;
+    a->small_cap = cap_for(std::max<int64_t>(1024, std::max<int64_t>(a->hint, 1024) >> pbits));
+    a->cap = a->small_cap;
+    a->shift = 64 - log2u(a->cap);
+    st = init_table(a, a->table, a->cap);
+  }
+  WG_TRY(st);
   WG_TRY(a->ctr.alloc(a->ctx, 64));
   WG_CUDA_TRY(cudaMemsetAsync(a->ctr.get(), 0, 64, a->ctx->stream));
   a->known_groups = 0;
@@ -671,6 +727,7 @@ static wg_status build_plan(const PipelineRun& r, wgd::Plan& P, VSchema& vs, std
 
 static wg_status run_partitioned(const PipelineRun& r, const wgd::Plan& P0, const std::vector<int>& in_map,
                                  bool* done);
+static wg_status spill_consume(const PipelineRun& r, const wgd::Plan& P0, const std::vector<int>& in_map);
 
 // Run the fused kernel over a device-resident input with the overflow policy.
 static wg_status run_device(const PipelineRun& r) {
@@ -687,6 +744,7 @@ static wg_status run_device(const PipelineRun& r) {
   const int64_t n_items = ls.P.n_items;
   if (n_items == 0) return WG_OK;
   const int64_t fan = r.join ? std::max<int64_t>(1, join_max_fanout(r.join)) : 1;
+  if (a->spill && !r.no_partition) return spill_consume(r, ls.P, in_map);
   if (!r.no_partition) {
     bool done = false;
     WG_TRY(run_partitioned(r, ls.P, in_map, &done));
@@ -985,6 +1043,215 @@ static wg_status run_partitioned(const PipelineRun& r, const wgd::Plan& P0, cons
   return WG_OK;
 }
 
+// Rows of the partition kernels' plan: the aggregate's key layout, the caller's
+// columns rebased to row r0, m rows.
+static wgd::Plan part_plan(wg_agg* a, const wgd::Plan& P0, int64_t r0, int64_t m) {
+  wgd::Plan P = P0;
+  for (int j = 0; j < P.n_in; ++j) {
+    const int cls = P.in[j].cls;
+    const int64_t es = cls == WG_CLS_I32 || cls == WG_CLS_F32 ? 4 : cls == WG_CLS_DEC ? 16 : 8;
+    P.in[j].data = (const char*)P.in[j].data + r0 * es;
+  }
+  P.n_items = m;
+  P.L = launch_layout(a, P0);
+  P.err = a->ctx->dev_error;
+  return P;
+}
+
+// Pinned host memory for spilled runs, from blocks of at least 256 MB, within
+// the context's pinned spill budget.
+static wg_status spill_host_alloc(wg_agg* a, int64_t bytes, char** out) {
+  bytes = (bytes + 255) & ~int64_t(255);
+  while (a->block_idx < a->host_blocks.size() && a->block_used + bytes > a->host_blocks[a->block_idx].second) {
+    ++a->block_idx;  // the rest of this block stays unused until the arena is rewound
+    a->block_used = 0;
+  }
+  if (a->block_idx == a->host_blocks.size()) {
+    const int64_t blk = std::max<int64_t>(bytes, int64_t(256) << 20);
+    if (a->host_bytes + blk > a->ctx->pinned_spill_bytes)
+      return fail(WG_E_NOMEM, "pinned spill budget exceeded by the spilled aggregation");
+    void* p = nullptr;
+    if (cudaMallocHost(&p, (size_t)blk) != cudaSuccess) return fail(WG_E_NOMEM, "pinned spill allocation failed");
+    a->host_blocks.push_back({(char*)p, blk});
+    a->host_bytes += blk;
+    a->block_used = 0;
+  }
+  *out = a->host_blocks[a->block_idx].first + a->block_used;
+  a->block_used += bytes;
+  return WG_OK;
+}
+
+// A spilled consume call: the input, in windows of up to 2^24 rows, reordered
+// on the device by partition (part_count_kernel / part_scatter_kernel) and
+// copied to pinned host runs. Filters and projections run later, per
+// partition, so every row is kept here.
+static wg_status spill_consume(const PipelineRun& r, const wgd::Plan& P0, const std::vector<int>& in_map) {
+  wg_agg* a = r.agg;
+  Ctx* ctx = a->ctx;
+  if (r.join || P0.sel) return fail(WG_E_UNSUPPORTED, "a spilled aggregation takes no join and no selection vector");
+  for (int j = 0; j < P0.n_in; ++j)
+    if (P0.in[j].valid) return fail(WG_E_UNSUPPORTED, "a spilled aggregation takes no NULLs");
+  if (a->sp_map.empty()) {  // remember the consume calls' shape for the per-partition runs
+    a->sp_cols.assign(r.in->cols, r.in->cols + r.in->ncols);
+    a->sp_map = in_map;
+    a->sp_es.assign((size_t)P0.n_in, 0);
+    for (int j = 0; j < P0.n_in; ++j) {
+      const int cls = P0.in[j].cls;
+      a->sp_es[(size_t)j] = cls == WG_CLS_I32 || cls == WG_CLS_F32 ? 4 : cls == WG_CLS_DEC ? 16 : 8;
+    }
+    a->sp_filters.assign(r.filters, r.filters + r.n_filters);
+    a->sp_exprs.assign(r.exprs, r.exprs + r.n_exprs);
+    a->sp_dev.resize((size_t)P0.n_in);
+  } else {
+    bool same = (int)a->sp_cols.size() == r.in->ncols && a->sp_map == in_map &&
+                (int)a->sp_filters.size() == r.n_filters && (int)a->sp_exprs.size() == r.n_exprs;
+    for (int c = 0; same && c < r.in->ncols; ++c)
+      same = a->sp_cols[(size_t)c].type_id == r.in->cols[c].type_id && a->sp_cols[(size_t)c].scale == r.in->cols[c].scale;
+    if (!same) return fail(WG_E_UNSUPPORTED, "every consume call of a spilled aggregation must have the same shape");
+  }
+  const int pbits = a->spill_pbits, np = 1 << pbits;
+  const unsigned grid = (unsigned)(ctx->sm_count * 2);
+  DevBuf counts, offs;
+  WG_TRY(counts.ensure(ctx, (int64_t)np * grid * 4));
+  WG_TRY(offs.ensure(ctx, (int64_t)np * grid * 8));
+  // windows of up to 2^24 rows, or what a quarter of the ledger's room holds
+  int64_t row_bytes = 0;
+  for (int e : a->sp_es) row_bytes += e;
+  const int64_t room = ctx->ledger.budget() > 0 ? ctx->ledger.budget() - ctx->ledger.used() : (int64_t(1) << 40);
+  const int64_t n = P0.n_items;
+  const int64_t win = std::max<int64_t>(int64_t(1) << 16, std::min<int64_t>(int64_t(1) << 24, room / 4 / std::max<int64_t>(row_bytes, 1)));
+  std::vector<uint32_t> hc((size_t)np * grid);
+  std::vector<unsigned long long> ho((size_t)np * grid);
+  for (int64_t r0 = 0; r0 < n; r0 += win) {
+    const int64_t m = std::min(win, n - r0);
+    const wgd::Plan P = part_plan(a, P0, r0, m);
+    wgd::part_count_kernel<<<grid, 256, (size_t)np * 4, ctx->stream>>>(P, pbits, counts.as<uint32_t>());
+    ctx->count_launch();
+    WG_CUDA_TRY(cudaGetLastError());
+    WG_CUDA_TRY(cudaMemcpyAsync(hc.data(), counts.get(), hc.size() * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    WG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    wg_agg::SpillRun run;
+    run.rows = m;
+    run.off.assign((size_t)np + 1, 0);
+    unsigned long long acc = 0;
+    for (int p = 0; p < np; ++p) {
+      run.off[(size_t)p] = (int64_t)acc;
+      for (unsigned c = 0; c < grid; ++c) { ho[(size_t)p * grid + c] = acc; acc += hc[(size_t)p * grid + c]; }
+    }
+    run.off[(size_t)np] = (int64_t)acc;
+    if ((int64_t)acc != m) return fail(WG_E_CUDA, "partition counts do not add up to the input rows");
+    WG_CUDA_TRY(cudaMemcpyAsync(offs.get(), ho.data(), ho.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
+    wgd::PartOut po{};
+    for (int j = 0; j < P.n_in; ++j) {
+      WG_TRY(a->sp_dev[(size_t)j].ensure(ctx, win * a->sp_es[(size_t)j]));
+      po.data[j] = a->sp_dev[(size_t)j].as<char>();
+      po.es[j] = a->sp_es[(size_t)j];
+    }
+    wgd::part_scatter_kernel<<<grid, 256, (size_t)np * 12, ctx->stream>>>(P, pbits, offs.as<unsigned long long>(), po);
+    ctx->count_launch();
+    WG_CUDA_TRY(cudaGetLastError());
+    run.col.assign((size_t)P.n_in, nullptr);
+    for (int j = 0; j < P.n_in; ++j) {
+      WG_TRY(spill_host_alloc(a, m * a->sp_es[(size_t)j], &run.col[(size_t)j]));
+      WG_CUDA_TRY(cudaMemcpyAsync(run.col[(size_t)j], po.data[j], (size_t)(m * a->sp_es[(size_t)j]),
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    WG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    a->runs.push_back(std::move(run));
+  }
+  return check_device_error(ctx);
+}
+
+static wg_status agg_compact(wg_agg* a);
+
+// Finalize of a spilled aggregation: per partition, its rows from every run
+// back to the device, the fused kernel into the small table, and the groups
+// appended to the compact result; the result then stands in for the table.
+static wg_status spill_finish(wg_agg* a) {
+  Ctx* ctx = a->ctx;
+  const int np = 1 << a->spill_pbits;
+  const int nin = (int)a->sp_es.size();
+  const int sw = a->L.slot_words;
+  int64_t max_rows = 0;
+  for (int p = 0; p < np; ++p) {
+    int64_t rows = 0;
+    for (const auto& run : a->runs) rows += run.off[(size_t)p + 1] - run.off[(size_t)p];
+    max_rows = std::max(max_rows, rows);
+  }
+  for (int j = 0; j < nin; ++j) {  // staging for one partition (the consume windows' buffers go first)
+    a->sp_dev[(size_t)j].reset();
+    WG_TRY(a->sp_dev[(size_t)j].alloc(ctx, std::max<int64_t>(max_rows, 1) * a->sp_es[(size_t)j]));
+  }
+  DevBuf res;
+  int64_t res_cap = std::max<int64_t>(a->hint, 1024), n_res = 0;
+  WG_TRY(res.alloc(ctx, res_cap * sw * 8));
+  std::vector<wg_column> cols = a->sp_cols;
+  wg_batch_desc d{};
+  d.ncols = (int32_t)cols.size();
+  d.cols = cols.data();
+  for (int p = 0; p < np; ++p) {
+    int64_t rows = 0;
+    for (const auto& run : a->runs) {
+      const int64_t c = run.off[(size_t)p + 1] - run.off[(size_t)p];
+      for (int j = 0; j < nin && c > 0; ++j) {
+        const int64_t es = a->sp_es[(size_t)j];
+        WG_CUDA_TRY(cudaMemcpyAsync(a->sp_dev[(size_t)j].as<char>() + rows * es, run.col[(size_t)j] + run.off[(size_t)p] * es,
+                                    (size_t)(c * es), cudaMemcpyHostToDevice, ctx->stream));
+      }
+      rows += c;
+    }
+    if (rows == 0) continue;
+    for (size_t c = 0; c < cols.size(); ++c) {
+      cols[c].len = rows;
+      cols[c].valid_words = nullptr;
+      if (a->sp_map[c] >= 0) cols[c].data = a->sp_dev[(size_t)a->sp_map[c]].get();
+    }
+    d.len = rows;
+    // the small table, empty again
+    const int64_t words = table_words(a, a->cap);
+    init_table_kernel<<<grid_cap(ctx, words, 256), 256, 0, ctx->stream>>>(a->table.as<unsigned long long>(), words,
+                                                                         sw, a->L);
+    ctx->count_launch();
+    WG_CUDA_TRY(cudaMemsetAsync(a->ctr.get(), 0, 64, ctx->stream));
+    a->known_groups = a->upper_groups = 0;
+    PipelineRun rp{a, &d, (int32_t)a->sp_filters.size(), a->sp_filters.data(), nullptr, (int32_t)a->sp_exprs.size(),
+                   a->sp_exprs.data()};
+    rp.no_partition = true;
+    WG_TRY(run_device(rp));
+    WG_TRY(agg_compact(a));
+    if (n_res + a->n_out > res_cap) {  // grow the result, keeping what it holds
+      const int64_t cap2 = std::max<int64_t>(res_cap * 2, n_res + a->n_out);
+      DevBuf bigger;
+      WG_TRY(bigger.alloc(ctx, cap2 * sw * 8));
+      if (n_res > 0)
+        WG_CUDA_TRY(cudaMemcpyAsync(bigger.get(), res.get(), (size_t)(n_res * sw * 8), cudaMemcpyDeviceToDevice, ctx->stream));
+      WG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+      res = std::move(bigger);
+      res_cap = cap2;
+    }
+    if (a->n_out > 0) {
+      gather_slots_kernel<<<grid_cap(ctx, a->n_out * sw, 256), 256, 0, ctx->stream>>>(
+          a->table.as<unsigned long long>(), sw, a->list.as<int64_t>(), a->n_out, res.as<unsigned long long>() + n_res * sw);
+      ctx->count_launch();
+      WG_CUDA_TRY(cudaGetLastError());
+    }
+    n_res += a->n_out;
+  }
+  // the compact result becomes the table: every slot a group, no NULL-key slot
+  a->table = std::move(res);
+  a->cap = uint64_t(1) << 62;
+  a->spilled = true;
+  WG_TRY(a->list.ensure(ctx, std::max<int64_t>(n_res, 1) * 8));
+  iota_kernel<<<grid_cap(ctx, std::max<int64_t>(n_res, 1), 256), 256, 0, ctx->stream>>>(a->list.as<int64_t>(), n_res);
+  ctx->count_launch();
+  WG_CUDA_TRY(cudaGetLastError());
+  a->n_out = n_res;
+  a->runs.clear();
+  a->block_idx = 0;  // rewind the arena for the next query on this aggregate
+  a->block_used = 0;
+  return check_device_error(ctx);
+}
+
 // Compact the occupied slots once; the list drives export and emit.
 static wg_status agg_compact(wg_agg* a) {
   Ctx* ctx = a->ctx;
@@ -1079,6 +1346,7 @@ wg_status wg_agg_merge(wg_agg* d, wg_agg* s) {
   if (!d || !s) return fail(WG_E_INVALID, "NULL argument");
   if (d->ctx != s->ctx) return fail(WG_E_INVALID, "aggregates belong to different contexts");
   if (d->key_cols != s->key_cols || d->specs.size() != s->specs.size()) return fail(WG_E_INVALID, "aggregate shapes differ");
+  if (d->spill || s->spill) return fail(WG_E_UNSUPPORTED, "spilled aggregations are not merged");
   WG_TRY(ensure_device(d->ctx));
   if (d->finalized) return fail(WG_E_STATE, "aggregate already finalized");
   if (!s->resolved) return WG_OK;
@@ -1128,7 +1396,8 @@ wg_status wg_agg_finalize(wg_agg* a, int64_t* n_groups) {
     return WG_OK;
   }
   if (!a->finalized) {
-    WG_TRY(agg_compact(a));
+    if (a->spill) WG_TRY(spill_finish(a));
+    else WG_TRY(agg_compact(a));
     a->finalized = true;
   }
   if (n_groups) *n_groups = a->n_out;
@@ -1235,6 +1504,18 @@ wg_status wg_agg_reset(wg_agg* a) {
   a->n_out = 0;
   if (!a->resolved) return WG_OK;
   Ctx* ctx = a->ctx;
+  if (a->spill) {
+    a->runs.clear();
+    a->block_idx = 0;
+    a->block_used = 0;
+  }
+  if (a->spilled) {  // the table holds a compact result: back to an empty small table
+    a->table.reset();
+    a->cap = a->small_cap;
+    a->shift = 64 - log2u(a->cap);
+    WG_TRY(a->table.alloc(ctx, table_words(a, a->cap) * 8));
+    a->spilled = false;
+  }
   const int64_t words = table_words(a, a->cap);
   init_table_kernel<<<grid_cap(ctx, words, 256), 256, 0, ctx->stream>>>(a->table.as<unsigned long long>(), words,
                                                                        a->L.slot_words, a->L);
