@@ -21,11 +21,11 @@ def to_host_dec(t):
 
 
 def test_spilled_packed_key_aggregate_matches_oracle():
-    """GROUP BY (a int32, b int64) over 2^22 rows (~3.9M groups) with a 480 MB budget: the full
-    table (512 MB) does not fit; the compact result (~250 MB) and its export do."""
+    """GROUP BY (a int32, b int64) over 2^22 rows (~3.9M groups) with a 512 MB budget: the full
+    table (just over 512 MB) does not fit; the compact result (~250 MB) and its export do."""
     import wadjet_b200 as wg
     from wadjet_b200 import synth
-    budget = 480 * MB
+    budget = 512 * MB
     with wg.Context(0, hbm_budget=budget, pinned_spill=2 << 30) as ctx:
         n = 1 << 22
         a, b, amt, x = synth.highcard(ctx, n)

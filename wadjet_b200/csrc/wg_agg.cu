@@ -1248,6 +1248,8 @@ static wg_status spill_finish(wg_agg* a) {
   WG_CUDA_TRY(cudaGetLastError());
   a->n_out = n_res;
   a->runs.clear();
+  for (auto& b : a->sp_dev) b.reset();  // staging and snapshots go back to the ledger
+  a->backup.reset();
   a->block_idx = 0;  // rewind the arena for the next query on this aggregate
   a->block_used = 0;
   return check_device_error(ctx);
