@@ -1415,32 +1415,43 @@ wg_status wg_agg_export(wg_agg* a, const wg_group_export* o) {
   if (!a->resolved || a->n_out == 0) return WG_OK;
   const int64_t n = a->n_out;
   const int nk = (int)a->key_cols.size(), na = (int)a->specs.size();
+  // in chunks of at most 2^18 groups, so the export's device staging stays small
+  const int64_t C = std::min<int64_t>(n, int64_t(1) << 18);
   DevBuf keys, kv, cnt, i64, f64, dec, has;
   FinalArgs A;
   fill_final_args(a, A);
-  A.start = 0; A.n = n; A.stride = n;
-  if (o->keys && nk) { WG_TRY(keys.alloc(ctx, nk * n * 8)); A.keys = keys.as<int64_t>(); }
-  if (o->key_valid && nk) { WG_TRY(kv.alloc(ctx, nk * n)); A.key_valid = kv.as<uint8_t>(); }
-  if (o->count && na) { WG_TRY(cnt.alloc(ctx, na * n * 8)); A.count = cnt.as<int64_t>(); }
-  if (o->i64 && na) { WG_TRY(i64.alloc(ctx, na * n * 8)); A.i64 = i64.as<int64_t>(); }
-  if (o->f64 && na) { WG_TRY(f64.alloc(ctx, na * n * 8)); A.f64 = f64.as<double>(); }
-  if (o->dec && na) { WG_TRY(dec.alloc(ctx, na * n * 16)); A.dec = dec.as<wg_int128>(); }
-  if (o->has && na) { WG_TRY(has.alloc(ctx, na * n)); A.has = has.as<uint8_t>(); }
-  export_kernel<<<grid_cap(ctx, n, 256), 256, 0, ctx->stream>>>(A);
-  ctx->count_launch();
-  WG_CUDA_TRY(cudaGetLastError());
-  auto back = [&](void* dst, DevBuf& src, int64_t bytes) -> wg_status {
-    if (dst && src.get() && bytes > 0) WG_CUDA_TRY(cudaMemcpyAsync(dst, src.get(), (size_t)bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  if (o->keys && nk) { WG_TRY(keys.alloc(ctx, nk * C * 8)); A.keys = keys.as<int64_t>(); }
+  if (o->key_valid && nk) { WG_TRY(kv.alloc(ctx, nk * C)); A.key_valid = kv.as<uint8_t>(); }
+  if (o->count && na) { WG_TRY(cnt.alloc(ctx, na * C * 8)); A.count = cnt.as<int64_t>(); }
+  if (o->i64 && na) { WG_TRY(i64.alloc(ctx, na * C * 8)); A.i64 = i64.as<int64_t>(); }
+  if (o->f64 && na) { WG_TRY(f64.alloc(ctx, na * C * 8)); A.f64 = f64.as<double>(); }
+  if (o->dec && na) { WG_TRY(dec.alloc(ctx, na * C * 16)); A.dec = dec.as<wg_int128>(); }
+  if (o->has && na) { WG_TRY(has.alloc(ctx, na * C)); A.has = has.as<uint8_t>(); }
+  // block b of a chunk (c rows at stride c on the device) to rows [s, s + c) of block b on the host (stride n)
+  auto back = [&](void* dst, DevBuf& src, int blocks, int64_t es, int64_t s0, int64_t c) -> wg_status {
+    if (!dst || !src.get()) return WG_OK;
+    for (int b = 0; b < blocks; ++b)
+      WG_CUDA_TRY(cudaMemcpyAsync((char*)dst + (b * n + s0) * es, src.as<char>() + b * c * es, (size_t)(c * es),
+                                  cudaMemcpyDeviceToHost, ctx->stream));
     return WG_OK;
   };
-  WG_TRY(back(o->keys, keys, nk * n * 8));
-  WG_TRY(back(o->key_valid, kv, nk * n));
-  WG_TRY(back(o->count, cnt, na * n * 8));
-  WG_TRY(back(o->i64, i64, na * n * 8));
-  WG_TRY(back(o->f64, f64, na * n * 8));
-  WG_TRY(back(o->dec, dec, na * n * 16));
-  WG_TRY(back(o->has, has, na * n));
-  WG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  for (int64_t s0 = 0; s0 < n; s0 += C) {
+    const int64_t c = std::min(C, n - s0);
+    A.start = s0;
+    A.n = c;
+    A.stride = c;
+    export_kernel<<<grid_cap(ctx, c, 256), 256, 0, ctx->stream>>>(A);
+    ctx->count_launch();
+    WG_CUDA_TRY(cudaGetLastError());
+    WG_TRY(back(o->keys, keys, nk, 8, s0, c));
+    WG_TRY(back(o->key_valid, kv, nk, 1, s0, c));
+    WG_TRY(back(o->count, cnt, na, 8, s0, c));
+    WG_TRY(back(o->i64, i64, na, 8, s0, c));
+    WG_TRY(back(o->f64, f64, na, 8, s0, c));
+    WG_TRY(back(o->dec, dec, na, 16, s0, c));
+    WG_TRY(back(o->has, has, na, 1, s0, c));
+    WG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));  // the staging is reused by the next chunk
+  }
   return check_device_error(ctx);
 }
 
