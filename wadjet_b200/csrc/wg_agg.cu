@@ -1415,8 +1415,8 @@ wg_status wg_agg_export(wg_agg* a, const wg_group_export* o) {
   if (!a->resolved || a->n_out == 0) return WG_OK;
   const int64_t n = a->n_out;
   const int nk = (int)a->key_cols.size(), na = (int)a->specs.size();
-  // in chunks of at most 2^18 groups, so the export's device staging stays small
-  const int64_t C = std::min<int64_t>(n, int64_t(1) << 18);
+  // in chunks of at most 2^16 groups, so the export's device staging stays small
+  const int64_t C = std::min<int64_t>(n, int64_t(1) << 16);
   DevBuf keys, kv, cnt, i64, f64, dec, has;
   FinalArgs A;
   fill_final_args(a, A);
