@@ -36,6 +36,9 @@ namespace {
 
 constexpr int64_t kSnapshotMaxBytes = 256LL << 20;
 constexpr double kMaxLoad = 0.75;
+// spill partitions take hash bits [20, 30): below the slot bits of any table up
+// to 2^34 slots, so each partition's keys spread over its whole table
+constexpr int kSpillPartShift = 20;
 
 __global__ void init_table_kernel(unsigned long long* slots, int64_t words, int sw, Layout L) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < words; i += (int64_t)gridDim.x * blockDim.x)
@@ -999,7 +1002,7 @@ static wg_status run_partitioned(const PipelineRun& r, const wgd::Plan& P0, cons
   DevBuf counts, offs;
   WG_TRY(counts.ensure(ctx, (int64_t)np * grid * 4));
   WG_TRY(offs.ensure(ctx, (int64_t)np * grid * 8));
-  wgd::part_count_kernel<<<grid, 256, (size_t)np * 4, ctx->stream>>>(P, pbits, counts.as<uint32_t>());
+  wgd::part_count_kernel<<<grid, 256, (size_t)np * 4, ctx->stream>>>(P, pbits, 64 - pbits, counts.as<uint32_t>());
   ctx->count_launch();
   WG_CUDA_TRY(cudaGetLastError());
   std::vector<uint32_t> hc((size_t)np * grid);
@@ -1019,7 +1022,8 @@ static wg_status run_partitioned(const PipelineRun& r, const wgd::Plan& P0, cons
     po.data[j] = bufs[(size_t)j].as<char>();
     po.es[j] = es;
   }
-  wgd::part_scatter_kernel<<<grid, 256, (size_t)np * 12, ctx->stream>>>(P, pbits, offs.as<unsigned long long>(), po);
+  wgd::part_scatter_kernel<<<grid, 256, (size_t)np * 12, ctx->stream>>>(P, pbits, 64 - pbits,
+                                                                        offs.as<unsigned long long>(), po);
   ctx->count_launch();
   WG_CUDA_TRY(cudaGetLastError());
   // the caller's batch with its referenced columns replaced by the reordered copy
@@ -1126,7 +1130,8 @@ static wg_status spill_consume(const PipelineRun& r, const wgd::Plan& P0, const 
   for (int64_t r0 = 0; r0 < n; r0 += win) {
     const int64_t m = std::min(win, n - r0);
     const wgd::Plan P = part_plan(a, P0, r0, m);
-    wgd::part_count_kernel<<<grid, 256, (size_t)np * 4, ctx->stream>>>(P, pbits, counts.as<uint32_t>());
+    wgd::part_count_kernel<<<grid, 256, (size_t)np * 4, ctx->stream>>>(P, pbits, kSpillPartShift,
+                                                                       counts.as<uint32_t>());
     ctx->count_launch();
     WG_CUDA_TRY(cudaGetLastError());
     WG_CUDA_TRY(cudaMemcpyAsync(hc.data(), counts.get(), hc.size() * 4, cudaMemcpyDeviceToHost, ctx->stream));
@@ -1148,7 +1153,8 @@ static wg_status spill_consume(const PipelineRun& r, const wgd::Plan& P0, const 
       po.data[j] = a->sp_dev[(size_t)j].as<char>();
       po.es[j] = a->sp_es[(size_t)j];
     }
-    wgd::part_scatter_kernel<<<grid, 256, (size_t)np * 12, ctx->stream>>>(P, pbits, offs.as<unsigned long long>(), po);
+    wgd::part_scatter_kernel<<<grid, 256, (size_t)np * 12, ctx->stream>>>(P, pbits, kSpillPartShift,
+                                                                          offs.as<unsigned long long>(), po);
     ctx->count_launch();
     WG_CUDA_TRY(cudaGetLastError());
     run.col.assign((size_t)P.n_in, nullptr);

@@ -814,15 +814,19 @@ __global__ void __launch_bounds__(Sh::kBlock, Sh::kMinBlocks) pipeline_kernel(co
 // time. The order is a pure permutation of the input: every row is kept
 // (filters still run in the aggregation pass) and NULL keys go to region 0.
 // ---------------------------------------------------------------------------
+// The partition is bits [pshift, pshift + pbits) of the 64-bit key hash: the
+// top bits (pshift = 64 - pbits) for the in-HBM reorder, whose table regions
+// they select; bits below any table's slot bits for the spill, whose
+// per-partition table must spread a partition's keys over all its slots.
 template <class Sh>
-__device__ __forceinline__ uint32_t row_partition(const Plan& P, const Sh& sh, int64_t row, int pbits) {
+__device__ __forceinline__ uint32_t row_partition(const Plan& P, const Sh& sh, int64_t row, int pbits, int pshift) {
   const SrcGlobal src{row};
   ExprVals ev;
   eval_exprs(P, sh, src, -1, ev);
-  const int shift = 64 - pbits;
+  const uint32_t mask = (1u << pbits) - 1u;
   if (sh.key_words() == 1) {
     const Val v = fetch(P, sh, src, sh.key_vcol(0), -1, ev);
-    return v.null ? 0u : (uint32_t)fib_slot(v.lo, shift);
+    return v.null ? 0u : (uint32_t)(fib_slot(v.lo, 0) >> pshift) & mask;
   }
   unsigned long long k0 = 0, k1 = 0;
 #pragma unroll
@@ -834,11 +838,12 @@ __device__ __forceinline__ uint32_t row_partition(const Plan& P, const Sh& sh, i
         sh.key_i32(k) ? ((unsigned long long)(uint32_t)(int32_t)v.lo) << sh.key_shift(k) : v.lo;
     if (sh.key_word(k) == 0) k0 |= w; else k1 |= w;
   }
-  return (uint32_t)packed_slot(k0, k1, shift);
+  return (uint32_t)(packed_slot(k0, k1, 0) >> pshift) & mask;
 }
 
 // Rows per partition seen by each CTA (counts[p * gridDim.x + cta]).
-static __global__ void __launch_bounds__(256) part_count_kernel(const __grid_constant__ Plan P, int pbits, uint32_t* counts) {
+static __global__ void __launch_bounds__(256) part_count_kernel(const __grid_constant__ Plan P, int pbits, int pshift,
+                                                                uint32_t* counts) {
   extern __shared__ uint32_t hist[];
   const int np = 1 << pbits;
   for (int i = threadIdx.x; i < np; i += blockDim.x) hist[i] = 0;
@@ -846,7 +851,7 @@ static __global__ void __launch_bounds__(256) part_count_kernel(const __grid_con
   const DynShape sh{P};
   for (int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < P.n_items;
        row += (int64_t)gridDim.x * blockDim.x)
-    atomicAdd(&hist[row_partition(P, sh, row, pbits)], 1u);
+    atomicAdd(&hist[row_partition(P, sh, row, pbits, pshift)], 1u);
   __syncthreads();
   for (int i = threadIdx.x; i < np; i += blockDim.x) counts[(size_t)i * gridDim.x + blockIdx.x] = hist[i];
 }
@@ -860,7 +865,8 @@ struct PartOut {
 // Same grid and row order as part_count_kernel: each CTA writes its rows of
 // partition p from offs[p * gridDim.x + cta] on.
 static __global__ void __launch_bounds__(256) part_scatter_kernel(const __grid_constant__ Plan P, int pbits,
-                                                           const unsigned long long* offs, PartOut out) {
+                                                                  int pshift, const unsigned long long* offs,
+                                                                  PartOut out) {
   extern __shared__ unsigned long long base[];  // np bases, then np 32-bit cursors
   const int np = 1 << pbits;
   uint32_t* cur = (uint32_t*)(base + np);
@@ -872,7 +878,7 @@ static __global__ void __launch_bounds__(256) part_scatter_kernel(const __grid_c
   const DynShape sh{P};
   for (int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < P.n_items;
        row += (int64_t)gridDim.x * blockDim.x) {
-    const uint32_t p = row_partition(P, sh, row, pbits);
+    const uint32_t p = row_partition(P, sh, row, pbits, pshift);
     const unsigned long long dst = base[p] + atomicAdd(&cur[p], 1u);
     for (int j = 0; j < P.n_in; ++j) {
       const int es = out.es[j];
