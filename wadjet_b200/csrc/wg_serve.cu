@@ -3,15 +3,18 @@
 //
 // n_slots worker threads each own a child context (own streams, a child ledger
 // sharing the server context's budget). A request is admitted when a slot is
-// free and the shared ledger can hold its estimated HBM footprint; admission is
+// free, the requests already on the device stream fewer input bytes than the
+// work limit (256 MB; WG_SERVE_WORK_LIMIT_MB) together with it, and the shared
+// ledger can hold its estimated HBM footprint. A request larger than the limit
+// runs alone (one such request already fills the GPU; sharing it only slows
+// both); small ones overlap, which is where concurrency pays. Admission is
 // first-come first-served, so a large request waits at the head of the queue
-// until memory frees rather than being overtaken forever. Admitted requests run
-// concurrently on their slots' streams, so a request that arrives while others
-// are on the GPU starts as soon as a slot and memory allow, overlapping them.
+// rather than being overtaken forever.
 // Results stay on the device until the caller releases them.
 #include "wg_internal.h"
 
 #include <algorithm>
+#include <cstdlib>
 #include <chrono>
 #include <condition_variable>
 #include <deque>
@@ -37,6 +40,7 @@ struct Req {
   std::vector<wg_agg_spec> aggs;
   int64_t hint = 0;
   int64_t est = 0;
+  int64_t work = 0;   // input bytes the request streams
   double t_submit = 0, t_start = 0, t_done = 0;
   wg_agg* agg = nullptr;
   wg_ctx* slot = nullptr;
@@ -80,6 +84,9 @@ struct wg_server {
   int64_t next_ticket = 1;
   bool stop = false;
   int64_t submitted = 0, completed = 0, failed = 0, running = 0;
+  // requests overlap on the device while their input bytes together stay under
+  // work_limit; a request at least that large runs alone (it fills the GPU)
+  int64_t inflight_work = 0, work_limit = int64_t(256) << 20;
   std::vector<double> lat;
   double queue_sum = 0, service_sum = 0;
   double t_first = -1, t_last = 0;
@@ -130,12 +137,15 @@ void worker_main(wg_server* s, int slot_idx) {
         if (s->stop) return;
         if (!s->queue.empty()) {
           Req* head = s->queue.front();
-          // admission: the head request's footprint must fit the shared ledger
-          if (s->ctx->ledger.reserve(head->est)) {
+          // admission: the device has room for more work (or is idle), and the
+          // head request's footprint fits the shared ledger
+          const bool room = s->running == 0 || s->inflight_work + head->work <= s->work_limit;
+          if (room && s->ctx->ledger.reserve(head->est)) {
             head->held = true;
             s->queue.pop_front();
             r = head;
             ++s->running;
+            s->inflight_work += r->work;
             break;
           }
           if (s->running == 0) {  // nothing will free memory: fail the request rather than wait forever
@@ -159,6 +169,7 @@ void worker_main(wg_server* s, int slot_idx) {
       r->t_done = now_s();
       r->done = true;
       --s->running;
+      s->inflight_work -= r->work;
       if (r->status == WG_OK) {
         ++s->completed;
         s->lat.push_back(r->t_done - r->t_submit);
@@ -193,6 +204,7 @@ wg_status wg_server_create(wg_ctx* ctx, int32_t n_slots, wg_server** out) {
   WG_TRY(ensure_device(ctx));
   wg_server* s = new wg_server();
   s->ctx = ctx;
+  if (const char* w = std::getenv("WG_SERVE_WORK_LIMIT_MB")) s->work_limit = std::max<int64_t>(1, std::atoll(w)) << 20;
   for (int i = 0; i < n_slots; ++i) {
     wg_ctx* c = nullptr;
     wg_status st = wg_ctx_create_child(ctx, &c);
@@ -221,6 +233,7 @@ wg_status wg_server_submit(wg_server* s, const wg_serve_request* q, int64_t* tic
   r->keys.assign(q->key_cols, q->key_cols + q->n_keys);
   r->aggs.assign(q->aggs, q->aggs + q->n_aggs);
   r->hint = q->ndv_hint;
+  for (const wg_column& c : r->cols) r->work += c.len * wg::elem_size(c.type_id);
   r->est = q->est_bytes > 0 ? q->est_bytes : 128 * std::max<int64_t>(q->ndv_hint, 1024) + (16 << 20);
   r->t_submit = now_s();
   const int64_t budget = s->ctx->ledger.budget();
