@@ -1635,9 +1635,11 @@ __device__ __forceinline__ void batched_item(const Plan& P, const BatchItem& w, 
   }
 }
 
-template <int NA>
-__global__ void __launch_bounds__(512) batched_kernel(const Plan* plans, const BatchItem* items, int64_t n_items,
-                                                      unsigned long long* cursor) {
+// STATIC_ONLY: every query has a compiled shape, so the generic path (and its
+// registers) is left out and MB CTAs of 512 threads fit an SM.
+template <int NA, bool STATIC_ONLY, int MB>
+__global__ void __launch_bounds__(512, MB) batched_kernel(const Plan* plans, const BatchItem* items, int64_t n_items,
+                                                          unsigned long long* cursor) {
   extern __shared__ unsigned long long sm[];
   __shared__ int s_groups;
   __shared__ long long s_item;
@@ -1651,7 +1653,9 @@ __global__ void __launch_bounds__(512) batched_kernel(const Plan* plans, const B
     switch (P.shape) {
       case SHAPE_BATCH_I64: batched_item<ShapeBatchI64::n_aggs, StatShape<ShapeBatchI64>>(P, w, sm, &s_groups); break;
       case SHAPE_BATCH_F64: batched_item<ShapeBatchF64::n_aggs, StatShape<ShapeBatchF64>>(P, w, sm, &s_groups); break;
-      default: batched_item<NA, DynShape>(P, w, sm, &s_groups); break;
+      default:
+        if constexpr (!STATIC_ONLY) batched_item<NA, DynShape>(P, w, sm, &s_groups);
+        break;
     }
     __syncthreads();
   }
@@ -1667,6 +1671,7 @@ struct wg_batched {
   std::vector<std::vector<wg_predicate>> filters;
   wg_tune_params tp{};
   int max_na = 4;
+  bool all_static = false;   // every query runs a compiled shape
   size_t dyn_smem = 0;
   std::vector<wgd::Plan> plans_h;
   std::vector<BatchItem> items_h;
@@ -1685,6 +1690,7 @@ static wg_status batched_plan(wg_batched* b) {
   b->plans_h.assign((size_t)n, wgd::Plan{});
   b->reset_h.assign((size_t)n, ResetDesc{});
   b->max_na = 4;
+  b->all_static = true;
   int64_t max_smem_words = 0;
   for (int q = 0; q < n; ++q) {
     wg_agg* a = b->aggs[q];
@@ -1720,6 +1726,7 @@ static wg_status batched_plan(wg_batched* b) {
     if (P.shape != wgd::SHAPE_BATCH_I64 && P.shape != wgd::SHAPE_BATCH_F64) P.shape = wgd::SHAPE_GENERIC;
     a->last_shape = P.shape;
     if (a->L.n_aggs > 4) b->max_na = 8;
+    if (P.shape == wgd::SHAPE_GENERIC) b->all_static = false;
     ResetDesc& rd = b->reset_h[q];
     rd.slots = a->table.as<unsigned long long>();
     rd.words = table_words(a, a->cap);
@@ -1757,14 +1764,15 @@ static void batched_enqueue(wg_batched* b, cudaStream_t st) {
   batched_reset_kernel<<<std::min(n, ctx->sm_count * 8), 256, 0, st>>>(b->resets.as<ResetDesc>(), n);
   cudaMemsetAsync(b->cursor.get(), 0, 8, st);
   const unsigned grid = (unsigned)(ctx->sm_count * std::max(1, b->tp.ctas_per_sm));
-  if (b->max_na <= 4) {
-    batched_kernel<4><<<grid, b->tp.block, b->dyn_smem, st>>>(b->plans.as<wgd::Plan>(), b->items.as<BatchItem>(),
-                                                             (int64_t)b->items_h.size(),
-                                                             b->cursor.as<unsigned long long>());
+  if (b->all_static) {
+    batched_kernel<4, true, 2><<<grid, b->tp.block, b->dyn_smem, st>>>(
+        b->plans.as<wgd::Plan>(), b->items.as<BatchItem>(), (int64_t)b->items_h.size(), b->cursor.as<unsigned long long>());
+  } else if (b->max_na <= 4) {
+    batched_kernel<4, false, 2><<<grid, b->tp.block, b->dyn_smem, st>>>(
+        b->plans.as<wgd::Plan>(), b->items.as<BatchItem>(), (int64_t)b->items_h.size(), b->cursor.as<unsigned long long>());
   } else {
-    batched_kernel<8><<<grid, b->tp.block, b->dyn_smem, st>>>(b->plans.as<wgd::Plan>(), b->items.as<BatchItem>(),
-                                                             (int64_t)b->items_h.size(),
-                                                             b->cursor.as<unsigned long long>());
+    batched_kernel<8, false, 2><<<grid, b->tp.block, b->dyn_smem, st>>>(
+        b->plans.as<wgd::Plan>(), b->items.as<BatchItem>(), (int64_t)b->items_h.size(), b->cursor.as<unsigned long long>());
   }
   batched_count_kernel<<<(n + 255) / 256, 256, 0, st>>>(b->resets.as<ResetDesc>(), n, b->counts.as<long long>());
   cudaMemcpyAsync(b->counts_host, b->counts.get(), 8 * (size_t)n, cudaMemcpyDeviceToHost, st);
@@ -1774,8 +1782,9 @@ static wg_status batched_capture(wg_batched* b) {
   Ctx* ctx = b->ctx;
   if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
   if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
-  WG_CUDA_TRY(cudaFuncSetAttribute(batched_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->dyn_smem));
-  WG_CUDA_TRY(cudaFuncSetAttribute(batched_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->dyn_smem));
+  WG_CUDA_TRY(cudaFuncSetAttribute(batched_kernel<4, true, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->dyn_smem));
+  WG_CUDA_TRY(cudaFuncSetAttribute(batched_kernel<4, false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->dyn_smem));
+  WG_CUDA_TRY(cudaFuncSetAttribute(batched_kernel<8, false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->dyn_smem));
   WG_CUDA_TRY(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
   batched_enqueue(b, ctx->stream);
   WG_CUDA_TRY(cudaStreamEndCapture(ctx->stream, &b->graph));
