@@ -845,6 +845,9 @@ static wg_status run_device(const PipelineRun& r) {
   ls.smem_bytes = ls.smem ? (size_t)S * ls.P.smem_sw * 8 : 0;
   ls.P.prefetch = std::max(0, env_int("WG_PREFETCH", 2));
   ls.P.smem_combine = env_int("WG_SMEM_COMBINE", 0) != 0;
+  // many rows per group: most MIN/MAX updates cannot win, so read before the atomic
+  const int mm = env_int("WG_MINMAX_TEST", -1);
+  ls.P.minmax_test = mm >= 0 ? (mm != 0) : (n_items >= 8 * std::max<int64_t>(expect, 1));
   const int64_t rows_per_cta = (int64_t)ls.block * (ls.vec ? ls.vec : 1);
   const int64_t want_ctas = (n_items + rows_per_cta - 1) / rows_per_cta + 1;
   ls.grid = (unsigned)std::min<int64_t>((int64_t)ctx->sm_count * blocks_per_sm, want_ctas);
@@ -1722,6 +1725,10 @@ static wg_status batched_plan(wg_batched* b) {
       max_smem_words = std::max<int64_t>(max_smem_words, (int64_t)S * a->L.slot_words);
     }
     P.smem_slots = S;
+    {
+      const int mm = env_int("WG_MINMAX_TEST", -1);
+      P.minmax_test = mm >= 0 ? (mm != 0) : (b->inputs[q].len >= 8 * std::max<int64_t>(a->hint, 1));
+    }
     P.shape = pick_shape(P);
     if (P.shape != wgd::SHAPE_BATCH_I64 && P.shape != wgd::SHAPE_BATCH_F64) P.shape = wgd::SHAPE_GENERIC;
     a->last_shape = P.shape;

@@ -91,6 +91,8 @@ struct Plan {
   int32_t gdense;                // 1: the shared table is indexed by key - gmin (keys known to lie in
                                  //    [gmin, gmin + smem_slots)), no hashing and no key words
   long long gmin;
+  int32_t minmax_test;           // 1: HBM MIN/MAX read the slot first and skip an atomic that cannot win
+  int32_t _pad2;
   DCol in[WG_MAX_IN];
   Pred filt[WG_MAX_FILTERS];
   JoinView join;

@@ -396,7 +396,8 @@ __device__ __forceinline__ void smem_add_limbs(unsigned* L, int nlimbs, unsigned
 // which divides those replays by about `rep`; the flush adds the copies.
 template <int NA, bool SH, class Lay>
 __device__ __forceinline__ void apply(const Lay& ly, unsigned long long* s, const Contrib<NA>& c,
-                                      unsigned long long rows, int rep = 1) {
+                                      unsigned long long rows, int rep = 1, bool test_first = false) {
+  const bool test = SH || test_first;  // MIN/MAX: read the slot, skip an atomic that cannot win
   if (SH) atomicAdd((unsigned*)(s + ly.key_words()), (unsigned)rows);
   else atomicAdd(s + ly.key_words(), rows);
   const int copy = SH && rep > 1 ? (int)(threadIdx.x & 31) & (rep - 1) : 0;
@@ -421,18 +422,18 @@ __device__ __forceinline__ void apply(const Lay& ly, unsigned long long* s, cons
         else atomic_add128(t, w0, w1);
         break;
       case K_MIN_I64:
-        if (w0 != 0x7FFFFFFFFFFFFFFFULL && (!SH || (long long)w0 < *(volatile long long*)t))
+        if (w0 != 0x7FFFFFFFFFFFFFFFULL && (!test || (long long)w0 < *(volatile long long*)t))
           atomicMin((long long*)t, (long long)w0);
         break;
       case K_MAX_I64:
-        if (w0 != 0x8000000000000000ULL && (!SH || (long long)w0 > *(volatile long long*)t))
+        if (w0 != 0x8000000000000000ULL && (!test || (long long)w0 > *(volatile long long*)t))
           atomicMax((long long*)t, (long long)w0);
         break;
       case K_MIN_F64:
-        if (w0 != ~0ULL && (!SH || w0 < *(volatile unsigned long long*)t)) atomicMin(t, w0);
+        if (w0 != ~0ULL && (!test || w0 < *(volatile unsigned long long*)t)) atomicMin(t, w0);
         break;
       case K_MAX_F64:
-        if (w0 != 0ULL && (!SH || w0 > *(volatile unsigned long long*)t)) atomicMax(t, w0);
+        if (w0 != 0ULL && (!test || w0 > *(volatile unsigned long long*)t)) atomicMax(t, w0);
         break;
       case K_MIN_DEC: atomic_min128((U128*)t, w0, w1); break;
       case K_MAX_DEC: atomic_max128((U128*)t, w0, w1); break;
@@ -612,7 +613,7 @@ __device__ __forceinline__ void warp_update(const Plan& P, const Sh& sh, bool cu
       }
     }
     unsigned long long* s = find_global(sh, P.T, k0, k1, knull, P.err);
-    if (s != nullptr) apply<NA, false>(sh, s, c, (unsigned long long)mysz);
+    if (s != nullptr) apply<NA, false>(sh, s, c, (unsigned long long)mysz, 1, P.minmax_test != 0);
   }
 }
 
