@@ -47,6 +47,8 @@ CPU_SAMPLE_ROWS = 1 << 24
 # profiles/pipeline_vec_kernel_starjoin_2p24.md
 NCU_TRAFFIC_BYTES_PER_FACT_ROW = 600.49e6 / (1 << 24)
 METRIC = "rows/s (filter+join+hash-agg, star join 2^28 fact rows)"
+STARJOIN_WORKLOAD = ("star join + aggregate: 2^28 fact rows x 2^22 dim rows, qty>10, GROUP BY grp (1000 groups), "
+                     "SUM(price*(1-disc)) f64 + SUM(price) Int128")
 
 
 def parse_args():
@@ -175,8 +177,9 @@ def run_reference(args, rank: int):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int128+f64", "data": "synthetic",
-        "config": {"workload": "star join + aggregate (sample of 2^24 fact rows per step)", "fact_rows": CPU_SAMPLE_ROWS,
-                   "dim_rows": DIM_ROWS, "groups": GROUPS, "parallelism": f"{threads} host threads"},
+        "config": {"workload": STARJOIN_WORKLOAD, "fact_rows_per_gpu": FACT_ROWS, "dim_rows": DIM_ROWS,
+                   "groups": GROUPS, "sample_fact_rows_per_step": CPU_SAMPLE_ROWS,
+                   "parallelism": f"{threads} host threads"},
         "cpu_baseline": {"value": value, "unit": "rows/s", "cores": threads, "kind": "port",
                          "sample": f"{CPU_SAMPLE_ROWS} fact rows per step (of the 2^28-row workload), "
                                    "C++ restatement of the reference's Pipeline.Run (Go toolchain absent)"},
@@ -328,8 +331,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
             "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int128+f64", "data": "synthetic",
-            "config": {"workload": "star join + aggregate: 2^28 fact rows x 2^22 dim rows, qty>10, GROUP BY grp "
-                                   "(1000 groups), SUM(price*(1-disc)) f64 + SUM(price) Int128",
+            "config": {"workload": STARJOIN_WORKLOAD,
                        "fact_rows_per_gpu": n, "dim_rows": DIM_ROWS, "groups": GROUPS,
                        "parallelism": f"dp{world}" if world > 1 else "single",
                        "l2": "inputs (8.6 GB/rank) larger than L2; no flush"},
