@@ -162,6 +162,28 @@ def cpu_pipeline_sample(rows: int, threads: int, repeats: int = 1):
     return rows / best, best
 
 
+def cpu_groupby_sample(rows: int, threads: int) -> float:
+    """rows/s of the oracle's Pipeline.Run on the group-by workload (host-resident sample)."""
+    from oracle import binding as ob
+    k, v, f, flag = ob.gen_groupby(rows, threads=threads)
+    batch = ob.HostBatch([(2, k, None, 0), (2, v, None, 0), (4, f, None, 0), (1, flag, None, 0)])
+    t0 = time.perf_counter()
+    agg = ob.Agg([0], [(0, 1, 0), (1, -1, 0), (2, 2, 0), (3, 2, 0)])
+    ob.pipeline(batch, agg, filters=[(3, 2, 7)], threads=threads)
+    return rows / (time.perf_counter() - t0)
+
+
+def cpu_highcard_sample(rows: int, threads: int) -> float:
+    """rows/s of the oracle's Pipeline.Run on the high-cardinality workload (host-resident sample)."""
+    from oracle import binding as ob
+    a, b, amt, x = ob.gen_highcard(rows, threads=threads)
+    batch = ob.HostBatch([(1, a, None, 0), (2, b, None, 0), (17, amt, None, 2), (4, x, None, 0)])
+    t0 = time.perf_counter()
+    agg = ob.Agg([0, 1], [(0, 2, 0), (1, -1, 0), (2, 3, 0), (3, 3, 0)])
+    ob.pipeline(batch, agg, threads=threads)
+    return rows / (time.perf_counter() - t0)
+
+
 def run_reference(args, rank: int):
     if rank != 0:
         return
@@ -393,10 +415,15 @@ def run_groupby(args):
 
         ms = _timed_ms(stream, step, args.steps, args.warmup)
         alg = n * 28 + 4096 * 40
+        threads = os.cpu_count() or 1
+        sample = min(n, 1 << 24)
+        cpu = None if args.no_cpu_baseline else {
+            "value": cpu_groupby_sample(sample, threads), "unit": "rows/s", "cores": threads, "kind": "port",
+            "sample": f"{sample} rows of the same workload, oracle Pipeline.Run, one worker per host thread"}
         print(json.dumps({"workload": "groupby", "metric": "rows/s", "rows": n, "value": n / (ms / 1e3),
                           "unit": "rows/s", "ms_per_step": ms, "hbm_gbs": alg / (ms / 1e3) / 1e9,
-                          "frac_of_peak": alg / (ms / 1e3) / 1e9 / peak, "peak_kind": peak_kind_note(kind)}),
-              flush=True)
+                          "frac_of_peak": alg / (ms / 1e3) / 1e9 / peak, "peak_kind": peak_kind_note(kind),
+                          "cpu_baseline": cpu}), flush=True)
         agg.close()
         del k, v, f, flag
         torch.cuda.empty_cache()
@@ -433,11 +460,18 @@ def run_highcard(args, hbm_cap: int = 0):
     ms = _timed_ms(stream, step, args.steps, max(1, args.warmup))
     peak, kind = measured_peak_hbm()
     alg = n * 36 + groups[0] * (16 + 16 + 8 + 8 + 8)
+    threads = os.cpu_count() or 1
+    sample = min(n, 1 << 22)
+    cpu = None if args.no_cpu_baseline or hbm_cap else {
+        "value": cpu_highcard_sample(sample, threads), "unit": "rows/s", "cores": threads, "kind": "port",
+        "sample": f"{sample} rows of the same workload (near-unique keys), oracle Pipeline.Run, one worker per "
+                  "host thread"}
     print(json.dumps({"workload": "highcard_spill" if hbm_cap else "highcard", "hbm_cap_bytes": hbm_cap,
                       "metric": "rows/s", "rows": n, "groups": groups[0],
                       "value": n / (ms / 1e3), "unit": "rows/s", "ms_per_step": ms,
                       "hbm_gbs": alg / (ms / 1e3) / 1e9, "frac_of_peak": alg / (ms / 1e3) / 1e9 / peak,
-                      "peak_kind": peak_kind_note(kind), "ledger_peak_bytes": ctx.ledger()["peak"]}), flush=True)
+                      "peak_kind": peak_kind_note(kind), "ledger_peak_bytes": ctx.ledger()["peak"],
+                      "cpu_baseline": cpu}), flush=True)
     agg.close()
     ctx.close()
 
