@@ -16,7 +16,6 @@
 #include "wg_launch.cuh"
 
 #include <algorithm>
-#include <type_traits>
 #include <cstdlib>
 
 namespace wg {
@@ -1612,45 +1611,30 @@ __global__ void batched_count_kernel(const ResetDesc* rd, int n, long long* out)
   }
 }
 
-// The rows of one work item.
-template <int NA, bool SMEM, class Sh>
-__device__ __forceinline__ void batched_rows(const Plan& P, const Sh& sh, const BatchItem& w, unsigned long long* sm,
-                                             int* s_groups, int s_limit) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  if constexpr (!std::is_same<Sh, DynShape>::value) {
-    // compiled shapes: two rows per lane with 16-byte loads, the item's next
-    // rows prefetched into L2 two warp-strides ahead
-    const int64_t end = w.row0 + w.rows;
-    const int64_t first = w.row0 + (int64_t)warp * 64;
-    Prefetcher<64> pf;
-    pf.init(P, sh, first + 2 * (int64_t)nw * 64, (int64_t)nw * 64, lane);
-    for (int64_t base = first; base < end; base += (int64_t)nw * 64) {
-      pf.next();
-      process_rows_vec<NA, SMEM, 2>(P, sh, base + 2 * lane, end, sm, s_groups, s_limit);
-    }
-  } else {
-    for (int base = warp * 32; base < w.rows; base += nw * 32) {
-      const int i = base + lane;
-      SrcGlobal src{w.row0 + (i < w.rows ? i : 0)};
-      process_rows<NA, SMEM>(P, sh, src, i < w.rows, sm, s_groups, s_limit);
-    }
-  }
-}
-
 // One work item (a window of one query's rows) on shape Sh.
 template <int NA, class Sh>
 __device__ __forceinline__ void batched_item(const Plan& P, const BatchItem& w, unsigned long long* sm,
                                              int* s_groups) {
   const Sh sh{P};
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int S = P.smem_slots;
   if (Sh::smem_ok && S > 0) {
     smem_table_init(P, sm, S, s_groups);
     __syncthreads();
-    batched_rows<NA, Sh::smem_ok>(P, sh, w, sm, s_groups, (S * 7) / 8);
+    const int s_limit = (S * 7) / 8;
+    for (int base = warp * 32; base < w.rows; base += nw * 32) {
+      const int i = base + lane;
+      SrcGlobal src{w.row0 + (i < w.rows ? i : 0)};
+      process_rows<NA, Sh::smem_ok>(P, sh, src, i < w.rows, sm, s_groups, s_limit);
+    }
     __syncthreads();
     smem_table_flush<NA>(P, sm, S);
   } else {
-    batched_rows<NA, false>(P, sh, w, sm, s_groups, 0);
+    for (int base = warp * 32; base < w.rows; base += nw * 32) {
+      const int i = base + lane;
+      SrcGlobal src{w.row0 + (i < w.rows ? i : 0)};
+      process_rows<NA, false>(P, sh, src, i < w.rows, sm, s_groups, 0);
+    }
   }
 }
 

@@ -909,8 +909,8 @@ struct SrcRow {
 // Rows r0 .. r0+U-1 (r0 a multiple of U, column starts 16-byte aligned): one
 // vector load per 16 bytes when all U rows exist, row by row at the end.
 template <int U, class Sh>
-__device__ __forceinline__ void load_rows(const Plan& P, const Sh& sh, int64_t r0, int64_t end, SrcRow (&rw)[U]) {
-  const bool full = r0 + U <= end;
+__device__ __forceinline__ void load_rows(const Plan& P, const Sh& sh, int64_t r0, SrcRow (&rw)[U]) {
+  const bool full = r0 + U <= P.n_items;
 #pragma unroll
   for (int j = 0; j < WG_MAX_IN; ++j) {
     if (j >= sh.n_in()) break;
@@ -952,7 +952,7 @@ __device__ __forceinline__ void load_rows(const Plan& P, const Sh& sh, int64_t r
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         const int64_t row = r0 + u;
-        if (row < end) {
+        if (row < P.n_items) {
           rw[u].v[j] = load_stream(P.in[j].data, cls, row);
           rw[u].v[j].null = is_null(P.in[j], row);
         } else {
@@ -964,18 +964,17 @@ __device__ __forceinline__ void load_rows(const Plan& P, const Sh& sh, int64_t r
 }
 
 // U rows per lane (no join, or the direct-payload join): filters and lookups
-// for all rows first, then one warp-wide update per row. Rows from `end` on
-// are not this call's.
+// for all rows first, then one warp-wide update per row.
 template <int NA, bool SMEM, int U, class Sh>
-__device__ __forceinline__ void process_rows_vec(const Plan& P, const Sh& sh, int64_t r0, int64_t end,
-                                                 unsigned long long* sm, int* s_groups, int s_limit) {
+__device__ __forceinline__ void process_rows_vec(const Plan& P, const Sh& sh, int64_t r0, unsigned long long* sm,
+                                                 int* s_groups, int s_limit) {
   SrcRow rw[U];
-  load_rows<U>(P, sh, r0, end, rw);
+  load_rows<U>(P, sh, r0, rw);
   bool act[U];
   int32_t brow[U];
 #pragma unroll
   for (int u = 0; u < U; ++u) {
-    act[u] = r0 + u < end;
+    act[u] = r0 + u < P.n_items;
     brow[u] = -1;
 #pragma unroll
     for (int f = 0; f < WG_MAX_FILTERS; ++f) {
@@ -1032,7 +1031,7 @@ __global__ void __launch_bounds__(512, MB) pipeline_vec_kernel(const __grid_cons
   if (ahead > 0) pf.init(P, sh, base0 + ahead, step, lane);
   for (int64_t base = base0; base < P.n_items; base += step) {
     pf.next();
-    process_rows_vec<NA, SMEM, U>(P, sh, base + (int64_t)lane * U, P.n_items, sm, &s_groups, s_limit);
+    process_rows_vec<NA, SMEM, U>(P, sh, base + (int64_t)lane * U, sm, &s_groups, s_limit);
   }
   if (SMEM) {
     __syncthreads();
