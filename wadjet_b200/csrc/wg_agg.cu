@@ -56,6 +56,7 @@ __device__ __forceinline__ bool slot_used(const Layout& L, const unsigned long l
 // layout upgrades are all this one kernel.
 template <int NA>
 __global__ void fold_kernel(Layout Ls, Table Ts, Layout Ld, Table Td, int32_t* err) {
+  Credit cr;
   const uint64_t cap = Ts.mask + 1;
   const uint64_t n = Ls.key_words == 0 ? 1 : cap + 2;
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
@@ -69,12 +70,13 @@ __global__ void fold_kernel(Layout Ls, Table Ts, Layout Ld, Table Td, int32_t* e
       else { k0 = s[0]; if (Ls.key_words == 2) k1 = s[1]; }
     }
     const LayoutAcc ls{Ls}, ld{Ld};
-    unsigned long long* d = find_global(ld, Td, k0, k1, knull, err);
+    unsigned long long* d = find_global(ld, Td, k0, k1, knull, err, &cr);
     if (!d) continue;
     Contrib<NA> c;
     slot_contrib<NA>(ls, s, c);
     apply<NA, false>(ld, d, c, s[Ls.key_words]);
   }
+  cr.release(Td);
 }
 
 // out[i] = the slot list[i] of a table (slot_words words each): one partition's
@@ -299,16 +301,31 @@ struct wg_agg {
 
 namespace wg {
 
+// Most threads one aggregate launch runs (pipeline grids of up to 4 CTAs of
+// 768 threads per SM; the batched mode checks its tables after the run).
+static int64_t max_launch_threads(Ctx* ctx) { return (int64_t)ctx->sm_count * 4 * 768; }
+
 static wgd::Table table_view(wg_agg* a) {
   wgd::Table T;
   T.slots = a->table.as<unsigned long long>();
   T.n_groups = a->ctr.as<unsigned long long>();
   T.overflow = (int32_t*)(a->ctr.as<unsigned long long>() + 1);
   T.shift = a->shift;
-  T._pad = 0;
   T.mask = a->cap - 1;
   T.limit = (unsigned long long)((double)a->cap * kMaxLoad);
+  // Large tables: a thread reserves up to 16 groups at a time, so the
+  // reservation counter is not one contended atomic per new group. Unused
+  // reservations held by running threads read as groups, so the chunk is kept
+  // to where they stay under 1/8 of the limit (credit_slack); small tables
+  // reserve one group per insert.
+  const int64_t per = (int64_t)T.limit / (8 * max_launch_threads(a->ctx));
+  T.credit_chunk = (int32_t)std::max<int64_t>(1, std::min<int64_t>(16, 1 + per));
   return T;
+}
+
+// Reservations that running threads may hold beyond the groups they inserted.
+static int64_t credit_slack(wg_agg* a) {
+  return (int64_t)(table_view(a).credit_chunk - 1) * max_launch_threads(a->ctx);
 }
 
 static int64_t table_words(const wg_agg* a, uint64_t cap) {
@@ -575,6 +592,10 @@ static wg_status launch_pipeline(wg_agg* a, const LaunchSpec& ls, int64_t n_item
   LaunchSpec l2 = ls;
   wgd::Plan& P = l2.P;
   P.T = table_view(a);
+  // a launch with more threads than the launch policy's slack assumes takes
+  // one reservation per insert
+  const int64_t threads = (int64_t)ls.grid * (ls.tile ? 32 * (1 + ls.cfg.consumers) : ls.block);
+  if (threads > max_launch_threads(ctx)) P.T.credit_chunk = 1;
   P.L = launch_layout(a, ls.P);
   P.n_items = n_items;
   if (l2.tile) l2.cfg.n_tiles = (n_items + l2.cfg.rows - 1) / l2.cfg.rows;
@@ -911,7 +932,9 @@ static wg_status run_device(const PipelineRun& r) {
     ls.smem_bytes = 0;
   }
   const wgd::Plan base = ls.P;
-  auto limit = [&]() { return (int64_t)((double)a->cap * kMaxLoad); };
+  // the room the launch policy plans with: the table's limit less the
+  // reservations threads may hold unused
+  auto limit = [&]() { return (int64_t)((double)a->cap * kMaxLoad) - credit_slack(a); };
 
   // 1) provably safe: one launch
   if (a->L.key_words == 0 || a->upper_groups + n_items * fan <= limit()) {
@@ -1616,6 +1639,7 @@ template <int NA, class Sh>
 __device__ __forceinline__ void batched_item(const Plan& P, const BatchItem& w, unsigned long long* sm,
                                              int* s_groups) {
   const Sh sh{P};
+  Credit cr;  // reservations in this query's table, handed back before the next item
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int S = P.smem_slots;
   if (Sh::smem_ok && S > 0) {
@@ -1625,17 +1649,18 @@ __device__ __forceinline__ void batched_item(const Plan& P, const BatchItem& w, 
     for (int base = warp * 32; base < w.rows; base += nw * 32) {
       const int i = base + lane;
       SrcGlobal src{w.row0 + (i < w.rows ? i : 0)};
-      process_rows<NA, Sh::smem_ok>(P, sh, src, i < w.rows, sm, s_groups, s_limit);
+      process_rows<NA, Sh::smem_ok>(P, sh, src, i < w.rows, sm, s_groups, s_limit, cr);
     }
     __syncthreads();
-    smem_table_flush<NA>(P, sm, S);
+    smem_table_flush<NA>(P, sm, S, cr);
   } else {
     for (int base = warp * 32; base < w.rows; base += nw * 32) {
       const int i = base + lane;
       SrcGlobal src{w.row0 + (i < w.rows ? i : 0)};
-      process_rows<NA, false>(P, sh, src, i < w.rows, sm, s_groups, 0);
+      process_rows<NA, false>(P, sh, src, i < w.rows, sm, s_groups, 0, cr);
     }
   }
+  cr.release(P.T);
 }
 
 // STATIC_ONLY: every query has a compiled shape, so the generic path (and its

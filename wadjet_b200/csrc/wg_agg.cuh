@@ -64,7 +64,7 @@ struct Table {
   unsigned long long* n_groups;  // regular slots taken (reservations)
   int32_t* overflow;             // set when an insert was refused at the limit
   int32_t shift;
-  int32_t _pad;
+  int32_t credit_chunk;          // group reservations a thread takes from n_groups at a time (1 = one per insert)
   uint64_t mask;                 // cap - 1
   unsigned long long limit;      // max regular groups before inserts are refused
 };

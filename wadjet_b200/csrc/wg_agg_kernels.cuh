@@ -456,12 +456,43 @@ __device__ __forceinline__ void slot_contrib(const Lay& ly, const unsigned long 
   }
 }
 
+// A thread's unused group reservations (Table::n_groups counts reserved groups;
+// an insert must hold one). Taken credit_chunk at a time and handed back when
+// the thread is done, so n_groups is exact again after the kernel.
+struct Credit {
+  unsigned long long n = 0;
+  __device__ __forceinline__ bool take(const Table& T, int chunk) {
+    if (n == 0) {
+      const unsigned long long want = (unsigned long long)max(1, chunk);
+      const unsigned long long r = atomicAdd(T.n_groups, want);
+      if (r >= T.limit) {
+        atomicAdd(T.n_groups, 0ULL - want);
+        return false;
+      }
+      const unsigned long long ok = min(want, T.limit - r);
+      if (ok < want) atomicAdd(T.n_groups, 0ULL - (want - ok));
+      n = ok;
+    }
+    --n;
+    return true;
+  }
+  __device__ __forceinline__ void give_back() { ++n; }
+  __device__ __forceinline__ void release(const Table& T) {
+    if (n) atomicAdd(T.n_groups, 0ULL - n);
+    n = 0;
+  }
+};
+
 // Find or insert the global slot of a key. Inserting claims a group
 // reservation first; past T.limit the insert is refused and the overflow flag
 // raised (the host then replays the launch on a larger table).
 template <class Lay>
 __device__ __forceinline__ unsigned long long* find_global(const Lay& ly, const Table& T, unsigned long long k0,
-                                                           unsigned long long k1, bool keynull, int32_t* err) {
+                                                           unsigned long long k1, bool keynull, int32_t* err,
+                                                           Credit* cr = nullptr) {
+  Credit local;  // without a caller's credit: exactly one reservation per insert
+  Credit& c = cr ? *cr : local;
+  const int chunk = cr ? T.credit_chunk : 1;
   const int sw = ly.slot_words();
   if (ly.key_words() == 0) return T.slots;
   const uint64_t cap = T.mask + 1;
@@ -474,15 +505,14 @@ __device__ __forceinline__ unsigned long long* find_global(const Lay& ly, const 
       unsigned long long cur = *((volatile unsigned long long*)s);
       if (cur == k0) return s;
       if (cur == WG_EMPTY_KEY) {
-        unsigned long long r = atomicAdd(T.n_groups, 1ULL);
-        if (r >= T.limit) {
-          atomicAdd(T.n_groups, ~0ULL);
+        if (!c.take(T, chunk)) {
           *T.overflow = 1;
           return nullptr;
         }
         unsigned long long old = atomicCAS(s, WG_EMPTY_KEY, k0);
         if (old == WG_EMPTY_KEY) return s;
-        atomicAdd(T.n_groups, ~0ULL);
+        c.give_back();
+        if (!cr) c.release(T);
         if (old == k0) return s;
       }
       h = (h + 1) & T.mask;
@@ -499,9 +529,7 @@ __device__ __forceinline__ unsigned long long* find_global(const Lay& ly, const 
       if (cur.lo != ~0ULL && cur.hi != ~0ULL) {
         if (cur.lo == k0 && cur.hi == k1) return s;
       } else {
-        unsigned long long r = atomicAdd(T.n_groups, 1ULL);
-        if (r >= T.limit) {
-          atomicAdd(T.n_groups, ~0ULL);
+        if (!c.take(T, chunk)) {
           *T.overflow = 1;
           return nullptr;
         }
@@ -509,7 +537,8 @@ __device__ __forceinline__ unsigned long long* find_global(const Lay& ly, const 
         U128 k; k.lo = k0; k.hi = k1;
         U128 old = cas128((U128*)s, e, k);
         if (old.lo == e.lo && old.hi == e.hi) return s;
-        atomicAdd(T.n_groups, ~0ULL);
+        c.give_back();
+        if (!cr) c.release(T);
         if (old.lo == k0 && old.hi == k1) return s;
       }
       h = (h + 1) & T.mask;
@@ -566,7 +595,7 @@ __device__ __forceinline__ unsigned long long* find_shared(const Plan& P, unsign
 template <int NA, bool SMEM, class Sh>
 __device__ __forceinline__ void warp_update(const Plan& P, const Sh& sh, bool cur, unsigned long long k0,
                                             unsigned long long k1, bool knull, Contrib<NA>& c,
-                                            unsigned long long* sm, int* s_groups, int s_limit) {
+                                            unsigned long long* sm, int* s_groups, int s_limit, Credit& cr) {
   const bool combine_first = SMEM && P.smem_combine != 0;
   if (SMEM && !combine_first && cur && !knull) {
     unsigned long long* s = find_shared(P, sm, k0, s_groups, s_limit);
@@ -612,7 +641,7 @@ __device__ __forceinline__ void warp_update(const Plan& P, const Sh& sh, bool cu
         return;
       }
     }
-    unsigned long long* s = find_global(sh, P.T, k0, k1, knull, P.err);
+    unsigned long long* s = find_global(sh, P.T, k0, k1, knull, P.err, &cr);
     if (s != nullptr) apply<NA, false>(sh, s, c, (unsigned long long)mysz, 1, P.minmax_test != 0);
   }
 }
@@ -662,7 +691,7 @@ __device__ __forceinline__ bool pred_val(const Plan& P, const Sh& sh, int f, con
 // HashAggregate.Consume. All 32 lanes call it together (act = row present).
 template <int NA, bool SMEM, class Sh, class Src>
 __device__ __forceinline__ void process_rows(const Plan& P, const Sh& sh, const Src& src, bool act,
-                                             unsigned long long* sm, int* s_groups, int s_limit) {
+                                             unsigned long long* sm, int* s_groups, int s_limit, Credit& cr) {
 #pragma unroll
   for (int f = 0; f < WG_MAX_FILTERS; ++f) {
     if (f >= sh.n_filters()) break;
@@ -693,7 +722,7 @@ __device__ __forceinline__ void process_rows(const Plan& P, const Sh& sh, const 
 #pragma unroll
       for (int a = 0; a < NA; ++a) { c.w0[a] = 0; c.w1[a] = 0; c.nul[a] = 0; }
     }
-    warp_update<NA, SMEM>(P, sh, cur, k0, k1, knull, c, sm, s_groups, s_limit);
+    warp_update<NA, SMEM>(P, sh, cur, k0, k1, knull, c, sm, s_groups, s_limit, cr);
     if (!sh.has_join() || sh.direct()) break;  // unique keys: at most one match
     if (act) {
       brow = __ldg(P.join.next + brow);         // arenaNext chain (join.go:2700)
@@ -714,7 +743,7 @@ __device__ __forceinline__ void smem_table_init(const Plan& P, unsigned long lon
 }
 
 template <int NA>
-__device__ __forceinline__ void smem_table_flush(const Plan& P, const unsigned long long* sm, int S) {
+__device__ __forceinline__ void smem_table_flush(const Plan& P, const unsigned long long* sm, int S, Credit& cr) {
   const LayoutAcc ly{P.L};
   const int sw = P.L.slot_words, ssw = smem_stride(P), rep = smem_copies(P);
   for (int i = threadIdx.x; i < S; i += blockDim.x) {
@@ -726,7 +755,7 @@ __device__ __forceinline__ void smem_table_flush(const Plan& P, const unsigned l
     } else if (key == WG_EMPTY_KEY) {
       continue;
     }
-    unsigned long long* g = find_global(ly, P.T, key, 0, false, P.err);
+    unsigned long long* g = find_global(ly, P.T, key, 0, false, P.err, &cr);
     if (g == nullptr) continue;
     Contrib<NA> c;
     slot_contrib<NA>(ly, s, c);
@@ -781,6 +810,7 @@ __global__ void __launch_bounds__(Sh::kBlock, Sh::kMinBlocks) pipeline_kernel(co
   extern __shared__ unsigned long long sm[];
   __shared__ int s_groups;
   const Sh sh{P};
+  Credit cr;  // this thread's group reservations, handed back at the end
   const int S = P.smem_slots;
   const int s_limit = (S * 7) / 8;
   if (SMEM) {
@@ -799,12 +829,13 @@ __global__ void __launch_bounds__(Sh::kBlock, Sh::kMinBlocks) pipeline_kernel(co
     const int64_t item = base + lane;
     const bool act = item < P.n_items;
     SrcGlobal src{act ? (P.sel ? (int64_t)__ldg(P.sel + item) : item) : 0};
-    process_rows<NA, SMEM>(P, sh, src, act, sm, &s_groups, s_limit);
+    process_rows<NA, SMEM>(P, sh, src, act, sm, &s_groups, s_limit, cr);
   }
   if (SMEM) {
     __syncthreads();
-    smem_table_flush<NA>(P, sm, S);
+    smem_table_flush<NA>(P, sm, S, cr);
   }
+  cr.release(P.T);
 }
 
 // ---------------------------------------------------------------------------
@@ -967,7 +998,7 @@ __device__ __forceinline__ void load_rows(const Plan& P, const Sh& sh, int64_t r
 // for all rows first, then one warp-wide update per row.
 template <int NA, bool SMEM, int U, class Sh>
 __device__ __forceinline__ void process_rows_vec(const Plan& P, const Sh& sh, int64_t r0, unsigned long long* sm,
-                                                 int* s_groups, int s_limit) {
+                                                 int* s_groups, int s_limit, Credit& cr) {
   SrcRow rw[U];
   load_rows<U>(P, sh, r0, rw);
   bool act[U];
@@ -1005,7 +1036,7 @@ __device__ __forceinline__ void process_rows_vec(const Plan& P, const Sh& sh, in
 #pragma unroll
       for (int a = 0; a < NA; ++a) { c.w0[a] = 0; c.w1[a] = 0; c.nul[a] = 0; }
     }
-    warp_update<NA, SMEM>(P, sh, cur, k0, k1, knull, c, sm, s_groups, s_limit);
+    warp_update<NA, SMEM>(P, sh, cur, k0, k1, knull, c, sm, s_groups, s_limit, cr);
   }
 }
 
@@ -1016,6 +1047,7 @@ __global__ void __launch_bounds__(512, MB) pipeline_vec_kernel(const __grid_cons
   extern __shared__ unsigned long long sm[];
   __shared__ int s_groups;
   const Sh sh{P};
+  Credit cr;  // this thread's group reservations, handed back at the end
   const int S = P.smem_slots;
   const int s_limit = (S * 7) / 8;
   if (SMEM) {
@@ -1031,12 +1063,13 @@ __global__ void __launch_bounds__(512, MB) pipeline_vec_kernel(const __grid_cons
   if (ahead > 0) pf.init(P, sh, base0 + ahead, step, lane);
   for (int64_t base = base0; base < P.n_items; base += step) {
     pf.next();
-    process_rows_vec<NA, SMEM, U>(P, sh, base + (int64_t)lane * U, sm, &s_groups, s_limit);
+    process_rows_vec<NA, SMEM, U>(P, sh, base + (int64_t)lane * U, sm, &s_groups, s_limit, cr);
   }
   if (SMEM) {
     __syncthreads();
-    smem_table_flush<NA>(P, sm, S);
+    smem_table_flush<NA>(P, sm, S, cr);
   }
+  cr.release(P.T);
 }
 
 // ---------------------------------------------------------------------------
@@ -1089,6 +1122,7 @@ __global__ void __launch_bounds__(544, 1) tile_pipeline_kernel(const __grid_cons
   unsigned long long* empty = bars + 8;
   unsigned long long* table = (unsigned long long*)(tsm + C.table_off);
   const Sh sh{P};
+  Credit cr;  // this thread's group reservations, handed back at the end
   const int S = P.smem_slots;
   const int s_limit = (S * 7) / 8;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1137,14 +1171,15 @@ __global__ void __launch_bounds__(544, 1) tile_pipeline_kernel(const __grid_cons
       for (int base = cw * 32; base < m; base += C.consumers * 32) {
         const int i = base + lane;
         SrcTile src{(const char*)st, row0, i < m ? i : 0, m, &C};
-        process_rows<NA, SMEM>(P, sh, src, i < m, table, &s_groups, s_limit);
+        process_rows<NA, SMEM>(P, sh, src, i < m, table, &s_groups, s_limit, cr);
       }
       __syncwarp();
       if (lane == 0) mbar_arrive(&empty[s]);
     }
   }
   __syncthreads();
-  if (SMEM) smem_table_flush<NA>(P, table, S);
+  if (SMEM) smem_table_flush<NA>(P, table, S, cr);
+  cr.release(P.T);
 }
 
 }  // namespace wgd
