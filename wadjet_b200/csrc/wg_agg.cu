@@ -866,8 +866,6 @@ static wg_status run_device(const PipelineRun& r) {
   ls.smem_bytes = ls.smem ? (size_t)S * ls.P.smem_sw * 8 : 0;
   ls.P.prefetch = std::max(0, env_int("WG_PREFETCH", 2));
   ls.P.smem_combine = env_int("WG_SMEM_COMBINE", 0) != 0;
-  // HBM tables well beyond L2: prefetch the next iteration's home slots
-  ls.P.slot_prefetch = env_int("WG_SLOT_PREFETCH", 1) != 0 && table_words(a, a->cap) * 8 > (int64_t(256) << 20);
   // many rows per group: most MIN/MAX updates cannot win, so read before the atomic
   const int mm = env_int("WG_MINMAX_TEST", -1);
   ls.P.minmax_test = mm >= 0 ? (mm != 0) : (n_items >= 8 * std::max<int64_t>(expect, 1));

@@ -92,7 +92,7 @@ struct Plan {
                                  //    [gmin, gmin + smem_slots)), no hashing and no key words
   long long gmin;
   int32_t minmax_test;           // 1: HBM MIN/MAX read the slot first and skip an atomic that cannot win
-  int32_t slot_prefetch;         // 1: HBM table larger than L2: prefetch next rows' home slots
+  int32_t _pad2;
   DCol in[WG_MAX_IN];
   Pred filt[WG_MAX_FILTERS];
   JoinView join;

@@ -1041,48 +1041,6 @@ __device__ __forceinline__ void process_rows_vec(const Plan& P, const Sh& sh, in
 }
 
 // Grid-stride over chunks of 32*U rows; MB CTAs of 512 threads per SM.
-// The 64-bit hash whose top bits are a key's home slot in the HBM table (the
-// hash fib_slot / packed_slot shift down), or nothing for a NULL key. Reads
-// only key columns (and projections), never sets an error.
-template <class Sh>
-__device__ __forceinline__ bool row_key_hash(const Plan& P, const Sh& sh, int64_t row, unsigned long long& h) {
-  const SrcGlobal src{row};
-  ExprVals ev;
-  eval_exprs(P, sh, src, -1, ev);
-  if (sh.key_words() == 1) {
-    const Val v = fetch(P, sh, src, sh.key_vcol(0), -1, ev);
-    h = fib_slot(v.lo, 0);
-    return !v.null && v.lo != WG_EMPTY_KEY;
-  }
-  unsigned long long k0 = 0, k1 = 0;
-#pragma unroll
-  for (int k = 0; k < WG_MAX_KEYS; ++k) {
-    if (k >= sh.n_keys()) break;
-    const Val v = fetch(P, sh, src, sh.key_vcol(k), -1, ev);
-    if (v.null) return false;
-    const unsigned long long w =
-        sh.key_i32(k) ? ((unsigned long long)(uint32_t)(int32_t)v.lo) << sh.key_shift(k) : v.lo;
-    if (sh.key_word(k) == 0) k0 |= w; else k1 |= w;
-  }
-  h = packed_slot(k0, k1, 0);
-  return true;
-}
-
-// Ask L2 for the home slots of this lane's U rows from r0: the probes of the
-// next grid-stride iteration then start from L2 instead of HBM (the table is
-// far larger than L2 and every row's slot is a random line).
-template <int U, class Sh>
-__device__ __forceinline__ void prefetch_slots(const Plan& P, const Sh& sh, int64_t r0) {
-#pragma unroll
-  for (int u = 0; u < U; ++u) {
-    unsigned long long h;
-    if (r0 + u < P.n_items && row_key_hash(P, sh, r0 + u, h)) {
-      const unsigned long long* s = P.T.slots + (h >> P.T.shift) * sh.slot_words();
-      asm volatile("prefetch.global.L2 [%0];" ::"l"(s));
-    }
-  }
-}
-
 template <int NA, bool SMEM, class Sh, int U, int MB>
 __global__ void __launch_bounds__(512, MB) pipeline_vec_kernel(const __grid_constant__ Plan P) {
   static_assert(U == 2 || U == 4, "rows per lane");
@@ -1103,11 +1061,8 @@ __global__ void __launch_bounds__(512, MB) pipeline_vec_kernel(const __grid_cons
   const int64_t base0 = ((int64_t)blockIdx.x * wpb + (threadIdx.x >> 5)) * 32 * U;
   Prefetcher<32 * U> pf;
   if (ahead > 0) pf.init(P, sh, base0 + ahead, step, lane);
-  const bool slots_ahead = !SMEM && sh.key_words() >= 1 && P.slot_prefetch != 0;
-  if (slots_ahead) prefetch_slots<U>(P, sh, base0 + (int64_t)lane * U);
   for (int64_t base = base0; base < P.n_items; base += step) {
     pf.next();
-    if (slots_ahead) prefetch_slots<U>(P, sh, base + step + (int64_t)lane * U);
     process_rows_vec<NA, SMEM, U>(P, sh, base + (int64_t)lane * U, sm, &s_groups, s_limit, cr);
   }
   if (SMEM) {
