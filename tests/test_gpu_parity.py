@@ -206,6 +206,26 @@ def test_aggregate_device_batches_and_growth(ctx):
     assert_groups_equal(res[1][0], res[1][1], kinds[6:], magnitude=res[1][4])
 
 
+def test_large_table_growth_with_chunked_reservations(ctx):
+    """2^23 rows of near-unique int64 keys into a table sized for 2^22 groups: the table is large
+    enough that threads reserve groups several at a time, and it has to grow mid-run; every row
+    must still land exactly once."""
+    import torch
+    import wadjet_b200 as wg
+    rng = np.random.default_rng(23)
+    n = 1 << 23
+    k = (rng.integers(0, 1 << 40, n).astype(np.int64) * 3) + 1
+    v = rng.integers(-1000, 1000, n).astype(np.int64)
+    g = wg.HashAggregate(ctx, [0], [wg.AggColumn(wg.AGG_COUNT, -1), wg.AggColumn(wg.AGG_SUM, 1)], ndv_hint=1 << 22)
+    wg.run_pipeline(ctx, wg.Batch([wg.Column(I64, torch.from_numpy(k).cuda()), wg.Column(I64, torch.from_numpy(v).cuda())]),
+                    g, device=True)
+    g.finalize()
+    o = ob.Agg([0], [(1, -1, 0), (0, 1, 0)])
+    ob.pipeline(ob.HostBatch([(I64, k, None, 0), (I64, v, None, 0)]), o, threads=8)
+    assert_groups_equal(g.export(), o.export(), ["count", "sum_i"])
+    g.close()
+
+
 def test_aggregate_low_cardinality_smem(ctx):
     rng = np.random.default_rng(4)
     cols = agg_setup(rng, 300_000, [I64], 900, 0.0, 0.0)
