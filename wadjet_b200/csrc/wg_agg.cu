@@ -790,11 +790,9 @@ static wg_status run_device(const PipelineRun& r) {
   // columns start on 16-byte boundaries, no join or the direct-payload one
   bool vec_ok = stat && ls.P.sel == nullptr && ls.P.n_in > 0 && (!ls.P.has_join || ls.P.join.direct);
   for (int j = 0; j < ls.P.n_in; ++j) vec_ok = vec_ok && ((uintptr_t)ls.P.in[j].data % 16 == 0);
-  const int vec_env = env_int("WG_VEC", 2);
-  ls.vec = vec_ok && (vec_env == 2 || vec_env == 4) ? vec_env : 0;
-  ls.vec_ctas = env_int("WG_VEC_CTAS", 2) == 3 ? 3 : 2;
+  ls.vec = vec_ok && env_int("WG_VEC", 2) != 0 ? 2 : 0;
   const int env_bps = env_int("WG_AGG_BLOCKS_PER_SM", 0);
-  const int pref_bps = env_bps > 0 ? env_bps : ls.vec ? ls.vec_ctas : 2;
+  const int pref_bps = env_bps > 0 ? env_bps : 2;
   int blocks_per_sm = pref_bps;
   ls.block = ls.vec ? 512 : stat ? wgd::StatShape<wgd::ShapeStarJoin>::kBlock : wgd::DynShape::kBlock;
   // copies of each float SUM per shared slot (lane-striped, see apply)
@@ -860,6 +858,8 @@ static wg_status run_device(const PipelineRun& r) {
     }
   }
   ls.smem = found;
+  // a shared table that takes a whole SM: one CTA of 1024 threads for the vector kernel
+  if (ls.vec && ls.smem && blocks_per_sm == 1) ls.block = 1024;
   ls.P.smem_slots = ls.smem ? S : 0;
   ls.P.smem_rep = rep;
   ls.P.smem_sw = stride_for(rep);

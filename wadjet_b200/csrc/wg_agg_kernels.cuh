@@ -1040,9 +1040,9 @@ __device__ __forceinline__ void process_rows_vec(const Plan& P, const Sh& sh, in
   }
 }
 
-// Grid-stride over chunks of 32*U rows; MB CTAs of 512 threads per SM.
-template <int NA, bool SMEM, class Sh, int U, int MB>
-__global__ void __launch_bounds__(512, MB) pipeline_vec_kernel(const __grid_constant__ Plan P) {
+// Grid-stride over chunks of 32*U rows; MB CTAs of BLK threads per SM.
+template <int NA, bool SMEM, class Sh, int U, int MB, int BLK>
+__global__ void __launch_bounds__(BLK, MB) pipeline_vec_kernel(const __grid_constant__ Plan P) {
   static_assert(U == 2 || U == 4, "rows per lane");
   extern __shared__ unsigned long long sm[];
   __shared__ int s_groups;

@@ -22,26 +22,22 @@ struct LaunchSpec {
   bool tile = false;          // TMA-staged tile kernel
   wgd::TileCfg cfg{};
   int vec = 0;                // compiled shapes: rows per lane of the vector kernel (0 = one-row kernel)
-  int vec_ctas = 2;           // vector kernel: 512-thread CTAs per SM it is compiled for (2 or 3)
 };
 
-template <int NA, bool SMEM, class Sh, int U, int MB>
+template <int NA, bool SMEM, class Sh, int U, int MB, int BLK>
 static void launch_vec_one(const LaunchSpec& ls, cudaStream_t st) {
   const size_t dyn = SMEM ? ls.smem_bytes : 0;
-  if (SMEM) cudaFuncSetAttribute(wgd::pipeline_vec_kernel<NA, SMEM, Sh, U, MB>,
+  if (SMEM) cudaFuncSetAttribute(wgd::pipeline_vec_kernel<NA, SMEM, Sh, U, MB, BLK>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
-  wgd::pipeline_vec_kernel<NA, SMEM, Sh, U, MB><<<ls.grid, 512, dyn, st>>>(ls.P);
+  wgd::pipeline_vec_kernel<NA, SMEM, Sh, U, MB, BLK><<<ls.grid, BLK, dyn, st>>>(ls.P);
 }
 
+// Two CTAs of 512 threads per SM, or one of 1024 when a shared table takes the
+// whole SM's shared memory.
 template <int NA, class Sh, bool SMEM>
 static void launch_vec_s(const LaunchSpec& ls, cudaStream_t st) {
-  if (ls.vec == 4) {
-    if (ls.vec_ctas == 3) launch_vec_one<NA, SMEM, Sh, 4, 3>(ls, st);
-    else launch_vec_one<NA, SMEM, Sh, 4, 2>(ls, st);
-  } else {
-    if (ls.vec_ctas == 3) launch_vec_one<NA, SMEM, Sh, 2, 3>(ls, st);
-    else launch_vec_one<NA, SMEM, Sh, 2, 2>(ls, st);
-  }
+  if (ls.block == 1024) launch_vec_one<NA, SMEM, Sh, 2, 1, 1024>(ls, st);
+  else launch_vec_one<NA, SMEM, Sh, 2, 2, 512>(ls, st);
 }
 
 // The vector kernel exists for compiled shapes only (DynShape never gets here).
