@@ -52,13 +52,15 @@ def test_device_generator_matches_host_generator(ctx):
 SHAPE_STARJOIN, SHAPE_GROUPBY, SHAPE_HIGHCARD = 1, 2, 3
 
 
-@pytest.mark.parametrize("spec", ["1", "0"])
-def test_groupby_workload_matches_oracle(ctx, spec, monkeypatch):
+@pytest.mark.parametrize("spec,wide", [("1", "1"), ("1", "0"), ("0", "1")])
+def test_groupby_workload_matches_oracle(ctx, spec, wide, monkeypatch):
     """SELECT k, SUM(v), COUNT(*), MIN(f), MAX(f) FROM t WHERE flag < 7 GROUP BY k, 2^20 rows,
-    on the kernel compiled for this query shape and on the generic kernel."""
+    on the kernel compiled for this query shape (its shared table takes a whole SM: one
+    1024-thread CTA, or 512 threads with WG_VEC_WIDE=0) and on the generic kernel."""
     import wadjet_b200 as wg
     from wadjet_b200 import synth
     monkeypatch.setenv("WG_SPECIALIZE", spec)
+    monkeypatch.setenv("WG_VEC_WIDE", wide)
     n = 1 << 20
     k, v, f, flag = synth.groupby(ctx, n)
     aggs = [wg.AggColumn(wg.AGG_SUM, 1), wg.AggColumn(wg.AGG_COUNT, -1), wg.AggColumn(wg.AGG_MIN, 2),

@@ -859,7 +859,7 @@ static wg_status run_device(const PipelineRun& r) {
   }
   ls.smem = found;
   // a shared table that takes a whole SM: one CTA of 1024 threads for the vector kernel
-  if (ls.vec && ls.smem && blocks_per_sm == 1) ls.block = 1024;
+  if (ls.vec && ls.smem && blocks_per_sm == 1 && env_int("WG_VEC_WIDE", 1) != 0) ls.block = 1024;
   ls.P.smem_slots = ls.smem ? S : 0;
   ls.P.smem_rep = rep;
   ls.P.smem_sw = stride_for(rep);
