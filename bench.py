@@ -404,7 +404,7 @@ def run_groupby(args):
     ctx = wg.Context(0)
     stream = torch.cuda.ExternalStream(ctx.stream)
     peak, kind = measured_peak_hbm()
-    for n in (1 << 20, 1 << 28):
+    for n in (1 << 20, args.rows):  # --rows: the large table (2^28 rows by default)
         k, v, f, flag = synth.groupby(ctx, n)
         batch = wg.Batch([wg.Column(wg.TYPE_INT64, k), wg.Column(wg.TYPE_INT64, v), wg.Column(wg.TYPE_FLOAT64, f),
                           wg.Column(wg.TYPE_INT32, flag)])

@@ -103,6 +103,54 @@ def test_join_matches_oracle(ctx, kt, dups, nulls):
     j.close()
 
 
+@pytest.mark.parametrize("dup", [False, True])
+@pytest.mark.parametrize("probe_first", [False, True])
+def test_join_dense_unique_build(ctx, dup, probe_first):
+    """Unique int32 keys over a narrow range with one int32 payload: the build makes only
+    the dense direct table, and the hash index waits for the first non-fused probe. A
+    duplicate key sends the build down the hash path. The fused pipeline (GROUP BY the
+    payload), the pair probe, the payload gather and the build stats agree with the oracle
+    whichever of the fused and non-fused calls comes first."""
+    import wadjet_b200 as wg
+    rng = np.random.default_rng(5 + dup)
+    nb, npr = 30_000, 200_000
+    bkeys = (rng.permutation(40_000)[:nb] + 1000).astype(np.int32)
+    if dup:
+        bkeys[-1] = bkeys[0]
+    grp = rng.integers(0, 300, nb).astype(np.int32)
+    pkeys = rng.integers(900, 41_100, npr).astype(np.int32)
+    j = wg.HashJoin(ctx, 0, 0, payload=[1])
+    j.build([wg.Batch([wg.Column(I32, bkeys), wg.Column(I32, grp)])])
+    oj = ob.Join()
+    oj.append(I32, bkeys, None)
+    assert j.stats()[1] == oj.distinct()
+
+    def fused():
+        g = wg.HashAggregate(ctx, [1], [wg.AggColumn(wg.AGG_COUNT, -1)], ndv_hint=300)
+        wg.run_pipeline(ctx, wg.Batch([wg.Column(I32, pkeys)]), g, join=j)
+        g.finalize()
+        o = ob.Agg([1], [(1, -1, 0)])
+        ob.pipeline(ob.HostBatch([(I32, pkeys, None, 0)]), o, join=oj, probe_key=0,
+                    build=ob.HostBatch([(I32, bkeys, None, 0), (I32, grp, None, 0)]), payload=[1], threads=8)
+        assert_groups_equal(g.export(), o.export(), ["count"])
+        g.close()
+
+    def probe():
+        want = sorted(zip(*[a.tolist() for a in oj.probe(I32, pkeys, None)]))
+        got = []
+        for pr, br in j.probe(wg.Batch([wg.Column(I32, pkeys)]), cap=50_000):
+            got += list(zip(pr.tolist(), br.tolist()))
+        assert sorted(got) == want
+        brows = np.array([b for _, b in got[:1000]], np.int64)
+        vals, ok = j.gather(0, brows, np.int32)
+        np.testing.assert_array_equal(vals, grp[brows])
+        assert ok.all()
+
+    for step in ((probe, fused) if probe_first else (fused, probe)):
+        step()
+    j.close()
+
+
 # ------------------------------------------------------------- aggregate --
 AGG_KINDS = {  # (func, input type) -> comparison kind
     (0, I32): "sum_i", (0, I64): "sum_i", (0, F64): "sum_f", (0, F32): "sum_f", (0, DEC): "sum_d",

@@ -199,6 +199,18 @@ __global__ void dense_table_kernel(DCol key, int64_t n, const uint32_t* pay, lon
   }
 }
 
+// Dense direct table built straight from the build rows, before any hash index
+// exists: each key claims its slot with a compare-and-swap from the empty word,
+// so a second row with the same key finds the slot taken and flags `dup`.
+__global__ void dense_build_kernel(DCol key, int64_t n, const uint32_t* pay, long long base,
+                                   unsigned long long empty, unsigned long long* out, int32_t* dup) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const long long k = ld_i64(key, i);
+    const unsigned long long mine = ((unsigned long long)__ldg(pay + i) << 32) | (uint32_t)(int32_t)k;
+    if (atomicCAS(out + (k - base), empty, mine) != empty) *dup = 1;
+  }
+}
+
 __global__ void fill_u64_kernel(unsigned long long* out, int64_t n, unsigned long long v) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     out[i] = v;
@@ -274,6 +286,7 @@ struct wg_join {
   int64_t distinct = 0;
   bool unique = true;
   int64_t max_fanout = 1;
+  bool hashed = false;  // the hash index (slots/next) is built; a dense unique build defers it to first use
   // direct-payload copy of the table for the fused kernel (see JoinView)
   wg::DevBuf dslots;
   bool direct = false;
@@ -385,7 +398,9 @@ static wg_status join_append(wg_join* j, const wg_batch_desc* b) {
 }
 
 // Device view for the fused pipeline and the probe kernels.
-wg_status join_view(wg_join* j, wgd::JoinView* v) {
+static wg_status build_hash(wg_join* j);
+
+static wg_status join_view_fields(wg_join* j, wgd::JoinView* v) {
   if (!j->finished) return fail(WG_E_STATE, "join build not finished");
   v->flavor = j->flavor;
   v->shift = j->shift;
@@ -403,10 +418,16 @@ wg_status join_view(wg_join* j, wgd::JoinView* v) {
   return WG_OK;
 }
 
+wg_status join_view(wg_join* j, wgd::JoinView* v) {
+  if (j->finished && !j->hashed) WG_TRY(build_hash(j));
+  return join_view_fields(j, v);
+}
+
 // The view the fused pipeline probes: the direct-payload table when one was built.
 wg_status join_view_fused(wg_join* j, wgd::JoinView* v) {
-  WG_TRY(join_view(j, v));
-  if (j->direct) {
+  if (!j->direct) return join_view(j, v);
+  WG_TRY(join_view_fields(j, v));
+  {
     v->slots = j->dslots.get();
     v->direct = 1;
     v->sentinel = j->sentinel;
@@ -431,6 +452,106 @@ bool join_payload_range(wg_join* j, int i, long long* lo, long long* hi) {
 }
 bool join_unique(wg_join* j) { return j->unique; }
 int64_t join_max_fanout(wg_join* j) { return j->max_fanout; }
+
+// The hash index (slots/next): one CAS insert per build row, heads chained
+// through `next`; counts distinct keys and flags duplicates.
+static wg_status build_hash(wg_join* j) {
+  Ctx* ctx = j->ctx;
+  const uint64_t cap = j->capacity;
+  const int64_t slot_bytes = j->flavor == 0 ? 8 : 16;
+  WG_TRY(j->slots.ensure(ctx, (int64_t)cap * slot_bytes));
+  WG_TRY(j->next.ensure(ctx, std::max<int64_t>(j->rows, 1) * 4));
+  WG_TRY(j->scratch.ensure(ctx, 64));
+  WG_CUDA_TRY(cudaMemsetAsync(j->slots.get(), 0xFF, (size_t)(cap * slot_bytes), ctx->stream));
+  WG_CUDA_TRY(cudaMemsetAsync(j->scratch.get(), 0, 64, ctx->stream));
+  if (j->rows > 0) {
+    BuildArgs a;
+    a.key = wgd::DCol{j->key.data.get(), j->key.has_valid ? j->key.valid.as<uint64_t>() : nullptr,
+                      class_of(j->key.type_id), 0};
+    a.n = j->rows;
+    a.flavor = j->flavor;
+    a.shift = j->shift;
+    a.mask = cap - 1;
+    a.slots = j->slots.get();
+    a.next = j->next.as<int32_t>();
+    a.distinct = j->scratch.as<unsigned long long>();
+    a.dup = (int32_t*)(j->scratch.as<char>() + 8);
+    a.err = ctx->dev_error;
+    join_build_kernel<<<grid_for(ctx, j->rows, 256), 256, 0, ctx->stream>>>(a);
+    ctx->count_launch();
+    WG_CUDA_TRY(cudaGetLastError());
+  }
+  int64_t back[2] = {0, 0};
+  WG_TRY(read_back_i64(ctx, j->scratch.as<int64_t>(), back, 2));
+  WG_TRY(check_device_error(ctx));
+  j->distinct = back[0];
+  j->unique = (int32_t)back[1] == 0;
+  j->hashed = true;
+  return WG_OK;
+}
+
+// Unique int32 build keys without NULLs, spanning at most 4x the build rows,
+// and one 4-byte payload column without NULLs: the dense direct table is built
+// straight from the rows and the hash index is deferred to its first use (the
+// fused probe never needs it). *done is false when this shape does not apply
+// or a duplicate key turned up; the caller then builds the hash index.
+static wg_status build_dense_unique(wg_join* j, bool* done) {
+  *done = false;
+  Ctx* ctx = j->ctx;
+  const char* dsw = std::getenv("WG_JOIN_DIRECT");
+  const char* dns = std::getenv("WG_JOIN_DENSE");
+  if ((dsw && std::atoi(dsw) == 0) || (dns && std::atoi(dns) == 0) || j->rows <= 0 || j->flavor != 0 ||
+      j->key.has_valid || j->pay.size() != 1 || j->pay[0].es != 4 || j->pay[0].has_valid)
+    return WG_OK;
+  const int pcls = class_of(j->pay[0].type_id);
+  const bool pay_int = pcls == WG_CLS_I32 || pcls == WG_CLS_I64;
+  long long* mm = (long long*)(j->scratch.as<char>() + 16);  // key lo, hi, payload lo, hi
+  const long long init[4] = {LLONG_MAX, LLONG_MIN, LLONG_MAX, LLONG_MIN};
+  WG_CUDA_TRY(cudaMemcpyAsync(mm, init, 32, cudaMemcpyHostToDevice, ctx->stream));
+  wgd::DCol kd{j->key.data.get(), nullptr, class_of(j->key.type_id), 0};
+  key_range_kernel<<<grid_for(ctx, j->rows, 256), 256, 0, ctx->stream>>>(kd, j->rows, mm, mm + 1);
+  ctx->count_launch();
+  if (pay_int) {
+    wgd::DCol pd{j->pay[0].data.get(), nullptr, pcls, 0};
+    key_range_kernel<<<grid_for(ctx, j->rows, 256), 256, 0, ctx->stream>>>(pd, j->rows, mm + 2, mm + 3);
+    ctx->count_launch();
+  }
+  WG_CUDA_TRY(cudaGetLastError());
+  int64_t r[4];
+  WG_TRY(read_back_i64(ctx, (const int64_t*)mm, r, 4));
+  int32_t sentinel;
+  if (r[0] > INT32_MIN) sentinel = (int32_t)(r[0] - 1);
+  else if (r[1] < INT32_MAX) sentinel = (int32_t)(r[1] + 1);
+  else return WG_OK;
+  const int64_t span = r[1] - r[0] + 1;
+  if (!(span > 0 && span <= std::max<int64_t>(4 * j->rows, 1024) && span <= (int64_t(1) << 30))) return WG_OK;
+  const unsigned long long empty = (unsigned long long)(uint32_t)sentinel;
+  WG_TRY(j->dslots.ensure(ctx, span * 8));
+  WG_CUDA_TRY(cudaMemsetAsync(j->scratch.get(), 0, 8, ctx->stream));
+  fill_u64_kernel<<<grid_for(ctx, span, 256), 256, 0, ctx->stream>>>(j->dslots.as<unsigned long long>(), span, empty);
+  ctx->count_launch();
+  dense_build_kernel<<<grid_for(ctx, j->rows, 256), 256, 0, ctx->stream>>>(
+      kd, j->rows, j->pay[0].data.as<uint32_t>(), r[0], empty, j->dslots.as<unsigned long long>(),
+      j->scratch.as<int32_t>());
+  ctx->count_launch();
+  WG_CUDA_TRY(cudaGetLastError());
+  int64_t dup = 0;
+  WG_TRY(read_back_i64(ctx, j->scratch.as<int64_t>(), &dup, 1));
+  if ((int32_t)dup != 0) return WG_OK;
+  j->pay_lo.assign(1, pay_int ? r[2] : 0);
+  j->pay_hi.assign(1, pay_int ? r[3] : 0);
+  j->pay_range.assign(1, pay_int);
+  j->distinct = j->rows;
+  j->unique = true;
+  j->max_fanout = 1;
+  j->direct = true;
+  j->dense = true;
+  j->sentinel = sentinel;
+  j->dense_base = r[0];
+  j->dense_slots = span;
+  *done = true;
+  return WG_OK;
+}
 
 }  // namespace wg
 
@@ -478,34 +599,15 @@ wg_status wg_join_build_finish(wg_join* j) {
   while ((1ULL << log2) < cap) ++log2;
   j->capacity = cap;
   j->shift = 64 - log2;
-  const int64_t slot_bytes = j->flavor == 0 ? 8 : 16;
-  WG_TRY(j->slots.ensure(ctx, (int64_t)cap * slot_bytes));
-  WG_TRY(j->next.ensure(ctx, std::max<int64_t>(j->rows, 1) * 4));
+  j->hashed = false;
   WG_TRY(j->scratch.ensure(ctx, 64));
-  WG_CUDA_TRY(cudaMemsetAsync(j->slots.get(), 0xFF, (size_t)(cap * slot_bytes), ctx->stream));
-  WG_CUDA_TRY(cudaMemsetAsync(j->scratch.get(), 0, 64, ctx->stream));
-  if (j->rows > 0) {
-    BuildArgs a;
-    a.key = wgd::DCol{j->key.data.get(), j->key.has_valid ? j->key.valid.as<uint64_t>() : nullptr,
-                      class_of(j->key.type_id), 0};
-    a.n = j->rows;
-    a.flavor = j->flavor;
-    a.shift = j->shift;
-    a.mask = cap - 1;
-    a.slots = j->slots.get();
-    a.next = j->next.as<int32_t>();
-    a.distinct = j->scratch.as<unsigned long long>();
-    a.dup = (int32_t*)(j->scratch.as<char>() + 8);
-    a.err = ctx->dev_error;
-    join_build_kernel<<<grid_for(ctx, j->rows, 256), 256, 0, ctx->stream>>>(a);
-    ctx->count_launch();
-    WG_CUDA_TRY(cudaGetLastError());
+  bool done = false;
+  WG_TRY(build_dense_unique(j, &done));
+  if (done) {
+    j->finished = true;
+    return check_device_error(ctx);
   }
-  int64_t back[2] = {0, 0};
-  WG_TRY(read_back_i64(ctx, j->scratch.as<int64_t>(), back, 2));
-  WG_TRY(check_device_error(ctx));
-  j->distinct = back[0];
-  j->unique = (int32_t)back[1] == 0;
+  WG_TRY(build_hash(j));
   j->finished = true;
   j->max_fanout = 1;
   if (!j->unique) {
