@@ -17,6 +17,7 @@
 
 #include <algorithm>
 #include <cstdlib>
+#include <cstring>
 
 namespace wg {
 wg_status resolve_pred(const wg_predicate& p, int32_t type_id, wgd::Pred* out);
@@ -294,8 +295,14 @@ struct wg_agg {
   std::vector<wg_predicate> sp_filters;
   std::vector<wg_expr> sp_exprs;
   std::vector<wg::DevBuf> sp_dev;    // device staging per plan input column
+  // export staging (kept for the next export): every output field of a chunk
+  // side by side on the device, read back in one copy through pinned memory
+  wg::DevBuf exp_dev;
+  char* exp_host = nullptr;
+  int64_t exp_host_bytes = 0;
   ~wg_agg() {
     for (auto& b : host_blocks) cudaFreeHost(b.first);
+    if (exp_host) cudaFreeHost(exp_host);
   }
 };
 
@@ -1447,26 +1454,41 @@ wg_status wg_agg_export(wg_agg* a, const wg_group_export* o) {
   if (!a->resolved || a->n_out == 0) return WG_OK;
   const int64_t n = a->n_out;
   const int nk = (int)a->key_cols.size(), na = (int)a->specs.size();
-  // in chunks of at most 2^16 groups, so the export's device staging stays small
+  // in chunks of at most 2^16 groups, so the export's staging stays small
   const int64_t C = std::min<int64_t>(n, int64_t(1) << 16);
-  DevBuf keys, kv, cnt, i64, f64, dec, has;
   FinalArgs A;
   fill_final_args(a, A);
-  if (o->keys && nk) { WG_TRY(keys.alloc(ctx, nk * C * 8)); A.keys = keys.as<int64_t>(); }
-  if (o->key_valid && nk) { WG_TRY(kv.alloc(ctx, nk * C)); A.key_valid = kv.as<uint8_t>(); }
-  if (o->count && na) { WG_TRY(cnt.alloc(ctx, na * C * 8)); A.count = cnt.as<int64_t>(); }
-  if (o->i64 && na) { WG_TRY(i64.alloc(ctx, na * C * 8)); A.i64 = i64.as<int64_t>(); }
-  if (o->f64 && na) { WG_TRY(f64.alloc(ctx, na * C * 8)); A.f64 = f64.as<double>(); }
-  if (o->dec && na) { WG_TRY(dec.alloc(ctx, na * C * 16)); A.dec = dec.as<wg_int128>(); }
-  if (o->has && na) { WG_TRY(has.alloc(ctx, na * C)); A.has = has.as<uint8_t>(); }
-  // block b of a chunk (c rows at stride c on the device) to rows [s, s + c) of block b on the host (stride n)
-  auto back = [&](void* dst, DevBuf& src, int blocks, int64_t es, int64_t s0, int64_t c) -> wg_status {
-    if (!dst || !src.get()) return WG_OK;
-    for (int b = 0; b < blocks; ++b)
-      WG_CUDA_TRY(cudaMemcpyAsync((char*)dst + (b * n + s0) * es, src.as<char>() + b * c * es, (size_t)(c * es),
-                                  cudaMemcpyDeviceToHost, ctx->stream));
-    return WG_OK;
-  };
+  // the fields the caller asked for, each a block of (keys or aggregates) x C
+  // values at a 256-byte aligned offset of one staging buffer
+  struct Field { void* dst; int blocks; int64_t es; int64_t off; };
+  Field f[7] = {{o->keys, nk, 8, 0}, {o->key_valid, nk, 1, 0}, {o->count, na, 8, 0}, {o->i64, na, 8, 0},
+                {o->f64, na, 8, 0}, {o->dec, na, 16, 0}, {o->has, na, 1, 0}};
+  int64_t total = 0;
+  for (Field& x : f) {
+    if (!x.dst || x.blocks == 0) { x.dst = nullptr; continue; }
+    x.off = total;
+    total += (x.blocks * C * x.es + 255) & ~int64_t(255);
+  }
+  if (total == 0) return WG_OK;
+  WG_TRY(a->exp_dev.ensure(ctx, total));
+  if (a->exp_host_bytes < total) {
+    if (a->exp_host) cudaFreeHost(a->exp_host);
+    a->exp_host = nullptr;
+    a->exp_host_bytes = 0;
+    if (cudaMallocHost((void**)&a->exp_host, (size_t)total) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(WG_E_NOMEM, "pinned export staging allocation failed");
+    }
+    a->exp_host_bytes = total;
+  }
+  char* dev = a->exp_dev.as<char>();
+  A.keys = f[0].dst ? (int64_t*)(dev + f[0].off) : nullptr;
+  A.key_valid = f[1].dst ? (uint8_t*)(dev + f[1].off) : nullptr;
+  A.count = f[2].dst ? (int64_t*)(dev + f[2].off) : nullptr;
+  A.i64 = f[3].dst ? (int64_t*)(dev + f[3].off) : nullptr;
+  A.f64 = f[4].dst ? (double*)(dev + f[4].off) : nullptr;
+  A.dec = f[5].dst ? (wg_int128*)(dev + f[5].off) : nullptr;
+  A.has = f[6].dst ? (uint8_t*)(dev + f[6].off) : nullptr;
   for (int64_t s0 = 0; s0 < n; s0 += C) {
     const int64_t c = std::min(C, n - s0);
     A.start = s0;
@@ -1475,14 +1497,19 @@ wg_status wg_agg_export(wg_agg* a, const wg_group_export* o) {
     export_kernel<<<grid_cap(ctx, c, 256), 256, 0, ctx->stream>>>(A);
     ctx->count_launch();
     WG_CUDA_TRY(cudaGetLastError());
-    WG_TRY(back(o->keys, keys, nk, 8, s0, c));
-    WG_TRY(back(o->key_valid, kv, nk, 1, s0, c));
-    WG_TRY(back(o->count, cnt, na, 8, s0, c));
-    WG_TRY(back(o->i64, i64, na, 8, s0, c));
-    WG_TRY(back(o->f64, f64, na, 8, s0, c));
-    WG_TRY(back(o->dec, dec, na, 16, s0, c));
-    WG_TRY(back(o->has, has, na, 1, s0, c));
+    // the chunk's fields sit at their offsets with block stride c: one copy up
+    // to the end of the last field in use
+    int64_t used = 0;
+    for (const Field& x : f)
+      if (x.dst) used = x.off + x.blocks * c * x.es;
+    WG_CUDA_TRY(cudaMemcpyAsync(a->exp_host, dev, (size_t)used, cudaMemcpyDeviceToHost, ctx->stream));
     WG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));  // the staging is reused by the next chunk
+    // block b of the chunk (c rows at stride c) to rows [s0, s0 + c) of block b on the host (stride n)
+    for (const Field& x : f) {
+      if (!x.dst) continue;
+      for (int b = 0; b < x.blocks; ++b)
+        std::memcpy((char*)x.dst + (b * n + s0) * x.es, a->exp_host + x.off + b * c * x.es, (size_t)(c * x.es));
+    }
   }
   return check_device_error(ctx);
 }

@@ -154,6 +154,10 @@ struct StatShape {
   static constexpr bool smem_ok = C::smem_ok;
   // straight-line code fits 40 registers: two 768-thread CTAs per SM (48 warps)
   static constexpr int kBlock = 768, kMinBlocks = 2;
+  // vector kernel: evaluate all of a lane's rows before their table updates
+  // when no projection program runs per row (short, independent chains the
+  // scheduler interleaves); with one, row by row keeps fewer values live
+  static constexpr bool kRowsTogether = C::n_exprs == 0;
   const Plan& P;
   __device__ __forceinline__ constexpr int n_in() const { return C::n_in; }
   __device__ __forceinline__ constexpr int in_cls(int j) const { return C::in_cls(j); }
@@ -1020,23 +1024,49 @@ __device__ __forceinline__ void process_rows_vec(const Plan& P, const Sh& sh, in
       if (act[u]) act[u] = !kv.null && join_direct(P.join, (int64_t)kv.lo, brow[u], P.err);
     }
   }
+  if (!Sh::kRowsTogether) {
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (!__any_sync(WG_FULL_MASK, act[u])) continue;
+      unsigned long long k0 = 0, k1 = 0;
+      bool knull = false;
+      Contrib<NA> c;
+      bool cur = act[u];
+      if (cur) {
+        ExprVals ev;
+        eval_exprs(P, sh, rw[u], brow[u], ev);
+        cur = make_key(P, sh, rw[u], brow[u], ev, k0, k1, knull);
+        make_contrib<NA>(P, sh, rw[u], brow[u], ev, c);
+      } else {
+#pragma unroll
+        for (int a = 0; a < NA; ++a) { c.w0[a] = 0; c.w1[a] = 0; c.nul[a] = 0; }
+      }
+      warp_update<NA, SMEM>(P, sh, cur, k0, k1, knull, c, sm, s_groups, s_limit, cr);
+    }
+    return;
+  }
+  // every row's key and contribution first (independent dependency chains
+  // the scheduler can interleave), then the table updates
+  unsigned long long k0[U], k1[U];
+  bool knull[U];
+  Contrib<NA> c[U];
+#pragma unroll
+  for (int u = 0; u < U; ++u) {
+    k0[u] = 0; k1[u] = 0; knull[u] = false;
+    if (act[u]) {
+      ExprVals ev;
+      eval_exprs(P, sh, rw[u], brow[u], ev);
+      act[u] = make_key(P, sh, rw[u], brow[u], ev, k0[u], k1[u], knull[u]);
+      make_contrib<NA>(P, sh, rw[u], brow[u], ev, c[u]);
+    } else {
+#pragma unroll
+      for (int a = 0; a < NA; ++a) { c[u].w0[a] = 0; c[u].w1[a] = 0; c[u].nul[a] = 0; }
+    }
+  }
 #pragma unroll
   for (int u = 0; u < U; ++u) {
     if (!__any_sync(WG_FULL_MASK, act[u])) continue;
-    unsigned long long k0 = 0, k1 = 0;
-    bool knull = false;
-    Contrib<NA> c;
-    bool cur = act[u];
-    if (cur) {
-      ExprVals ev;
-      eval_exprs(P, sh, rw[u], brow[u], ev);
-      cur = make_key(P, sh, rw[u], brow[u], ev, k0, k1, knull);
-      make_contrib<NA>(P, sh, rw[u], brow[u], ev, c);
-    } else {
-#pragma unroll
-      for (int a = 0; a < NA; ++a) { c.w0[a] = 0; c.w1[a] = 0; c.nul[a] = 0; }
-    }
-    warp_update<NA, SMEM>(P, sh, cur, k0, k1, knull, c, sm, s_groups, s_limit, cr);
+    warp_update<NA, SMEM>(P, sh, act[u], k0[u], k1[u], knull[u], c[u], sm, s_groups, s_limit, cr);
   }
 }
 
