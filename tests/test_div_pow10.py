@@ -19,7 +19,7 @@ def pow10_go(n: int) -> float:
 
 def recip_table() -> list[float]:
     src = open(os.path.join(CSRC, "wg_device.cuh")).read()
-    body = re.search(r"c_pow10_recip\[128\] = \{(.*?)\};", src, re.S).group(1)
+    body = re.search(r"#define WG_POW10_RECIP \\\n(.*?)\nstatic __constant__ double c_pow10_recip", src, re.S).group(1)
     return [float.fromhex(x) for x in re.findall(r"0x[0-9a-fA-Fp.+-]+", body)]
 
 

@@ -749,6 +749,7 @@ static wg_status build_plan(const PipelineRun& r, wgd::Plan& P, VSchema& vs, std
     P.vcls[nin + npay + e] = d.result_cls;
     P.vscale[nin + npay + e] = 0;
   }
+  for (int j = 0; j < nin + npay + r.n_exprs; ++j) pow10_divisor_host(P.vscale[j], &P.vdiv_b[j], &P.vdiv_y[j]);
   for (int k = 0; k < (int)r.agg->key_cols.size(); ++k) P.L.key_vcol[k] = vmap(r.agg->key_cols[k]);
   for (size_t i = 0; i < r.agg->specs.size(); ++i) P.L.agg[i].vcol = vmap(r.agg->specs[i].input_col);
   P.sel = in->sel;

@@ -99,6 +99,10 @@ struct Plan {
   ExprD expr[WG_MAX_EXPRS];
   int32_t vcls[WG_MAX_IN + WG_MAX_PAYLOAD + WG_MAX_EXPRS];
   int32_t vscale[WG_MAX_IN + WG_MAX_PAYLOAD + WG_MAX_EXPRS];
+  // DECIMAL columns: pow10_divisor_host(vscale) — the divisor and its rounded
+  // reciprocal of the conversion to float64, so rows need no table lookups
+  double vdiv_b[WG_MAX_IN + WG_MAX_PAYLOAD + WG_MAX_EXPRS];
+  double vdiv_y[WG_MAX_IN + WG_MAX_PAYLOAD + WG_MAX_EXPRS];
   Layout L;
   Table T;
   int32_t* err;

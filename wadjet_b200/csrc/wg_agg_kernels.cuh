@@ -242,7 +242,10 @@ __device__ __forceinline__ Val eval_expr(const Plan& P, const Sh& sh, int e, con
       null |= v.null;
       const int cls = sh.vcls(j);
       if (cls == WG_CLS_I32 || cls == WG_CLS_I64) { w = v.lo; isf = false; }
-      else if (cls == WG_CLS_DEC) { w = as_w(dec_to_f64((int64_t)v.hi, v.lo, P.vscale[j])); isf = true; }
+      else if (cls == WG_CLS_DEC) {
+        w = as_w(div_by_recip(int128_to_f64((int64_t)v.hi, v.lo), P.vdiv_b[j], P.vdiv_y[j]));
+        isf = true;
+      }
       else { w = v.lo; isf = true; }
     } else if (opc == 1) {
       w = (unsigned long long)P.expr[e].imm[k]; isf = false;
@@ -582,8 +585,10 @@ __device__ __forceinline__ unsigned long long* find_smem(unsigned long long* sm,
 __device__ __forceinline__ unsigned long long* find_shared(const Plan& P, unsigned long long* sm, unsigned long long k0,
                                                            int* s_groups, int s_limit) {
   if (P.gdense) {
-    const unsigned long long d = k0 - (unsigned long long)P.gmin;
-    return d < (unsigned long long)P.smem_slots ? sm + d * smem_stride(P) : nullptr;
+    // every key lies in [gmin, gmin + smem_slots), fewer than 2^14 apart: the
+    // low 32 bits give the exact offset
+    const uint32_t d = (uint32_t)k0 - (uint32_t)P.gmin;
+    return d < (uint32_t)P.smem_slots ? sm + d * (uint32_t)smem_stride(P) : nullptr;
   }
   return find_smem(sm, P.smem_slots, smem_stride(P), k0, s_groups, s_limit);
 }
@@ -1021,7 +1026,12 @@ __device__ __forceinline__ void process_rows_vec(const Plan& P, const Sh& sh, in
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const Val kv = rw[u].v[sh.probe_col()];
-      if (act[u]) act[u] = !kv.null && join_direct(P.join, (int64_t)kv.lo, brow[u], P.err);
+      if (act[u]) {
+        if (sh.in_cls(sh.probe_col()) == WG_CLS_I32)
+          act[u] = !kv.null && join_direct_i32(P.join, (int32_t)kv.lo, brow[u], P.err);
+        else
+          act[u] = !kv.null && join_direct(P.join, (int64_t)kv.lo, brow[u], P.err);
+      }
     }
   }
   if (!Sh::kRowsTogether) {

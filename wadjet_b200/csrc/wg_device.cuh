@@ -39,61 +39,61 @@ __device__ __forceinline__ int64_t ld_i64(const DCol& c, int64_t i) {
 }
 
 // math.Pow10 as Go computes it for n in [0, 128): pow10tab[n%32] * pow10postab32[n/32]
-static __constant__ double c_pow10_tab[32] = {1e0,  1e1,  1e2,  1e3,  1e4,  1e5,  1e6,  1e7,  1e8,  1e9,  1e10,
-                                              1e11, 1e12, 1e13, 1e14, 1e15, 1e16, 1e17, 1e18, 1e19, 1e20, 1e21,
-                                              1e22, 1e23, 1e24, 1e25, 1e26, 1e27, 1e28, 1e29, 1e30, 1e31};
-static __constant__ double c_pow10_post[4] = {1e0, 1e32, 1e64, 1e96};
+#define WG_POW10_TAB 1e0,  1e1,  1e2,  1e3,  1e4,  1e5,  1e6,  1e7,  1e8,  1e9,  1e10, 1e11, 1e12, 1e13, 1e14, \
+                     1e15, 1e16, 1e17, 1e18, 1e19, 1e20, 1e21, 1e22, 1e23, 1e24, 1e25, 1e26, 1e27, 1e28, 1e29, 1e30, 1e31
+#define WG_POW10_POST 1e0, 1e32, 1e64, 1e96
+static __constant__ double c_pow10_tab[32] = {WG_POW10_TAB};
+static __constant__ double c_pow10_post[4] = {WG_POW10_POST};
 __device__ __forceinline__ double pow10_go(int n) {
   if (n < 0 || n >= 128) return 1.0;
   return __dmul_rn(c_pow10_tab[n & 31], c_pow10_post[n >> 5]);
 }
 
 // RN(1 / pow10_go(n)) for n in [0, 128), as exact binary64 literals.
-static __constant__ double c_pow10_recip[128] = {
-    0x1.0000000000000p+0, 0x1.999999999999ap-4, 0x1.47ae147ae147bp-7, 0x1.0624dd2f1a9fcp-10,
-    0x1.a36e2eb1c432dp-14, 0x1.4f8b588e368f1p-17, 0x1.0c6f7a0b5ed8dp-20, 0x1.ad7f29abcaf48p-24,
-    0x1.5798ee2308c3ap-27, 0x1.12e0be826d695p-30, 0x1.b7cdfd9d7bdbbp-34, 0x1.5fd7fe1796495p-37,
-    0x1.19799812dea11p-40, 0x1.c25c268497682p-44, 0x1.6849b86a12b9bp-47, 0x1.203af9ee75616p-50,
-    0x1.cd2b297d889bcp-54, 0x1.70ef54646d497p-57, 0x1.2725dd1d243acp-60, 0x1.d83c94fb6d2acp-64,
-    0x1.79ca10c924223p-67, 0x1.2e3b40a0e9b4fp-70, 0x1.e392010175ee6p-74, 0x1.82db34012b252p-77,
-    0x1.357c299a88ea8p-80, 0x1.ef2d0f5da7dd8p-84, 0x1.8c240c4aecb13p-87, 0x1.3ce9a36f23c10p-90,
-    0x1.fb0f6be50601ap-94, 0x1.95a5efea6b348p-97, 0x1.4484bfeebc29fp-100, 0x1.039d665896880p-103,
-    0x1.9f623d5a8a732p-107, 0x1.4c4e977ba1f5bp-110, 0x1.09d8792fb4c49p-113, 0x1.a95a5b7f87a0fp-117,
-    0x1.54484932d2e72p-120, 0x1.1039d428a8b8ep-123, 0x1.b38fb9daa78e4p-127, 0x1.5c72fb1552d83p-130,
-    0x1.16c262777579cp-133, 0x1.be03d0bf225c7p-137, 0x1.64cfda3281e38p-140, 0x1.1d7314f534b61p-143,
-    0x1.c8b8218854567p-147, 0x1.6d601ad376ab9p-150, 0x1.244ce242c5561p-153, 0x1.d3ae36d13bbcep-157,
-    0x1.7624f8a762fd8p-160, 0x1.2b50c6ec4f313p-163, 0x1.dee7a4ad4b81ep-167, 0x1.7f1fb6f10934cp-170,
-    0x1.327fc58da0f70p-173, 0x1.ea6608e29b24dp-177, 0x1.8851a0b548ea3p-180, 0x1.39dae6f76d883p-183,
-    0x1.f62b0b257c0d1p-187, 0x1.91bc08eac9a40p-190, 0x1.41633a556e1cdp-193, 0x1.011c2eaabe7d8p-196,
-    0x1.9b604aaaca627p-200, 0x1.4919d5556eb52p-203, 0x1.0747ddddf22a8p-206, 0x1.a53fc9631d10cp-210,
-    0x1.50ffd44f4a73dp-213, 0x1.0d9976a5d5297p-216, 0x1.af5bf109550f3p-220, 0x1.59165a6ddda5bp-223,
-    0x1.1411e1f17e1e2p-226, 0x1.b9b6364f30304p-230, 0x1.615e91d8f359dp-233, 0x1.1ab20e472914ap-236,
-    0x1.c45016d841babp-240, 0x1.69d9abe034955p-243, 0x1.217aefe690777p-246, 0x1.cf2b1970e7259p-250,
-    0x1.7288e1271f513p-253, 0x1.286d80ec190dcp-256, 0x1.da48ce468e7c7p-260, 0x1.7b6d71d20b96cp-263,
-    0x1.2f8ac174d6123p-266, 0x1.e5aacf2156839p-270, 0x1.8488a5b445361p-273, 0x1.36d3b7c36a91ap-276,
-    0x1.f152bf9f10e8fp-280, 0x1.8ddbcc7f40ba6p-283, 0x1.3e497065cd61ep-286, 0x1.fd424d6faf031p-290,
-    0x1.97683df2f268ep-293, 0x1.45ecfe5bf520ap-296, 0x1.04bd984990e6fp-299, 0x1.a12f5a0f4e3e4p-303,
-    0x1.4dbf7b3f71cb7p-306, 0x1.0aff95cc5b093p-309, 0x1.ab328946f80eap-313, 0x1.55c2076bf9a55p-316,
-    0x1.116805effaeaap-319, 0x1.b5733cb32b110p-323, 0x1.5df5ca28ef40dp-326, 0x1.17f7d4ed8c33dp-329,
-    0x1.bff2ee48e0530p-333, 0x1.665bf1d3e6a8dp-336, 0x1.1eaff4a98553dp-339, 0x1.cab3210f3bb95p-343,
-    0x1.6ef5b40c2fc77p-346, 0x1.25915cd68c9f9p-349, 0x1.d5b561574765bp-353, 0x1.77c44ddf6c516p-356,
-    0x1.2c9d0b1923745p-359, 0x1.e0fb44f50586ep-363, 0x1.80c903f7379f1p-366, 0x1.33d4032c2c7f4p-369,
-    0x1.ec866b79e0cb9p-373, 0x1.8a0522c7e7095p-376, 0x1.3b374f06526dep-379, 0x1.f8587e7083e2fp-383,
-    0x1.9379fec069826p-386, 0x1.42c7ff0054685p-389, 0x1.023998cd10537p-392, 0x1.9d28f47b4d525p-396,
-    0x1.4a8729fc3ddb7p-399, 0x1.086c219697e2bp-402, 0x1.a71368f0f3046p-406, 0x1.5275ed8d8f36bp-409,
-    0x1.0ec4be0ad8f89p-412, 0x1.b13ac9aaf4c0fp-416, 0x1.5a956e225d672p-419, 0x1.1544581b7dec2p-422,
-};
+#define WG_POW10_RECIP \
+    0x1.0000000000000p+0, 0x1.999999999999ap-4, 0x1.47ae147ae147bp-7, 0x1.0624dd2f1a9fcp-10, \
+    0x1.a36e2eb1c432dp-14, 0x1.4f8b588e368f1p-17, 0x1.0c6f7a0b5ed8dp-20, 0x1.ad7f29abcaf48p-24, \
+    0x1.5798ee2308c3ap-27, 0x1.12e0be826d695p-30, 0x1.b7cdfd9d7bdbbp-34, 0x1.5fd7fe1796495p-37, \
+    0x1.19799812dea11p-40, 0x1.c25c268497682p-44, 0x1.6849b86a12b9bp-47, 0x1.203af9ee75616p-50, \
+    0x1.cd2b297d889bcp-54, 0x1.70ef54646d497p-57, 0x1.2725dd1d243acp-60, 0x1.d83c94fb6d2acp-64, \
+    0x1.79ca10c924223p-67, 0x1.2e3b40a0e9b4fp-70, 0x1.e392010175ee6p-74, 0x1.82db34012b252p-77, \
+    0x1.357c299a88ea8p-80, 0x1.ef2d0f5da7dd8p-84, 0x1.8c240c4aecb13p-87, 0x1.3ce9a36f23c10p-90, \
+    0x1.fb0f6be50601ap-94, 0x1.95a5efea6b348p-97, 0x1.4484bfeebc29fp-100, 0x1.039d665896880p-103, \
+    0x1.9f623d5a8a732p-107, 0x1.4c4e977ba1f5bp-110, 0x1.09d8792fb4c49p-113, 0x1.a95a5b7f87a0fp-117, \
+    0x1.54484932d2e72p-120, 0x1.1039d428a8b8ep-123, 0x1.b38fb9daa78e4p-127, 0x1.5c72fb1552d83p-130, \
+    0x1.16c262777579cp-133, 0x1.be03d0bf225c7p-137, 0x1.64cfda3281e38p-140, 0x1.1d7314f534b61p-143, \
+    0x1.c8b8218854567p-147, 0x1.6d601ad376ab9p-150, 0x1.244ce242c5561p-153, 0x1.d3ae36d13bbcep-157, \
+    0x1.7624f8a762fd8p-160, 0x1.2b50c6ec4f313p-163, 0x1.dee7a4ad4b81ep-167, 0x1.7f1fb6f10934cp-170, \
+    0x1.327fc58da0f70p-173, 0x1.ea6608e29b24dp-177, 0x1.8851a0b548ea3p-180, 0x1.39dae6f76d883p-183, \
+    0x1.f62b0b257c0d1p-187, 0x1.91bc08eac9a40p-190, 0x1.41633a556e1cdp-193, 0x1.011c2eaabe7d8p-196, \
+    0x1.9b604aaaca627p-200, 0x1.4919d5556eb52p-203, 0x1.0747ddddf22a8p-206, 0x1.a53fc9631d10cp-210, \
+    0x1.50ffd44f4a73dp-213, 0x1.0d9976a5d5297p-216, 0x1.af5bf109550f3p-220, 0x1.59165a6ddda5bp-223, \
+    0x1.1411e1f17e1e2p-226, 0x1.b9b6364f30304p-230, 0x1.615e91d8f359dp-233, 0x1.1ab20e472914ap-236, \
+    0x1.c45016d841babp-240, 0x1.69d9abe034955p-243, 0x1.217aefe690777p-246, 0x1.cf2b1970e7259p-250, \
+    0x1.7288e1271f513p-253, 0x1.286d80ec190dcp-256, 0x1.da48ce468e7c7p-260, 0x1.7b6d71d20b96cp-263, \
+    0x1.2f8ac174d6123p-266, 0x1.e5aacf2156839p-270, 0x1.8488a5b445361p-273, 0x1.36d3b7c36a91ap-276, \
+    0x1.f152bf9f10e8fp-280, 0x1.8ddbcc7f40ba6p-283, 0x1.3e497065cd61ep-286, 0x1.fd424d6faf031p-290, \
+    0x1.97683df2f268ep-293, 0x1.45ecfe5bf520ap-296, 0x1.04bd984990e6fp-299, 0x1.a12f5a0f4e3e4p-303, \
+    0x1.4dbf7b3f71cb7p-306, 0x1.0aff95cc5b093p-309, 0x1.ab328946f80eap-313, 0x1.55c2076bf9a55p-316, \
+    0x1.116805effaeaap-319, 0x1.b5733cb32b110p-323, 0x1.5df5ca28ef40dp-326, 0x1.17f7d4ed8c33dp-329, \
+    0x1.bff2ee48e0530p-333, 0x1.665bf1d3e6a8dp-336, 0x1.1eaff4a98553dp-339, 0x1.cab3210f3bb95p-343, \
+    0x1.6ef5b40c2fc77p-346, 0x1.25915cd68c9f9p-349, 0x1.d5b561574765bp-353, 0x1.77c44ddf6c516p-356, \
+    0x1.2c9d0b1923745p-359, 0x1.e0fb44f50586ep-363, 0x1.80c903f7379f1p-366, 0x1.33d4032c2c7f4p-369, \
+    0x1.ec866b79e0cb9p-373, 0x1.8a0522c7e7095p-376, 0x1.3b374f06526dep-379, 0x1.f8587e7083e2fp-383, \
+    0x1.9379fec069826p-386, 0x1.42c7ff0054685p-389, 0x1.023998cd10537p-392, 0x1.9d28f47b4d525p-396, \
+    0x1.4a8729fc3ddb7p-399, 0x1.086c219697e2bp-402, 0x1.a71368f0f3046p-406, 0x1.5275ed8d8f36bp-409, \
+    0x1.0ec4be0ad8f89p-412, 0x1.b13ac9aaf4c0fp-416, 0x1.5a956e225d672p-419, 0x1.1544581b7dec2p-422
+static __constant__ double c_pow10_recip[128] = {WG_POW10_RECIP};
 
-// a / pow10_go(n) correctly rounded, without a division: Markstein's
+// a / b correctly rounded given y = RN(1/b) (b = pow10_go(n) for div_pow10),
+// without a division: Markstein's
 // correction (P. Markstein, "Computation of elementary functions on the IBM
 // RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990): with y = RN(1/b)
 // and q within one ulp of a/b, the remainder r = a - b*q is exact in one FMA
 // and RN(q + r*y) is RN(a/b). q = RN(a*y) can be up to 1.5 ulp off, so one
 // correction brings it within one ulp and a second one makes it exact. Valid
 // while nothing overflows or underflows: |a| < 2^128 and b <= 1e127 here.
-__device__ __forceinline__ double div_pow10(double a, int n) {
-  if (n <= 0 || n >= 128) return a;  // pow10_go is 1 there
-  const double b = pow10_go(n), y = c_pow10_recip[n];
+__device__ __forceinline__ double div_by_recip(double a, double b, double y) {
   double q = __dmul_rn(a, y);
   double r = __fma_rn(-q, b, a);
   q = __fma_rn(r, y, q);
@@ -101,13 +101,31 @@ __device__ __forceinline__ double div_pow10(double a, int n) {
   return __fma_rn(r, y, q);
 }
 
+__device__ __forceinline__ double div_pow10(double a, int n) {
+  if (n <= 0 || n >= 128) return a;  // pow10_go is 1 there
+  return div_by_recip(a, pow10_go(n), c_pow10_recip[n]);
+}
+
+// The divisor pair div_pow10 uses for scale n, for a plan to carry per column:
+// b = pow10_go(n), y = RN(1/b); b = y = 1 outside (0, 128), where the
+// correction steps then return the dividend unchanged.
+inline void pow10_divisor_host(int n, double* b, double* y) {
+  static const double tab[32] = {WG_POW10_TAB}, post[4] = {WG_POW10_POST}, recip[128] = {WG_POW10_RECIP};
+  if (n <= 0 || n >= 128) { *b = 1.0; *y = 1.0; return; }
+  *b = tab[n & 31] * post[n >> 5];  // one IEEE product, as pow10_go
+  *y = recip[n];
+}
+
+// Int128 to float64 before the scale division, as decimal.go:39-51 does
+__device__ __forceinline__ double int128_to_f64(int64_t hi, uint64_t lo) {
+  if (hi == ((long long)lo >> 63)) return __ll2double_rn((long long)lo);  // fits int64
+  return __dadd_rn(__dmul_rn(__ll2double_rn(hi), 18446744073709551616.0), __ull2double_rn(lo));
+}
+
 // Int128.ToFloat64 (internal/engine/batch/decimal.go:39-51), IEEE round-to-nearest
 // at every step and no contraction, so the result is Go's bit for bit.
 __device__ __forceinline__ double dec_to_f64(int64_t hi, uint64_t lo, int scale) {
-  if ((hi == 0 && lo <= 0x7FFFFFFFFFFFFFFFULL) || (hi == -1 && lo > 0x7FFFFFFFFFFFFFFFULL))
-    return div_pow10(__ll2double_rn((long long)lo), scale);
-  double f = __dadd_rn(__dmul_rn(__ll2double_rn(hi), 18446744073709551616.0), __ull2double_rn(lo));
-  return div_pow10(f, scale);
+  return div_pow10(int128_to_f64(hi, lo), scale);
 }
 
 // expr.ColRef.EvalFloat64 (internal/engine/expr/expr.go:206-228)

@@ -66,6 +66,19 @@ __device__ __forceinline__ bool join_direct(const JoinView& j, int64_t key, int3
   return false;
 }
 
+// join_direct for an int32 probe key: the dense index in 32-bit arithmetic.
+// A slot holds the key base + index, and every build key is an int32, so an
+// index that wrapped around 2^32 lies past the last key and fails the bound.
+__device__ __forceinline__ bool join_direct_i32(const JoinView& j, int32_t key, int32_t& out, int32_t* err) {
+  if (!j.dense) return join_direct(j, (int64_t)key, out, err);
+  const uint32_t i = (uint32_t)key - (uint32_t)j.base;
+  if (i >= (uint32_t)j.mask) return false;  // mask = key span <= 2^30
+  const unsigned long long v = __ldg((const unsigned long long*)j.slots + i);
+  if ((uint32_t)v != (uint32_t)key) return false;
+  out = (int32_t)(v >> 32);
+  return true;
+}
+
 // Chain head of `key`, or -1 when absent (HashJoinProbe's idx.Get, join.go:2700).
 __device__ __forceinline__ int32_t join_head(const JoinView& j, int64_t key, int32_t* err) {
   uint64_t h = fib_slot((uint64_t)key, j.shift);
