@@ -117,6 +117,7 @@ struct DynShape {
   static constexpr bool smem_ok = true;
   static constexpr int kBlock = 512, kMinBlocks = 2;  // launch shape of the plain fused kernel
   const Plan& P;
+  __device__ __forceinline__ bool nullable() const { return true; }
   __device__ __forceinline__ int n_in() const { return P.n_in; }
   __device__ __forceinline__ int in_cls(int j) const { return P.in[j].cls; }
   __device__ __forceinline__ int n_filters() const { return P.n_filters; }
@@ -159,6 +160,9 @@ struct StatShape {
   // scheduler interleaves); with one, row by row keeps fewer values live
   static constexpr bool kRowsTogether = C::n_exprs == 0;
   const Plan& P;
+  // compiled shapes take inputs without validity bitmaps (shape_matches), so
+  // no value they read is NULL
+  __device__ __forceinline__ constexpr bool nullable() const { return false; }
   __device__ __forceinline__ constexpr int n_in() const { return C::n_in; }
   __device__ __forceinline__ constexpr int in_cls(int j) const { return C::in_cls(j); }
   __device__ __forceinline__ constexpr int n_filters() const { return C::n_filters; }
@@ -198,7 +202,7 @@ struct SrcGlobal {
   template <class Sh>
   __device__ __forceinline__ Val in(const Plan& P, const Sh& sh, int j) const {
     Val v = load_stream(P.in[j].data, sh.in_cls(j), row);
-    v.null = is_null(P.in[j], row);
+    v.null = sh.nullable() && is_null(P.in[j], row);
     return v;
   }
 };
@@ -215,7 +219,7 @@ __device__ __forceinline__ Val fetch_base(const Plan& P, const Sh& sh, const Src
   }
   const int p = j - sh.n_in();
   Val v = load_typed(P.join.pay[p].data, sh.pay_cls(p), brow);
-  v.null = is_null(P.join.pay[p], brow);
+  v.null = sh.nullable() && is_null(P.join.pay[p], brow);
   return v;
 }
 
@@ -986,7 +990,7 @@ __device__ __forceinline__ void load_rows(const Plan& P, const Sh& sh, int64_t r
         } else {
           v.lo = w[u];
         }
-        v.null = is_null(P.in[j], r0 + u);
+        v.null = sh.nullable() && is_null(P.in[j], r0 + u);
       }
     } else {
 #pragma unroll
@@ -994,7 +998,7 @@ __device__ __forceinline__ void load_rows(const Plan& P, const Sh& sh, int64_t r
         const int64_t row = r0 + u;
         if (row < P.n_items) {
           rw[u].v[j] = load_stream(P.in[j].data, cls, row);
-          rw[u].v[j].null = is_null(P.in[j], row);
+          rw[u].v[j].null = sh.nullable() && is_null(P.in[j], row);
         } else {
           rw[u].v[j].lo = 0; rw[u].v[j].hi = 0; rw[u].v[j].null = true;
         }
@@ -1147,7 +1151,7 @@ struct SrcTile {
     const int64_t row = row0 + i;
     const char* p = i < staged ? stage + C->col_off[j] + (size_t)i * es : (const char*)c.data + row * es;
     Val v = load_generic(p, cls);
-    v.null = is_null(c, row);
+    v.null = sh.nullable() && is_null(c, row);
     return v;
   }
 };

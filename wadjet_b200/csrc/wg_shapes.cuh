@@ -8,8 +8,9 @@
 //
 // A plan runs on a StatShape<C> instantiation only when shape_matches<C> finds
 // every one of these facts equal to the plan's (the plan's compact column
-// numbering is part of the shape), so a specialised launch computes exactly
-// what the generic DynShape launch computes for the same plan.
+// numbering is part of the shape) and no input or payload column carries a
+// validity bitmap, so a specialised launch computes exactly what the generic
+// DynShape launch computes for the same plan, with every NULL test compiled out.
 //
 // Shapes (ids are what wg_agg_kernel_shape reports; 0 = generic):
 //  1 star join    WHERE qty > c, fk → dim (direct payload), GROUP BY grp,
@@ -200,14 +201,14 @@ inline bool shape_matches(const Plan& P) {
   if (P.n_in != C::n_in || P.n_filters != C::n_filters || P.has_join != C::has_join || P.n_exprs != C::n_exprs)
     return false;
   for (int j = 0; j < C::n_in; ++j)
-    if (P.in[j].cls != C::in_cls(j)) return false;
+    if (P.in[j].cls != C::in_cls(j) || P.in[j].valid != nullptr) return false;
   for (int f = 0; f < C::n_filters; ++f)
     if (P.filt[f].col != C::filt_col(f) || P.filt[f].cls != C::filt_cls(f) || P.filt[f].op != C::filt_op(f))
       return false;
   if (C::has_join) {
     if (P.join.direct != C::direct || P.probe_col != C::probe_col || P.join.n_pay != C::n_pay) return false;
     for (int p = 0; p < C::n_pay; ++p)
-      if (P.join.pay[p].cls != C::pay_cls(p)) return false;
+      if (P.join.pay[p].cls != C::pay_cls(p) || P.join.pay[p].valid != nullptr) return false;
   }
   for (int e = 0; e < C::n_exprs; ++e) {
     if (P.expr[e].n_ops != C::expr_nops(e, 0) || P.expr[e].result_cls != C::expr_cls(e)) return false;
