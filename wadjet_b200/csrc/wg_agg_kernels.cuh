@@ -380,18 +380,25 @@ __device__ __forceinline__ void combine(int kind, unsigned long long& a0, unsign
 // words end up holding the exact sum mod 2^(32*nlimbs) in any interleaving.
 // (64-bit shared-memory atomic adds are compare-and-swap loops that replay
 // while lanes of a warp hit the same hot group; 32-bit adds are not.)
+// In 32-bit arithmetic: a = limb + carry wraps to 0 only for limb 2^32-1 with
+// a carry, which adds nothing here and passes the carry on, and a = 0 without
+// a carry passes none: either way the carry is unchanged and no atomic runs.
+// The top limb's carry out is dropped (mod 2^(32*nlimbs)), so its atomic
+// returns nothing.
 __device__ __forceinline__ void smem_add_limbs(unsigned* L, int nlimbs, unsigned long long lo, unsigned long long hi) {
   const unsigned x[4] = {(unsigned)lo, (unsigned)(lo >> 32), (unsigned)hi, (unsigned)(hi >> 32)};
   unsigned carry = 0;
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     if (i >= nlimbs) break;
-    const unsigned long long t = (unsigned long long)x[i] + carry;
-    if (t == 0) { carry = 0; continue; }
-    if (t == (1ULL << 32)) { carry = 1; continue; }  // adds 0 here, carries 1
-    const unsigned a = (unsigned)t;
-    const unsigned old = atomicAdd(L + i, a);
-    carry = (unsigned)(old + a) < old ? 1u : 0u;
+    const unsigned a = x[i] + carry;
+    if (a == 0) continue;
+    if (i == nlimbs - 1) {
+      atomicAdd(L + i, a);
+    } else {
+      const unsigned old = atomicAdd(L + i, a);
+      carry = old > ~a ? 1u : 0u;  // old + a overflowed 32 bits
+    }
   }
 }
 
