@@ -868,10 +868,46 @@ static wg_status run_device(const PipelineRun& r) {
   ls.smem = found;
   // a shared table that takes a whole SM: one CTA of 1024 threads for the vector kernel
   if (ls.vec && ls.smem && blocks_per_sm == 1 && env_int("WG_VEC_WIDE", 1) != 0) ls.block = 1024;
+  // self-staged vector kernel (WG_STAGE=1; off by default: on the star join
+  // it measured slower than the plain vector kernel, whose L2 prefetch already
+  // hides the HBM latency): one CTA of 1024 threads whose 32 warps each
+  // double-buffer a 64-row chunk of every input column next to the shared
+  // table, when the table (as many float-SUM copies as still fit) leaves room
+  int64_t stage_bytes = 0;
+  if (ls.vec && ls.smem && env_int("WG_STAGE", 0) != 0) {
+    int64_t chunk = 0;
+    for (int j = 0; j < ls.P.n_in; ++j) chunk += 64 * wgd::cls_bytes(ls.P.in[j].cls);
+    const int64_t sb = 32 * 2 * chunk;
+    const int64_t budget = (int64_t)ctx->max_smem_optin - sb - 2048;
+    int S2 = 0, rep2 = 0;
+    const int save_bps = blocks_per_sm;
+    blocks_per_sm = 1;  // the 3/4 fill rule of a table that has the SM to itself
+    for (int r2 = max_rep; r2 >= 1 && rep2 == 0 && budget > 0; r2 /= 2) {
+      if (ls.P.gdense) {
+        if ((int64_t)S * stride_for(r2) * 8 <= budget) { S2 = S; rep2 = r2; }
+      } else {
+        const int cand = (int)std::min<int64_t>(budget / (stride_for(r2) * 8), 16384);
+        if (fits(expect, cand)) { S2 = cand; rep2 = r2; }
+      }
+    }
+    blocks_per_sm = save_bps;
+    if (rep2 > 0) {
+      ls.stage = true;
+      ls.block = 1024;
+      blocks_per_sm = 1;
+      S = S2;
+      rep = rep2;
+      stage_bytes = sb;
+    }
+  }
   ls.P.smem_slots = ls.smem ? S : 0;
   ls.P.smem_rep = rep;
   ls.P.smem_sw = stride_for(rep);
   ls.smem_bytes = ls.smem ? (size_t)S * ls.P.smem_sw * 8 : 0;
+  if (ls.stage) {
+    ls.P.stage_off = (int32_t)((ls.smem_bytes + 127) & ~size_t(127));
+    ls.smem_bytes = (size_t)ls.P.stage_off + (size_t)stage_bytes;
+  }
   ls.P.prefetch = std::max(0, env_int("WG_PREFETCH", 2));
   ls.P.smem_combine = env_int("WG_SMEM_COMBINE", 0) != 0;
   // many rows per group: most MIN/MAX updates cannot win, so read before the atomic

@@ -92,7 +92,8 @@ struct Plan {
                                  //    [gmin, gmin + smem_slots)), no hashing and no key words
   long long gmin;
   int32_t minmax_test;           // 1: HBM MIN/MAX read the slot first and skip an atomic that cannot win
-  int32_t _pad2;
+  int32_t stage_off;             // self-staged vector kernel: byte offset of the warps' staging buffers
+                                 // in dynamic shared memory (after the shared table)
   DCol in[WG_MAX_IN];
   Pred filt[WG_MAX_FILTERS];
   JoinView join;

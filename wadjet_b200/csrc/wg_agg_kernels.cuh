@@ -82,7 +82,7 @@ __device__ __forceinline__ Val load_generic(const char* p, int cls) {
   return v;
 }
 
-__device__ __forceinline__ int cls_bytes(int cls) {
+__host__ __device__ __forceinline__ constexpr int cls_bytes(int cls) {
   return cls == WG_CLS_I32 || cls == WG_CLS_F32 ? 4 : cls == WG_CLS_DEC ? 16 : 8;
 }
 
@@ -1014,13 +1014,65 @@ __device__ __forceinline__ void load_rows(const Plan& P, const Sh& sh, int64_t r
   }
 }
 
-// U rows per lane (no join, or the direct-payload join): filters and lookups
-// for all rows first, then one warp-wide update per row.
+// Byte offset of input column j inside a staged chunk of CH rows (the columns
+// one after another, each CH values long), and the chunk's size.
+template <int CH, class Sh>
+__device__ __forceinline__ constexpr int stage_col_off(const Sh& sh, int j) {
+  int off = 0;
+  for (int i = 0; i < WG_MAX_IN; ++i) {
+    if (i >= j || i >= sh.n_in()) break;
+    off += CH * cls_bytes(sh.in_cls(i));
+  }
+  return off;
+}
+
+// Rows l .. l+U-1 of a chunk staged in shared memory (all present).
+template <int U, class Sh>
+__device__ __forceinline__ void load_rows_staged(const Sh& sh, const unsigned char* stg, int l, SrcRow (&rw)[U]) {
+#pragma unroll
+  for (int j = 0; j < WG_MAX_IN; ++j) {
+    if (j >= sh.n_in()) break;
+    const int cls = sh.in_cls(j);
+    const int es = cls_bytes(cls);
+    const unsigned char* p = stg + stage_col_off<32 * U>(sh, j) + l * es;
+    unsigned long long w[2 * U];
+    const int nbytes = U * es;
+    if (nbytes == 4) {
+      w[0] = *(const uint32_t*)p;
+    } else if (nbytes == 8) {
+      w[0] = *(const unsigned long long*)p;
+    } else {
+#pragma unroll
+      for (int q = 0; q < 2 * U; q += 2) {
+        if (q * 8 >= nbytes) break;
+        const ulonglong2 d = *((const ulonglong2*)p + q / 2);
+        w[q] = d.x;
+        w[q + 1] = d.y;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      Val& v = rw[u].v[j];
+      v.hi = 0;
+      v.null = false;
+      if (cls == WG_CLS_I32 || cls == WG_CLS_F32) {
+        const uint32_t b = (uint32_t)(w[u >> 1] >> ((u & 1) * 32));
+        v.lo = cls == WG_CLS_I32 ? (unsigned long long)(long long)(int32_t)b : as_w((double)__uint_as_float(b));
+      } else if (cls == WG_CLS_DEC) {
+        v.hi = w[2 * u];      // {int64 hi; uint64 lo}
+        v.lo = w[2 * u + 1];
+      } else {
+        v.lo = w[u];
+      }
+    }
+  }
+}
+
+// U rows per lane (no join, or the direct-payload join) already loaded:
+// filters and lookups for all rows first, then one warp-wide update per row.
 template <int NA, bool SMEM, int U, class Sh>
-__device__ __forceinline__ void process_rows_vec(const Plan& P, const Sh& sh, int64_t r0, unsigned long long* sm,
-                                                 int* s_groups, int s_limit, Credit& cr) {
-  SrcRow rw[U];
-  load_rows<U>(P, sh, r0, rw);
+__device__ __forceinline__ void process_loaded_vec(const Plan& P, const Sh& sh, int64_t r0, SrcRow (&rw)[U],
+                                                   unsigned long long* sm, int* s_groups, int s_limit, Credit& cr) {
   bool act[U];
   int32_t brow[U];
 #pragma unroll
@@ -1091,6 +1143,14 @@ __device__ __forceinline__ void process_rows_vec(const Plan& P, const Sh& sh, in
   }
 }
 
+template <int NA, bool SMEM, int U, class Sh>
+__device__ __forceinline__ void process_rows_vec(const Plan& P, const Sh& sh, int64_t r0, unsigned long long* sm,
+                                                 int* s_groups, int s_limit, Credit& cr) {
+  SrcRow rw[U];
+  load_rows<U>(P, sh, r0, rw);
+  process_loaded_vec<NA, SMEM, U>(P, sh, r0, rw, sm, s_groups, s_limit, cr);
+}
+
 // Grid-stride over chunks of 32*U rows; MB CTAs of BLK threads per SM.
 template <int NA, bool SMEM, class Sh, int U, int MB, int BLK>
 __global__ void __launch_bounds__(BLK, MB) pipeline_vec_kernel(const __grid_constant__ Plan P) {
@@ -1120,6 +1180,88 @@ __global__ void __launch_bounds__(BLK, MB) pipeline_vec_kernel(const __grid_cons
     __syncthreads();
     smem_table_flush<NA>(P, sm, S, cr);
   }
+  cr.release(P.T);
+}
+
+// Self-staged vector kernel: one CTA of 1024 threads per SM with a shared
+// table. Each warp copies its next chunk of 32*U rows (every input column, one
+// bulk asynchronous copy per column, completing on the warp's own mbarrier)
+// into one half of its shared-memory double buffer while it evaluates the
+// current chunk out of the other half, so the warp's HBM reads for the next
+// chunk are in flight during the current chunk's lookups and table updates.
+// A warp's last chunk, when it is cut short by the end of the input, is read
+// from HBM directly. Every wait is bounded (wg_tma.cuh); a timeout records
+// WG_DERR_TIMEOUT, and the warp stops after waiting (bounded) for the copy it
+// still has in flight.
+template <int NA, class Sh, int U>
+__global__ void __launch_bounds__(1024, 1) pipeline_stage_kernel(const __grid_constant__ Plan P) {
+  extern __shared__ __align__(128) unsigned long long sm[];  // [shared table][staging]
+  __shared__ int s_groups;
+  __shared__ __align__(8) unsigned long long bars[64];      // two per warp
+  constexpr int CH = 32 * U;
+  const Sh sh{P};
+  Credit cr;
+  const int S = P.smem_slots;
+  const int s_limit = (S * 7) / 8;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int cbytes = stage_col_off<CH>(sh, WG_MAX_IN);
+  unsigned char* stg = (unsigned char*)sm + P.stage_off + (size_t)warp * 2 * cbytes;
+  unsigned long long* bar = bars + 2 * warp;
+  if (lane == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_init_fence();
+  }
+  smem_table_init(P, sm, S, &s_groups);
+  __syncthreads();
+  const int64_t wpb = blockDim.x >> 5;
+  const int64_t step = (int64_t)gridDim.x * wpb * CH;
+  const int64_t base0 = ((int64_t)blockIdx.x * wpb + warp) * CH;
+  // chunk k of this warp (base0 + k * step) goes to stage k & 1 and completes
+  // that stage's phase k >> 1
+  auto issue = [&](int64_t k) {
+    const int s = (int)(k & 1);
+    const int64_t b = base0 + k * step;
+    unsigned char* dst = stg + s * cbytes;
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // earlier reads of this half come first
+    mbar_arrive_expect_tx(&bar[s], (uint32_t)cbytes);
+#pragma unroll
+    for (int j = 0; j < WG_MAX_IN; ++j) {
+      if (j >= sh.n_in()) break;
+      const int es = cls_bytes(sh.in_cls(j));
+      bulk_g2s(dst + stage_col_off<CH>(sh, j), (const char*)P.in[j].data + b * es, (uint32_t)(CH * es), &bar[s]);
+    }
+  };
+  // chunks [0, issued) have been started, chunks [0, landed) waited for
+  int64_t issued = 0, landed = 0;
+  if (base0 + CH <= P.n_items) {
+    if (lane == 0) issue(0);
+    issued = 1;
+  }
+  int64_t k = 0;
+  for (int64_t base = base0; base < P.n_items; base += step, ++k) {
+    const bool staged = base + CH <= P.n_items;
+    if (base + step + CH <= P.n_items) {  // the next chunk is whole: start its copy now
+      if (lane == 0) issue(k + 1);
+      issued = k + 2;
+    }
+    SrcRow rw[U];
+    const int64_t r0 = base + (int64_t)lane * U;
+    if (staged) {
+      const bool ok = __all_sync(WG_FULL_MASK, mbar_wait(&bar[k & 1], (uint32_t)((k >> 1) & 1), P.err));
+      if (!ok) break;
+      landed = k + 1;
+      load_rows_staged<U>(sh, stg + (k & 1) * cbytes, lane * U, rw);
+    } else {
+      load_rows<U>(P, sh, r0, rw);
+    }
+    process_loaded_vec<NA, true, U>(P, sh, r0, rw, sm, &s_groups, s_limit, cr);
+    __syncwarp();
+  }
+  // no copy outlives the CTA: after a timeout, wait (bounded) for what is in flight
+  for (int64_t c = landed; c < issued; ++c) mbar_wait(&bar[c & 1], (uint32_t)((c >> 1) & 1), P.err);
+  __syncthreads();
+  smem_table_flush<NA>(P, sm, S, cr);
   cr.release(P.T);
 }
 

@@ -22,6 +22,7 @@ struct LaunchSpec {
   bool tile = false;          // TMA-staged tile kernel
   wgd::TileCfg cfg{};
   int vec = 0;                // compiled shapes: rows per lane of the vector kernel (0 = one-row kernel)
+  bool stage = false;         // vector kernel with a shared table: the self-staged variant (1024 threads, 1 CTA/SM)
 };
 
 template <int NA, bool SMEM, class Sh, int U, int MB, int BLK>
@@ -40,6 +41,15 @@ static void launch_vec_s(const LaunchSpec& ls, cudaStream_t st) {
   else launch_vec_one<NA, SMEM, Sh, 2, 2, 512>(ls, st);
 }
 
+// Self-staged vector kernel: smem_bytes covers the shared table and the
+// staging buffers at P.stage_off.
+template <int NA, class Sh>
+static void launch_stage_one(const LaunchSpec& ls, cudaStream_t st) {
+  cudaFuncSetAttribute(wgd::pipeline_stage_kernel<NA, Sh, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)ls.smem_bytes);
+  wgd::pipeline_stage_kernel<NA, Sh, 2><<<ls.grid, 1024, ls.smem_bytes, st>>>(ls.P);
+}
+
 // The vector kernel exists for compiled shapes only (DynShape never gets here).
 template <int NA, class Sh>
 static void launch_vec_t(const LaunchSpec& ls, cudaStream_t st, bool smem) {
@@ -47,6 +57,7 @@ static void launch_vec_t(const LaunchSpec& ls, cudaStream_t st, bool smem) {
     (void)ls; (void)st; (void)smem;
   } else {
     if constexpr (Sh::smem_ok) {
+      if (smem && ls.stage) { launch_stage_one<NA, Sh>(ls, st); return; }
       if (smem) { launch_vec_s<NA, Sh, true>(ls, st); return; }
     }
     launch_vec_s<NA, Sh, false>(ls, st);
