@@ -66,6 +66,7 @@ def parse_args():
     p.add_argument("--qps", type=float, default=2000.0, help="serving: Poisson arrival rate")
     p.add_argument("--seconds", type=float, default=3.0, help="serving: arrival window")
     p.add_argument("--slots", type=int, default=8, help="serving: concurrent request slots")
+    p.add_argument("--groupby-log2-rows", default="20,28", help="groupby: table sizes (log2 rows), comma-separated")
     return p.parse_args()
 
 
@@ -404,7 +405,7 @@ def run_groupby(args):
     ctx = wg.Context(0)
     stream = torch.cuda.ExternalStream(ctx.stream)
     peak, kind = measured_peak_hbm()
-    for n in (1 << 20, args.rows):  # --rows: the large table (2^28 rows by default)
+    for n in [1 << int(b) for b in args.groupby_log2_rows.split(",")]:
         k, v, f, flag = synth.groupby(ctx, n)
         batch = wg.Batch([wg.Column(wg.TYPE_INT64, k), wg.Column(wg.TYPE_INT64, v), wg.Column(wg.TYPE_FLOAT64, f),
                           wg.Column(wg.TYPE_INT32, flag)])

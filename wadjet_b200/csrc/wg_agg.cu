@@ -986,7 +986,21 @@ static wg_status run_device(const PipelineRun& r) {
     a->upper_groups += a->L.key_words == 0 ? 0 : n_items * fan;
     return check_device_error(ctx);
   }
-  // 2) small table: snapshot, run, replay on overflow
+  // 2) small table: snapshot, run, replay on overflow. Threads that race to
+  // insert the same new key each hold a reservation until they lose, so the
+  // table leaves room for one per launched thread beside the expected groups
+  // (else a first run over few hot keys could be refused and replayed).
+  // Best effort: not for a spilled aggregate's partition tables, and only
+  // within the snapshot size and half of what the HBM ledger has left.
+  if (!a->spill) {
+    const int64_t want = std::max<int64_t>(a->hint, a->known_groups) + (int64_t)ls.grid * ls.block;
+    const int64_t nb = (int64_t)table_words(a, cap_for(want)) * 8;
+    const int64_t budget = ctx->ledger.budget();
+    if (limit() < want && nb <= kSnapshotMaxBytes && (budget <= 0 || 2 * nb <= budget - ctx->ledger.used())) {
+      WG_TRY(rebuild_table(a, cap_for(want), a->L));
+      WG_TRY(refresh_groups(a));
+    }
+  }
   const int64_t tbytes = table_words(a, a->cap) * 8;
   if (tbytes <= kSnapshotMaxBytes) {
     for (int attempt = 0; attempt < 16; ++attempt) {
