@@ -766,7 +766,12 @@ template <int NA>
 __device__ __forceinline__ void smem_table_flush(const Plan& P, const unsigned long long* sm, int S, Credit& cr) {
   const LayoutAcc ly{P.L};
   const int sw = P.L.slot_words, ssw = smem_stride(P), rep = smem_copies(P);
-  for (int i = threadIdx.x; i < S; i += blockDim.x) {
+  // CTAs start their pass at different slots: CTAs that finish together then
+  // insert and update different groups at any moment instead of racing on the
+  // same new keys, the same reservation counter and the same state words
+  const int off = (int)(((long long)blockIdx.x * S) / max(1, (int)gridDim.x));
+  for (int i0 = threadIdx.x; i0 < S; i0 += blockDim.x) {
+    const int i = i0 + off < S ? i0 + off : i0 + off - S;
     const unsigned long long* s = sm + (size_t)i * ssw;
     unsigned long long key = s[0];
     if (P.gdense) {  // a direct slot is in use once it counted a row
