@@ -199,14 +199,15 @@ def test_starjoin_with_missing_and_out_of_range_keys(ctx, dense, monkeypatch):
 
 @pytest.mark.parametrize("tile,spec,part", [("0", "1", "1"), ("0", "1", "0"), ("1", "1", "1"), ("0", "0", "1")])
 def test_highcard_workload_matches_oracle(ctx, tile, spec, part, monkeypatch):
-    """GROUP BY (a int32, b int64) packed key, 2^22 rows (~3.9M groups), with and without the
-    hash-partitioned reorder of the input (the table is large enough for it to apply)."""
+    """GROUP BY (a int32, b int64) packed key, 2^22 + 1234 rows (~3.9M groups, a ragged last
+    partition tile), with and without the hash-partitioned reorder of the input (the table is
+    large enough for it to apply)."""
     import wadjet_b200 as wg
     from wadjet_b200 import synth
     monkeypatch.setenv("WG_TILE", tile)
     monkeypatch.setenv("WG_SPECIALIZE", spec)
     monkeypatch.setenv("WG_AGG_PARTITION", part)
-    n = 1 << 22
+    n = (1 << 22) + 1234
     a, b, amt, x = synth.highcard(ctx, n)
     aggs = [wg.AggColumn(wg.AGG_SUM, 2), wg.AggColumn(wg.AGG_COUNT, -1), wg.AggColumn(wg.AGG_MIN, 3),
             wg.AggColumn(wg.AGG_MAX, 3)]

@@ -1086,7 +1086,7 @@ static wg_status run_partitioned(const PipelineRun& r, const wgd::Plan& P0, cons
   DevBuf counts, offs;
   WG_TRY(counts.ensure(ctx, (int64_t)np * grid * 4));
   WG_TRY(offs.ensure(ctx, (int64_t)np * grid * 8));
-  wgd::part_count_kernel<<<grid, 256, (size_t)np * 4, ctx->stream>>>(P, pbits, 64 - pbits, counts.as<uint32_t>());
+  wgd::part_count_kernel<<<grid, wgd::kPartThreads, wgd::part_count_smem(np), ctx->stream>>>(P, pbits, 64 - pbits, counts.as<uint32_t>());
   ctx->count_launch();
   WG_CUDA_TRY(cudaGetLastError());
   std::vector<uint32_t> hc((size_t)np * grid);
@@ -1106,7 +1106,7 @@ static wg_status run_partitioned(const PipelineRun& r, const wgd::Plan& P0, cons
     po.data[j] = bufs[(size_t)j].as<char>();
     po.es[j] = es;
   }
-  wgd::part_scatter_kernel<<<grid, 256, (size_t)np * 12, ctx->stream>>>(P, pbits, 64 - pbits,
+  wgd::part_scatter_kernel<<<grid, wgd::kPartThreads, wgd::part_scatter_smem(np), ctx->stream>>>(P, pbits, 64 - pbits,
                                                                         offs.as<unsigned long long>(), po);
   ctx->count_launch();
   WG_CUDA_TRY(cudaGetLastError());
@@ -1214,7 +1214,7 @@ static wg_status spill_consume(const PipelineRun& r, const wgd::Plan& P0, const 
   for (int64_t r0 = 0; r0 < n; r0 += win) {
     const int64_t m = std::min(win, n - r0);
     const wgd::Plan P = part_plan(a, P0, r0, m);
-    wgd::part_count_kernel<<<grid, 256, (size_t)np * 4, ctx->stream>>>(P, pbits, kSpillPartShift,
+    wgd::part_count_kernel<<<grid, wgd::kPartThreads, wgd::part_count_smem(np), ctx->stream>>>(P, pbits, kSpillPartShift,
                                                                        counts.as<uint32_t>());
     ctx->count_launch();
     WG_CUDA_TRY(cudaGetLastError());
@@ -1237,7 +1237,7 @@ static wg_status spill_consume(const PipelineRun& r, const wgd::Plan& P0, const 
       po.data[j] = a->sp_dev[(size_t)j].as<char>();
       po.es[j] = a->sp_es[(size_t)j];
     }
-    wgd::part_scatter_kernel<<<grid, 256, (size_t)np * 12, ctx->stream>>>(P, pbits, kSpillPartShift,
+    wgd::part_scatter_kernel<<<grid, wgd::kPartThreads, wgd::part_scatter_smem(np), ctx->stream>>>(P, pbits, kSpillPartShift,
                                                                           offs.as<unsigned long long>(), po);
     ctx->count_launch();
     WG_CUDA_TRY(cudaGetLastError());

@@ -898,17 +898,29 @@ __device__ __forceinline__ uint32_t row_partition(const Plan& P, const Sh& sh, i
   return (uint32_t)(packed_slot(k0, k1, 0) >> pshift) & mask;
 }
 
+// Both partition kernels walk the input in tiles of kPartTile rows, CTA c
+// taking tiles c, c + gridDim.x, ...; so the rows a CTA counts per partition
+// are exactly the rows it later scatters there.
+constexpr int kPartThreads = 512;
+constexpr int kPartTile = 4096;
+static_assert(kPartTile <= 65536, "tile-local row indices are 16-bit");
+__host__ __device__ constexpr size_t part_count_smem(int np) { return (size_t)np * 4; }
+__host__ __device__ constexpr size_t part_scatter_smem(int np) {
+  return (size_t)np * 8 + (size_t)np * 12 + (size_t)kPartTile * 4;
+}
+
 // Rows per partition seen by each CTA (counts[p * gridDim.x + cta]).
-static __global__ void __launch_bounds__(256) part_count_kernel(const __grid_constant__ Plan P, int pbits, int pshift,
-                                                                uint32_t* counts) {
+static __global__ void __launch_bounds__(kPartThreads) part_count_kernel(const __grid_constant__ Plan P, int pbits,
+                                                                         int pshift, uint32_t* counts) {
   extern __shared__ uint32_t hist[];
   const int np = 1 << pbits;
   for (int i = threadIdx.x; i < np; i += blockDim.x) hist[i] = 0;
   __syncthreads();
   const DynShape sh{P};
-  for (int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < P.n_items;
-       row += (int64_t)gridDim.x * blockDim.x)
-    atomicAdd(&hist[row_partition(P, sh, row, pbits, pshift)], 1u);
+  for (int64_t t0 = (int64_t)blockIdx.x * kPartTile; t0 < P.n_items; t0 += (int64_t)gridDim.x * kPartTile) {
+    const int m = (int)min((int64_t)kPartTile, P.n_items - t0);
+    for (int k = threadIdx.x; k < m; k += blockDim.x) atomicAdd(&hist[row_partition(P, sh, t0 + k, pbits, pshift)], 1u);
+  }
   __syncthreads();
   for (int i = threadIdx.x; i < np; i += blockDim.x) counts[(size_t)i * gridDim.x + blockIdx.x] = hist[i];
 }
@@ -919,32 +931,90 @@ struct PartOut {
   int32_t es[WG_MAX_IN];
 };
 
-// Same grid and row order as part_count_kernel: each CTA writes its rows of
-// partition p from offs[p * gridDim.x + cta] on.
-static __global__ void __launch_bounds__(256) part_scatter_kernel(const __grid_constant__ Plan P, int pbits,
-                                                                  int pshift, const unsigned long long* offs,
-                                                                  PartOut out) {
-  extern __shared__ unsigned long long base[];  // np bases, then np 32-bit cursors
+// Exclusive prefix sums of v[0..n) in place (n <= 2 * blockDim.x, blockDim.x a
+// multiple of 32, at most 32 warps); every thread of the CTA calls it.
+__device__ __forceinline__ void block_exclusive_scan(uint32_t* v, int n, uint32_t* warp_tot) {
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5, nw = blockDim.x >> 5;
+  const uint32_t a = 2 * t < n ? v[2 * t] : 0u, b = 2 * t + 1 < n ? v[2 * t + 1] : 0u;
+  uint32_t x = a + b;  // inclusive scan of the pair sums within the warp
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(WG_FULL_MASK, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warp_tot[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    uint32_t z = lane < nw ? warp_tot[lane] : 0u;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(WG_FULL_MASK, z, o);
+      if (lane >= o) z += y;
+    }
+    if (lane < nw) warp_tot[lane] = z;  // inclusive warp totals
+  }
+  __syncthreads();
+  const uint32_t before = (w > 0 ? warp_tot[w - 1] : 0u) + x - (a + b);
+  if (2 * t < n) v[2 * t] = before;
+  if (2 * t + 1 < n) v[2 * t + 1] = before + a;
+  __syncthreads();
+}
+
+// Same tiles as part_count_kernel: CTA c writes its rows of partition p from
+// offs[p * gridDim.x + c] on. Per tile, the rows are counting-sorted by
+// partition in shared memory (tile-local row indices), then written column by
+// column in that order, so consecutive threads store consecutive rows of one
+// partition instead of one row each to scattered partitions.
+static __global__ void __launch_bounds__(kPartThreads) part_scatter_kernel(const __grid_constant__ Plan P, int pbits,
+                                                                           int pshift,
+                                                                           const unsigned long long* offs,
+                                                                           PartOut out) {
+  extern __shared__ unsigned long long gcur[];  // np output cursors, then the arrays below
+  __shared__ uint32_t warp_tot[32];
   const int np = 1 << pbits;
-  uint32_t* cur = (uint32_t*)(base + np);
+  uint32_t* hist = (uint32_t*)(gcur + np);      // rows of partition p in this tile
+  uint32_t* loff = hist + np;                   // their first position in the tile order
+  uint32_t* lcur = loff + np;
+  uint16_t* part = (uint16_t*)(lcur + np);      // partition of tile row k
+  uint16_t* perm = part + kPartTile;            // tile row at position k of the order
   for (int i = threadIdx.x; i < np; i += blockDim.x) {
-    base[i] = offs[(size_t)i * gridDim.x + blockIdx.x];
-    cur[i] = 0;
+    gcur[i] = offs[(size_t)i * gridDim.x + blockIdx.x];
+    hist[i] = 0;
   }
   __syncthreads();
   const DynShape sh{P};
-  for (int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; row < P.n_items;
-       row += (int64_t)gridDim.x * blockDim.x) {
-    const uint32_t p = row_partition(P, sh, row, pbits, pshift);
-    const unsigned long long dst = base[p] + atomicAdd(&cur[p], 1u);
+  for (int64_t t0 = (int64_t)blockIdx.x * kPartTile; t0 < P.n_items; t0 += (int64_t)gridDim.x * kPartTile) {
+    const int m = (int)min((int64_t)kPartTile, P.n_items - t0);
+    for (int k = threadIdx.x; k < m; k += blockDim.x) {
+      const uint32_t p = row_partition(P, sh, t0 + k, pbits, pshift);
+      part[k] = (uint16_t)p;
+      atomicAdd(&hist[p], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < np; i += blockDim.x) { loff[i] = hist[i]; lcur[i] = 0; }
+    __syncthreads();
+    block_exclusive_scan(loff, np, warp_tot);
+    for (int k = threadIdx.x; k < m; k += blockDim.x) {
+      const uint32_t p = part[k];
+      perm[loff[p] + atomicAdd(&lcur[p], 1u)] = (uint16_t)k;
+    }
+    __syncthreads();
     for (int j = 0; j < P.n_in; ++j) {
       const int es = out.es[j];
-      const char* src = (const char*)P.in[j].data + row * es;
-      char* d = out.data[j] + dst * es;
-      if (es == 4) *(uint32_t*)d = __ldcs((const uint32_t*)src);
-      else if (es == 8) *(unsigned long long*)d = __ldcs((const unsigned long long*)src);
-      else *(longlong2*)d = __ldcs((const longlong2*)src);
+      const char* src = (const char*)P.in[j].data + t0 * es;
+      char* dcol = out.data[j];
+      for (int q = threadIdx.x; q < m; q += blockDim.x) {
+        const int k = perm[q];
+        const uint32_t p = part[k];
+        char* d = dcol + (gcur[p] + (q - loff[p])) * es;
+        if (es == 4) *(uint32_t*)d = __ldg((const uint32_t*)(src + (size_t)k * 4));
+        else if (es == 8) *(unsigned long long*)d = __ldg((const unsigned long long*)(src + (size_t)k * 8));
+        else *(longlong2*)d = __ldg((const longlong2*)(src + (size_t)k * 16));
+      }
     }
+    __syncthreads();
+    for (int i = threadIdx.x; i < np; i += blockDim.x) { gcur[i] += hist[i]; hist[i] = 0; }
+    __syncthreads();
   }
 }
 
