@@ -298,6 +298,10 @@ struct wg_agg {
   // export staging (kept for the next export): every output field of a chunk
   // side by side on the device, read back in one copy through pinned memory
   wg::DevBuf exp_dev;
+  // the in-HBM key-hash reorder's copy of the input and its counters (kept for
+  // the next query: allocating and freeing GBs per query costs milliseconds)
+  std::vector<wg::DevBuf> part_bufs;
+  wg::DevBuf part_counts, part_offs;
   char* exp_host = nullptr;
   int64_t exp_host_bytes = 0;
   ~wg_agg() {
@@ -1061,15 +1065,17 @@ static wg_status run_device(const PipelineRun& r) {
 // order, so the atomics of any stretch of the run land in one L2-sized region
 // of the table instead of all over HBM. Applies to inputs of at least 2^22
 // rows, without a join, selection vector or NULL bitmaps, whose table is at
-// least 64 MB, when WG_AGG_PARTITION=1 (off by default: on the 2^28-row,
-// 65.9M-group case it measured slower than the direct run). *done says whether it ran.
+// least 64 MB (WG_AGG_PARTITION=0 turns it off; on the 2^28-row, 65.9M-group
+// case it takes 40 ms against 59 ms direct). The reordered copy is kept on the
+// aggregate for the next query; when the ledger has no room for it the input
+// runs directly. *done says whether it ran.
 static wg_status run_partitioned(const PipelineRun& r, const wgd::Plan& P0, const std::vector<int>& in_map,
                                  bool* done) {
   *done = false;
   wg_agg* a = r.agg;
   Ctx* ctx = a->ctx;
   const int64_t n = P0.n_items;
-  if (env_int("WG_AGG_PARTITION", 0) == 0 || r.join || P0.sel || a->L.key_words == 0 || n < (int64_t(1) << 22))
+  if (env_int("WG_AGG_PARTITION", 1) == 0 || r.join || P0.sel || a->L.key_words == 0 || n < (int64_t(1) << 22))
     return WG_OK;
   for (int j = 0; j < P0.n_in; ++j)
     if (P0.in[j].valid) return WG_OK;
@@ -1083,7 +1089,8 @@ static wg_status run_partitioned(const PipelineRun& r, const wgd::Plan& P0, cons
   P.L = launch_layout(a, P0);
   P.err = ctx->dev_error;
   const unsigned grid = (unsigned)(ctx->sm_count * 2);
-  DevBuf counts, offs;
+  DevBuf& counts = a->part_counts;
+  DevBuf& offs = a->part_offs;
   WG_TRY(counts.ensure(ctx, (int64_t)np * grid * 4));
   WG_TRY(offs.ensure(ctx, (int64_t)np * grid * 8));
   wgd::part_count_kernel<<<grid, wgd::kPartThreads, wgd::part_count_smem(np), ctx->stream>>>(P, pbits, 64 - pbits, counts.as<uint32_t>());
@@ -1097,12 +1104,16 @@ static wg_status run_partitioned(const PipelineRun& r, const wgd::Plan& P0, cons
   for (size_t i = 0; i < hc.size(); ++i) { ho[i] = acc; acc += hc[i]; }  // partition-major, then CTA
   if ((int64_t)acc != n) return fail(WG_E_CUDA, "partition counts do not add up to the input rows");
   WG_CUDA_TRY(cudaMemcpyAsync(offs.get(), ho.data(), ho.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
-  std::vector<DevBuf> bufs((size_t)P.n_in);
+  std::vector<DevBuf>& bufs = a->part_bufs;
+  if ((int)bufs.size() < P.n_in) bufs.resize((size_t)P.n_in);
   wgd::PartOut po{};
   for (int j = 0; j < P.n_in; ++j) {
     const int cls = P.in[j].cls;
     const int es = cls == WG_CLS_I32 || cls == WG_CLS_F32 ? 4 : cls == WG_CLS_DEC ? 16 : 8;
-    WG_TRY(bufs[(size_t)j].alloc(ctx, n * es));
+    if (bufs[(size_t)j].ensure(ctx, n * es) != WG_OK) {  // no room for the copy: run directly
+      bufs.clear();
+      return WG_OK;
+    }
     po.data[j] = bufs[(size_t)j].as<char>();
     po.es[j] = es;
   }
@@ -1127,7 +1138,6 @@ static wg_status run_partitioned(const PipelineRun& r, const wgd::Plan& P0, cons
   r2.in = &d2;
   r2.no_partition = true;
   WG_TRY(run_device(r2));
-  WG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));  // the copy is freed on return
   *done = true;
   return WG_OK;
 }
