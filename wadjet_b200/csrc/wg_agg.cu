@@ -94,20 +94,49 @@ __global__ void iota_kernel(int64_t* out, int64_t n) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) out[i] = i;
 }
 
+// The used slots' indices into `list` (any order). Each thread checks
+// kCompactK slots per pass (coalesced per step), the CTA sums its finds with a
+// block scan and takes one range of `list` with a single atomic per pass,
+// instead of one atomic per warp on the shared counter.
+constexpr int kCompactK = 8;
 __global__ void compact_kernel(Layout L, Table T, int64_t* list, unsigned long long* count) {
+  __shared__ unsigned warp_sum[32];
+  __shared__ unsigned long long s_base;
   const uint64_t cap = T.mask + 1;
   const uint64_t n = L.key_words == 0 ? 1 : cap + 2;
-  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < n; base += stride) {
-    const uint64_t i = base + threadIdx.x;
-    const bool used = i < n && slot_used(L, T.slots + i * L.slot_words, i, cap);
-    const unsigned m = __ballot_sync(WG_FULL_MASK, used);
-    if (m == 0) continue;
-    const int lane = threadIdx.x & 31;
-    unsigned long long off = 0;
-    if (lane == 0) off = atomicAdd(count, (unsigned long long)__popc(m));
-    off = __shfl_sync(WG_FULL_MASK, off, 0);
-    if (used) list[off + __popc(m & ((1u << lane) - 1))] = (int64_t)i;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const uint64_t span = (uint64_t)blockDim.x * kCompactK;
+  for (uint64_t base = (uint64_t)blockIdx.x * span; base < n; base += (uint64_t)gridDim.x * span) {
+    unsigned bits = 0, c = 0;
+#pragma unroll
+    for (int j = 0; j < kCompactK; ++j) {
+      const uint64_t i = base + (uint64_t)j * blockDim.x + threadIdx.x;
+      if (i < n && slot_used(L, T.slots + i * L.slot_words, i, cap)) { bits |= 1u << j; ++c; }
+    }
+    unsigned x = c;  // inclusive scan within the warp
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned y = __shfl_up_sync(WG_FULL_MASK, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sum[w] = x;
+    __syncthreads();
+    if (w == 0) {
+      unsigned z = lane < nw ? warp_sum[lane] : 0u;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned y = __shfl_up_sync(WG_FULL_MASK, z, o);
+        if (lane >= o) z += y;
+      }
+      if (lane < nw) warp_sum[lane] = z;
+      if (lane == nw - 1) s_base = z ? atomicAdd(count, (unsigned long long)z) : 0ULL;
+    }
+    __syncthreads();
+    unsigned long long off = s_base + (w > 0 ? warp_sum[w - 1] : 0u) + x - c;
+#pragma unroll
+    for (int j = 0; j < kCompactK; ++j)
+      if (bits >> j & 1u) list[off++] = (int64_t)(base + (uint64_t)j * blockDim.x + threadIdx.x);
+    __syncthreads();  // warp_sum and s_base are reused by the next pass
   }
 }
 
