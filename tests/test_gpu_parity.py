@@ -105,16 +105,18 @@ def test_join_matches_oracle(ctx, kt, dups, nulls):
 
 @pytest.mark.parametrize("dup", [False, True])
 @pytest.mark.parametrize("probe_first", [False, True])
-def test_join_dense_unique_build(ctx, dup, probe_first):
+@pytest.mark.parametrize("full", [False, True])
+def test_join_dense_unique_build(ctx, dup, probe_first, full):
     """Unique int32 keys over a narrow range with one int32 payload: the build makes only
-    the dense direct table, and the hash index waits for the first non-fused probe. A
-    duplicate key sends the build down the hash path. The fused pipeline (GROUP BY the
-    payload), the pair probe, the payload gather and the build stats agree with the oracle
-    whichever of the fused and non-fused calls comes first."""
+    the dense direct table (payloads alone when the keys fill their range), and the hash
+    index waits for the first non-fused probe. A duplicate key sends the build down the
+    hash path. The fused pipeline (GROUP BY the payload), the pair probe, the payload
+    gather and the build stats agree with the oracle whichever of the fused and non-fused
+    calls comes first."""
     import wadjet_b200 as wg
     rng = np.random.default_rng(5 + dup)
     nb, npr = 30_000, 200_000
-    bkeys = (rng.permutation(40_000)[:nb] + 1000).astype(np.int32)
+    bkeys = (rng.permutation(nb if full else 40_000)[:nb] + 1000).astype(np.int32)
     if dup:
         bkeys[-1] = bkeys[0]
     grp = rng.integers(0, 300, nb).astype(np.int32)

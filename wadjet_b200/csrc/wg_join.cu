@@ -211,6 +211,12 @@ __global__ void dense_build_kernel(DCol key, int64_t n, const uint32_t* pay, lon
   }
 }
 
+// Payload-only dense table from a full dense direct table (every slot used).
+__global__ void dense_payload_kernel(const unsigned long long* slots, int64_t n, uint32_t* out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = (uint32_t)(__ldg(slots + i) >> 32);
+}
+
 __global__ void fill_u64_kernel(unsigned long long* out, int64_t n, unsigned long long v) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     out[i] = v;
@@ -288,8 +294,9 @@ struct wg_join {
   int64_t max_fanout = 1;
   bool hashed = false;  // the hash index (slots/next) is built; a dense unique build defers it to first use
   // direct-payload copy of the table for the fused kernel (see JoinView)
-  wg::DevBuf dslots;
+  wg::DevBuf dslots, dpay;
   bool direct = false;
+  bool full = false;  // dense and every key of the range present: dpay holds the payloads
   int32_t sentinel = 0;
   bool dense = false;
   long long dense_base = 0;
@@ -435,6 +442,10 @@ wg_status join_view_fused(wg_join* j, wgd::JoinView* v) {
       v->dense = 1;
       v->base = j->dense_base;
       v->mask = (uint64_t)j->dense_slots;
+      if (j->full) {
+        v->dense = 2;
+        v->slots = j->dpay.get();
+      }
     }
   }
   return WG_OK;
@@ -495,6 +506,11 @@ static wg_status build_hash(wg_join* j) {
 // straight from the rows and the hash index is deferred to its first use (the
 // fused probe never needs it). *done is false when this shape does not apply
 // or a duplicate key turned up; the caller then builds the hash index.
+static bool env_full_dense() {
+  const char* e = std::getenv("WG_JOIN_FULL_DENSE");
+  return !e || std::atoi(e) != 0;
+}
+
 static wg_status build_dense_unique(wg_join* j, bool* done) {
   *done = false;
   Ctx* ctx = j->ctx;
@@ -549,6 +565,16 @@ static wg_status build_dense_unique(wg_join* j, bool* done) {
   j->sentinel = sentinel;
   j->dense_base = r[0];
   j->dense_slots = span;
+  // unique keys filling their whole range: the payloads alone (half the bytes a probe's cache lines carry)
+  j->full = false;
+  if (span == j->rows && env_full_dense()) {
+    WG_TRY(j->dpay.ensure(ctx, span * 4));
+    dense_payload_kernel<<<grid_for(ctx, span, 256), 256, 0, ctx->stream>>>(j->dslots.as<unsigned long long>(), span,
+                                                                          j->dpay.as<uint32_t>());
+    ctx->count_launch();
+    WG_CUDA_TRY(cudaGetLastError());
+    j->full = true;
+  }
   *done = true;
   return WG_OK;
 }
@@ -645,6 +671,7 @@ wg_status wg_join_build_finish(wg_join* j) {
   // 4-byte payload column without NULLs, and an int32 value that is no key.
   j->direct = false;
   j->dense = false;
+  j->full = false;
   const char* dsw = std::getenv("WG_JOIN_DIRECT");
   if ((!dsw || std::atoi(dsw) != 0) && j->unique && j->flavor == 0 && j->pay.size() == 1 && j->pay[0].es == 4 &&
       !j->pay[0].has_valid && j->rows > 0) {

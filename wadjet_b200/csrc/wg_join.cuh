@@ -36,7 +36,9 @@ struct JoinView {
   int32_t sentinel;
   // Dense direct table (unique keys spanning a range at most a few times the
   // build size): slot i holds key base+i, so a probe is one load with no hash
-  // and no probing; `mask` then holds the number of slots.
+  // and no probing; `mask` then holds the number of slots. dense = 2: every
+  // key of the range is present, so `slots` is just the 4-byte payloads
+  // (payload of key base+i at i) and a key in range always matches.
   int32_t dense;
   long long base;
   DCol pay[WG_MAX_PAYLOAD];
@@ -45,6 +47,12 @@ struct JoinView {
 // Direct-payload lookup: the payload's raw 32 bits of `key`, or false.
 __device__ __forceinline__ bool join_direct(const JoinView& j, int64_t key, int32_t& out, int32_t* err) {
   const unsigned long long* s = (const unsigned long long*)j.slots;
+  if (j.dense == 2) {
+    const unsigned long long i = (unsigned long long)(key - j.base);
+    if (i >= j.mask) return false;
+    out = (int32_t)__ldg((const uint32_t*)j.slots + i);
+    return true;
+  }
   if (j.dense) {
     const unsigned long long i = (unsigned long long)(key - j.base);
     if (i >= j.mask) return false;
@@ -73,6 +81,10 @@ __device__ __forceinline__ bool join_direct_i32(const JoinView& j, int32_t key, 
   if (!j.dense) return join_direct(j, (int64_t)key, out, err);
   const uint32_t i = (uint32_t)key - (uint32_t)j.base;
   if (i >= (uint32_t)j.mask) return false;  // mask = key span <= 2^30
+  if (j.dense == 2) {
+    out = (int32_t)__ldg((const uint32_t*)j.slots + i);
+    return true;
+  }
   const unsigned long long v = __ldg((const unsigned long long*)j.slots + i);
   if ((uint32_t)v != (uint32_t)key) return false;
   out = (int32_t)(v >> 32);
