@@ -30,6 +30,24 @@ struct DCol {
   int32_t scale;
 };
 
+// Read-only loads that ask L2 to keep their lines (evict-last) while streamed
+// data passes through: for small tables probed once per streamed row.
+__device__ __forceinline__ uint64_t l2_keep_policy() {
+  uint64_t pol;
+  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+__device__ __forceinline__ uint32_t ld_keep_u32(const uint32_t* p) {
+  uint32_t v;
+  asm("ld.global.nc.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(l2_keep_policy()));
+  return v;
+}
+__device__ __forceinline__ unsigned long long ld_keep_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm("ld.global.nc.L2::cache_hint.u64 %0, [%1], %2;" : "=l"(v) : "l"(p), "l"(l2_keep_policy()));
+  return v;
+}
+
 __device__ __forceinline__ bool is_null(const DCol& c, int64_t i) {
   return c.valid != nullptr && ((__ldg(&c.valid[i >> 6]) >> (i & 63)) & 1ULL) == 0;
 }

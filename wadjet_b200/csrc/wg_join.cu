@@ -418,6 +418,7 @@ static wg_status join_view_fields(wg_join* j, wgd::JoinView* v) {
   v->direct = 0;
   v->sentinel = 0;
   v->dense = 0;
+  v->l2keep = 0;
   v->base = 0;
   for (size_t i = 0; i < j->pay.size() && i < WG_MAX_PAYLOAD; ++i)
     v->pay[i] = wgd::DCol{j->pay[i].data.get(), j->pay[i].has_valid ? j->pay[i].valid.as<uint64_t>() : nullptr,
@@ -440,6 +441,8 @@ wg_status join_view_fused(wg_join* j, wgd::JoinView* v) {
     v->sentinel = j->sentinel;
     if (j->dense) {
       v->dense = 1;
+      const char* keep = std::getenv("WG_JOIN_L2_KEEP");
+      v->l2keep = !keep || std::atoi(keep) != 0;
       v->base = j->dense_base;
       v->mask = (uint64_t)j->dense_slots;
       if (j->full) {

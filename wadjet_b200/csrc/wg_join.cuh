@@ -40,6 +40,7 @@ struct JoinView {
   // key of the range is present, so `slots` is just the 4-byte payloads
   // (payload of key base+i at i) and a key in range always matches.
   int32_t dense;
+  int32_t l2keep;          // dense probes ask L2 to keep the table's lines (evict-last)
   long long base;
   DCol pay[WG_MAX_PAYLOAD];
 };
@@ -82,10 +83,12 @@ __device__ __forceinline__ bool join_direct_i32(const JoinView& j, int32_t key, 
   const uint32_t i = (uint32_t)key - (uint32_t)j.base;
   if (i >= (uint32_t)j.mask) return false;  // mask = key span <= 2^30
   if (j.dense == 2) {
-    out = (int32_t)__ldg((const uint32_t*)j.slots + i);
+    const uint32_t* p = (const uint32_t*)j.slots + i;
+    out = (int32_t)(j.l2keep ? ld_keep_u32(p) : __ldg(p));
     return true;
   }
-  const unsigned long long v = __ldg((const unsigned long long*)j.slots + i);
+  const unsigned long long* q = (const unsigned long long*)j.slots + i;
+  const unsigned long long v = j.l2keep ? ld_keep_u64(q) : __ldg(q);
   if ((uint32_t)v != (uint32_t)key) return false;
   out = (int32_t)(v >> 32);
   return true;
