@@ -43,9 +43,9 @@ DIM_BYTES_PER_ROW = 4 + 4                # key, grp
 GROUP_STATE_BYTES = 8 + 8 + 16 + 8       # key, rows, SUM f64, SUM Int128
 CPU_SAMPLE_ROWS = 1 << 24
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one fused-kernel launch per fact row,
-# from an ncu capture of the 2^24-row case (598.4 MB / 2^24 rows), scaled by the rows of a launch:
+# from an ncu capture of the 2^24-row case (558.2 MB / 2^24 rows), scaled by the rows of a launch:
 # profiles/pipeline_vec_kernel_starjoin_2p24.md
-NCU_TRAFFIC_BYTES_PER_FACT_ROW = 598.38e6 / (1 << 24)
+NCU_TRAFFIC_BYTES_PER_FACT_ROW = 558.24e6 / (1 << 24)
 METRIC = "rows/s (filter+join+hash-agg, star join 2^28 fact rows)"
 STARJOIN_WORKLOAD = ("star join + aggregate: 2^28 fact rows x 2^22 dim rows, qty>10, GROUP BY grp (1000 groups), "
                      "SUM(price*(1-disc)) f64 + SUM(price) Int128")
