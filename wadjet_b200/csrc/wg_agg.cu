@@ -1426,6 +1426,16 @@ wg_status agg_run_device(wg_agg* a, const wg_batch_desc* in, int32_t nf, const w
   return run_device(r);
 }
 Ctx* agg_ctx(wg_agg* a) { return a->ctx; }
+// Frees what an aggregate keeps only to speed up its next query (the
+// reordered input copy and its counters), for an aggregate parked in a pool.
+void agg_trim(wg_agg* a) {
+  if (a->part_bufs.empty() && !a->part_counts.get()) return;
+  ensure_device(a->ctx);
+  cudaStreamSynchronize(a->ctx->stream);  // no launch still reads them
+  a->part_bufs.clear();
+  a->part_counts.reset();
+  a->part_offs.reset();
+}
 std::vector<int32_t> agg_input_cols(wg_agg* a) {
   std::vector<int32_t> r = a->key_cols;
   for (const wg_agg_spec& s : a->specs) r.push_back(s.input_col);

@@ -23,6 +23,10 @@
 
 using namespace wg;
 
+namespace wg {
+void agg_trim(wg_agg* a);  // wg_agg.cu
+}  // namespace wg
+
 namespace {
 
 double now_s() {
@@ -300,6 +304,7 @@ wg_status wg_server_release(wg_server* s, int64_t ticket) {
     // keep enough finished aggregates that a slot rarely has to allocate a new
     // one while the previous result of the same shape is still held
     if (r->agg && r->status == WG_OK && s->pool.size() < 16 * s->slots.size()) {
+      agg_trim(r->agg);  // a parked aggregate keeps its table, not its reorder copy
       s->pool.push_back(Pooled{r->agg, r->slot, r->keys, r->aggs, r->hint});
       r->agg = nullptr;
     }
