@@ -1146,6 +1146,7 @@ static wg_status run_partitioned(const PipelineRun& r, const wgd::Plan& P0, cons
     po.data[j] = bufs[(size_t)j].as<char>();
     po.es[j] = es;
   }
+  cudaFuncSetAttribute(wgd::part_scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wgd::part_scatter_smem(np));
   wgd::part_scatter_kernel<<<grid, wgd::kPartThreads, wgd::part_scatter_smem(np), ctx->stream>>>(P, pbits, 64 - pbits,
                                                                         offs.as<unsigned long long>(), po);
   ctx->count_launch();
@@ -1276,6 +1277,7 @@ static wg_status spill_consume(const PipelineRun& r, const wgd::Plan& P0, const 
       po.data[j] = a->sp_dev[(size_t)j].as<char>();
       po.es[j] = a->sp_es[(size_t)j];
     }
+    cudaFuncSetAttribute(wgd::part_scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wgd::part_scatter_smem(np));
     wgd::part_scatter_kernel<<<grid, wgd::kPartThreads, wgd::part_scatter_smem(np), ctx->stream>>>(P, pbits, kSpillPartShift,
                                                                           offs.as<unsigned long long>(), po);
     ctx->count_launch();

@@ -902,7 +902,7 @@ __device__ __forceinline__ uint32_t row_partition(const Plan& P, const Sh& sh, i
 // taking tiles c, c + gridDim.x, ...; so the rows a CTA counts per partition
 // are exactly the rows it later scatters there.
 constexpr int kPartThreads = 512;
-constexpr int kPartTile = 4096;
+constexpr int kPartTile = 16384;
 static_assert(kPartTile <= 65536, "tile-local row indices are 16-bit");
 __host__ __device__ constexpr size_t part_count_smem(int np) { return (size_t)np * 4; }
 __host__ __device__ constexpr size_t part_scatter_smem(int np) {
