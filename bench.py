@@ -13,14 +13,16 @@ One step = the whole query: build the join index from the dimension, run the
 fused filter → probe → project → aggregate pass over every fact row, finalize
 (compact the groups) and read the group count back. `value` is fact rows per
 second with the inputs resident in HBM; `e2e` is the same query through the
-public API from pinned host buffers (host→device copies and the result read
-inside the timed region). Inputs (8.6 GB per rank) are far larger than the
-126 MB L2, so no flush is needed between steps.
+public API from ordinary (pageable) host buffers, as a cgo caller hands over
+Go slices, with the host→device copies and the result read inside the timed
+region (`e2e_pinned`: the same from pinned buffers). Inputs (8.6 GB per rank)
+are far larger than the 126 MB L2, so no flush is needed between steps.
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 For N > 1 launch with torchrun (one rank per GPU); ranks process disjoint fact
-shards (weak scaling) and the per-group partial states are combined on rank 0
-after an all-gather.
+shards (weak scaling); inside each step the partial groups are hash-partitioned
+by owner rank on the device and exchanged with an NCCL all-to-all
+(wadjet_b200.exchange.exchange_aggregate), and each rank finishes its key range.
 """
 from __future__ import annotations
 
@@ -41,7 +43,7 @@ GROUPS = 1000
 FACT_BYTES_PER_ROW = 4 + 4 + 16 + 8      # fk, qty, price (Int128), disc
 DIM_BYTES_PER_ROW = 4 + 4                # key, grp
 GROUP_STATE_BYTES = 8 + 8 + 16 + 8       # key, rows, SUM f64, SUM Int128
-CPU_SAMPLE_ROWS = 1 << 24
+CPU_SAMPLE_ROWS = 1 << 24   # the group-by / high-cardinality CPU baselines
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one fused-kernel launch per fact row,
 # from an ncu capture of the 2^24-row case (558.2 MB / 2^24 rows), scaled by the rows of a launch:
 # profiles/pipeline_vec_kernel_starjoin_2p24.md
@@ -59,6 +61,8 @@ def parse_args():
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--rows", type=int, default=FACT_ROWS)
     p.add_argument("--e2e-steps", type=int, default=3)
+    p.add_argument("--ref-rows", type=int, default=FACT_ROWS,
+                   help="fact rows per reference (CPU) step; the default is the whole workload")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--workload", choices=["starjoin", "groupby", "highcard", "highcard_spill", "batched", "serving"],
                    default="starjoin", help="starjoin is the headline; the others print their own lines")
@@ -138,31 +142,6 @@ class ClockSampler:
 
 
 # -------------------------------------------------------------- reference --
-def cpu_pipeline_sample(rows: int, threads: int, repeats: int = 1):
-    """The oracle's Pipeline.Run (the reference algorithm restated in C++) on a
-    host-resident sample of the same workload; returns rows/s of the best repeat."""
-    import numpy as np
-    from oracle import binding as ob
-    fk, qty, price, disc = ob.gen_starjoin_fact(rows, threads=threads)
-    key, grp = ob.gen_starjoin_dim(DIM_ROWS)
-    build = ob.HostBatch([(1, key, None, 0), (1, grp, None, 0)])
-    batch = ob.HostBatch([(1, fk, None, 0), (1, qty, None, 0), (17, price, None, 2), (4, disc, None, 0)])
-    expr = ob.expr(4, [("col", 2), ("cf", 1.0), ("col", 3), "-", "*"])
-    best = None
-    for _ in range(repeats):
-        t0 = time.perf_counter()
-        j = ob.Join(DIM_ROWS)
-        j.append(1, key)
-        agg = ob.Agg([4], [(0, 5, 0), (0, 2, 0)])
-        ob.pipeline(batch, agg, filters=[(1, 4, 10)], join=j, probe_key=0, build=build, payload=[1], exprs=[expr],
-                    threads=threads)
-        groups = agg.groups()
-        dt = time.perf_counter() - t0
-        assert groups == GROUPS, groups
-        best = dt if best is None else min(best, dt)
-    return rows / best, best
-
-
 def cpu_groupby_sample(rows: int, threads: int) -> float:
     """rows/s of the oracle's Pipeline.Run on the group-by workload (host-resident sample)."""
     from oracle import binding as ob
@@ -185,27 +164,62 @@ def cpu_highcard_sample(rows: int, threads: int) -> float:
     return rows / (time.perf_counter() - t0)
 
 
+class CpuStarJoin:
+    """The reference algorithm (the oracle's C++ restatement of Pipeline.Run: chained hash-join
+    build, filter, probe, projection and hash aggregate, one worker per host thread) over a
+    host-resident copy of the star-join workload. One step is the same unit of work as a GPU
+    step: build the join from the 2^22-row dimension, then every fact row."""
+
+    def __init__(self, rows: int, threads: int):
+        from oracle import binding as ob
+        self.ob, self.rows, self.threads = ob, rows, threads
+        self.fact = ob.gen_starjoin_fact(rows, threads=threads)
+        self.dim = ob.gen_starjoin_dim(DIM_ROWS)
+        fk, qty, price, disc = self.fact
+        key, grp = self.dim
+        self.build = ob.HostBatch([(1, key, None, 0), (1, grp, None, 0)])
+        self.batch = ob.HostBatch([(1, fk, None, 0), (1, qty, None, 0), (17, price, None, 2), (4, disc, None, 0)])
+        self.expr = ob.expr(4, [("col", 2), ("cf", 1.0), ("col", 3), "-", "*"])
+
+    def step(self) -> float:
+        ob = self.ob
+        t0 = time.perf_counter()
+        j = ob.Join(DIM_ROWS)
+        j.append(1, self.dim[0])
+        agg = ob.Agg([4], [(0, 5, 0), (0, 2, 0)])
+        ob.pipeline(self.batch, agg, filters=[(1, 4, 10)], join=j, probe_key=0, build=self.build, payload=[1],
+                    exprs=[self.expr], threads=self.threads)
+        groups = agg.groups()
+        dt = time.perf_counter() - t0
+        assert groups == GROUPS, groups
+        return dt
+
+
 def run_reference(args, rank: int):
     if rank != 0:
         return
     threads = os.cpu_count() or 1
+    rows = args.ref_rows
+    cpu = CpuStarJoin(rows, threads)
     times = []
     for i in range(args.warmup + args.steps):
-        rps, dt = cpu_pipeline_sample(CPU_SAMPLE_ROWS, threads)
+        dt = cpu.step()
         if i >= args.warmup:
             times.append(dt)
     total = sum(times)
-    value = CPU_SAMPLE_ROWS * len(times) / total
+    value = rows * len(times) / total
+    sample = (f"the whole workload per step ({rows} fact rows, join build included)" if rows == FACT_ROWS else
+              f"{rows} fact rows per step of the 2^28-row workload, join build included")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int128+f64", "data": "synthetic",
         "config": {"workload": STARJOIN_WORKLOAD, "fact_rows_per_gpu": FACT_ROWS, "dim_rows": DIM_ROWS,
-                   "groups": GROUPS, "sample_fact_rows_per_step": CPU_SAMPLE_ROWS,
+                   "groups": GROUPS, "fact_rows_per_step": rows, "same_config": rows == FACT_ROWS,
                    "parallelism": f"{threads} host threads"},
         "cpu_baseline": {"value": value, "unit": "rows/s", "cores": threads, "kind": "port",
-                         "sample": f"{CPU_SAMPLE_ROWS} fact rows per step (of the 2^28-row workload), "
-                                   "C++ restatement of the reference's Pipeline.Run (Go toolchain absent)"},
+                         "sample": sample + "; C++ restatement of the reference's Pipeline.Run "
+                                            "(the Go toolchain is absent)"},
         "e2e": {"value": value, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -255,24 +269,20 @@ def run_ours(args, rank: int, world: int, local_rank: int):
             kev[1].record(stream)
         return agg.finalize()
 
-    def combine_partials():
-        """Per-group partial states of every rank, merged on rank 0 (the exchange step)."""
-        e = agg.export()
-        part = {"keys": e["keys"][0], "count": e["count"][0], "f64": e["f64"][0],
-                "hi": e["dec"][1]["hi"], "lo": e["dec"][1]["lo"]}
+    owner = wg.HashAggregate(ctx, [4], [wg.AggColumn(wg.AGG_SUM, 5), wg.AggColumn(wg.AGG_SUM, 2)],
+                             ndv_hint=GROUPS) if dist is not None else None
+
+    def combine_partials() -> int:
+        """The exchange step (N > 1): this rank's partial groups hash-partitioned by owner on the
+        device, exchanged with an NCCL all-to-all, merged by their owners; returns all groups."""
         if dist is None:
-            return part
-        parts = [None] * world
-        dist.all_gather_object(parts, part)
-        if rank != 0:
-            return None
-        acc = {}
-        for p in parts:
-            for i, k in enumerate(p["keys"].tolist()):
-                v = (int(p["hi"][i]) << 64) | int(p["lo"][i])
-                a = acc.setdefault(k, [0, 0.0, 0])
-                a[0] += int(p["count"][i]); a[1] += float(p["f64"][i]); a[2] += v
-        return acc
+            return GROUPS
+        from wadjet_b200.exchange import exchange_aggregate
+        owner.reset()
+        exchange_aggregate(dist, agg, owner)
+        t = torch.tensor([owner.finalize()], dtype=torch.int64, device="cuda")
+        dist.all_reduce(t)
+        return int(t.item())
 
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
 
@@ -305,7 +315,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         assert g == GROUPS, g
         torch.cuda.synchronize()
         kernel_ms.append(kev[0].elapsed_time(kev[1]))
-        combine_partials()
+        assert combine_partials() == GROUPS
 
     for _ in range(args.warmup):
         dev_step()
@@ -316,37 +326,46 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     ms_step = ms_total / args.steps
     value = world * n / (ms_step / 1e3)
 
-    # ---- end to end from pinned host buffers ------------------------------
-    e2e = None
+    # ---- end to end from host buffers (pageable, then pinned) ---------------
+    e2e = e2e_pinned = None
     if args.e2e_steps > 0:
-        h = [t.cpu().pin_memory() for t in (fk, qty, price, disc, key, grp)]
-        fact_host = wg.Batch([wg.Column(I32, h[0].numpy()), wg.Column(I32, h[1].numpy()),
-                              wg.Column(DEC, h[2].numpy().reshape(-1).view(wg.DEC_DTYPE), scale=2),
-                              wg.Column(F64, h[3].numpy())])
-        dim_host = wg.Batch([wg.Column(I32, h[4].numpy()), wg.Column(I32, h[5].numpy())])
-        d2h = [0]
+        def e2e_run(pinned: bool):
+            h = [t.cpu() for t in (fk, qty, price, disc, key, grp)]
+            if pinned:
+                h = [t.pin_memory() for t in h]
+            fact_host = wg.Batch([wg.Column(I32, h[0].numpy()), wg.Column(I32, h[1].numpy()),
+                                  wg.Column(DEC, h[2].numpy().reshape(-1).view(wg.DEC_DTYPE), scale=2),
+                                  wg.Column(F64, h[3].numpy())])
+            dim_host = wg.Batch([wg.Column(I32, h[4].numpy()), wg.Column(I32, h[5].numpy())])
+            d2h = [0]
 
-        def e2e_step():
-            g = step(fact_host, dim_host, False)
-            rows = agg.collect()
-            d2h[0] = sum(v.nbytes + len(ok) for v, ok in rows)
-            assert g == GROUPS
-            combine_partials()
+            def e2e_step():
+                g = step(fact_host, dim_host, False)
+                rows = agg.collect()
+                d2h[0] = sum(v.nbytes + len(ok) for v, ok in rows)
+                assert g == GROUPS
+                assert combine_partials() == GROUPS
 
-        e2e_ms, _ = timed(e2e_step, args.e2e_steps, 1)
-        e2e = {"value": world * n / (e2e_ms / args.e2e_steps / 1e3), "unit": "rows/s",
-               "h2d_bytes_per_step": n * FACT_BYTES_PER_ROW + DIM_ROWS * DIM_BYTES_PER_ROW,
-               "d2h_bytes_per_step": d2h[0]}
-        del h
+            e2e_ms, _ = timed(e2e_step, args.e2e_steps, 1)
+            return {"value": world * n / (e2e_ms / args.e2e_steps / 1e3), "unit": "rows/s",
+                    "h2d_bytes_per_step": n * FACT_BYTES_PER_ROW + DIM_ROWS * DIM_BYTES_PER_ROW,
+                    "d2h_bytes_per_step": d2h[0],
+                    "host_memory": "pinned" if pinned else "pageable (as a cgo caller passes Go slices)"}
+
+        e2e = e2e_run(False)
+        e2e_pinned = e2e_run(True)
 
     # ---- CPU baseline (rank 0, N = 1) ---------------------------------------
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        rps, _ = cpu_pipeline_sample(CPU_SAMPLE_ROWS, threads, repeats=2)
-        cpu = {"value": rps, "unit": "rows/s", "cores": threads, "kind": "port",
-               "sample": f"{CPU_SAMPLE_ROWS} fact rows of the same workload (best of 2), C++ restatement of "
-                         "the reference's Pipeline.Run with one worker per host thread"}
+        ref_rows = min(args.ref_rows, n)
+        c = CpuStarJoin(ref_rows, threads)
+        dt = min(c.step() for _ in range(2))
+        del c
+        cpu = {"value": ref_rows / dt, "unit": "rows/s", "cores": threads, "kind": "port",
+               "sample": f"{ref_rows} fact rows per step (the whole workload, join build included; best of 2), "
+                         "C++ restatement of the reference's Pipeline.Run with one worker per host thread"}
 
     if rank == 0:
         peak, peak_kind = measured_peak_hbm()
@@ -369,6 +388,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                          "peak_kind": peak_kind},
             "cpu_baseline": cpu,
             "e2e": e2e,
+            "e2e_pinned": e2e_pinned,
             "gpu_launches": launches,
             "gpu_launches_per_step": launches / args.steps,
             "clocks": clk,
@@ -376,6 +396,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         print(json.dumps(line), flush=True)
     join.close()
     agg.close()
+    if owner is not None:
+        owner.close()
     ctx.close()
     if dist is not None:
         dist.barrier()

@@ -5,9 +5,9 @@
  *
  * Every entry point is plain C: opaque handles, raw pointers and sizes, an int
  * status. A Go cgo wrapper implements exec.UnaryOperator / exec.Sink /
- * exec.MergeableSink on top of these calls (the binding is shown in
- * INTEGRATION.md). The reference interface each function replaces is cited
- * beside it as path:line within the Wadjet source tree.
+ * exec.MergeableSink on top of these calls. The reference interface each
+ * function replaces is cited beside it as path:line within the Wadjet source
+ * tree.
  *
  * Conventions
  *  - Status: 0 = WG_OK; WG_E_NOMEM maps to memory.ErrMemoryExceeded
@@ -47,6 +47,7 @@ typedef int32_t wg_status;
 #define WG_E_CUDA         4  /* a CUDA runtime call failed                                   */
 #define WG_E_UNSUPPORTED  5  /* shape the GPU path does not cover (e.g. string keys)          */
 #define WG_E_STATE        6  /* call out of order (consume after finalize, ...)               */
+#define WG_E_CANCELLED    7  /* a queued serving request was cancelled (context.Canceled)      */
 
 /* ---- type ids: values of parquet.TypeID (internal/storage/parquet/schema.go:13-34) ---- */
 #define WG_TYPE_BOOL       0
@@ -340,6 +341,34 @@ WG_API wg_status wg_agg_emit(wg_agg* a, int64_t start, int64_t max_rows,
 WG_API wg_status wg_agg_export(wg_agg* a, const wg_group_export* out);
 /* Forget all groups and input (the state after wg_agg_create). */
 WG_API wg_status wg_agg_reset(wg_agg* a);
+/* ---- exchange of partial state between ranks (one process per GPU) ----
+ * The multi-GPU GROUP BY pre-aggregates each rank's shard, then hash-partitions
+ * the partial groups by owner rank and exchanges them (an NCCL all-to-all into
+ * each rank's HBM) so every rank finishes a disjoint key range: the device form
+ * of partitionFor (internal/engine/exec/partitioned_agg.go:221) and the
+ * distributed shuffle (internal/worker/partitioned_shuffle_sink.go:1039).
+ * A state row is (1 + slot_words) uint64 words: a flag (0 a regular key, 1 the
+ * key equal to the table's empty pattern, 2 the NULL key) and the group's slot. */
+typedef struct wg_state_layout {
+  int32_t key_words, slot_words, n_keys, n_aggs;
+  int32_t key_type[4];                        /* parquet.TypeID of each group column */
+  int32_t key_i32[4], key_word[4], key_shift[4];  /* packed-key placement (buildPackedLayout) */
+  int32_t agg_kind[8], agg_off[8], agg_null_off[8];
+  int32_t agg_in_cls[8], agg_in_scale[8], agg_out_type[8], agg_nullable[8];
+} wg_state_layout;
+/* The row layout of a's state (a must have consumed or merged something). */
+WG_API wg_status wg_agg_state_layout(wg_agg* a, wg_state_layout* out);
+/* After finalize: every group's state row into rows_dev (device, rows_cap rows of
+ * 1 + slot_words words), grouped by owner = hi64(route_hash * n_parts) where
+ * route_hash is fibHash(key) / packedHash(lo, hi) / routeNullHash as partitionFor's
+ * router computes it (partitioned_agg.go:508-535); part_rows[p] (host) = rows of owner p,
+ * stored from row sum(part_rows[0..p)) on. */
+WG_API wg_status wg_agg_partition_state(wg_agg* a, int32_t n_parts, void* rows_dev, int64_t rows_cap,
+                                        int64_t* part_rows);
+/* MergeSink (aggregate.go:4682) of n_rows state rows (device) laid out as *src into a,
+ * which must not be finalized; an aggregate that has consumed nothing adopts the
+ * source's schema. */
+WG_API wg_status wg_agg_merge_state(wg_agg* a, const wg_state_layout* src, const void* rows_dev, int64_t n_rows);
 /* Diagnostic, no counterpart in the reference: the compiled query shape the
  * last fused launch into `a` ran on (1..6: a kernel built for exactly that
  * query shape; 0: the generic kernel; -1: no fused launch yet). Results never
@@ -432,7 +461,7 @@ typedef struct wg_serve_request {
 } wg_serve_request;
 
 typedef struct wg_serve_stats {
-  int64_t submitted, completed, failed, in_flight, queued;
+  int64_t submitted, completed, failed, in_flight, queued, cancelled;
   double  p50_s, p99_s, mean_s, max_s;   /* latency = completion - submission */
   double  qps;                           /* completed / (last completion - first submission) */
   double  mean_queue_s;                  /* mean time from submission to a slot starting the request */
@@ -447,6 +476,12 @@ WG_API wg_status wg_server_wait(wg_server* s, int64_t ticket, double timeout_s, 
 WG_API wg_status wg_server_export(wg_server* s, int64_t ticket, const wg_group_export* out);
 /* Free a finished request's result and its HBM. */
 WG_API wg_status wg_server_release(wg_server* s, int64_t ticket);
+/* Cancel a request that is still queued (the caller's context was cancelled,
+ * as a gRPC handler sees ctx.Done(), internal/server/grpc.go:120): it leaves the
+ * queue without touching the device and its wait returns WG_E_CANCELLED.
+ * A request a slot has already started runs to completion (WG_E_STATE); the
+ * caller then releases it as usual. The ticket stays valid until released. */
+WG_API wg_status wg_server_cancel(wg_server* s, int64_t ticket);
 WG_API wg_status wg_server_stats(wg_server* s, wg_serve_stats* out);
 /* Forget latency statistics (e.g. after a warm-up). */
 WG_API wg_status wg_server_reset_stats(wg_server* s);

@@ -1,7 +1,10 @@
 """The multi-rank path on CPU: two gloo ranks each aggregate a shard of the star
-join, all-gather their per-group partial states and merge them; the merged
-table must equal one aggregate over the whole table (partitioned_agg_test.go:91
-'parallel = serial', with ranks in place of workers)."""
+join, route their partial groups to owner ranks by the key's route hash
+(partitionFor, partitioned_agg.go:221), exchange them with the same all-to-all
+protocol the device path uses (exchange.exchange_rows) and merge what they own.
+The union of the owned groups must equal one aggregate over the whole table
+(partitioned_agg_test.go:91 'parallel = serial', with ranks in place of
+workers), and every rank must own exactly the groups the route hash gives it."""
 import os
 import socket
 
@@ -41,16 +44,22 @@ def _rank_main(rank: int, world: int, port: int, out_path: str):
     import sys
     sys.path.insert(0, ROOT)
     import torch.distributed as dist
-    from wadjet_b200.exchange import merge_exports, shard_range
+    import datetime
+    from wadjet_b200.exchange import exchange_export, merge_exports, partition_for, route_hash_int, shard_range
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
-    dist.init_process_group("gloo", rank=rank, world_size=world)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
     row0, n = shard_range(N_ROWS, rank, world)
     part = _oracle_starjoin(row0, n)
+    owned = exchange_export(dist, part, KINDS)
+    # every group this rank finished is one the route hash assigns to it
+    assert (partition_for(route_hash_int(owned["keys"][0]), world) == rank).all()
     parts = [None] * world
-    dist.all_gather_object(parts, part)
+    dist.all_gather_object(parts, owned)
     if rank == 0:
+        # owned key ranges are disjoint, so concatenating them is the whole result
         merged = merge_exports(parts, KINDS)
+        assert merged["keys"].shape[1] == sum(p["keys"].shape[1] for p in parts)
         np.savez(out_path, **{k: merged[k] for k in ("keys", "key_valid", "count", "i64", "f64", "has")},
                  dec_hi=merged["dec"]["hi"], dec_lo=merged["dec"]["lo"])
     dist.barrier()
@@ -103,3 +112,17 @@ def test_merge_exports_decimal_and_wrapping(kind):
     else:
         d = m["dec"][0][keys.index(1)]
         assert (int(d["hi"]), int(d["lo"])) == ((-1, 2**64 - 5) if kind == "min_d" else (0, 4))
+
+
+def test_partition_for_matches_multiply_shift():
+    """partitionFor is hi64(hash * parts): the numpy form equals exact integer arithmetic."""
+    from wadjet_b200.exchange import partition_for, route_hash_int
+    rng = np.random.default_rng(3)
+    keys = rng.integers(-2**63, 2**63 - 1, 10000, dtype=np.int64)
+    h = route_hash_int(keys)
+    for parts in (1, 2, 3, 7, 8, 96):
+        want = [(int(x) * parts) >> 64 for x in h.tolist()]
+        np.testing.assert_array_equal(partition_for(h, parts), want)
+        assert ((partition_for(h, parts) >= 0) & (partition_for(h, parts) < parts)).all()
+    # fibHash is the multiply by the golden-ratio constant mod 2^64
+    assert int(route_hash_int(np.array([3]))[0]) == (3 * 11400714819323198485) % 2**64

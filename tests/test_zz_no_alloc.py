@@ -73,3 +73,40 @@ def test_noalloc_rejects_inputs_over_the_limit(ctx):
                                                  data.data_ptr(), C.byref(n))
     assert st == over
     assert b"limit" in wg.lib.wg_last_error()
+
+
+def test_noalloc_rejects_more_items_than_the_column_holds(ctx):
+    # without a selection vector the items are the column's rows; a larger count
+    # would read past the column, so the call refuses it before any launch
+    import wadjet_b200 as wg
+    import torch
+    data = torch.zeros(1000, dtype=torch.int32, device="cuda")
+    out = torch.empty(2000, dtype=torch.int32, device="cuda")
+    col = wg._abi.wg_column(1, 0, data.data_ptr(), None, 1000)
+    n = C.c_int64(-1)
+    st = wg.lib.wg_filter_execute_device_noalloc(ctx.stream, C.byref(col), None, 1001, wg.OP_EQ, 0, 0, 0.0,
+                                                 out.data_ptr(), C.byref(n))
+    assert st == wg._abi.WG_E_INVALID
+    assert b"column length" in wg.lib.wg_last_error()
+
+
+def test_noalloc_timeout_then_clean_call(ctx, monkeypatch):
+    # an expired look-back wait leaves its mark in the shared scratch's error word;
+    # the next call must clear it and return the regular entry point's selection
+    import torch
+    import wadjet_b200 as wg
+    rng = np.random.default_rng(11)
+    host = rng.integers(0, 1000, 1 << 22).astype(np.int32)
+    data = torch.from_numpy(host).cuda()
+    monkeypatch.setenv("WG_FILTER_SPIN_LIMIT", "0")
+    kind_i = int(500)
+    col = wg._abi.wg_column(1, 0, data.data_ptr(), None, int(data.shape[0]))
+    out = torch.empty(int(data.shape[0]), dtype=torch.int32, device="cuda")
+    n = C.c_int64(-1)
+    st = wg.lib.wg_filter_execute_device_noalloc(ctx.stream, C.byref(col), None, int(data.shape[0]), wg.OP_LT, 0,
+                                                 kind_i, 0.0, out.data_ptr(), C.byref(n))
+    assert st == wg._abi.WG_E_TIMEOUT
+    monkeypatch.delenv("WG_FILTER_SPIN_LIMIT")
+    want = _regular(wg, ctx, 1, data, None, None, wg.OP_LT, 500)
+    got = _noalloc(wg, ctx.stream, 1, data, None, None, wg.OP_LT, 500)
+    np.testing.assert_array_equal(got, want)

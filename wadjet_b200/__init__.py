@@ -31,7 +31,7 @@ from ._abi import (AGG_AVG, AGG_COUNT, AGG_MAX, AGG_MIN, AGG_SUM, CONST_FLOAT, C
 
 __all__ = [
     "Context", "Column", "Batch", "KernelFilter", "HashJoin", "HashAggregate", "AggColumn", "Expr", "run_pipeline",
-    "WadjetGPUError", "MemoryExceeded", "DEC_DTYPE", "lib",
+    "WadjetGPUError", "MemoryExceeded", "Cancelled", "DEC_DTYPE", "lib",
 ]
 
 DEC_DTYPE = np.dtype([("hi", "<i8"), ("lo", "<u8")])
@@ -64,11 +64,17 @@ class MemoryExceeded(WadjetGPUError):
     """memory.ErrMemoryExceeded (internal/engine/memory/tracker.go:15)."""
 
 
+class Cancelled(WadjetGPUError):
+    """A queued serving request was withdrawn (context.Canceled)."""
+
+
 def _check(status: int) -> None:
     if status != abi.WG_OK:
         msg = (lib.wg_last_error() or b"").decode()
         if status == abi.WG_E_NOMEM:
             raise MemoryExceeded(status, msg)
+        if status == abi.WG_E_CANCELLED:
+            raise Cancelled(status, msg)
         raise WadjetGPUError(status, msg)
 
 
@@ -149,6 +155,7 @@ class Context:
         h = C.c_void_p()
         _check(lib.wg_ctx_create(device, hbm_budget, pinned_spill, C.byref(h)))
         self.h = h
+        self.device = device
 
     def close(self) -> None:
         if self.h:
@@ -343,6 +350,31 @@ class HashAggregate:
         self._out_pos = 0
 
     @property
+    def state_layout(self) -> "abi.wg_state_layout":
+        """The row layout of this aggregate's partial state (wg_agg_state_layout)."""
+        lay = abi.wg_state_layout()
+        _check(lib.wg_agg_state_layout(self.h, C.byref(lay)))
+        return lay
+
+    def partition_state(self, n_parts: int):
+        """After finalize: every group's state row on the device, grouped by owner rank
+        (partitionFor over the key's route hash). Returns (rows, part_rows): rows is a
+        uint64 CUDA tensor of shape (groups, 1 + slot_words), part_rows the rows per owner."""
+        import torch
+        n = self.finalize()
+        lay = self.state_layout() if n else None
+        width = 1 + (lay.slot_words if lay is not None else 0)
+        rows = torch.empty((max(n, 1), max(width, 1)), dtype=torch.int64, device=f"cuda:{self.ctx.device}")
+        counts = (C.c_int64 * n_parts)()
+        _check(lib.wg_agg_partition_state(self.h, n_parts, rows.data_ptr(), n, counts))
+        return rows[:n], [int(c) for c in counts]
+
+    def merge_state(self, layout: "abi.wg_state_layout", rows) -> None:
+        """MergeSink of state rows (a CUDA tensor of shape (n, 1 + slot_words)) laid out as `layout`."""
+        n = int(rows.shape[0]) if rows is not None else 0
+        ptr = rows.data_ptr() if n else None
+        _check(lib.wg_agg_merge_state(self.h, C.byref(layout), ptr, n))
+
     def kernel_shape(self) -> int:
         """Compiled query shape of the last fused launch (0 generic, -1 none yet); a diagnostic only."""
         return int(lib.wg_agg_kernel_shape(self.h))
@@ -570,6 +602,10 @@ class Server:
     def release(self, ticket: int) -> None:
         _check(lib.wg_server_release(self.h, ticket))
         self._shapes.pop(ticket, None)
+
+    def cancel(self, ticket: int) -> None:
+        """Withdraw a request that is still queued; its wait() then raises Cancelled."""
+        _check(lib.wg_server_cancel(self.h, ticket))
 
     def stats(self) -> dict:
         s = abi.wg_serve_stats()

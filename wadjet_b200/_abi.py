@@ -8,7 +8,7 @@ _PKG = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_PKG, "libwadjetgpu.so")
 
 # status codes
-WG_OK, WG_E_NOMEM, WG_E_INVALID, WG_E_TIMEOUT, WG_E_CUDA, WG_E_UNSUPPORTED, WG_E_STATE = range(7)
+WG_OK, WG_E_NOMEM, WG_E_INVALID, WG_E_TIMEOUT, WG_E_CUDA, WG_E_UNSUPPORTED, WG_E_STATE, WG_E_CANCELLED = range(8)
 
 # parquet.TypeID values (internal/storage/parquet/schema.go:13-34)
 TYPE_BOOL, TYPE_INT32, TYPE_INT64, TYPE_FLOAT32, TYPE_FLOAT64 = 0, 1, 2, 3, 4
@@ -79,6 +79,14 @@ class wg_tune_params(C.Structure):
                 ("smem_max_groups", C.c_int32), ("max_load", C.c_double)]
 
 
+class wg_state_layout(C.Structure):
+    _fields_ = [("key_words", C.c_int32), ("slot_words", C.c_int32), ("n_keys", C.c_int32), ("n_aggs", C.c_int32),
+                ("key_type", C.c_int32 * 4), ("key_i32", C.c_int32 * 4), ("key_word", C.c_int32 * 4),
+                ("key_shift", C.c_int32 * 4), ("agg_kind", C.c_int32 * 8), ("agg_off", C.c_int32 * 8),
+                ("agg_null_off", C.c_int32 * 8), ("agg_in_cls", C.c_int32 * 8), ("agg_in_scale", C.c_int32 * 8),
+                ("agg_out_type", C.c_int32 * 8), ("agg_nullable", C.c_int32 * 8)]
+
+
 class wg_serve_request(C.Structure):
     _fields_ = [("plan", C.POINTER(wg_pipeline_desc)), ("key_cols", C.POINTER(C.c_int32)),
                 ("aggs", C.POINTER(wg_agg_spec)), ("n_keys", C.c_int32), ("n_aggs", C.c_int32),
@@ -87,7 +95,8 @@ class wg_serve_request(C.Structure):
 
 class wg_serve_stats(C.Structure):
     _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("failed", C.c_int64),
-                ("in_flight", C.c_int64), ("queued", C.c_int64), ("p50_s", C.c_double), ("p99_s", C.c_double),
+                ("in_flight", C.c_int64), ("queued", C.c_int64), ("cancelled", C.c_int64),
+                ("p50_s", C.c_double), ("p99_s", C.c_double),
                 ("mean_s", C.c_double), ("max_s", C.c_double), ("qps", C.c_double),
                 ("mean_queue_s", C.c_double), ("mean_service_s", C.c_double)]
 
@@ -134,6 +143,9 @@ SIGNATURES = {
     "wg_agg_export": (I32, [P, C.POINTER(wg_group_export)]),
     "wg_agg_reset": (I32, [P]),
     "wg_agg_kernel_shape": (I32, [P]),
+    "wg_agg_state_layout": (I32, [P, C.POINTER(wg_state_layout)]),
+    "wg_agg_partition_state": (I32, [P, I32, P, I64, PI64]),
+    "wg_agg_merge_state": (I32, [P, C.POINTER(wg_state_layout), P, I64]),
     "wg_agg_destroy": (I32, [P]),
     "wg_pipeline_run": (I32, [P, C.POINTER(wg_pipeline_desc)]),
     "wg_pipeline_run_device": (I32, [P, C.POINTER(wg_pipeline_desc)]),
@@ -146,6 +158,7 @@ SIGNATURES = {
     "wg_server_wait": (I32, [P, I64, F64, PI64, C.POINTER(C.c_double)]),
     "wg_server_export": (I32, [P, I64, C.POINTER(wg_group_export)]),
     "wg_server_release": (I32, [P, I64]),
+    "wg_server_cancel": (I32, [P, I64]),
     "wg_server_stats": (I32, [P, C.POINTER(wg_serve_stats)]),
     "wg_server_reset_stats": (I32, [P]),
     "wg_server_destroy": (I32, [P]),

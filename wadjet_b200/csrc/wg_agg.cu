@@ -254,6 +254,93 @@ __global__ void emit_kernel(FinalArgs A) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Exchange of partial group state between ranks (one process per GPU). A
+// state row is [flag][the group's slot words]: flag 0 = a regular key, 1 = the
+// group whose key equals the table's empty pattern, 2 = the NULL-key group.
+// Rows are routed like partitionFor (internal/engine/exec/partitioned_agg.go:221):
+// owner = high 64 bits of route_hash * parts, with route_hash = fibHash(key)
+// for one int key (routeHashInt64, :515), packedHash(lo, hi) for a packed key
+// (routeHashPacked, :529) and routeNullHash for a NULL key (:197).
+// ---------------------------------------------------------------------------
+constexpr unsigned long long kRouteNullHash = 0x9ae16a3b2f90404fULL;
+
+__device__ __forceinline__ int state_flag(const Layout& L, const unsigned long long* s, uint64_t idx, uint64_t cap) {
+  if (L.key_words == 0) return 0;
+  if (idx == cap + 1) return 2;
+  if (idx == cap) return 1;
+  if (L.key_words == 1) return s[0] == WG_EMPTY_KEY ? 1 : 0;
+  return (s[0] == ~0ULL && s[1] == ~0ULL) ? 1 : 0;
+}
+
+__device__ __forceinline__ uint32_t state_owner(const Layout& L, const unsigned long long* s, int flag, int parts) {
+  unsigned long long h = 0;
+  if (L.key_words == 0) return 0;
+  if (flag == 2) h = kRouteNullHash;
+  else if (L.key_words == 1) h = (flag == 1 ? WG_EMPTY_KEY : s[0]) * 0x9E3779B97F4A7C15ULL;
+  else {
+    const unsigned long long lo = flag == 1 ? ~0ULL : s[0], hi = flag == 1 ? ~0ULL : s[1];
+    const unsigned long long a = lo ^ 0x9E3779B97F4A7C15ULL, b = hi ^ 0x517CC1B727220A95ULL;
+    h = __umul64hi(a, b) ^ (a * b) ^ (lo + hi);
+  }
+  return (uint32_t)__umul64hi(h, (unsigned long long)parts);
+}
+
+// Rows per owner (counts[p], zeroed by the caller).
+__global__ void state_count_kernel(Layout L, Table T, const int64_t* list, int64_t n, int parts,
+                                   unsigned long long* counts) {
+  const uint64_t cap = T.mask + 1;
+  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n; g += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t idx = (uint64_t)list[g];
+    const unsigned long long* s = T.slots + idx * L.slot_words;
+    atomicAdd(&counts[state_owner(L, s, state_flag(L, s, idx, cap), parts)], 1ULL);
+  }
+}
+
+// Every group's state row at cursor[owner] (cursor starts at each owner's
+// first row; rows of one owner come out in any order).
+__global__ void state_scatter_kernel(Layout L, Table T, const int64_t* list, int64_t n, int parts,
+                                     unsigned long long* cursor, unsigned long long* rows) {
+  const uint64_t cap = T.mask + 1;
+  const int W = 1 + L.slot_words;
+  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n; g += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t idx = (uint64_t)list[g];
+    const unsigned long long* s = T.slots + idx * L.slot_words;
+    const int flag = state_flag(L, s, idx, cap);
+    const unsigned long long at = atomicAdd(&cursor[state_owner(L, s, flag, parts)], 1ULL);
+    unsigned long long* r = rows + at * W;
+    r[0] = (unsigned long long)flag;
+    for (int w = 0; w < L.slot_words; ++w) r[1 + w] = s[w];
+  }
+}
+
+// MergeSink of state rows laid out by Ls into the table (Ld, Td).
+template <int NA>
+__global__ void state_merge_kernel(Layout Ls, const unsigned long long* rows, int64_t n, Layout Ld, Table Td,
+                                   int32_t* err) {
+  Credit cr;
+  const int W = 1 + Ls.slot_words;
+  const LayoutAcc ls{Ls}, ld{Ld};
+  for (int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < n; g += (int64_t)gridDim.x * blockDim.x) {
+    const unsigned long long* r = rows + g * W;
+    const unsigned long long* s = r + 1;
+    const int flag = (int)r[0];
+    unsigned long long k0 = 0, k1 = 0;
+    bool knull = false;
+    if (Ls.key_words >= 1) {
+      if (flag == 2) knull = true;
+      else if (flag == 1) { k0 = Ls.key_words == 1 ? WG_EMPTY_KEY : ~0ULL; k1 = ~0ULL; }
+      else { k0 = s[0]; if (Ls.key_words == 2) k1 = s[1]; }
+    }
+    unsigned long long* d = find_global(ld, Td, k0, k1, knull, err, &cr);
+    if (!d) continue;
+    Contrib<NA> c;
+    slot_contrib<NA>(ls, s, c);
+    apply<NA, false>(ld, d, c, s[Ls.key_words]);
+  }
+  cr.release(Td);
+}
+
 template <int NA>
 void launch_fold(const Layout& Ls, const Table& Ts, const Layout& Ld, const Table& Td, int32_t* err, unsigned grid,
                  cudaStream_t st) {
@@ -1277,7 +1364,8 @@ static wg_status spill_consume(const PipelineRun& r, const wgd::Plan& P0, const 
       po.data[j] = a->sp_dev[(size_t)j].as<char>();
       po.es[j] = a->sp_es[(size_t)j];
     }
-    cudaFuncSetAttribute(wgd::part_scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wgd::part_scatter_smem(np));
+    WG_CUDA_TRY(cudaFuncSetAttribute(wgd::part_scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)wgd::part_scatter_smem(np)));
     wgd::part_scatter_kernel<<<grid, wgd::kPartThreads, wgd::part_scatter_smem(np), ctx->stream>>>(P, pbits, kSpillPartShift,
                                                                           offs.as<unsigned long long>(), po);
     ctx->count_launch();
@@ -1700,6 +1788,145 @@ wg_status wg_agg_reset(wg_agg* a) {
   a->known_groups = 0;
   a->upper_groups = 0;
   return WG_OK;
+}
+
+// ---- exchange of partial state between ranks -------------------------------
+
+wg_status wg_agg_state_layout(wg_agg* a, wg_state_layout* out) {
+  if (!a || !out) return fail(WG_E_INVALID, "NULL argument");
+  if (!a->resolved) return fail(WG_E_STATE, "aggregate has no state yet (nothing consumed or merged)");
+  std::memset(out, 0, sizeof(*out));
+  out->key_words = a->L.key_words;
+  out->slot_words = a->L.slot_words;
+  out->n_keys = (int32_t)a->key_cols.size();
+  out->n_aggs = (int32_t)a->specs.size();
+  for (int k = 0; k < out->n_keys; ++k) {
+    out->key_type[k] = a->key_types[(size_t)k];
+    out->key_i32[k] = a->L.key_i32[k];
+    out->key_word[k] = a->L.key_word[k];
+    out->key_shift[k] = a->L.key_shift[k];
+  }
+  for (int i = 0; i < out->n_aggs; ++i) {
+    out->agg_kind[i] = a->L.agg[i].kind;
+    out->agg_off[i] = a->L.agg[i].off;
+    out->agg_null_off[i] = a->L.agg[i].null_off;
+    out->agg_in_cls[i] = a->in_cls[(size_t)i];
+    out->agg_in_scale[i] = a->in_scale[(size_t)i];
+    out->agg_out_type[i] = a->out_type[(size_t)i];
+    out->agg_nullable[i] = a->nullable[(size_t)i] ? 1 : 0;
+  }
+  return WG_OK;
+}
+
+wg_status wg_agg_partition_state(wg_agg* a, int32_t n_parts, void* rows_dev, int64_t rows_cap, int64_t* part_rows) {
+  if (!a || !part_rows || n_parts < 1 || n_parts > 4096) return fail(WG_E_INVALID, "bad partition arguments");
+  if (!a->finalized) return fail(WG_E_STATE, "aggregate not finalized");
+  Ctx* ctx = a->ctx;
+  WG_TRY(ensure_device(ctx));
+  for (int p = 0; p < n_parts; ++p) part_rows[p] = 0;
+  if (!a->resolved || a->n_out == 0) return WG_OK;
+  if (a->n_out > rows_cap) return fail(WG_E_INVALID, "rows_cap is smaller than the aggregate's group count");
+  if (!rows_dev) return fail(WG_E_INVALID, "rows_dev is NULL");
+  DevBuf cnt;
+  WG_TRY(cnt.alloc(ctx, (int64_t)n_parts * 8));
+  WG_CUDA_TRY(cudaMemsetAsync(cnt.get(), 0, (size_t)n_parts * 8, ctx->stream));
+  const Table T = table_view(a);
+  const unsigned grid = grid_cap(ctx, a->n_out, 256);
+  state_count_kernel<<<grid, 256, 0, ctx->stream>>>(a->L, T, a->list.as<int64_t>(), a->n_out, n_parts,
+                                                    cnt.as<unsigned long long>());
+  ctx->count_launch();
+  WG_CUDA_TRY(cudaGetLastError());
+  std::vector<unsigned long long> c((size_t)n_parts), cur((size_t)n_parts);
+  WG_CUDA_TRY(cudaMemcpyAsync(c.data(), cnt.get(), (size_t)n_parts * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  WG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  unsigned long long acc = 0;
+  for (int p = 0; p < n_parts; ++p) { cur[(size_t)p] = acc; acc += c[(size_t)p]; part_rows[p] = (int64_t)c[(size_t)p]; }
+  if ((int64_t)acc != a->n_out) return fail(WG_E_CUDA, "state partition counts do not add up to the group count");
+  WG_CUDA_TRY(cudaMemcpyAsync(cnt.get(), cur.data(), (size_t)n_parts * 8, cudaMemcpyHostToDevice, ctx->stream));
+  state_scatter_kernel<<<grid, 256, 0, ctx->stream>>>(a->L, T, a->list.as<int64_t>(), a->n_out, n_parts,
+                                                      cnt.as<unsigned long long>(), (unsigned long long*)rows_dev);
+  ctx->count_launch();
+  WG_CUDA_TRY(cudaGetLastError());
+  WG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return check_device_error(ctx);
+}
+
+wg_status wg_agg_merge_state(wg_agg* a, const wg_state_layout* src, const void* rows_dev, int64_t n_rows) {
+  if (!a || !src || n_rows < 0 || (n_rows > 0 && !rows_dev)) return fail(WG_E_INVALID, "NULL argument");
+  if (a->finalized) return fail(WG_E_STATE, "aggregate already finalized");
+  if (a->spill) return fail(WG_E_UNSUPPORTED, "spilled aggregations are not merged");
+  if (src->n_keys != (int32_t)a->key_cols.size() || src->n_aggs != (int32_t)a->specs.size() ||
+      src->n_aggs > WG_MAX_AGGS || src->n_keys > WG_MAX_KEYS || src->slot_words > WG_MAX_SLOT_WORDS)
+    return fail(WG_E_INVALID, "state layout does not match the aggregate's shape");
+  Ctx* ctx = a->ctx;
+  WG_TRY(ensure_device(ctx));
+  // the layout a source with these kinds and null counters has
+  wg_agg ref;
+  ref.key_cols = a->key_cols;
+  ref.specs = a->specs;
+  ref.kind.assign(src->agg_kind, src->agg_kind + src->n_aggs);
+  ref.nullable.assign((size_t)src->n_aggs, false);
+  for (int i = 0; i < src->n_aggs; ++i) ref.nullable[(size_t)i] = src->agg_nullable[i] != 0;
+  std::memset(&ref.L, 0, sizeof(ref.L));
+  ref.L.key_words = src->key_words;
+  build_layout(&ref);
+  for (int k = 0; k < src->n_keys; ++k) {
+    ref.L.key_i32[k] = src->key_i32[k];
+    ref.L.key_word[k] = src->key_word[k];
+    ref.L.key_shift[k] = src->key_shift[k];
+    ref.L.key_vcol[k] = a->key_cols[(size_t)k];
+  }
+  bool same = ref.L.slot_words == src->slot_words;
+  for (int i = 0; i < src->n_aggs && same; ++i)
+    same = ref.L.agg[i].off == src->agg_off[i] && ref.L.agg[i].null_off == src->agg_null_off[i];
+  if (!same) return fail(WG_E_INVALID, "state layout is inconsistent with its aggregate kinds");
+  if (!a->resolved) {
+    // adopt the source's resolved schema (mergeSinkState inherits it, aggregate.go:4722)
+    a->key_types.assign(src->key_type, src->key_type + src->n_keys);
+    a->in_cls.assign(src->agg_in_cls, src->agg_in_cls + src->n_aggs);
+    a->in_scale.assign(src->agg_in_scale, src->agg_in_scale + src->n_aggs);
+    a->out_type.assign(src->agg_out_type, src->agg_out_type + src->n_aggs);
+    a->kind = ref.kind;
+    a->nullable = ref.nullable;
+    a->L = ref.L;
+    a->cap = a->L.key_words == 0 ? 1 : cap_for(std::max<int64_t>(std::max<int64_t>(a->hint, n_rows), 1024));
+    a->shift = 64 - log2u(a->cap);
+    WG_TRY(init_table(a, a->table, a->cap));
+    WG_TRY(a->ctr.alloc(ctx, 64));
+    WG_CUDA_TRY(cudaMemsetAsync(a->ctr.get(), 0, 64, ctx->stream));
+    a->known_groups = a->upper_groups = 0;
+    a->resolved = true;
+  }
+  if (a->L.key_words != src->key_words || a->kind != ref.kind)
+    return fail(WG_E_INVALID, "aggregate input types differ");
+  // the destination must carry every null counter the source has
+  bool upgrade = false;
+  std::vector<bool> nn = a->nullable;
+  for (size_t i = 0; i < nn.size(); ++i) if (ref.nullable[i] && !nn[i]) { nn[i] = true; upgrade = true; }
+  if (upgrade) {
+    wg_agg tmp;
+    tmp.key_cols = a->key_cols; tmp.specs = a->specs; tmp.kind = a->kind; tmp.nullable = nn; tmp.L = a->L;
+    build_layout(&tmp);
+    for (int k = 0; k < WG_MAX_KEYS; ++k) tmp.L.key_vcol[k] = a->L.key_vcol[k];
+    a->nullable = nn;
+    WG_TRY(rebuild_table(a, a->cap, tmp.L));
+  }
+  if (n_rows == 0) return WG_OK;
+  WG_TRY(refresh_groups(a));
+  const int64_t need = a->known_groups + n_rows + credit_slack(a);
+  if (a->L.key_words != 0 && need > (int64_t)((double)a->cap * kMaxLoad)) WG_TRY(rebuild_table(a, cap_for(need), a->L));
+  const unsigned grid = grid_cap(ctx, n_rows, 256);
+  if (ref.L.n_aggs <= 4) state_merge_kernel<4><<<grid, 256, 0, ctx->stream>>>(ref.L, (const unsigned long long*)rows_dev,
+                                                                          n_rows, a->L, table_view(a), ctx->dev_error);
+  else state_merge_kernel<8><<<grid, 256, 0, ctx->stream>>>(ref.L, (const unsigned long long*)rows_dev, n_rows, a->L,
+                                                           table_view(a), ctx->dev_error);
+  ctx->count_launch();
+  WG_CUDA_TRY(cudaGetLastError());
+  WG_TRY(refresh_groups(a));
+  int64_t v[2];
+  WG_TRY(read_back_i64(ctx, (const int64_t*)a->ctr.get(), v, 2));
+  if ((int32_t)v[1] != 0) return fail(WG_E_NOMEM, "aggregate table overflow while merging state rows");
+  return check_device_error(ctx);
 }
 
 int32_t wg_agg_kernel_shape(const wg_agg* a) { return a ? a->last_shape : -1; }

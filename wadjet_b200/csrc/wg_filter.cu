@@ -12,6 +12,9 @@
 #include "wg_internal.h"
 #include "wg_pred.cuh"
 
+#include <algorithm>
+#include <cstdlib>
+
 namespace wg {
 
 // Resolve a predicate constant against the column type (ResolveFilterKernel,
@@ -59,7 +62,16 @@ constexpr int kRows = 4;
 constexpr unsigned long long kFlagAgg = 1ULL << 62;
 constexpr unsigned long long kFlagInc = 2ULL << 62;
 constexpr unsigned long long kValMask = (1ULL << 62) - 1;
+// Failed polls of a predecessor's status word before a tile gives up
+// (WG_DERR_TIMEOUT). WG_FILTER_SPIN_LIMIT overrides it; 0 makes every tile
+// after the first give up at once, which tests the timeout path
+// deterministically without a wait that never ends.
 constexpr long long kSpinLimit = 1LL << 20;
+
+long long spin_limit() {
+  const char* v = std::getenv("WG_FILTER_SPIN_LIMIT");
+  return v ? std::max(0LL, std::atoll(v)) : kSpinLimit;
+}
 
 struct FilterArgs {
   DCol col;
@@ -72,6 +84,7 @@ struct FilterArgs {
   int64_t* out_n;
   int32_t* err;
   int64_t num_tiles;
+  long long spin_limit;
 };
 
 template <typename T> struct VecOf;
@@ -151,10 +164,13 @@ __global__ void __launch_bounds__(kBlock) filter_compact_kernel(const FilterArgs
       int64_t pred = tile - 1;
       long long spins = 0;
       while (pred >= 0) {
+        // the tile publishes its (partial) prefix on expiry, so no successor waits
+        // forever and every position it writes stays below the true one
+        if (spins >= a.spin_limit) { set_error(a.err, WG_DERR_TIMEOUT); break; }
         unsigned long long s = *((volatile unsigned long long*)(a.status + pred));
         unsigned long long flag = s & ~kValMask;
         if (flag == 0) {
-          if (++spins > kSpinLimit) { set_error(a.err, WG_DERR_TIMEOUT); break; }
+          ++spins;
           __nanosleep(64);
           continue;
         }
@@ -230,6 +246,7 @@ wg_status filter_launch(Ctx* ctx, const wgd::Pred& p, const wg_column& col, cons
   a.out_n = n_out_dev;
   a.err = ctx->dev_error;
   a.num_tiles = tiles;
+  a.spin_limit = spin_limit();
   dim3 grid((unsigned)tiles);
   switch (cls) {
     case WG_CLS_I32: launch_cls<WG_CLS_I32>(vec, a, grid, ctx->stream); break;
@@ -351,6 +368,10 @@ extern "C" wg_status wg_filter_execute_device_noalloc(void* stream, const wg_col
                                   std::to_string((long long)WG_NOALLOC_MAX_ITEMS));
   if (op < WG_OP_EQ || op > WG_OP_GE || (const_kind != WG_CONST_INT && const_kind != WG_CONST_FLOAT))
     return fail(WG_E_INVALID, "unknown compare op or constant kind");
+  // without a selection vector the items are the column's rows: more would read past it
+  if (!sel && n_items > col->len)
+    return fail(WG_E_INVALID, "n_items (" + std::to_string(n_items) + ") exceeds the column length (" +
+                                  std::to_string(col->len) + ")");
   wgd::Pred p;
   WG_TRY(resolve_pred(wg_predicate{0, op, const_kind, 0, const_i64, const_f64}, col->type_id, &p));
   int dev = -1;
@@ -392,6 +413,7 @@ extern "C" wg_status wg_filter_execute_device_noalloc(void* stream, const wg_col
     a.out_n = count;
     a.err = err;
     a.num_tiles = tiles;
+    a.spin_limit = spin_limit();
     dim3 grid((unsigned)tiles);
     switch (cls) {
       case WG_CLS_I32: launch_cls<WG_CLS_I32>(vec, a, grid, st); break;

@@ -87,7 +87,7 @@ struct wg_server {
   std::unordered_map<int64_t, Req*> reqs;
   int64_t next_ticket = 1;
   bool stop = false;
-  int64_t submitted = 0, completed = 0, failed = 0, running = 0;
+  int64_t submitted = 0, completed = 0, failed = 0, cancelled = 0, running = 0;
   // requests overlap on the device while their input bytes together stay under
   // work_limit; a request at least that large runs alone (it fills the GPU)
   int64_t inflight_work = 0, work_limit = int64_t(256) << 20;
@@ -294,6 +294,7 @@ wg_status wg_server_export(wg_server* s, int64_t ticket, const wg_group_export* 
 wg_status wg_server_release(wg_server* s, int64_t ticket) {
   if (!s) return fail(WG_E_INVALID, "server is NULL");
   Req* r = nullptr;
+  bool park = false;
   {
     std::lock_guard<std::mutex> lk(s->mu);
     auto it = s->reqs.find(ticket);
@@ -303,8 +304,18 @@ wg_status wg_server_release(wg_server* s, int64_t ticket) {
     s->reqs.erase(it);
     // keep enough finished aggregates that a slot rarely has to allocate a new
     // one while the previous result of the same shape is still held
-    if (r->agg && r->status == WG_OK && s->pool.size() < 16 * s->slots.size()) {
-      agg_trim(r->agg);  // a parked aggregate keeps its table, not its reorder copy
+    park = r->agg && r->status == WG_OK && s->pool.size() < 16 * s->slots.size();
+  }
+  // Trimming frees device memory (a device-wide synchronisation) and switches
+  // this thread's current device, so it runs with the server lock released:
+  // workers keep taking pooled aggregates and finishing requests meanwhile.
+  if (park) {
+    int prev_dev = -1;
+    cudaGetDevice(&prev_dev);
+    agg_trim(r->agg);  // a parked aggregate keeps its table, not its reorder copy
+    if (prev_dev >= 0) cudaSetDevice(prev_dev);
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->pool.size() < 16 * s->slots.size()) {
       s->pool.push_back(Pooled{r->agg, r->slot, r->keys, r->aggs, r->hint});
       r->agg = nullptr;
     }
@@ -316,12 +327,35 @@ wg_status wg_server_release(wg_server* s, int64_t ticket) {
   return WG_OK;
 }
 
+wg_status wg_server_cancel(wg_server* s, int64_t ticket) {
+  if (!s) return fail(WG_E_INVALID, "server is NULL");
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->reqs.find(ticket);
+    if (it == s->reqs.end()) return fail(WG_E_INVALID, "unknown ticket");
+    Req* r = it->second;
+    if (r->done) return fail(WG_E_STATE, "request already finished");
+    auto q = std::find(s->queue.begin(), s->queue.end(), r);
+    if (q == s->queue.end()) return fail(WG_E_STATE, "request already running");
+    s->queue.erase(q);
+    r->status = WG_E_CANCELLED;
+    r->err = "request cancelled before it was admitted";
+    r->done = true;
+    r->t_done = now_s();
+    ++s->cancelled;
+  }
+  s->cv_done.notify_all();
+  s->cv_work.notify_all();
+  return WG_OK;
+}
+
 wg_status wg_server_stats(wg_server* s, wg_serve_stats* o) {
   if (!s || !o) return fail(WG_E_INVALID, "NULL argument");
   std::lock_guard<std::mutex> lk(s->mu);
   o->submitted = s->submitted;
   o->completed = s->completed;
   o->failed = s->failed;
+  o->cancelled = s->cancelled;
   o->in_flight = s->running;
   o->queued = (int64_t)s->queue.size();
   o->p50_s = percentile(s->lat, 0.50);
@@ -341,7 +375,7 @@ wg_status wg_server_reset_stats(wg_server* s) {
   std::lock_guard<std::mutex> lk(s->mu);
   s->lat.clear();
   s->queue_sum = s->service_sum = 0;
-  s->completed = s->failed = s->submitted = 0;
+  s->completed = s->failed = s->submitted = s->cancelled = 0;
   s->t_first = -1;
   s->t_last = 0;
   return WG_OK;
