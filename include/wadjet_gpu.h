@@ -92,6 +92,9 @@ typedef int32_t wg_status;
 
 /* ---- join types: exec.JoinType (internal/engine/exec/join.go:20-30) ---- */
 #define WG_JOIN_INNER 0
+#define WG_JOIN_LEFT  1   /* unmatched probe rows once, build columns NULL */
+#define WG_JOIN_SEMI  5   /* probe rows with a match, once each; no build columns */
+#define WG_JOIN_ANTI  6   /* probe rows without a match (NULL keys included); no build columns */
 
 /* Int128 DECIMAL element. Field order is Go's batch.Int128{Hi int64; Lo uint64}
  * (internal/engine/batch/decimal.go:11), i.e. the opposite of a little-endian
@@ -275,10 +278,12 @@ WG_API wg_status wg_filter_execute_device_noalloc(void* stream, const wg_column*
 /* Hash join: exec.HashJoin / HashJoinProbe (internal/engine/exec/join.go)   */
 /* ======================================================================== */
 
-/* Inner equi-join on one integer-class key column (tryEnableIntKey,
- * join.go:520). build_key_col indexes the build batches; probe_key_col the
- * probe batches; payload_cols are build columns carried to the output.
- * build_row_hint pre-sizes the build buffers (HashJoin.BuildRowHint). */
+/* Equi-join on one integer-class key column (tryEnableIntKey, join.go:520).
+ * join_type: WG_JOIN_INNER, WG_JOIN_LEFT, WG_JOIN_SEMI or WG_JOIN_ANTI
+ * (semi and anti carry no payload columns, as executeSemiAntiJoin returns only
+ * probe rows, join.go:3247). build_key_col indexes the build batches;
+ * probe_key_col the probe batches; payload_cols are build columns carried to
+ * the output. build_row_hint pre-sizes the build buffers (HashJoin.BuildRowHint). */
 WG_API wg_status wg_join_create(wg_ctx* ctx, int32_t join_type, int32_t build_key_col,
                          int32_t probe_key_col, int32_t n_payload,
                          const int32_t* payload_cols, int64_t build_row_hint,
@@ -292,16 +297,19 @@ WG_API wg_status wg_join_build_finish(wg_join* j);
 /* Number of build rows stored and number of distinct keys indexed. */
 WG_API wg_status wg_join_build_stats(wg_join* j, int64_t* build_rows, int64_t* distinct_keys);
 /* HashJoinProbe.Execute → inlineIntProbe (join.go:2306,2670), bounded output
- * (BoundedOutputOperator, operators.go:86): emits at most `cap` match pairs
- * (probe_row, build_row) ordered by probe position, starting at probe position
- * *cursor (0 on the first call). On return *cursor is the next position to
- * resume from (== active rows when done) and *out_n the number of pairs. */
+ * (BoundedOutputOperator, operators.go:86): emits at most `cap` output pairs
+ * (probe_row, build_row) ordered by probe position, starting at output pair
+ * *cursor (0 on the first call). On return *cursor is the next pair to resume
+ * from and *out_n the number of pairs written. build_row is -1 where the output
+ * has no build row: an unmatched LEFT row (matchPair{matched: false},
+ * join.go:3180) and every SEMI / ANTI row. */
 WG_API wg_status wg_join_probe(wg_join* j, const wg_batch_desc* probe,
                         uint32_t* out_probe_rows, int64_t* out_build_rows,
                         int64_t cap, int64_t* cursor, int64_t* out_n);
 /* Gather build payload column `payload_idx` for `n` build rows
  * (gatherVector, exec/sort.go:611). out/out_valid are host buffers
- * (out_valid may be NULL; it receives one byte per row, 1 = valid). */
+ * (out_valid may be NULL; it receives one byte per row, 1 = valid); a build
+ * row of -1 (an unmatched LEFT row) gathers NULL. */
 WG_API wg_status wg_join_gather(wg_join* j, int32_t payload_idx, const int64_t* build_rows,
                          int64_t n, void* out, uint8_t* out_valid);
 /* Forget the build side so the handle can build again (a fresh HashJoin for the
@@ -353,6 +361,7 @@ typedef struct wg_state_layout {
   int32_t key_words, slot_words, n_keys, n_aggs;
   int32_t key_type[4];                        /* parquet.TypeID of each group column */
   int32_t key_i32[4], key_word[4], key_shift[4];  /* packed-key placement (buildPackedLayout) */
+  int32_t null_word, null_shift;              /* packed keys: 4-bit NULL field (-1: none) */
   int32_t agg_kind[8], agg_off[8], agg_null_off[8];
   int32_t agg_in_cls[8], agg_in_scale[8], agg_out_type[8], agg_nullable[8];
 } wg_state_layout;

@@ -76,6 +76,7 @@ def lib() -> C.CDLL:
             "or_join_distinct": (I64, [P]),
             "or_join_probe": (I64, [P, C.POINTER(Column), I64, P, I64, P, P, I64]),
             "or_join_free": (None, [P]),
+            "or_join_set_type": (None, [P, I32]),
             "or_agg_new": (P, [I32, P, I32, P]),
             "or_agg_consume": (C.c_int, [P, C.POINTER(BatchDesc)]),
             "or_agg_groups": (I64, [P]),
@@ -154,9 +155,11 @@ def filter_(t, data, valid, op, value, sel=None) -> np.ndarray:
 
 
 class Join:
-    def __init__(self, hint=64):
+    def __init__(self, hint=64, join_type=0):
         self.h = lib().or_join_new(hint)
         self.rows = 0
+        if join_type:
+            lib().or_join_set_type(self.h, join_type)
 
     def append(self, t, keys, valid=None):
         b = HostBatch([(t, keys, valid, 0)])

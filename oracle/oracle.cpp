@@ -291,6 +291,7 @@ bool build_packed_layout(const std::vector<int>& types, std::vector<PackedField>
 // HashJoin, int key (exec/join.go:520-575 build, 2670-2820 probe)
 // ---------------------------------------------------------------------------
 struct Join {
+  int type = WG_JOIN_INNER;         // exec.JoinType (join.go:20-30)
   std::unique_ptr<IntHashTable> index;
   std::vector<int64_t> arena;       // build row of each arena entry (buildRef)
   std::vector<int32_t> arena_next;  // chain to the previously built row with the same key
@@ -680,10 +681,15 @@ int run_worker(const wg_batch_desc& in, int32_t nf, const wg_predicate* filters,
         const wg_column& src = c < in.ncols ? cols[c] : build->cols[pay[c - in.ncols]];
         int64_t es = cls_of(src.type_id) == C_DEC ? 16 : (cls_of(src.type_id) == C_I32 || cls_of(src.type_id) == C_F32) ? 4 : 8;
         bufs[c].resize((size_t)(total * es));
-        bool nullable = src.valid_words != nullptr;
+        // build columns of a LEFT join are NULL where a probe row found no match
+        bool nullable = src.valid_words != nullptr || (c >= in.ncols && join->type == WG_JOIN_LEFT);
         if (nullable) valid[c].assign((size_t)((total + 63) / 64), 0);
         for (int64_t k = 0; k < total; ++k) {
           int64_t r = c < in.ncols ? (int64_t)pr[k] : br[k];
+          if (r < 0) {
+            std::memset(&bufs[c][k * es], 0, (size_t)es);
+            continue;  // valid bit stays 0
+          }
           std::memcpy(&bufs[c][k * es], (const uint8_t*)src.data + r * es, (size_t)es);
           if (nullable) set_valid(valid[c].data(), k, !is_null(src, r));
         }
@@ -770,20 +776,33 @@ int or_join_append(void* jp, const wg_column* key, int64_t base_row) {  // arena
 int64_t or_join_rows(void* jp) { return (int64_t)((Join*)jp)->arena.size(); }
 int64_t or_join_distinct(void* jp) { return ((Join*)jp)->index->size; }
 
+void or_join_set_type(void* jp, int32_t type) { ((Join*)jp)->type = type; }
+
+// inlineIntProbe for inner joins (join.go:2670-2820); the generic probe's
+// LEFT emission of an unmatched row as one NULL-padded pair (join.go:3180-3186,
+// NULL keys included since they never match); executeSemiAntiJoin's SEMI (a
+// matched row once) and ANTI (an unmatched or NULL-key row once)
+// (join.go:3247-3300). Pairs without a build row carry -1.
 int64_t or_join_probe(void* jp, const wg_column* key, int64_t len, const uint32_t* sel, int64_t sel_len,
                       uint32_t* out_probe, int64_t* out_build, int64_t cap) {
   Join* j = (Join*)jp;
   int64_t n = 0;
   const int64_t cnt = sel ? sel_len : len;
+  auto emit = [&](int64_t row, int64_t b) {
+    if (n < cap) { out_probe[n] = (uint32_t)row; out_build[n] = b; }
+    ++n;
+  };
   for (int64_t p = 0; p < cnt; ++p) {
     int64_t row = sel ? (int64_t)sel[p] : p;
-    if (is_null(*key, row)) continue;
-    auto h = j->index->get(get_i64(*key, row));
-    if (!h.second) continue;
-    for (int32_t ref = h.first; ref >= 0; ref = j->arena_next[(size_t)ref]) {
-      if (n < cap) { out_probe[n] = (uint32_t)row; out_build[n] = j->arena[(size_t)ref]; }
-      ++n;
+    std::pair<int32_t, bool> h{-1, false};
+    if (!is_null(*key, row)) h = j->index->get(get_i64(*key, row));
+    if (j->type == WG_JOIN_SEMI) { if (h.second) emit(row, -1); continue; }
+    if (j->type == WG_JOIN_ANTI) { if (!h.second) emit(row, -1); continue; }
+    if (!h.second) {
+      if (j->type == WG_JOIN_LEFT) emit(row, -1);
+      continue;
     }
+    for (int32_t ref = h.first; ref >= 0; ref = j->arena_next[(size_t)ref]) emit(row, j->arena[(size_t)ref]);
   }
   return n;
 }

@@ -36,10 +36,13 @@ int     or_join_append(void* j, const wg_column* key, int64_t base_row);
 int64_t or_join_rows(void* j);
 int64_t or_join_distinct(void* j);
 /* Emits (probe_row, build_row) pairs in probe order, chain order inside a
- * probe row (most recently built first, as arenaNext links). Returns the total
- * number of pairs; only the first `cap` are written. */
+ * probe row (most recently built first, as arenaNext links); build_row is -1
+ * where the output has none (unmatched LEFT rows, SEMI and ANTI rows).
+ * Returns the total number of pairs; only the first `cap` are written. */
 int64_t or_join_probe(void* j, const wg_column* key, int64_t len, const uint32_t* sel,
                       int64_t sel_len, uint32_t* out_probe, int64_t* out_build, int64_t cap);
+/* exec.JoinType of the probe: WG_JOIN_INNER (default), _LEFT, _SEMI, _ANTI. */
+void    or_join_set_type(void* j, int32_t type);
 void    or_join_free(void* j);
 
 /* HashAggregate (exec/aggregate.go:1296-2613, agg_scatter.go, kernel/types.go). */

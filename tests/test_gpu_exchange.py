@@ -83,7 +83,8 @@ def test_starjoin_partials_partition_and_merge(ctx, n_parts):
 
 
 def test_packed_and_null_keys_route_like_partition_for(ctx):
-    """Packed (a int32, b int64) keys route by packedHash; a NULL single key by routeNullHash."""
+    """Packed (a int32, b int64) keys route by packedHash, a packed key with a NULL column
+    and a NULL single key by routeNullHash (routeHashPacked / routeHashInt64)."""
     import wadjet_b200 as wg
     from wadjet_b200.exchange import (ROUTE_NULL_HASH, pack_key_words, partition_for, route_hash_int,
                                       route_hash_packed)
@@ -95,19 +96,22 @@ def test_packed_and_null_keys_route_like_partition_for(ctx):
     x = rng.standard_normal(n)
     aggs = [wg.AggColumn(wg.AGG_SUM, 2), wg.AggColumn(wg.AGG_COUNT, -1), wg.AggColumn(wg.AGG_MIN, 3),
             wg.AggColumn(wg.AGG_MAX, 3)]
+    a_valid = rng.random(n) > 0.02  # NULLs in one composite-key column
     partials = []
     for r0, r1 in ((0, n // 2), (n // 2, n)):
         p = wg.HashAggregate(ctx, [0, 1], aggs, ndv_hint=n)
-        p.consume(wg.Batch([wg.Column(I32, a_col[r0:r1]), wg.Column(I64, b_col[r0:r1]),
+        p.consume(wg.Batch([wg.Column(I32, a_col[r0:r1], a_valid[r0:r1]), wg.Column(I64, b_col[r0:r1]),
                             wg.Column(DEC, amt[r0:r1], scale=2), wg.Column(F64, x[r0:r1])]))
         partials.append(p)
     lay = partials[0].state_layout()
     owned = _owner_split(wg, partials, ([0, 1], aggs), 4)
     for p, e in enumerate(owned):
-        lo, hi = pack_key_words(e["keys"], lay)
-        assert (partition_for(route_hash_packed(lo, hi), 4) == p).all()
+        lo, hi = pack_key_words(e["keys"], lay, e["key_valid"])
+        full = e["key_valid"].all(axis=0)
+        h = np.where(full, route_hash_packed(lo, hi), np.uint64(ROUTE_NULL_HASH))
+        assert (partition_for(h, 4) == p).all()
     whole = wg.HashAggregate(ctx, [0, 1], aggs, ndv_hint=n)
-    whole.consume(wg.Batch([wg.Column(I32, a_col), wg.Column(I64, b_col), wg.Column(DEC, amt, scale=2),
+    whole.consume(wg.Batch([wg.Column(I32, a_col, a_valid), wg.Column(I64, b_col), wg.Column(DEC, amt, scale=2),
                             wg.Column(F64, x)]))
     whole.finalize()
     assert_groups_equal(_concat(owned), whole.export(), ["sum_d", "count", "min_f", "max_f"])

@@ -233,8 +233,6 @@ def run_both(ctx, cols, key_idx, specs, hint=0, batches=3, device=False):
 @pytest.mark.parametrize("key_types,ncard", [([I64], 5000), ([I32], 300), ([I32, I64], 20_000), ([], 1)])
 @pytest.mark.parametrize("nulls,key_nulls", [(0.0, 0.0), (0.1, 0.05)])
 def test_aggregate_matches_oracle(ctx, key_types, ncard, nulls, key_nulls):
-    if len(key_types) > 1 and key_nulls:
-        pytest.skip("NULL in a composite key is outside the GPU path")
     rng = np.random.default_rng(ncard + len(key_types))
     cols = agg_setup(rng, 60_000, key_types, ncard, nulls, key_nulls)
     specs, kinds = make_aggs(len(key_types))
@@ -383,3 +381,43 @@ def test_ledger_refuses_over_budget():
         with pytest.raises(wg.MemoryExceeded):
             g.consume(wg.Batch([wg.Column(I64, np.arange(10, dtype=np.int64))]))
         g.close()
+
+
+@pytest.mark.parametrize("key_types", [[I32, I64], [I32, I32, I32], [I32, I32]])
+def test_nullable_composite_keys_match_oracle(ctx, key_types):
+    """A NULL in any column of a composite key is that column's own value (the generic
+    path the reference migrates to, aggregate.go:1822-1840): rows agreeing on every
+    non-NULL column and on which columns are NULL form one group."""
+    import wadjet_b200 as wg
+    rng = np.random.default_rng(len(key_types) * 13)
+    n = 80_000
+    cols = []
+    for t in key_types:
+        v = rng.integers(0, 40, n).astype(np.int32 if t == I32 else np.int64)
+        cols.append((t, v, rng.random(n) > 0.15))
+    val = rng.integers(-10**6, 10**6, n).astype(np.int64)
+    cols.append((I64, val, None))
+    nk = len(key_types)
+    aggs = [(0, nk, 0), (1, -1, 0), (2, nk, 0)]
+    g = wg.HashAggregate(ctx, list(range(nk)), [wg.AggColumn(f, c, o) for f, c, o in aggs], ndv_hint=1000)
+    for r0, r1 in ((0, n // 2), (n // 2, n)):
+        g.consume(wg.Batch([wg.Column(t, d[r0:r1], None if v is None else v[r0:r1]) for t, d, v in cols]))
+    g.finalize()
+    o = ob.Agg(list(range(nk)), aggs)
+    o.consume(ob.HostBatch([(t, d, v, 0) for t, d, v in cols]))
+    got, want = g.export(), o.export()
+    assert (want["key_valid"] == 0).any()
+    assert_groups_equal(got, want, ["sum_i", "count", "min_i"])
+    g.close()
+
+
+def test_nullable_key_filling_128_bits_is_refused(ctx):
+    """Two int64 key columns take all 128 bits of the packed key: no room for the NULL
+    field, so a NULL there is refused rather than merged into another group."""
+    import wadjet_b200 as wg
+    a = np.arange(100, dtype=np.int64)
+    g = wg.HashAggregate(ctx, [0, 1], [wg.AggColumn(wg.AGG_COUNT, -1)], ndv_hint=100)
+    with pytest.raises(wg.WadjetGPUError) as ei:
+        g.consume(wg.Batch([wg.Column(I64, a, a % 7 != 0), wg.Column(I64, a)]))
+    assert ei.value.status == wg._abi.WG_E_UNSUPPORTED
+    g.close()

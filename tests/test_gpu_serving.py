@@ -116,3 +116,33 @@ def test_admission_refuses_what_never_fits(ctx, tables):
     s.release(t_big)
     s.release(t_ok)
     s.close()
+
+
+def test_cancel_withdraws_queued_requests(ctx, tables):
+    """A request still in the queue can be withdrawn (the caller's context was
+    cancelled): its wait raises Cancelled, it never runs, and the requests ahead
+    of it and after it finish with their usual results."""
+    import wadjet_b200 as wg
+    tpl = templates(wg, tables)
+    s = wg.Server(ctx, 1)  # one slot: requests behind the first one stay queued
+    ahead = [s.submit(**tpl["join"]) for _ in range(4)]
+    doomed = [s.submit(**tpl["groupby"]) for _ in range(2)]
+    after = s.submit(**tpl["ipv4"])
+    for t in doomed:
+        s.cancel(t)
+    for t in doomed:
+        with pytest.raises(wg.Cancelled):
+            s.wait(t, timeout=60.0)
+    for t in ahead:
+        n, _ = s.wait(t, timeout=120.0)
+        assert 990 <= n <= 1000
+    n, _ = s.wait(after, timeout=120.0)
+    assert 60000 < n <= 1 << 16
+    with pytest.raises(wg.WadjetGPUError) as ei:
+        s.cancel(after)  # finished requests cannot be cancelled
+    assert ei.value.status == wg._abi.WG_E_STATE
+    st = s.stats()
+    assert st["cancelled"] == 2 and st["completed"] == 5 and st["failed"] == 0
+    for t in ahead + doomed + [after]:
+        s.release(t)
+    s.close()

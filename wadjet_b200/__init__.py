@@ -25,7 +25,8 @@ from typing import Iterable, Optional, Sequence
 import numpy as np
 
 from . import _abi as abi
-from ._abi import (AGG_AVG, AGG_COUNT, AGG_MAX, AGG_MIN, AGG_SUM, CONST_FLOAT, CONST_INT, OP_EQ, OP_GE, OP_GT,
+from ._abi import (AGG_AVG, AGG_COUNT, AGG_MAX, AGG_MIN, AGG_SUM, CONST_FLOAT, CONST_INT, JOIN_ANTI, JOIN_INNER,
+                   JOIN_LEFT, JOIN_SEMI, OP_EQ, OP_GE, OP_GT,
                    OP_LE, OP_LT, OP_NE, TYPE_DATE, TYPE_DECIMAL, TYPE_DURATION, TYPE_FLOAT32, TYPE_FLOAT64,
                    TYPE_INT32, TYPE_INT64, TYPE_IPV4, TYPE_MAC, TYPE_PORT, TYPE_PROTOCOL, TYPE_TIMESTAMP)
 
@@ -228,16 +229,20 @@ class KernelFilter:
 
 
 class HashJoin:
-    """exec.HashJoin (inner, one integer-class key) + HashJoinProbe."""
+    """exec.HashJoin on one integer-class key + HashJoinProbe.
+
+    join_type: JOIN_INNER, JOIN_LEFT (unmatched probe rows once, NULL build
+    columns), JOIN_SEMI or JOIN_ANTI (probe rows only, no payload columns)."""
 
     def __init__(self, ctx: Context, build_key: int, probe_key: int, payload: Sequence[int] = (),
-                 build_row_hint: int = 0):
+                 build_row_hint: int = 0, join_type: int = abi.JOIN_INNER):
         self.ctx = ctx
         self.payload = list(payload)
         self.payload_types: list[int] = []
+        self.join_type = join_type
         pay = (C.c_int32 * max(1, len(payload)))(*payload)
         h = C.c_void_p()
-        _check(lib.wg_join_create(ctx.h, abi.JOIN_INNER, build_key, probe_key, len(payload), pay, build_row_hint,
+        _check(lib.wg_join_create(ctx.h, join_type, build_key, probe_key, len(payload), pay, build_row_hint,
                                   C.byref(h)))
         self.h = h
 

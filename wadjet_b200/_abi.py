@@ -20,7 +20,7 @@ OP_EQ, OP_NE, OP_LT, OP_LE, OP_GT, OP_GE = range(6)
 CONST_INT, CONST_FLOAT = 0, 1
 # exec.AggFunc
 AGG_SUM, AGG_COUNT, AGG_MIN, AGG_MAX, AGG_AVG = range(5)
-JOIN_INNER = 0
+JOIN_INNER, JOIN_LEFT, JOIN_SEMI, JOIN_ANTI = 0, 1, 5, 6
 # expression opcodes
 EXPR_COL, EXPR_CONST_I, EXPR_CONST_F, EXPR_ADD, EXPR_SUB, EXPR_MUL, EXPR_DIV, EXPR_SHR, EXPR_AND = range(9)
 EXPR_MAX_OPS = 12
@@ -82,7 +82,8 @@ class wg_tune_params(C.Structure):
 class wg_state_layout(C.Structure):
     _fields_ = [("key_words", C.c_int32), ("slot_words", C.c_int32), ("n_keys", C.c_int32), ("n_aggs", C.c_int32),
                 ("key_type", C.c_int32 * 4), ("key_i32", C.c_int32 * 4), ("key_word", C.c_int32 * 4),
-                ("key_shift", C.c_int32 * 4), ("agg_kind", C.c_int32 * 8), ("agg_off", C.c_int32 * 8),
+                ("key_shift", C.c_int32 * 4), ("null_word", C.c_int32), ("null_shift", C.c_int32),
+                ("agg_kind", C.c_int32 * 8), ("agg_off", C.c_int32 * 8),
                 ("agg_null_off", C.c_int32 * 8), ("agg_in_cls", C.c_int32 * 8), ("agg_in_scale", C.c_int32 * 8),
                 ("agg_out_type", C.c_int32 * 8), ("agg_nullable", C.c_int32 * 8)]
 

@@ -29,6 +29,7 @@ int32_t join_payload_scale(wg_join* j, int i);
 bool join_payload_nullable(wg_join* j, int i);
 bool join_payload_range(wg_join* j, int i, long long* lo, long long* hi);
 int64_t join_max_fanout(wg_join* j);
+int32_t join_type_of(wg_join* j);
 }  // namespace wg
 
 using namespace wgd;
@@ -182,6 +183,14 @@ __device__ __forceinline__ int64_t slot_key(const Layout& L, const unsigned long
   return L.key_i32[k] ? (int64_t)(int32_t)(uint32_t)(w >> L.key_shift[k]) : (int64_t)w;
 }
 
+// Whether key column k of a packed slot is NULL (its bit in the NULL field).
+__device__ __forceinline__ bool slot_key_null(const Layout& L, const unsigned long long* s, uint64_t idx, uint64_t cap,
+                                              int k) {
+  if (L.key_words == 1) return idx == cap + 1;
+  if (L.key_words != 2 || L.null_word < 0 || idx == cap) return false;
+  return (s[L.null_word] >> (L.null_shift + k)) & 1ULL;
+}
+
 __global__ void export_kernel(FinalArgs A) {
   const Layout& L = A.L;
   const uint64_t cap = A.T.mask + 1;
@@ -190,7 +199,7 @@ __global__ void export_kernel(FinalArgs A) {
     const unsigned long long* s = A.T.slots + idx * L.slot_words;
     const int64_t o = g;
     for (int k = 0; k < L.n_keys; ++k) {
-      const bool valid = !(L.key_words >= 1 && idx == cap + 1);
+      const bool valid = !slot_key_null(L, s, idx, cap, k);
       if (A.keys) A.keys[k * A.stride + o] = valid ? slot_key(L, s, k) : 0;
       if (A.key_valid) A.key_valid[k * A.stride + o] = valid ? 1 : 0;
     }
@@ -214,7 +223,7 @@ __global__ void emit_kernel(FinalArgs A) {
     const uint64_t idx = (uint64_t)A.list[A.start + g];
     const unsigned long long* s = A.T.slots + idx * L.slot_words;
     for (int k = 0; k < L.n_keys; ++k) {
-      const bool valid = !(L.key_words >= 1 && idx == cap + 1);
+      const bool valid = !slot_key_null(L, s, idx, cap, k);
       const int64_t v = valid ? slot_key(L, s, k) : 0;
       if (A.key_cls[k] == WG_CLS_I32) ((int32_t*)A.out[k])[g] = (int32_t)v;
       else ((int64_t*)A.out[k])[g] = v;
@@ -278,7 +287,9 @@ __device__ __forceinline__ uint32_t state_owner(const Layout& L, const unsigned 
   if (L.key_words == 0) return 0;
   if (flag == 2) h = kRouteNullHash;
   else if (L.key_words == 1) h = (flag == 1 ? WG_EMPTY_KEY : s[0]) * 0x9E3779B97F4A7C15ULL;
-  else {
+  else if (flag == 0 && L.null_word >= 0 && ((s[L.null_word] >> L.null_shift) & 0xFULL) != 0) {
+    h = kRouteNullHash;  // routeHashPacked: a row with any NULL key column (partitioned_agg.go:530)
+  } else {
     const unsigned long long lo = flag == 1 ? ~0ULL : s[0], hi = flag == 1 ? ~0ULL : s[1];
     const unsigned long long a = lo ^ 0x9E3779B97F4A7C15ULL, b = hi ^ 0x517CC1B727220A95ULL;
     h = __umul64hi(a, b) ^ (a * b) ^ (lo + hi);
@@ -605,6 +616,10 @@ static wg_status agg_resolve(wg_agg* a, const VSchema& vs) {
       if (class_of(a->key_types[k]) == WG_CLS_I32) {
         a->L.key_word[k] = slots[nn].first; a->L.key_shift[k] = slots[nn].second; a->L.key_i32[k] = 1; ++nn;
       }
+    // the first 32-bit half the packing leaves unused holds the NULL field
+    a->L.null_word = -1;
+    a->L.null_shift = 0;
+    if (nn < slots.size()) { a->L.null_word = slots[nn].first; a->L.null_shift = slots[nn].second; }
   }
   for (int k = 0; k < nk; ++k) a->L.key_vcol[k] = a->key_cols[k];
   const size_t na = a->specs.size();
@@ -772,9 +787,11 @@ static wg_status build_plan(const PipelineRun& r, wgd::Plan& P, VSchema& vs, std
     vs.type.push_back(in->cols[c].type_id); vs.scale.push_back(in->cols[c].scale);
     vs.nullable.push_back(in->cols[c].valid_words != nullptr);
   }
+  // an unmatched LEFT-join row carries NULL build columns
+  const bool outer = r.join && join_type_of(r.join) == WG_JOIN_LEFT;
   for (int p = 0; p < npay; ++p) {
     vs.type.push_back(join_payload_type(r.join, p)); vs.scale.push_back(join_payload_scale(r.join, p));
-    vs.nullable.push_back(join_payload_nullable(r.join, p));
+    vs.nullable.push_back(outer || join_payload_nullable(r.join, p));
   }
   if (r.n_exprs < 0 || r.n_exprs > WG_MAX_EXPRS) return fail(WG_E_UNSUPPORTED, "at most 2 projection expressions");
   for (int e = 0; e < r.n_exprs; ++e) {
@@ -964,6 +981,7 @@ static wg_status run_device(const PipelineRun& r) {
     const int kv = ls.P.L.key_vcol[0];
     const int npay = r.join ? join_n_payload(r.join) : 0;
     const bool cand = smem_ok && env_int("WG_GROUP_DENSE", 1) != 0 && a->L.n_keys == 1 && r.join != nullptr &&
+                      join_type_of(r.join) == WG_JOIN_INNER &&
                       kv >= ls.P.n_in && kv < ls.P.n_in + npay &&
                       join_payload_range(r.join, kv - ls.P.n_in, &glo, &ghi) && ghi >= glo && ghi - glo < 16384;
     bool placed = false;
@@ -1800,6 +1818,8 @@ wg_status wg_agg_state_layout(wg_agg* a, wg_state_layout* out) {
   out->slot_words = a->L.slot_words;
   out->n_keys = (int32_t)a->key_cols.size();
   out->n_aggs = (int32_t)a->specs.size();
+  out->null_word = a->L.key_words == 2 ? a->L.null_word : -1;
+  out->null_shift = a->L.null_shift;
   for (int k = 0; k < out->n_keys; ++k) {
     out->key_type[k] = a->key_types[(size_t)k];
     out->key_i32[k] = a->L.key_i32[k];
@@ -1870,6 +1890,8 @@ wg_status wg_agg_merge_state(wg_agg* a, const wg_state_layout* src, const void* 
   std::memset(&ref.L, 0, sizeof(ref.L));
   ref.L.key_words = src->key_words;
   build_layout(&ref);
+  ref.L.null_word = src->null_word;
+  ref.L.null_shift = src->null_shift;
   for (int k = 0; k < src->n_keys; ++k) {
     ref.L.key_i32[k] = src->key_i32[k];
     ref.L.key_word[k] = src->key_word[k];

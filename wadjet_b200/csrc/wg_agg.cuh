@@ -55,6 +55,12 @@ struct Layout {
   int32_t key_i32[WG_MAX_KEYS];    // packed field is 4 bytes wide
   int32_t key_word[WG_MAX_KEYS];
   int32_t key_shift[WG_MAX_KEYS];
+  // Packed keys with NULLs: bit k of the 4-bit field at (null_word, null_shift)
+  // marks key column k NULL (its value bits are then 0). The field lies in a
+  // 32-bit half the packing leaves unused, so a key without NULLs keeps its
+  // plain packing; null_word = -1 when every bit is taken (NULLs refused).
+  int32_t null_word;
+  int32_t null_shift;
   AggD agg[WG_MAX_AGGS];
   unsigned long long init[WG_MAX_SLOT_WORDS];   // empty-slot pattern
 };

@@ -218,6 +218,11 @@ __device__ __forceinline__ Val fetch_base(const Plan& P, const Sh& sh, const Src
     return v;
   }
   const int p = j - sh.n_in();
+  if (sh.nullable() && brow < 0) {  // LEFT join, unmatched probe row: NULL build columns
+    Val v;
+    v.lo = 0; v.hi = 0; v.null = true;
+    return v;
+  }
   Val v = load_typed(P.join.pay[p].data, sh.pay_cls(p), brow);
   v.null = sh.nullable() && is_null(P.join.pay[p], brow);
   return v;
@@ -685,7 +690,14 @@ __device__ __forceinline__ bool make_key(const Plan& P, const Sh& sh, const Src&
   for (int k = 0; k < WG_MAX_KEYS; ++k) {
     if (k >= sh.n_keys()) break;
     Val v = fetch(P, sh, src, sh.key_vcol(k), brow, ev);
-    if (v.null) { set_error(P.err, WG_DERR_NULL_PACKED); return false; }
+    if (v.null) {
+      // a NULL composite-key column is its own value (the generic path's NULL,
+      // aggregate.go:1822-1840): its bit in the NULL field, value bits 0
+      if (P.L.null_word < 0) { set_error(P.err, WG_DERR_NULL_PACKED); return false; }
+      const unsigned long long m = 1ULL << (P.L.null_shift + k);
+      if (P.L.null_word == 0) k0 |= m; else k1 |= m;
+      continue;
+    }
     const unsigned long long w =
         sh.key_i32(k) ? ((unsigned long long)(uint32_t)(int32_t)v.lo) << sh.key_shift(k) : v.lo;
     if (sh.key_word(k) == 0) k0 |= w; else k1 |= w;
@@ -718,14 +730,20 @@ __device__ __forceinline__ void process_rows(const Plan& P, const Sh& sh, const 
     if (act) act = pred_val(P, sh, f, src.in(P, sh, sh.filt_col(f)));
   }
   int32_t brow = -1;
+  // exec.JoinType: inner and left walk the chain; semi and anti only test it
+  const int jt = sh.has_join() ? (sh.direct() ? WG_JOIN_INNER : P.join.jtype) : WG_JOIN_INNER;
   if (sh.has_join() && act) {
     const Val kv = src.in(P, sh, sh.probe_col());
-    if (kv.null) act = false;
-    else if (sh.direct()) act = join_direct(P.join, (int64_t)kv.lo, brow, P.err);
+    bool found = false;
+    if (kv.null) found = false;  // NULL keys never match (join.go:2700)
+    else if (sh.direct()) found = join_direct(P.join, (int64_t)kv.lo, brow, P.err);
     else {
       brow = join_head(P.join, (int64_t)kv.lo, P.err);
-      act = brow >= 0;
+      found = brow >= 0;
     }
+    if (jt == WG_JOIN_INNER) act = found;
+    else if (jt == WG_JOIN_LEFT) { if (!found) brow = -1; }     // kept; NULL build columns
+    else { act = jt == WG_JOIN_SEMI ? found : !found; brow = -1; }  // executeSemiAntiJoin (join.go:3247)
   }
   for (;;) {
     if (!__any_sync(WG_FULL_MASK, act)) break;
@@ -745,8 +763,11 @@ __device__ __forceinline__ void process_rows(const Plan& P, const Sh& sh, const 
     warp_update<NA, SMEM>(P, sh, cur, k0, k1, knull, c, sm, s_groups, s_limit, cr);
     if (!sh.has_join() || sh.direct()) break;  // unique keys: at most one match
     if (act) {
-      brow = __ldg(P.join.next + brow);         // arenaNext chain (join.go:2700)
-      act = brow >= 0;
+      if (brow < 0) act = false;                // semi, anti, or an unmatched left row: emitted once
+      else {
+        brow = __ldg(P.join.next + brow);       // arenaNext chain (join.go:2700)
+        act = brow >= 0;
+      }
     }
   }
 }

@@ -115,12 +115,24 @@ struct ProbeArgs {
   int32_t* err;
 };
 
+// Output pairs of one probe row by join type: inner = the chain's length;
+// left = at least one (an unmatched row once, NULL-padded, join.go:3180);
+// semi = one when the chain is not empty; anti = one when it is (a NULL key
+// never matches, so it passes an anti join, join.go:3290).
+__device__ __forceinline__ int32_t probe_head(const ProbeArgs& a, int64_t row) {
+  return is_null(a.key, row) ? -1 : join_head(a.j, ld_i64(a.key, row), a.err);
+}
+
 __global__ void join_probe_count_kernel(const ProbeArgs a) {
   for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < a.n; p += (int64_t)gridDim.x * blockDim.x) {
     const int64_t row = a.sel ? (int64_t)a.sel[p] : p;
+    const int32_t head = probe_head(a, row);
     int64_t c = 0;
-    if (!is_null(a.key, row)) {
-      for (int32_t ref = join_head(a.j, ld_i64(a.key, row), a.err); ref >= 0; ref = __ldg(a.j.next + ref)) ++c;
+    if (a.j.jtype == WG_JOIN_SEMI) c = head >= 0;
+    else if (a.j.jtype == WG_JOIN_ANTI) c = head < 0;
+    else {
+      for (int32_t ref = head; ref >= 0; ref = __ldg(a.j.next + ref)) ++c;
+      if (a.j.jtype == WG_JOIN_LEFT && c == 0) c = 1;
     }
     a.counts[p] = c;
   }
@@ -132,8 +144,13 @@ __global__ void join_probe_emit_kernel(const ProbeArgs a) {
     int64_t j = a.offs[p];
     if (j >= a.cursor + a.cap || j + a.counts[p] <= a.cursor) continue;
     const int64_t row = a.sel ? (int64_t)a.sel[p] : p;
-    for (int32_t ref = join_head(a.j, ld_i64(a.key, row), a.err); ref >= 0 && j < a.cursor + a.cap;
-         ref = __ldg(a.j.next + ref), ++j) {
+    const int32_t head = probe_head(a, row);
+    if (a.j.jtype == WG_JOIN_SEMI || a.j.jtype == WG_JOIN_ANTI || head < 0) {  // one pair, no build row
+      a.out_probe[j - a.cursor] = (uint32_t)row;
+      a.out_build[j - a.cursor] = -1;
+      continue;
+    }
+    for (int32_t ref = head; ref >= 0 && j < a.cursor + a.cap; ref = __ldg(a.j.next + ref), ++j) {
       if (j >= a.cursor) {
         a.out_probe[j - a.cursor] = (uint32_t)row;
         a.out_build[j - a.cursor] = ref;
@@ -240,6 +257,11 @@ __global__ void gather_kernel(const char* src, int64_t es, const uint64_t* valid
                               char* dst, uint8_t* dst_valid) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const int64_t r = rows[i];
+    if (r < 0) {  // no build row (an unmatched LEFT row): NULL
+      for (int64_t b = 0; b < es; ++b) dst[i * es + b] = 0;
+      if (dst_valid) dst_valid[i] = 0;
+      continue;
+    }
     for (int64_t b = 0; b < es; ++b) dst[i * es + b] = src[r * es + b];
     if (dst_valid) dst_valid[i] = valid ? (uint8_t)((valid[r >> 6] >> (r & 63)) & 1ULL) : (uint8_t)1;
   }
@@ -276,6 +298,7 @@ struct BuildCol {
 
 struct wg_join {
   wg::Ctx* ctx;
+  int32_t jtype = WG_JOIN_INNER;  // exec.JoinType (join.go:20-30)
   int32_t build_key_col, probe_key_col;
   std::vector<int32_t> payload_cols;
   int64_t hint;
@@ -415,6 +438,8 @@ static wg_status join_view_fields(wg_join* j, wgd::JoinView* v) {
   v->slots = j->slots.get();
   v->next = j->next.as<int32_t>();
   v->n_pay = (int32_t)j->pay.size();
+  v->jtype = j->jtype;
+  v->_pad = 0;
   v->direct = 0;
   v->sentinel = 0;
   v->dense = 0;
@@ -433,7 +458,9 @@ wg_status join_view(wg_join* j, wgd::JoinView* v) {
 
 // The view the fused pipeline probes: the direct-payload table when one was built.
 wg_status join_view_fused(wg_join* j, wgd::JoinView* v) {
-  if (!j->direct) return join_view(j, v);
+  // the direct-payload table answers "which payload", not "was there a match":
+  // outer, semi and anti joins probe the hash index
+  if (!j->direct || j->jtype != WG_JOIN_INNER) return join_view(j, v);
   WG_TRY(join_view_fields(j, v));
   {
     v->slots = j->dslots.get();
@@ -465,6 +492,7 @@ bool join_payload_range(wg_join* j, int i, long long* lo, long long* hi) {
   return true;
 }
 bool join_unique(wg_join* j) { return j->unique; }
+int32_t join_type_of(wg_join* j) { return j->jtype; }
 int64_t join_max_fanout(wg_join* j) { return j->max_fanout; }
 
 // The hash index (slots/next): one CAS insert per build row, heads chained
@@ -591,11 +619,16 @@ extern "C" {
 wg_status wg_join_create(wg_ctx* ctx, int32_t join_type, int32_t build_key_col, int32_t probe_key_col,
                          int32_t n_payload, const int32_t* payload_cols, int64_t build_row_hint, wg_join** out) {
   if (!ctx || !out) return fail(WG_E_INVALID, "NULL argument");
-  if (join_type != WG_JOIN_INNER) return fail(WG_E_UNSUPPORTED, "only inner joins are on the GPU path");
+  if (join_type != WG_JOIN_INNER && join_type != WG_JOIN_LEFT && join_type != WG_JOIN_SEMI &&
+      join_type != WG_JOIN_ANTI)
+    return fail(WG_E_UNSUPPORTED, "join type is not on the GPU path (inner, left, semi and anti are)");
   if (n_payload < 0 || n_payload > WG_MAX_PAYLOAD || (n_payload > 0 && !payload_cols))
     return fail(WG_E_INVALID, "at most 4 payload columns");
+  if ((join_type == WG_JOIN_SEMI || join_type == WG_JOIN_ANTI) && n_payload > 0)
+    return fail(WG_E_INVALID, "a semi or anti join returns probe rows only: no payload columns");
   wg_join* j = new wg_join();
   j->ctx = ctx;
+  j->jtype = join_type;
   j->build_key_col = build_key_col;
   j->probe_key_col = probe_key_col;
   j->payload_cols.assign(payload_cols, payload_cols + n_payload);
@@ -795,7 +828,7 @@ wg_status wg_join_gather(wg_join* j, int32_t payload_idx, const int64_t* build_r
   WG_TRY(ensure_device(ctx));
   if (n == 0) return WG_OK;
   for (int64_t i = 0; i < n; ++i)
-    if (build_rows[i] < 0 || build_rows[i] >= j->rows) return fail(WG_E_INVALID, "build row out of range");
+    if (build_rows[i] < -1 || build_rows[i] >= j->rows) return fail(WG_E_INVALID, "build row out of range");
   BuildCol& c = j->pay[payload_idx];
   WG_TRY(j->rows_dev.ensure(ctx, n * 8));
   WG_TRY(j->gath.ensure(ctx, n * c.es));

@@ -15,6 +15,7 @@
 // A slot is empty when its head is -1 (every occupied slot has head >= 0).
 #pragma once
 
+#include "wadjet_gpu.h"
 #include "wg_device.cuh"
 
 #define WG_MAX_PAYLOAD 4
@@ -41,6 +42,12 @@ struct JoinView {
   // (payload of key base+i at i) and a key in range always matches.
   int32_t dense;
   int32_t l2keep;          // dense probes ask L2 to keep the table's lines (evict-last)
+  // exec.JoinType of the probe (join.go:20-30): WG_JOIN_INNER, WG_JOIN_LEFT
+  // (an unmatched probe row once, with NULL build columns), WG_JOIN_SEMI (a
+  // matched probe row once, no build columns), WG_JOIN_ANTI (a probe row with
+  // no match or a NULL key, no build columns)
+  int32_t jtype;
+  int32_t _pad;
   long long base;
   DCol pay[WG_MAX_PAYLOAD];
 };

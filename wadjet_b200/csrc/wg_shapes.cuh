@@ -206,7 +206,9 @@ inline bool shape_matches(const Plan& P) {
     if (P.filt[f].col != C::filt_col(f) || P.filt[f].cls != C::filt_cls(f) || P.filt[f].op != C::filt_op(f))
       return false;
   if (C::has_join) {
-    if (P.join.direct != C::direct || P.probe_col != C::probe_col || P.join.n_pay != C::n_pay) return false;
+    if (P.join.direct != C::direct || P.probe_col != C::probe_col || P.join.n_pay != C::n_pay ||
+        P.join.jtype != WG_JOIN_INNER)
+      return false;
     for (int p = 0; p < C::n_pay; ++p)
       if (P.join.pay[p].cls != C::pay_cls(p) || P.join.pay[p].valid != nullptr) return false;
   }

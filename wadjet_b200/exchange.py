@@ -71,13 +71,16 @@ def route_hash_packed(lo: np.ndarray, hi: np.ndarray) -> np.ndarray:
     return out
 
 
-def pack_key_words(keys: np.ndarray, layout) -> tuple[np.ndarray, np.ndarray]:
+def pack_key_words(keys: np.ndarray, layout, key_valid: np.ndarray | None = None) -> tuple[np.ndarray, np.ndarray]:
     """(lo, hi) packed words of unpacked key columns, placed as buildPackedLayout does
-    (exec/packed_hash.go:386); `layout` carries key_word / key_shift / key_i32 per column."""
+    (exec/packed_hash.go:386); `layout` carries key_word / key_shift / key_i32 per column.
+    A NULL column (key_valid 0) contributes no value bits."""
     lo = np.zeros(keys.shape[1], np.uint64)
     hi = np.zeros(keys.shape[1], np.uint64)
     for k in range(keys.shape[0]):
         v = keys[k].astype(np.int64)
+        if key_valid is not None:
+            v = np.where(key_valid[k].astype(bool), v, 0)
         w = (v.astype(np.uint32).astype(np.uint64) << np.uint64(layout.key_shift[k])) if layout.key_i32[k] \
             else v.astype(np.uint64)
         if layout.key_word[k] == 0:
