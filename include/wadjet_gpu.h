@@ -229,6 +229,70 @@ WG_API void*     wg_ctx_stream(wg_ctx* ctx);
 WG_API int64_t   wg_ctx_launch_count(wg_ctx* ctx);
 
 /* ======================================================================== */
+/* Batches on the device: the scan's hand-off to the pipeline                */
+/* (internal/planner/physical/plan.go:11096-11115)                          */
+/* ======================================================================== */
+typedef struct wg_batch wg_batch;
+
+/* Upload a decoded host batch: device copies of every column (data, validity)
+ * and of the selection vector, charged to the context's ledger
+ * (memory.Tracker, tracker.go:53); WG_E_NOMEM when they do not fit. */
+WG_API wg_status wg_batch_upload(wg_ctx* ctx, const wg_batch_desc* host, wg_batch** out);
+/* The batch's device descriptor, for the "_device" entry points; its pointers
+ * stay valid until wg_batch_destroy. cols must have room for the batch's
+ * columns (*out->ncols on return). */
+WG_API wg_status wg_batch_device_desc(wg_batch* b, wg_batch_desc* out, wg_column* cols, int32_t max_cols);
+WG_API wg_status wg_batch_destroy(wg_batch* b);
+
+/* ---- Parquet pages decoded on the device -------------------------------- */
+/* Encodings of a page's values section (parquet.Encoding values,
+ * internal/storage/parquet/page_reader.go:610-640). */
+#define WG_ENC_PLAIN             0
+#define WG_ENC_PLAIN_DICTIONARY  2
+#define WG_ENC_RLE_DICTIONARY    8
+
+/* One data page of a flat column, after decompression (the reader's Decompress
+ * step stays on the host). def_levels: the RLE / bit-packed hybrid definition
+ * levels (bit width 1) of an optional column, NULL for a required one; a row is
+ * NULL where its level is 0. data: the values section, i.e. PLAIN values of the
+ * page's non-NULL rows (physical width: 4 bytes for INT32-class and FLOAT, 8
+ * for INT64-class, DOUBLE and DECIMAL's INT64), or for a dictionary encoding
+ * one bit-width byte followed by the hybrid-encoded indices (rle.go). */
+typedef struct wg_page {
+  int32_t        encoding;
+  int32_t        _pad;
+  int64_t        num_values;   /* rows of the page, NULLs included */
+  const uint8_t* def_levels;
+  int64_t        def_len;
+  const uint8_t* data;
+  int64_t        data_len;
+} wg_page;
+
+/* A column chunk: its pages in order and its dictionary page's values (PLAIN,
+ * physical width, dict_len entries; NULL without one). type_id is the
+ * column's logical type; a DECIMAL chunk holds INT64 physical values that
+ * decode to Int128 as Int128From does (scan/columnar_native.go:619-625). */
+typedef struct wg_column_chunk {
+  int32_t        type_id;
+  int32_t        scale;
+  int32_t        n_pages;
+  int32_t        _pad;
+  const wg_page* pages;
+  const void*    dict;
+  int64_t        dict_len;
+} wg_column_chunk;
+
+/* Decode column chunks into a device batch, one column per chunk, every chunk
+ * with the same row count: the native scan's page decode and copy into a
+ * batch.Vector (ColumnPageReader.decodeValues, page_reader.go:607; dictionary
+ * gather with its index bounds check, columnar_native.go:470-520;
+ * copyNativeDataDirect, :612) on the GPU. Page and dictionary bytes are host
+ * memory; only these encoded bytes cross to the device. A malformed page
+ * (levels or indices that end early, an index past the dictionary, PLAIN data
+ * shorter than its values) fails with WG_E_INVALID. */
+WG_API wg_status wg_batch_decode(wg_ctx* ctx, const wg_column_chunk* chunks, int32_t n_chunks, wg_batch** out);
+
+/* ======================================================================== */
 /* Filter: exec.KernelFilter (internal/engine/exec/filter.go:347-425) with    */
 /* kernel.ResolveFilterKernel / compareFilterImpl (kernel/compare.go:47,145)  */
 /* ======================================================================== */

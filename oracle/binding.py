@@ -92,6 +92,8 @@ def lib() -> C.CDLL:
             "or_gen_groupby": (None, [C.c_uint64, I64, I64, I64, P, P, P, P, I32]),
             "or_gen_highcard": (None, [C.c_uint64, I64, I64, P, P, P, P, I32]),
             "or_i128_to_f64": (C.c_double, [I64, C.c_uint64, I32]),
+            "or_rle_decode": (I64, [P, I64, I32, I64, P]),
+            "or_page_decode": (C.c_int, [P, P, P]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -300,3 +302,23 @@ def gen_highcard(n, seed=42, row0=0, threads=8):
 
 def i128_to_f64(hi, lo, scale) -> float:
     return lib().or_i128_to_f64(int(hi), int(lo) & ((1 << 64) - 1), scale)
+
+
+def rle_decode(data: bytes, bit_width: int, count: int) -> np.ndarray:
+    """DecodeRLEInt32 (rle.go): the hybrid stream's values (fewer than count when it ends early)."""
+    buf = np.frombuffer(bytes(data), np.uint8) if len(data) else np.zeros(1, np.uint8)
+    out = np.zeros(max(1, count), np.int32)
+    n = lib().or_rle_decode(buf.ctypes.data, len(data), bit_width, count, out.ctypes.data)
+    if n < 0:
+        raise RuntimeError(_err())
+    return out[:n].copy()
+
+
+def page_decode(chunk, rows: int, out_dtype):
+    """A column chunk (wadjet_b200._abi.wg_column_chunk) decoded on the CPU: (values, valid bool per row)."""
+    out = np.zeros(max(1, rows), out_dtype)
+    words = np.zeros(max(1, (rows + 63) // 64), np.uint64)
+    if lib().or_page_decode(C.byref(chunk), out.ctypes.data, words.ctypes.data) != 0:
+        raise RuntimeError(_err())
+    valid = np.unpackbits(words.view(np.uint8), bitorder="little")[:rows].astype(bool)
+    return out[:rows], valid

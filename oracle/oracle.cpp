@@ -725,6 +725,69 @@ int run_worker(const wg_batch_desc& in, int32_t nf, const wg_predicate* filters,
   return 0;
 }
 
+// ---------------------------------------------------------------------------
+// Parquet page decode (internal/storage/parquet/rle.go, page_reader.go:607-690,
+// engine/scan/columnar_native.go:470-640)
+// ---------------------------------------------------------------------------
+// decodeBitPackedRange (rle.go:214-250): value i of a run reads up to four
+// little-endian bytes from its first byte, bytes past the run reading as zero.
+void bitpacked_range(int32_t* dst, const uint8_t* data, int64_t len, int bw, int64_t from, int64_t n) {
+  if (bw == 0) { for (int64_t i = 0; i < n; ++i) dst[i] = 0; return; }
+  const int32_t mask = bw >= 32 ? -1 : (int32_t)((1u << bw) - 1u);
+  int64_t bit = from * bw;
+  for (int64_t i = 0; i < n; ++i) {
+    const int64_t byte = bit / 8;
+    const int sh = (int)(bit % 8);
+    uint32_t raw = 0;
+    const int64_t rem = len - byte;
+    for (int k = 0; k < 4; ++k)
+      if (k < rem) raw |= (uint32_t)data[byte + k] << (8 * k);
+    dst[i] = (int32_t)(raw >> sh) & mask;
+    bit += bw;
+  }
+}
+
+// DecodeRLEInt32Into / decodeAllBatch (rle.go:219-300): returns the values
+// decoded (fewer than count when the stream ends), or -1 on a truncated varint
+// or a repeated value missing its bytes.
+int64_t rle_decode(const uint8_t* data, int64_t len, int bw, int64_t count, int32_t* dst) {
+  int64_t off = 0, pos = 0;
+  const int vbytes = (bw + 7) / 8;
+  while (off < len && pos < count) {
+    uint64_t h = 0;
+    unsigned shift = 0;
+    for (;;) {
+      if (off >= len) return -1;                 // varint truncated
+      const uint8_t b = data[off++];
+      h |= (uint64_t)(b & 0x7F) << shift;
+      if (!(b & 0x80)) break;
+      shift += 7;
+      if (shift >= 64) return -1;                // varint overflow
+    }
+    if ((h & 1) == 0) {
+      const int64_t c = (int64_t)(h >> 1);
+      if (off + vbytes > len) return -1;
+      int32_t v = 0;
+      for (int i = 0; i < vbytes; ++i) v |= (int32_t)data[off + i] << (8 * i);
+      off += vbytes;
+      const int64_t end = std::min(count, pos + c);
+      for (int64_t i = pos; i < end; ++i) dst[i] = v;
+      pos = end;
+    } else {
+      const int64_t groups = (int64_t)(h >> 1);
+      if (groups <= 0) continue;
+      if (groups > INT64_MAX / 8 || (bw > 0 && groups > INT64_MAX / bw)) return -1;
+      int64_t nv = std::min(groups * 8, count - pos);
+      int64_t bc = groups * bw;
+      if (off + bc > len) bc = len - off;
+      bitpacked_range(dst + pos, data + off, bc, bw, 0, nv);
+      off += bc;
+      pos += nv;
+    }
+  }
+  return pos;
+}
+
 template <typename F>
 void par_for(int64_t n, int32_t threads, F f) {
   if (threads <= 1 || n < 65536) { f(0, n); return; }
@@ -743,6 +806,69 @@ extern "C" {
 const char* or_last_error(void) { return g_err.c_str(); }
 
 double or_i128_to_f64(int64_t hi, uint64_t lo, int32_t scale) { return i128_to_f64(I128{hi, lo}, scale); }
+
+int64_t or_rle_decode(const uint8_t* data, int64_t len, int32_t bw, int64_t count, int32_t* out) {
+  return rle_decode(data, len, bw, count, out);
+}
+
+// One column chunk's pages into a host column (out: rows * element size;
+// valid_words: (rows + 63) / 64 words or NULL): definition levels to validity
+// (level 1 = a value), the values section decoded (PLAIN, or dictionary
+// indices with the gather loops' bounds check, columnar_native.go:470-520) and
+// written to the non-NULL rows in order, INT64 DECIMAL widened with
+// Int128From (columnar_native.go:619-625). Returns 0, or -1 on a malformed page.
+int or_page_decode(const wg_column_chunk* ch, void* out, uint64_t* valid_words) {
+  const int cls = cls_of(ch->type_id);
+  const int64_t es = ch->type_id == WG_TYPE_DECIMAL ? 8 : (cls == C_I32 || cls == C_F32) ? 4 : 8;
+  const int64_t oes = ch->type_id == WG_TYPE_DECIMAL ? 16 : es;
+  int64_t row0 = 0;
+  for (int p = 0; p < ch->n_pages; ++p) {
+    const wg_page& pg = ch->pages[p];
+    const int64_t n = pg.num_values;
+    std::vector<int32_t> lv((size_t)n, 1);
+    if (pg.def_levels) {
+      if (rle_decode(pg.def_levels, pg.def_len, 1, n, lv.data()) != n) return fail("definition levels end early");
+    }
+    int64_t nn = 0;
+    for (int64_t i = 0; i < n; ++i) nn += lv[(size_t)i] == 1;
+    std::vector<uint8_t> vals((size_t)(nn * es));
+    if (pg.encoding == WG_ENC_PLAIN) {
+      if (pg.data_len < nn * es) return fail("PLAIN data shorter than its values");
+      if (nn) std::memcpy(vals.data(), pg.data, (size_t)(nn * es));
+    } else if (nn > 0) {
+      if (pg.data_len < 1 || pg.data[0] > 32) return fail("dictionary page without a bit width");
+      std::vector<int32_t> idx((size_t)nn);
+      if (rle_decode(pg.data + 1, pg.data_len - 1, pg.data[0], nn, idx.data()) != nn)
+        return fail("fewer dictionary indices than values");
+      for (int64_t k = 0; k < nn; ++k) {
+        if ((uint64_t)(uint32_t)idx[(size_t)k] >= (uint64_t)ch->dict_len) return fail("dictionary index out of range");
+        std::memcpy(&vals[(size_t)(k * es)], (const uint8_t*)ch->dict + (int64_t)(uint32_t)idx[(size_t)k] * es, (size_t)es);
+      }
+    }
+    int64_t k = 0;
+    for (int64_t i = 0; i < n; ++i) {
+      const int64_t r = row0 + i;
+      uint8_t* o = (uint8_t*)out + r * oes;
+      const bool valid = lv[(size_t)i] == 1;
+      if (valid_words) {
+        if (valid) valid_words[r >> 6] |= 1ULL << (r & 63);
+        else valid_words[r >> 6] &= ~(1ULL << (r & 63));
+      }
+      if (!valid) { std::memset(o, 0, (size_t)oes); continue; }
+      if (ch->type_id == WG_TYPE_DECIMAL) {
+        int64_t v;
+        std::memcpy(&v, &vals[(size_t)(k * es)], 8);
+        const wg_int128 d{v < 0 ? -1 : 0, (uint64_t)v};
+        std::memcpy(o, &d, 16);
+      } else {
+        std::memcpy(o, &vals[(size_t)(k * es)], (size_t)es);
+      }
+      ++k;
+    }
+    row0 += n;
+  }
+  return 0;
+}
 
 int64_t or_filter(const wg_column* col, int64_t len, const uint32_t* sel, int64_t sel_len, const wg_predicate* p,
                   uint32_t* out_sel) {

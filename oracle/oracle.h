@@ -76,6 +76,15 @@ void    or_gen_groupby(uint64_t seed, int64_t row0, int64_t n, int64_t ngroups, 
 void    or_gen_highcard(uint64_t seed, int64_t row0, int64_t n, int32_t* a, int64_t* b,
                         wg_int128* amt, double* x, int32_t threads);
 
+/* The Parquet RLE / bit-packed hybrid (rle.go DecodeRLEInt32Into): values
+ * decoded into out (fewer than count when the stream ends), -1 on a malformed
+ * stream. */
+int64_t or_rle_decode(const uint8_t* data, int64_t len, int32_t bit_width, int64_t count, int32_t* out);
+/* A column chunk's pages decoded into a host column and validity words (the
+ * native scan's page decode, page_reader.go:607, columnar_native.go:470-640);
+ * 0, or -1 on a malformed page. */
+int     or_page_decode(const wg_column_chunk* chunk, void* out, uint64_t* valid_words);
+
 /* Int128.ToFloat64 (batch/decimal.go:39) for fixture checks. */
 double  or_i128_to_f64(int64_t hi, uint64_t lo, int32_t scale);
 

@@ -149,6 +149,43 @@ ROUND_TRIP = {
 }
 
 
+# ---- Parquet RLE / bit-packed hybrid: internal/storage/parquet/rle_test.go -----------------------------
+def _le16(*vals):
+    out = []
+    for v in vals:
+        out += [v & 0xFF, v >> 8]
+    return out
+
+
+def _varint(v):
+    out = []
+    while v >= 0x80:
+        out.append((v & 0x7F) | 0x80)
+        v >>= 7
+    return out + [v]
+
+
+# (ref, stream bytes, bit width, count, expected values). Bit-packed vectors of
+# TestDecodeBitPacked are wrapped as one bit-packed run (header (groups << 1) | 1)
+# of the stream the hybrid decoder reads.
+RLE = [
+    ("internal/storage/parquet/rle_test.go:17 (1bit_8values)", [3, 0b10110010], 1, 8, [0, 1, 0, 0, 1, 1, 0, 1]),
+    ("internal/storage/parquet/rle_test.go:23 (2bit_4values)", [3, 0b11100100, 0, 0, 0, 0, 0, 0, 0][:3], 2, 4,
+     [0, 1, 2, 3]),
+    ("internal/storage/parquet/rle_test.go:47 (0bit)", [3], 0, 5, [0, 0, 0, 0, 0]),
+    ("internal/storage/parquet/rle_test.go:52 (8bit)", [3, 10, 20, 30, 0, 0, 0, 0, 0], 8, 3, [10, 20, 30]),
+    ("internal/storage/parquet/rle_test.go:57 (16bit)", [3] + _le16(1000, 2000) + [0] * 12, 16, 2, [1000, 2000]),
+    ("internal/storage/parquet/rle_test.go:91 (TestRLERun)", [20, 42], 8, 10, [42] * 10),
+    ("internal/storage/parquet/rle_test.go:112 (TestRLERunMultiByte)", [10, 0x2C, 0x01], 16, 5, [300] * 5),
+    ("internal/storage/parquet/rle_test.go:134 (TestRLEBitPackedRun)", [3, 10, 20, 30, 40, 50, 60, 70, 80], 8, 8,
+     [10, 20, 30, 40, 50, 60, 70, 80]),
+    ("internal/storage/parquet/rle_test.go:154 (TestRLEMixed)", [8, 0, 3, 0x55], 1, 12,
+     [0, 0, 0, 0, 1, 0, 1, 0, 1, 0, 1, 0]),
+    ("internal/storage/parquet/rle_test.go:217 (TestRLEBitWidth1)", _varint(100 << 1) + [1], 1, 100, [1] * 100),
+    ("internal/storage/parquet/rle_test.go:239 (TestRLEEmpty)", [], 8, 0, []),
+]
+
+
 def main() -> None:
     out = {
         "filters": [dict(ref=r, type=t, values=v, nulls=n, sel=s, op=o, const=c, expect=e)
@@ -162,6 +199,7 @@ def main() -> None:
         "packed_layout": PACKED_LAYOUT,
         "extreme_keys": EXTREME_KEYS,
         "round_trip": ROUND_TRIP,
+        "rle": [dict(ref=r, data=d, bit_width=b, count=c, expect=e) for r, d, b, c, e in RLE],
     }
     path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "known_answers.json")
     with open(path, "w") as f:

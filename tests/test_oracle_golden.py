@@ -146,3 +146,47 @@ def test_packed_round_trip_values():
     agg.consume(ob.HostBatch([(1, i32, None, 0), (2, i64, None, 0)]))
     e = agg.export()
     assert sorted(zip(e["keys"][0].tolist(), e["keys"][1].tolist())) == sorted(zip(i32.tolist(), i64.tolist()))
+
+
+@pytest.mark.parametrize("case", GOLD["rle"], ids=lambda c: c["ref"])
+def test_rle_hybrid_known_answers(case):
+    """The oracle's RLE / bit-packed hybrid decoder on the reference's rle_test.go vectors."""
+    got = ob.rle_decode(bytes(case["data"]), case["bit_width"], case["count"])
+    assert got.tolist() == case["expect"]
+
+
+@pytest.mark.parametrize("bw", [1, 3, 7, 12, 20, 32])
+def test_page_encoder_round_trips_through_the_oracle(bw):
+    """wadjet_b200.pages writes hybrid streams the oracle's decoder reads back, runs of
+    repeated values and bit-packed stretches alike."""
+    from wadjet_b200 import pages
+    rng = np.random.default_rng(bw)
+    top = (1 << bw) - 1
+    v = rng.integers(0, top + 1, 5000, dtype=np.int64)
+    v[1000:1400] = top          # a long repeated run
+    v[2000:2005] = 0            # a short one, bit-packed
+    enc = pages.encode_hybrid(v, bw)
+    np.testing.assert_array_equal(ob.rle_decode(enc, bw, len(v)), v.astype(np.int32))
+
+
+def test_page_decode_oracle_plain_dictionary_and_nulls():
+    """The oracle's page decode: PLAIN and dictionary pages, NULL rows from the levels,
+    DECIMAL INT64 widened to Int128 (Int128From)."""
+    from tests.helpers import dec_array
+    from wadjet_b200 import pages
+    rng = np.random.default_rng(9)
+    n = 3000
+    vals = rng.integers(-50, 50, n).astype(np.int64)
+    valid = rng.random(n) > 0.2
+    for dictionary in (False, True):
+        ch = pages.chunk(vals, 2, valid, page_rows=1000, dictionary=dictionary)
+        out, ok = ob.page_decode(ch.to_c(), n, np.int64)
+        np.testing.assert_array_equal(ok, valid)
+        np.testing.assert_array_equal(out[valid], vals[valid])
+        assert (out[~valid] == 0).all()
+    dec = dec_array(vals)
+    ch = pages.chunk(dec, 17, None, page_rows=700, dictionary=True, scale=2)
+    out, ok = ob.page_decode(ch.to_c(), n, dec.dtype)
+    assert ok.all()
+    np.testing.assert_array_equal(out["lo"], dec["lo"])
+    np.testing.assert_array_equal(out["hi"], dec["hi"])

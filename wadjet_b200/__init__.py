@@ -31,7 +31,7 @@ from ._abi import (AGG_AVG, AGG_COUNT, AGG_MAX, AGG_MIN, AGG_SUM, CONST_FLOAT, C
                    TYPE_INT32, TYPE_INT64, TYPE_IPV4, TYPE_MAC, TYPE_PORT, TYPE_PROTOCOL, TYPE_TIMESTAMP)
 
 __all__ = [
-    "Context", "Column", "Batch", "KernelFilter", "HashJoin", "HashAggregate", "AggColumn", "Expr", "run_pipeline",
+    "Context", "Column", "Batch", "DeviceBatch", "KernelFilter", "HashJoin", "HashAggregate", "AggColumn", "Expr", "run_pipeline",
     "WadjetGPUError", "MemoryExceeded", "Cancelled", "DEC_DTYPE", "lib",
 ]
 
@@ -147,6 +147,61 @@ class Batch:
         d = abi.wg_batch_desc(len(self.cols), 0, arr, self.len, sel_ptr, sel_len)
         keep.append(d)
         return d, keep
+
+
+class _DevColType:
+    """Type facts of a device-batch column (what run_pipeline reads from a column)."""
+
+    def __init__(self, type_id: int, scale: int, n: int):
+        self.type_id, self.scale, self._n = type_id, scale, n
+
+    def __len__(self) -> int:
+        return self._n
+
+
+class DeviceBatch:
+    """A batch resident on the device (wg_batch): uploaded from a decoded host batch
+    (`upload`) or decoded on the GPU from Parquet column chunks (`decode`). It stands
+    in for a device-resident Batch in run_pipeline(..., device=True)."""
+
+    def __init__(self, ctx: "Context", h, ncols: int):
+        self.ctx, self.h = ctx, h
+        cols = (abi.wg_column * max(1, ncols))()
+        d = abi.wg_batch_desc()
+        _check(lib.wg_batch_device_desc(h, C.byref(d), cols, ncols))
+        self._d, self._arr = d, cols
+        self.len = d.len
+        self.sel = None
+        self.cols = [_DevColType(cols[i].type_id, cols[i].scale, d.len) for i in range(ncols)]
+
+    @classmethod
+    def upload(cls, ctx: "Context", batch: Batch) -> "DeviceBatch":
+        d, keep = batch.desc()
+        h = C.c_void_p()
+        _check(lib.wg_batch_upload(ctx.h, C.byref(d), C.byref(h)))
+        return cls(ctx, h, len(batch.cols))
+
+    @classmethod
+    def decode(cls, ctx: "Context", chunks) -> "DeviceBatch":
+        """chunks: wadjet_b200.pages.Chunk objects, one per column."""
+        cs = [c.to_c() for c in chunks]
+        arr = (abi.wg_column_chunk * len(cs))(*cs)
+        h = C.c_void_p()
+        _check(lib.wg_batch_decode(ctx.h, arr, len(cs), C.byref(h)))
+        return cls(ctx, h, len(cs))
+
+    def desc(self):
+        return self._d, [self._arr]
+
+    def column_pointer(self, i: int) -> tuple[int, int]:
+        """(data, validity words) device addresses of column i (0 when it has no NULLs)."""
+        c = self._arr[i]
+        return int(c.data or 0), int(c.valid_words or 0)
+
+    def close(self) -> None:
+        if self.h:
+            lib.wg_batch_destroy(self.h)
+            self.h = None
 
 
 class Context:

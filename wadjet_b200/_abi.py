@@ -21,6 +21,8 @@ CONST_INT, CONST_FLOAT = 0, 1
 # exec.AggFunc
 AGG_SUM, AGG_COUNT, AGG_MIN, AGG_MAX, AGG_AVG = range(5)
 JOIN_INNER, JOIN_LEFT, JOIN_SEMI, JOIN_ANTI = 0, 1, 5, 6
+# parquet.Encoding of a page's values section
+ENC_PLAIN, ENC_PLAIN_DICTIONARY, ENC_RLE_DICTIONARY = 0, 2, 8
 # expression opcodes
 EXPR_COL, EXPR_CONST_I, EXPR_CONST_F, EXPR_ADD, EXPR_SUB, EXPR_MUL, EXPR_DIV, EXPR_SHR, EXPR_AND = range(9)
 EXPR_MAX_OPS = 12
@@ -77,6 +79,16 @@ class wg_batched_query(C.Structure):
 class wg_tune_params(C.Structure):
     _fields_ = [("tile_rows", C.c_int32), ("block", C.c_int32), ("ctas_per_sm", C.c_int32),
                 ("smem_max_groups", C.c_int32), ("max_load", C.c_double)]
+
+
+class wg_page(C.Structure):
+    _fields_ = [("encoding", C.c_int32), ("_pad", C.c_int32), ("num_values", C.c_int64),
+                ("def_levels", C.c_void_p), ("def_len", C.c_int64), ("data", C.c_void_p), ("data_len", C.c_int64)]
+
+
+class wg_column_chunk(C.Structure):
+    _fields_ = [("type_id", C.c_int32), ("scale", C.c_int32), ("n_pages", C.c_int32), ("_pad", C.c_int32),
+                ("pages", C.POINTER(wg_page)), ("dict", C.c_void_p), ("dict_len", C.c_int64)]
 
 
 class wg_state_layout(C.Structure):
@@ -144,6 +156,10 @@ SIGNATURES = {
     "wg_agg_export": (I32, [P, C.POINTER(wg_group_export)]),
     "wg_agg_reset": (I32, [P]),
     "wg_agg_kernel_shape": (I32, [P]),
+    "wg_batch_upload": (I32, [P, C.POINTER(wg_batch_desc), PP]),
+    "wg_batch_device_desc": (I32, [P, C.POINTER(wg_batch_desc), C.POINTER(wg_column), I32]),
+    "wg_batch_destroy": (I32, [P]),
+    "wg_batch_decode": (I32, [P, C.POINTER(wg_column_chunk), I32, PP]),
     "wg_agg_state_layout": (I32, [P, C.POINTER(wg_state_layout)]),
     "wg_agg_partition_state": (I32, [P, I32, P, I64, PI64]),
     "wg_agg_merge_state": (I32, [P, C.POINTER(wg_state_layout), P, I64]),

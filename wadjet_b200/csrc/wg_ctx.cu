@@ -95,6 +95,7 @@ wg_status check_device_error(Ctx* ctx) {
     case WG_DERR_TIMEOUT: return fail(WG_E_TIMEOUT, "bounded device wait expired");
     case WG_DERR_NULL_PACKED: return fail(WG_E_UNSUPPORTED, "NULL in a composite GROUP BY key");
     case WG_DERR_STACK: return fail(WG_E_INVALID, "malformed expression program");
+    case WG_DERR_BAD_PAGE: return fail(WG_E_INVALID, "malformed Parquet page");
     default: return fail(WG_E_CUDA, "device error " + std::to_string(h));
   }
 }

@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "wadjet_gpu.h"
+
 // storage classes of the column types the GPU path reads
 #define WG_CLS_I32 0   // Int32Data: INT32, PORT, PROTOCOL, DATE
 #define WG_CLS_I64 1   // Int64Data: INT64, TIMESTAMP, IPV4, MAC, DURATION
@@ -18,6 +20,7 @@
 #define WG_DERR_TIMEOUT     2   // a bounded wait gave up
 #define WG_DERR_NULL_PACKED 3   // NULL in a composite (packed) group key
 #define WG_DERR_STACK       4   // malformed expression program
+#define WG_DERR_BAD_PAGE    5   // a Parquet page whose levels, indices or values are malformed
 
 #define WG_FULL_MASK 0xFFFFFFFFu
 
