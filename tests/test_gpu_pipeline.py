@@ -208,6 +208,7 @@ def test_highcard_workload_matches_oracle(ctx, tile, spec, part, monkeypatch):
     monkeypatch.setenv("WG_TILE", tile)
     monkeypatch.setenv("WG_SPECIALIZE", spec)
     monkeypatch.setenv("WG_AGG_PARTITION", part)
+    monkeypatch.setenv("WG_AGG_HC", "0")  # the one-table paths; the two-level mode is tested below
     n = (1 << 22) + 1234
     a, b, amt, x = synth.highcard(ctx, n)
     aggs = [wg.AggColumn(wg.AGG_SUM, 2), wg.AggColumn(wg.AGG_COUNT, -1), wg.AggColumn(wg.AGG_MIN, 3),
@@ -222,6 +223,50 @@ def test_highcard_workload_matches_oracle(ctx, tile, spec, part, monkeypatch):
     ob.pipeline(ob.HostBatch([(I32, ha, None, 0), (I64, hb, None, 0), (DEC, hamt, None, 2), (F64, hx, None, 0)]),
                 o, threads=8)
     assert_groups_equal(g.export(), o.export(), ["sum_d", "count", "min_f", "max_f"])
+    g.close()
+
+
+@pytest.mark.parametrize("spec,bucket_groups,out_cap", [("1", 0, 0), ("0", 0, 0), ("1", 20000, 0), ("1", 0, 4096)])
+def test_highcard_two_level_matches_oracle(ctx, spec, bucket_groups, out_cap, monkeypatch):
+    """The two-level partitioned mode (first-level runs in HBM, buckets aggregated in shared
+    memory) on 2^22 + 1234 rows, ~3.9M groups, in two consume calls: compiled and generic
+    bucket kernels; buckets sized past their shared table (later new groups spill to the HBM
+    table); a compact result sized too small at first (replayed larger)."""
+    import wadjet_b200 as wg
+    from wadjet_b200 import synth
+    monkeypatch.setenv("WG_SPECIALIZE", spec)
+    if bucket_groups:
+        monkeypatch.setenv("WG_HC_BUCKET_GROUPS", str(bucket_groups))
+    if out_cap:
+        monkeypatch.setenv("WG_HC_OUT_CAP", str(out_cap))
+    n = (1 << 22) + 1234
+    a, b, amt, x = synth.highcard(ctx, n)
+    aggs = [wg.AggColumn(wg.AGG_SUM, 2), wg.AggColumn(wg.AGG_COUNT, -1), wg.AggColumn(wg.AGG_MIN, 3),
+            wg.AggColumn(wg.AGG_MAX, 3)]
+    g = wg.HashAggregate(ctx, [0, 1], aggs, ndv_hint=1 << 22)
+    cut = 1 << 22  # the first call decides the mode: at least 2^22 rows
+    for r0, r1 in ((0, cut), (cut, n)):
+        batch = wg.Batch([wg.Column(I32, a[r0:r1]), wg.Column(I64, b[r0:r1]), wg.Column(DEC, amt[r0:r1], scale=2),
+                          wg.Column(F64, x[r0:r1])])
+        wg.run_pipeline(ctx, batch, g, device=True)
+    g.finalize()
+    assert g.kernel_shape == (SHAPE_HIGHCARD if spec == "1" else 0)
+    ha, hb, hamt, hx = a.cpu().numpy(), b.cpu().numpy(), to_host_dec(amt), x.cpu().numpy()
+    o = ob.Agg([0, 1], [(0, 2, 0), (1, -1, 0), (2, 3, 0), (3, 3, 0)])
+    ob.pipeline(ob.HostBatch([(I32, ha, None, 0), (I64, hb, None, 0), (DEC, hamt, None, 2), (F64, hx, None, 0)]),
+                o, threads=8)
+    want = o.export()
+    assert_groups_equal(g.export(), want, ["sum_d", "count", "min_f", "max_f"])
+    # the same aggregate again after a reset (kept buffers), then merged into a fresh one
+    g.reset()
+    batch = wg.Batch([wg.Column(I32, a), wg.Column(I64, b), wg.Column(DEC, amt, scale=2), wg.Column(F64, x)])
+    wg.run_pipeline(ctx, batch, g, device=True)
+    g.finalize()
+    m = g.clone_sink()
+    m.merge_sink(g)
+    m.finalize()
+    assert_groups_equal(m.export(), want, ["sum_d", "count", "min_f", "max_f"])
+    m.close()
     g.close()
 
 

@@ -409,7 +409,6 @@ class HashAggregate:
         self._n_groups = None
         self._out_pos = 0
 
-    @property
     def state_layout(self) -> "abi.wg_state_layout":
         """The row layout of this aggregate's partial state (wg_agg_state_layout)."""
         lay = abi.wg_state_layout()
@@ -435,6 +434,7 @@ class HashAggregate:
         ptr = rows.data_ptr() if n else None
         _check(lib.wg_agg_merge_state(self.h, C.byref(layout), ptr, n))
 
+    @property
     def kernel_shape(self) -> int:
         """Compiled query shape of the last fused launch (0 generic, -1 none yet); a diagnostic only."""
         return int(lib.wg_agg_kernel_shape(self.h))

@@ -14,6 +14,7 @@
 //    the global table at the end of the kernel.
 #include "wg_internal.h"
 #include "wg_launch.cuh"
+#include "wg_hc.cuh"
 
 #include <algorithm>
 #include <cstdlib>
@@ -56,14 +57,16 @@ __device__ __forceinline__ bool slot_used(const Layout& L, const unsigned long l
 
 // Fold every group of table (Ls, Ts) into (Ld, Td): MergeSink, table growth and
 // layout upgrades are all this one kernel.
+// compact_n >= 0: the source is a compact result of compact_n groups (every
+// row a group; a key equal to the empty pattern is that key's group).
 template <int NA>
-__global__ void fold_kernel(Layout Ls, Table Ts, Layout Ld, Table Td, int32_t* err) {
+__global__ void fold_kernel(Layout Ls, Table Ts, Layout Ld, Table Td, int32_t* err, int64_t compact_n) {
   Credit cr;
-  const uint64_t cap = Ts.mask + 1;
-  const uint64_t n = Ls.key_words == 0 ? 1 : cap + 2;
+  const uint64_t cap = compact_n >= 0 ? ~0ULL - 2 : Ts.mask + 1;
+  const uint64_t n = compact_n >= 0 ? (uint64_t)compact_n : Ls.key_words == 0 ? 1 : cap + 2;
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
     const unsigned long long* s = Ts.slots + i * Ls.slot_words;
-    if (!slot_used(Ls, s, i, cap)) continue;
+    if (compact_n < 0 && !slot_used(Ls, s, i, cap)) continue;
     unsigned long long k0 = 0, k1 = 0;
     bool knull = false;
     if (Ls.key_words >= 1) {
@@ -354,8 +357,8 @@ __global__ void state_merge_kernel(Layout Ls, const unsigned long long* rows, in
 
 template <int NA>
 void launch_fold(const Layout& Ls, const Table& Ts, const Layout& Ld, const Table& Td, int32_t* err, unsigned grid,
-                 cudaStream_t st) {
-  fold_kernel<NA><<<grid, 256, 0, st>>>(Ls, Ts, Ld, Td, err);
+                 cudaStream_t st, int64_t compact_n = -1) {
+  fold_kernel<NA><<<grid, 256, 0, st>>>(Ls, Ts, Ld, Td, err, compact_n);
 }
 
 unsigned grid_cap(wg::Ctx* ctx, int64_t n, int block, int per_sm = 16) {
@@ -431,6 +434,25 @@ struct wg_agg {
   wg::DevBuf part_counts, part_offs;
   char* exp_host = nullptr;
   int64_t exp_host_bytes = 0;
+  // Two-level partitioned mode (wg_hc.cuh), for tables far larger than L2:
+  // each consume call writes its filtered rows, as the columns the aggregate
+  // reads, to a first-level run in HBM; finalize re-partitions the runs into
+  // buckets and aggregates each bucket in one SM's shared memory, leaving a
+  // compact result that stands in for the table (`spilled`).
+  bool hc = false;
+  int hc_b1 = 0, hc_b2 = 0;
+  bool hc_hist_zero = true;         // the bucket histogram must be cleared before the next count
+  std::vector<int32_t> hc_cols;     // copy columns: caller-numbered virtual columns (keys, then agg inputs)
+  std::vector<int32_t> hc_es, hc_cls;
+  struct HcRun {
+    int64_t rows = 0;
+    std::vector<int64_t> off1;      // first-level partition starts (np1 + 1)
+    std::vector<wg::DevBuf> cols;
+  };
+  std::vector<HcRun> hc_runs;
+  std::vector<HcRun> hc_free;       // runs of earlier queries, kept for reuse
+  std::vector<wg::DevBuf> hc_copy2;
+  wg::DevBuf hc_hist, hc_counts1, hc_offs1, hc_dev, hc_out, hc_scalars;
   ~wg_agg() {
     for (auto& b : host_blocks) cudaFreeHost(b.first);
     if (exp_host) cudaFreeHost(exp_host);
@@ -528,12 +550,13 @@ static uint64_t cap_for(int64_t groups) {
 
 static int log2u(uint64_t v) { int l = 0; while ((1ULL << l) < v) ++l; return l; }
 
-static void run_fold(wg_agg* a, const wgd::Layout& Ls, const wgd::Table& Ts, const wgd::Layout& Ld, const wgd::Table& Td) {
+static void run_fold(wg_agg* a, const wgd::Layout& Ls, const wgd::Table& Ts, const wgd::Layout& Ld, const wgd::Table& Td,
+                     int64_t compact_n = -1) {
   Ctx* ctx = a->ctx;
-  const int64_t n = Ls.key_words == 0 ? 1 : (int64_t)(Ts.mask + 3);
+  const int64_t n = compact_n >= 0 ? std::max<int64_t>(compact_n, 1) : Ls.key_words == 0 ? 1 : (int64_t)(Ts.mask + 3);
   const unsigned grid = grid_cap(ctx, n, 256);
-  if (Ls.n_aggs <= 4) launch_fold<4>(Ls, Ts, Ld, Td, ctx->dev_error, grid, ctx->stream);
-  else launch_fold<8>(Ls, Ts, Ld, Td, ctx->dev_error, grid, ctx->stream);
+  if (Ls.n_aggs <= 4) launch_fold<4>(Ls, Ts, Ld, Td, ctx->dev_error, grid, ctx->stream, compact_n);
+  else launch_fold<8>(Ls, Ts, Ld, Td, ctx->dev_error, grid, ctx->stream, compact_n);
   ctx->count_launch();
 }
 
@@ -650,7 +673,10 @@ static wg_status agg_resolve(wg_agg* a, const VSchema& vs) {
   if (na > WG_MAX_AGGS) return fail(WG_E_UNSUPPORTED, "more than 8 aggregates");
   build_layout(a);
   if (a->L.slot_words > WG_MAX_SLOT_WORDS) return fail(WG_E_UNSUPPORTED, "aggregate state too wide");
-  a->cap = a->L.key_words == 0 ? 1 : cap_for(std::max<int64_t>(a->hint, 1024));
+  // the two-level mode keeps only the groups that outgrow a bucket's shared
+  // table in HBM: a small table, grown on demand
+  a->cap = a->L.key_words == 0 ? 1 : cap_for(a->hc ? (int64_t(1) << 16) : std::max<int64_t>(a->hint, 1024));
+  if (a->hc) a->small_cap = a->cap;
   a->shift = 64 - log2u(a->cap);
   wg_status st = init_table(a, a->table, a->cap);
   if (st == WG_E_NOMEM && a->L.key_words >= 1 && a->ctx->pinned_spill_bytes > 0 && env_int("WG_AGG_SPILL", 1) != 0) {
@@ -897,6 +923,9 @@ static wg_status build_plan(const PipelineRun& r, wgd::Plan& P, VSchema& vs, std
 static wg_status run_partitioned(const PipelineRun& r, const wgd::Plan& P0, const std::vector<int>& in_map,
                                  bool* done);
 static wg_status spill_consume(const PipelineRun& r, const wgd::Plan& P0, const std::vector<int>& in_map);
+static bool hc_eligible(const PipelineRun& r, const wgd::Plan& P);
+static wg_status hc_consume(const PipelineRun& r, const wgd::Plan& P0);
+static wg_status agg_compact(wg_agg* a);
 
 // Run the fused kernel over a device-resident input with the overflow policy.
 static wg_status run_device(const PipelineRun& r) {
@@ -907,12 +936,17 @@ static wg_status run_device(const PipelineRun& r) {
   VSchema vs;
   std::vector<int> in_map;
   WG_TRY(build_plan(r, ls.P, vs, in_map));
-  if (!a->resolved) WG_TRY(agg_resolve(a, vs));
-  else WG_TRY(agg_check_nullable(a, vs));
+  if (!a->resolved) {
+    a->hc = hc_eligible(r, ls.P);
+    WG_TRY(agg_resolve(a, vs));
+  } else {
+    WG_TRY(agg_check_nullable(a, vs));
+  }
   ls.P.err = ctx->dev_error;
   const int64_t n_items = ls.P.n_items;
   if (n_items == 0) return WG_OK;
   const int64_t fan = r.join ? std::max<int64_t>(1, join_max_fanout(r.join)) : 1;
+  if (a->hc && !r.no_partition) return hc_consume(r, ls.P);
   if (a->spill && !r.no_partition) return spill_consume(r, ls.P, in_map);
   if (!r.no_partition) {
     bool done = false;
@@ -939,7 +973,8 @@ static wg_status run_device(const PipelineRun& r) {
   const int env_bps = env_int("WG_AGG_BLOCKS_PER_SM", 0);
   const int pref_bps = env_bps > 0 ? env_bps : 2;
   int blocks_per_sm = pref_bps;
-  ls.block = ls.vec ? 512 : stat ? wgd::StatShape<wgd::ShapeStarJoin>::kBlock : wgd::DynShape::kBlock;
+  ls.block = ls.vec ? (env_int("WG_VEC_BLOCK", 512) == 768 ? 768 : 512)
+                    : stat ? wgd::StatShape<wgd::ShapeStarJoin>::kBlock : wgd::DynShape::kBlock;
   // copies of each float SUM per shared slot (lane-striped, see apply)
   int n_fsum = 0;
   for (int i = 0; i < a->L.n_aggs; ++i) n_fsum += a->L.agg[i].kind == wgd::K_SUM_F64;
@@ -1277,6 +1312,306 @@ static wg_status run_partitioned(const PipelineRun& r, const wgd::Plan& P0, cons
   return WG_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Two-level partitioned mode (wg_hc.cuh)
+// ---------------------------------------------------------------------------
+// Rows the mode needs before it pays (smaller inputs fit the direct path).
+constexpr int64_t kHcMinRows = int64_t(1) << 22;
+// Groups a bucket is sized for: the shared table's slots hold about twice that.
+constexpr int64_t kHcBucketGroups = 1800;
+
+// Large-table GROUP BY on a plain input: no join, no selection vector, no
+// validity bitmaps (a NULL key has no bucket), one or more integer keys, and a
+// table for the expected groups of at least 64 MB (WG_AGG_HC=0 turns it off).
+static bool hc_eligible(const PipelineRun& r, const wgd::Plan& P) {
+  wg_agg* a = r.agg;
+  if (env_int("WG_AGG_HC", 1) == 0 || r.join || P.sel || a->key_cols.empty() || P.n_items < kHcMinRows) return false;
+  for (int j = 0; j < P.n_in; ++j)
+    if (P.in[j].valid) return false;
+  if ((int)a->specs.size() > WG_MAX_AGGS) return false;
+  const int64_t words = (int64_t)a->key_cols.size() + 1 + 2 * (int64_t)a->specs.size();
+  if ((int64_t)cap_for(std::max<int64_t>(a->hint, 1024)) * words * 8 < (int64_t(64) << 20)) return false;
+  // room for the first-level run and the second-level copy of the input, and the result
+  int64_t row_bytes = 0;
+  for (int j = 0; j < P.n_in; ++j) row_bytes += wgd::cls_bytes(P.in[j].cls);
+  const int64_t need = 2 * P.n_items * row_bytes + std::max<int64_t>(a->hint, 1024) * words * 8 * 5 / 4;
+  const Ledger& L = a->ctx->ledger;
+  return L.budget() <= 0 || L.budget() - L.used() >= need;
+}
+
+// The copy's column j as a plan input: class and element size from the plan
+// that wrote it.
+static wg_status hc_setup(wg_agg* a, const PipelineRun& r, const wgd::Plan& P0) {
+  a->hc_cols.clear();
+  auto add = [&](int32_t c) {
+    if (c < 0) return;
+    for (int32_t x : a->hc_cols) if (x == c) return;
+    a->hc_cols.push_back(c);
+  };
+  for (int32_t k : a->key_cols) add(k);
+  for (const wg_agg_spec& sp : a->specs) add(sp.input_col);
+  if ((int)a->hc_cols.size() > WG_MAX_IN) return fail(WG_E_UNSUPPORTED, "more than 8 grouped or aggregated columns");
+  a->hc_cls.clear();
+  a->hc_es.clear();
+  (void)r;
+  (void)P0;
+  const int64_t expect = std::max<int64_t>(a->hint, 1024);
+  const int64_t per_bucket = std::max(16, env_int("WG_HC_BUCKET_GROUPS", (int)kHcBucketGroups));
+  int bits = 0;
+  while (bits < 15 && (expect >> bits) > per_bucket) ++bits;
+  bits = std::max(bits, 4);
+  a->hc_b1 = std::min(bits, 8);
+  a->hc_b2 = bits - a->hc_b1;
+  return WG_OK;
+}
+
+// A plan over the copy's columns: inputs are the copy columns, keys and
+// aggregates point at them, no filters, projections or join.
+static wgd::Plan hc_plan(wg_agg* a, const std::vector<wg::DevBuf>& cols, int64_t n) {
+  wgd::Plan P;
+  std::memset(&P, 0, sizeof(P));
+  P.n_in = (int32_t)a->hc_cols.size();
+  for (int j = 0; j < P.n_in; ++j) {
+    P.in[j] = wgd::DCol{cols[(size_t)j].get(), nullptr, a->hc_cls[(size_t)j], 0};
+    P.vcls[j] = a->hc_cls[(size_t)j];
+    pow10_divisor_host(0, &P.vdiv_b[j], &P.vdiv_y[j]);
+  }
+  P.L = a->L;
+  auto idx = [&](int32_t c) -> int32_t {
+    for (size_t j = 0; j < a->hc_cols.size(); ++j) if (a->hc_cols[j] == c) return (int32_t)j;
+    return -1;
+  };
+  for (size_t k = 0; k < a->key_cols.size(); ++k) P.L.key_vcol[k] = idx(a->key_cols[k]);
+  for (size_t i = 0; i < a->specs.size(); ++i) P.L.agg[i].vcol = idx(a->specs[i].input_col);
+  P.n_items = n;
+  P.err = a->ctx->dev_error;
+  return P;
+}
+
+// One consume call: count the rows per partition and bucket, then write them
+// to a first-level run.
+static wg_status hc_consume(const PipelineRun& r, const wgd::Plan& P0) {
+  wg_agg* a = r.agg;
+  Ctx* ctx = a->ctx;
+  if (a->hc_cols.empty()) WG_TRY(hc_setup(a, r, P0));
+  wgd::Plan P = P0;
+  P.L = launch_layout(a, P0);
+  P.err = ctx->dev_error;
+  const int np1 = 1 << a->hc_b1, nb = 1 << (a->hc_b1 + a->hc_b2);
+  // the copy columns in this call's compact numbering
+  wgd::HcCols out{};
+  out.n = (int32_t)a->hc_cols.size();
+  std::vector<int32_t> cls((size_t)out.n);
+  for (int j = 0; j < out.n; ++j) {
+    const int32_t c = a->hc_cols[(size_t)j];
+    int32_t v = -1;
+    for (size_t k = 0; k < a->key_cols.size(); ++k) if (a->key_cols[k] == c) v = P.L.key_vcol[k];
+    for (size_t i = 0; i < a->specs.size() && v < 0; ++i) if (a->specs[i].input_col == c) v = P.L.agg[i].vcol;
+    if (v < 0) return fail(WG_E_INVALID, "grouped column missing from the plan");
+    out.vcol[j] = v;
+    cls[(size_t)j] = P.vcls[v];
+    out.es[j] = wgd::cls_bytes(P.vcls[v]);
+  }
+  if (a->hc_cls.empty()) { a->hc_cls = cls; for (int j = 0; j < out.n; ++j) a->hc_es.push_back(out.es[j]); }
+  else if (a->hc_cls != cls) return fail(WG_E_INVALID, "column classes changed between consume calls");
+  const unsigned grid = (unsigned)ctx->sm_count;
+  WG_TRY(a->hc_counts1.ensure(ctx, (int64_t)np1 * grid * 4));
+  WG_TRY(a->hc_offs1.ensure(ctx, (int64_t)np1 * grid * 8));
+  WG_TRY(a->hc_hist.ensure(ctx, (int64_t)nb * 8));
+  if (a->hc_hist_zero) {
+    WG_CUDA_TRY(cudaMemsetAsync(a->hc_hist.get(), 0, (size_t)nb * 8, ctx->stream));
+    a->hc_hist_zero = false;
+  }
+  const size_t cs = wgd::hc_count_smem(np1, nb);
+  WG_CUDA_TRY(cudaFuncSetAttribute(wgd::hc_count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cs));
+  wgd::hc_count_kernel<<<grid, wgd::kPartThreads, cs, ctx->stream>>>(P, a->hc_b1, a->hc_b2, a->hc_counts1.as<uint32_t>(),
+                                                                       a->hc_hist.as<unsigned long long>());
+  ctx->count_launch();
+  WG_CUDA_TRY(cudaGetLastError());
+  std::vector<uint32_t> hc((size_t)np1 * grid);
+  std::vector<unsigned long long> ho((size_t)np1 * grid);
+  WG_CUDA_TRY(cudaMemcpyAsync(hc.data(), a->hc_counts1.get(), hc.size() * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  WG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  wg_agg::HcRun run;
+  if (!a->hc_free.empty()) { run = std::move(a->hc_free.back()); a->hc_free.pop_back(); }
+  run.off1.assign((size_t)np1 + 1, 0);
+  unsigned long long acc = 0;
+  for (int p = 0; p < np1; ++p) {
+    run.off1[(size_t)p] = (int64_t)acc;
+    for (unsigned c = 0; c < grid; ++c) { ho[(size_t)p * grid + c] = acc; acc += hc[(size_t)p * grid + c]; }
+  }
+  run.off1[(size_t)np1] = (int64_t)acc;
+  run.rows = (int64_t)acc;
+  if (run.rows > P.n_items) return fail(WG_E_CUDA, "partition counts exceed the input rows");
+  WG_CUDA_TRY(cudaMemcpyAsync(a->hc_offs1.get(), ho.data(), ho.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
+  if ((int)run.cols.size() < out.n) run.cols.resize((size_t)out.n);
+  for (int j = 0; j < out.n; ++j) {
+    WG_TRY(run.cols[(size_t)j].ensure(ctx, std::max<int64_t>(run.rows, 1) * out.es[j]));
+    out.data[j] = run.cols[(size_t)j].as<char>();
+  }
+  const size_t ss = wgd::hc_scatter_smem(np1);
+  WG_CUDA_TRY(cudaFuncSetAttribute(wgd::hc_scatter1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss));
+  wgd::hc_scatter1_kernel<<<grid, wgd::kPartThreads, ss, ctx->stream>>>(P, a->hc_b1, a->hc_offs1.as<unsigned long long>(),
+                                                                          out);
+  ctx->count_launch();
+  WG_CUDA_TRY(cudaGetLastError());
+  a->hc_runs.push_back(std::move(run));
+  return check_device_error(ctx);
+}
+
+template <int NA, class Sh>
+static void launch_hc_bucket(const wgd::Plan& P, size_t smem, const int64_t* boff, int64_t nb, unsigned long long* out,
+                             unsigned long long* cursor, int64_t cap, int32_t* over, unsigned grid, cudaStream_t st) {
+  cudaFuncSetAttribute(wgd::hc_bucket_kernel<NA, Sh>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  wgd::hc_bucket_kernel<NA, Sh><<<grid, 1024, smem, st>>>(P, boff, nb, out, cursor, cap, over);
+}
+
+// Finalize of the two-level mode: the runs re-partitioned into buckets, the
+// buckets aggregated into a compact result, the groups that outgrew their
+// bucket's shared table appended from the HBM table; the result then stands
+// in for the table.
+static wg_status hc_finish(wg_agg* a) {
+  Ctx* ctx = a->ctx;
+  const int b1 = a->hc_b1, b2 = a->hc_b2;
+  const int np1 = 1 << b1, np2 = 1 << b2;
+  const int64_t nb = int64_t(1) << (b1 + b2);
+  const int ncol = (int)a->hc_cols.size();
+  const int sw = a->L.slot_words;
+  int64_t rows = 0;
+  for (const auto& r : a->hc_runs) rows += r.rows;
+  // bucket starts in the second copy
+  std::vector<unsigned long long> hist((size_t)nb);
+  WG_CUDA_TRY(cudaMemcpyAsync(hist.data(), a->hc_hist.get(), (size_t)nb * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  WG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  std::vector<int64_t> boff((size_t)nb + 1);
+  int64_t acc = 0;
+  for (int64_t b = 0; b < nb; ++b) { boff[(size_t)b] = acc; acc += (int64_t)hist[(size_t)b]; }
+  boff[(size_t)nb] = acc;
+  if (acc != rows) return fail(WG_E_CUDA, "bucket counts do not add up to the partitioned rows");
+  // device scratch: boff (nb + 1), cursors (nb), then per run off1 and item0 (np1 + 1 each)
+  const int64_t scal = (nb + 1) + nb + 2 * ((int64_t)np1 + 1);
+  WG_TRY(a->hc_dev.ensure(ctx, scal * 8));
+  int64_t* d_boff = a->hc_dev.as<int64_t>();
+  unsigned long long* d_cur = (unsigned long long*)(d_boff + nb + 1);
+  int64_t* d_off1 = (int64_t*)(d_cur + nb);
+  int64_t* d_item0 = d_off1 + np1 + 1;
+  WG_CUDA_TRY(cudaMemcpyAsync(d_boff, boff.data(), (size_t)(nb + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
+  WG_CUDA_TRY(cudaMemcpyAsync(d_cur, boff.data(), (size_t)nb * 8, cudaMemcpyHostToDevice, ctx->stream));
+  if ((int)a->hc_copy2.size() < ncol) a->hc_copy2.resize((size_t)ncol);
+  wgd::HcCols out2{};
+  out2.n = ncol;
+  for (int j = 0; j < ncol; ++j) {
+    WG_TRY(a->hc_copy2[(size_t)j].ensure(ctx, std::max<int64_t>(rows, 1) * a->hc_es[(size_t)j]));
+    out2.data[j] = a->hc_copy2[(size_t)j].as<char>();
+    out2.es[j] = a->hc_es[(size_t)j];
+    out2.vcol[j] = j;
+  }
+  const size_t ss = wgd::hc_scatter_smem(np2);
+  WG_CUDA_TRY(cudaFuncSetAttribute(wgd::hc_scatter2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss));
+  for (auto& run : a->hc_runs) {
+    if (run.rows == 0) continue;
+    std::vector<int64_t> item0((size_t)np1 + 1);
+    int64_t items = 0;
+    for (int p = 0; p < np1; ++p) {
+      item0[(size_t)p] = items;
+      items += (run.off1[(size_t)p + 1] - run.off1[(size_t)p] + wgd::kPartTile - 1) / wgd::kPartTile;
+    }
+    item0[(size_t)np1] = items;
+    WG_CUDA_TRY(cudaMemcpyAsync(d_off1, run.off1.data(), (size_t)(np1 + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
+    WG_CUDA_TRY(cudaMemcpyAsync(d_item0, item0.data(), (size_t)(np1 + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
+    wgd::Plan Pc = hc_plan(a, run.cols, run.rows);
+    const unsigned grid = (unsigned)std::min<int64_t>((int64_t)ctx->sm_count * 3, std::max<int64_t>(items, 1));
+    wgd::hc_scatter2_kernel<<<grid, wgd::kPartThreads, ss, ctx->stream>>>(Pc, b1, b2, d_off1, d_item0, np1, items, d_cur,
+                                                                           out2);
+    ctx->count_launch();
+    WG_CUDA_TRY(cudaGetLastError());
+    // the next run's offsets reuse the same device words
+    WG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  }
+  // buckets into the compact result
+  wgd::Plan Pb = hc_plan(a, a->hc_copy2, rows);
+  int n_fsum = 0;
+  for (int i = 0; i < a->L.n_aggs; ++i) n_fsum += a->L.agg[i].kind == wgd::K_SUM_F64;
+  const int rep = n_fsum > 0 ? 2 : 1;
+  const int ssw = (sw + n_fsum * (rep - 1)) | 1;
+  const int S = (int)std::min<int64_t>(((int64_t)ctx->max_smem_optin - 2048) / (ssw * 8), 1 << 14);
+  Pb.smem_slots = S;
+  Pb.smem_sw = ssw;
+  Pb.smem_rep = rep;
+  Pb.smem_hash_shift = b1 + b2;
+  const size_t smem = (size_t)S * ssw * 8;
+  WG_TRY(a->hc_scalars.ensure(ctx, 64));
+  unsigned long long* d_ocur = a->hc_scalars.as<unsigned long long>();
+  int32_t* d_over = (int32_t*)(d_ocur + 1);
+  int64_t cap = std::max<int64_t>(1024, std::min<int64_t>(rows, std::max<int64_t>(a->hint, a->known_groups) * 5 / 4 + 65536));
+  if (env_int("WG_HC_OUT_CAP", 0) > 0) cap = env_int("WG_HC_OUT_CAP", 0);  // a small first guess (replay paths)
+  wgd::Plan probe = Pb;
+  const bool stat = wgd::shape_matches<wgd::ShapeHighCard>(probe) && env_int("WG_SPECIALIZE", 1) != 0;
+  a->last_shape = stat ? wgd::SHAPE_HIGHCARD : wgd::SHAPE_GENERIC;
+  for (int attempt = 0; attempt < 8; ++attempt) {
+    WG_TRY(a->hc_out.ensure(ctx, cap * sw * 8));
+    WG_CUDA_TRY(cudaMemsetAsync(a->hc_scalars.get(), 0, 64, ctx->stream));
+    Pb.T = table_view(a);
+    const unsigned grid = (unsigned)ctx->sm_count;
+    if (stat) launch_hc_bucket<4, wgd::StatShape<wgd::ShapeHighCard>>(Pb, smem, d_boff, nb, a->hc_out.as<unsigned long long>(),
+                                                                     d_ocur, cap, d_over, grid, ctx->stream);
+    else if (a->L.n_aggs <= 4) launch_hc_bucket<4, wgd::DynShape>(Pb, smem, d_boff, nb, a->hc_out.as<unsigned long long>(),
+                                                                  d_ocur, cap, d_over, grid, ctx->stream);
+    else launch_hc_bucket<8, wgd::DynShape>(Pb, smem, d_boff, nb, a->hc_out.as<unsigned long long>(), d_ocur, cap,
+                                            d_over, grid, ctx->stream);
+    ctx->count_launch();
+    WG_CUDA_TRY(cudaGetLastError());
+    int64_t v[2], t[2];
+    WG_TRY(read_back_i64(ctx, (const int64_t*)a->hc_scalars.get(), v, 2));
+    WG_TRY(read_back_i64(ctx, (const int64_t*)a->ctr.get(), t, 2));
+    WG_TRY(check_device_error(ctx));
+    const bool out_over = (int32_t)v[1] != 0, tab_over = (int32_t)t[1] != 0;
+    if (!out_over && !tab_over) {
+      // the groups that outgrew their bucket's shared table, appended from the HBM table
+      WG_TRY(agg_compact(a));
+      const int64_t n_sm = v[0], n_tab = a->n_out;
+      if (n_sm + n_tab > cap) {
+        DevBuf bigger;
+        WG_TRY(bigger.alloc(ctx, (n_sm + n_tab) * sw * 8));
+        WG_CUDA_TRY(cudaMemcpyAsync(bigger.get(), a->hc_out.get(), (size_t)(n_sm * sw * 8), cudaMemcpyDeviceToDevice,
+                                    ctx->stream));
+        a->hc_out = std::move(bigger);
+      }
+      if (n_tab > 0) {
+        gather_slots_kernel<<<grid_cap(ctx, n_tab * sw, 256), 256, 0, ctx->stream>>>(
+            a->table.as<unsigned long long>(), sw, a->list.as<int64_t>(), n_tab,
+            a->hc_out.as<unsigned long long>() + n_sm * sw);
+        ctx->count_launch();
+        WG_CUDA_TRY(cudaGetLastError());
+      }
+      const int64_t n_res = n_sm + n_tab;
+      // the compact result becomes the table (every slot a group, no NULL-key slot)
+      std::swap(a->table, a->hc_out);
+      a->cap = uint64_t(1) << 62;
+      a->spilled = true;
+      WG_TRY(a->list.ensure(ctx, std::max<int64_t>(n_res, 1) * 8));
+      iota_kernel<<<grid_cap(ctx, std::max<int64_t>(n_res, 1), 256), 256, 0, ctx->stream>>>(a->list.as<int64_t>(), n_res);
+      ctx->count_launch();
+      WG_CUDA_TRY(cudaGetLastError());
+      a->n_out = n_res;
+      for (auto& r : a->hc_runs) a->hc_free.push_back(std::move(r));
+      a->hc_runs.clear();
+      a->hc_hist_zero = true;
+      return check_device_error(ctx);
+    }
+    // replay: a larger result, or a larger HBM table for the groups that outgrew their buckets
+    if (out_over) cap = std::max<int64_t>(cap * 2, v[0] + 1024);
+    if (tab_over) WG_TRY(rebuild_table(a, a->cap * 4, a->L));
+    const int64_t words = table_words(a, a->cap);
+    init_table_kernel<<<grid_cap(ctx, words, 256), 256, 0, ctx->stream>>>(a->table.as<unsigned long long>(), words,
+                                                                         a->L.slot_words, a->L);
+    ctx->count_launch();
+    WG_CUDA_TRY(cudaMemsetAsync(a->ctr.get(), 0, 64, ctx->stream));
+    a->known_groups = a->upper_groups = 0;
+  }
+  return fail(WG_E_NOMEM, "two-level aggregation did not converge");
+}
+
 // Rows of the partition kernels' plan: the aggregate's key layout, the caller's
 // columns rebased to row r0, m rows.
 static wgd::Plan part_plan(wg_agg* a, const wgd::Plan& P0, int64_t r0, int64_t m) {
@@ -1596,7 +1931,10 @@ wg_status wg_agg_merge(wg_agg* d, wg_agg* s) {
   if (!d || !s) return fail(WG_E_INVALID, "NULL argument");
   if (d->ctx != s->ctx) return fail(WG_E_INVALID, "aggregates belong to different contexts");
   if (d->key_cols != s->key_cols || d->specs.size() != s->specs.size()) return fail(WG_E_INVALID, "aggregate shapes differ");
-  if (d->spill || s->spill) return fail(WG_E_UNSUPPORTED, "spilled aggregations are not merged");
+  // a destination that parks its input in runs (spill, two-level mode) takes no
+  // merges; a source of either kind merges once finalized (its compact result)
+  if (d->spill || d->hc) return fail(WG_E_UNSUPPORTED, "a spilled or two-level aggregation takes no merges");
+  if ((s->spill || s->hc) && !s->spilled) return fail(WG_E_STATE, "finalize a spilled or two-level source first");
   WG_TRY(ensure_device(d->ctx));
   if (d->finalized) return fail(WG_E_STATE, "aggregate already finalized");
   if (!s->resolved) return WG_OK;
@@ -1626,10 +1964,14 @@ wg_status wg_agg_merge(wg_agg* d, wg_agg* s) {
     WG_TRY(rebuild_table(d, d->cap, tmp.L));
   }
   WG_TRY(refresh_groups(d));
-  WG_TRY(refresh_groups(s));
-  const int64_t need = d->known_groups + s->known_groups;
+  int64_t s_groups = s->n_out;
+  if (!s->spilled) {
+    WG_TRY(refresh_groups(s));
+    s_groups = s->known_groups;
+  }
+  const int64_t need = d->known_groups + s_groups + credit_slack(d);
   if (d->L.key_words != 0 && need > (int64_t)((double)d->cap * kMaxLoad)) WG_TRY(rebuild_table(d, cap_for(need), d->L));
-  run_fold(d, s->L, table_view(s), d->L, table_view(d));
+  run_fold(d, s->L, table_view(s), d->L, table_view(d), s->spilled ? s->n_out : -1);
   WG_CUDA_TRY(cudaGetLastError());
   WG_TRY(refresh_groups(d));
   return check_device_error(ctx);
@@ -1646,7 +1988,8 @@ wg_status wg_agg_finalize(wg_agg* a, int64_t* n_groups) {
     return WG_OK;
   }
   if (!a->finalized) {
-    if (a->spill) WG_TRY(spill_finish(a));
+    if (a->hc) WG_TRY(hc_finish(a));
+    else if (a->spill) WG_TRY(spill_finish(a));
     else WG_TRY(agg_compact(a));
     a->finalized = true;
   }
@@ -1789,6 +2132,11 @@ wg_status wg_agg_reset(wg_agg* a) {
     a->runs.clear();
     a->block_idx = 0;
     a->block_used = 0;
+  }
+  if (a->hc) {  // the runs' buffers are kept for the next query
+    for (auto& r : a->hc_runs) a->hc_free.push_back(std::move(r));
+    a->hc_runs.clear();
+    a->hc_hist_zero = true;
   }
   if (a->spilled) {  // the table holds a compact result: back to an empty small table
     a->table.reset();

@@ -100,6 +100,8 @@ struct Plan {
   int32_t minmax_test;           // 1: HBM MIN/MAX read the slot first and skip an atomic that cannot win
   int32_t stage_off;             // self-staged vector kernel: byte offset of the warps' staging buffers
                                  // in dynamic shared memory (after the shared table)
+  int32_t smem_hash_shift;       // shared-table slot from the key hash's bits below the top
+                                 // smem_hash_shift (the bits that picked the rows' bucket)
   DCol in[WG_MAX_IN];
   Pred filt[WG_MAX_FILTERS];
   JoinView join;

@@ -596,16 +596,67 @@ __device__ __forceinline__ unsigned long long* find_smem(unsigned long long* sm,
   return nullptr;
 }
 
-// The shared slot of key k0: direct (k0 - gmin) when the keys' range is known
-// and fits the table, else the hashed table.
+// Shared-table lookups for rows already bucketed by the top `shift` bits of
+// their key hash: the slot comes from the hash bits below those (the top bits
+// are the same for every row of a bucket). One-word keys hash like fib_slot,
+// packed keys like packed_slot; a packed key is installed with one 16-byte CAS
+// (its words change once, from {~0, ~0} to the key, as in find_global).
+__device__ __forceinline__ unsigned long long* find_smem_bucketed(unsigned long long* sm, int S, int sw, int kw,
+                                                                  unsigned long long k0, unsigned long long k1,
+                                                                  int shift, int* s_groups, int s_limit) {
+  unsigned long long h;
+  if (kw == 1) {
+    if (k0 == WG_EMPTY_KEY) return nullptr;
+    h = k0 * 0x9E3779B97F4A7C15ULL;
+  } else {
+    if (k0 == ~0ULL && k1 == ~0ULL) return nullptr;
+    const unsigned long long a = k0 ^ 0x9E3779B97F4A7C15ULL, b = k1 ^ 0x517CC1B727220A95ULL;
+    h = (__umul64hi(a, b) ^ (a * b) ^ (k0 + k1)) * 0x9E3779B97F4A7C15ULL;
+  }
+  uint32_t i = (uint32_t)__umul64hi(shift > 0 ? h << shift : h, (unsigned long long)S);
+  for (int p = 0; p < S; ++p) {
+    unsigned long long* s = sm + (size_t)i * sw;
+    if (kw == 1) {
+      const unsigned long long cur = *((volatile unsigned long long*)s);
+      if (cur == k0) return s;
+      if (cur == WG_EMPTY_KEY) {
+        if (*((volatile int*)s_groups) >= s_limit) return nullptr;
+        const unsigned long long old = atomicCAS(s, WG_EMPTY_KEY, k0);
+        if (old == WG_EMPTY_KEY) { atomicAdd(s_groups, 1); return s; }
+        if (old == k0) return s;
+      }
+    } else {
+      const U128 cur = read128(s);
+      if (cur.lo != ~0ULL && cur.hi != ~0ULL) {
+        if (cur.lo == k0 && cur.hi == k1) return s;
+      } else {
+        if (*((volatile int*)s_groups) >= s_limit) return nullptr;
+        U128 e; e.lo = ~0ULL; e.hi = ~0ULL;
+        U128 k; k.lo = k0; k.hi = k1;
+        const U128 old = cas128((U128*)s, e, k);
+        if (old.lo == e.lo && old.hi == e.hi) { atomicAdd(s_groups, 1); return s; }
+        if (old.lo == k0 && old.hi == k1) return s;
+      }
+    }
+    i = (i + 1 == (uint32_t)S) ? 0u : i + 1;
+  }
+  return nullptr;
+}
+
+// The shared slot of a key: direct (k0 - gmin) when the keys' range is known
+// and fits the table, the bucketed table for rows of one hash bucket, else the
+// hashed one-word table.
 __device__ __forceinline__ unsigned long long* find_shared(const Plan& P, unsigned long long* sm, unsigned long long k0,
-                                                           int* s_groups, int s_limit) {
+                                                           unsigned long long k1, int* s_groups, int s_limit) {
   if (P.gdense) {
     // every key lies in [gmin, gmin + smem_slots), fewer than 2^14 apart: the
     // low 32 bits give the exact offset
     const uint32_t d = (uint32_t)k0 - (uint32_t)P.gmin;
     return d < (uint32_t)P.smem_slots ? sm + d * (uint32_t)smem_stride(P) : nullptr;
   }
+  if (P.smem_hash_shift > 0)
+    return find_smem_bucketed(sm, P.smem_slots, smem_stride(P), P.L.key_words, k0, k1, P.smem_hash_shift, s_groups,
+                              s_limit);
   return find_smem(sm, P.smem_slots, smem_stride(P), k0, s_groups, s_limit);
 }
 
@@ -623,7 +674,7 @@ __device__ __forceinline__ void warp_update(const Plan& P, const Sh& sh, bool cu
                                             unsigned long long* sm, int* s_groups, int s_limit, Credit& cr) {
   const bool combine_first = SMEM && P.smem_combine != 0;
   if (SMEM && !combine_first && cur && !knull) {
-    unsigned long long* s = find_shared(P, sm, k0, s_groups, s_limit);
+    unsigned long long* s = find_shared(P, sm, k0, k1, s_groups, s_limit);
     if (s != nullptr) {
       apply<NA, true>(sh, s, c, 1ULL, smem_copies(P));
       cur = false;
@@ -660,7 +711,7 @@ __device__ __forceinline__ void warp_update(const Plan& P, const Sh& sh, bool cu
   }
   if (leader) {
     if (combine_first && !knull) {
-      unsigned long long* s = find_shared(P, sm, k0, s_groups, s_limit);
+      unsigned long long* s = find_shared(P, sm, k0, k1, s_groups, s_limit);
       if (s != nullptr) {
         apply<NA, true>(sh, s, c, (unsigned long long)mysz, smem_copies(P));
         return;

@@ -2,9 +2,73 @@
 #include "wg_internal.h"
 #include "wg_device.cuh"
 
+#include <condition_variable>
 #include <cstdio>
+#include <thread>
 
 namespace wg {
+
+// ---- host copy threads -------------------------------------------------------
+namespace {
+struct CopyPool {
+  std::mutex mu;
+  std::condition_variable cv_job, cv_done;
+  std::vector<std::thread> threads;
+  // the current job: piece i of n copies [i * per, min(bytes, (i + 1) * per))
+  char* dst = nullptr;
+  const char* src = nullptr;
+  int64_t bytes = 0, per = 0;
+  int n = 0, next = 0, left = 0;
+  uint64_t gen = 0;
+  std::mutex job_mu;  // one job at a time
+  explicit CopyPool(int t) {
+    for (int i = 0; i < t; ++i) threads.emplace_back([this] { run(); });
+  }
+  void run() {
+    std::unique_lock<std::mutex> lk(mu);
+    for (;;) {
+      cv_job.wait(lk, [&] { return next < n; });
+      const int i = next++;
+      char* d = dst;
+      const char* s = src;
+      const int64_t b0 = (int64_t)i * per, b1 = std::min(bytes, b0 + per);
+      lk.unlock();
+      if (b1 > b0) std::memcpy(d + b0, s + b0, (size_t)(b1 - b0));
+      lk.lock();
+      if (--left == 0) cv_done.notify_all();
+    }
+  }
+};
+CopyPool* copy_pool() {
+  // threads live until the process exits (the pool is never destroyed, so no
+  // thread is joined from a static destructor)
+  static CopyPool* p = new CopyPool((int)std::max(1u, std::min(16u, std::thread::hardware_concurrency())));
+  return p;
+}
+}  // namespace
+
+void parallel_copy(void* dst, const void* src, int64_t bytes) {
+  if (bytes <= 0) return;
+  if (bytes < (int64_t(4) << 20)) {
+    std::memcpy(dst, src, (size_t)bytes);
+    return;
+  }
+  CopyPool* p = copy_pool();
+  std::lock_guard<std::mutex> job(p->job_mu);
+  std::unique_lock<std::mutex> lk(p->mu);
+  const int t = (int)p->threads.size();
+  p->dst = (char*)dst;
+  p->src = (const char*)src;
+  p->bytes = bytes;
+  p->per = ((bytes + t - 1) / t + 4095) & ~int64_t(4095);
+  p->n = (int)((bytes + p->per - 1) / p->per);
+  p->next = 0;
+  p->left = p->n;
+  p->cv_job.notify_all();
+  p->cv_done.wait(lk, [&] { return p->left == 0; });
+  p->n = 0;
+  p->next = 0;
+}
 
 thread_local std::string t_err;
 
@@ -167,6 +231,7 @@ static wg_status ctx_make(int32_t device, int64_t budget, wg::Ledger* parent, in
   for (int i = 0; i < 2; ++i) {
     cudaEventCreateWithFlags(&c->staged[i], cudaEventDisableTiming);
     cudaEventCreateWithFlags(&c->consumed[i], cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&c->h2d_done[i], cudaEventDisableTiming);
   }
   cudaMemset(c->dev_error, 0, 256);
   cudaMemset(c->dev_scalar, 0, 64 * sizeof(int64_t));
@@ -206,6 +271,8 @@ wg_status wg_ctx_destroy(wg_ctx* c) {
   for (int i = 0; i < 2; ++i) {
     if (c->staged[i]) cudaEventDestroy(c->staged[i]);
     if (c->consumed[i]) cudaEventDestroy(c->consumed[i]);
+    if (c->h2d_done[i]) cudaEventDestroy(c->h2d_done[i]);
+    c->win[i].reset();
   }
   if (c->pinned) cudaFreeHost(c->pinned);
   if (c->host_scalar) cudaFreeHost(c->host_scalar);

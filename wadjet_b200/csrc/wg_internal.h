@@ -125,10 +125,20 @@ struct Ctx {
   // device-side error word written by bounded waits / invariants
   int32_t* dev_error = nullptr;
   std::mutex mu;                    // serialises scalar read-backs
+  // host-input pipeline runs: two device windows and (for pageable sources) two
+  // pinned slots the host threads fill, kept for the next run; one run at a time
+  std::mutex stage_mu;
+  DevBuf win[2];
+  cudaEvent_t h2d_done[2] = {nullptr, nullptr};
 
   explicit Ctx(int64_t budget, Ledger* parent = nullptr) : ledger(budget, parent) {}
   void count_launch(int n = 1) { launches.fetch_add(n); }
 };
+
+// Copy `bytes` from src to dst with the library's host threads (a pool shared by
+// every context, sized to the host's cores): the pageable-to-pinned leg of
+// host-input staging.
+void parallel_copy(void* dst, const void* src, int64_t bytes);
 
 wg_status ensure_device(Ctx* ctx);           // cudaSetDevice(ctx->device)
 wg_status read_back_i64(Ctx* ctx, const int64_t* dev, int64_t* out, int n);

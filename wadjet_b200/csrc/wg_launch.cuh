@@ -38,6 +38,7 @@ static void launch_vec_one(const LaunchSpec& ls, cudaStream_t st) {
 template <int NA, class Sh, bool SMEM>
 static void launch_vec_s(const LaunchSpec& ls, cudaStream_t st) {
   if (ls.block == 1024) launch_vec_one<NA, SMEM, Sh, 2, 1, 1024>(ls, st);
+  else if (ls.block == 768) launch_vec_one<NA, SMEM, Sh, 2, 2, 768>(ls, st);
   else launch_vec_one<NA, SMEM, Sh, 2, 2, 512>(ls, st);
 }
 
