@@ -146,3 +146,41 @@ def test_cancel_withdraws_queued_requests(ctx, tables):
     for t in ahead + doomed + [after]:
         s.release(t)
     s.close()
+
+
+def test_large_requests_match_oracle_in_the_mix(ctx, tables):
+    """Requests of 1.2 * 10^7 and 3 * 10^7 rows (the configured sizes reach 10^8) served
+    beside small ones: each result equals the oracle's over the same rows."""
+    import torch
+    import wadjet_b200 as wg
+    from wadjet_b200 import synth
+    n = 30_000_000
+    k, v, f, flag = synth.groupby(ctx, n)
+    aggs = [wg.AggColumn(wg.AGG_SUM, 1), wg.AggColumn(wg.AGG_COUNT, -1), wg.AggColumn(wg.AGG_MIN, 2),
+            wg.AggColumn(wg.AGG_MAX, 2)]
+
+    def spec(m):
+        return dict(batch=wg.Batch([wg.Column(I64, k[:m]), wg.Column(I64, v[:m]), wg.Column(F64, f[:m]),
+                                    wg.Column(I32, flag[:m])]), group_by=[0], aggs=aggs,
+                    filters=[(3, wg.OP_LT, 7)], ndv_hint=4096)
+
+    small = templates(wg, tables)
+    s = wg.Server(ctx, 4)
+    sizes = [12_000_000, n]
+    big = [s.submit(**spec(m)) for m in sizes]
+    others = [s.submit(**small[name]) for name in ("join", "ipv4", "groupby") * 3]
+    hk, hv, hf, hflag = (t.cpu().numpy() for t in (k, v, f, flag))
+    for m, t in zip(sizes, big):
+        cnt, _ = s.wait(t, timeout=300.0)
+        got = s.export(t, cnt)
+        s.release(t)
+        o = ob.Agg([0], [(0, 1, 0), (1, -1, 0), (2, 2, 0), (3, 2, 0)])
+        ob.pipeline(ob.HostBatch([(I64, hk[:m], None, 0), (I64, hv[:m], None, 0), (F64, hf[:m], None, 0),
+                                  (I32, hflag[:m], None, 0)]), o, filters=[(3, 2, 7)], threads=8)
+        assert_groups_equal(got, o.export(), KINDS["groupby"])
+    for t in others:
+        s.wait(t, timeout=300.0)
+        s.release(t)
+    s.close()
+    del k, v, f, flag
+    torch.cuda.empty_cache()

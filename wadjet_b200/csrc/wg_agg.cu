@@ -787,6 +787,8 @@ struct PipelineRun {
   int32_t n_exprs;
   const wg_expr* exprs;
   bool no_partition = false;    // set on the reordered copy (hash partitioning runs once)
+  bool defer_check = false;     // a launch that needs no read-back returns without waiting for it
+                                // (windowed host input checks the device error word once, at the end)
 };
 
 namespace wg {
@@ -1157,7 +1159,7 @@ static wg_status run_device(const PipelineRun& r) {
   if (a->L.key_words == 0 || a->upper_groups + n_items * fan <= limit()) {
     WG_TRY(launch_pipeline(a, ls, n_items));
     a->upper_groups += a->L.key_words == 0 ? 0 : n_items * fan;
-    return check_device_error(ctx);
+    return r.defer_check ? WG_OK : check_device_error(ctx);
   }
   // 2) small table: snapshot, run, replay on overflow. Threads that race to
   // insert the same new key each hold a reservation until they lose, so the
@@ -1533,7 +1535,12 @@ static wg_status hc_finish(wg_agg* a) {
   int n_fsum = 0;
   for (int i = 0; i < a->L.n_aggs; ++i) n_fsum += a->L.agg[i].kind == wgd::K_SUM_F64;
   const int rep = n_fsum > 0 ? 2 : 1;
-  const int ssw = (sw + n_fsum * (rep - 1)) | 1;
+  // an odd stride spreads slots over the banks, but a packed key (and an Int128
+  // MIN/MAX) is updated with 16-byte atomics, which need 16-byte aligned slots
+  bool wide = a->L.key_words == 2;
+  for (int i = 0; i < a->L.n_aggs; ++i)
+    wide |= a->L.agg[i].kind == wgd::K_MIN_DEC || a->L.agg[i].kind == wgd::K_MAX_DEC;
+  const int ssw = wide ? ((sw + n_fsum * (rep - 1) + 1) & ~1) : ((sw + n_fsum * (rep - 1)) | 1);
   const int S = (int)std::min<int64_t>(((int64_t)ctx->max_smem_optin - 2048) / (ssw * 8), 1 << 14);
   Pb.smem_slots = S;
   Pb.smem_sw = ssw;
@@ -1864,8 +1871,9 @@ using namespace wg;
 namespace wg {
 // Access for the pipeline entry points (wg_pipeline.cu).
 wg_status agg_run_device(wg_agg* a, const wg_batch_desc* in, int32_t nf, const wg_predicate* f, wg_join* j, int32_t ne,
-                         const wg_expr* e) {
+                         const wg_expr* e, bool defer_check) {
   PipelineRun r{a, in, nf, f, j, ne, e};
+  r.defer_check = defer_check;
   return run_device(r);
 }
 Ctx* agg_ctx(wg_agg* a) { return a->ctx; }

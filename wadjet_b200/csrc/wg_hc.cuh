@@ -250,7 +250,7 @@ __global__ void __launch_bounds__(1024, 1) hc_bucket_kernel(const __grid_constan
                                                             int64_t nb, unsigned long long* out,
                                                             unsigned long long* out_cursor, int64_t out_cap,
                                                             int32_t* out_over) {
-  extern __shared__ unsigned long long sm[];
+  extern __shared__ __align__(16) unsigned long long sm[];
   __shared__ int s_groups;
   __shared__ uint32_t warp_tot[32];
   __shared__ unsigned long long s_base;

@@ -12,7 +12,7 @@
 
 namespace wg {
 wg_status agg_run_device(wg_agg* a, const wg_batch_desc* in, int32_t nf, const wg_predicate* f, wg_join* j, int32_t ne,
-                         const wg_expr* e);
+                         const wg_expr* e, bool defer_check = false);
 Ctx* agg_ctx(wg_agg* a);
 }  // namespace wg
 
@@ -179,7 +179,7 @@ wg_status wg_pipeline_run(wg_ctx* ctx, const wg_pipeline_desc* p) {
     WG_CUDA_TRY(cudaStreamWaitEvent(ctx->stream, ctx->staged[s], 0));
     wg_batch_desc d{ncols, 0, cols[s].data(), m, nullptr, 0};
     for (int c = 0; c < ncols; ++c) cols[s][c].len = m;
-    wg_status st = agg_run_device(p->agg, &d, p->n_filters, p->filters, p->join, p->n_exprs, p->exprs);
+    wg_status st = agg_run_device(p->agg, &d, p->n_filters, p->filters, p->join, p->n_exprs, p->exprs, true);
     if (st != WG_OK) { drain(); return st; }
     WG_CUDA_TRY(cudaEventRecord(ctx->consumed[s], ctx->stream));
     // the next window's host copy overlaps this window's kernel
