@@ -653,23 +653,64 @@ def run_serving(args):
         srv.close()
         return st
 
+    def drive_plain(gaps):
+        """The plain per-query path at the same arrivals: each request, in arrival order,
+        is one wg_pipeline_run_device + finalize on one context (one aggregate kept per
+        template shape, reset between requests), with no server; latency counts from the
+        request's arrival, so a request that arrives while another runs waits."""
+        aggs = {}
+        lat, t_last = [], 0.0
+
+        def agg_for(spec):
+            key = (tuple(spec["group_by"]), tuple((a.func, a.input_col) for a in spec["aggs"]), spec["ndv_hint"])
+            if key not in aggs:
+                aggs[key] = wg.HashAggregate(ctx, spec["group_by"], spec["aggs"], ndv_hint=spec["ndv_hint"])
+            return aggs[key]
+
+        for spec in specs[:12]:  # warm the aggregates (tables and buffers allocated once)
+            a = agg_for(spec)
+            a.reset()
+            wg.run_pipeline(ctx, spec["batch"], a, filters=spec.get("filters", ()), join=spec.get("join"),
+                            exprs=spec.get("exprs", ()), device=True)
+            a.finalize()
+        t0 = time.perf_counter()
+        due = t0
+        for gap, spec in zip(gaps, specs):
+            due += gap
+            while True:
+                left = due - time.perf_counter()
+                if left <= 0:
+                    break
+                time.sleep(left if left > 2e-4 else 0)
+            a = agg_for(spec)
+            a.reset()
+            wg.run_pipeline(ctx, spec["batch"], a, filters=spec.get("filters", ()), join=spec.get("join"),
+                            exprs=spec.get("exprs", ()), device=True)
+            a.finalize()
+            t_last = time.perf_counter()
+            lat.append(t_last - due)
+        for a in aggs.values():
+            a.close()
+        return {"qps": len(lat) / (t_last - t0), "p50_s": float(np.percentile(lat, 50)),
+                "p99_s": float(np.percentile(lat, 99)), "mean_service_s": float("nan")}
+
     sys.setswitchinterval(2e-4)  # the submitting and completing threads hand over quickly
     cont = drive(args.slots, gaps)
-    plain = drive(1, gaps)
+    plain = drive_plain(gaps)
     # capacity: the same requests all queued at once (the server runs saturated)
     burst = np.zeros(min(n_req, 4000))
     cont_sat = drive(args.slots, burst)
-    plain_sat = drive(1, burst)
+    plain_sat = drive_plain(burst)
     print(json.dumps({
         "workload": "serving", "metric": "queries/s", "offered_qps": args.qps, "requests": n_req,
         "value": cont["qps"], "unit": "queries/s", "slots": args.slots,
         "p50_ms": 1e3 * cont["p50_s"], "p99_ms": 1e3 * cont["p99_s"],
         "mean_service_ms": 1e3 * cont["mean_service_s"], "mean_queue_ms": 1e3 * cont["mean_queue_s"],
-        "plain": {"qps": plain["qps"], "p50_ms": 1e3 * plain["p50_s"], "p99_ms": 1e3 * plain["p99_s"],
-                  "mean_service_ms": 1e3 * plain["mean_service_s"]},
+        "plain": {"path": "one wg_pipeline_run_device + finalize per request, in arrival order, no server",
+                  "qps": plain["qps"], "p50_ms": 1e3 * plain["p50_s"], "p99_ms": 1e3 * plain["p99_s"]},
         "capacity_qps": {"served": cont_sat["qps"], "plain": plain_sat["qps"],
                          "served_mean_service_ms": 1e3 * cont_sat["mean_service_s"],
-                         "plain_mean_service_ms": 1e3 * plain_sat["mean_service_s"]},
+                         "plain_p99_ms": 1e3 * plain_sat["p99_s"], "served_p99_ms": 1e3 * cont_sat["p99_s"]},
         "mean_rows_per_request": float(sizes.mean()), "templates": ["groupby", "join+agg", "ipv4 /24"]}),
         flush=True)
     join.close()

@@ -485,11 +485,14 @@ typedef struct wg_batched_query {
   int32_t              n_filters;
   int32_t              n_aggs;
   const wg_predicate*  filters;  /* AND chain on input columns */
-  const int32_t*       key_cols; /* n_keys group columns */
+  const int32_t*       key_cols; /* n_keys group columns (of the virtual schema, as wg_pipeline_desc) */
   int32_t              n_keys;
-  int32_t              _pad;
+  int32_t              n_exprs;  /* projections appended to the virtual schema (0..2) */
   const wg_agg_spec*   aggs;
   int64_t              ndv_hint; /* expected groups; sizes the query's table */
+  wg_join*             join;     /* NULL = no join; else a finished build, probed per row (a fused
+                                    filter + probe + aggregate); it must outlive the batched handle */
+  const wg_expr*       exprs;
 } wg_batched_query;
 
 /* Launch shape and table sizing (picked per workload by the autotuner,

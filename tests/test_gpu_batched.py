@@ -71,3 +71,50 @@ def test_batched_hint_too_small_is_rerun(ctx):
             want = oracle_query(key, val, filt, vt, thr)
             assert_groups_equal(b.export(q, int(counts[q])), want, kinds(vt))
     b.close()
+
+
+def test_batched_queries_with_joins_match_oracle(ctx):
+    """Batched queries that each run filter → hash-join probe → projection → GROUP BY in
+    the one persistent launch (star-join shaped queries over fact slices of uneven sizes,
+    sharing one resident dimension; plain group-by queries mixed in)."""
+    import wadjet_b200 as wg
+    from tests.helpers import DEC_DTYPE
+    from wadjet_b200 import synth
+    nd = 1 << 22
+    key, grp = synth.starjoin_dim(ctx)
+    join = wg.HashJoin(ctx, 0, 0, payload=[1], build_row_hint=nd)
+    join.build([wg.Batch([wg.Column(I32, key), wg.Column(I32, grp)])], device=True)
+    fk, qty, price, disc = synth.starjoin_fact(ctx, 3_000_000)
+    expr = wg.Expr(F64, [wg.Expr.col(2), wg.Expr.const_f(1.0), wg.Expr.col(3), "-", "*"])
+    qs, spans = [], []
+    r0 = 0
+    for q, n in enumerate([10_000, 250_000, 1_700_000, 40_000, 999_999]):
+        b = wg.Batch([wg.Column(I32, fk[r0:r0 + n]), wg.Column(I32, qty[r0:r0 + n]),
+                      wg.Column(DEC, price[r0:r0 + n], scale=2), wg.Column(F64, disc[r0:r0 + n])])
+        qs.append({"batch": b, "group_by": [4], "aggs": [wg.AggColumn(wg.AGG_SUM, 5), wg.AggColumn(wg.AGG_SUM, 2),
+                                                         wg.AggColumn(wg.AGG_COUNT, -1)],
+                   "filters": [(1, wg.OP_GT, 10 + q)], "join": join, "exprs": [expr], "ndv_hint": 1000})
+        spans.append((r0, n, 10 + q))
+        r0 += n
+    plain, host = make_queries(ctx, 3, 200_000)
+    qs += plain
+    bq = wg.BatchedQueries(ctx, qs)
+    counts = bq.run()
+    hkey, hgrp = key.cpu().numpy(), grp.cpu().numpy()
+    oj = ob.Join(nd)
+    oj.append(I32, hkey)
+    hfk, hqty, hdisc = fk.cpu().numpy(), qty.cpu().numpy(), disc.cpu().numpy()
+    hprice = price.cpu().numpy().reshape(-1).view(DEC_DTYPE)
+    for q, (s0, n, thr) in enumerate(spans):
+        o = ob.Agg([4], [(0, 5, 0), (0, 2, 0), (1, -1, 0)])
+        ob.pipeline(ob.HostBatch([(I32, hfk[s0:s0 + n], None, 0), (I32, hqty[s0:s0 + n], None, 0),
+                                  (DEC, hprice[s0:s0 + n], None, 2), (F64, hdisc[s0:s0 + n], None, 0)]), o,
+                    filters=[(1, 4, thr)], join=oj, probe_key=0,
+                    build=ob.HostBatch([(I32, hkey, None, 0), (I32, hgrp, None, 0)]), payload=[1],
+                    exprs=[ob.expr(F64, [("col", 2), ("cf", 1.0), ("col", 3), "-", "*"])], threads=4)
+        assert_groups_equal(bq.export(q, int(counts[q])), o.export(), ["sum_f", "sum_d", "count"])
+    for i, h in enumerate(host):
+        q = len(spans) + i
+        assert_groups_equal(bq.export(q, int(counts[q])), oracle_query(*h), kinds(h[3]))
+    bq.close()
+    join.close()

@@ -421,3 +421,28 @@ def test_nullable_key_filling_128_bits_is_refused(ctx):
         g.consume(wg.Batch([wg.Column(I64, a, a % 7 != 0), wg.Column(I64, a)]))
     assert ei.value.status == wg._abi.WG_E_UNSUPPORTED
     g.close()
+
+
+@pytest.mark.parametrize("n_keys", [7, 900])
+def test_shared_table_float_sums_across_the_fixed_point_range(ctx, n_keys):
+    """Low-cardinality float SUMs accumulate in the shared table as exact fixed point
+    for 2^-12 <= |x| < 2^30 and in float for the rest (zeros, tiny and huge values, both
+    signs): every group's sum equals the oracle's within the reordered-sum bound."""
+    import wadjet_b200 as wg
+    rng = np.random.default_rng(n_keys)
+    n = 400_000
+    k = rng.integers(0, n_keys, n).astype(np.int64)
+    mag = 10.0 ** rng.uniform(-9, 13, n)
+    v = np.where(rng.random(n) < 0.5, -mag, mag)
+    v[rng.random(n) < 0.05] = 0.0
+    v[rng.random(n) < 0.01] = 2.0 ** 30          # the first value past the fixed range
+    v[rng.random(n) < 0.01] = 2.0 ** -12         # the smallest value inside it
+    g = wg.HashAggregate(ctx, [0], [wg.AggColumn(wg.AGG_SUM, 1), wg.AggColumn(wg.AGG_COUNT, -1)], ndv_hint=n_keys)
+    wg.run_pipeline(ctx, wg.Batch([wg.Column(I64, k), wg.Column(F64, v)]), g)
+    g.finalize()
+    o = ob.Agg([0], [(0, 1, 0), (1, -1, 0)])
+    o.consume(ob.HostBatch([(I64, k, None, 0), (F64, v, None, 0)]))
+    m = ob.Agg([0], [(0, 1, 0), (1, -1, 0)])
+    m.consume(ob.HostBatch([(I64, k, None, 0), (F64, np.abs(v), None, 0)]))
+    assert_groups_equal(g.export(), o.export(), ["sum_f", "count"], magnitude=m.export())
+    g.close()

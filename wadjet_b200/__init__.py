@@ -567,9 +567,10 @@ class TuneParams:
 
 
 class BatchedQueries:
-    """Many independent filter + GROUP BY queries run by one persistent launch
+    """Many independent filter + probe + GROUP BY queries run by one persistent launch
     replayed from a CUDA graph. queries: list of dicts with keys
-    batch (device Batch), group_by, aggs (AggColumn), filters [(col, op, value)], ndv_hint."""
+    batch (device Batch), group_by, aggs (AggColumn), filters [(col, op, value)], ndv_hint,
+    and optionally join (a built HashJoin) and exprs (Expr) over the virtual schema."""
 
     def __init__(self, ctx: Context, queries: Sequence[dict], params: Optional[TuneParams] = None):
         self.ctx = ctx
@@ -583,9 +584,13 @@ class BatchedQueries:
             keys = (C.c_int32 * max(1, len(q["group_by"])))(*q["group_by"])
             specs = (abi.wg_agg_spec * max(1, len(q["aggs"])))(*[abi.wg_agg_spec(a.func, a.input_col, a.out_type, 0)
                                                                  for a in q["aggs"]])
-            self._keep += [f, keys, specs]
+            exprs = list(q.get("exprs", ()))
+            ex = (abi.wg_expr * max(1, len(exprs)))(*[e.to_c() for e in exprs])
+            join = q.get("join")
+            self._keep += [f, keys, specs, ex, join]
             arr[i] = abi.wg_batched_query(C.pointer(d), len(q.get("filters", ())), len(q["aggs"]), f, keys,
-                                          len(q["group_by"]), 0, specs, int(q.get("ndv_hint", 0)))
+                                          len(q["group_by"]), len(exprs), specs, int(q.get("ndv_hint", 0)),
+                                          join.h if join is not None else None, ex)
             self.shapes.append((len(q["group_by"]), len(q["aggs"])))
         self._keep.append(arr)
         tp = params or TuneParams()

@@ -73,7 +73,8 @@ class wg_pipeline_desc(C.Structure):
 class wg_batched_query(C.Structure):
     _fields_ = [("input", C.POINTER(wg_batch_desc)), ("n_filters", C.c_int32), ("n_aggs", C.c_int32),
                 ("filters", C.POINTER(wg_predicate)), ("key_cols", C.POINTER(C.c_int32)), ("n_keys", C.c_int32),
-                ("_pad", C.c_int32), ("aggs", C.POINTER(wg_agg_spec)), ("ndv_hint", C.c_int64)]
+                ("n_exprs", C.c_int32), ("aggs", C.POINTER(wg_agg_spec)), ("ndv_hint", C.c_int64),
+                ("join", C.c_void_p), ("exprs", C.POINTER(wg_expr))]
 
 
 class wg_tune_params(C.Structure):

@@ -980,10 +980,14 @@ static wg_status run_device(const PipelineRun& r) {
   // copies of each float SUM per shared slot (lane-striped, see apply)
   int n_fsum = 0;
   for (int i = 0; i < a->L.n_aggs; ++i) n_fsum += a->L.agg[i].kind == wgd::K_SUM_F64;
-  const int max_rep = n_fsum > 0 ? std::max(1, std::min(8, env_int("WG_SMEM_REPLICAS", 4))) : 1;
+  // float SUMs in a shared table: exact fixed-point accumulation (two words
+  // each, 32-bit atomics; WG_SMEM_FIXED=1, the default) or `rep` lane-striped
+  // float copies
+  const bool fixed = n_fsum > 0 && env_int("WG_SMEM_FIXED", 1) != 0;
+  const int max_rep = n_fsum > 0 && !fixed ? std::max(1, std::min(8, env_int("WG_SMEM_REPLICAS", 4))) : 1;
   // an odd number of 8-byte words per shared slot spreads the slots over all
   // 16 bank pairs (an even stride maps them onto a few)
-  auto stride_for = [&](int rep) { return (a->L.slot_words + n_fsum * (rep - 1)) | 1; };
+  auto stride_for = [&](int rep) { return (a->L.slot_words + n_fsum * (fixed ? 2 : rep - 1)) | 1; };
   auto slots_for = [&](int bps, int rep) {
     return (int)std::min<int64_t>(((int64_t)ctx->max_smem_optin / bps - 2048) / (stride_for(rep) * 8), 16384);
   };
@@ -1076,7 +1080,7 @@ static wg_status run_device(const PipelineRun& r) {
     }
   }
   ls.P.smem_slots = ls.smem ? S : 0;
-  ls.P.smem_rep = rep;
+  ls.P.smem_rep = fixed ? -1 : rep;
   ls.P.smem_sw = stride_for(rep);
   ls.smem_bytes = ls.smem ? (size_t)S * ls.P.smem_sw * 8 : 0;
   if (ls.stage) {
@@ -1283,12 +1287,17 @@ static wg_status run_partitioned(const PipelineRun& r, const wgd::Plan& P0, cons
     const int es = cls == WG_CLS_I32 || cls == WG_CLS_F32 ? 4 : cls == WG_CLS_DEC ? 16 : 8;
     if (bufs[(size_t)j].ensure(ctx, n * es) != WG_OK) {  // no room for the copy: run directly
       bufs.clear();
+      set_error("");  // the ledger's refusal is handled here, not reported
       return WG_OK;
     }
     po.data[j] = bufs[(size_t)j].as<char>();
     po.es[j] = es;
   }
-  cudaFuncSetAttribute(wgd::part_scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wgd::part_scatter_smem(np));
+  if (cudaFuncSetAttribute(wgd::part_scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)wgd::part_scatter_smem(np)) != cudaSuccess) {
+    cudaGetLastError();  // the scatter's shared memory is refused: run directly
+    return WG_OK;
+  }
   wgd::part_scatter_kernel<<<grid, wgd::kPartThreads, wgd::part_scatter_smem(np), ctx->stream>>>(P, pbits, 64 - pbits,
                                                                         offs.as<unsigned long long>(), po);
   ctx->count_launch();
@@ -2431,6 +2440,8 @@ struct wg_batched {
   std::vector<wg_batch_desc> inputs;
   std::vector<std::vector<wg_column>> cols;
   std::vector<std::vector<wg_predicate>> filters;
+  std::vector<wg_join*> joins;
+  std::vector<std::vector<wg_expr>> exprs;
   wg_tune_params tp{};
   int max_na = 4;
   bool all_static = false;   // every query runs a compiled shape
@@ -2456,7 +2467,8 @@ static wg_status batched_plan(wg_batched* b) {
   int64_t max_smem_words = 0;
   for (int q = 0; q < n; ++q) {
     wg_agg* a = b->aggs[q];
-    PipelineRun r{a, &b->inputs[q], (int32_t)b->filters[q].size(), b->filters[q].data(), nullptr, 0, nullptr};
+    PipelineRun r{a, &b->inputs[q], (int32_t)b->filters[q].size(), b->filters[q].data(), b->joins[q],
+                  (int32_t)b->exprs[q].size(), b->exprs[q].data()};
     LaunchSpec ls;
     VSchema vs;
     std::vector<int> in_map;
@@ -2583,6 +2595,8 @@ wg_status wg_batched_create(wg_ctx* ctx, int32_t n, const wg_batched_query* qs, 
   b->inputs.resize((size_t)n);
   b->cols.resize((size_t)n);
   b->filters.resize((size_t)n);
+  b->joins.assign((size_t)n, nullptr);
+  b->exprs.resize((size_t)n);
   auto cleanup = [&](wg_status s) { wg_batched_destroy(b); return s; };
   for (int q = 0; q < n; ++q) {
     const wg_batched_query& x = qs[q];
@@ -2592,11 +2606,16 @@ wg_status wg_batched_create(wg_ctx* ctx, int32_t n, const wg_batched_query* qs, 
     b->inputs[q] = *x.input;
     b->inputs[q].cols = b->cols[q].data();
     b->filters[q].assign(x.filters, x.filters + x.n_filters);
+    if (x.n_exprs < 0 || x.n_exprs > WG_MAX_EXPRS || (x.n_exprs > 0 && !x.exprs))
+      return cleanup(fail(WG_E_INVALID, "batched query " + std::to_string(q) + ": bad projections"));
+    b->exprs[q].assign(x.exprs, x.exprs + x.n_exprs);
+    b->joins[q] = x.join;
     wg_status s = wg_agg_create(ctx, x.n_keys, x.key_cols, x.n_aggs, x.aggs, x.ndv_hint, &b->aggs[q]);
     if (s != WG_OK) return cleanup(s);
     wg_agg* a = b->aggs[q];
     // resolve the aggregate against the query's schema, sized for its hint
-    PipelineRun r{a, &b->inputs[q], (int32_t)b->filters[q].size(), b->filters[q].data(), nullptr, 0, nullptr};
+    PipelineRun r{a, &b->inputs[q], (int32_t)b->filters[q].size(), b->filters[q].data(), b->joins[q],
+                  (int32_t)b->exprs[q].size(), b->exprs[q].data()};
     LaunchSpec ls;
     VSchema vs;
     std::vector<int> in_map;

@@ -407,6 +407,53 @@ __device__ __forceinline__ void smem_add_limbs(unsigned* L, int nlimbs, unsigned
   }
 }
 
+// Float SUMs in a shared-memory table can accumulate exactly instead of in
+// float: a finite x with 2^-12 <= |x| < 2^30 is a multiple of 2^-64 below 2^30,
+// so x * 2^64 is an integer below 2^94, added into a 128-bit two's-complement
+// accumulator with 32-bit shared-memory atomics (fast even when many lanes hit
+// one hot group, where 64-bit shared atomics serialise). The sum is exact for
+// fewer than 2^32 rows, and the flush rounds it to float64 once. Values
+// outside that range (zero, tiny, huge, NaN, Inf) add into the slot's float
+// word instead. The result is the correctly rounded sum of the in-range values
+// plus the float sum of the rest: a different summation order from the
+// reference, within the same bound as any reordered float sum.
+__device__ __forceinline__ bool f64_to_fixed(double d, unsigned long long& lo, unsigned long long& hi) {
+  const double ad = fabs(d);
+  if (!(ad >= 0x1p-12 && ad < 0x1p30)) return false;
+  const double y = __dmul_rn(d, 0x1p64);                 // exact: a power-of-two scaling, |y| < 2^94
+  const double a = trunc(__dmul_rn(y, 0x1p-62));         // |a| < 2^32, exact
+  const double r = __dsub_rn(y, __dmul_rn(a, 0x1p62));   // exact: y's bits below 2^62, |r| < 2^62
+  const long long ai = (long long)a, ri = (long long)r;
+  const unsigned long long l0 = (unsigned long long)ai << 62;
+  const long long h0 = ai >> 2;                          // a * 2^62 as (h0:l0)
+  lo = l0 + (unsigned long long)ri;
+  hi = (unsigned long long)(h0 + (ri < 0 ? -1LL : 0LL) + (lo < l0 ? 1LL : 0LL));
+  return true;
+}
+
+// The 128-bit two's-complement integer (hi:lo) times 2^-64, rounded to nearest
+// even once: the top 64 significant bits with a sticky bit for the rest convert
+// exactly as the whole would, then scale by a power of two.
+__device__ __forceinline__ double fixed_to_f64(unsigned long long lo, unsigned long long hi) {
+  if ((long long)hi == ((long long)lo >> 63)) return __dmul_rn(__ll2double_rn((long long)lo), 0x1p-64);
+  const bool neg = (long long)hi < 0;
+  if (neg) {  // magnitude
+    lo = ~lo + 1ULL;
+    hi = ~hi + (lo == 0 ? 1ULL : 0ULL);
+  }
+  double v;
+  if (hi == 0) {  // a magnitude in [2^63, 2^64)
+    v = __dmul_rn(__ull2double_rn(lo), 0x1p-64);
+  } else {
+    const int n = 64 - __clzll((long long)hi);           // bits of the high word, 1..64
+    unsigned long long t = n == 64 ? hi : ((hi << (64 - n)) | (lo >> n));
+    const unsigned long long dropped = n == 64 ? lo : (lo << (64 - n));
+    if (dropped) t |= 1ULL;                               // sticky: only breaks ties
+    v = scalbn(__ull2double_rn(t), n - 64);               // exact power-of-two scaling
+  }
+  return neg ? -v : v;
+}
+
 // Fold a combined contribution into a slot with atomics. SH: the slot is in a
 // CTA-private shared-memory table, where the row count is a 32-bit counter in
 // the low half of its word (a CTA applies fewer than 2^32 rows), integer and
@@ -417,12 +464,15 @@ __device__ __forceinline__ void smem_add_limbs(unsigned* L, int nlimbs, unsigned
 // slot may hold `rep` copies of each float SUM: lane l adds into copy l % rep
 // (copy 0 is the layout's word, copies 1.. follow the slot's regular words),
 // which divides those replays by about `rep`; the flush adds the copies.
+// rep < 0: float SUMs accumulate in fixed point (f64_to_fixed), in two words per
+// float SUM after the slot's regular words.
 template <int NA, bool SH, class Lay>
 __device__ __forceinline__ void apply(const Lay& ly, unsigned long long* s, const Contrib<NA>& c,
                                       unsigned long long rows, int rep = 1, bool test_first = false) {
   const bool test = SH || test_first;  // MIN/MAX: read the slot, skip an atomic that cannot win
   if (SH) atomicAdd((unsigned*)(s + ly.key_words()), (unsigned)rows);
   else atomicAdd(s + ly.key_words(), rows);
+  const bool fix = SH && rep < 0;
   const int copy = SH && rep > 1 ? (int)(threadIdx.x & 31) & (rep - 1) : 0;
   int nf = 0;  // float SUMs before aggregate a
 #pragma unroll
@@ -431,15 +481,23 @@ __device__ __forceinline__ void apply(const Lay& ly, unsigned long long* s, cons
     const int kind = ly.agg_kind(a), off = ly.agg_off(a), noff = ly.agg_null_off(a);
     const unsigned long long w0 = c.w0[a], w1 = c.w1[a];
     unsigned long long* t = s + off;
+    unsigned long long* tf = nullptr;
     if (SH && kind == K_SUM_F64) {
-      if (copy > 0) t = s + ly.slot_words() + nf * (rep - 1) + (copy - 1);
+      if (fix) tf = s + ly.slot_words() + 2 * nf;
+      else if (copy > 0) t = s + ly.slot_words() + nf * (rep - 1) + (copy - 1);
       ++nf;
     }
     switch (kind) {
       case K_SUM_I64:
         if (w0) { if (SH) smem_add_limbs((unsigned*)t, 2, w0, 0); else atomicAdd(t, w0); }
         break;
-      case K_SUM_F64: { const double d = as_f(w0); if (d != 0.0) atomicAdd((double*)t, d); } break;
+      case K_SUM_F64: {
+        const double d = as_f(w0);
+        unsigned long long flo, fhi;
+        if (tf != nullptr && f64_to_fixed(d, flo, fhi)) smem_add_limbs((unsigned*)tf, 4, flo, fhi);
+        else if (d != 0.0) atomicAdd((double*)t, d);
+        break;
+      }
       case K_SUM_DEC:
         if (SH) smem_add_limbs((unsigned*)t, 4, w0, w1);
         else atomic_add128(t, w0, w1);
@@ -573,7 +631,7 @@ __device__ __forceinline__ unsigned long long* find_global(const Lay& ly, const 
 
 // Words per shared slot and copies of each float SUM in it.
 __device__ __forceinline__ int smem_stride(const Plan& P) { return P.smem_sw > 0 ? P.smem_sw : P.L.slot_words; }
-__device__ __forceinline__ int smem_copies(const Plan& P) { return P.smem_rep > 1 ? P.smem_rep : 1; }
+__device__ __forceinline__ int smem_copies(const Plan& P) { return P.smem_rep > 1 ? P.smem_rep : P.smem_rep < 0 ? -1 : 1; }
 
 // CTA-private shared-memory table (single int64 key, no NULL words). Returns
 // nullptr when the key is absent and the table has reached its fill limit.
@@ -861,6 +919,7 @@ __device__ __forceinline__ void smem_table_flush(const Plan& P, const unsigned l
     for (int a = 0; a < NA; ++a) {
       if (a >= P.L.n_aggs || P.L.agg[a].kind != K_SUM_F64) continue;
       double d = as_f(c.w0[a]);
+      if (rep < 0) d = __dadd_rn(fixed_to_f64(s[sw + 2 * nf], s[sw + 2 * nf + 1]), d);
       for (int r = 1; r < rep; ++r) d = __dadd_rn(d, as_f(s[sw + nf * (rep - 1) + (r - 1)]));
       c.w0[a] = as_w(d);
       ++nf;
