@@ -9,7 +9,7 @@ from tests.helpers import assert_groups_equal
 
 pytestmark = pytest.mark.gpu
 
-I32, I64, F64 = 1, 2, 4
+I32, I64, F64, DEC = 1, 2, 4, 17
 
 
 def make_queries(ctx, nq, max_rows, hint_scale=1.0):

@@ -980,10 +980,11 @@ static wg_status run_device(const PipelineRun& r) {
   // copies of each float SUM per shared slot (lane-striped, see apply)
   int n_fsum = 0;
   for (int i = 0; i < a->L.n_aggs; ++i) n_fsum += a->L.agg[i].kind == wgd::K_SUM_F64;
-  // float SUMs in a shared table: exact fixed-point accumulation (two words
-  // each, 32-bit atomics; WG_SMEM_FIXED=1, the default) or `rep` lane-striped
-  // float copies
-  const bool fixed = n_fsum > 0 && env_int("WG_SMEM_FIXED", 1) != 0;
+  // float SUMs in a shared table: `rep` lane-striped float copies, or
+  // (WG_SMEM_FIXED=1) exact fixed-point accumulation in two words each with
+  // 32-bit atomics, order-independent but measured slower on the star join
+  // (3 dependent limb atomics per row against one float atomic)
+  const bool fixed = n_fsum > 0 && env_int("WG_SMEM_FIXED", 0) != 0;
   const int max_rep = n_fsum > 0 && !fixed ? std::max(1, std::min(8, env_int("WG_SMEM_REPLICAS", 4))) : 1;
   // an odd number of 8-byte words per shared slot spreads the slots over all
   // 16 bank pairs (an even stride maps them onto a few)

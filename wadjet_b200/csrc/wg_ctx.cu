@@ -3,6 +3,7 @@
 #include "wg_device.cuh"
 
 #include <condition_variable>
+#include <cstdlib>
 #include <cstdio>
 #include <thread>
 
@@ -42,7 +43,11 @@ struct CopyPool {
 CopyPool* copy_pool() {
   // threads live until the process exits (the pool is never destroyed, so no
   // thread is joined from a static destructor)
-  static CopyPool* p = new CopyPool((int)std::max(1u, std::min(16u, std::thread::hardware_concurrency())));
+  static CopyPool* p = new CopyPool([] {
+    const char* v = std::getenv("WG_COPY_THREADS");  // default: the host's cores, at most 16
+    const int t = v ? std::atoi(v) : (int)std::min(16u, std::thread::hardware_concurrency());
+    return std::max(1, std::min(64, t));
+  }());
   return p;
 }
 }  // namespace

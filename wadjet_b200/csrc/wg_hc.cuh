@@ -151,7 +151,20 @@ __global__ void __launch_bounds__(kPartThreads) hc_scatter1_kernel(const __grid_
     for (int j = 0; j < out.n; ++j) {
       const int es = out.es[j];
       char* dcol = out.data[j];
-      for (uint32_t q = threadIdx.x; q < kept; q += blockDim.x) {
+      if (out.vcol[j] < P.n_in) {  // an input column: its bytes as they are
+        const char* scol = (const char*)P.in[out.vcol[j]].data + t0 * es;
+        for (uint32_t q = threadIdx.x; q < kept; q += blockDim.x) {
+          const int k = perm[q];
+          const uint32_t p = part[k];
+          char* d = dcol + (gcur[p] + (q - loff[p])) * es;
+          const char* sp = scol + (size_t)k * es;
+          if (es == 4) *(uint32_t*)d = __ldg((const uint32_t*)sp);
+          else if (es == 8) *(unsigned long long*)d = __ldg((const unsigned long long*)sp);
+          else *(longlong2*)d = __ldg((const longlong2*)sp);
+        }
+        continue;
+      }
+      for (uint32_t q = threadIdx.x; q < kept; q += blockDim.x) {  // a projection, evaluated per row
         const int k = perm[q];
         const uint32_t p = part[k];
         const SrcGlobal src{t0 + k};

@@ -10,6 +10,8 @@
 // are first copied into pinned slots by host threads, which then overlap both.
 #include "wg_internal.h"
 
+#include <cstdlib>
+
 namespace wg {
 wg_status agg_run_device(wg_agg* a, const wg_batch_desc* in, int32_t nf, const wg_predicate* f, wg_join* j, int32_t ne,
                          const wg_expr* e, bool defer_check = false);
@@ -85,7 +87,8 @@ wg_status wg_pipeline_run(wg_ctx* ctx, const wg_pipeline_desc* p) {
   }
   // windows of rows: a multiple of 64 (validity words stay whole); pageable
   // sources take smaller windows so the pinned slots stay modest
-  const int64_t max_win = pageable ? std::max<int64_t>(1 << 16, ((int64_t(64) << 20) / std::max<int64_t>(row_bytes, 1)) & ~int64_t(63))
+  const int64_t stage_mb = std::max<int64_t>(1, std::getenv("WG_STAGE_WINDOW_MB") ? std::atoll(std::getenv("WG_STAGE_WINDOW_MB")) : 64);
+  const int64_t max_win = pageable ? std::max<int64_t>(1 << 16, ((stage_mb << 20) / std::max<int64_t>(row_bytes, 1)) & ~int64_t(63))
                                    : kWindowRows;
   const int64_t win = std::min<int64_t>(max_win, std::max<int64_t>((n + 63) & ~int64_t(63), 64));
   // one host-input run at a time per context: it owns the context's windows
