@@ -475,7 +475,7 @@ def run_highcard(args, hbm_cap: int = 0):
                       wg.Column(wg.TYPE_DECIMAL, amt, scale=2), wg.Column(wg.TYPE_FLOAT64, x)])
     agg = wg.HashAggregate(ctx, [0, 1], [wg.AggColumn(wg.AGG_SUM, 2), wg.AggColumn(wg.AGG_COUNT, -1),
                                          wg.AggColumn(wg.AGG_MIN, 3), wg.AggColumn(wg.AGG_MAX, 3)],
-                           ndv_hint=1 << 26)
+                           ndv_hint=max(1024, synth.highcard_groups(n)))
     groups = [0]
 
     def step():

@@ -226,12 +226,15 @@ def test_highcard_workload_matches_oracle(ctx, tile, spec, part, monkeypatch):
     g.close()
 
 
-@pytest.mark.parametrize("spec,bucket_groups,out_cap", [("1", 0, 0), ("0", 0, 0), ("1", 20000, 0), ("1", 0, 4096)])
-def test_highcard_two_level_matches_oracle(ctx, spec, bucket_groups, out_cap, monkeypatch):
+@pytest.mark.parametrize("spec,bucket_groups,out_cap,hint", [("1", 0, 0, 1 << 22), ("0", 0, 0, 1 << 22),
+                                                              ("1", 20000, 0, 1 << 22), ("1", 0, 4096, 1 << 22),
+                                                              ("1", 0, 0, 1 << 26)])
+def test_highcard_two_level_matches_oracle(ctx, spec, bucket_groups, out_cap, hint, monkeypatch):
     """The two-level partitioned mode (first-level runs in HBM, buckets aggregated in shared
     memory) on 2^22 + 1234 rows, ~3.9M groups, in two consume calls: compiled and generic
     bucket kernels; buckets sized past their shared table (later new groups spill to the HBM
-    table); a compact result sized too small at first (replayed larger)."""
+    table); a compact result sized too small at first (replayed larger); a hint 16x the real
+    group count (the bucket count comes from the counting pass's distinct-key sketch)."""
     import wadjet_b200 as wg
     from wadjet_b200 import synth
     monkeypatch.setenv("WG_SPECIALIZE", spec)
@@ -243,7 +246,7 @@ def test_highcard_two_level_matches_oracle(ctx, spec, bucket_groups, out_cap, mo
     a, b, amt, x = synth.highcard(ctx, n)
     aggs = [wg.AggColumn(wg.AGG_SUM, 2), wg.AggColumn(wg.AGG_COUNT, -1), wg.AggColumn(wg.AGG_MIN, 3),
             wg.AggColumn(wg.AGG_MAX, 3)]
-    g = wg.HashAggregate(ctx, [0, 1], aggs, ndv_hint=1 << 22)
+    g = wg.HashAggregate(ctx, [0, 1], aggs, ndv_hint=hint)
     cut = 1 << 22  # the first call decides the mode: at least 2^22 rows
     for r0, r1 in ((0, cut), (cut, n)):
         batch = wg.Batch([wg.Column(I32, a[r0:r1]), wg.Column(I64, b[r0:r1]), wg.Column(DEC, amt[r0:r1], scale=2),

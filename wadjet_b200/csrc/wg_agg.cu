@@ -17,6 +17,7 @@
 #include "wg_hc.cuh"
 
 #include <algorithm>
+#include <cmath>
 #include <cstdlib>
 #include <cstring>
 
@@ -395,6 +396,11 @@ struct wg_agg {
   int shift = 0;
   int64_t known_groups = 0;        // regular groups, exact as of the last read-back
   int64_t upper_groups = 0;        // upper bound since then
+  // the keys of every group in the table lie in [dom_lo, dom_hi]: dom 0 = no
+  // group yet, 1 = so bounded, 2 = unknown (a launch whose keys had no known
+  // range, a merge, a partitioned or spilled run)
+  int dom = 0;
+  long long dom_lo = 0, dom_hi = -1;
   // finalize
   wg::DevBuf list, cnt;
   int64_t n_out = 0;
@@ -441,18 +447,19 @@ struct wg_agg {
   // compact result that stands in for the table (`spilled`).
   bool hc = false;
   int hc_b1 = 0, hc_b2 = 0;
-  bool hc_hist_zero = true;         // the bucket histogram must be cleared before the next count
   std::vector<int32_t> hc_cols;     // copy columns: caller-numbered virtual columns (keys, then agg inputs)
   std::vector<int32_t> hc_es, hc_cls;
   struct HcRun {
     int64_t rows = 0;
     std::vector<int64_t> off1;      // first-level partition starts (np1 + 1)
     std::vector<wg::DevBuf> cols;
+    wg::DevBuf bucket;              // per row: its bucket within the partition
   };
   std::vector<HcRun> hc_runs;
   std::vector<HcRun> hc_free;       // runs of earlier queries, kept for reuse
   std::vector<wg::DevBuf> hc_copy2;
   wg::DevBuf hc_hist, hc_counts1, hc_offs1, hc_dev, hc_out, hc_scalars;
+  wg::DevBuf hc_hll;                // distinct-key sketch of the rows consumed so far
   ~wg_agg() {
     for (auto& b : host_blocks) cudaFreeHost(b.first);
     if (exp_host) cudaFreeHost(exp_host);
@@ -698,6 +705,7 @@ static wg_status agg_resolve(wg_agg* a, const VSchema& vs) {
   WG_CUDA_TRY(cudaMemsetAsync(a->ctr.get(), 0, 64, a->ctx->stream));
   a->known_groups = 0;
   a->upper_groups = 0;
+  a->dom = 0;
   a->resolved = true;
   return WG_OK;
 }
@@ -948,12 +956,12 @@ static wg_status run_device(const PipelineRun& r) {
   const int64_t n_items = ls.P.n_items;
   if (n_items == 0) return WG_OK;
   const int64_t fan = r.join ? std::max<int64_t>(1, join_max_fanout(r.join)) : 1;
-  if (a->hc && !r.no_partition) return hc_consume(r, ls.P);
-  if (a->spill && !r.no_partition) return spill_consume(r, ls.P, in_map);
+  if (a->hc && !r.no_partition) { a->dom = 2; return hc_consume(r, ls.P); }
+  if (a->spill && !r.no_partition) { a->dom = 2; return spill_consume(r, ls.P, in_map); }
   if (!r.no_partition) {
     bool done = false;
     WG_TRY(run_partitioned(r, ls.P, in_map, &done));
-    if (done) return WG_OK;
+    if (done) { a->dom = 2; return WG_OK; }
   }
 
   // kernel shape: shared-memory table for low-cardinality single int keys
@@ -1160,12 +1168,52 @@ static wg_status run_device(const PipelineRun& r) {
   // reservations threads may hold unused
   auto limit = [&]() { return (int64_t)((double)a->cap * kMaxLoad) - credit_slack(a); };
 
+  // The groups after this launch are at most the groups before it plus its
+  // rows (times the join's fan-out), and, when every key so far and every key
+  // of this launch lies in a known range (a group key that is an inner join's
+  // payload column with a known value range), at most that range's size.
+  bool dom_ok = false;
+  long long dlo = 0, dhi = -1;
+  if (a->L.key_words == 1 && a->L.n_keys == 1 && a->dom != 2 && r.join && join_type_of(r.join) == WG_JOIN_INNER) {
+    const int kv = ls.P.L.key_vcol[0];
+    const int npay = join_n_payload(r.join);
+    if (kv >= ls.P.n_in && kv < ls.P.n_in + npay && join_payload_range(r.join, kv - ls.P.n_in, &dlo, &dhi) &&
+        dhi >= dlo) {
+      if (a->dom == 1) { dlo = std::min(dlo, a->dom_lo); dhi = std::max(dhi, a->dom_hi); }
+      dom_ok = dhi - dlo < (int64_t(1) << 40);
+    }
+  }
+  auto note_domain = [&]() {
+    if (a->L.key_words == 0) return;
+    if (dom_ok) { a->dom = 1; a->dom_lo = dlo; a->dom_hi = dhi; }
+    else a->dom = 2;
+  };
+  int64_t bound = a->upper_groups + n_items * fan;
+  // Threads that race to insert the same new key each hold a reservation until
+  // they lose: a bound below the launch's rows must leave room for one per
+  // launched thread beside the groups.
+  int64_t race = 0;
+  if (dom_ok && (int64_t)(dhi - dlo) + 2 < bound) {
+    bound = (int64_t)(dhi - dlo) + 2;  // + a NULL key's group
+    race = (int64_t)ls.grid * (ls.tile ? 32 * (1 + ls.cfg.consumers) : ls.block);
+    if (bound + race > limit() && !a->spill) {  // a table that holds them, when it is small
+      const int64_t nb = (int64_t)table_words(a, cap_for(bound + race)) * 8;
+      const int64_t budget = ctx->ledger.budget();
+      if (nb <= kSnapshotMaxBytes && (budget <= 0 || 2 * nb <= budget - ctx->ledger.used())) {
+        WG_TRY(rebuild_table(a, cap_for(bound + race), a->L));
+        WG_TRY(refresh_groups(a));
+      }
+    }
+  }
+
   // 1) provably safe: one launch
-  if (a->L.key_words == 0 || a->upper_groups + n_items * fan <= limit()) {
+  if (a->L.key_words == 0 || bound + race <= limit()) {
     WG_TRY(launch_pipeline(a, ls, n_items));
-    a->upper_groups += a->L.key_words == 0 ? 0 : n_items * fan;
+    a->upper_groups = a->L.key_words == 0 ? 0 : bound;
+    note_domain();
     return r.defer_check ? WG_OK : check_device_error(ctx);
   }
+  note_domain();  // the launches below insert this run's keys whatever they find
   // 2) small table: snapshot, run, replay on overflow. Threads that race to
   // insert the same new key each hold a reservation until they lose, so the
   // table leaves room for one per launched thread beside the expected groups
@@ -1329,8 +1377,30 @@ static wg_status run_partitioned(const PipelineRun& r, const wgd::Plan& P0, cons
 // ---------------------------------------------------------------------------
 // Rows the mode needs before it pays (smaller inputs fit the direct path).
 constexpr int64_t kHcMinRows = int64_t(1) << 22;
-// Groups a bucket is sized for: the shared table's slots hold about twice that.
-constexpr int64_t kHcBucketGroups = 1800;
+// Bucket CTAs per SM (WG_HC_BUCKET_CTAS, 1 or 2): two CTAs, each with half of
+// the SM's shared memory and half as many groups per bucket, overlap one
+// bucket's table sweeps with the other's row updates.
+static int hc_bucket_ctas() { return env_int("WG_HC_BUCKET_CTAS", 2) == 1 ? 1 : 2; }
+
+// The bucket kernel's shared table: slot stride (words) and slots per CTA. An
+// odd stride spreads slots over the banks, but a packed key (and an Int128
+// MIN/MAX) is updated with 16-byte atomics, which need 16-byte aligned slots.
+static void hc_table_shape(const wg_agg* a, int* ssw_out, int* slots_out, int* rep_out) {
+  const int sw = a->L.slot_words;
+  int n_fsum = 0;
+  for (int i = 0; i < a->L.n_aggs; ++i) n_fsum += a->L.agg[i].kind == wgd::K_SUM_F64;
+  const int rep = n_fsum > 0 ? 2 : 1;
+  bool wide = a->L.key_words == 2;
+  for (int i = 0; i < a->L.n_aggs; ++i)
+    wide |= a->L.agg[i].kind == wgd::K_MIN_DEC || a->L.agg[i].kind == wgd::K_MAX_DEC;
+  const int ssw = wide ? ((sw + n_fsum * (rep - 1) + 1) & ~1) : ((sw + n_fsum * (rep - 1)) | 1);
+  const int ctas = hc_bucket_ctas();
+  // per CTA: its share of the SM, less the 1 KB the runtime reserves per CTA and room for static shared memory
+  const int64_t bytes = std::min<int64_t>(a->ctx->max_smem_optin, a->ctx->smem_per_sm / ctas - 1024) - 1024;
+  *ssw_out = ssw;
+  *slots_out = (int)std::min<int64_t>(bytes / (ssw * 8 + 4), 1 << 14);  // slot words and a used-slot list entry
+  *rep_out = rep;
+}
 
 // Large-table GROUP BY on a plain input: no join, no selection vector, no
 // validity bitmaps (a NULL key has no bucket), one or more integer keys, and a
@@ -1367,13 +1437,12 @@ static wg_status hc_setup(wg_agg* a, const PipelineRun& r, const wgd::Plan& P0) 
   a->hc_es.clear();
   (void)r;
   (void)P0;
-  const int64_t expect = std::max<int64_t>(a->hint, 1024);
-  const int64_t per_bucket = std::max(16, env_int("WG_HC_BUCKET_GROUPS", (int)kHcBucketGroups));
-  int bits = 0;
-  while (bits < 15 && (expect >> bits) > per_bucket) ++bits;
-  bits = std::max(bits, 4);
-  a->hc_b1 = std::min(bits, 8);
-  a->hc_b2 = bits - a->hc_b1;
+  // 256 first-level partitions; the second level's bits are chosen at finalize
+  // from the distinct-key sketch
+  a->hc_b1 = 8;
+  a->hc_b2 = 0;
+  WG_TRY(a->hc_hll.ensure(a->ctx, (int64_t(1) << wgd::kHllBits) * 4));
+  WG_CUDA_TRY(cudaMemsetAsync(a->hc_hll.get(), 0, (size_t(1) << wgd::kHllBits) * 4, a->ctx->stream));
   return WG_OK;
 }
 
@@ -1409,7 +1478,7 @@ static wg_status hc_consume(const PipelineRun& r, const wgd::Plan& P0) {
   wgd::Plan P = P0;
   P.L = launch_layout(a, P0);
   P.err = ctx->dev_error;
-  const int np1 = 1 << a->hc_b1, nb = 1 << (a->hc_b1 + a->hc_b2);
+  const int np1 = 1 << a->hc_b1;
   // the copy columns in this call's compact numbering
   wgd::HcCols out{};
   out.n = (int32_t)a->hc_cols.size();
@@ -1426,18 +1495,19 @@ static wg_status hc_consume(const PipelineRun& r, const wgd::Plan& P0) {
   }
   if (a->hc_cls.empty()) { a->hc_cls = cls; for (int j = 0; j < out.n; ++j) a->hc_es.push_back(out.es[j]); }
   else if (a->hc_cls != cls) return fail(WG_E_INVALID, "column classes changed between consume calls");
-  const unsigned grid = (unsigned)ctx->sm_count;
+  const unsigned grid = (unsigned)ctx->sm_count * 2;  // count and scatter1 share it (2 CTAs per SM)
   WG_TRY(a->hc_counts1.ensure(ctx, (int64_t)np1 * grid * 4));
   WG_TRY(a->hc_offs1.ensure(ctx, (int64_t)np1 * grid * 8));
-  WG_TRY(a->hc_hist.ensure(ctx, (int64_t)nb * 8));
-  if (a->hc_hist_zero) {
-    WG_CUDA_TRY(cudaMemsetAsync(a->hc_hist.get(), 0, (size_t)nb * 8, ctx->stream));
-    a->hc_hist_zero = false;
-  }
-  const size_t cs = wgd::hc_count_smem(np1, nb);
-  WG_CUDA_TRY(cudaFuncSetAttribute(wgd::hc_count_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cs));
-  wgd::hc_count_kernel<<<grid, wgd::kPartThreads, cs, ctx->stream>>>(P, a->hc_b1, a->hc_b2, a->hc_counts1.as<uint32_t>(),
-                                                                       a->hc_hist.as<unsigned long long>());
+  // the compiled high-cardinality shape when the input matches it
+  wgd::Plan probe = P;
+  const bool stat = wgd::shape_matches<wgd::ShapeHighCard>(probe) && env_int("WG_SPECIALIZE", 1) != 0;
+  if (stat)
+    wgd::hc_count_kernel<wgd::StatShape<wgd::ShapeHighCard>><<<grid, wgd::kHcThreads, wgd::hc_count_smem(np1),
+                                                                ctx->stream>>>(P, a->hc_b1, a->hc_counts1.as<uint32_t>(),
+                                                                               a->hc_hll.as<uint32_t>());
+  else
+    wgd::hc_count_kernel<wgd::DynShape><<<grid, wgd::kHcThreads, wgd::hc_count_smem(np1), ctx->stream>>>(
+        P, a->hc_b1, a->hc_counts1.as<uint32_t>(), a->hc_hll.as<uint32_t>());
   ctx->count_launch();
   WG_CUDA_TRY(cudaGetLastError());
   std::vector<uint32_t> hc((size_t)np1 * grid);
@@ -1461,10 +1531,19 @@ static wg_status hc_consume(const PipelineRun& r, const wgd::Plan& P0) {
     WG_TRY(run.cols[(size_t)j].ensure(ctx, std::max<int64_t>(run.rows, 1) * out.es[j]));
     out.data[j] = run.cols[(size_t)j].as<char>();
   }
-  const size_t ss = wgd::hc_scatter_smem(np1);
-  WG_CUDA_TRY(cudaFuncSetAttribute(wgd::hc_scatter1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss));
-  wgd::hc_scatter1_kernel<<<grid, wgd::kPartThreads, ss, ctx->stream>>>(P, a->hc_b1, a->hc_offs1.as<unsigned long long>(),
-                                                                          out);
+  WG_TRY(run.bucket.ensure(ctx, std::max<int64_t>(run.rows, 1)));
+  const size_t ss = wgd::hc_scatter_smem(np1, true);
+  if (stat) {
+    auto* k = wgd::hc_scatter1_kernel<wgd::StatShape<wgd::ShapeHighCard>>;
+    WG_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss));
+    k<<<grid, wgd::kHcThreads, ss, ctx->stream>>>(P, a->hc_b1, a->hc_offs1.as<unsigned long long>(), out,
+                                                    run.bucket.as<uint8_t>());
+  } else {
+    auto* k = wgd::hc_scatter1_kernel<wgd::DynShape>;
+    WG_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss));
+    k<<<grid, wgd::kHcThreads, ss, ctx->stream>>>(P, a->hc_b1, a->hc_offs1.as<unsigned long long>(), out,
+                                                    run.bucket.as<uint8_t>());
+  }
   ctx->count_launch();
   WG_CUDA_TRY(cudaGetLastError());
   a->hc_runs.push_back(std::move(run));
@@ -1473,17 +1552,54 @@ static wg_status hc_consume(const PipelineRun& r, const wgd::Plan& P0) {
 
 template <int NA, class Sh>
 static void launch_hc_bucket(const wgd::Plan& P, size_t smem, const int64_t* boff, int64_t nb, unsigned long long* out,
-                             unsigned long long* cursor, int64_t cap, int32_t* over, unsigned grid, cudaStream_t st) {
-  cudaFuncSetAttribute(wgd::hc_bucket_kernel<NA, Sh>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  wgd::hc_bucket_kernel<NA, Sh><<<grid, 1024, smem, st>>>(P, boff, nb, out, cursor, cap, over);
+                             unsigned long long* cursor, int64_t cap, int32_t* over, int sms, int ctas,
+                             cudaStream_t st) {
+  if (ctas == 1) {
+    cudaFuncSetAttribute(wgd::hc_bucket_kernel<NA, Sh, 1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    wgd::hc_bucket_kernel<NA, Sh, 1024><<<sms, 1024, smem, st>>>(P, boff, nb, out, cursor, cap, over);
+  } else {
+    cudaFuncSetAttribute(wgd::hc_bucket_kernel<NA, Sh, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    wgd::hc_bucket_kernel<NA, Sh, 512><<<sms * 2, 512, smem, st>>>(P, boff, nb, out, cursor, cap, over);
+  }
 }
 
 // Finalize of the two-level mode: the runs re-partitioned into buckets, the
 // buckets aggregated into a compact result, the groups that outgrew their
 // bucket's shared table appended from the HBM table; the result then stands
 // in for the table.
+// Distinct keys estimated from the sketch (HyperLogLog: the harmonic mean of
+// 2^-rank over the registers, with the small-range linear-counting estimate
+// while registers are still empty).
+static wg_status hc_estimate_groups(wg_agg* a, double* out) {
+  const int m = 1 << wgd::kHllBits;
+  std::vector<uint32_t> reg((size_t)m);
+  WG_CUDA_TRY(cudaMemcpyAsync(reg.data(), a->hc_hll.get(), (size_t)m * 4, cudaMemcpyDeviceToHost, a->ctx->stream));
+  WG_CUDA_TRY(cudaStreamSynchronize(a->ctx->stream));
+  double z = 0.0;
+  int zeros = 0;
+  for (uint32_t r : reg) { z += std::ldexp(1.0, -(int)r); zeros += r == 0; }
+  const double alpha = 0.7213 / (1.0 + 1.079 / m);
+  double e = alpha * m * m / z;
+  if (e <= 2.5 * m && zeros > 0) e = m * std::log((double)m / zeros);
+  *out = e;
+  return WG_OK;
+}
+
 static wg_status hc_finish(wg_agg* a) {
   Ctx* ctx = a->ctx;
+  // second-level bits: buckets of about half a shared table of groups (the
+  // sketch's estimate plus 10%, its error being about 3% at 1024 registers)
+  {
+    double groups = 0.0;
+    WG_TRY(hc_estimate_groups(a, &groups));
+    int ssw = 0, slots = 0, rep = 0;
+    hc_table_shape(a, &ssw, &slots, &rep);
+    const double per_bucket = (double)std::max(16, env_int("WG_HC_BUCKET_GROUPS", slots / 2));
+    const double want = groups * 1.1 / per_bucket;
+    int b2 = 0;
+    while (b2 < wgd::kHcByteBits && std::ldexp(1.0, a->hc_b1 + b2) < want) ++b2;
+    a->hc_b2 = b2;
+  }
   const int b1 = a->hc_b1, b2 = a->hc_b2;
   const int np1 = 1 << b1, np2 = 1 << b2;
   const int64_t nb = int64_t(1) << (b1 + b2);
@@ -1491,6 +1607,41 @@ static wg_status hc_finish(wg_agg* a) {
   const int sw = a->L.slot_words;
   int64_t rows = 0;
   for (const auto& r : a->hc_runs) rows += r.rows;
+  // device scratch: boff (nb + 1), cursors (nb), then per run off1 and item0 (np1 + 1 each)
+  const int64_t scal = (nb + 1) + nb + 2 * ((int64_t)np1 + 1) * (int64_t)std::max<size_t>(a->hc_runs.size(), 1);
+  WG_TRY(a->hc_dev.ensure(ctx, scal * 8));
+  int64_t* d_boff = a->hc_dev.as<int64_t>();
+  unsigned long long* d_cur = (unsigned long long*)(d_boff + nb + 1);
+  // per run: its partition starts and first work items (tiles of kHcTile rows) on the device
+  std::vector<int64_t> run_items(a->hc_runs.size(), 0);
+  for (size_t ri = 0; ri < a->hc_runs.size(); ++ri) {
+    const auto& run = a->hc_runs[ri];
+    std::vector<int64_t> item0((size_t)np1 + 1);
+    int64_t items = 0;
+    for (int p = 0; p < np1; ++p) {
+      item0[(size_t)p] = items;
+      items += (run.off1[(size_t)p + 1] - run.off1[(size_t)p] + wgd::kHcTile - 1) / wgd::kHcTile;
+    }
+    item0[(size_t)np1] = items;
+    run_items[ri] = items;
+    int64_t* d_off1 = (int64_t*)(d_cur + nb) + 2 * ((int64_t)np1 + 1) * (int64_t)ri;
+    WG_CUDA_TRY(cudaMemcpyAsync(d_off1, run.off1.data(), (size_t)(np1 + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
+    WG_CUDA_TRY(cudaMemcpyAsync(d_off1 + np1 + 1, item0.data(), (size_t)(np1 + 1) * 8, cudaMemcpyHostToDevice,
+                                ctx->stream));
+  }
+  // rows per bucket, from the runs' bucket bytes
+  WG_TRY(a->hc_hist.ensure(ctx, nb * 8));
+  WG_CUDA_TRY(cudaMemsetAsync(a->hc_hist.get(), 0, (size_t)nb * 8, ctx->stream));
+  for (size_t ri = 0; ri < a->hc_runs.size(); ++ri) {
+    if (a->hc_runs[ri].rows == 0) continue;
+    const int64_t* d_off1 = (const int64_t*)(d_cur + nb) + 2 * ((int64_t)np1 + 1) * (int64_t)ri;
+    const unsigned grid = (unsigned)std::min<int64_t>((int64_t)ctx->sm_count * 4, run_items[ri]);
+    wgd::hc_count2_kernel<<<grid, wgd::kHcThreads, 0, ctx->stream>>>(a->hc_runs[ri].bucket.as<uint8_t>(), b2, d_off1,
+                                                                      d_off1 + np1 + 1, np1, run_items[ri],
+                                                                      a->hc_hist.as<unsigned long long>());
+    ctx->count_launch();
+    WG_CUDA_TRY(cudaGetLastError());
+  }
   // bucket starts in the second copy
   std::vector<unsigned long long> hist((size_t)nb);
   WG_CUDA_TRY(cudaMemcpyAsync(hist.data(), a->hc_hist.get(), (size_t)nb * 8, cudaMemcpyDeviceToHost, ctx->stream));
@@ -1500,13 +1651,6 @@ static wg_status hc_finish(wg_agg* a) {
   for (int64_t b = 0; b < nb; ++b) { boff[(size_t)b] = acc; acc += (int64_t)hist[(size_t)b]; }
   boff[(size_t)nb] = acc;
   if (acc != rows) return fail(WG_E_CUDA, "bucket counts do not add up to the partitioned rows");
-  // device scratch: boff (nb + 1), cursors (nb), then per run off1 and item0 (np1 + 1 each)
-  const int64_t scal = (nb + 1) + nb + 2 * ((int64_t)np1 + 1);
-  WG_TRY(a->hc_dev.ensure(ctx, scal * 8));
-  int64_t* d_boff = a->hc_dev.as<int64_t>();
-  unsigned long long* d_cur = (unsigned long long*)(d_boff + nb + 1);
-  int64_t* d_off1 = (int64_t*)(d_cur + nb);
-  int64_t* d_item0 = d_off1 + np1 + 1;
   WG_CUDA_TRY(cudaMemcpyAsync(d_boff, boff.data(), (size_t)(nb + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
   WG_CUDA_TRY(cudaMemcpyAsync(d_cur, boff.data(), (size_t)nb * 8, cudaMemcpyHostToDevice, ctx->stream));
   if ((int)a->hc_copy2.size() < ncol) a->hc_copy2.resize((size_t)ncol);
@@ -1518,45 +1662,31 @@ static wg_status hc_finish(wg_agg* a) {
     out2.es[j] = a->hc_es[(size_t)j];
     out2.vcol[j] = j;
   }
-  const size_t ss = wgd::hc_scatter_smem(np2);
+  const size_t ss = wgd::hc_scatter_smem(np2, false);
   WG_CUDA_TRY(cudaFuncSetAttribute(wgd::hc_scatter2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss));
-  for (auto& run : a->hc_runs) {
+  for (size_t ri = 0; ri < a->hc_runs.size(); ++ri) {
+    auto& run = a->hc_runs[ri];
     if (run.rows == 0) continue;
-    std::vector<int64_t> item0((size_t)np1 + 1);
-    int64_t items = 0;
-    for (int p = 0; p < np1; ++p) {
-      item0[(size_t)p] = items;
-      items += (run.off1[(size_t)p + 1] - run.off1[(size_t)p] + wgd::kPartTile - 1) / wgd::kPartTile;
-    }
-    item0[(size_t)np1] = items;
-    WG_CUDA_TRY(cudaMemcpyAsync(d_off1, run.off1.data(), (size_t)(np1 + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
-    WG_CUDA_TRY(cudaMemcpyAsync(d_item0, item0.data(), (size_t)(np1 + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
+    const int64_t* d_off1 = (const int64_t*)(d_cur + nb) + 2 * ((int64_t)np1 + 1) * (int64_t)ri;
     wgd::Plan Pc = hc_plan(a, run.cols, run.rows);
-    const unsigned grid = (unsigned)std::min<int64_t>((int64_t)ctx->sm_count * 3, std::max<int64_t>(items, 1));
-    wgd::hc_scatter2_kernel<<<grid, wgd::kPartThreads, ss, ctx->stream>>>(Pc, b1, b2, d_off1, d_item0, np1, items, d_cur,
-                                                                           out2);
+    const unsigned grid = (unsigned)std::min<int64_t>((int64_t)ctx->sm_count * 2, run_items[ri]);
+    wgd::hc_scatter2_kernel<<<grid, wgd::kHcThreads, ss, ctx->stream>>>(Pc, b2, run.bucket.as<uint8_t>(), d_off1,
+                                                                         d_off1 + np1 + 1, np1, run_items[ri], d_cur,
+                                                                         out2);
     ctx->count_launch();
     WG_CUDA_TRY(cudaGetLastError());
-    // the next run's offsets reuse the same device words
-    WG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   }
   // buckets into the compact result
   wgd::Plan Pb = hc_plan(a, a->hc_copy2, rows);
-  int n_fsum = 0;
-  for (int i = 0; i < a->L.n_aggs; ++i) n_fsum += a->L.agg[i].kind == wgd::K_SUM_F64;
-  const int rep = n_fsum > 0 ? 2 : 1;
-  // an odd stride spreads slots over the banks, but a packed key (and an Int128
-  // MIN/MAX) is updated with 16-byte atomics, which need 16-byte aligned slots
-  bool wide = a->L.key_words == 2;
-  for (int i = 0; i < a->L.n_aggs; ++i)
-    wide |= a->L.agg[i].kind == wgd::K_MIN_DEC || a->L.agg[i].kind == wgd::K_MAX_DEC;
-  const int ssw = wide ? ((sw + n_fsum * (rep - 1) + 1) & ~1) : ((sw + n_fsum * (rep - 1)) | 1);
-  const int S = (int)std::min<int64_t>(((int64_t)ctx->max_smem_optin - 2048) / (ssw * 8), 1 << 14);
+  int ssw = 0, S = 0, rep = 0;
+  hc_table_shape(a, &ssw, &S, &rep);
+  const int ctas = hc_bucket_ctas();
   Pb.smem_slots = S;
   Pb.smem_sw = ssw;
   Pb.smem_rep = rep;
   Pb.smem_hash_shift = b1 + b2;
-  const size_t smem = (size_t)S * ssw * 8;
+  Pb.smem_list = S * ssw;
+  const size_t smem = (size_t)S * ssw * 8 + (size_t)S * 4;
   WG_TRY(a->hc_scalars.ensure(ctx, 64));
   unsigned long long* d_ocur = a->hc_scalars.as<unsigned long long>();
   int32_t* d_over = (int32_t*)(d_ocur + 1);
@@ -1569,13 +1699,13 @@ static wg_status hc_finish(wg_agg* a) {
     WG_TRY(a->hc_out.ensure(ctx, cap * sw * 8));
     WG_CUDA_TRY(cudaMemsetAsync(a->hc_scalars.get(), 0, 64, ctx->stream));
     Pb.T = table_view(a);
-    const unsigned grid = (unsigned)ctx->sm_count;
+    const int sms = ctx->sm_count;
     if (stat) launch_hc_bucket<4, wgd::StatShape<wgd::ShapeHighCard>>(Pb, smem, d_boff, nb, a->hc_out.as<unsigned long long>(),
-                                                                     d_ocur, cap, d_over, grid, ctx->stream);
+                                                                     d_ocur, cap, d_over, sms, ctas, ctx->stream);
     else if (a->L.n_aggs <= 4) launch_hc_bucket<4, wgd::DynShape>(Pb, smem, d_boff, nb, a->hc_out.as<unsigned long long>(),
-                                                                  d_ocur, cap, d_over, grid, ctx->stream);
+                                                                  d_ocur, cap, d_over, sms, ctas, ctx->stream);
     else launch_hc_bucket<8, wgd::DynShape>(Pb, smem, d_boff, nb, a->hc_out.as<unsigned long long>(), d_ocur, cap,
-                                            d_over, grid, ctx->stream);
+                                            d_over, sms, ctas, ctx->stream);
     ctx->count_launch();
     WG_CUDA_TRY(cudaGetLastError());
     int64_t v[2], t[2];
@@ -1613,7 +1743,6 @@ static wg_status hc_finish(wg_agg* a) {
       a->n_out = n_res;
       for (auto& r : a->hc_runs) a->hc_free.push_back(std::move(r));
       a->hc_runs.clear();
-      a->hc_hist_zero = true;
       return check_device_error(ctx);
     }
     // replay: a larger result, or a larger HBM table for the groups that outgrew their buckets
@@ -1625,6 +1754,7 @@ static wg_status hc_finish(wg_agg* a) {
     ctx->count_launch();
     WG_CUDA_TRY(cudaMemsetAsync(a->ctr.get(), 0, 64, ctx->stream));
     a->known_groups = a->upper_groups = 0;
+    a->dom = 0;
   }
   return fail(WG_E_NOMEM, "two-level aggregation did not converge");
 }
@@ -1804,6 +1934,7 @@ static wg_status spill_finish(wg_agg* a) {
     ctx->count_launch();
     WG_CUDA_TRY(cudaMemsetAsync(a->ctr.get(), 0, 64, ctx->stream));
     a->known_groups = a->upper_groups = 0;
+    a->dom = 0;
     PipelineRun rp{a, &d, (int32_t)a->sp_filters.size(), a->sp_filters.data(), nullptr, (int32_t)a->sp_exprs.size(),
                    a->sp_exprs.data()};
     rp.no_partition = true;
@@ -1969,6 +2100,7 @@ wg_status wg_agg_merge(wg_agg* d, wg_agg* s) {
     d->resolved = true;
   }
   if (d->kind != s->kind) return fail(WG_E_INVALID, "aggregate input types differ");
+  d->dom = 2;  // the source's keys have no range this side tracks
   // destination must carry every null counter the source has
   bool upgrade = false;
   std::vector<bool> nn = d->nullable;
@@ -2151,10 +2283,11 @@ wg_status wg_agg_reset(wg_agg* a) {
     a->block_idx = 0;
     a->block_used = 0;
   }
-  if (a->hc) {  // the runs' buffers are kept for the next query
+  if (a->hc) {  // the runs' buffers are kept for the next query; the sketch starts over
     for (auto& r : a->hc_runs) a->hc_free.push_back(std::move(r));
     a->hc_runs.clear();
-    a->hc_hist_zero = true;
+    if (a->hc_hll.get())
+      WG_CUDA_TRY(cudaMemsetAsync(a->hc_hll.get(), 0, (size_t(1) << wgd::kHllBits) * 4, ctx->stream));
   }
   if (a->spilled) {  // the table holds a compact result: back to an empty small table
     a->table.reset();
@@ -2171,6 +2304,7 @@ wg_status wg_agg_reset(wg_agg* a) {
   WG_CUDA_TRY(cudaMemsetAsync(a->ctr.get(), 0, 64, ctx->stream));
   a->known_groups = 0;
   a->upper_groups = 0;
+  a->dom = 0;
   return WG_OK;
 }
 
@@ -2246,6 +2380,7 @@ wg_status wg_agg_merge_state(wg_agg* a, const wg_state_layout* src, const void* 
     return fail(WG_E_INVALID, "state layout does not match the aggregate's shape");
   Ctx* ctx = a->ctx;
   WG_TRY(ensure_device(ctx));
+  a->dom = 2;  // merged keys have no tracked range
   // the layout a source with these kinds and null counters has
   wg_agg ref;
   ref.key_cols = a->key_cols;
@@ -2283,6 +2418,7 @@ wg_status wg_agg_merge_state(wg_agg* a, const wg_state_layout* src, const void* 
     WG_TRY(a->ctr.alloc(ctx, 64));
     WG_CUDA_TRY(cudaMemsetAsync(a->ctr.get(), 0, 64, ctx->stream));
     a->known_groups = a->upper_groups = 0;
+    a->dom = 0;
     a->resolved = true;
   }
   if (a->L.key_words != src->key_words || a->kind != ref.kind)

@@ -102,6 +102,8 @@ struct Plan {
                                  // in dynamic shared memory (after the shared table)
   int32_t smem_hash_shift;       // shared-table slot from the key hash's bits below the top
                                  // smem_hash_shift (the bits that picked the rows' bucket)
+  int32_t smem_list;             // >0: word offset in shared memory of a list of the bucketed
+                                 // table's used slots, entry i written by its i-th insert
   DCol in[WG_MAX_IN];
   Pred filt[WG_MAX_FILTERS];
   JoinView join;

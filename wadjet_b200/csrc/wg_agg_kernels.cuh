@@ -661,7 +661,8 @@ __device__ __forceinline__ unsigned long long* find_smem(unsigned long long* sm,
 // (its words change once, from {~0, ~0} to the key, as in find_global).
 __device__ __forceinline__ unsigned long long* find_smem_bucketed(unsigned long long* sm, int S, int sw, int kw,
                                                                   unsigned long long k0, unsigned long long k1,
-                                                                  int shift, int* s_groups, int s_limit) {
+                                                                  int shift, int* s_groups, int s_limit,
+                                                                  uint32_t* list) {
   unsigned long long h;
   if (kw == 1) {
     if (k0 == WG_EMPTY_KEY) return nullptr;
@@ -680,19 +681,27 @@ __device__ __forceinline__ unsigned long long* find_smem_bucketed(unsigned long 
       if (cur == WG_EMPTY_KEY) {
         if (*((volatile int*)s_groups) >= s_limit) return nullptr;
         const unsigned long long old = atomicCAS(s, WG_EMPTY_KEY, k0);
-        if (old == WG_EMPTY_KEY) { atomicAdd(s_groups, 1); return s; }
+        if (old == WG_EMPTY_KEY) {
+          const int g = atomicAdd(s_groups, 1);
+          if (list) list[g] = i;
+          return s;
+        }
         if (old == k0) return s;
       }
     } else {
       const U128 cur = read128(s);
-      if (cur.lo != ~0ULL && cur.hi != ~0ULL) {
+      if (cur.lo != ~0ULL && cur.hi != ~0ULL) {  // a complete key (as in find_global)
         if (cur.lo == k0 && cur.hi == k1) return s;
       } else {
         if (*((volatile int*)s_groups) >= s_limit) return nullptr;
         U128 e; e.lo = ~0ULL; e.hi = ~0ULL;
         U128 k; k.lo = k0; k.hi = k1;
         const U128 old = cas128((U128*)s, e, k);
-        if (old.lo == e.lo && old.hi == e.hi) { atomicAdd(s_groups, 1); return s; }
+        if (old.lo == e.lo && old.hi == e.hi) {
+          const int g = atomicAdd(s_groups, 1);
+          if (list) list[g] = i;
+          return s;
+        }
         if (old.lo == k0 && old.hi == k1) return s;
       }
     }
@@ -714,7 +723,7 @@ __device__ __forceinline__ unsigned long long* find_shared(const Plan& P, unsign
   }
   if (P.smem_hash_shift > 0)
     return find_smem_bucketed(sm, P.smem_slots, smem_stride(P), P.L.key_words, k0, k1, P.smem_hash_shift, s_groups,
-                              s_limit);
+                              s_limit, P.smem_list > 0 ? (uint32_t*)(sm + P.smem_list) : nullptr);
   return find_smem(sm, P.smem_slots, smem_stride(P), k0, s_groups, s_limit);
 }
 

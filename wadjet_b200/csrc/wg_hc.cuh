@@ -10,12 +10,16 @@
 // times faster, so the rows are bucketed until one bucket's groups fit one SM:
 //
 //  count    one pass over the key columns: rows per first-level partition per
-//           CTA (the scatter's offsets) and per (first, second)-level bucket;
+//           CTA (the scatter's offsets) and a distinct-key sketch, from which
+//           finalize picks b2 (the second level's bits, at most 8) so buckets
+//           hold about half a shared table of groups;
 //  scatter1 the rows passing the filters, as the columns the aggregate reads
 //           (keys and aggregate inputs, projections evaluated), written in
-//           first-level order (top b1 bits of the key hash);
-//  scatter2 each first-level partition re-partitioned by the next b2 hash
-//           bits, so every bucket's rows are contiguous;
+//           first-level order (top b1 bits of the key hash), with a byte per
+//           row holding the next 8 hash bits;
+//  count2   rows per (partition, bucket), from the top b2 bits of the bytes;
+//  scatter2 each first-level partition re-partitioned by its bucket bytes, so
+//           every bucket's rows are contiguous;
 //  buckets  persistent CTAs take buckets; each aggregates its bucket in a
 //           shared-memory table (slots picked by the hash bits below the
 //           bucket's) and appends its groups, in the table's slot layout, to a
@@ -58,33 +62,51 @@ __device__ __forceinline__ bool row_passes(const Plan& P, const Sh& sh, int64_t 
   return true;
 }
 
-constexpr size_t hc_count_smem(int np1, int nb) { return (size_t)np1 * 4 + (size_t)nb * 4; }
+// The count and the first-level scatter walk the input in tiles of kHcTile
+// rows, CTA c taking tiles c, c + gridDim.x, ... (both launched on the same
+// grid), so the rows a CTA counts per partition are exactly the rows it later
+// writes there.
+constexpr int kHcThreads = 512;
+constexpr int kHcTile = 8192;
+static_assert(kHcTile <= 65536, "tile-local row indices are 16-bit");
+
+// Bits of the per-row bucket byte the first level writes: the second level
+// uses its top b2 <= 8 bits, b2 chosen when the groups have been estimated.
+constexpr int kHcByteBits = 8;
+// Distinct-key sketch of the counting pass: 2^kHllBits registers, each the
+// largest rank (leading zeros + 1) among the hashes that select it.
+constexpr int kHllBits = 10;
+constexpr size_t hc_count_smem(int np1) { return (size_t)np1 * 4 + ((size_t)1 << kHllBits) * 4; }
 
 // Rows passing the filters per first-level partition seen by each CTA
-// (counts1[p * gridDim.x + cta]) and per bucket over the whole input
-// (hist[p1 << b2 | p2], accumulated across calls).
-__global__ void __launch_bounds__(kPartThreads) hc_count_kernel(const __grid_constant__ Plan P, int b1, int b2,
-                                                                uint32_t* counts1, unsigned long long* hist) {
-  extern __shared__ uint32_t hsm[];
-  const int np1 = 1 << b1, nb = 1 << (b1 + b2);
-  uint32_t* h1 = hsm;
-  uint32_t* h2 = hsm + np1;
-  for (int i = threadIdx.x; i < np1 + nb; i += blockDim.x) hsm[i] = 0;
+// (counts1[p * gridDim.x + cta]), and the distinct-key sketch of those rows
+// (max-merged into hll). Register index: the hash's low kHllBits bits; rank:
+// leading zeros of the remaining bits, plus one. The low bits are independent
+// of the top bits that pick partitions and buckets.
+template <class Sh>
+__global__ void __launch_bounds__(kHcThreads, 2) hc_count_kernel(const __grid_constant__ Plan P, int b1,
+                                                                 uint32_t* counts1, uint32_t* hll) {
+  extern __shared__ uint32_t h1[];
+  const int np1 = 1 << b1;
+  uint32_t* reg = h1 + np1;
+  for (int i = threadIdx.x; i < np1 + (1 << kHllBits); i += blockDim.x) h1[i] = 0;
   __syncthreads();
-  const DynShape sh{P};
-  for (int64_t t0 = (int64_t)blockIdx.x * kPartTile; t0 < P.n_items; t0 += (int64_t)gridDim.x * kPartTile) {
-    const int m = (int)min((int64_t)kPartTile, P.n_items - t0);
+  const Sh sh{P};
+  for (int64_t t0 = (int64_t)blockIdx.x * kHcTile; t0 < P.n_items; t0 += (int64_t)gridDim.x * kHcTile) {
+    const int m = (int)min((int64_t)kHcTile, P.n_items - t0);
     for (int k = threadIdx.x; k < m; k += blockDim.x) {
       if (!row_passes(P, sh, t0 + k)) continue;
       const unsigned long long h = row_key_hash(P, sh, t0 + k);
       atomicAdd(&h1[(uint32_t)(h >> (64 - b1))], 1u);
-      atomicAdd(&h2[(uint32_t)(h >> (64 - b1 - b2))], 1u);
+      const uint32_t rank = (uint32_t)(__clzll((long long)((h >> kHllBits) | 1ULL)) - kHllBits + 1);
+      const uint32_t r = (uint32_t)h & ((1u << kHllBits) - 1u);
+      if (rank > reg[r]) atomicMax(&reg[r], rank);
     }
   }
   __syncthreads();
   for (int i = threadIdx.x; i < np1; i += blockDim.x) counts1[(size_t)i * gridDim.x + blockIdx.x] = h1[i];
-  for (int i = threadIdx.x; i < nb; i += blockDim.x)
-    if (h2[i]) atomicAdd(&hist[i], (unsigned long long)h2[i]);
+  for (int i = threadIdx.x; i < (1 << kHllBits); i += blockDim.x)
+    if (reg[i]) atomicMax(&hll[i], reg[i]);
 }
 
 // The columns of the partitioned copy: value of plan virtual column vcol[j],
@@ -96,43 +118,94 @@ struct HcCols {
   int32_t n;
 };
 
-__device__ __forceinline__ void store_val(char* d, int es, const Val& v) {
-  if (es == 4) *(uint32_t*)d = (uint32_t)v.lo;
-  else if (es == 8) *(unsigned long long*)d = v.lo;
-  else { longlong2 x; x.x = (long long)v.hi; x.y = (long long)v.lo; *(longlong2*)d = x; }  // {hi, lo}
+// Word w of a value as the copy stores it: 4- and 8-byte values whole, a
+// 16-byte one as {hi, lo}.
+__device__ __forceinline__ unsigned long long val_word(int es, const Val& v, int w) {
+  return es == 16 ? (w == 0 ? v.hi : v.lo) : v.lo;
 }
 
-__host__ __device__ constexpr size_t hc_scatter_smem(int np) {
-  return (size_t)np * 8 + (size_t)np * 12 + (size_t)kPartTile * 4;
+// Shared memory of the scatter kernels: kHcTile staging words, np output
+// cursors (8 B) and per-partition hist / offset / cursor (12 B), then per tile
+// row its partition and its place in the order (2 B each) and, for the first
+// level, its bucket byte. Two CTAs fit an SM.
+__host__ __device__ constexpr size_t hc_scatter_smem(int np, bool bucket_bytes) {
+  return (size_t)kHcTile * 8 + (size_t)np * 20 + (size_t)kHcTile * (bucket_bytes ? 5 : 4);
+}
+
+// Tile rows in partition order. Position q of the order holds tile row
+// perm[q] of partition part[perm[q]], which goes to output row
+// dst[p] + q - loff[p]. Each copy column is staged in shared memory in tile-row
+// order (reads coalesced), then stored in partition order (stores in runs of
+// one partition): `stage_fn(k, w)` gives word w of tile row k's value (16-byte
+// values go as two 8-byte words).
+template <class StageFn>
+__device__ __forceinline__ void hc_write_column(unsigned long long* stage, int m, uint32_t kept, const uint16_t* perm,
+                                                const uint16_t* part, const unsigned long long* dst,
+                                                const uint32_t* loff, char* dcol, int es, StageFn stage_fn) {
+  const int words = es == 16 ? 2 : 1;
+  for (int w = 0; w < words; ++w) {
+    if (es == 4) {
+      uint32_t* st = (uint32_t*)stage;
+#pragma unroll 4
+      for (int k = threadIdx.x; k < m; k += blockDim.x) st[k] = (uint32_t)stage_fn(k, w);
+    } else {
+#pragma unroll 4
+      for (int k = threadIdx.x; k < m; k += blockDim.x) stage[k] = stage_fn(k, w);
+    }
+    __syncthreads();
+    for (uint32_t q = threadIdx.x; q < kept; q += blockDim.x) {
+      const int k = perm[q];
+      const uint32_t p = part[k];
+      const unsigned long long row = dst[p] + (q - loff[p]);
+      if (es == 4) ((uint32_t*)dcol)[row] = ((const uint32_t*)stage)[k];
+      else if (es == 8) ((unsigned long long*)dcol)[row] = stage[k];
+      else ((unsigned long long*)dcol)[row * 2 + w] = stage[k];
+    }
+    __syncthreads();
+  }
+}
+
+// Word w of input column j at row r, read as it lies.
+__device__ __forceinline__ unsigned long long hc_raw_word(const Plan& P, int j, int es, int64_t r, int w) {
+  const char* base = (const char*)P.in[j].data;
+  if (es == 4) return __ldg((const uint32_t*)base + r);
+  if (es == 8) return __ldg((const unsigned long long*)base + r);
+  return __ldg((const unsigned long long*)base + r * 2 + w);
 }
 
 // First level: the input's rows passing the filters, written as the copy's
 // columns in partition order (partition p of CTA c from offs[p * gridDim.x + c];
-// tiles as hc_count_kernel). Per tile the rows are counting-sorted by
-// partition in shared memory and written column by column in that order.
-__global__ void __launch_bounds__(kPartThreads) hc_scatter1_kernel(const __grid_constant__ Plan P, int b1,
-                                                                   const unsigned long long* offs,
-                                                                   const __grid_constant__ HcCols out) {
-  extern __shared__ unsigned long long gcur[];
+// tiles as hc_count_kernel), and with each row its bucket byte (the next 8
+// hash bits), from which the second level splits without hashing again.
+template <class Sh>
+__global__ void __launch_bounds__(kHcThreads, 2) hc_scatter1_kernel(const __grid_constant__ Plan P, int b1,
+                                                                    const unsigned long long* offs,
+                                                                    const __grid_constant__ HcCols out,
+                                                                    uint8_t* bucket_out) {
+  extern __shared__ __align__(16) unsigned long long stage[];
   __shared__ uint32_t warp_tot[32];
   const int np = 1 << b1;
+  unsigned long long* gcur = stage + kHcTile;
   uint32_t* hist = (uint32_t*)(gcur + np);
   uint32_t* loff = hist + np;
   uint32_t* lcur = loff + np;
-  uint16_t* part = (uint16_t*)(lcur + np);      // partition of tile row k (np = dropped)
-  uint16_t* perm = part + kPartTile;
+  uint16_t* part = (uint16_t*)(lcur + np);  // partition of tile row k (np = dropped)
+  uint16_t* perm = part + kHcTile;
+  uint8_t* bkt = (uint8_t*)(perm + kHcTile);
   for (int i = threadIdx.x; i < np; i += blockDim.x) {
     gcur[i] = offs[(size_t)i * gridDim.x + blockIdx.x];
     hist[i] = 0;
   }
   __syncthreads();
-  const DynShape sh{P};
-  for (int64_t t0 = (int64_t)blockIdx.x * kPartTile; t0 < P.n_items; t0 += (int64_t)gridDim.x * kPartTile) {
-    const int m = (int)min((int64_t)kPartTile, P.n_items - t0);
+  const Sh sh{P};
+  for (int64_t t0 = (int64_t)blockIdx.x * kHcTile; t0 < P.n_items; t0 += (int64_t)gridDim.x * kHcTile) {
+    const int m = (int)min((int64_t)kHcTile, P.n_items - t0);
     for (int k = threadIdx.x; k < m; k += blockDim.x) {
       uint32_t p = (uint32_t)np;
       if (row_passes(P, sh, t0 + k)) {
-        p = (uint32_t)(row_key_hash(P, sh, t0 + k) >> (64 - b1));
+        const unsigned long long h = row_key_hash(P, sh, t0 + k);
+        p = (uint32_t)(h >> (64 - b1));
+        bkt[k] = (uint8_t)(h >> (64 - b1 - kHcByteBits));
         atomicAdd(&hist[p], 1u);
       }
       part[k] = (uint16_t)p;
@@ -141,38 +214,31 @@ __global__ void __launch_bounds__(kPartThreads) hc_scatter1_kernel(const __grid_
     for (int i = threadIdx.x; i < np; i += blockDim.x) { loff[i] = hist[i]; lcur[i] = 0; }
     __syncthreads();
     block_exclusive_scan(loff, np, warp_tot);
-    uint32_t kept = 0;  // rows of the tile that pass (loff[np - 1] + hist[np - 1])
-    kept = loff[np - 1] + hist[np - 1];
+    const uint32_t kept = loff[np - 1] + hist[np - 1];  // rows of the tile that pass
     for (int k = threadIdx.x; k < m; k += blockDim.x) {
       const uint32_t p = part[k];
       if (p < (uint32_t)np) perm[loff[p] + atomicAdd(&lcur[p], 1u)] = (uint16_t)k;
     }
     __syncthreads();
     for (int j = 0; j < out.n; ++j) {
-      const int es = out.es[j];
-      char* dcol = out.data[j];
-      if (out.vcol[j] < P.n_in) {  // an input column: its bytes as they are
-        const char* scol = (const char*)P.in[out.vcol[j]].data + t0 * es;
-        for (uint32_t q = threadIdx.x; q < kept; q += blockDim.x) {
-          const int k = perm[q];
-          const uint32_t p = part[k];
-          char* d = dcol + (gcur[p] + (q - loff[p])) * es;
-          const char* sp = scol + (size_t)k * es;
-          if (es == 4) *(uint32_t*)d = __ldg((const uint32_t*)sp);
-          else if (es == 8) *(unsigned long long*)d = __ldg((const unsigned long long*)sp);
-          else *(longlong2*)d = __ldg((const longlong2*)sp);
-        }
-        continue;
+      const int es = out.es[j], vc = out.vcol[j];
+      if (vc < P.n_in) {  // an input column: its bytes as they are
+        hc_write_column(stage, m, kept, perm, part, gcur, loff, out.data[j], es,
+                        [&](int k, int w) { return hc_raw_word(P, vc, es, t0 + k, w); });
+      } else {  // a projection, evaluated per kept row
+        hc_write_column(stage, m, kept, perm, part, gcur, loff, out.data[j], es, [&](int k, int w) {
+          if (part[k] >= (uint16_t)np) return 0ULL;
+          const SrcGlobal src{t0 + k};
+          ExprVals ev;
+          eval_exprs(P, sh, src, -1, ev);
+          return val_word(es, fetch(P, sh, src, vc, -1, ev), w);
+        });
       }
-      for (uint32_t q = threadIdx.x; q < kept; q += blockDim.x) {  // a projection, evaluated per row
-        const int k = perm[q];
-        const uint32_t p = part[k];
-        const SrcGlobal src{t0 + k};
-        ExprVals ev;
-        eval_exprs(P, sh, src, -1, ev);
-        const Val v = fetch(P, sh, src, out.vcol[j], -1, ev);
-        store_val(dcol + (gcur[p] + (q - loff[p])) * es, es, v);
-      }
+    }
+    for (uint32_t q = threadIdx.x; q < kept; q += blockDim.x) {
+      const int k = perm[q];
+      const uint32_t p = part[k];
+      bucket_out[gcur[p] + (q - loff[p])] = bkt[k];
     }
     __syncthreads();
     for (int i = threadIdx.x; i < np; i += blockDim.x) { gcur[i] += hist[i]; hist[i] = 0; }
@@ -180,42 +246,83 @@ __global__ void __launch_bounds__(kPartThreads) hc_scatter1_kernel(const __grid_
   }
 }
 
-// Second level, over the copy (plan Pc: its columns are the copy's, no filters
-// or projections). Work item w is tile (w - item0[p]) of first-level partition
-// p (rows [off1[p], off1[p + 1]) of the copy); its rows go to the buckets
-// p << b2 | p2 of the second copy, each tile claiming its rows of a bucket
-// with one atomic on the bucket's cursor.
-__global__ void __launch_bounds__(kPartThreads) hc_scatter2_kernel(const __grid_constant__ Plan Pc, int b1, int b2,
-                                                                   const int64_t* off1, const int64_t* item0,
-                                                                   int np1, int64_t n_items_total,
-                                                                   unsigned long long* cursor,
-                                                                   const __grid_constant__ HcCols out) {
-  extern __shared__ unsigned long long base[];  // np2 claimed starts, then the arrays below
-  __shared__ uint32_t warp_tot[32];
-  __shared__ int s_p;
+// A run's partition starts and first work items, copied to shared memory once
+// per CTA (np1 <= 256).
+struct HcRunIndex {
+  int64_t off1[257];
+  int64_t item0[257];
+};
+__device__ __forceinline__ void hc_load_index(HcRunIndex& ix, const int64_t* off1, const int64_t* item0, int np1) {
+  for (int i = threadIdx.x; i <= np1; i += blockDim.x) {
+    ix.off1[i] = off1[i];
+    ix.item0[i] = item0[i];
+  }
+  __syncthreads();
+}
+
+// The partition holding work item w (item0: first item of each partition).
+__device__ __forceinline__ int hc_item_partition(const int64_t* item0, int np1, int64_t w) {
+  int lo = 0, hi = np1 - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (item0[mid] <= w) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Rows per bucket of a first-level run: work item w is tile (w - item0[p]) of
+// partition p (rows [off1[p], off1[p + 1]) of the run); bucket q of the
+// partition is the top b2 bits of the row's byte; hist[p << b2 | q]
+// accumulates across runs.
+__global__ void __launch_bounds__(kHcThreads) hc_count2_kernel(const uint8_t* bucket, int b2, const int64_t* off1,
+                                                               const int64_t* item0, int np1, int64_t n_items_total,
+                                                               unsigned long long* hist) {
+  __shared__ uint32_t h[256];
+  __shared__ HcRunIndex ix;
   const int np2 = 1 << b2;
+  hc_load_index(ix, off1, item0, np1);
+  for (int64_t w = blockIdx.x; w < n_items_total; w += gridDim.x) {
+    for (int i = threadIdx.x; i < np2; i += blockDim.x) h[i] = 0;
+    __syncthreads();
+    const int p = hc_item_partition(ix.item0, np1, w);
+    const int64_t t0 = ix.off1[p] + (w - ix.item0[p]) * kHcTile;
+    const int m = (int)min((int64_t)kHcTile, ix.off1[p + 1] - t0);
+    for (int k = threadIdx.x; k < m; k += blockDim.x) atomicAdd(&h[bucket[t0 + k] >> (kHcByteBits - b2)], 1u);
+    __syncthreads();
+    for (int i = threadIdx.x; i < np2; i += blockDim.x)
+      if (h[i]) atomicAdd(&hist[((size_t)p << b2) | (size_t)i], (unsigned long long)h[i]);
+    __syncthreads();
+  }
+}
+
+// Second level, over a run (plan Pc: its columns are the copy's, no filters or
+// projections), items as hc_count2_kernel; each tile's rows go to the buckets
+// p << b2 | q of the second copy, the tile claiming its rows of a bucket
+// with one atomic on the bucket's cursor.
+__global__ void __launch_bounds__(kHcThreads, 2) hc_scatter2_kernel(const __grid_constant__ Plan Pc, int b2,
+                                                                    const uint8_t* bucket, const int64_t* off1,
+                                                                    const int64_t* item0, int np1,
+                                                                    int64_t n_items_total, unsigned long long* cursor,
+                                                                    const __grid_constant__ HcCols out) {
+  extern __shared__ __align__(16) unsigned long long stage[];
+  __shared__ uint32_t warp_tot[32];
+  __shared__ HcRunIndex ix;
+  const int np2 = 1 << b2;
+  unsigned long long* base = stage + kHcTile;
   uint32_t* hist = (uint32_t*)(base + np2);
   uint32_t* loff = hist + np2;
   uint32_t* lcur = loff + np2;
   uint16_t* part = (uint16_t*)(lcur + np2);
-  uint16_t* perm = part + kPartTile;
-  const DynShape sh{Pc};
+  uint16_t* perm = part + kHcTile;
+  hc_load_index(ix, off1, item0, np1);
   for (int64_t w = blockIdx.x; w < n_items_total; w += gridDim.x) {
-    if (threadIdx.x == 0) {  // the partition holding item w
-      int lo = 0, hi = np1 - 1;
-      while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (item0[mid] <= w) lo = mid; else hi = mid - 1;
-      }
-      s_p = lo;
-    }
     for (int i = threadIdx.x; i < np2; i += blockDim.x) hist[i] = 0;
     __syncthreads();
-    const int p = s_p;
-    const int64_t t0 = off1[p] + (w - item0[p]) * kPartTile;
-    const int m = (int)min((int64_t)kPartTile, off1[p + 1] - t0);
+    const int p = hc_item_partition(ix.item0, np1, w);
+    const int64_t t0 = ix.off1[p] + (w - ix.item0[p]) * kHcTile;
+    const int m = (int)min((int64_t)kHcTile, ix.off1[p + 1] - t0);
     for (int k = threadIdx.x; k < m; k += blockDim.x) {
-      const uint32_t q = (uint32_t)(row_key_hash(Pc, sh, t0 + k) >> (64 - b1 - b2)) & (uint32_t)(np2 - 1);
+      const uint32_t q = (uint32_t)bucket[t0 + k] >> (kHcByteBits - b2);
       part[k] = (uint16_t)q;
       atomicAdd(&hist[q], 1u);
     }
@@ -234,48 +341,42 @@ __global__ void __launch_bounds__(kPartThreads) hc_scatter2_kernel(const __grid_
     __syncthreads();
     for (int j = 0; j < out.n; ++j) {
       const int es = out.es[j];
-      const char* scol = (const char*)Pc.in[j].data;
-      char* dcol = out.data[j];
-      for (int qi = threadIdx.x; qi < m; qi += blockDim.x) {
-        const int k = perm[qi];
-        const uint32_t q = part[k];
-        char* d = dcol + (base[q] + (qi - loff[q])) * es;
-        const char* sp = scol + (t0 + k) * es;
-        if (es == 4) *(uint32_t*)d = __ldg((const uint32_t*)sp);
-        else if (es == 8) *(unsigned long long*)d = __ldg((const unsigned long long*)sp);
-        else *(longlong2*)d = __ldg((const longlong2*)sp);
-      }
+      hc_write_column(stage, m, (uint32_t)m, perm, part, base, loff, out.data[j], es,
+                      [&](int k, int w) { return hc_raw_word(Pc, j, es, t0 + k, w); });
     }
-    __syncthreads();
   }
 }
 
-// Buckets: persistent CTAs take buckets b, b + gridDim.x, ...; bucket b's rows
-// are [boff[b], boff[b + 1]) of the plan's columns (the second copy). Each
-// bucket is aggregated in the shared table (P.smem_slots slots, P.smem_sw
-// words each, slot from the hash bits below the bucket's), new groups that no
-// longer fit going to the HBM table P.T; then its groups are appended to
-// `out` (P.L.slot_words words each, float-SUM copies folded in) from a cursor
-// claimed with one atomic. A result that would pass out_cap rows raises
+// Buckets: persistent CTAs (1024 / THREADS per SM, each with its share of the
+// SM's shared memory) take buckets b, b + gridDim.x, ...; bucket b's rows are
+// [boff[b], boff[b + 1]) of the plan's columns (the second copy). Each bucket
+// is aggregated in the shared table (P.smem_slots slots of P.smem_sw words,
+// slot from the hash bits below the bucket's; new groups that no longer fit go
+// to the HBM table P.T). Each insert appends its slot to the used-slot list
+// (P.smem_list), so a bucket's groups are appended to `out` (P.L.slot_words
+// words each, float-SUM copies folded in, from a cursor claimed with one
+// atomic) and their slots re-initialised without sweeping the whole table,
+// which is initialised once. A result that would pass out_cap rows raises
 // *out_over and writes nothing past it.
-template <int NA, class Sh>
-__global__ void __launch_bounds__(1024, 1) hc_bucket_kernel(const __grid_constant__ Plan P, const int64_t* boff,
-                                                            int64_t nb, unsigned long long* out,
-                                                            unsigned long long* out_cursor, int64_t out_cap,
-                                                            int32_t* out_over) {
+template <int NA, class Sh, int THREADS>
+__global__ void __launch_bounds__(THREADS, 1024 / THREADS) hc_bucket_kernel(const __grid_constant__ Plan P,
+                                                                            const int64_t* boff, int64_t nb,
+                                                                            unsigned long long* out,
+                                                                            unsigned long long* out_cursor,
+                                                                            int64_t out_cap, int32_t* out_over) {
   extern __shared__ __align__(16) unsigned long long sm[];
   __shared__ int s_groups;
-  __shared__ uint32_t warp_tot[32];
   __shared__ unsigned long long s_base;
   const Sh sh{P};
   Credit cr;
   const int S = P.smem_slots;
   const int s_limit = (S * 7) / 8;
   const int sw = P.L.slot_words, ssw = smem_stride(P), rep = smem_copies(P);
+  const uint32_t* list = (const uint32_t*)(sm + P.smem_list);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  smem_table_init(P, sm, S, &s_groups);
+  __syncthreads();
   for (int64_t b = blockIdx.x; b < nb; b += gridDim.x) {
-    smem_table_init(P, sm, S, &s_groups);
-    __syncthreads();
     const int64_t r0 = boff[b], r1 = boff[b + 1];
     for (int64_t base = r0 + (int64_t)wid * 32; base < r1; base += (int64_t)nw * 32) {
       const int64_t row = base + lane;
@@ -284,48 +385,30 @@ __global__ void __launch_bounds__(1024, 1) hc_bucket_kernel(const __grid_constan
       process_rows<NA, true>(P, sh, src, act, sm, &s_groups, s_limit, cr);
     }
     __syncthreads();
-    // this thread's used slots: i = threadIdx.x + k * blockDim.x
-    uint32_t mine = 0;
-    for (int i = threadIdx.x; i < S; i += blockDim.x) mine += sm[(size_t)i * ssw] != P.L.init[0] ||
-                                                             (P.L.key_words == 2 && sm[(size_t)i * ssw + 1] != P.L.init[1]);
-    uint32_t x = mine;  // exclusive scan of `mine` over the CTA
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t y = __shfl_up_sync(WG_FULL_MASK, x, o);
-      if (lane >= o) x += y;
-    }
-    if (lane == 31) warp_tot[wid] = x;
+    const int ng = min(s_groups, S);
+    if (threadIdx.x == 0) s_base = ng ? atomicAdd(out_cursor, (unsigned long long)ng) : 0ULL;
     __syncthreads();
-    if (wid == 0) {
-      uint32_t z = lane < nw ? warp_tot[lane] : 0u;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(WG_FULL_MASK, z, o);
-        if (lane >= o) z += y;
+    for (int i = threadIdx.x; i < ng; i += blockDim.x) {
+      unsigned long long* s = sm + (size_t)list[i] * ssw;
+      const unsigned long long at = s_base + (unsigned long long)i;
+      if ((int64_t)at >= out_cap) {
+        *out_over = 1;
+      } else {
+        unsigned long long* d = out + at * (unsigned long long)sw;
+        for (int w = 0; w < sw; ++w) d[w] = s[w];
+        int nf = 0;
+        for (int a = 0; a < P.L.n_aggs; ++a) {
+          if (P.L.agg[a].kind != K_SUM_F64) continue;
+          double t = as_f(s[P.L.agg[a].off]);
+          for (int r = 1; r < rep; ++r) t = __dadd_rn(t, as_f(s[sw + nf * (rep - 1) + (r - 1)]));
+          d[P.L.agg[a].off] = as_w(t);
+          ++nf;
+        }
       }
-      if (lane < nw) warp_tot[lane] = z;
-      if (lane == nw - 1) s_base = z ? atomicAdd(out_cursor, (unsigned long long)z) : 0ULL;
+      for (int w = 0; w < ssw; ++w) s[w] = w < sw ? P.L.init[w] : 0ULL;  // empty again for the next bucket
     }
+    if (threadIdx.x == 0) s_groups = 0;
     __syncthreads();
-    unsigned long long at = s_base + (wid > 0 ? warp_tot[wid - 1] : 0u) + x - mine;
-    for (int i = threadIdx.x; i < S; i += blockDim.x) {
-      const unsigned long long* s = sm + (size_t)i * ssw;
-      const bool used = s[0] != P.L.init[0] || (P.L.key_words == 2 && s[1] != P.L.init[1]);
-      if (!used) continue;
-      if ((int64_t)at >= out_cap) { *out_over = 1; ++at; continue; }
-      unsigned long long* d = out + at * (unsigned long long)sw;
-      for (int w = 0; w < sw; ++w) d[w] = s[w];
-      int nf = 0;
-      for (int a = 0; a < P.L.n_aggs; ++a) {
-        if (P.L.agg[a].kind != K_SUM_F64) continue;
-        double t = as_f(s[P.L.agg[a].off]);
-        for (int r = 1; r < rep; ++r) t = __dadd_rn(t, as_f(s[sw + nf * (rep - 1) + (r - 1)]));
-        d[P.L.agg[a].off] = as_w(t);
-        ++nf;
-      }
-      ++at;
-    }
-    __syncthreads();  // the table is re-initialised for the next bucket
   }
   cr.release(P.T);
 }

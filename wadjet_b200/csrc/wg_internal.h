@@ -109,6 +109,7 @@ struct Ctx {
   int device = 0;
   int sm_count = 148;
   int max_smem_optin = 227 * 1024;
+  int smem_per_sm = 228 * 1024;
   cudaStream_t stream = nullptr;      // compute stream
   cudaStream_t copy_stream = nullptr; // host→device staging stream
   Ledger ledger{0};

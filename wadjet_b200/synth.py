@@ -57,6 +57,15 @@ def highcard(ctx, n: int, seed: int = SEED, row0: int = 0, device: int = 0):
     return a, b, amt, x
 
 
+HC_KEY_SPACE = 1 << 26  # the b column's values are drawn uniformly from this many keys
+
+
+def highcard_groups(n: int) -> int:
+    """Expected distinct (a, b) groups among n rows of the high-cardinality table."""
+    import math
+    return int(HC_KEY_SPACE * -math.expm1(-n / HC_KEY_SPACE))
+
+
 def batched_params(q: int, seed: int = SEED) -> tuple[int, int, int]:
     """(rows, key cardinality, filter threshold) of query q of the batched workload."""
     import ctypes as C
