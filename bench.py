@@ -64,7 +64,8 @@ def parse_args():
     p.add_argument("--ref-rows", type=int, default=FACT_ROWS,
                    help="fact rows per reference (CPU) step; the default is the whole workload")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", choices=["starjoin", "groupby", "highcard", "highcard_spill", "batched", "serving"],
+    p.add_argument("--workload", choices=["starjoin", "groupby", "highcard", "highcard_spill", "batched", "serving",
+                                          "filter"],
                    default="starjoin", help="starjoin is the headline; the others print their own lines")
     p.add_argument("--queries", type=int, default=512, help="batched: queries per batch")
     p.add_argument("--qps", type=float, default=2000.0, help="serving: Poisson arrival rate")
@@ -405,17 +406,25 @@ def run_ours(args, rank: int, world: int, local_rank: int):
 
 
 # ------------------------------------------------------- other workloads --
+_LAST_CLOCKS = [None]  # the clock record of the last timed region
+
+
 def _timed_ms(stream, fn, steps, warmup):
+    """Device time per step (CUDA events on the launching stream, after warm-up), with the SM
+    clocks and throttle reasons sampled during the timed region into _LAST_CLOCKS."""
     import torch
     for _ in range(warmup):
         fn()
     torch.cuda.synchronize()
+    clk = ClockSampler(torch.cuda.current_device())
+    clk.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(steps):
         fn()
     e1.record(stream)
     torch.cuda.synchronize()
+    _LAST_CLOCKS[0] = clk.stop()
     return e0.elapsed_time(e1) / steps
 
 
@@ -449,7 +458,7 @@ def run_groupby(args):
         print(json.dumps({"workload": "groupby", "metric": "rows/s", "rows": n, "value": n / (ms / 1e3),
                           "unit": "rows/s", "ms_per_step": ms, "hbm_gbs": alg / (ms / 1e3) / 1e9,
                           "frac_of_peak": alg / (ms / 1e3) / 1e9 / peak, "peak_kind": peak_kind_note(kind),
-                          "cpu_baseline": cpu}), flush=True)
+                          "algorithmic_bytes": alg, "clocks": _LAST_CLOCKS[0], "cpu_baseline": cpu}), flush=True)
         agg.close()
         del k, v, f, flag
         torch.cuda.empty_cache()
@@ -458,6 +467,52 @@ def run_groupby(args):
 
 def peak_kind_note(kind):
     return f"of {kind} hbm_gbs"
+
+
+def cpu_filter_sample(rows: int) -> float:
+    """rows/s of the oracle's KernelFilter (one host thread, as compareFilterImpl runs per batch)."""
+    import wadjet_b200 as wg
+    from oracle import binding as ob
+    _, qty, _, _ = ob.gen_starjoin_fact(rows, threads=os.cpu_count() or 1)
+    t0 = time.perf_counter()
+    ob.filter_(wg.TYPE_INT32, qty, None, wg.OP_GT, 10)
+    return rows / (time.perf_counter() - t0)
+
+
+def run_filter(args):
+    """KernelFilter on its own: `qty > 10` over the star join's 2^28-row int32 qty column, the
+    compacted selection written to HBM (about 80% of rows pass)."""
+    import torch
+    import wadjet_b200 as wg
+    from wadjet_b200 import synth
+    ctx = wg.Context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    n = args.rows
+    fk, qty, price, disc = synth.starjoin_fact(ctx, n)
+    del fk, price, disc
+    torch.cuda.empty_cache()
+    f = wg.KernelFilter(ctx, 0, wg.OP_GT, 10)
+    batch = wg.Batch([wg.Column(wg.TYPE_INT32, qty)])
+    out = torch.empty(n, dtype=torch.int32, device=qty.device)
+    kept = [0]
+
+    def step():
+        kept[0] = f.execute_device(batch, out)
+
+    ms = _timed_ms(stream, step, args.steps, args.warmup)
+    peak, kind = measured_peak_hbm()
+    alg = n * 4 + kept[0] * 4
+    sample = min(n, 1 << 26)
+    cpu = None if args.no_cpu_baseline else {
+        "value": cpu_filter_sample(sample), "unit": "rows/s", "cores": 1, "kind": "port",
+        "sample": f"{sample} rows of the same column, oracle KernelFilter on one host thread"}
+    print(json.dumps({"workload": "filter", "metric": "rows/s", "rows": n, "kept": kept[0],
+                      "value": n / (ms / 1e3), "unit": "rows/s", "ms_per_step": ms,
+                      "hbm_gbs": alg / (ms / 1e3) / 1e9, "frac_of_peak": alg / (ms / 1e3) / 1e9 / peak,
+                      "peak_kind": peak_kind_note(kind), "algorithmic_bytes": alg, "clocks": _LAST_CLOCKS[0],
+                      "cpu_baseline": cpu}), flush=True)
+    f.close()
+    ctx.close()
 
 
 def run_highcard(args, hbm_cap: int = 0):
@@ -497,7 +552,7 @@ def run_highcard(args, hbm_cap: int = 0):
                       "value": n / (ms / 1e3), "unit": "rows/s", "ms_per_step": ms,
                       "hbm_gbs": alg / (ms / 1e3) / 1e9, "frac_of_peak": alg / (ms / 1e3) / 1e9 / peak,
                       "peak_kind": peak_kind_note(kind), "ledger_peak_bytes": ctx.ledger()["peak"],
-                      "cpu_baseline": cpu}), flush=True)
+                      "algorithmic_bytes": alg, "clocks": _LAST_CLOCKS[0], "cpu_baseline": cpu}), flush=True)
     agg.close()
     ctx.close()
 
@@ -524,6 +579,7 @@ def run_batched(args):
     params = autotune.load_tuned()
     bq = wg.BatchedQueries(ctx, qs, params)
     ms_batched = _timed_ms(stream, bq.run, args.steps, args.warmup)
+    clk_batched = _LAST_CLOCKS[0]
     bq.close()
     # plain path: one aggregate and one pipeline call per query, run back to back
     aggs = [wg.HashAggregate(ctx, q["group_by"], q["aggs"], ndv_hint=q["ndv_hint"]) for q in qs]
@@ -549,7 +605,8 @@ def run_batched(args):
         "speedup_vs_plain": ms_plain / ms_batched,
         "p50_ms": {"batched": ms_batched, "plain": float(np.percentile(done_ms, 50))},
         "p99_ms": {"batched": ms_batched, "plain": float(np.percentile(done_ms, 99))},
-        "hbm_gbs": rows * 20 / (ms_batched / 1e3) / 1e9, "peak": peak, "peak_kind": kind,
+        "hbm_gbs": rows * 20 / (ms_batched / 1e3) / 1e9, "frac_of_peak": rows * 20 / (ms_batched / 1e3) / 1e9 / peak,
+        "peak": peak, "peak_kind": kind, "clocks": clk_batched,
         "tuned": params.__dict__ if params else None}), flush=True)
     ctx.close()
 
@@ -695,7 +752,10 @@ def run_serving(args):
                 "p99_s": float(np.percentile(lat, 99)), "mean_service_s": float("nan")}
 
     sys.setswitchinterval(2e-4)  # the submitting and completing threads hand over quickly
+    clk = ClockSampler(torch.cuda.current_device())
+    clk.start()
     cont = drive(args.slots, gaps)
+    clk_served = clk.stop()
     plain = drive_plain(gaps)
     # capacity: the same requests all queued at once (the server runs saturated)
     burst = np.zeros(min(n_req, 4000))
@@ -711,7 +771,8 @@ def run_serving(args):
         "capacity_qps": {"served": cont_sat["qps"], "plain": plain_sat["qps"],
                          "served_mean_service_ms": 1e3 * cont_sat["mean_service_s"],
                          "plain_p99_ms": 1e3 * plain_sat["p99_s"], "served_p99_ms": 1e3 * cont_sat["p99_s"]},
-        "mean_rows_per_request": float(sizes.mean()), "templates": ["groupby", "join+agg", "ipv4 /24"]}),
+        "mean_rows_per_request": float(sizes.mean()), "templates": ["groupby", "join+agg", "ipv4 /24"],
+        "clocks": clk_served}),
         flush=True)
     join.close()
     ctx.close()
@@ -727,7 +788,7 @@ def main():
         return
     if args.workload != "starjoin":
         {"groupby": run_groupby, "highcard": run_highcard, "batched": run_batched, "serving": run_serving,
-         "highcard_spill": lambda a: run_highcard(a, hbm_cap=8 << 30)}[args.workload](args)
+         "filter": run_filter, "highcard_spill": lambda a: run_highcard(a, hbm_cap=8 << 30)}[args.workload](args)
         return
     run_ours(args, rank, world, local_rank)
 

@@ -447,6 +447,7 @@ struct wg_agg {
   // compact result that stands in for the table (`spilled`).
   bool hc = false;
   int hc_b1 = 0, hc_b2 = 0;
+  int hc_tile = 8192;               // rows per tile of the partition kernels
   std::vector<int32_t> hc_cols;     // copy columns: caller-numbered virtual columns (keys, then agg inputs)
   std::vector<int32_t> hc_es, hc_cls;
   struct HcRun {
@@ -983,7 +984,10 @@ static wg_status run_device(const PipelineRun& r) {
   const int env_bps = env_int("WG_AGG_BLOCKS_PER_SM", 0);
   const int pref_bps = env_bps > 0 ? env_bps : 2;
   int blocks_per_sm = pref_bps;
-  ls.block = ls.vec ? (env_int("WG_VEC_BLOCK", 512) == 768 ? 768 : 512)
+  // vector kernel: 768-thread CTAs (48 warps per SM, no L2 prefetcher: 2.57 ms
+  // against 2.81 ms for 512 threads with it on the 2^28-row star join);
+  // WG_VEC_BLOCK=512 selects the prefetching variant
+  ls.block = ls.vec ? (env_int("WG_VEC_BLOCK", 768) == 512 ? 512 : 768)
                     : stat ? wgd::StatShape<wgd::ShapeStarJoin>::kBlock : wgd::DynShape::kBlock;
   // copies of each float SUM per shared slot (lane-striped, see apply)
   int n_fsum = 0;
@@ -1441,6 +1445,7 @@ static wg_status hc_setup(wg_agg* a, const PipelineRun& r, const wgd::Plan& P0) 
   // from the distinct-key sketch
   a->hc_b1 = 8;
   a->hc_b2 = 0;
+  a->hc_tile = env_int("WG_HC_TILE", 8192) == 4096 ? 4096 : 8192;
   WG_TRY(a->hc_hll.ensure(a->ctx, (int64_t(1) << wgd::kHllBits) * 4));
   WG_CUDA_TRY(cudaMemsetAsync(a->hc_hll.get(), 0, (size_t(1) << wgd::kHllBits) * 4, a->ctx->stream));
   return WG_OK;
@@ -1469,6 +1474,39 @@ static wgd::Plan hc_plan(wg_agg* a, const std::vector<wg::DevBuf>& cols, int64_t
   return P;
 }
 
+// The first level's kernels for one tile size and shape (hc_count_kernel and
+// hc_scatter1_kernel on the same grid).
+template <int TILE, class Sh>
+static wg_status hc_first_level(wg_agg* a, const wgd::Plan& P, unsigned grid, int phase, const wgd::HcCols& out,
+                                int n_pre, uint8_t* bucket_out) {
+  Ctx* ctx = a->ctx;
+  const int np1 = 1 << a->hc_b1;
+  constexpr int threads = wgd::HcGeom<TILE>::threads;
+  if (phase == 0) {
+    wgd::hc_count_kernel<TILE, Sh><<<grid, threads, wgd::hc_count_smem(np1), ctx->stream>>>(
+        P, a->hc_b1, a->hc_counts1.as<uint32_t>(), a->hc_hll.as<uint32_t>());
+  } else {
+    const size_t ss = wgd::hc_scatter_smem(TILE, np1, true);
+    WG_CUDA_TRY(cudaFuncSetAttribute(wgd::hc_scatter1_kernel<TILE, Sh>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)ss));
+    wgd::hc_scatter1_kernel<TILE, Sh><<<grid, threads, ss, ctx->stream>>>(P, a->hc_b1, a->hc_offs1.as<unsigned long long>(),
+                                                                          out, n_pre, bucket_out);
+  }
+  ctx->count_launch();
+  WG_CUDA_TRY(cudaGetLastError());
+  return WG_OK;
+}
+
+static wg_status hc_first_level_any(wg_agg* a, const wgd::Plan& P, bool stat, unsigned grid, int phase,
+                                    const wgd::HcCols& out, int n_pre, uint8_t* bucket_out) {
+  using HC = wgd::StatShape<wgd::ShapeHighCard>;
+  if (a->hc_tile == 4096)
+    return stat ? hc_first_level<4096, HC>(a, P, grid, phase, out, n_pre, bucket_out)
+                : hc_first_level<4096, wgd::DynShape>(a, P, grid, phase, out, n_pre, bucket_out);
+  return stat ? hc_first_level<8192, HC>(a, P, grid, phase, out, n_pre, bucket_out)
+              : hc_first_level<8192, wgd::DynShape>(a, P, grid, phase, out, n_pre, bucket_out);
+}
+
 // One consume call: count the rows per partition and bucket, then write them
 // to a first-level run.
 static wg_status hc_consume(const PipelineRun& r, const wgd::Plan& P0) {
@@ -1495,21 +1533,14 @@ static wg_status hc_consume(const PipelineRun& r, const wgd::Plan& P0) {
   }
   if (a->hc_cls.empty()) { a->hc_cls = cls; for (int j = 0; j < out.n; ++j) a->hc_es.push_back(out.es[j]); }
   else if (a->hc_cls != cls) return fail(WG_E_INVALID, "column classes changed between consume calls");
-  const unsigned grid = (unsigned)ctx->sm_count * 2;  // count and scatter1 share it (2 CTAs per SM)
+  // count and scatter1 share the grid: one CTA per SM (8192-row tiles) or two (4096)
+  const unsigned grid = (unsigned)ctx->sm_count * (a->hc_tile == 4096 ? 2u : 1u);
   WG_TRY(a->hc_counts1.ensure(ctx, (int64_t)np1 * grid * 4));
   WG_TRY(a->hc_offs1.ensure(ctx, (int64_t)np1 * grid * 8));
   // the compiled high-cardinality shape when the input matches it
   wgd::Plan probe = P;
   const bool stat = wgd::shape_matches<wgd::ShapeHighCard>(probe) && env_int("WG_SPECIALIZE", 1) != 0;
-  if (stat)
-    wgd::hc_count_kernel<wgd::StatShape<wgd::ShapeHighCard>><<<grid, wgd::kHcThreads, wgd::hc_count_smem(np1),
-                                                                ctx->stream>>>(P, a->hc_b1, a->hc_counts1.as<uint32_t>(),
-                                                                               a->hc_hll.as<uint32_t>());
-  else
-    wgd::hc_count_kernel<wgd::DynShape><<<grid, wgd::kHcThreads, wgd::hc_count_smem(np1), ctx->stream>>>(
-        P, a->hc_b1, a->hc_counts1.as<uint32_t>(), a->hc_hll.as<uint32_t>());
-  ctx->count_launch();
-  WG_CUDA_TRY(cudaGetLastError());
+  WG_TRY(hc_first_level_any(a, P, stat, grid, 0, out, 0, nullptr));
   std::vector<uint32_t> hc((size_t)np1 * grid);
   std::vector<unsigned long long> ho((size_t)np1 * grid);
   WG_CUDA_TRY(cudaMemcpyAsync(hc.data(), a->hc_counts1.get(), hc.size() * 4, cudaMemcpyDeviceToHost, ctx->stream));
@@ -1532,20 +1563,17 @@ static wg_status hc_consume(const PipelineRun& r, const wgd::Plan& P0) {
     out.data[j] = run.cols[(size_t)j].as<char>();
   }
   WG_TRY(run.bucket.ensure(ctx, std::max<int64_t>(run.rows, 1)));
-  const size_t ss = wgd::hc_scatter_smem(np1, true);
-  if (stat) {
-    auto* k = wgd::hc_scatter1_kernel<wgd::StatShape<wgd::ShapeHighCard>>;
-    WG_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss));
-    k<<<grid, wgd::kHcThreads, ss, ctx->stream>>>(P, a->hc_b1, a->hc_offs1.as<unsigned long long>(), out,
-                                                    run.bucket.as<uint8_t>());
-  } else {
-    auto* k = wgd::hc_scatter1_kernel<wgd::DynShape>;
-    WG_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss));
-    k<<<grid, wgd::kHcThreads, ss, ctx->stream>>>(P, a->hc_b1, a->hc_offs1.as<unsigned long long>(), out,
-                                                    run.bucket.as<uint8_t>());
+  // the leading copy columns that are input columns of 4 or 8 bytes (the keys
+  // come first) are staged while the rows are hashed
+  int n_pre = 0;
+  for (int j = 0, bytes = 0; j < out.n; ++j) {
+    if (out.vcol[j] >= P.n_in || (out.es[j] != 4 && out.es[j] != 8) || bytes + a->hc_tile * out.es[j] > a->hc_tile * 16)
+      break;
+    bytes += a->hc_tile * out.es[j];
+    n_pre = j + 1;
   }
-  ctx->count_launch();
-  WG_CUDA_TRY(cudaGetLastError());
+  if (n_pre > (int)a->key_cols.size()) n_pre = (int)a->key_cols.size();
+  WG_TRY(hc_first_level_any(a, P, stat, grid, 1, out, n_pre, run.bucket.as<uint8_t>()));
   a->hc_runs.push_back(std::move(run));
   return check_device_error(ctx);
 }
@@ -1612,7 +1640,7 @@ static wg_status hc_finish(wg_agg* a) {
   WG_TRY(a->hc_dev.ensure(ctx, scal * 8));
   int64_t* d_boff = a->hc_dev.as<int64_t>();
   unsigned long long* d_cur = (unsigned long long*)(d_boff + nb + 1);
-  // per run: its partition starts and first work items (tiles of kHcTile rows) on the device
+  // per run: its partition starts and first work items (tiles of hc_tile rows) on the device
   std::vector<int64_t> run_items(a->hc_runs.size(), 0);
   for (size_t ri = 0; ri < a->hc_runs.size(); ++ri) {
     const auto& run = a->hc_runs[ri];
@@ -1620,7 +1648,7 @@ static wg_status hc_finish(wg_agg* a) {
     int64_t items = 0;
     for (int p = 0; p < np1; ++p) {
       item0[(size_t)p] = items;
-      items += (run.off1[(size_t)p + 1] - run.off1[(size_t)p] + wgd::kHcTile - 1) / wgd::kHcTile;
+      items += (run.off1[(size_t)p + 1] - run.off1[(size_t)p] + a->hc_tile - 1) / a->hc_tile;
     }
     item0[(size_t)np1] = items;
     run_items[ri] = items;
@@ -1636,9 +1664,14 @@ static wg_status hc_finish(wg_agg* a) {
     if (a->hc_runs[ri].rows == 0) continue;
     const int64_t* d_off1 = (const int64_t*)(d_cur + nb) + 2 * ((int64_t)np1 + 1) * (int64_t)ri;
     const unsigned grid = (unsigned)std::min<int64_t>((int64_t)ctx->sm_count * 4, run_items[ri]);
-    wgd::hc_count2_kernel<<<grid, wgd::kHcThreads, 0, ctx->stream>>>(a->hc_runs[ri].bucket.as<uint8_t>(), b2, d_off1,
-                                                                      d_off1 + np1 + 1, np1, run_items[ri],
-                                                                      a->hc_hist.as<unsigned long long>());
+    if (a->hc_tile == 4096)
+      wgd::hc_count2_kernel<4096><<<grid, wgd::kHcThreads, 0, ctx->stream>>>(
+          a->hc_runs[ri].bucket.as<uint8_t>(), b2, d_off1, d_off1 + np1 + 1, np1, run_items[ri],
+          a->hc_hist.as<unsigned long long>());
+    else
+      wgd::hc_count2_kernel<8192><<<grid, wgd::kHcThreads, 0, ctx->stream>>>(
+          a->hc_runs[ri].bucket.as<uint8_t>(), b2, d_off1, d_off1 + np1 + 1, np1, run_items[ri],
+          a->hc_hist.as<unsigned long long>());
     ctx->count_launch();
     WG_CUDA_TRY(cudaGetLastError());
   }
@@ -1662,17 +1695,24 @@ static wg_status hc_finish(wg_agg* a) {
     out2.es[j] = a->hc_es[(size_t)j];
     out2.vcol[j] = j;
   }
-  const size_t ss = wgd::hc_scatter_smem(np2, false);
-  WG_CUDA_TRY(cudaFuncSetAttribute(wgd::hc_scatter2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss));
+  const size_t ss = wgd::hc_scatter_smem(a->hc_tile, np2, false);
+  if (a->hc_tile == 4096)
+    WG_CUDA_TRY(cudaFuncSetAttribute(wgd::hc_scatter2_kernel<4096>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss));
+  else
+    WG_CUDA_TRY(cudaFuncSetAttribute(wgd::hc_scatter2_kernel<8192>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss));
   for (size_t ri = 0; ri < a->hc_runs.size(); ++ri) {
     auto& run = a->hc_runs[ri];
     if (run.rows == 0) continue;
     const int64_t* d_off1 = (const int64_t*)(d_cur + nb) + 2 * ((int64_t)np1 + 1) * (int64_t)ri;
     wgd::Plan Pc = hc_plan(a, run.cols, run.rows);
-    const unsigned grid = (unsigned)std::min<int64_t>((int64_t)ctx->sm_count * 2, run_items[ri]);
-    wgd::hc_scatter2_kernel<<<grid, wgd::kHcThreads, ss, ctx->stream>>>(Pc, b2, run.bucket.as<uint8_t>(), d_off1,
-                                                                         d_off1 + np1 + 1, np1, run_items[ri], d_cur,
-                                                                         out2);
+    const int64_t slots = (int64_t)ctx->sm_count * (a->hc_tile == 4096 ? 2 : 1);
+    const unsigned grid = (unsigned)std::min<int64_t>(slots, run_items[ri]);
+    if (a->hc_tile == 4096)
+      wgd::hc_scatter2_kernel<4096><<<grid, wgd::HcGeom<4096>::threads, ss, ctx->stream>>>(
+          Pc, b2, run.bucket.as<uint8_t>(), d_off1, d_off1 + np1 + 1, np1, run_items[ri], d_cur, out2);
+    else
+      wgd::hc_scatter2_kernel<8192><<<grid, wgd::HcGeom<8192>::threads, ss, ctx->stream>>>(
+          Pc, b2, run.bucket.as<uint8_t>(), d_off1, d_off1 + np1 + 1, np1, run_items[ri], d_cur, out2);
     ctx->count_launch();
     WG_CUDA_TRY(cudaGetLastError());
   }
@@ -2290,6 +2330,9 @@ wg_status wg_agg_reset(wg_agg* a) {
       WG_CUDA_TRY(cudaMemsetAsync(a->hc_hll.get(), 0, (size_t(1) << wgd::kHllBits) * 4, ctx->stream));
   }
   if (a->spilled) {  // the table holds a compact result: back to an empty small table
+    // a two-level aggregate keeps the result buffer for its next finalize (as
+    // it keeps its runs), instead of freeing and allocating gigabytes per query
+    if (a->hc && a->table.bytes() > a->hc_out.bytes()) a->hc_out = std::move(a->table);
     a->table.reset();
     a->cap = a->small_cap;
     a->shift = 64 - log2u(a->cap);

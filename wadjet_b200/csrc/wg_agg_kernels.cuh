@@ -1385,10 +1385,13 @@ __global__ void __launch_bounds__(BLK, MB) pipeline_vec_kernel(const __grid_cons
   const int64_t step = (int64_t)gridDim.x * wpb * 32 * U;
   const int64_t ahead = (int64_t)P.prefetch * step;
   const int64_t base0 = ((int64_t)blockIdx.x * wpb + (threadIdx.x >> 5)) * 32 * U;
+  // the 768-thread variant (48 warps per SM) hides HBM latency with warps and
+  // leaves the prefetcher's registers to the rows (40 per thread)
+  constexpr bool kPrefetch = BLK != 768;
   Prefetcher<32 * U> pf;
-  if (ahead > 0) pf.init(P, sh, base0 + ahead, step, lane);
+  if (kPrefetch && ahead > 0) pf.init(P, sh, base0 + ahead, step, lane);
   for (int64_t base = base0; base < P.n_items; base += step) {
-    pf.next();
+    if (kPrefetch) pf.next();
     process_rows_vec<NA, SMEM, U>(P, sh, base + (int64_t)lane * U, sm, &s_groups, s_limit, cr);
   }
   if (SMEM) {

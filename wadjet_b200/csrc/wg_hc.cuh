@@ -62,13 +62,20 @@ __device__ __forceinline__ bool row_passes(const Plan& P, const Sh& sh, int64_t 
   return true;
 }
 
-// The count and the first-level scatter walk the input in tiles of kHcTile
+// The count and the first-level scatter walk the input in tiles of TILE
 // rows, CTA c taking tiles c, c + gridDim.x, ... (both launched on the same
-// grid), so the rows a CTA counts per partition are exactly the rows it later
-// writes there.
-constexpr int kHcThreads = 512;
-constexpr int kHcTile = 8192;
-static_assert(kHcTile <= 65536, "tile-local row indices are 16-bit");
+// grid, one 1024-thread CTA per SM), so the rows a CTA counts per partition
+// are exactly the rows it later writes there.
+// Tiles of TILE rows, 8 per thread: 8192-row tiles in one 1024-thread CTA per
+// SM, or 4096-row tiles in two 512-thread CTAs per SM (WG_HC_TILE), whose
+// phases then overlap.
+constexpr int kHcThreads = 1024;  // count2's CTAs
+template <int TILE> struct HcGeom {
+  static_assert(TILE == 8192 || TILE == 4096, "tile rows");
+  static constexpr int threads = TILE / 8;
+  static constexpr int ctas = 8192 / TILE;  // per SM
+  static constexpr int stage_bytes = TILE * 16;  // one column of up to 16-byte values
+};
 
 // Bits of the per-row bucket byte the first level writes: the second level
 // uses its top b2 <= 8 bits, b2 chosen when the groups have been estimated.
@@ -83,8 +90,8 @@ constexpr size_t hc_count_smem(int np1) { return (size_t)np1 * 4 + ((size_t)1 <<
 // (max-merged into hll). Register index: the hash's low kHllBits bits; rank:
 // leading zeros of the remaining bits, plus one. The low bits are independent
 // of the top bits that pick partitions and buckets.
-template <class Sh>
-__global__ void __launch_bounds__(kHcThreads, 2) hc_count_kernel(const __grid_constant__ Plan P, int b1,
+template <int TILE, class Sh>
+__global__ void __launch_bounds__(HcGeom<TILE>::threads, HcGeom<TILE>::ctas) hc_count_kernel(const __grid_constant__ Plan P, int b1,
                                                                  uint32_t* counts1, uint32_t* hll) {
   extern __shared__ uint32_t h1[];
   const int np1 = 1 << b1;
@@ -92,8 +99,8 @@ __global__ void __launch_bounds__(kHcThreads, 2) hc_count_kernel(const __grid_co
   for (int i = threadIdx.x; i < np1 + (1 << kHllBits); i += blockDim.x) h1[i] = 0;
   __syncthreads();
   const Sh sh{P};
-  for (int64_t t0 = (int64_t)blockIdx.x * kHcTile; t0 < P.n_items; t0 += (int64_t)gridDim.x * kHcTile) {
-    const int m = (int)min((int64_t)kHcTile, P.n_items - t0);
+  for (int64_t t0 = (int64_t)blockIdx.x * TILE; t0 < P.n_items; t0 += (int64_t)gridDim.x * TILE) {
+    const int m = (int)min((int64_t)TILE, P.n_items - t0);
     for (int k = threadIdx.x; k < m; k += blockDim.x) {
       if (!row_passes(P, sh, t0 + k)) continue;
       const unsigned long long h = row_key_hash(P, sh, t0 + k);
@@ -118,90 +125,104 @@ struct HcCols {
   int32_t n;
 };
 
-// Word w of a value as the copy stores it: 4- and 8-byte values whole, a
-// 16-byte one as {hi, lo}.
-__device__ __forceinline__ unsigned long long val_word(int es, const Val& v, int w) {
-  return es == 16 ? (w == 0 ? v.hi : v.lo) : v.lo;
+// Shared memory of the scatter kernels: the staging area, np output cursors
+// (8 B) and per-partition hist / offset / cursor (12 B), then per tile row its
+// partition and its place in the order (2 B each) and, for the first level,
+// its bucket byte. One CTA per SM.
+__host__ __device__ constexpr size_t hc_scatter_smem(int tile, int np, bool bucket_bytes) {
+  return (size_t)tile * 16 + (size_t)np * 20 + (size_t)tile * (bucket_bytes ? 5 : 4);
 }
 
-// Shared memory of the scatter kernels: kHcTile staging words, np output
-// cursors (8 B) and per-partition hist / offset / cursor (12 B), then per tile
-// row its partition and its place in the order (2 B each) and, for the first
-// level, its bucket byte. Two CTAs fit an SM.
-__host__ __device__ constexpr size_t hc_scatter_smem(int np, bool bucket_bytes) {
-  return (size_t)kHcTile * 8 + (size_t)np * 20 + (size_t)kHcTile * (bucket_bytes ? 5 : 4);
+// A column value as the copy stores it: 4 or 8 bytes in x, a 16-byte one as
+// {x = hi, y = lo}.
+__device__ __forceinline__ ulonglong2 copy_val(int es, const Val& v) {
+  ulonglong2 r;
+  r.x = es == 16 ? v.hi : v.lo;
+  r.y = v.lo;
+  return r;
+}
+
+// Row r of input column j read as it lies (es bytes).
+__device__ __forceinline__ ulonglong2 hc_raw(const Plan& P, int j, int es, int64_t r) {
+  const char* base = (const char*)P.in[j].data;
+  ulonglong2 v;
+  v.y = 0;
+  if (es == 4) {
+    v.x = __ldg((const uint32_t*)base + r);
+  } else if (es == 8) {
+    v.x = __ldg((const unsigned long long*)base + r);
+  } else {
+    const longlong2 t = __ldg((const longlong2*)base + r);
+    v.x = (unsigned long long)t.x;
+    v.y = (unsigned long long)t.y;
+  }
+  return v;
+}
+
+__device__ __forceinline__ void stage_put(void* stage, int es, int k, ulonglong2 v) {
+  if (es == 4) ((uint32_t*)stage)[k] = (uint32_t)v.x;
+  else if (es == 8) ((unsigned long long*)stage)[k] = v.x;
+  else ((ulonglong2*)stage)[k] = v;
 }
 
 // Tile rows in partition order. Position q of the order holds tile row
 // perm[q] of partition part[perm[q]], which goes to output row
-// dst[p] + q - loff[p]. Each copy column is staged in shared memory in tile-row
-// order (reads coalesced), then stored in partition order (stores in runs of
-// one partition): `stage_fn(k, w)` gives word w of tile row k's value (16-byte
-// values go as two 8-byte words).
-template <class StageFn>
-__device__ __forceinline__ void hc_write_column(unsigned long long* stage, int m, uint32_t kept, const uint16_t* perm,
+// dst[p] + q - loff[p]. The column's tile values are in `stage` in tile-row
+// order (staged with coalesced reads); they are stored in partition order
+// (stores in runs of one partition).
+__device__ __forceinline__ void hc_store_column(const void* stage, uint32_t kept, const uint16_t* perm,
                                                 const uint16_t* part, const unsigned long long* dst,
-                                                const uint32_t* loff, char* dcol, int es, StageFn stage_fn) {
-  const int words = es == 16 ? 2 : 1;
-  for (int w = 0; w < words; ++w) {
-    if (es == 4) {
-      uint32_t* st = (uint32_t*)stage;
-#pragma unroll 4
-      for (int k = threadIdx.x; k < m; k += blockDim.x) st[k] = (uint32_t)stage_fn(k, w);
-    } else {
-#pragma unroll 4
-      for (int k = threadIdx.x; k < m; k += blockDim.x) stage[k] = stage_fn(k, w);
-    }
-    __syncthreads();
-    for (uint32_t q = threadIdx.x; q < kept; q += blockDim.x) {
-      const int k = perm[q];
-      const uint32_t p = part[k];
-      const unsigned long long row = dst[p] + (q - loff[p]);
-      if (es == 4) ((uint32_t*)dcol)[row] = ((const uint32_t*)stage)[k];
-      else if (es == 8) ((unsigned long long*)dcol)[row] = stage[k];
-      else ((unsigned long long*)dcol)[row * 2 + w] = stage[k];
-    }
-    __syncthreads();
+                                                const uint32_t* loff, char* dcol, int es) {
+  for (uint32_t q = threadIdx.x; q < kept; q += blockDim.x) {
+    const int k = perm[q];
+    const uint32_t p = part[k];
+    const unsigned long long row = dst[p] + (q - loff[p]);
+    if (es == 4) ((uint32_t*)dcol)[row] = ((const uint32_t*)stage)[k];
+    else if (es == 8) ((unsigned long long*)dcol)[row] = ((const unsigned long long*)stage)[k];
+    else ((ulonglong2*)dcol)[row] = ((const ulonglong2*)stage)[k];
   }
-}
-
-// Word w of input column j at row r, read as it lies.
-__device__ __forceinline__ unsigned long long hc_raw_word(const Plan& P, int j, int es, int64_t r, int w) {
-  const char* base = (const char*)P.in[j].data;
-  if (es == 4) return __ldg((const uint32_t*)base + r);
-  if (es == 8) return __ldg((const unsigned long long*)base + r);
-  return __ldg((const unsigned long long*)base + r * 2 + w);
 }
 
 // First level: the input's rows passing the filters, written as the copy's
 // columns in partition order (partition p of CTA c from offs[p * gridDim.x + c];
 // tiles as hc_count_kernel), and with each row its bucket byte (the next 8
 // hash bits), from which the second level splits without hashing again.
-template <class Sh>
-__global__ void __launch_bounds__(kHcThreads, 2) hc_scatter1_kernel(const __grid_constant__ Plan P, int b1,
+// Every input byte is read from HBM once: the first n_pre copy columns (input
+// key columns of 4 or 8 bytes) are staged side by side while the rows are
+// hashed, the other columns one at a time afterwards.
+template <int TILE, class Sh>
+__global__ void __launch_bounds__(HcGeom<TILE>::threads, HcGeom<TILE>::ctas) hc_scatter1_kernel(const __grid_constant__ Plan P, int b1,
                                                                     const unsigned long long* offs,
-                                                                    const __grid_constant__ HcCols out,
+                                                                    const __grid_constant__ HcCols out, int n_pre,
                                                                     uint8_t* bucket_out) {
   extern __shared__ __align__(16) unsigned long long stage[];
   __shared__ uint32_t warp_tot[32];
+  __shared__ int pre_off[WG_MAX_IN];
   const int np = 1 << b1;
-  unsigned long long* gcur = stage + kHcTile;
+  char* stg = (char*)stage;
+  unsigned long long* gcur = (unsigned long long*)(stg + HcGeom<TILE>::stage_bytes);
   uint32_t* hist = (uint32_t*)(gcur + np);
   uint32_t* loff = hist + np;
   uint32_t* lcur = loff + np;
   uint16_t* part = (uint16_t*)(lcur + np);  // partition of tile row k (np = dropped)
-  uint16_t* perm = part + kHcTile;
-  uint8_t* bkt = (uint8_t*)(perm + kHcTile);
+  uint16_t* perm = part + TILE;
+  uint8_t* bkt = (uint8_t*)(perm + TILE);
+  if (threadIdx.x == 0) {
+    int off = 0;
+    for (int j = 0; j < n_pre; ++j) { pre_off[j] = off; off += TILE * out.es[j]; }
+  }
   for (int i = threadIdx.x; i < np; i += blockDim.x) {
     gcur[i] = offs[(size_t)i * gridDim.x + blockIdx.x];
     hist[i] = 0;
   }
   __syncthreads();
   const Sh sh{P};
-  for (int64_t t0 = (int64_t)blockIdx.x * kHcTile; t0 < P.n_items; t0 += (int64_t)gridDim.x * kHcTile) {
-    const int m = (int)min((int64_t)kHcTile, P.n_items - t0);
+  for (int64_t t0 = (int64_t)blockIdx.x * TILE; t0 < P.n_items; t0 += (int64_t)gridDim.x * TILE) {
+    const int m = (int)min((int64_t)TILE, P.n_items - t0);
     for (int k = threadIdx.x; k < m; k += blockDim.x) {
       uint32_t p = (uint32_t)np;
+      for (int j = 0; j < n_pre; ++j)
+        stage_put(stg + pre_off[j], out.es[j], k, hc_raw(P, out.vcol[j], out.es[j], t0 + k));
       if (row_passes(P, sh, t0 + k)) {
         const unsigned long long h = row_key_hash(P, sh, t0 + k);
         p = (uint32_t)(h >> (64 - b1));
@@ -220,25 +241,30 @@ __global__ void __launch_bounds__(kHcThreads, 2) hc_scatter1_kernel(const __grid
       if (p < (uint32_t)np) perm[loff[p] + atomicAdd(&lcur[p], 1u)] = (uint16_t)k;
     }
     __syncthreads();
-    for (int j = 0; j < out.n; ++j) {
-      const int es = out.es[j], vc = out.vcol[j];
-      if (vc < P.n_in) {  // an input column: its bytes as they are
-        hc_write_column(stage, m, kept, perm, part, gcur, loff, out.data[j], es,
-                        [&](int k, int w) { return hc_raw_word(P, vc, es, t0 + k, w); });
-      } else {  // a projection, evaluated per kept row
-        hc_write_column(stage, m, kept, perm, part, gcur, loff, out.data[j], es, [&](int k, int w) {
-          if (part[k] >= (uint16_t)np) return 0ULL;
-          const SrcGlobal src{t0 + k};
-          ExprVals ev;
-          eval_exprs(P, sh, src, -1, ev);
-          return val_word(es, fetch(P, sh, src, vc, -1, ev), w);
-        });
-      }
-    }
+    for (int j = 0; j < n_pre; ++j)  // staged while hashing
+      hc_store_column(stg + pre_off[j], kept, perm, part, gcur, loff, out.data[j], out.es[j]);
     for (uint32_t q = threadIdx.x; q < kept; q += blockDim.x) {
       const int k = perm[q];
       const uint32_t p = part[k];
       bucket_out[gcur[p] + (q - loff[p])] = bkt[k];
+    }
+    for (int j = n_pre; j < out.n; ++j) {
+      const int es = out.es[j], vc = out.vcol[j];
+      __syncthreads();  // the staging area is free again
+      if (vc < P.n_in) {  // an input column: its bytes as they are
+#pragma unroll 4
+        for (int k = threadIdx.x; k < m; k += blockDim.x) stage_put(stg, es, k, hc_raw(P, vc, es, t0 + k));
+      } else {  // a projection, evaluated per kept row
+        for (int k = threadIdx.x; k < m; k += blockDim.x) {
+          if (part[k] >= (uint16_t)np) continue;
+          const SrcGlobal src{t0 + k};
+          ExprVals ev;
+          eval_exprs(P, sh, src, -1, ev);
+          stage_put(stg, es, k, copy_val(es, fetch(P, sh, src, vc, -1, ev)));
+        }
+      }
+      __syncthreads();
+      hc_store_column(stg, kept, perm, part, gcur, loff, out.data[j], es);
     }
     __syncthreads();
     for (int i = threadIdx.x; i < np; i += blockDim.x) { gcur[i] += hist[i]; hist[i] = 0; }
@@ -274,6 +300,7 @@ __device__ __forceinline__ int hc_item_partition(const int64_t* item0, int np1, 
 // partition p (rows [off1[p], off1[p + 1]) of the run); bucket q of the
 // partition is the top b2 bits of the row's byte; hist[p << b2 | q]
 // accumulates across runs.
+template <int TILE>
 __global__ void __launch_bounds__(kHcThreads) hc_count2_kernel(const uint8_t* bucket, int b2, const int64_t* off1,
                                                                const int64_t* item0, int np1, int64_t n_items_total,
                                                                unsigned long long* hist) {
@@ -285,8 +312,8 @@ __global__ void __launch_bounds__(kHcThreads) hc_count2_kernel(const uint8_t* bu
     for (int i = threadIdx.x; i < np2; i += blockDim.x) h[i] = 0;
     __syncthreads();
     const int p = hc_item_partition(ix.item0, np1, w);
-    const int64_t t0 = ix.off1[p] + (w - ix.item0[p]) * kHcTile;
-    const int m = (int)min((int64_t)kHcTile, ix.off1[p + 1] - t0);
+    const int64_t t0 = ix.off1[p] + (w - ix.item0[p]) * TILE;
+    const int m = (int)min((int64_t)TILE, ix.off1[p + 1] - t0);
     for (int k = threadIdx.x; k < m; k += blockDim.x) atomicAdd(&h[bucket[t0 + k] >> (kHcByteBits - b2)], 1u);
     __syncthreads();
     for (int i = threadIdx.x; i < np2; i += blockDim.x)
@@ -299,7 +326,8 @@ __global__ void __launch_bounds__(kHcThreads) hc_count2_kernel(const uint8_t* bu
 // projections), items as hc_count2_kernel; each tile's rows go to the buckets
 // p << b2 | q of the second copy, the tile claiming its rows of a bucket
 // with one atomic on the bucket's cursor.
-__global__ void __launch_bounds__(kHcThreads, 2) hc_scatter2_kernel(const __grid_constant__ Plan Pc, int b2,
+template <int TILE>
+__global__ void __launch_bounds__(HcGeom<TILE>::threads, HcGeom<TILE>::ctas) hc_scatter2_kernel(const __grid_constant__ Plan Pc, int b2,
                                                                     const uint8_t* bucket, const int64_t* off1,
                                                                     const int64_t* item0, int np1,
                                                                     int64_t n_items_total, unsigned long long* cursor,
@@ -308,19 +336,20 @@ __global__ void __launch_bounds__(kHcThreads, 2) hc_scatter2_kernel(const __grid
   __shared__ uint32_t warp_tot[32];
   __shared__ HcRunIndex ix;
   const int np2 = 1 << b2;
-  unsigned long long* base = stage + kHcTile;
+  char* stg = (char*)stage;
+  unsigned long long* base = (unsigned long long*)(stg + HcGeom<TILE>::stage_bytes);
   uint32_t* hist = (uint32_t*)(base + np2);
   uint32_t* loff = hist + np2;
   uint32_t* lcur = loff + np2;
   uint16_t* part = (uint16_t*)(lcur + np2);
-  uint16_t* perm = part + kHcTile;
+  uint16_t* perm = part + TILE;
   hc_load_index(ix, off1, item0, np1);
   for (int64_t w = blockIdx.x; w < n_items_total; w += gridDim.x) {
     for (int i = threadIdx.x; i < np2; i += blockDim.x) hist[i] = 0;
     __syncthreads();
     const int p = hc_item_partition(ix.item0, np1, w);
-    const int64_t t0 = ix.off1[p] + (w - ix.item0[p]) * kHcTile;
-    const int m = (int)min((int64_t)kHcTile, ix.off1[p + 1] - t0);
+    const int64_t t0 = ix.off1[p] + (w - ix.item0[p]) * TILE;
+    const int m = (int)min((int64_t)TILE, ix.off1[p + 1] - t0);
     for (int k = threadIdx.x; k < m; k += blockDim.x) {
       const uint32_t q = (uint32_t)bucket[t0 + k] >> (kHcByteBits - b2);
       part[k] = (uint16_t)q;
@@ -338,12 +367,15 @@ __global__ void __launch_bounds__(kHcThreads, 2) hc_scatter2_kernel(const __grid
       const uint32_t q = part[k];
       perm[loff[q] + atomicAdd(&lcur[q], 1u)] = (uint16_t)k;
     }
-    __syncthreads();
     for (int j = 0; j < out.n; ++j) {
       const int es = out.es[j];
-      hc_write_column(stage, m, (uint32_t)m, perm, part, base, loff, out.data[j], es,
-                      [&](int k, int w) { return hc_raw_word(Pc, j, es, t0 + k, w); });
+      __syncthreads();  // perm complete; the staging area free again
+#pragma unroll 4
+      for (int k = threadIdx.x; k < m; k += blockDim.x) stage_put(stg, es, k, hc_raw(Pc, j, es, t0 + k));
+      __syncthreads();
+      hc_store_column(stg, (uint32_t)m, perm, part, base, loff, out.data[j], es);
     }
+    __syncthreads();
   }
 }
 
