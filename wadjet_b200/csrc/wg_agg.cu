@@ -30,6 +30,9 @@ int32_t join_payload_type(wg_join* j, int i);
 int32_t join_payload_scale(wg_join* j, int i);
 bool join_payload_nullable(wg_join* j, int i);
 bool join_payload_range(wg_join* j, int i, long long* lo, long long* hi);
+bool join_is_grace(wg_join* j);
+int join_grace_passes(wg_join* j);
+wg_status join_grace_pass(wg_join* j, int g, wg_join** out);
 int64_t join_max_fanout(wg_join* j);
 int32_t join_type_of(wg_join* j);
 }  // namespace wg
@@ -2053,6 +2056,17 @@ namespace wg {
 // Access for the pipeline entry points (wg_pipeline.cu).
 wg_status agg_run_device(wg_agg* a, const wg_batch_desc* in, int32_t nf, const wg_predicate* f, wg_join* j, int32_t ne,
                          const wg_expr* e, bool defer_check) {
+  if (j && join_is_grace(j)) {
+    // a partitioned build: one pass per group of its partitions, each probe row
+    // taking part in the pass of its key's partition
+    for (int g = 0; g < join_grace_passes(j); ++g) {
+      wg_join* pj = nullptr;
+      WG_TRY(join_grace_pass(j, g, &pj));
+      PipelineRun r{a, in, nf, f, pj, ne, e};
+      WG_TRY(run_device(r));
+    }
+    return WG_OK;
+  }
   PipelineRun r{a, in, nf, f, j, ne, e};
   r.defer_check = defer_check;
   return run_device(r);
@@ -2789,6 +2803,9 @@ wg_status wg_batched_create(wg_ctx* ctx, int32_t n, const wg_batched_query* qs, 
     if (x.n_exprs < 0 || x.n_exprs > WG_MAX_EXPRS || (x.n_exprs > 0 && !x.exprs))
       return cleanup(fail(WG_E_INVALID, "batched query " + std::to_string(q) + ": bad projections"));
     b->exprs[q].assign(x.exprs, x.exprs + x.n_exprs);
+    if (x.join && join_is_grace(x.join))
+      return cleanup(fail(WG_E_UNSUPPORTED, "batched query " + std::to_string(q) +
+                                                ": a partitioned join build runs through the pipeline entry points"));
     b->joins[q] = x.join;
     wg_status s = wg_agg_create(ctx, x.n_keys, x.key_cols, x.n_aggs, x.aggs, x.ndv_hint, &b->aggs[q]);
     if (s != WG_OK) return cleanup(s);

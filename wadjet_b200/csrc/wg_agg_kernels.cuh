@@ -852,6 +852,10 @@ __device__ __forceinline__ void process_rows(const Plan& P, const Sh& sh, const 
   const int jt = sh.has_join() ? (sh.direct() ? WG_JOIN_INNER : P.join.jtype) : WG_JOIN_INNER;
   if (sh.has_join() && act) {
     const Val kv = src.in(P, sh, sh.probe_col());
+    if (!join_pass_mine(P.join, kv.null, (long long)kv.lo)) act = false;  // another pass's row
+  }
+  if (sh.has_join() && act) {
+    const Val kv = src.in(P, sh, sh.probe_col());
     bool found = false;
     if (kv.null) found = false;  // NULL keys never match (join.go:2700)
     else if (sh.direct()) found = join_direct(P.join, (int64_t)kv.lo, brow, P.err);
@@ -1304,6 +1308,7 @@ __device__ __forceinline__ void process_loaded_vec(const Plan& P, const Sh& sh, 
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const Val kv = rw[u].v[sh.probe_col()];
+      if (act[u] && !join_pass_mine(P.join, kv.null, (long long)kv.lo)) act[u] = false;  // another pass's row
       if (act[u]) {
         if (sh.in_cls(sh.probe_col()) == WG_CLS_I32)
           act[u] = !kv.null && join_direct_i32(P.join, (int32_t)kv.lo, brow[u], P.err);

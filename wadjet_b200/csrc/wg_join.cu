@@ -328,6 +328,28 @@ struct wg_join {
   std::vector<long long> pay_lo, pay_hi;
   std::vector<bool> pay_range;
   wg::StagedBatch staged;
+  // Partitioned build (the partition-on-arrival grace build of
+  // join_partition_arrival.go:48): when the HBM ledger refuses the build's
+  // columns or index, its rows move to host memory split into 64 partitions by
+  // key hash (join_partition, NULL keys dropped: they match nothing), and the
+  // fused pipeline probes in passes, each over a group of consecutive
+  // partitions whose rows and index fit half of what the ledger has left,
+  // built into `pass` (an ordinary join) for that pass. Probe rows take part
+  // only in the pass of their key's partition (JoinView.part_*).
+  bool grace = false;
+  struct HostPart {
+    int64_t rows = 0;
+    std::vector<char> key;
+    std::vector<std::vector<char>> pay;
+    std::vector<std::vector<uint8_t>> ok;  // per payload column and row: 1 = not NULL
+  };
+  std::vector<HostPart> parts;
+  std::vector<std::pair<int, int>> passes;  // partition ranges [lo, hi)
+  wg_join* pass = nullptr;
+  int pass_built = -1;
+  // on a pass join: the partitions it covers (part_shift 0 = all)
+  int32_t pass_shift = 0, pass_lo = 0, pass_hi = 0;
+  ~wg_join() { delete pass; }
 };
 
 namespace wg {
@@ -389,6 +411,11 @@ static wg_status append_col(Ctx* ctx, BuildCol& c, const wg_column& src, int64_t
   return WG_OK;
 }
 
+static bool grace_allowed(const wg_join* j);
+static wg_status grace_convert(wg_join* j);
+static wg_status grace_append(wg_join* j, const wg_batch_desc* b);
+static wg_status grace_plan(wg_join* j);
+
 static wg_status join_append(wg_join* j, const wg_batch_desc* b) {
   Ctx* ctx = j->ctx;
   if (j->finished) return fail(WG_E_STATE, "join build already finished");
@@ -413,19 +440,239 @@ static wg_status join_append(wg_join* j, const wg_batch_desc* b) {
     return fail(WG_E_INVALID, "build key type changed between batches");
   }
   const int64_t n = b->len;
+  for (size_t i = 0; i < j->pay.size(); ++i)
+    if (b->cols[j->payload_cols[i]].type_id != j->pay[i].type_id)
+      return fail(WG_E_INVALID, "payload type changed between batches");
+  if (j->grace) return grace_append(j, b);
   int64_t hint = std::max<int64_t>(j->hint, j->rows + n);
-  WG_TRY(grow_col(ctx, j->key, hint, j->rows));
-  WG_TRY(append_col(ctx, j->key, kc, n, j->rows));
-  for (size_t i = 0; i < j->pay.size(); ++i) {
+  wg_status st = grow_col(ctx, j->key, hint, j->rows);
+  if (st == WG_OK) st = append_col(ctx, j->key, kc, n, j->rows);
+  for (size_t i = 0; i < j->pay.size() && st == WG_OK; ++i) {
     const wg_column& c = b->cols[j->payload_cols[i]];
-    if (c.type_id != j->pay[i].type_id) return fail(WG_E_INVALID, "payload type changed between batches");
-    WG_TRY(grow_col(ctx, j->pay[i], hint, j->rows));
-    WG_TRY(append_col(ctx, j->pay[i], c, n, j->rows));
+    st = grow_col(ctx, j->pay[i], hint, j->rows);
+    if (st == WG_OK) st = append_col(ctx, j->pay[i], c, n, j->rows);
   }
+  if (st == WG_E_NOMEM && grace_allowed(j)) {  // the ledger refused: partition the build into host memory
+    WG_TRY(grace_convert(j));
+    return grace_append(j, b);
+  }
+  WG_TRY(st);
   j->rows += n;
   WG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
   return WG_OK;
 }
+
+// ---- partitioned (grace) build ---------------------------------------------
+constexpr int kJoinPartBits = 6;  // 64 partitions, as the reference's partitioned build
+constexpr int kJoinPartShift = 64 - kJoinPartBits;
+
+static bool grace_allowed(const wg_join* j) {
+  const char* v = std::getenv("WG_JOIN_GRACE");
+  return j->ctx->ledger.budget() > 0 && (!v || std::atoi(v) != 0);
+}
+
+// `bytes` of host or device memory into a host vector.
+static wg_status to_host(Ctx* ctx, const void* src, int64_t bytes, std::vector<char>& out) {
+  out.resize((size_t)std::max<int64_t>(bytes, 0));
+  if (bytes <= 0) return WG_OK;
+  WG_CUDA_TRY(cudaMemcpyAsync(out.data(), src, (size_t)bytes, cudaMemcpyDefault, ctx->stream));
+  WG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return WG_OK;
+}
+
+static inline bool bit_at(const std::vector<char>& words, int64_t i) {
+  return words.empty() || ((((const uint64_t*)words.data())[i >> 6] >> (i & 63)) & 1ULL);
+}
+
+// n rows (host copies of the key, its validity words, each payload column and
+// its validity words; empty validity = no NULLs) appended to their partitions.
+static void grace_partition(wg_join* j, const std::vector<char>& key, const std::vector<char>& key_valid,
+                            const std::vector<std::vector<char>>& pay, const std::vector<std::vector<char>>& pay_valid,
+                            int64_t n) {
+  const int np = 1 << kJoinPartBits;
+  if ((int)j->parts.size() != np) j->parts.assign((size_t)np, wg_join::HostPart{});
+  const int kes = (int)j->key.es;
+  std::vector<uint8_t> part((size_t)n);
+  std::vector<int64_t> cnt((size_t)np, 0);
+  for (int64_t i = 0; i < n; ++i) {
+    if (!bit_at(key_valid, i)) { part[(size_t)i] = 0xFF; continue; }  // a NULL key matches nothing
+    const long long k = kes == 4 ? (long long)((const int32_t*)key.data())[i] : ((const long long*)key.data())[i];
+    part[(size_t)i] = (uint8_t)wgd::join_partition(k, kJoinPartShift);
+    ++cnt[part[(size_t)i]];
+  }
+  const size_t npay = j->pay.size();
+  std::vector<int64_t> at((size_t)np);
+  for (int p = 0; p < np; ++p) {
+    wg_join::HostPart& hp = j->parts[(size_t)p];
+    at[(size_t)p] = hp.rows;
+    hp.rows += cnt[(size_t)p];
+    hp.key.resize((size_t)(hp.rows * kes));
+    hp.pay.resize(npay);
+    hp.ok.resize(npay);
+    for (size_t c = 0; c < npay; ++c) {
+      hp.pay[c].resize((size_t)(hp.rows * j->pay[c].es));
+      hp.ok[c].resize((size_t)hp.rows, 1);
+    }
+  }
+  for (int64_t i = 0; i < n; ++i) {
+    const uint8_t p = part[(size_t)i];
+    if (p == 0xFF) continue;
+    wg_join::HostPart& hp = j->parts[p];
+    const int64_t r = at[p]++;
+    std::memcpy(hp.key.data() + r * kes, key.data() + i * kes, (size_t)kes);
+    for (size_t c = 0; c < npay; ++c) {
+      const int64_t es = j->pay[c].es;
+      std::memcpy(hp.pay[c].data() + r * es, pay[c].data() + i * es, (size_t)es);
+      hp.ok[c][(size_t)r] = bit_at(pay_valid[c], i) ? 1 : 0;
+    }
+  }
+}
+
+// The build rows already on the device moved to host partitions; the device
+// columns and index freed.
+static wg_status grace_convert(wg_join* j) {
+  Ctx* ctx = j->ctx;
+  WG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  const int64_t n = j->rows;
+  std::vector<char> key, key_valid;
+  std::vector<std::vector<char>> pay(j->pay.size()), pay_valid(j->pay.size());
+  WG_TRY(to_host(ctx, j->key.data.get(), n * j->key.es, key));
+  if (j->key.has_valid) WG_TRY(to_host(ctx, j->key.valid.get(), (n + 63) / 64 * 8, key_valid));
+  for (size_t c = 0; c < j->pay.size(); ++c) {
+    WG_TRY(to_host(ctx, j->pay[c].data.get(), n * j->pay[c].es, pay[c]));
+    if (j->pay[c].has_valid) WG_TRY(to_host(ctx, j->pay[c].valid.get(), (n + 63) / 64 * 8, pay_valid[c]));
+  }
+  j->grace = true;
+  j->parts.clear();
+  grace_partition(j, key, key_valid, pay, pay_valid, n);
+  auto drop = [](BuildCol& c) { c.data.reset(); c.valid.reset(); c.cap_rows = 0; };
+  drop(j->key);
+  for (BuildCol& c : j->pay) drop(c);
+  j->slots.reset(); j->next.reset(); j->dslots.reset(); j->dpay.reset();
+  j->counts.reset(); j->offs.reset(); j->outp.reset(); j->outb.reset();
+  return WG_OK;
+}
+
+// A batch appended to the host partitions.
+static wg_status grace_append(wg_join* j, const wg_batch_desc* b) {
+  Ctx* ctx = j->ctx;
+  const int64_t n = b->len;
+  const wg_column& kc = b->cols[j->build_key_col];
+  std::vector<char> key, key_valid;
+  std::vector<std::vector<char>> pay(j->pay.size()), pay_valid(j->pay.size());
+  WG_TRY(to_host(ctx, kc.data, n * j->key.es, key));
+  if (kc.valid_words) WG_TRY(to_host(ctx, kc.valid_words, (n + 63) / 64 * 8, key_valid));
+  for (size_t c = 0; c < j->pay.size(); ++c) {
+    const wg_column& pc = b->cols[j->payload_cols[c]];
+    WG_TRY(to_host(ctx, pc.data, n * j->pay[c].es, pay[c]));
+    if (pc.valid_words) WG_TRY(to_host(ctx, pc.valid_words, (n + 63) / 64 * 8, pay_valid[c]));
+  }
+  grace_partition(j, key, key_valid, pay, pay_valid, n);
+  j->rows += n;
+  return WG_OK;
+}
+
+// Passes: consecutive partitions grouped while their rows, stored and indexed
+// on the device, fit half of what the ledger has left.
+static wg_status grace_plan(wg_join* j) {
+  Ctx* ctx = j->ctx;
+  int64_t row_bytes = j->key.es + 4 /* chain */ + 64 /* index and direct tables, at most 2 x 16-byte slots */;
+  for (const BuildCol& c : j->pay) row_bytes += c.es + 1;
+  const int64_t left = ctx->ledger.budget() - ctx->ledger.used();
+  const int64_t room = std::max<int64_t>(left / 2, 1 << 20);
+  j->passes.clear();
+  const int np = (int)j->parts.size();
+  int lo = 0;
+  int64_t bytes = 0;
+  for (int p = 0; p < np; ++p) {
+    const int64_t b = j->parts[(size_t)p].rows * row_bytes;
+    if (b > room) return fail(WG_E_NOMEM, "a join build partition does not fit the HBM budget");
+    if (bytes + b > room && p > lo) {
+      j->passes.push_back({lo, p});
+      lo = p;
+      bytes = 0;
+    }
+    bytes += b;
+  }
+  j->passes.push_back({lo, np});
+  j->pass_built = -1;
+  j->distinct = -1;  // not counted across partitions
+  return WG_OK;
+}
+
+// The join for pass g: an ordinary join over that pass's partitions, whose
+// probe view admits only rows of those partitions.
+wg_status join_grace_pass(wg_join* j, int g, wg_join** out) {
+  Ctx* ctx = j->ctx;
+  if (j->pass_built == g && j->pass) { *out = j->pass; return WG_OK; }
+  delete j->pass;
+  j->pass = nullptr;
+  j->pass_built = -1;
+  const int lo = j->passes[(size_t)g].first, hi = j->passes[(size_t)g].second;
+  int64_t n = 0;
+  for (int p = lo; p < hi; ++p) n += j->parts[(size_t)p].rows;
+  const int npay = (int)j->pay.size();
+  std::vector<int32_t> pcols((size_t)npay);
+  for (int c = 0; c < npay; ++c) pcols[(size_t)c] = c + 1;
+  wg_join* pj = nullptr;
+  // every context is created as a wg_ctx (ctx_make)
+  WG_TRY(wg_join_create(static_cast<wg_ctx*>(ctx), j->jtype, 0, j->probe_key_col, npay, pcols.data(),
+                        std::max<int64_t>(n, 1), &pj));
+  j->pass = pj;
+  pj->pass_shift = kJoinPartShift;
+  pj->pass_lo = lo;
+  pj->pass_hi = hi;
+  // the pass's rows as one host batch (key, then the payload columns with their validity words)
+  std::vector<char> key((size_t)(n * j->key.es));
+  std::vector<std::vector<char>> pay((size_t)npay);
+  std::vector<std::vector<uint64_t>> valid((size_t)npay);
+  std::vector<bool> any_null((size_t)npay, false);
+  for (int c = 0; c < npay; ++c) {
+    pay[(size_t)c].resize((size_t)(n * j->pay[(size_t)c].es));
+    valid[(size_t)c].assign((size_t)((n + 63) / 64 + 1), ~0ULL);
+  }
+  int64_t r0 = 0;
+  for (int p = lo; p < hi; ++p) {
+    const wg_join::HostPart& hp = j->parts[(size_t)p];
+    if (hp.rows == 0) continue;
+    std::memcpy(key.data() + r0 * j->key.es, hp.key.data(), (size_t)(hp.rows * j->key.es));
+    for (int c = 0; c < npay; ++c) {
+      const int64_t es = j->pay[(size_t)c].es;
+      std::memcpy(pay[(size_t)c].data() + r0 * es, hp.pay[(size_t)c].data(), (size_t)(hp.rows * es));
+      for (int64_t i = 0; i < hp.rows; ++i)
+        if (!hp.ok[(size_t)c][(size_t)i]) {
+          const int64_t r = r0 + i;
+          valid[(size_t)c][(size_t)(r >> 6)] &= ~(1ULL << (r & 63));
+          any_null[(size_t)c] = true;
+        }
+    }
+    r0 += hp.rows;
+  }
+  std::vector<wg_column> cols((size_t)npay + 1);
+  cols[0] = wg_column{j->key.type_id, 0, key.data(), nullptr, n};
+  for (int c = 0; c < npay; ++c)
+    cols[(size_t)c + 1] = wg_column{j->pay[(size_t)c].type_id, j->pay[(size_t)c].scale, pay[(size_t)c].data(),
+                                    any_null[(size_t)c] ? valid[(size_t)c].data() : nullptr, n};
+  wg_batch_desc d{npay + 1, 0, cols.data(), n, nullptr, 0};
+  if (n > 0) WG_TRY(join_append(pj, &d));
+  else {  // an empty pass still needs the schema
+    pj->key.type_id = j->key.type_id; pj->key.es = j->key.es;
+    pj->pay.resize((size_t)npay);
+    for (int c = 0; c < npay; ++c) {
+      pj->pay[(size_t)c].type_id = j->pay[(size_t)c].type_id;
+      pj->pay[(size_t)c].scale = j->pay[(size_t)c].scale;
+      pj->pay[(size_t)c].es = j->pay[(size_t)c].es;
+    }
+    pj->flavor = j->flavor;
+    pj->schema_set = true;
+  }
+  WG_TRY(wg_join_build_finish(pj));
+  j->pass_built = g;
+  *out = pj;
+  return WG_OK;
+}
+bool join_is_grace(wg_join* j) { return j->grace; }
+int join_grace_passes(wg_join* j) { return (int)j->passes.size(); }
 
 // Device view for the fused pipeline and the probe kernels.
 static wg_status build_hash(wg_join* j);
@@ -439,7 +686,9 @@ static wg_status join_view_fields(wg_join* j, wgd::JoinView* v) {
   v->next = j->next.as<int32_t>();
   v->n_pay = (int32_t)j->pay.size();
   v->jtype = j->jtype;
-  v->_pad = 0;
+  v->part_shift = j->pass_shift;
+  v->part_lo = j->pass_lo;
+  v->part_hi = j->pass_hi;
   v->direct = 0;
   v->sentinel = 0;
   v->dense = 0;
@@ -649,11 +898,24 @@ wg_status wg_join_build_append_device(wg_join* j, const wg_batch_desc* b) {
   return join_append(j, b);
 }
 
+static wg_status build_finish_device(wg_join* j);
+
 wg_status wg_join_build_finish(wg_join* j) {
   if (!j) return fail(WG_E_INVALID, "join is NULL");
   if (j->finished) return WG_OK;
+  WG_TRY(ensure_device(j->ctx));
+  if (!j->grace) {
+    const wg_status st = build_finish_device(j);
+    if (st != WG_E_NOMEM || !grace_allowed(j) || !j->schema_set) return st;
+    WG_TRY(grace_convert(j));  // the index did not fit: partition the build into host memory
+  }
+  WG_TRY(grace_plan(j));
+  j->finished = true;
+  return WG_OK;
+}
+
+static wg_status build_finish_device(wg_join* j) {
   Ctx* ctx = j->ctx;
-  WG_TRY(ensure_device(ctx));
   if (!j->schema_set) { j->flavor = 0; j->key.type_id = WG_TYPE_INT32; j->key.es = 4; }
   uint64_t cap = 1024;
   while (cap < (uint64_t)std::max<int64_t>(2 * j->rows, 1)) cap <<= 1;
@@ -767,6 +1029,7 @@ wg_status wg_join_probe(wg_join* j, const wg_batch_desc* probe, uint32_t* out_pr
   Ctx* ctx = j->ctx;
   WG_TRY(ensure_device(ctx));
   if (!j->finished) return fail(WG_E_STATE, "join build not finished");
+  if (j->grace) return fail(WG_E_UNSUPPORTED, "a partitioned build is probed through the fused pipeline");
   if (j->probe_key_col < 0 || j->probe_key_col >= probe->ncols) return fail(WG_E_INVALID, "probe key column out of range");
   const wg_column& kc = probe->cols[j->probe_key_col];
   if (class_of(kc.type_id) != WG_CLS_I32 && class_of(kc.type_id) != WG_CLS_I64)
@@ -826,6 +1089,7 @@ wg_status wg_join_gather(wg_join* j, int32_t payload_idx, const int64_t* build_r
   if (payload_idx < 0 || payload_idx >= (int32_t)j->pay.size()) return fail(WG_E_INVALID, "payload index out of range");
   Ctx* ctx = j->ctx;
   WG_TRY(ensure_device(ctx));
+  if (j->grace) return fail(WG_E_UNSUPPORTED, "a partitioned build is probed through the fused pipeline");
   if (n == 0) return WG_OK;
   for (int64_t i = 0; i < n; ++i)
     if (build_rows[i] < -1 || build_rows[i] >= j->rows) return fail(WG_E_INVALID, "build row out of range");
@@ -857,6 +1121,12 @@ wg_status wg_join_reset(wg_join* j) {
   j->distinct = 0;
   j->unique = true;
   j->max_fanout = 1;
+  j->grace = false;
+  j->parts.clear();
+  j->passes.clear();
+  delete j->pass;
+  j->pass = nullptr;
+  j->pass_built = -1;
   return WG_OK;
 }
 

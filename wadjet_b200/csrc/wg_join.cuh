@@ -47,10 +47,29 @@ struct JoinView {
   // matched probe row once, no build columns), WG_JOIN_ANTI (a probe row with
   // no match or a NULL key, no build columns)
   int32_t jtype;
-  int32_t _pad;
+  // A pass over a partitioned build (one group of its key-hash partitions):
+  // only probe rows whose key falls in partitions [part_lo, part_hi) take part
+  // (partition = (key * fib) >> part_shift; NULL keys belong to the pass that
+  // starts at partition 0). part_shift = 0: no partitioning.
+  int32_t part_shift;
+  int32_t part_lo, part_hi;
   long long base;
   DCol pay[WG_MAX_PAYLOAD];
 };
+
+// Key-hash partition of a join key (the partitioned build's, host side:
+// join_partition_of in wg_join.cu).
+__host__ __device__ __forceinline__ uint32_t join_partition(long long key, int shift) {
+  return (uint32_t)(((unsigned long long)key * 0x9E3779B97F4A7C15ULL) >> shift);
+}
+
+// Whether a probe row takes part in this pass of a partitioned build.
+__device__ __forceinline__ bool join_pass_mine(const JoinView& j, bool null, long long key) {
+  if (j.part_shift == 0) return true;
+  if (null) return j.part_lo == 0;
+  const uint32_t p = join_partition(key, j.part_shift);
+  return p >= (uint32_t)j.part_lo && p < (uint32_t)j.part_hi;
+}
 
 // Direct-payload lookup: the payload's raw 32 bits of `key`, or false.
 __device__ __forceinline__ bool join_direct(const JoinView& j, int64_t key, int32_t& out, int32_t* err) {
