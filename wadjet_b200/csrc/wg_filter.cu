@@ -58,7 +58,7 @@ namespace {
 using namespace wgd;
 
 constexpr int kBlock = 256;
-constexpr int kRows = 4;
+constexpr int kRows = 8;
 constexpr unsigned long long kFlagAgg = 1ULL << 62;
 constexpr unsigned long long kFlagInc = 2ULL << 62;
 constexpr unsigned long long kValMask = (1ULL << 62) - 1;
@@ -108,6 +108,7 @@ __global__ void __launch_bounds__(kBlock) filter_compact_kernel(const FilterArgs
   __shared__ int s_warp[kRows][kBlock / 32];
   __shared__ int s_total;
   __shared__ long long s_prefix;
+  __shared__ uint32_t s_out[kTile];
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0) s_tile = atomicAdd(a.tile_counter, 1);
@@ -150,51 +151,72 @@ __global__ void __launch_bounds__(kBlock) filter_compact_kernel(const FilterArgs
     if (lane == 31) s_warp[r][warp] = incl;
   }
   __syncthreads();
-  if (tid == 0) {
+  // Decoupled look-back by warp 0: each step reads the status words of the 32
+  // closest unread predecessors at once, waits (bounded) until all of them
+  // have published, and adds their aggregates up to the closest inclusive one.
+  if (warp == 0) {
     int run = 0;
-    for (int r = 0; r < kRows; ++r)
-      for (int w = 0; w < kBlock / 32; ++w) { int t = s_warp[r][w]; s_warp[r][w] = run; run += t; }
-    s_total = run;
-    // decoupled look-back
+    if (lane == 0) {
+      for (int r = 0; r < kRows; ++r)
+        for (int w = 0; w < kBlock / 32; ++w) { int t = s_warp[r][w]; s_warp[r][w] = run; run += t; }
+      s_total = run;
+      atomicExch(a.status + tile, (tile == 0 ? kFlagInc : kFlagAgg) | (unsigned long long)run);
+    }
+    run = __shfl_sync(WG_FULL_MASK, run, 0);
     long long prefix = 0;
-    if (tile == 0) {
-      atomicExch(a.status, kFlagInc | (unsigned long long)run);
-    } else {
-      atomicExch(a.status + tile, kFlagAgg | (unsigned long long)run);
-      int64_t pred = tile - 1;
+    if (tile > 0) {
+      int64_t tail = tile - 1;
       long long spins = 0;
-      while (pred >= 0) {
-        // the tile publishes its (partial) prefix on expiry, so no successor waits
-        // forever and every position it writes stays below the true one
-        if (spins >= a.spin_limit) { set_error(a.err, WG_DERR_TIMEOUT); break; }
-        unsigned long long s = *((volatile unsigned long long*)(a.status + pred));
-        unsigned long long flag = s & ~kValMask;
-        if (flag == 0) {
+      bool expired = false;
+      for (;;) {
+        const int64_t idx = tail - lane;
+        unsigned long long st = idx >= 0 ? 0ULL : kFlagInc;  // before tile 0: an inclusive 0
+        // the tile publishes its (partial) prefix on expiry, so no successor
+        // waits forever and every position it writes stays below the true one
+        for (;;) {
+          if (spins >= a.spin_limit) { expired = true; break; }
+          if ((st & ~kValMask) == 0) st = *((volatile unsigned long long*)(a.status + idx));
+          if (!__any_sync(WG_FULL_MASK, (st & ~kValMask) == 0)) break;
           ++spins;
           __nanosleep(64);
-          continue;
         }
-        prefix += (long long)(s & kValMask);
-        if (flag == kFlagInc) break;
-        --pred;
+        if (expired) {
+          if (lane == 0) set_error(a.err, WG_DERR_TIMEOUT);
+          break;
+        }
+        const unsigned inc = __ballot_sync(WG_FULL_MASK, (st & ~kValMask) == kFlagInc);
+        const int stop = inc ? __ffs(inc) - 1 : 31;  // lanes 0..stop count
+        long long v = lane <= stop ? (long long)(st & kValMask) : 0LL;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(WG_FULL_MASK, v, o);
+        prefix += v;
+        if (inc) break;
+        tail -= 32;
       }
-      atomicExch(a.status + tile, kFlagInc | (unsigned long long)(prefix + run));
+      if (lane == 0) atomicExch(a.status + tile, kFlagInc | (unsigned long long)(prefix + run));
     }
-    s_prefix = prefix;
-    if (tile == a.num_tiles - 1) *a.out_n = prefix + run;
+    if (lane == 0) {
+      s_prefix = prefix;
+      if (tile == a.num_tiles - 1) *a.out_n = prefix + run;
+    }
   }
   __syncthreads();
+  // the tile's survivors gathered in shared memory in order, then written out
+  // contiguously (coalesced stores instead of each thread's scattered ones)
   const long long prefix = s_prefix;
 #pragma unroll
   for (int r = 0; r < kRows; ++r) {
     unsigned b = bits[r];
     if (!b) continue;
-    long long pos = prefix + s_warp[r][warp] + excl[r];
+    int pos = s_warp[r][warp] + excl[r];
     const int64_t i0 = tile_base + ((int64_t)r * kBlock + tid) * V;
 #pragma unroll
     for (int k = 0; k < V; ++k)
-      if (b & (1u << k)) a.out[pos++] = a.sel ? __ldg(a.sel + i0 + k) : (uint32_t)(i0 + k);
+      if (b & (1u << k)) s_out[pos++] = a.sel ? __ldg(a.sel + i0 + k) : (uint32_t)(i0 + k);
   }
+  __syncthreads();
+  const int total = s_total;
+  for (int i = tid; i < total; i += kBlock) a.out[prefix + i] = s_out[i];
 }
 
 template <int CLS>

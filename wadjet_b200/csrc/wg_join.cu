@@ -576,7 +576,10 @@ static wg_status grace_append(wg_join* j, const wg_batch_desc* b) {
 // on the device, fit half of what the ledger has left.
 static wg_status grace_plan(wg_join* j) {
   Ctx* ctx = j->ctx;
-  int64_t row_bytes = j->key.es + 4 /* chain */ + 64 /* index and direct tables, at most 2 x 16-byte slots */;
+  // per build row: the key, its chain link, the hash index (at most 4 slots of
+  // 16 bytes per row: capacity is the power of two at or above twice the rows)
+  // and the direct table (at most 4 slots of 8 bytes), and each payload column
+  int64_t row_bytes = j->key.es + 4 + 64 + 32;
   for (const BuildCol& c : j->pay) row_bytes += c.es + 1;
   const int64_t left = ctx->ledger.budget() - ctx->ledger.used();
   const int64_t room = std::max<int64_t>(left / 2, 1 << 20);
