@@ -356,9 +356,16 @@ WG_API wg_status wg_join_create(wg_ctx* ctx, int32_t join_type, int32_t build_ke
 WG_API wg_status wg_join_build_append(wg_join* j, const wg_batch_desc* build);
 WG_API wg_status wg_join_build_append_device(wg_join* j, const wg_batch_desc* build);
 /* Build the device hash index over everything appended (end of
- * HashJoin.Build, join.go:771). Null keys never join. */
+ * HashJoin.Build, join.go:771). Null keys never join.
+ * When the context's HBM budget refuses the build's columns (at append) or its
+ * index (here), the build becomes partitioned (HashJoin.buildPartitioned,
+ * join_partition_arrival.go:48): its rows move to host memory in 64 key-hash
+ * partitions, and the pipeline entry points probe it in passes over groups of
+ * partitions that fit; wg_join_probe and wg_join_gather then return
+ * WG_E_UNSUPPORTED. */
 WG_API wg_status wg_join_build_finish(wg_join* j);
-/* Number of build rows stored and number of distinct keys indexed. */
+/* Number of build rows stored and number of distinct keys indexed (-1 for a
+ * partitioned build: keys are not counted across partitions). */
 WG_API wg_status wg_join_build_stats(wg_join* j, int64_t* build_rows, int64_t* distinct_keys);
 /* HashJoinProbe.Execute → inlineIntProbe (join.go:2306,2670), bounded output
  * (BoundedOutputOperator, operators.go:86): emits at most `cap` output pairs

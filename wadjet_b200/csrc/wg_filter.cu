@@ -99,7 +99,7 @@ template <> struct ClsT<WG_CLS_I64> { using T = long long; };
 template <> struct ClsT<WG_CLS_F32> { using T = float; };
 template <> struct ClsT<WG_CLS_F64> { using T = double; };
 
-template <int CLS, bool VEC>
+template <int CLS, bool VEC, int OP>
 __global__ void __launch_bounds__(kBlock) filter_compact_kernel(const FilterArgs a) {
   using T = typename ClsT<CLS>::T;
   constexpr int V = VEC ? (int)(16 / sizeof(T)) : 1;
@@ -128,14 +128,14 @@ __global__ void __launch_bounds__(kBlock) filter_compact_kernel(const FilterArgs
       const T* e = reinterpret_cast<const T*>(&v);
 #pragma unroll
       for (int k = 0; k < V; ++k)
-        if (cmp_op<T>(e[k], cval, a.p.op) && !is_null(a.col, i0 + k)) b |= 1u << k;
+        if (cmp_op<T>(e[k], cval, OP) && !is_null(a.col, i0 + k)) b |= 1u << k;
     } else {
 #pragma unroll
       for (int k = 0; k < V; ++k) {
         const int64_t it = i0 + k;
         if (it < a.n) {
           const int64_t row = a.sel ? (int64_t)__ldg(a.sel + it) : it;
-          if (!is_null(a.col, row) && cmp_op<T>(__ldg((const T*)a.col.data + row), cval, a.p.op)) b |= 1u << k;
+          if (!is_null(a.col, row) && cmp_op<T>(__ldg((const T*)a.col.data + row), cval, OP)) b |= 1u << k;
         }
       }
     }
@@ -219,10 +219,24 @@ __global__ void __launch_bounds__(kBlock) filter_compact_kernel(const FilterArgs
   for (int i = tid; i < total; i += kBlock) a.out[prefix + i] = s_out[i];
 }
 
+// One kernel per column class, vector width and comparison (the operator
+// compiled in rather than switched on per element).
+template <int CLS, int OP>
+void launch_op(bool vec, const FilterArgs& a, dim3 grid, cudaStream_t s) {
+  if (vec) filter_compact_kernel<CLS, true, OP><<<grid, kBlock, 0, s>>>(a);
+  else filter_compact_kernel<CLS, false, OP><<<grid, kBlock, 0, s>>>(a);
+}
+
 template <int CLS>
 void launch_cls(bool vec, const FilterArgs& a, dim3 grid, cudaStream_t s) {
-  if (vec) filter_compact_kernel<CLS, true><<<grid, kBlock, 0, s>>>(a);
-  else filter_compact_kernel<CLS, false><<<grid, kBlock, 0, s>>>(a);
+  switch (a.p.op) {
+    case 0: launch_op<CLS, 0>(vec, a, grid, s); break;
+    case 1: launch_op<CLS, 1>(vec, a, grid, s); break;
+    case 2: launch_op<CLS, 2>(vec, a, grid, s); break;
+    case 3: launch_op<CLS, 3>(vec, a, grid, s); break;
+    case 4: launch_op<CLS, 4>(vec, a, grid, s); break;
+    default: launch_op<CLS, 5>(vec, a, grid, s); break;
+  }
 }
 
 }  // namespace
