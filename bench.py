@@ -385,7 +385,10 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                          "frac": (achieved / peak) if achieved else None,
                          "traffic": NCU_TRAFFIC_BYTES_PER_FACT_ROW * n,
                          "traffic_source": "ncu capture at 2^24 fact rows scaled to this launch's rows",
-                         "kernel": "pipeline_vec_kernel (compiled star-join shape)", "kernel_ms": k_ms, "algorithmic_bytes": alg_bytes,
+                         "kernel": ("starjoin_dense_kernel (compiled star-join shape, payload-only dense join index, "
+                                    "dense shared-memory groups)" if os.environ.get("WG_STAR_LEAN", "1") != "0"
+                                    else "pipeline_vec_kernel (compiled star-join shape)"),
+                         "kernel_ms": k_ms, "algorithmic_bytes": alg_bytes,
                          "peak_kind": peak_kind},
             "cpu_baseline": cpu,
             "e2e": e2e,

@@ -103,19 +103,28 @@ def test_compiled_shape_query_with_nulls_runs_generic(ctx):
 
 
 KNOB_NAMES = ("WG_TILE", "WG_JOIN_DIRECT", "WG_AGG_SMEM", "WG_SPECIALIZE", "WG_JOIN_DENSE", "WG_SMEM_REPLICAS",
-              "WG_GROUP_DENSE", "WG_VEC", "WG_SMEM_COMBINE", "WG_STAGE", "WG_JOIN_FULL_DENSE")
+              "WG_GROUP_DENSE", "WG_VEC", "WG_SMEM_COMBINE", "WG_STAGE", "WG_JOIN_FULL_DENSE", "WG_STAR_LEAN")
 KNOBS = [  # the defaults first, then every GPU lever off, on and mixed
-    ("0", "1", "1", "1", "1", "4", "1", "2", "0", "0", "1"), ("0", "0", "0", "0", "0", "1", "0", "0", "0", "0", "0"),
-    ("1", "1", "1", "1", "1", "4", "1", "2", "0", "1", "1"), ("1", "0", "1", "1", "1", "1", "0", "2", "1", "1", "1"),
-    ("0", "1", "0", "1", "1", "4", "1", "4", "0", "1", "0"), ("1", "1", "0", "1", "0", "4", "1", "0", "0", "1", "1"),
-    ("0", "1", "1", "0", "1", "2", "1", "2", "1", "1", "1"), ("0", "1", "1", "1", "0", "1", "0", "0", "1", "1", "1"),
-    ("0", "1", "1", "1", "1", "8", "0", "4", "0", "1", "0"), ("0", "1", "1", "1", "1", "2", "1", "0", "1", "1", "1"),
-    ("0", "1", "1", "1", "1", "4", "1", "2", "0", "1", "1"), ("0", "1", "1", "1", "1", "1", "0", "2", "1", "1", "0")]
+    ("0", "1", "1", "1", "1", "4", "1", "2", "0", "0", "1", "1"),
+    ("0", "0", "0", "0", "0", "1", "0", "0", "0", "0", "0", "0"),
+    ("1", "1", "1", "1", "1", "4", "1", "2", "0", "1", "1", "1"),
+    ("1", "0", "1", "1", "1", "1", "0", "2", "1", "1", "1", "1"),
+    ("0", "1", "0", "1", "1", "4", "1", "4", "0", "1", "0", "1"),
+    ("1", "1", "0", "1", "0", "4", "1", "0", "0", "1", "1", "1"),
+    ("0", "1", "1", "0", "1", "2", "1", "2", "1", "1", "1", "1"),
+    ("0", "1", "1", "1", "0", "1", "0", "0", "1", "1", "1", "1"),
+    ("0", "1", "1", "1", "1", "8", "0", "4", "0", "1", "0", "1"),
+    ("0", "1", "1", "1", "1", "2", "1", "0", "1", "1", "1", "1"),
+    ("0", "1", "1", "1", "1", "4", "1", "2", "0", "1", "1", "0"),  # the generic vector kernel for the star shape
+    ("0", "1", "1", "1", "1", "1", "0", "2", "1", "1", "0", "1"),
+    ("0", "1", "1", "1", "1", "8", "1", "2", "0", "0", "1", "1"),  # the lean kernel with 8 float-SUM copies
+    ("0", "1", "1", "1", "1", "2", "1", "2", "0", "0", "1", "1"),  # ... and with 2
+    ("0", "1", "1", "1", "1", "1", "1", "2", "0", "0", "1", "1")]  # ... and with 1
 
 
 @pytest.mark.parametrize("knobs", KNOBS,
                          ids=lambda k: "tile%s-direct%s-smem%s-spec%s-jdense%s-rep%s-gdense%s-vec%s-comb%s-stage%s"
-                                       "-full%s" % k)
+                                       "-full%s-lean%s" % k)
 @pytest.mark.parametrize("host_input", [False, True])
 def test_starjoin_workload_matches_oracle(ctx, host_input, knobs, monkeypatch):
     """Star join + aggregate, 2^22 - 37 fact rows against the full 2^22-row dimension, with
