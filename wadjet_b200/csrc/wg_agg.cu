@@ -17,6 +17,7 @@
 #include "wg_hc.cuh"
 
 #include <algorithm>
+#include <type_traits>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -2572,30 +2573,48 @@ __global__ void batched_count_kernel(const ResetDesc* rd, int n, long long* out)
 }
 
 // One work item (a window of one query's rows) on shape Sh.
+// The rows of one work item: 2 consecutive rows per lane with vector loads
+// (every row's loads in flight before its updates) when the query has a
+// compiled shape and vector-aligned columns (P.vec_rows, set by the host), one
+// row per lane otherwise.
+template <int NA, bool SMEM, class Sh>
+__device__ __forceinline__ void batched_rows(const Plan& P, const Sh& sh, const BatchItem& w, unsigned long long* sm,
+                                             int* s_groups, int s_limit, Credit& cr) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if constexpr (!std::is_same<Sh, DynShape>::value) {
+    if (P.vec_rows) {
+      constexpr int U = 2;
+      const int64_t end = w.row0 + w.rows;
+      for (int64_t base = w.row0 + (int64_t)warp * 32 * U; base < end; base += (int64_t)nw * 32 * U) {
+        const int64_t r0 = base + (int64_t)lane * U;
+        SrcRow rw[U];
+        load_rows<U>(P, sh, r0, rw, end);
+        process_loaded_vec<NA, SMEM, U>(P, sh, r0, rw, sm, s_groups, s_limit, cr, end);
+      }
+      return;
+    }
+  }
+  for (int base = warp * 32; base < w.rows; base += nw * 32) {
+    const int i = base + lane;
+    SrcGlobal src{w.row0 + (i < w.rows ? i : 0)};
+    process_rows<NA, SMEM>(P, sh, src, i < w.rows, sm, s_groups, s_limit, cr);
+  }
+}
+
 template <int NA, class Sh>
 __device__ __forceinline__ void batched_item(const Plan& P, const BatchItem& w, unsigned long long* sm,
                                              int* s_groups) {
   const Sh sh{P};
   Credit cr;  // reservations in this query's table, handed back before the next item
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int S = P.smem_slots;
   if (Sh::smem_ok && S > 0) {
     smem_table_init(P, sm, S, s_groups);
     __syncthreads();
-    const int s_limit = (S * 7) / 8;
-    for (int base = warp * 32; base < w.rows; base += nw * 32) {
-      const int i = base + lane;
-      SrcGlobal src{w.row0 + (i < w.rows ? i : 0)};
-      process_rows<NA, Sh::smem_ok>(P, sh, src, i < w.rows, sm, s_groups, s_limit, cr);
-    }
+    batched_rows<NA, Sh::smem_ok>(P, sh, w, sm, s_groups, (S * 7) / 8, cr);
     __syncthreads();
     smem_table_flush<NA>(P, sm, S, cr);
   } else {
-    for (int base = warp * 32; base < w.rows; base += nw * 32) {
-      const int i = base + lane;
-      SrcGlobal src{w.row0 + (i < w.rows ? i : 0)};
-      process_rows<NA, false>(P, sh, src, i < w.rows, sm, s_groups, 0, cr);
-    }
+    batched_rows<NA, false>(P, sh, w, sm, s_groups, 0, cr);
   }
   cr.release(P.T);
 }
@@ -2696,6 +2715,12 @@ static wg_status batched_plan(wg_batched* b) {
     }
     P.shape = pick_shape(P);
     if (P.shape != wgd::SHAPE_BATCH_I64 && P.shape != wgd::SHAPE_BATCH_F64) P.shape = wgd::SHAPE_GENERIC;
+    // compiled shapes over 16-byte aligned columns take 2 rows per lane with vector loads
+    {
+      bool vec = P.shape != wgd::SHAPE_GENERIC && !P.has_join && env_int("WG_BATCH_VEC", 1) != 0;
+      for (int j = 0; j < P.n_in; ++j) vec = vec && ((uintptr_t)P.in[j].data % 16 == 0);
+      P.vec_rows = vec ? 1 : 0;
+    }
     a->last_shape = P.shape;
     if (a->L.n_aggs > 4) b->max_na = 8;
     if (P.shape == wgd::SHAPE_GENERIC) b->all_static = false;

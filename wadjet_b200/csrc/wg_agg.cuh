@@ -104,6 +104,8 @@ struct Plan {
                                  // smem_hash_shift (the bits that picked the rows' bucket)
   int32_t smem_list;             // >0: word offset in shared memory of a list of the bucketed
                                  // table's used slots, entry i written by its i-th insert
+  int32_t vec_rows;              // batched work items: 2 rows per lane with vector loads (compiled
+                                 // shape, 16-byte aligned columns, no join or the direct one, no selection)
   DCol in[WG_MAX_IN];
   Pred filt[WG_MAX_FILTERS];
   JoinView join;

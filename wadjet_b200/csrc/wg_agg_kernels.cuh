@@ -1179,8 +1179,9 @@ struct SrcRow {
 // Rows r0 .. r0+U-1 (r0 a multiple of U, column starts 16-byte aligned): one
 // vector load per 16 bytes when all U rows exist, row by row at the end.
 template <int U, class Sh>
-__device__ __forceinline__ void load_rows(const Plan& P, const Sh& sh, int64_t r0, SrcRow (&rw)[U]) {
-  const bool full = r0 + U <= P.n_items;
+__device__ __forceinline__ void load_rows(const Plan& P, const Sh& sh, int64_t r0, SrcRow (&rw)[U], int64_t n_end = -1) {
+  const int64_t n = n_end >= 0 ? n_end : P.n_items;  // rows past n are absent
+  const bool full = r0 + U <= n;
 #pragma unroll
   for (int j = 0; j < WG_MAX_IN; ++j) {
     if (j >= sh.n_in()) break;
@@ -1222,7 +1223,7 @@ __device__ __forceinline__ void load_rows(const Plan& P, const Sh& sh, int64_t r
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         const int64_t row = r0 + u;
-        if (row < P.n_items) {
+        if (row < n) {
           rw[u].v[j] = load_stream(P.in[j].data, cls, row);
           rw[u].v[j].null = sh.nullable() && is_null(P.in[j], row);
         } else {
@@ -1291,12 +1292,14 @@ __device__ __forceinline__ void load_rows_staged(const Sh& sh, const unsigned ch
 // filters and lookups for all rows first, then one warp-wide update per row.
 template <int NA, bool SMEM, int U, class Sh>
 __device__ __forceinline__ void process_loaded_vec(const Plan& P, const Sh& sh, int64_t r0, SrcRow (&rw)[U],
-                                                   unsigned long long* sm, int* s_groups, int s_limit, Credit& cr) {
+                                                   unsigned long long* sm, int* s_groups, int s_limit, Credit& cr,
+                                                   int64_t n_end = -1) {
   bool act[U];
   int32_t brow[U];
+  const int64_t n = n_end >= 0 ? n_end : P.n_items;
 #pragma unroll
   for (int u = 0; u < U; ++u) {
-    act[u] = r0 + u < P.n_items;
+    act[u] = r0 + u < n;
     brow[u] = -1;
 #pragma unroll
     for (int f = 0; f < WG_MAX_FILTERS; ++f) {
