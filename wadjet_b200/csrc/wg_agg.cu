@@ -99,6 +99,39 @@ __global__ void gather_slots_kernel(const unsigned long long* slots, int sw, con
   }
 }
 
+// Spill input normalisation. The rows a selection vector keeps, gathered into
+// a contiguous column (es = 4, 8 or 16 bytes).
+__global__ void spill_gather_kernel(const char* src, int es, const uint32_t* sel, int64_t n, char* dst) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t row = sel ? (int64_t)sel[i] : i;
+    if (es == 4) ((uint32_t*)dst)[i] = __ldg((const uint32_t*)src + row);
+    else if (es == 8) ((unsigned long long*)dst)[i] = __ldg((const unsigned long long*)src + row);
+    else ((longlong2*)dst)[i] = __ldg((const longlong2*)src + row);
+  }
+}
+
+// One validity flag per row (1 = a value; every row when `valid` is null), of
+// the rows a selection vector keeps.
+__global__ void spill_valid_kernel(const uint64_t* valid, const uint32_t* sel, int64_t n, int32_t* ok) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t row = sel ? (int64_t)sel[i] : i;
+    ok[i] = valid ? (int32_t)((__ldg(valid + (row >> 6)) >> (row & 63)) & 1ULL) : 1;
+  }
+}
+
+// Validity words (LSB first) from per-row flags.
+__global__ void pack_valid_kernel(const int32_t* ok, int64_t n, uint64_t* words) {
+  const int64_t nw = (n + 63) / 64;
+  for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < nw; w += (int64_t)gridDim.x * blockDim.x) {
+    uint64_t bits = 0;
+    for (int b = 0; b < 64; ++b) {
+      const int64_t r = w * 64 + b;
+      if (r < n && ok[r]) bits |= 1ULL << b;
+    }
+    words[w] = bits;
+  }
+}
+
 __global__ void iota_kernel(int64_t* out, int64_t n) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) out[i] = i;
 }
@@ -424,6 +457,7 @@ struct wg_agg {
     int64_t rows = 0;
     std::vector<int64_t> off;        // start of each partition in the run (np + 1)
     std::vector<char*> col;          // pinned host copy of each plan input column
+    std::vector<char*> ok;           // pinned host copy of each nullable input's validity flags
   };
   std::vector<SpillRun> runs;
   std::vector<std::pair<char*, int64_t>> host_blocks;  // pinned arena (kept for the next query)
@@ -435,6 +469,11 @@ struct wg_agg {
   std::vector<wg_predicate> sp_filters;
   std::vector<wg_expr> sp_exprs;
   std::vector<wg::DevBuf> sp_dev;    // device staging per plan input column
+  // NULLs and selection vectors: per plan input whether it is nullable; the
+  // gathered rows, validity flags (int32 per row, moved with the rows) and
+  // packed words of a consume call; the flags' and words' staging at finalize
+  std::vector<bool> sp_null;
+  std::vector<wg::DevBuf> sp_norm, sp_ok, sp_words, sp_okdev;
   // export staging (kept for the next export): every output field of a chunk
   // side by side on the device, read back in one copy through pinned memory
   wg::DevBuf exp_dev;
@@ -1109,7 +1148,17 @@ static wg_status run_device(const PipelineRun& r) {
   // many rows per group: most MIN/MAX updates cannot win, so read before the atomic
   const int mm = env_int("WG_MINMAX_TEST", -1);
   ls.P.minmax_test = mm >= 0 ? (mm != 0) : (n_items >= 8 * std::max<int64_t>(expect, 1));
-  const int64_t rows_per_cta = (int64_t)ls.block * (ls.vec ? ls.vec : 1);
+  int64_t rows_per_cta = (int64_t)ls.block * (ls.vec ? ls.vec : 1);
+  // a CTA with a shared table flushes up to all of its slots into the HBM table
+  // at the end, every CTA onto the same hot groups: a small input takes fewer
+  // CTAs, each with at least four rows per slot (16K rows at least), so the
+  // flushes do not outweigh the rows (a 2^20-row query over 4096 groups: 80 us
+  // on 148 CTAs, all flushing every group)
+  if (ls.smem) {
+    const int64_t floor_rows = env_int("WG_SMEM_ROWS_PER_CTA", 0) > 0 ? env_int("WG_SMEM_ROWS_PER_CTA", 0)
+                                                                       : std::max<int64_t>(16384, 4 * (int64_t)S);
+    rows_per_cta = std::max(rows_per_cta, floor_rows);
+  }
   const int64_t want_ctas = (n_items + rows_per_cta - 1) / rows_per_cta + 1;
   ls.grid = (unsigned)std::min<int64_t>((int64_t)ctx->sm_count * blocks_per_sm, want_ctas);
   if (!ls.smem && !stat) ls.grid = (unsigned)std::min<int64_t>((int64_t)ctx->sm_count * 4, (n_items + 1023) / 1024 + 1);
@@ -1811,6 +1860,7 @@ static wgd::Plan part_plan(wg_agg* a, const wgd::Plan& P0, int64_t r0, int64_t m
     const int cls = P.in[j].cls;
     const int64_t es = cls == WG_CLS_I32 || cls == WG_CLS_F32 ? 4 : cls == WG_CLS_DEC ? 16 : 8;
     P.in[j].data = (const char*)P.in[j].data + r0 * es;
+    if (P.in[j].valid) P.in[j].valid += r0 / 64;  // windows start on 64-row boundaries
   }
   P.n_items = m;
   P.L = launch_layout(a, P0);
@@ -1845,29 +1895,70 @@ static wg_status spill_host_alloc(wg_agg* a, int64_t bytes, char** out) {
 // on the device by partition (part_count_kernel / part_scatter_kernel) and
 // copied to pinned host runs. Filters and projections run later, per
 // partition, so every row is kept here.
-static wg_status spill_consume(const PipelineRun& r, const wgd::Plan& P0, const std::vector<int>& in_map) {
+static wg_status spill_consume(const PipelineRun& r, const wgd::Plan& P0in, const std::vector<int>& in_map) {
   wg_agg* a = r.agg;
   Ctx* ctx = a->ctx;
-  if (r.join || P0.sel) return fail(WG_E_UNSUPPORTED, "a spilled aggregation takes no join and no selection vector");
-  for (int j = 0; j < P0.n_in; ++j)
-    if (P0.in[j].valid) return fail(WG_E_UNSUPPORTED, "a spilled aggregation takes no NULLs");
+  if (r.join) return fail(WG_E_UNSUPPORTED, "a spilled aggregation takes no join");
   if (a->sp_map.empty()) {  // remember the consume calls' shape for the per-partition runs
     a->sp_cols.assign(r.in->cols, r.in->cols + r.in->ncols);
     a->sp_map = in_map;
-    a->sp_es.assign((size_t)P0.n_in, 0);
-    for (int j = 0; j < P0.n_in; ++j) {
-      const int cls = P0.in[j].cls;
+    a->sp_es.assign((size_t)P0in.n_in, 0);
+    a->sp_null.assign((size_t)P0in.n_in, false);
+    for (int j = 0; j < P0in.n_in; ++j) {
+      const int cls = P0in.in[j].cls;
       a->sp_es[(size_t)j] = cls == WG_CLS_I32 || cls == WG_CLS_F32 ? 4 : cls == WG_CLS_DEC ? 16 : 8;
+      a->sp_null[(size_t)j] = P0in.in[j].valid != nullptr;
     }
     a->sp_filters.assign(r.filters, r.filters + r.n_filters);
     a->sp_exprs.assign(r.exprs, r.exprs + r.n_exprs);
-    a->sp_dev.resize((size_t)P0.n_in);
+    a->sp_dev.resize((size_t)P0in.n_in);
+    a->sp_norm.resize((size_t)P0in.n_in);
+    a->sp_ok.resize((size_t)P0in.n_in);
+    a->sp_words.resize((size_t)P0in.n_in);
+    a->sp_okdev.resize((size_t)P0in.n_in);
   } else {
     bool same = (int)a->sp_cols.size() == r.in->ncols && a->sp_map == in_map &&
                 (int)a->sp_filters.size() == r.n_filters && (int)a->sp_exprs.size() == r.n_exprs;
     for (int c = 0; same && c < r.in->ncols; ++c)
       same = a->sp_cols[(size_t)c].type_id == r.in->cols[c].type_id && a->sp_cols[(size_t)c].scale == r.in->cols[c].scale;
     if (!same) return fail(WG_E_UNSUPPORTED, "every consume call of a spilled aggregation must have the same shape");
+    for (int j = 0; j < P0in.n_in; ++j)
+      if (P0in.in[j].valid && !a->sp_null[(size_t)j])
+        return fail(WG_E_UNSUPPORTED, "NULLs in a column the spilled aggregation's first call had none in");
+  }
+  // The rows a selection vector keeps, gathered; each nullable input's
+  // validity as one flag per row (moved with the rows into the runs) and as
+  // packed words the partition kernels read (NULL keys hash like the table).
+  wgd::Plan P0 = P0in;
+  bool any_null = false;
+  for (int j = 0; j < P0in.n_in; ++j) any_null = any_null || a->sp_null[(size_t)j];
+  if (P0in.sel || any_null) {
+    const int64_t nn = P0in.n_items;
+    for (int j = 0; j < P0in.n_in; ++j) {
+      const int64_t es = a->sp_es[(size_t)j];
+      if (P0in.sel) {
+        WG_TRY(a->sp_norm[(size_t)j].ensure(ctx, std::max<int64_t>(nn, 1) * es));
+        spill_gather_kernel<<<grid_cap(ctx, nn, 256), 256, 0, ctx->stream>>>(
+            (const char*)P0in.in[j].data, (int)es, P0in.sel, nn, a->sp_norm[(size_t)j].as<char>());
+        ctx->count_launch();
+        WG_CUDA_TRY(cudaGetLastError());
+        P0.in[j].data = a->sp_norm[(size_t)j].get();
+      }
+      P0.in[j].valid = nullptr;
+      if (a->sp_null[(size_t)j]) {
+        WG_TRY(a->sp_ok[(size_t)j].ensure(ctx, std::max<int64_t>(nn, 1) * 4));
+        WG_TRY(a->sp_words[(size_t)j].ensure(ctx, ((nn + 63) / 64 + 1) * 8));
+        spill_valid_kernel<<<grid_cap(ctx, nn, 256), 256, 0, ctx->stream>>>(P0in.in[j].valid, P0in.sel, nn,
+                                                                           a->sp_ok[(size_t)j].as<int32_t>());
+        ctx->count_launch();
+        pack_valid_kernel<<<grid_cap(ctx, (nn + 63) / 64, 256), 256, 0, ctx->stream>>>(
+            a->sp_ok[(size_t)j].as<int32_t>(), nn, a->sp_words[(size_t)j].as<uint64_t>());
+        ctx->count_launch();
+        WG_CUDA_TRY(cudaGetLastError());
+        P0.in[j].valid = a->sp_words[(size_t)j].as<uint64_t>();
+      }
+    }
+    P0.sel = nullptr;
   }
   const int pbits = a->spill_pbits, np = 1 << pbits;
   const unsigned grid = (unsigned)(ctx->sm_count * 2);
@@ -1879,7 +1970,9 @@ static wg_status spill_consume(const PipelineRun& r, const wgd::Plan& P0, const 
   for (int e : a->sp_es) row_bytes += e;
   const int64_t room = ctx->ledger.budget() > 0 ? ctx->ledger.budget() - ctx->ledger.used() : (int64_t(1) << 40);
   const int64_t n = P0.n_items;
-  const int64_t win = std::max<int64_t>(int64_t(1) << 16, std::min<int64_t>(int64_t(1) << 24, room / 4 / std::max<int64_t>(row_bytes, 1)));
+  for (int j = 0; j < P0.n_in; ++j) row_bytes += a->sp_null[(size_t)j] ? 4 : 0;
+  const int64_t win = std::max<int64_t>(int64_t(1) << 16, std::min<int64_t>(int64_t(1) << 24, room / 4 / std::max<int64_t>(row_bytes, 1))) &
+                      ~int64_t(63);  // validity words stay whole
   std::vector<uint32_t> hc((size_t)np * grid);
   std::vector<unsigned long long> ho((size_t)np * grid);
   for (int64_t r0 = 0; r0 < n; r0 += win) {
@@ -1907,6 +2000,12 @@ static wg_status spill_consume(const PipelineRun& r, const wgd::Plan& P0, const 
       WG_TRY(a->sp_dev[(size_t)j].ensure(ctx, win * a->sp_es[(size_t)j]));
       po.data[j] = a->sp_dev[(size_t)j].as<char>();
       po.es[j] = a->sp_es[(size_t)j];
+      if (a->sp_null[(size_t)j]) {  // the validity flags move with the rows
+        WG_TRY(a->sp_okdev[(size_t)j].ensure(ctx, win * 4));
+        po.side_src[po.n_side] = a->sp_ok[(size_t)j].as<int32_t>() + r0;
+        po.side_dst[po.n_side] = a->sp_okdev[(size_t)j].as<int32_t>();
+        ++po.n_side;
+      }
     }
     WG_CUDA_TRY(cudaFuncSetAttribute(wgd::part_scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)wgd::part_scatter_smem(np)));
@@ -1915,10 +2014,16 @@ static wg_status spill_consume(const PipelineRun& r, const wgd::Plan& P0, const 
     ctx->count_launch();
     WG_CUDA_TRY(cudaGetLastError());
     run.col.assign((size_t)P.n_in, nullptr);
+    run.ok.assign((size_t)P.n_in, nullptr);
     for (int j = 0; j < P.n_in; ++j) {
       WG_TRY(spill_host_alloc(a, m * a->sp_es[(size_t)j], &run.col[(size_t)j]));
       WG_CUDA_TRY(cudaMemcpyAsync(run.col[(size_t)j], po.data[j], (size_t)(m * a->sp_es[(size_t)j]),
                                   cudaMemcpyDeviceToHost, ctx->stream));
+      if (a->sp_null[(size_t)j]) {
+        WG_TRY(spill_host_alloc(a, m * 4, &run.ok[(size_t)j]));
+        WG_CUDA_TRY(cudaMemcpyAsync(run.ok[(size_t)j], a->sp_okdev[(size_t)j].get(), (size_t)(m * 4),
+                                    cudaMemcpyDeviceToHost, ctx->stream));
+      }
     }
     WG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     a->runs.push_back(std::move(run));
@@ -1944,7 +2049,15 @@ static wg_status spill_finish(wg_agg* a) {
   }
   for (int j = 0; j < nin; ++j) {  // staging for one partition (the consume windows' buffers go first)
     a->sp_dev[(size_t)j].reset();
+    a->sp_norm[(size_t)j].reset();
+    a->sp_ok[(size_t)j].reset();
     WG_TRY(a->sp_dev[(size_t)j].alloc(ctx, std::max<int64_t>(max_rows, 1) * a->sp_es[(size_t)j]));
+    if (a->sp_null[(size_t)j]) {
+      a->sp_okdev[(size_t)j].reset();
+      a->sp_words[(size_t)j].reset();
+      WG_TRY(a->sp_okdev[(size_t)j].alloc(ctx, std::max<int64_t>(max_rows, 1) * 4));
+      WG_TRY(a->sp_words[(size_t)j].alloc(ctx, ((max_rows + 63) / 64 + 1) * 8));
+    }
   }
   DevBuf res;
   int64_t res_cap = std::max<int64_t>(a->hint, 1024), n_res = 0;
@@ -1961,14 +2074,28 @@ static wg_status spill_finish(wg_agg* a) {
         const int64_t es = a->sp_es[(size_t)j];
         WG_CUDA_TRY(cudaMemcpyAsync(a->sp_dev[(size_t)j].as<char>() + rows * es, run.col[(size_t)j] + run.off[(size_t)p] * es,
                                     (size_t)(c * es), cudaMemcpyHostToDevice, ctx->stream));
+        if (a->sp_null[(size_t)j])
+          WG_CUDA_TRY(cudaMemcpyAsync(a->sp_okdev[(size_t)j].as<char>() + rows * 4, run.ok[(size_t)j] + run.off[(size_t)p] * 4,
+                                      (size_t)(c * 4), cudaMemcpyHostToDevice, ctx->stream));
       }
       rows += c;
     }
     if (rows == 0) continue;
+    for (int j = 0; j < nin; ++j) {  // the partition's validity words from its rows' flags
+      if (!a->sp_null[(size_t)j]) continue;
+      pack_valid_kernel<<<grid_cap(ctx, (rows + 63) / 64, 256), 256, 0, ctx->stream>>>(
+          a->sp_okdev[(size_t)j].as<int32_t>(), rows, a->sp_words[(size_t)j].as<uint64_t>());
+      ctx->count_launch();
+      WG_CUDA_TRY(cudaGetLastError());
+    }
     for (size_t c = 0; c < cols.size(); ++c) {
       cols[c].len = rows;
       cols[c].valid_words = nullptr;
-      if (a->sp_map[c] >= 0) cols[c].data = a->sp_dev[(size_t)a->sp_map[c]].get();
+      const int j = a->sp_map[c];
+      if (j >= 0) {
+        cols[c].data = a->sp_dev[(size_t)j].get();
+        if (a->sp_null[(size_t)j]) cols[c].valid_words = a->sp_words[(size_t)j].as<uint64_t>();
+      }
     }
     d.len = rows;
     // the small table, empty again

@@ -1073,6 +1073,11 @@ static __global__ void __launch_bounds__(kPartThreads) part_count_kernel(const _
 struct PartOut {
   char* data[WG_MAX_IN];
   int32_t es[WG_MAX_IN];
+  // side columns moved with the rows (4 bytes each, e.g. one validity flag per
+  // row of a nullable input): side_src[k] + row, in the rows' order
+  const int32_t* side_src[WG_MAX_IN];
+  int32_t* side_dst[WG_MAX_IN];
+  int32_t n_side;
 };
 
 // Exclusive prefix sums of v[0..n) in place (n <= 2 * blockDim.x, blockDim.x a
@@ -1154,6 +1159,14 @@ static __global__ void __launch_bounds__(kPartThreads) part_scatter_kernel(const
         if (es == 4) *(uint32_t*)d = __ldg((const uint32_t*)(src + (size_t)k * 4));
         else if (es == 8) *(unsigned long long*)d = __ldg((const unsigned long long*)(src + (size_t)k * 8));
         else *(longlong2*)d = __ldg((const longlong2*)(src + (size_t)k * 16));
+      }
+    }
+    for (int j = 0; j < out.n_side; ++j) {
+      const int32_t* src = out.side_src[j] + t0;
+      for (int q = threadIdx.x; q < m; q += blockDim.x) {
+        const int k = perm[q];
+        const uint32_t p = part[k];
+        out.side_dst[j][gcur[p] + (q - loff[p])] = __ldg(src + k);
       }
     }
     __syncthreads();
