@@ -141,7 +141,9 @@ def test_spilled_aggregate_with_nulls_and_a_selection_matches_oracle():
         got = g.export()
         g.close()
     o = ob.Agg([0], [(0, 1, 0), (1, 1, 0), (2, 2, 0), (3, 2, 0)])
-    ob.pipeline(ob.HostBatch([(I64, hk, kvalid, 0), (I64, hv, vvalid, 0), (F64, hf, None, 0)], sel=sel), o, threads=8)
+    # the oracle's pipeline takes flat batches: the selected rows themselves
+    ob.pipeline(ob.HostBatch([(I64, hk[sel], kvalid[sel], 0), (I64, hv[sel], vvalid[sel], 0), (F64, hf[sel], None, 0)]),
+                o, threads=8)
     want = o.export()
     assert (want["key_valid"][0] == 0).any()  # the NULL-key group exists
     assert_groups_equal(got, want, kinds)

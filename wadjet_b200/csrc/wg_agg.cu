@@ -62,21 +62,25 @@ __device__ __forceinline__ bool slot_used(const Layout& L, const unsigned long l
 
 // Fold every group of table (Ls, Ts) into (Ld, Td): MergeSink, table growth and
 // layout upgrades are all this one kernel.
-// compact_n >= 0: the source is a compact result of compact_n groups (every
-// row a group; a key equal to the empty pattern is that key's group).
+// compact_n >= 0: the source is a compact result of compact_n groups, slot
+// list[i] for group i (every listed slot a group; a key equal to the empty
+// pattern is that key's group, and the slot at the view's capacity + 1, when
+// listed, is the NULL-key group).
 template <int NA>
-__global__ void fold_kernel(Layout Ls, Table Ts, Layout Ld, Table Td, int32_t* err, int64_t compact_n) {
+__global__ void fold_kernel(Layout Ls, Table Ts, Layout Ld, Table Td, int32_t* err, int64_t compact_n,
+                            const int64_t* list) {
   Credit cr;
-  const uint64_t cap = compact_n >= 0 ? ~0ULL - 2 : Ts.mask + 1;
+  const uint64_t cap = Ts.mask + 1;
   const uint64_t n = compact_n >= 0 ? (uint64_t)compact_n : Ls.key_words == 0 ? 1 : cap + 2;
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-    const unsigned long long* s = Ts.slots + i * Ls.slot_words;
-    if (compact_n < 0 && !slot_used(Ls, s, i, cap)) continue;
+    const uint64_t idx = compact_n >= 0 ? (uint64_t)list[i] : i;
+    const unsigned long long* s = Ts.slots + idx * Ls.slot_words;
+    if (compact_n < 0 && !slot_used(Ls, s, idx, cap)) continue;
     unsigned long long k0 = 0, k1 = 0;
     bool knull = false;
     if (Ls.key_words >= 1) {
-      if (i == cap + 1) knull = true;
-      else if (i == cap) { k0 = Ls.key_words == 1 ? WG_EMPTY_KEY : ~0ULL; k1 = ~0ULL; }
+      if (idx == cap + 1) knull = true;
+      else if (compact_n < 0 && idx == cap) { k0 = Ls.key_words == 1 ? WG_EMPTY_KEY : ~0ULL; k1 = ~0ULL; }
       else { k0 = s[0]; if (Ls.key_words == 2) k1 = s[1]; }
     }
     const LayoutAcc ls{Ls}, ld{Ld};
@@ -395,8 +399,8 @@ __global__ void state_merge_kernel(Layout Ls, const unsigned long long* rows, in
 
 template <int NA>
 void launch_fold(const Layout& Ls, const Table& Ts, const Layout& Ld, const Table& Td, int32_t* err, unsigned grid,
-                 cudaStream_t st, int64_t compact_n = -1) {
-  fold_kernel<NA><<<grid, 256, 0, st>>>(Ls, Ts, Ld, Td, err, compact_n);
+                 cudaStream_t st, int64_t compact_n = -1, const int64_t* list = nullptr) {
+  fold_kernel<NA><<<grid, 256, 0, st>>>(Ls, Ts, Ld, Td, err, compact_n, list);
 }
 
 unsigned grid_cap(wg::Ctx* ctx, int64_t n, int block, int per_sm = 16) {
@@ -602,12 +606,12 @@ static uint64_t cap_for(int64_t groups) {
 static int log2u(uint64_t v) { int l = 0; while ((1ULL << l) < v) ++l; return l; }
 
 static void run_fold(wg_agg* a, const wgd::Layout& Ls, const wgd::Table& Ts, const wgd::Layout& Ld, const wgd::Table& Td,
-                     int64_t compact_n = -1) {
+                     int64_t compact_n = -1, const int64_t* list = nullptr) {
   Ctx* ctx = a->ctx;
   const int64_t n = compact_n >= 0 ? std::max<int64_t>(compact_n, 1) : Ls.key_words == 0 ? 1 : (int64_t)(Ts.mask + 3);
   const unsigned grid = grid_cap(ctx, n, 256);
-  if (Ls.n_aggs <= 4) launch_fold<4>(Ls, Ts, Ld, Td, ctx->dev_error, grid, ctx->stream, compact_n);
-  else launch_fold<8>(Ls, Ts, Ld, Td, ctx->dev_error, grid, ctx->stream, compact_n);
+  if (Ls.n_aggs <= 4) launch_fold<4>(Ls, Ts, Ld, Td, ctx->dev_error, grid, ctx->stream, compact_n, list);
+  else launch_fold<8>(Ls, Ts, Ld, Td, ctx->dev_error, grid, ctx->stream, compact_n, list);
   ctx->count_launch();
 }
 
@@ -2059,7 +2063,8 @@ static wg_status spill_finish(wg_agg* a) {
       WG_TRY(a->sp_words[(size_t)j].alloc(ctx, ((max_rows + 63) / 64 + 1) * 8));
     }
   }
-  DevBuf res;
+  DevBuf res, null_slot;
+  bool has_null = false;
   int64_t res_cap = std::max<int64_t>(a->hint, 1024), n_res = 0;
   WG_TRY(res.alloc(ctx, res_cap * sw * 8));
   std::vector<wg_column> cols = a->sp_cols;
@@ -2110,6 +2115,20 @@ static wg_status spill_finish(wg_agg* a) {
                    a->sp_exprs.data()};
     rp.no_partition = true;
     WG_TRY(run_device(rp));
+    if (a->L.key_words == 1) {
+      // the NULL-key group (single-word keys: the table's slot cap + 1; every
+      // NULL-key row is in partition 0) is kept aside and appended last
+      const unsigned long long* ns = a->table.as<unsigned long long>() + (a->cap + 1) * (uint64_t)sw;
+      int64_t rows_null = 0;
+      WG_TRY(read_back_i64(ctx, (const int64_t*)(ns + a->L.key_words), &rows_null, 1));
+      if (rows_null != 0) {
+        if (has_null) return fail(WG_E_CUDA, "NULL-key rows in more than one spill partition");
+        WG_TRY(null_slot.ensure(ctx, sw * 8));
+        WG_CUDA_TRY(cudaMemcpyAsync(null_slot.get(), ns, (size_t)(sw * 8), cudaMemcpyDeviceToDevice, ctx->stream));
+        WG_CUDA_TRY(cudaMemsetAsync((void*)(ns + a->L.key_words), 0, 8, ctx->stream));  // out of this compaction
+        has_null = true;
+      }
+    }
     WG_TRY(agg_compact(a));
     if (n_res + a->n_out > res_cap) {  // grow the result, keeping what it holds
       const int64_t cap2 = std::max<int64_t>(res_cap * 2, n_res + a->n_out);
@@ -2129,15 +2148,36 @@ static wg_status spill_finish(wg_agg* a) {
     }
     n_res += a->n_out;
   }
-  // the compact result becomes the table: every slot a group, no NULL-key slot
+  // The compact result becomes the table: every listed slot a group. With a
+  // NULL-key group the slots are [groups][unused][NULL group] and the view's
+  // capacity is the number of groups, so the NULL group sits at capacity + 1
+  // where the readers of a table look for it; the list skips the unused slot.
+  if (has_null) {
+    if (n_res + 2 > res_cap) {
+      DevBuf bigger;
+      WG_TRY(bigger.alloc(ctx, (n_res + 2) * sw * 8));
+      if (n_res > 0)
+        WG_CUDA_TRY(cudaMemcpyAsync(bigger.get(), res.get(), (size_t)(n_res * sw * 8), cudaMemcpyDeviceToDevice, ctx->stream));
+      WG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+      res = std::move(bigger);
+    }
+    WG_CUDA_TRY(cudaMemcpyAsync(res.as<unsigned long long>() + (n_res + 1) * sw, null_slot.get(), (size_t)(sw * 8),
+                                cudaMemcpyDeviceToDevice, ctx->stream));
+  }
   a->table = std::move(res);
-  a->cap = uint64_t(1) << 62;
+  a->cap = has_null ? (uint64_t)n_res : uint64_t(1) << 62;
   a->spilled = true;
-  WG_TRY(a->list.ensure(ctx, std::max<int64_t>(n_res, 1) * 8));
+  const int64_t n_list = n_res + (has_null ? 1 : 0);
+  WG_TRY(a->list.ensure(ctx, std::max<int64_t>(n_list, 1) * 8));
   iota_kernel<<<grid_cap(ctx, std::max<int64_t>(n_res, 1), 256), 256, 0, ctx->stream>>>(a->list.as<int64_t>(), n_res);
   ctx->count_launch();
   WG_CUDA_TRY(cudaGetLastError());
-  a->n_out = n_res;
+  if (has_null) {
+    const int64_t at = n_res + 1;
+    WG_CUDA_TRY(cudaMemcpyAsync(a->list.as<int64_t>() + n_res, &at, 8, cudaMemcpyHostToDevice, ctx->stream));
+    WG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));  // `at` is on this stack
+  }
+  a->n_out = n_list;
   a->runs.clear();
   for (auto& b : a->sp_dev) b.reset();  // staging and snapshots go back to the ledger
   a->backup.reset();
@@ -2303,7 +2343,8 @@ wg_status wg_agg_merge(wg_agg* d, wg_agg* s) {
   }
   const int64_t need = d->known_groups + s_groups + credit_slack(d);
   if (d->L.key_words != 0 && need > (int64_t)((double)d->cap * kMaxLoad)) WG_TRY(rebuild_table(d, cap_for(need), d->L));
-  run_fold(d, s->L, table_view(s), d->L, table_view(d), s->spilled ? s->n_out : -1);
+  run_fold(d, s->L, table_view(s), d->L, table_view(d), s->spilled ? s->n_out : -1,
+           s->spilled ? s->list.as<int64_t>() : nullptr);
   WG_CUDA_TRY(cudaGetLastError());
   WG_TRY(refresh_groups(d));
   return check_device_error(ctx);
