@@ -1636,16 +1636,21 @@ static wg_status hc_consume(const PipelineRun& r, const wgd::Plan& P0) {
 }
 
 template <int NA, class Sh>
-static void launch_hc_bucket(const wgd::Plan& P, size_t smem, const int64_t* boff, int64_t nb, unsigned long long* out,
-                             unsigned long long* cursor, int64_t cap, int32_t* over, int sms, int ctas,
-                             cudaStream_t st) {
+static cudaError_t launch_hc_bucket(const wgd::Plan& P, size_t smem, const int64_t* boff, int64_t nb,
+                                    unsigned long long* out, unsigned long long* cursor, int64_t cap, int32_t* over,
+                                    int sms, int ctas, cudaStream_t st) {
   if (ctas == 1) {
-    cudaFuncSetAttribute(wgd::hc_bucket_kernel<NA, Sh, 1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const cudaError_t e =
+        cudaFuncSetAttribute(wgd::hc_bucket_kernel<NA, Sh, 1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
     wgd::hc_bucket_kernel<NA, Sh, 1024><<<sms, 1024, smem, st>>>(P, boff, nb, out, cursor, cap, over);
   } else {
-    cudaFuncSetAttribute(wgd::hc_bucket_kernel<NA, Sh, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const cudaError_t e =
+        cudaFuncSetAttribute(wgd::hc_bucket_kernel<NA, Sh, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
     wgd::hc_bucket_kernel<NA, Sh, 512><<<sms * 2, 512, smem, st>>>(P, boff, nb, out, cursor, cap, over);
   }
+  return cudaGetLastError();
 }
 
 // Finalize of the two-level mode: the runs re-partitioned into buckets, the
@@ -1797,12 +1802,15 @@ static wg_status hc_finish(wg_agg* a) {
     WG_CUDA_TRY(cudaMemsetAsync(a->hc_scalars.get(), 0, 64, ctx->stream));
     Pb.T = table_view(a);
     const int sms = ctx->sm_count;
-    if (stat) launch_hc_bucket<4, wgd::StatShape<wgd::ShapeHighCard>>(Pb, smem, d_boff, nb, a->hc_out.as<unsigned long long>(),
-                                                                     d_ocur, cap, d_over, sms, ctas, ctx->stream);
-    else if (a->L.n_aggs <= 4) launch_hc_bucket<4, wgd::DynShape>(Pb, smem, d_boff, nb, a->hc_out.as<unsigned long long>(),
-                                                                  d_ocur, cap, d_over, sms, ctas, ctx->stream);
-    else launch_hc_bucket<8, wgd::DynShape>(Pb, smem, d_boff, nb, a->hc_out.as<unsigned long long>(), d_ocur, cap,
-                                            d_over, sms, ctas, ctx->stream);
+    if (stat)
+      WG_CUDA_TRY((launch_hc_bucket<4, wgd::StatShape<wgd::ShapeHighCard>>(
+          Pb, smem, d_boff, nb, a->hc_out.as<unsigned long long>(), d_ocur, cap, d_over, sms, ctas, ctx->stream)));
+    else if (a->L.n_aggs <= 4)
+      WG_CUDA_TRY((launch_hc_bucket<4, wgd::DynShape>(Pb, smem, d_boff, nb, a->hc_out.as<unsigned long long>(), d_ocur,
+                                                      cap, d_over, sms, ctas, ctx->stream)));
+    else
+      WG_CUDA_TRY((launch_hc_bucket<8, wgd::DynShape>(Pb, smem, d_boff, nb, a->hc_out.as<unsigned long long>(), d_ocur,
+                                                      cap, d_over, sms, ctas, ctx->stream)));
     ctx->count_launch();
     WG_CUDA_TRY(cudaGetLastError());
     int64_t v[2], t[2];
