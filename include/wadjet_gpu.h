@@ -364,6 +364,14 @@ WG_API wg_status wg_join_build_append_device(wg_join* j, const wg_batch_desc* bu
  * partitions that fit; wg_join_probe and wg_join_gather then return
  * WG_E_UNSUPPORTED. */
 WG_API wg_status wg_join_build_finish(wg_join* j);
+/* BloomFilterOp.Execute (exec/bloom_filter_op.go:39) for the join's probe key:
+ * the rows of `probe` (or its selection entries) whose non-NULL key the build
+ * side's bloom filter (HashJoin.buildBloom, join.go:1441: about 10 bits per
+ * distinct key, two bits per key from bloomHashInt) may contain, ascending, in
+ * out_sel (host memory with room for every row or selection entry); *n_out
+ * their count. The fused pipeline's hash probe checks the same bloom first
+ * when the hash index is larger than half of L2 (WG_JOIN_BLOOM=0/1 forces). */
+WG_API wg_status wg_join_bloom_filter(wg_join* j, const wg_batch_desc* probe, uint32_t* out_sel, int64_t* n_out);
 /* Number of build rows stored and number of distinct keys indexed (-1 for a
  * partitioned build: keys are not counted across partitions). */
 WG_API wg_status wg_join_build_stats(wg_join* j, int64_t* build_rows, int64_t* distinct_keys);

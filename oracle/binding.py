@@ -71,6 +71,7 @@ def lib() -> C.CDLL:
             "or_last_error": (C.c_char_p, []),
             "or_filter": (I64, [C.POINTER(Column), I64, P, I64, C.POINTER(Predicate), P]),
             "or_join_new": (P, [I64]),
+            "or_join_bloom_filter": (I64, [P, C.POINTER(Column), I64, P, I64, P, P]),
             "or_join_append": (C.c_int, [P, C.POINTER(Column), I64]),
             "or_join_rows": (I64, [P]),
             "or_join_distinct": (I64, [P]),
@@ -181,6 +182,18 @@ class Join:
 
     def distinct(self):
         return lib().or_join_distinct(self.h)
+
+    def bloom_filter(self, t, keys, valid=None, sel=None):
+        """BloomFilterOp.Execute over one int key column: (selected rows, bloom words)."""
+        b = HostBatch([(t, keys, valid, 0)], sel=sel)
+        s = b.keep[-1] if sel is not None else None
+        sp, sl = (_ptr(s), len(s)) if s is not None else (None, 0)
+        out = np.empty(max(1, len(keys) if s is None else len(s)), np.uint32)
+        nw = C.c_int64()
+        n = lib().or_join_bloom_filter(self.h, C.byref(b.arr[0]), len(keys), sp, sl, out.ctypes.data, C.byref(nw))
+        if n < 0:
+            raise RuntimeError(_err())
+        return out[:n].copy(), nw.value
 
     def __del__(self):
         if getattr(self, "h", None):

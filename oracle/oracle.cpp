@@ -877,6 +877,52 @@ int64_t or_filter(const wg_column* col, int64_t len, const uint32_t* sel, int64_
   return n;
 }
 
+// HashJoin.buildBloom (join.go:1441) over the join's distinct keys, then
+// BloomFilterOp.Execute (bloom_filter_op.go:39) for one int key: the probe rows
+// (or selection entries) with a non-NULL key that the bloom may contain, in
+// order. bloomHashInt (join.go:1650), bloomSet (:1475), bloomContains
+// (bloom_filter_op.go:268): 64-bit words, about 10 bits per distinct key
+// rounded up to a power-of-two word count (at least 8), two bits per key.
+static uint64_t bloom_hash_int(int64_t key) {
+  const uint64_t x = (uint64_t)key * 0x9E3779B97F4A7C15ULL;
+  return x ^ (x >> 32);
+}
+
+int64_t or_join_bloom_filter(void* jp, const wg_column* key, int64_t len, const uint32_t* sel, int64_t sel_len,
+                             uint32_t* out_sel, int64_t* n_words) {
+  Join* j = (Join*)jp;
+  if (!is_int_cls(key->type_id)) return fail("bloom filter key is not an integer-class column");
+  const int64_t n_keys = j->index->size;
+  std::vector<uint64_t> bloom;
+  uint64_t mask = 0;
+  if (n_keys > 0) {
+    const int64_t n_bits = n_keys * 10;
+    int64_t slots = 1;
+    while (slots * 64 < n_bits) slots *= 2;
+    if (slots < 8) slots = 8;
+    bloom.assign((size_t)slots, 0);
+    mask = (uint64_t)slots - 1;
+    for (const auto& e : j->index->e) {
+      if (e.key == kIntHashEmpty) continue;
+      const uint64_t h = bloom_hash_int(e.key);
+      bloom[h & mask] |= 1ULL << (h & 63);
+      bloom[(h >> 17) & mask] |= 1ULL << ((h >> 6) & 63);
+    }
+  }
+  if (n_words) *n_words = (int64_t)bloom.size();
+  const int64_t n = sel ? sel_len : len;
+  int64_t m = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    const int64_t row = sel ? (int64_t)sel[i] : i;
+    if (is_null(*key, row)) continue;
+    if (bloom.empty()) continue;  // no build keys: nothing may match
+    const uint64_t h = bloom_hash_int(get_i64(*key, row));
+    if (((bloom[h & mask] >> (h & 63)) & 1ULL) && ((bloom[(h >> 17) & mask] >> ((h >> 6) & 63)) & 1ULL))
+      out_sel[m++] = (uint32_t)row;
+  }
+  return m;
+}
+
 void* or_join_new(int64_t hint) {
   Join* j = new Join();
   j->index.reset(new IntHashTable(hint > 0 ? hint : 64));

@@ -26,6 +26,8 @@ const char* or_last_error(void);
 /* KernelFilter.Execute + compareFilterImpl (exec/filter.go:373-425,
  * exec/kernel/compare.go:47-90,145-182). Returns the number of selected rows
  * written to out_sel (ascending), or -1 on an unsupported column type. */
+int64_t or_join_bloom_filter(void* join, const wg_column* key, int64_t len, const uint32_t* sel, int64_t sel_len,
+                             uint32_t* out_sel, int64_t* n_words);
 int64_t or_filter(const wg_column* col, int64_t len, const uint32_t* sel, int64_t sel_len,
                   const wg_predicate* p, uint32_t* out_sel);
 

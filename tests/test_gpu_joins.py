@@ -115,3 +115,35 @@ def test_fused_pipeline_matches_oracle(ctx, jt, dups, nulls):
         assert (want["key_valid"][0] == 0).any()  # the NULL-padded rows form the NULL group
     g.close()
     j.close()
+
+
+@pytest.mark.parametrize("kt", [I32, I64])
+@pytest.mark.parametrize("dups,nulls", [(False, 0.0), (True, 0.05)])
+@pytest.mark.parametrize("use_sel", [False, True])
+def test_bloom_filter_matches_oracle(ctx, kt, dups, nulls, use_sel):
+    """BloomFilterOp.Execute (bloom_filter_op.go:39) over the probe keys, with the build side's
+    bloom (HashJoin.buildBloom, join.go:1441): the same rows as the oracle's restatement, bit for
+    bit (same hash, same sizing over the distinct keys), every true match among them."""
+    import wadjet_b200 as wg
+    bkeys, bvalid, _, pkeys, pvalid, _, _ = _data(41 + kt + dups, dups, nulls, kt)
+    j = wg.HashJoin(ctx, 0, 0)
+    j.build([wg.Batch([wg.Column(kt, bkeys, bvalid)])])
+    oj = ob.Join(1024)
+    oj.append(kt, bkeys, bvalid)
+    rng = np.random.default_rng(2)
+    sel = np.sort(rng.choice(len(pkeys), size=len(pkeys) // 2, replace=False)).astype(np.uint32) if use_sel else None
+    got = j.bloom_filter(wg.Batch([wg.Column(kt, pkeys, pvalid)], sel=sel))
+    want, _ = oj.bloom_filter(kt, pkeys, pvalid, sel=sel)
+    np.testing.assert_array_equal(got, want)
+    matched = np.unique(oj.probe(kt, pkeys, pvalid, sel=sel)[0])
+    assert np.isin(matched, got).all()  # no false negatives
+    assert len(got) < (len(sel) if use_sel else len(pkeys))  # the misses (key + 3) are mostly rejected
+    j.close()
+
+
+@pytest.mark.parametrize("jt", ["left", "semi", "anti"])
+def test_fused_pipeline_with_bloom_matches_oracle(ctx, jt, monkeypatch):
+    """The fused probe with the bloom checked before the hash index (WG_JOIN_BLOOM=1): the
+    same groups as without it."""
+    monkeypatch.setenv("WG_JOIN_BLOOM", "1")
+    test_fused_pipeline_matches_oracle(ctx, jt, True, 0.05)

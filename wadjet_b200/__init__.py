@@ -334,6 +334,16 @@ class HashJoin:
             if n.value < cap:
                 return
 
+    def bloom_filter(self, batch: Batch) -> np.ndarray:
+        """BloomFilterOp.Execute: the rows (or selection entries) whose probe key the build side's
+        bloom filter may contain, ascending."""
+        d, keep = batch.desc()
+        n_items = len(batch.sel) if batch.sel is not None else batch.len
+        out = np.empty(max(1, n_items), np.uint32)
+        n = C.c_int64()
+        _check(lib.wg_join_bloom_filter(self.h, C.byref(d), out.ctypes.data, C.byref(n)))
+        return out[: n.value].copy()
+
     def gather(self, payload_idx: int, build_rows: np.ndarray, dtype) -> tuple[np.ndarray, np.ndarray]:
         rows = np.ascontiguousarray(build_rows, np.int64)
         out = np.empty(max(1, len(rows)), dtype)

@@ -145,6 +145,7 @@ SIGNATURES = {
     "wg_join_build_stats": (I32, [P, PI64, PI64]),
     "wg_join_probe": (I32, [P, C.POINTER(wg_batch_desc), P, P, I64, PI64, PI64]),
     "wg_join_gather": (I32, [P, I32, P, I64, P, P]),
+    "wg_join_bloom_filter": (I32, [P, C.POINTER(wg_batch_desc), P, PI64]),
     "wg_join_reset": (I32, [P]),
     "wg_join_destroy": (I32, [P]),
     "wg_agg_create": (I32, [P, I32, C.POINTER(C.c_int32), I32, C.POINTER(wg_agg_spec), I64, PP]),

@@ -228,6 +228,28 @@ __global__ void dense_build_kernel(DCol key, int64_t n, const uint32_t* pay, lon
   }
 }
 
+// The bloom's bits for every build row with a key (duplicates set the same
+// bits as their key's first row, so this is the bloom over distinct keys).
+__global__ void bloom_build_kernel(DCol key, int64_t n, unsigned long long* bloom, unsigned long long mask) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    if (is_null(key, i)) continue;
+    const unsigned long long h = bloom_hash_int(ld_i64(key, i));
+    atomicOr(bloom + (h & mask), 1ULL << (h & 63));
+    atomicOr(bloom + ((h >> 17) & mask), 1ULL << ((h >> 6) & 63));
+  }
+}
+
+// BloomFilterOp over a probe key column: per item (row, or selection entry),
+// its row number and whether the bloom may contain its (non-NULL) key.
+__global__ void bloom_probe_kernel(DCol key, const uint32_t* sel, int64_t n, const unsigned long long* bloom,
+                                   unsigned long long mask, uint32_t* rows, uint8_t* flags) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t row = sel ? (int64_t)sel[i] : i;
+    rows[i] = (uint32_t)row;
+    flags[i] = !is_null(key, row) && bloom_contains(bloom, mask, bloom_hash_int(ld_i64(key, row))) ? 1 : 0;
+  }
+}
+
 // Payload-only dense table from a full dense direct table (every slot used).
 __global__ void dense_payload_kernel(const unsigned long long* slots, int64_t n, uint32_t* out) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -349,6 +371,10 @@ struct wg_join {
   int pass_built = -1;
   // on a pass join: the partitions it covers (part_shift 0 = all)
   int32_t pass_shift = 0, pass_lo = 0, pass_hi = 0;
+  // the bloom pre-filter (HashJoin.buildBloom), built on first use
+  wg::DevBuf bloom, bloom_rows, bloom_flags, bloom_out, bloom_tmp;
+  uint64_t bloom_mask = 0;
+  bool bloom_built = false;
   ~wg_join() { delete pass; }
 };
 
@@ -692,6 +718,8 @@ static wg_status join_view_fields(wg_join* j, wgd::JoinView* v) {
   v->part_shift = j->pass_shift;
   v->part_lo = j->pass_lo;
   v->part_hi = j->pass_hi;
+  v->bloom = nullptr;
+  v->bloom_mask = 0;
   v->direct = 0;
   v->sentinel = 0;
   v->dense = 0;
@@ -703,9 +731,50 @@ static wg_status join_view_fields(wg_join* j, wgd::JoinView* v) {
   return WG_OK;
 }
 
+// The bloom over the build side's distinct keys (HashJoin.buildBloom,
+// join.go:1441): about 10 bits per key, a power-of-two count of 64-bit words,
+// at least 8; built once per build.
+static wg_status build_bloom(wg_join* j) {
+  if (j->bloom_built) return WG_OK;
+  Ctx* ctx = j->ctx;
+  const int64_t nk = j->distinct;
+  j->bloom_mask = 0;
+  if (nk > 0) {
+    int64_t slots = 1;
+    while (slots * 64 < nk * 10) slots *= 2;
+    if (slots < 8) slots = 8;
+    WG_TRY(j->bloom.ensure(ctx, slots * 8));
+    WG_CUDA_TRY(cudaMemsetAsync(j->bloom.get(), 0, (size_t)(slots * 8), ctx->stream));
+    j->bloom_mask = (uint64_t)slots - 1;
+    wgd::DCol kd{j->key.data.get(), j->key.has_valid ? j->key.valid.as<uint64_t>() : nullptr, class_of(j->key.type_id), 0};
+    bloom_build_kernel<<<grid_for(ctx, j->rows, 256), 256, 0, ctx->stream>>>(kd, j->rows, j->bloom.as<unsigned long long>(),
+                                                                           j->bloom_mask);
+    ctx->count_launch();
+    WG_CUDA_TRY(cudaGetLastError());
+  }
+  j->bloom_built = true;
+  return WG_OK;
+}
+
+// Whether the hash probe checks the bloom first: WG_JOIN_BLOOM=1 always, 0
+// never; by default when the hash index is larger than half of L2 (64 MB), so
+// a key the bloom rules out saves a random HBM read.
+static bool bloom_for_probe(const wg_join* j) {
+  const char* v = std::getenv("WG_JOIN_BLOOM");
+  if (v) return std::atoi(v) != 0;
+  const int64_t index_bytes = (int64_t)j->capacity * (j->flavor == 0 ? 8 : 16);
+  return index_bytes >= (int64_t(64) << 20);
+}
+
 wg_status join_view(wg_join* j, wgd::JoinView* v) {
   if (j->finished && !j->hashed) WG_TRY(build_hash(j));
-  return join_view_fields(j, v);
+  WG_TRY(join_view_fields(j, v));
+  if (j->finished && j->distinct > 0 && bloom_for_probe(j)) {
+    WG_TRY(build_bloom(j));
+    v->bloom = j->bloom.as<unsigned long long>();
+    v->bloom_mask = j->bloom_mask;
+  }
+  return WG_OK;
 }
 
 // The view the fused pipeline probes: the direct-payload table when one was built.
@@ -1112,6 +1181,55 @@ wg_status wg_join_gather(wg_join* j, int32_t payload_idx, const int64_t* build_r
   return WG_OK;
 }
 
+wg_status wg_join_bloom_filter(wg_join* j, const wg_batch_desc* probe, uint32_t* out_sel, int64_t* n_out) {
+  if (!j || !probe || !n_out) return fail(WG_E_INVALID, "NULL argument");
+  Ctx* ctx = j->ctx;
+  WG_TRY(ensure_device(ctx));
+  if (!j->finished) return fail(WG_E_STATE, "join build not finished");
+  if (j->grace) return fail(WG_E_UNSUPPORTED, "a partitioned build has no bloom filter");
+  if (j->probe_key_col < 0 || j->probe_key_col >= probe->ncols) return fail(WG_E_INVALID, "probe key column out of range");
+  const wg_column& kc = probe->cols[j->probe_key_col];
+  if (class_of(kc.type_id) != WG_CLS_I32 && class_of(kc.type_id) != WG_CLS_I64)
+    return fail(WG_E_UNSUPPORTED, "probe key is not an integer-class column");
+  const int64_t n = probe->sel ? probe->sel_len : probe->len;
+  *n_out = 0;
+  if (n == 0 || j->distinct == 0) return WG_OK;
+  if (!out_sel) return fail(WG_E_INVALID, "NULL argument");
+  WG_TRY(build_bloom(j));
+  wg_column only = kc;
+  wg_batch_desc one{1, 0, &only, probe->len, probe->sel, probe->sel_len};
+  WG_TRY(stage_batch(ctx, &one, &j->staged));
+  WG_TRY(j->bloom_rows.ensure(ctx, n * 4));
+  WG_TRY(j->bloom_flags.ensure(ctx, n));
+  const int64_t count_off = (n * 4 + 7) & ~int64_t(7);  // the count's 8-byte word after the rows
+  WG_TRY(j->bloom_out.ensure(ctx, count_off + 16));
+  const wgd::DCol key{j->staged.cols[0].data, j->staged.cols[0].valid_words, class_of(kc.type_id), 0};
+  bloom_probe_kernel<<<grid_for(ctx, n, 256), 256, 0, ctx->stream>>>(key, j->staged.desc.sel, n,
+                                                                      j->bloom.as<unsigned long long>(), j->bloom_mask,
+                                                                      j->bloom_rows.as<uint32_t>(),
+                                                                      j->bloom_flags.as<uint8_t>());
+  ctx->count_launch();
+  WG_CUDA_TRY(cudaGetLastError());
+  // order-preserving compaction of the kept rows
+  int64_t* d_count = (int64_t*)(j->bloom_out.as<char>() + count_off);
+  size_t tmp = 0;
+  cub::DeviceSelect::Flagged(nullptr, tmp, j->bloom_rows.as<uint32_t>(), j->bloom_flags.as<uint8_t>(),
+                             j->bloom_out.as<uint32_t>(), d_count, (int)n, ctx->stream);
+  WG_TRY(j->bloom_tmp.ensure(ctx, std::max<int64_t>((int64_t)tmp, 16)));
+  cub::DeviceSelect::Flagged(j->bloom_tmp.get(), tmp, j->bloom_rows.as<uint32_t>(), j->bloom_flags.as<uint8_t>(),
+                             j->bloom_out.as<uint32_t>(), d_count, (int)n, ctx->stream);
+  ctx->count_launch();
+  WG_CUDA_TRY(cudaGetLastError());
+  int64_t m = 0;
+  WG_TRY(read_back_i64(ctx, d_count, &m, 1));
+  if (m > 0)
+    WG_CUDA_TRY(cudaMemcpyAsync(out_sel, j->bloom_out.get(), (size_t)(m * 4), cudaMemcpyDeviceToHost, ctx->stream));
+  WG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  WG_TRY(check_device_error(ctx));
+  *n_out = m;
+  return WG_OK;
+}
+
 wg_status wg_join_reset(wg_join* j) {
   if (!j) return fail(WG_E_INVALID, "join is NULL");
   WG_TRY(ensure_device(j->ctx));
@@ -1124,6 +1242,7 @@ wg_status wg_join_reset(wg_join* j) {
   j->distinct = 0;
   j->unique = true;
   j->max_fanout = 1;
+  j->bloom_built = false;
   j->grace = false;
   j->parts.clear();
   j->passes.clear();

@@ -55,7 +55,23 @@ struct JoinView {
   int32_t part_lo, part_hi;
   long long base;
   DCol pay[WG_MAX_PAYLOAD];
+  // Bloom pre-filter of the hash probe (nullptr: none): a key the bloom rules
+  // out misses without reading the index (bloom_contains below).
+  const unsigned long long* bloom;
+  unsigned long long bloom_mask;
 };
+
+// HashJoin.buildBloom (join.go:1441) / BloomFilterOp (bloom_filter_op.go):
+// bloomHashInt (join.go:1650), and the two bits bloomSet / bloomContains
+// (bloom_filter_op.go:268) take from it in a table of 64-bit words.
+__host__ __device__ __forceinline__ unsigned long long bloom_hash_int(long long key) {
+  const unsigned long long x = (unsigned long long)key * 0x9E3779B97F4A7C15ULL;
+  return x ^ (x >> 32);
+}
+__device__ __forceinline__ bool bloom_contains(const unsigned long long* bloom, unsigned long long mask,
+                                               unsigned long long h) {
+  return ((__ldg(bloom + (h & mask)) >> (h & 63)) & 1ULL) && ((__ldg(bloom + ((h >> 17) & mask)) >> ((h >> 6) & 63)) & 1ULL);
+}
 
 // Key-hash partition of a join key (the partitioned build's, host side:
 // join_partition_of in wg_join.cu).
@@ -122,6 +138,7 @@ __device__ __forceinline__ bool join_direct_i32(const JoinView& j, int32_t key, 
 
 // Chain head of `key`, or -1 when absent (HashJoinProbe's idx.Get, join.go:2700).
 __device__ __forceinline__ int32_t join_head(const JoinView& j, int64_t key, int32_t* err) {
+  if (j.bloom != nullptr && !bloom_contains(j.bloom, j.bloom_mask, bloom_hash_int(key))) return -1;
   uint64_t h = fib_slot((uint64_t)key, j.shift);
   if (j.flavor == 0) {
     if (key < INT32_MIN || key > INT32_MAX) return -1;
