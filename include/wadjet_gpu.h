@@ -115,6 +115,17 @@ typedef struct wg_column {
   int64_t         len;
 } wg_column;
 
+/* A STRING or BYTES column (batch.BytesColumn, internal/engine/batch/vector.go:92):
+ * its wg_column.data points to this descriptor, in host memory; offsets
+ * (len + 1 entries: row i is bytes[offsets[i], offsets[i + 1])) and bytes lie in
+ * the batch's memory (host or device). On the GPU path a string column can be
+ * an aggregate's single GROUP BY key (consumeBatchStrGroup,
+ * exec/aggregate.go:3038); see wg_agg_key_strings. */
+typedef struct wg_bytes {
+  const uint32_t* offsets;
+  const uint8_t*  bytes;
+} wg_bytes;
+
 /* One record batch (batch.RecordBatch, internal/engine/batch/batch.go:9).
  * sel: NULL = all rows active, else sel_len ascending row indices (batch.go:13). */
 typedef struct wg_batch_desc {
@@ -426,6 +437,14 @@ WG_API wg_status wg_agg_emit(wg_agg* a, int64_t start, int64_t max_rows,
                       wg_column* out_cols, int64_t* n_out);
 /* Raw accumulator state of every group, for bit-exact checks. */
 WG_API wg_status wg_agg_export(wg_agg* a, const wg_group_export* out);
+/* An aggregate grouped by one STRING / BYTES column keys its groups by dense
+ * ids (its exports' and emits' key column holds the id; the NULL-key group is
+ * the NULL key as for any column): the strings of n ids, as offsets (n + 1
+ * entries, from 0) and bytes, into host buffers. *need_bytes receives the
+ * bytes the strings take; nothing is written to out_bytes when that is more
+ * than bytes_cap (call again with room). */
+WG_API wg_status wg_agg_key_strings(wg_agg* a, const int64_t* ids, int64_t n, uint32_t* out_offsets,
+                                    uint8_t* out_bytes, int64_t bytes_cap, int64_t* need_bytes);
 /* Forget all groups and input (the state after wg_agg_create). */
 WG_API wg_status wg_agg_reset(wg_agg* a);
 /* ---- exchange of partial state between ranks (one process per GPU) ----

@@ -335,3 +335,31 @@ def page_decode(chunk, rows: int, out_dtype):
         raise RuntimeError(_err())
     valid = np.unpackbits(words.view(np.uint8), bitorder="little")[:rows].astype(bool)
     return out[:rows], valid
+
+
+class StrGroupIndex:
+    """String GROUP BY keys as consumeBatchStrGroup numbers them
+    (internal/engine/exec/aggregate.go:3038-3110): each distinct string takes the
+    next group index at its first appearance, in row (selection) order across
+    batches; a NULL string is the NULL-key group. `map` returns an INT32 column of
+    group indexes and its validity, to aggregate like an int key."""
+
+    def __init__(self):
+        self.index: dict[bytes, int] = {}
+        self.strings: list[bytes] = []
+
+    def map(self, values, valid=None, sel=None):
+        n = len(values)
+        ids = np.zeros(n, np.int32)
+        rows = range(n) if sel is None else [int(r) for r in sel]
+        for r in rows:
+            if valid is not None and not valid[r]:
+                continue
+            v = values[r]
+            g = self.index.get(v)
+            if g is None:
+                g = len(self.strings)
+                self.index[v] = g
+                self.strings.append(v)
+            ids[r] = g
+        return ids, (None if valid is None else np.asarray(valid, bool))

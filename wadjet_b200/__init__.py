@@ -27,8 +27,9 @@ import numpy as np
 from . import _abi as abi
 from ._abi import (AGG_AVG, AGG_COUNT, AGG_MAX, AGG_MIN, AGG_SUM, CONST_FLOAT, CONST_INT, JOIN_ANTI, JOIN_INNER,
                    JOIN_LEFT, JOIN_SEMI, OP_EQ, OP_GE, OP_GT,
-                   OP_LE, OP_LT, OP_NE, TYPE_DATE, TYPE_DECIMAL, TYPE_DURATION, TYPE_FLOAT32, TYPE_FLOAT64,
-                   TYPE_INT32, TYPE_INT64, TYPE_IPV4, TYPE_MAC, TYPE_PORT, TYPE_PROTOCOL, TYPE_TIMESTAMP)
+                   OP_LE, OP_LT, OP_NE, TYPE_BYTES, TYPE_DATE, TYPE_DECIMAL, TYPE_DURATION, TYPE_FLOAT32, TYPE_FLOAT64,
+                   TYPE_INT32, TYPE_INT64, TYPE_IPV4, TYPE_MAC, TYPE_PORT, TYPE_PROTOCOL, TYPE_STRING,
+                   TYPE_TIMESTAMP)
 
 __all__ = [
     "Context", "Column", "Batch", "DeviceBatch", "KernelFilter", "HashJoin", "HashAggregate", "AggColumn", "Expr", "run_pipeline",
@@ -106,9 +107,46 @@ class Column:
     scale: int = 0
 
     def __len__(self) -> int:
+        if self.type_id in (TYPE_STRING, TYPE_BYTES):
+            return int(self.data[0].shape[0]) - 1
         return int(self.data.shape[0])
 
+    @classmethod
+    def strings(cls, values: Sequence, type_id: int = TYPE_STRING) -> "Column":
+        """A STRING / BYTES column (batch.BytesColumn) from str / bytes values, None = NULL:
+        data is (offsets uint32[n + 1], bytes uint8)."""
+        enc = [b"" if v is None else (v.encode() if isinstance(v, str) else bytes(v)) for v in values]
+        offs = np.zeros(len(enc) + 1, np.uint32)
+        if enc:
+            offs[1:] = np.cumsum([len(b) for b in enc], dtype=np.uint64).astype(np.uint32)
+        data = np.frombuffer(b"".join(enc), np.uint8).copy() if enc else np.zeros(0, np.uint8)
+        valid = None
+        if any(v is None for v in values):
+            valid = np.array([v is not None for v in values], bool)
+        return cls(type_id, (offs, data), valid)
+
     def _desc(self, keep: list) -> abi.wg_column:
+        if self.type_id in (TYPE_STRING, TYPE_BYTES):
+            # data = (offsets, bytes), numpy arrays or CUDA tensors; the column's
+            # data pointer is a wg_bytes descriptor in host memory
+            offs, raw = self.data
+            if _is_torch(offs):
+                desc = abi.wg_bytes(offs.data_ptr(), raw.data_ptr() if raw.numel() else offs.data_ptr())
+                vptr = self.valid.data_ptr() if self.valid is not None else None
+            else:
+                o = np.ascontiguousarray(offs, dtype=np.uint32)
+                b = np.ascontiguousarray(raw, dtype=np.uint8)
+                if b.size == 0:
+                    b = np.zeros(1, np.uint8)
+                keep += [o, b]
+                desc = abi.wg_bytes(o.ctypes.data, b.ctypes.data)
+                vptr = None
+                if self.valid is not None:
+                    w = pack_validity(self.valid) if np.asarray(self.valid).dtype == bool else np.asarray(self.valid, np.uint64)
+                    keep.append(w)
+                    vptr = w.ctypes.data
+            keep.append(desc)
+            return abi.wg_column(self.type_id, 0, C.addressof(desc), vptr, len(self))
         if _is_torch(self.data):
             ptr = self.data.data_ptr()
             vptr = self.valid.data_ptr() if self.valid is not None else None
@@ -464,8 +502,31 @@ class HashAggregate:
         _check(lib.wg_agg_export(self.h, C.byref(e)))
         return r
 
+    @property
+    def string_keyed(self) -> bool:
+        """Grouped by one STRING / BYTES column: the table keys its groups by dense ids."""
+        return bool(self._key_types) and self._key_types[0] in (TYPE_STRING, TYPE_BYTES)
+
+    def key_strings(self, ids) -> list[bytes]:
+        """The strings of dictionary ids (wg_agg_key_strings), as bytes."""
+        ids = np.ascontiguousarray(ids, dtype=np.int64)
+        n = len(ids)
+        offs = np.zeros(n + 1, np.uint32)
+        need = C.c_int64()
+        cap = 1 << 16
+        while True:
+            buf = np.zeros(max(cap, 1), np.uint8)
+            _check(lib.wg_agg_key_strings(self.h, ids.ctypes.data_as(C.POINTER(C.c_int64)), n, offs.ctypes.data,
+                                          buf.ctypes.data, cap, C.byref(need)))
+            if need.value <= cap:
+                break
+            cap = need.value
+        raw = buf.tobytes()
+        return [raw[offs[i]:offs[i + 1]] for i in range(n)]
+
     def output_types(self) -> list[int]:
         key_types = self._key_types or [TYPE_INT64] * len(self.group_by)
+        key_types = [TYPE_INT32 if t in (TYPE_STRING, TYPE_BYTES) else t for t in key_types]
         outs = []
         for i, a in enumerate(self.aggs):
             if a.out_type:
@@ -498,7 +559,16 @@ class HashAggregate:
         n = C.c_int64()
         _check(lib.wg_agg_emit(self.h, self._out_pos, m, cols, C.byref(n)))
         self._out_pos += n.value
-        return [(b[: n.value], unpack_validity(w, n.value)) for b, w in zip(bufs, words)]
+        out = [(b[: n.value], unpack_validity(w, n.value)) for b, w in zip(bufs, words)]
+        if self.string_keyed:  # ids back to their strings (None for the NULL key)
+            ids, ok = out[0]
+            strs = self.key_strings(ids[ok])
+            col = np.empty(n.value, object)
+            col[ok] = strs
+            if self._key_types[0] == TYPE_STRING:
+                col[ok] = [x.decode() for x in strs]
+            out[0] = (col, ok)
+        return out
 
     def collect(self) -> list[tuple[np.ndarray, np.ndarray]]:
         """Every finalized row (all pages of next() concatenated)."""

@@ -37,6 +37,10 @@ class wg_column(C.Structure):
                 ("valid_words", C.c_void_p), ("len", C.c_int64)]
 
 
+class wg_bytes(C.Structure):
+    _fields_ = [("offsets", C.c_void_p), ("bytes", C.c_void_p)]
+
+
 class wg_batch_desc(C.Structure):
     _fields_ = [("ncols", C.c_int32), ("_pad", C.c_int32), ("cols", C.POINTER(wg_column)),
                 ("len", C.c_int64), ("sel", C.c_void_p), ("sel_len", C.c_int64)]
@@ -156,6 +160,7 @@ SIGNATURES = {
     "wg_agg_finalize": (I32, [P, PI64]),
     "wg_agg_emit": (I32, [P, I64, I64, C.POINTER(wg_column), PI64]),
     "wg_agg_export": (I32, [P, C.POINTER(wg_group_export)]),
+    "wg_agg_key_strings": (I32, [P, PI64, I64, P, P, I64, PI64]),
     "wg_agg_reset": (I32, [P]),
     "wg_agg_kernel_shape": (I32, [P]),
     "wg_batch_upload": (I32, [P, C.POINTER(wg_batch_desc), PP]),

@@ -448,6 +448,10 @@ struct wg_agg {
   std::vector<wg::DevBuf> emit_bufs, emit_valid;
   bool emitted = false;
   int32_t last_shape = -1;         // compiled shape of the last fused launch
+  // a single STRING / BYTES key: the dictionary whose ids the table groups by
+  // (str_keyed -1 no input yet, 0 an integer key, 1 a string key)
+  wg::StrDict* sdict = nullptr;
+  int str_keyed = -1;
   // Spill (the table for the expected groups does not fit the HBM ledger): the
   // consume calls partition their rows by the key hash's top bits into runs in
   // pinned host memory; finalize aggregates one partition at a time into a
@@ -845,6 +849,7 @@ struct PipelineRun {
   bool no_partition = false;    // set on the reordered copy (hash partitioning runs once)
   bool defer_check = false;     // a launch that needs no read-back returns without waiting for it
                                 // (windowed host input checks the device error word once, at the end)
+  bool str_ids = false;         // the key column holds a string dictionary's ids
 };
 
 namespace wg {
@@ -986,10 +991,22 @@ static wg_status hc_consume(const PipelineRun& r, const wgd::Plan& P0);
 static wg_status agg_compact(wg_agg* a);
 
 // Run the fused kernel over a device-resident input with the overflow policy.
+static bool is_str_type(int32_t t) { return t == WG_TYPE_STRING || t == WG_TYPE_BYTES; }
+
 static wg_status run_device(const PipelineRun& r) {
   wg_agg* a = r.agg;
   Ctx* ctx = a->ctx;
   if (a->finalized) return fail(WG_E_STATE, "aggregate already finalized");
+  // a string key reaches the table as its dictionary's ids (the consume entry
+  // points map it first)
+  for (int kc : a->key_cols)
+    if (kc >= 0 && kc < r.in->ncols && is_str_type(r.in->cols[kc].type_id))
+      return fail(WG_E_UNSUPPORTED, a->key_cols.size() == 1
+                                        ? "a string GROUP BY key is taken by wg_agg_consume / wg_agg_consume_device"
+                                        : "a string column in a composite GROUP BY key is not on the GPU path");
+  if (a->str_keyed >= 0 && a->str_keyed != (r.str_ids ? 1 : 0))
+    return fail(WG_E_INVALID, "the GROUP BY column changed between a string and an integer type");
+  a->str_keyed = r.str_ids ? 1 : 0;
   LaunchSpec ls;
   VSchema vs;
   std::vector<int> in_map;
@@ -1243,6 +1260,13 @@ static wg_status run_device(const PipelineRun& r) {
       if (a->dom == 1) { dlo = std::min(dlo, a->dom_lo); dhi = std::max(dhi, a->dom_hi); }
       dom_ok = dhi - dlo < (int64_t(1) << 40);
     }
+  }
+  if (r.str_ids && a->L.key_words == 1 && a->dom != 2) {
+    // a string dictionary's ids are dense: [0, its distinct strings)
+    dlo = 0;
+    dhi = std::max<int64_t>(0, strdict_size(a->sdict) - 1);
+    if (a->dom == 1) { dlo = std::min(dlo, a->dom_lo); dhi = std::max(dhi, a->dom_hi); }
+    dom_ok = true;
   }
   auto note_domain = [&]() {
     if (a->L.key_words == 0) return;
@@ -2282,9 +2306,29 @@ wg_status wg_agg_create(wg_ctx* ctx, int32_t n_keys, const int32_t* key_cols, in
   return WG_OK;
 }
 
+// The batch column holding the aggregate's single string GROUP BY key, or -1.
+static int str_key_col(const wg_agg* a, const wg_batch_desc* in) {
+  if (a->key_cols.size() != 1 || in->ncols < 0 || (in->ncols > 0 && !in->cols)) return -1;
+  const int kc = a->key_cols[0];
+  return kc >= 0 && kc < in->ncols && is_str_type(in->cols[kc].type_id) ? kc : -1;
+}
+
 wg_status wg_agg_consume_device(wg_agg* a, const wg_batch_desc* in) {
   if (!a || !in) return fail(WG_E_INVALID, "NULL argument");
   WG_TRY(ensure_device(a->ctx));
+  const int sk = str_key_col(a, in);
+  if (sk >= 0) {
+    // consumeBatchStrGroup (aggregate.go:3038): the strings become dense ids,
+    // which the table groups by
+    if (a->finalized) return fail(WG_E_STATE, "aggregate already finalized");
+    std::vector<wg_column> cols(in->cols, in->cols + in->ncols);
+    WG_TRY(strdict_map(a->ctx, &a->sdict, in, sk, false, a->hint, &cols[(size_t)sk]));
+    wg_batch_desc d = *in;
+    d.cols = cols.data();
+    PipelineRun r{a, &d, 0, nullptr, nullptr, 0, nullptr};
+    r.str_ids = true;
+    return run_device(r);
+  }
   PipelineRun r{a, in, 0, nullptr, nullptr, 0, nullptr};
   return run_device(r);
 }
@@ -2292,9 +2336,13 @@ wg_status wg_agg_consume_device(wg_agg* a, const wg_batch_desc* in) {
 wg_status wg_agg_consume(wg_agg* a, const wg_batch_desc* in) {
   if (!a || !in) return fail(WG_E_INVALID, "NULL argument");
   WG_TRY(ensure_device(a->ctx));
+  const int sk = str_key_col(a, in);
+  if (sk >= 0 && a->finalized) return fail(WG_E_STATE, "aggregate already finalized");
   StagedBatch sb;
-  WG_TRY(stage_batch(a->ctx, in, &sb));
+  WG_TRY(stage_batch(a->ctx, in, &sb));  // a string column is left for the dictionary
+  if (sk >= 0) WG_TRY(strdict_map(a->ctx, &a->sdict, in, sk, true, a->hint, &sb.cols[(size_t)sk]));
   PipelineRun r{a, &sb.desc, 0, nullptr, nullptr, 0, nullptr};
+  r.str_ids = sk >= 0;
   WG_TRY(run_device(r));
   WG_CUDA_TRY(cudaStreamSynchronize(a->ctx->stream));
   return WG_OK;
@@ -2310,6 +2358,8 @@ wg_status wg_agg_merge(wg_agg* d, wg_agg* s) {
   if (!d || !s) return fail(WG_E_INVALID, "NULL argument");
   if (d->ctx != s->ctx) return fail(WG_E_INVALID, "aggregates belong to different contexts");
   if (d->key_cols != s->key_cols || d->specs.size() != s->specs.size()) return fail(WG_E_INVALID, "aggregate shapes differ");
+  // two dictionaries number their strings independently
+  if (d->str_keyed == 1 || s->str_keyed == 1) return fail(WG_E_UNSUPPORTED, "string-keyed aggregates are not merged");
   // a destination that parks its input in runs (spill, two-level mode) takes no
   // merges; a source of either kind merges once finalized (its compact result)
   if (d->spill || d->hc) return fail(WG_E_UNSUPPORTED, "a spilled or two-level aggregation takes no merges");
@@ -2507,6 +2557,10 @@ wg_status wg_agg_reset(wg_agg* a) {
   WG_TRY(ensure_device(a->ctx));
   a->finalized = false;
   a->n_out = 0;
+  if (a->sdict) {
+    cudaStreamSynchronize(a->ctx->stream);
+    strdict_reset(a->sdict);  // the schema (and str_keyed) stays resolved
+  }
   if (!a->resolved) return WG_OK;
   Ctx* ctx = a->ctx;
   if (a->spill) {
@@ -2575,6 +2629,7 @@ wg_status wg_agg_state_layout(wg_agg* a, wg_state_layout* out) {
 wg_status wg_agg_partition_state(wg_agg* a, int32_t n_parts, void* rows_dev, int64_t rows_cap, int64_t* part_rows) {
   if (!a || !part_rows || n_parts < 1 || n_parts > 4096) return fail(WG_E_INVALID, "bad partition arguments");
   if (!a->finalized) return fail(WG_E_STATE, "aggregate not finalized");
+  if (a->str_keyed == 1) return fail(WG_E_UNSUPPORTED, "string-keyed aggregates are not exchanged");
   Ctx* ctx = a->ctx;
   WG_TRY(ensure_device(ctx));
   for (int p = 0; p < n_parts; ++p) part_rows[p] = 0;
@@ -2609,6 +2664,7 @@ wg_status wg_agg_merge_state(wg_agg* a, const wg_state_layout* src, const void* 
   if (!a || !src || n_rows < 0 || (n_rows > 0 && !rows_dev)) return fail(WG_E_INVALID, "NULL argument");
   if (a->finalized) return fail(WG_E_STATE, "aggregate already finalized");
   if (a->spill) return fail(WG_E_UNSUPPORTED, "spilled aggregations are not merged");
+  if (a->str_keyed == 1) return fail(WG_E_UNSUPPORTED, "string-keyed aggregates are not merged");
   if (src->n_keys != (int32_t)a->key_cols.size() || src->n_aggs != (int32_t)a->specs.size() ||
       src->n_aggs > WG_MAX_AGGS || src->n_keys > WG_MAX_KEYS || src->slot_words > WG_MAX_SLOT_WORDS)
     return fail(WG_E_INVALID, "state layout does not match the aggregate's shape");
@@ -2693,8 +2749,18 @@ wg_status wg_agg_destroy(wg_agg* a) {
   if (!a) return WG_OK;
   ensure_device(a->ctx);
   cudaStreamSynchronize(a->ctx->stream);
+  strdict_free(a->sdict);
   delete a;
   return WG_OK;
+}
+
+wg_status wg_agg_key_strings(wg_agg* a, const int64_t* ids, int64_t n, uint32_t* out_offsets, uint8_t* out_bytes,
+                             int64_t bytes_cap, int64_t* need_bytes) {
+  if (!a || n < 0 || (n > 0 && !ids) || !out_offsets || !need_bytes || bytes_cap < 0 || (bytes_cap > 0 && !out_bytes))
+    return fail(WG_E_INVALID, "bad key-string arguments");
+  if (a->str_keyed != 1) return fail(WG_E_STATE, "the aggregate is not grouped by a string column");
+  WG_TRY(ensure_device(a->ctx));
+  return strdict_strings(a->ctx, a->sdict, ids, n, out_offsets, out_bytes, bytes_cap, need_bytes);
 }
 
 }  // extern "C"

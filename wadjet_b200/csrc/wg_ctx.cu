@@ -165,6 +165,7 @@ wg_status check_device_error(Ctx* ctx) {
     case WG_DERR_NULL_PACKED: return fail(WG_E_UNSUPPORTED, "NULL in a composite GROUP BY key");
     case WG_DERR_STACK: return fail(WG_E_INVALID, "malformed expression program");
     case WG_DERR_BAD_PAGE: return fail(WG_E_INVALID, "malformed Parquet page");
+    case WG_DERR_HASH_COLLISION: return fail(WG_E_UNSUPPORTED, "two GROUP BY strings share a 128-bit hash");
     default: return fail(WG_E_CUDA, "device error " + std::to_string(h));
   }
 }

@@ -21,6 +21,7 @@
 #define WG_DERR_NULL_PACKED 3   // NULL in a composite (packed) group key
 #define WG_DERR_STACK       4   // malformed expression program
 #define WG_DERR_BAD_PAGE    5   // a Parquet page whose levels, indices or values are malformed
+#define WG_DERR_HASH_COLLISION 6  // two different strings with one 128-bit dictionary hash
 
 #define WG_FULL_MASK 0xFFFFFFFFu
 

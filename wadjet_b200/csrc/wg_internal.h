@@ -158,6 +158,18 @@ struct StagedBatch {
 };
 wg_status stage_batch(Ctx* ctx, const wg_batch_desc* in, StagedBatch* out);
 
+// String GROUP BY keys (wg_strkey.cu): a device dictionary from each distinct
+// string to a dense id. strdict_map maps column `col` of `in` (its string
+// column in host memory when `host`, else on the device) and sets *out to an
+// INT32 column of the ids on the device, with the string column's validity.
+struct StrDict;
+wg_status strdict_map(Ctx* ctx, StrDict** d, const wg_batch_desc* in, int col, bool host, int64_t hint, wg_column* out);
+wg_status strdict_strings(Ctx* ctx, StrDict* d, const int64_t* ids, int64_t n, uint32_t* out_offsets,
+                          uint8_t* out_bytes, int64_t bytes_cap, int64_t* need_bytes);
+void strdict_reset(StrDict* d);
+void strdict_free(StrDict* d);
+int64_t strdict_size(const StrDict* d);
+
 }  // namespace wg
 
 // Opaque handle bodies live in their .cu files; only the context is shared.

@@ -1,0 +1,426 @@
+// wg_strkey.cu — string GROUP BY keys: a device dictionary from each distinct
+// string to a dense group id.
+//
+// The reference groups one STRING / BYTES column through strHashTable
+// (consumeBatchStrGroup, exec/aggregate.go:3038): a string's bytes are the
+// key, a NULL string has its own group. Here a consume call first maps every
+// row's string to a dense int32 id in a dictionary that lives with the
+// aggregate, then aggregates over the ids like any int key (the NULL rows keep
+// the string column's validity, so they form the NULL-key group); an export
+// or emit reports ids, and wg_agg_key_strings turns ids back into strings.
+//
+// The dictionary is an open-addressing table of 128-bit key hashes (two
+// independent 64-bit hashes of the bytes and the length) installed with one
+// 16-byte compare-and-swap, plus an arena holding each distinct string once.
+// Per batch: (1) every row finds or installs its hash's slot; (2) the rows of
+// slots installed in this batch elect the lowest row; (3) that row takes the
+// next id and copies its bytes into the arena; (4) every row compares its
+// bytes with its slot's stored string and takes the id. A 128-bit collision
+// between two different strings would make (4) fail, which the call reports
+// instead of merging the groups. No step waits on another thread.
+#include "wg_internal.h"
+#include "wg_device.cuh"
+
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+namespace {
+
+using namespace wgd;
+
+constexpr unsigned long long kEmpty = ~0ULL;
+constexpr uint32_t kNoRep = 0xFFFFFFFFu;
+constexpr unsigned long long kNoId = ~0ULL;  // a slot whose string has no id yet
+constexpr int kLenShift = 40;  // slot / id location: arena offset | length << 40
+
+struct StrSrc {
+  const uint32_t* offs;
+  const uint8_t* bytes;
+  const uint64_t* valid;  // the column's validity words (nullptr: no NULLs)
+  const uint32_t* sel;    // selection entries (nullptr: rows 0 .. n - 1)
+  int64_t n;              // items
+};
+
+__device__ __forceinline__ int64_t item_row(const StrSrc& s, int64_t i) { return s.sel ? (int64_t)s.sel[i] : i; }
+
+__device__ __forceinline__ bool row_null(const StrSrc& s, int64_t row) {
+  return s.valid != nullptr && ((s.valid[row >> 6] >> (row & 63)) & 1ULL) == 0;
+}
+
+// Two independent 64-bit hashes of a string: FNV-1a over the bytes, and a
+// multiply-xorshift mix over the bytes; both fold in the length. Neither word
+// is ~0, so {~0, ~0} stays the empty slot.
+__device__ __forceinline__ U128 str_hash(const uint8_t* p, uint32_t n) {
+  unsigned long long a = 0xcbf29ce484222325ULL, b = 0x9E3779B97F4A7C15ULL ^ (unsigned long long)n;
+  for (uint32_t i = 0; i < n; ++i) {
+    const unsigned long long c = p[i];
+    a = (a ^ c) * 0x100000001b3ULL;
+    b = (b ^ c) * 0xff51afd7ed558ccdULL;
+    b ^= b >> 29;
+  }
+  a ^= (unsigned long long)n * 0xc4ceb9fe1a85ec53ULL;
+  U128 h;
+  h.lo = a == kEmpty ? kEmpty - 1 : a;
+  h.hi = b == kEmpty ? kEmpty - 1 : b;
+  return h;
+}
+
+// (1) Find or install each non-NULL item's hash: rowslot[i] = its slot, -1 for
+// a NULL string. ctr[0] counts the slots in use; once it passes `limit` (3/4
+// of the table) ctr[1] is raised and the items still probing stop (rowslot
+// -2), so the host grows the table and runs the pass again; a walk over the
+// whole table raises it too.
+__global__ void str_insert_kernel(StrSrc s, unsigned long long* slots, uint64_t mask, int32_t* rowslot,
+                                  unsigned long long* ctr, unsigned long long limit) {
+  volatile unsigned long long* full = ctr + 1;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < s.n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t row = item_row(s, i);
+    if (row_null(s, row)) { rowslot[i] = -1; continue; }
+    if (*full != 0) { rowslot[i] = -2; continue; }
+    const uint32_t b0 = s.offs[row], b1 = s.offs[row + 1];
+    const U128 k = str_hash(s.bytes + b0, b1 - b0);
+    uint64_t idx = k.lo & mask;
+    int32_t found = -2;
+    for (uint64_t probe = 0; probe <= mask && *full == 0; ++probe) {
+      unsigned long long* sl = slots + idx * 4;
+      const U128 cur = read128(sl);
+      if (cur.lo == k.lo && cur.hi == k.hi) { found = (int32_t)idx; break; }
+      if (cur.lo == kEmpty || cur.hi == kEmpty) {  // empty, or a key being installed
+        U128 e; e.lo = kEmpty; e.hi = kEmpty;
+        const U128 old = cas128((U128*)sl, e, k);
+        if (old.lo == e.lo && old.hi == e.hi) {
+          if (atomicAdd(ctr, 1ULL) + 1 > limit) *full = 1;
+          found = (int32_t)idx;
+          break;
+        }
+        if (old.lo == k.lo && old.hi == k.hi) { found = (int32_t)idx; break; }
+      }
+      idx = (idx + 1) & mask;
+    }
+    if (found == -2 && *full == 0) *full = 1;  // walked the whole table
+    rowslot[i] = found;
+  }
+}
+
+// (2) The lowest item of each slot that has no id yet.
+__global__ void str_elect_kernel(int64_t n, const unsigned long long* slots, const int32_t* rowslot, uint32_t* rep) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t sl = rowslot[i];
+    if (sl < 0) continue;
+    if (slots[(int64_t)sl * 4 + 2] == kNoId) atomicMin(rep + sl, (uint32_t)i);
+  }
+}
+
+// (3a) Each elected item's (1 id, its length) packed as 1 << 32 | length, so one
+// exclusive scan gives both its id and its arena offset in item order (a
+// batch's bytes stay below 2^32: its offsets are 32-bit).
+__global__ void str_flag_kernel(StrSrc s, const int32_t* rowslot, const uint32_t* rep, unsigned long long* pack) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < s.n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t sl = rowslot[i];
+    unsigned long long v = 0;
+    if (sl >= 0 && rep[sl] == (uint32_t)i) {
+      const int64_t row = item_row(s, i);
+      v = (1ULL << 32) | (unsigned long long)(s.offs[row + 1] - s.offs[row]);
+    }
+    pack[i] = v;
+  }
+}
+
+// (3b) The elected item takes its id (first appearance order, as the
+// reference's group indexes) and stores its string.
+__global__ void str_assign_kernel(StrSrc s, unsigned long long* slots, const int32_t* rowslot, uint32_t* rep,
+                                  const unsigned long long* pre, unsigned long long id0, unsigned long long off0,
+                                  uint8_t* arena, unsigned long long* id_loc) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < s.n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t sl = rowslot[i];
+    if (sl < 0 || rep[sl] != (uint32_t)i) continue;
+    const int64_t row = item_row(s, i);
+    const uint32_t b0 = s.offs[row], len = s.offs[row + 1] - b0;
+    const unsigned long long id = id0 + (pre[i] >> 32);
+    const unsigned long long off = off0 + (pre[i] & 0xFFFFFFFFULL);
+    for (uint32_t k = 0; k < len; ++k) arena[off + k] = s.bytes[b0 + k];
+    const unsigned long long loc = off | ((unsigned long long)len << kLenShift);
+    id_loc[id] = loc;
+    slots[(int64_t)sl * 4 + 3] = loc;
+    slots[(int64_t)sl * 4 + 2] = id;
+    rep[sl] = kNoRep;
+  }
+}
+
+// (4) Every item checks its bytes against its slot's string and takes the id
+// (ids are indexed by row; rows outside the selection are not written).
+__global__ void str_gid_kernel(StrSrc s, const unsigned long long* slots, const int32_t* rowslot, const uint8_t* arena,
+                               int32_t* gid, int32_t* err) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < s.n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t row = item_row(s, i);
+    const int32_t sl = rowslot[i];
+    if (sl < 0) { gid[row] = 0; continue; }
+    const unsigned long long loc = slots[(int64_t)sl * 4 + 3];
+    const unsigned long long off = loc & ((1ULL << kLenShift) - 1);
+    const uint32_t len = (uint32_t)(loc >> kLenShift);
+    const uint32_t b0 = s.offs[row], n = s.offs[row + 1] - b0;
+    bool same = n == len;
+    for (uint32_t k = 0; same && k < n; ++k) same = s.bytes[b0 + k] == arena[off + k];
+    if (!same) set_error(err, WG_DERR_HASH_COLLISION);
+    gid[row] = (int32_t)slots[(int64_t)sl * 4 + 2];
+  }
+}
+
+// The dictionary's slots moved into a larger table.
+__global__ void str_rehash_kernel(const unsigned long long* old, uint64_t old_cap, unsigned long long* slots,
+                                  uint64_t mask) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < old_cap; i += (uint64_t)gridDim.x * blockDim.x) {
+    const unsigned long long* o = old + i * 4;
+    if (o[0] == kEmpty && o[1] == kEmpty) continue;
+    U128 k; k.lo = o[0]; k.hi = o[1];
+    uint64_t idx = k.lo & mask;
+    for (uint64_t probe = 0; probe <= mask; ++probe) {
+      unsigned long long* sl = slots + idx * 4;
+      U128 e; e.lo = kEmpty; e.hi = kEmpty;
+      const U128 prev = cas128((U128*)sl, e, k);
+      if (prev.lo == e.lo && prev.hi == e.hi) {
+        sl[2] = o[2];
+        sl[3] = o[3];
+        break;
+      }
+      idx = (idx + 1) & mask;
+    }
+  }
+}
+
+__global__ void str_init_slots_kernel(unsigned long long* slots, uint64_t cap) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cap; i += (uint64_t)gridDim.x * blockDim.x) {
+    slots[i * 4] = kEmpty;
+    slots[i * 4 + 1] = kEmpty;
+    slots[i * 4 + 2] = kNoId;
+    slots[i * 4 + 3] = 0;
+  }
+}
+
+// ctr[0] = the slots in use, ctr[1] = 0 (not full)
+__global__ void str_ctr_kernel(unsigned long long* ctr, unsigned long long used) {
+  ctr[0] = used;
+  ctr[1] = 0;
+}
+
+// ctr[2] = the scan's total: new ids << 32 | their bytes
+__global__ void str_total_kernel(const unsigned long long* pre, const unsigned long long* pack, int64_t n,
+                                 unsigned long long* ctr) {
+  ctr[2] = pre[n - 1] + pack[n - 1];
+}
+
+}  // namespace
+
+namespace wg {
+
+struct StrDict {
+  DevBuf slots, rep, ctr, arena, id_loc;
+  uint64_t cap = 0;                 // table slots (a power of two)
+  int64_t n_ids = 0, used = 0;      // distinct strings and arena bytes
+  int64_t slots_used = 0;           // installed hashes (n_ids after every complete batch)
+  DevBuf rowslot, pack, pre, scan_tmp, gid;           // per-batch scratch
+  DevBuf h_offs, h_bytes, h_valid, h_sel;             // a host batch's string column on the device
+  std::vector<unsigned long long> loc_host;           // host copies for wg_agg_key_strings,
+  std::vector<uint8_t> arena_host;                    // valid while no batch came since
+  bool host_fresh = false;
+};
+
+namespace {
+
+unsigned str_grid(Ctx* ctx, int64_t n, int block) {
+  const int64_t want = (n + block - 1) / block;
+  return (unsigned)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)ctx->sm_count * 16));
+}
+
+// Grow a device buffer to `need` bytes, keeping its first `keep` bytes.
+wg_status grow_keep(Ctx* ctx, DevBuf& b, int64_t keep, int64_t need) {
+  if (b.bytes() >= need) return WG_OK;
+  DevBuf nb;
+  WG_TRY(nb.alloc(ctx, std::max<int64_t>(need, b.bytes() * 2)));
+  if (keep > 0) WG_CUDA_TRY(cudaMemcpyAsync(nb.get(), b.get(), (size_t)keep, cudaMemcpyDeviceToDevice, ctx->stream));
+  b = std::move(nb);  // the old buffer's cudaFree waits for the copy
+  return WG_OK;
+}
+
+// A table of `cap` slots holding the old table's strings.
+wg_status str_table(Ctx* ctx, StrDict* d, uint64_t cap) {
+  DevBuf ns, nr;
+  WG_TRY(ns.alloc(ctx, (int64_t)cap * 32));
+  WG_TRY(nr.alloc(ctx, (int64_t)cap * 4));
+  str_init_slots_kernel<<<str_grid(ctx, (int64_t)cap, 256), 256, 0, ctx->stream>>>(ns.as<unsigned long long>(), cap);
+  ctx->count_launch();
+  WG_CUDA_TRY(cudaMemsetAsync(nr.get(), 0xFF, (size_t)cap * 4, ctx->stream));
+  if (d->cap > 0) {
+    str_rehash_kernel<<<str_grid(ctx, (int64_t)d->cap, 256), 256, 0, ctx->stream>>>(
+        d->slots.as<unsigned long long>(), d->cap, ns.as<unsigned long long>(), cap - 1);
+    ctx->count_launch();
+  }
+  WG_CUDA_TRY(cudaGetLastError());
+  d->slots = std::move(ns);
+  d->rep = std::move(nr);
+  d->cap = cap;
+  return WG_OK;
+}
+
+uint64_t pow2_at_least(uint64_t v) {
+  uint64_t c = 1024;
+  while (c < v) c <<= 1;
+  return c;
+}
+
+}  // namespace
+
+void strdict_free(StrDict* d) { delete d; }
+
+void strdict_reset(StrDict* d) {
+  if (!d) return;
+  d->slots.reset(); d->rep.reset(); d->arena.reset(); d->id_loc.reset();
+  d->rowslot.reset(); d->pack.reset(); d->pre.reset(); d->scan_tmp.reset(); d->gid.reset();
+  d->h_offs.reset(); d->h_bytes.reset(); d->h_valid.reset(); d->h_sel.reset();
+  d->cap = 0; d->n_ids = 0; d->used = 0; d->slots_used = 0;
+  d->loc_host.clear(); d->arena_host.clear(); d->host_fresh = false;
+}
+
+int64_t strdict_size(const StrDict* d) { return d ? d->n_ids : 0; }
+
+
+wg_status strdict_map(Ctx* ctx, StrDict** dp, const wg_batch_desc* in, int col, bool host, int64_t hint,
+                      wg_column* out) {
+  const wg_column& c = in->cols[col];
+  const wg_bytes* sb = static_cast<const wg_bytes*>(c.data);
+  const int64_t len = in->len;
+  if (!sb || (len > 0 && (!sb->offsets || !sb->bytes))) return fail(WG_E_INVALID, "string column without offsets or bytes");
+  if (len >= (int64_t)INT32_MAX) return fail(WG_E_UNSUPPORTED, "a string-keyed batch holds fewer than 2^31 rows");
+  if (in->sel && in->sel_len > len) return fail(WG_E_INVALID, "selection longer than the batch");
+  if (!*dp) *dp = new StrDict();
+  StrDict* d = *dp;
+  d->host_fresh = false;
+  const int64_t n = in->sel ? in->sel_len : len;
+  StrSrc s{sb->offsets, sb->bytes, c.valid_words, in->sel, n};
+  if (host) {
+    // the string column (and the selection) on the device; the other columns
+    // are staged by the caller
+    const int64_t total = len > 0 ? (int64_t)sb->offsets[len] : 0;
+    WG_TRY(d->h_offs.ensure(ctx, std::max<int64_t>((len + 1) * 4, 16)));
+    WG_TRY(d->h_bytes.ensure(ctx, std::max<int64_t>(total, 16)));
+    if (len > 0)
+      WG_CUDA_TRY(cudaMemcpyAsync(d->h_offs.get(), sb->offsets, (size_t)(len + 1) * 4, cudaMemcpyHostToDevice, ctx->stream));
+    if (total > 0)
+      WG_CUDA_TRY(cudaMemcpyAsync(d->h_bytes.get(), sb->bytes, (size_t)total, cudaMemcpyHostToDevice, ctx->stream));
+    s.offs = d->h_offs.as<uint32_t>();
+    s.bytes = d->h_bytes.as<uint8_t>();
+    if (c.valid_words) {
+      const int64_t words = (len + 63) / 64;
+      WG_TRY(d->h_valid.ensure(ctx, std::max<int64_t>(words * 8, 16)));
+      if (words > 0)
+        WG_CUDA_TRY(cudaMemcpyAsync(d->h_valid.get(), c.valid_words, (size_t)words * 8, cudaMemcpyHostToDevice, ctx->stream));
+      s.valid = d->h_valid.as<uint64_t>();
+    }
+    if (in->sel) {
+      WG_TRY(d->h_sel.ensure(ctx, std::max<int64_t>(n * 4, 16)));
+      if (n > 0) WG_CUDA_TRY(cudaMemcpyAsync(d->h_sel.get(), in->sel, (size_t)n * 4, cudaMemcpyHostToDevice, ctx->stream));
+      s.sel = d->h_sel.as<uint32_t>();
+    }
+  }
+  WG_TRY(d->gid.ensure(ctx, std::max<int64_t>(len * 4, 16)));
+  *out = wg_column{WG_TYPE_INT32, 0, d->gid.get(), s.valid, len};
+  if (n == 0) return WG_OK;
+
+  // (1) install the hashes, growing the table whenever it passes 3/4 full
+  const uint64_t want = pow2_at_least(2 * (uint64_t)(d->slots_used + std::min<int64_t>(n, std::max<int64_t>(hint, 1 << 16))));
+  if (d->cap < want) WG_TRY(str_table(ctx, d, want));
+  WG_TRY(d->rowslot.ensure(ctx, n * 4));
+  WG_TRY(d->ctr.ensure(ctx, 64));
+  unsigned long long* ctr = d->ctr.as<unsigned long long>();
+  const unsigned grid = str_grid(ctx, n, 256);
+  int64_t cv[4] = {0, 0, 0, 0};
+  for (int pass = 0;; ++pass) {
+    str_ctr_kernel<<<1, 1, 0, ctx->stream>>>(ctr, (unsigned long long)d->slots_used);
+    str_insert_kernel<<<grid, 256, 0, ctx->stream>>>(s, d->slots.as<unsigned long long>(), d->cap - 1,
+                                                     d->rowslot.as<int32_t>(), ctr, d->cap / 4 * 3);
+    ctx->count_launch(2);
+    WG_CUDA_TRY(cudaGetLastError());
+    WG_TRY(read_back_i64(ctx, reinterpret_cast<int64_t*>(ctr), cv, 2));
+    if (cv[1] == 0) break;
+    if (pass >= 24 || d->cap >= (1ULL << 31)) return fail(WG_E_NOMEM, "string dictionary table cannot grow");
+    d->slots_used = cv[0];  // the installs of the stopped pass stay in the table
+    WG_TRY(str_table(ctx, d, std::max<uint64_t>(d->cap * 4, pow2_at_least(2 * (uint64_t)cv[0]))));
+  }
+  d->slots_used = cv[0];
+
+  // (2)-(3) ids and arena offsets of the strings new in this batch, in item order
+  WG_TRY(d->pack.ensure(ctx, n * 8));
+  WG_TRY(d->pre.ensure(ctx, n * 8));
+  size_t tmp = 0;
+  WG_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tmp, d->pack.as<unsigned long long>(),
+                                            d->pre.as<unsigned long long>(), (int)n, ctx->stream));
+  WG_TRY(d->scan_tmp.ensure(ctx, std::max<int64_t>((int64_t)tmp, 16)));
+  str_elect_kernel<<<grid, 256, 0, ctx->stream>>>(n, d->slots.as<unsigned long long>(), d->rowslot.as<int32_t>(),
+                                                  d->rep.as<uint32_t>());
+  str_flag_kernel<<<grid, 256, 0, ctx->stream>>>(s, d->rowslot.as<int32_t>(), d->rep.as<uint32_t>(),
+                                                 d->pack.as<unsigned long long>());
+  ctx->count_launch(2);
+  WG_CUDA_TRY(cub::DeviceScan::ExclusiveSum(d->scan_tmp.get(), tmp, d->pack.as<unsigned long long>(),
+                                            d->pre.as<unsigned long long>(), (int)n, ctx->stream));
+  str_total_kernel<<<1, 1, 0, ctx->stream>>>(d->pre.as<unsigned long long>(), d->pack.as<unsigned long long>(), n, ctr);
+  ctx->count_launch(2);
+  WG_CUDA_TRY(cudaGetLastError());
+  WG_TRY(read_back_i64(ctx, reinterpret_cast<int64_t*>(ctr), cv, 3));
+  const int64_t new_ids = (int64_t)((unsigned long long)cv[2] >> 32);
+  const int64_t new_bytes = (int64_t)((unsigned long long)cv[2] & 0xFFFFFFFFULL);
+  if (d->n_ids + new_ids >= (int64_t)INT32_MAX) return fail(WG_E_UNSUPPORTED, "more than 2^31 - 1 distinct strings");
+  WG_TRY(grow_keep(ctx, d->arena, d->used, std::max<int64_t>(d->used + new_bytes, 16)));
+  WG_TRY(grow_keep(ctx, d->id_loc, d->n_ids * 8, std::max<int64_t>((d->n_ids + new_ids) * 8, 16)));
+  str_assign_kernel<<<grid, 256, 0, ctx->stream>>>(s, d->slots.as<unsigned long long>(), d->rowslot.as<int32_t>(),
+                                                   d->rep.as<uint32_t>(), d->pre.as<unsigned long long>(),
+                                                   (unsigned long long)d->n_ids, (unsigned long long)d->used,
+                                                   d->arena.as<uint8_t>(), d->id_loc.as<unsigned long long>());
+  // (4) every item's id, its bytes checked against the stored string
+  str_gid_kernel<<<grid, 256, 0, ctx->stream>>>(s, d->slots.as<unsigned long long>(), d->rowslot.as<int32_t>(),
+                                                d->arena.as<uint8_t>(), d->gid.as<int32_t>(), ctx->dev_error);
+  ctx->count_launch(2);
+  WG_CUDA_TRY(cudaGetLastError());
+  d->n_ids += new_ids;
+  d->used += new_bytes;
+  return check_device_error(ctx);
+}
+
+wg_status strdict_strings(Ctx* ctx, StrDict* d, const int64_t* ids, int64_t n, uint32_t* out_offsets,
+                          uint8_t* out_bytes, int64_t bytes_cap, int64_t* need_bytes) {
+  const int64_t n_ids = d ? d->n_ids : 0;
+  if (d && !d->host_fresh) {
+    d->loc_host.resize((size_t)n_ids);
+    d->arena_host.resize((size_t)d->used);
+    if (n_ids > 0)
+      WG_CUDA_TRY(cudaMemcpyAsync(d->loc_host.data(), d->id_loc.get(), (size_t)n_ids * 8, cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+    if (d->used > 0)
+      WG_CUDA_TRY(cudaMemcpyAsync(d->arena_host.data(), d->arena.get(), (size_t)d->used, cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+    WG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    d->host_fresh = true;
+  }
+  int64_t total = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    if (ids[i] < 0 || ids[i] >= n_ids) return fail(WG_E_INVALID, "string id out of range");
+    total += (int64_t)(d->loc_host[(size_t)ids[i]] >> kLenShift);
+  }
+  if (total > (int64_t)UINT32_MAX) return fail(WG_E_UNSUPPORTED, "strings longer than 32-bit offsets reach");
+  *need_bytes = total;
+  if (total > bytes_cap) return WG_OK;
+  int64_t pos = 0;
+  out_offsets[0] = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    const unsigned long long loc = d->loc_host[(size_t)ids[i]];
+    const int64_t len = (int64_t)(loc >> kLenShift), off = (int64_t)(loc & ((1ULL << kLenShift) - 1));
+    if (len > 0) std::memcpy(out_bytes + pos, d->arena_host.data() + off, (size_t)len);
+    pos += len;
+    out_offsets[i + 1] = (uint32_t)pos;
+  }
+  return WG_OK;
+}
+
+}  // namespace wg
