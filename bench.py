@@ -27,6 +27,7 @@ by owner rank on the device and exchanged with an NCCL all-to-all
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -65,7 +66,7 @@ def parse_args():
                    help="fact rows per reference (CPU) step; the default is the whole workload")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--workload", choices=["starjoin", "groupby", "highcard", "highcard_spill", "batched", "serving",
-                                          "filter"],
+                                          "filter", "strgroup"],
                    default="starjoin", help="starjoin is the headline; the others print their own lines")
     p.add_argument("--queries", type=int, default=512, help="batched: queries per batch")
     p.add_argument("--qps", type=float, default=2000.0, help="serving: Poisson arrival rate")
@@ -451,7 +452,22 @@ def run_groupby(args):
             wg.run_pipeline(ctx, batch, agg, filters=[(3, wg.OP_LT, 7)], device=True)
             assert agg.finalize() == 4096
 
-        ms = _timed_ms(stream, step, args.steps, args.warmup)
+        py_ms = _timed_ms(stream, step, args.steps, args.warmup)
+        # the same query through the C ABI with its descriptors built once, as a
+        # cgo caller holds them: reset, the fused pipeline, finalize
+        d, keep = batch.desc()
+        preds = (wg.abi.wg_predicate * 1)(wg.predicate(3, wg.OP_LT, 7))
+        ex = (wg.abi.wg_expr * 1)()
+        pdesc = wg.abi.wg_pipeline_desc(ctypes.pointer(d), 1, 0, preds, None, ex, agg.h)
+        ng = ctypes.c_int64()
+
+        def c_step():
+            wg._check(wg.lib.wg_agg_reset(agg.h))
+            wg._check(wg.lib.wg_pipeline_run_device(ctx.h, ctypes.byref(pdesc)))
+            wg._check(wg.lib.wg_agg_finalize(agg.h, ctypes.byref(ng)))
+
+        ms = _timed_ms(stream, c_step, args.steps, args.warmup)
+        assert ng.value == 4096, ng.value
         alg = n * 28 + 4096 * 40
         threads = os.cpu_count() or 1
         sample = min(n, 1 << 24)
@@ -459,7 +475,8 @@ def run_groupby(args):
             "value": cpu_groupby_sample(sample, threads), "unit": "rows/s", "cores": threads, "kind": "port",
             "sample": f"{sample} rows of the same workload, oracle Pipeline.Run, one worker per host thread"}
         print(json.dumps({"workload": "groupby", "metric": "rows/s", "rows": n, "value": n / (ms / 1e3),
-                          "unit": "rows/s", "ms_per_step": ms, "hbm_gbs": alg / (ms / 1e3) / 1e9,
+                          "unit": "rows/s", "ms_per_step": ms, "python_api_ms_per_step": py_ms,
+                          "hbm_gbs": alg / (ms / 1e3) / 1e9,
                           "frac_of_peak": alg / (ms / 1e3) / 1e9 / peak, "peak_kind": peak_kind_note(kind),
                           "algorithmic_bytes": alg, "clocks": _LAST_CLOCKS[0], "cpu_baseline": cpu}), flush=True)
         agg.close()
@@ -515,6 +532,78 @@ def run_filter(args):
                       "peak_kind": peak_kind_note(kind), "algorithmic_bytes": alg, "clocks": _LAST_CLOCKS[0],
                       "cpu_baseline": cpu}), flush=True)
     f.close()
+    ctx.close()
+
+
+def cpu_strgroup_sample(offs, raw, v) -> float:
+    """rows/s of the oracle's string GROUP BY (or_strindex_map numbering the strings as
+    consumeBatchStrGroup does, then the oracle aggregate over the ids) on one host thread."""
+    from oracle import binding as ob
+    n = len(v)
+    t0 = time.perf_counter()
+    idx = ob.StrGroupIndex()
+    agg = ob.Agg([0], [(1, -1, 0), (0, 1, 0)])
+    for r0 in range(0, n, 2048):  # batch.DefaultBatchSize rows per Consume
+        r1 = min(n, r0 + 2048)
+        o = offs[r0:r1 + 1]
+        ids = idx.map_arrays(o - o[0], raw[o[0]:o[-1]])
+        agg.consume(ob.HostBatch([(1, ids, None, 0), (2, v[r0:r1], None, 0)]))
+    return n / (time.perf_counter() - t0)
+
+
+def run_strgroup(args):
+    """SELECT s, COUNT(*), SUM(v) FROM t GROUP BY s: a BYTES column of 2^26 rows over 2^20 distinct
+    URL-like strings of 8-56 bytes (consumeBatchStrGroup's path)."""
+    import numpy as np
+    import torch
+    import wadjet_b200 as wg
+    from wadjet_b200 import synth
+    ctx = wg.Context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    n = args.rows if args.rows != FACT_ROWS else 1 << 26
+    distinct = 1 << 20
+    offs, raw, v = synth.strgroup(n, distinct)
+    agg = wg.HashAggregate(ctx, [0], [wg.AggColumn(wg.AGG_COUNT, -1), wg.AggColumn(wg.AGG_SUM, 1)])
+    batch = wg.Batch([wg.Column(wg.TYPE_BYTES, (offs, raw)), wg.Column(wg.TYPE_INT64, v)])
+    got = [0]
+
+    def step():
+        agg.reset()
+        agg.consume(batch, device=True)
+        got[0] = agg.finalize()
+
+    l0 = ctx.launches
+    ms = _timed_ms(stream, step, args.steps, args.warmup)
+    launches = (ctx.launches - l0) // max(1, args.steps + args.warmup)
+    clocks = _LAST_CLOCKS[0]
+    assert got[0] == distinct, got[0]
+    total = int(raw.numel())
+    alg = 4 * (n + 1) + total + 8 * n
+    peak, kind = measured_peak_hbm()
+    # end to end: the same query from host buffers (wg_agg_consume copies them in)
+    h_offs = offs.cpu().numpy().view(np.uint32)
+    h_raw, h_v = raw.cpu().numpy(), v.cpu().numpy()
+    hbatch = wg.Batch([wg.Column(wg.TYPE_BYTES, (h_offs, h_raw)), wg.Column(wg.TYPE_INT64, h_v)])
+
+    def e2e_step():
+        agg.reset()
+        agg.consume(hbatch)
+        got[0] = agg.finalize()
+
+    e2e_ms = _timed_ms(stream, e2e_step, args.e2e_steps, 1)
+    sample = min(n, 1 << 22)
+    cpu = None if args.no_cpu_baseline else {
+        "value": cpu_strgroup_sample(h_offs[:sample + 1].astype(np.int64), h_raw, h_v[:sample]), "unit": "rows/s",
+        "cores": 1, "kind": "port",
+        "sample": f"the first {sample} rows, 2048-row batches, oracle string numbering + aggregate on one host thread"}
+    print(json.dumps({"workload": "strgroup", "metric": "rows/s", "rows": n, "distinct": distinct,
+                      "bytes": total, "value": n / (ms / 1e3), "unit": "rows/s", "ms_per_step": ms,
+                      "hbm_gbs": alg / (ms / 1e3) / 1e9, "frac_of_peak": alg / (ms / 1e3) / 1e9 / peak,
+                      "peak_kind": peak_kind_note(kind), "algorithmic_bytes": alg, "gpu_launches": launches,
+                      "e2e": {"value": n / (e2e_ms / 1e3), "unit": "rows/s", "h2d_bytes_per_step": alg,
+                              "d2h_bytes_per_step": 8},
+                      "clocks": clocks, "cpu_baseline": cpu}), flush=True)
+    agg.close()
     ctx.close()
 
 
@@ -791,7 +880,8 @@ def main():
         return
     if args.workload != "starjoin":
         {"groupby": run_groupby, "highcard": run_highcard, "batched": run_batched, "serving": run_serving,
-         "filter": run_filter, "highcard_spill": lambda a: run_highcard(a, hbm_cap=8 << 30)}[args.workload](args)
+         "filter": run_filter, "strgroup": run_strgroup,
+         "highcard_spill": lambda a: run_highcard(a, hbm_cap=8 << 30)}[args.workload](args)
         return
     run_ours(args, rank, world, local_rank)
 

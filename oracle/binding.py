@@ -95,6 +95,10 @@ def lib() -> C.CDLL:
             "or_i128_to_f64": (C.c_double, [I64, C.c_uint64, I32]),
             "or_rle_decode": (I64, [P, I64, I32, I64, P]),
             "or_page_decode": (C.c_int, [P, P, P]),
+            "or_strindex_new": (P, []),
+            "or_strindex_map": (I64, [P, P, P, P, I64, P, I64, P]),
+            "or_strindex_get": (I64, [P, I64, P, I64]),
+            "or_strindex_free": (None, [P]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -338,28 +342,48 @@ def page_decode(chunk, rows: int, out_dtype):
 
 
 class StrGroupIndex:
-    """String GROUP BY keys as consumeBatchStrGroup numbers them
-    (internal/engine/exec/aggregate.go:3038-3110): each distinct string takes the
+    """String GROUP BY keys numbered as consumeBatchStrGroup numbers them
+    (or_strindex_*, exec/aggregate.go:3038-3110): each distinct string takes the
     next group index at its first appearance, in row (selection) order across
-    batches; a NULL string is the NULL-key group. `map` returns an INT32 column of
-    group indexes and its validity, to aggregate like an int key."""
+    batches; a NULL string is the NULL-key group. `map` returns an INT32 column
+    of group indexes and its validity, to aggregate like an int key."""
 
     def __init__(self):
-        self.index: dict[bytes, int] = {}
-        self.strings: list[bytes] = []
+        self.h = lib().or_strindex_new()
+        self.n = 0
+
+    def map_arrays(self, offs, raw, valid_words=None, sel=None, length=None):
+        """Columnar form: offsets (uint32, len + 1), bytes (uint8), validity words."""
+        n = len(offs) - 1 if length is None else length
+        ids = np.zeros(max(n, 1), np.int32)
+        o = np.ascontiguousarray(offs, np.uint32)
+        b = np.ascontiguousarray(raw, np.uint8) if len(raw) else np.zeros(1, np.uint8)
+        s = None if sel is None else np.ascontiguousarray(sel, np.uint32)
+        self.n = lib().or_strindex_map(self.h, o.ctypes.data, b.ctypes.data, _ptr(valid_words), n, _ptr(s),
+                                       0 if s is None else len(s), ids.ctypes.data)
+        return ids[:n]
 
     def map(self, values, valid=None, sel=None):
-        n = len(values)
-        ids = np.zeros(n, np.int32)
-        rows = range(n) if sel is None else [int(r) for r in sel]
-        for r in rows:
-            if valid is not None and not valid[r]:
-                continue
-            v = values[r]
-            g = self.index.get(v)
-            if g is None:
-                g = len(self.strings)
-                self.index[v] = g
-                self.strings.append(v)
-            ids[r] = g
+        enc = [b"" if (valid is not None and not valid[i]) else v for i, v in enumerate(values)]
+        offs = np.zeros(len(enc) + 1, np.uint32)
+        if enc:
+            offs[1:] = np.cumsum([len(v) for v in enc])
+        raw = np.frombuffer(b"".join(enc), np.uint8)
+        w = None if valid is None else pack_validity(np.asarray(valid, bool))
+        ids = self.map_arrays(offs, raw, w, sel)
         return ids, (None if valid is None else np.asarray(valid, bool))
+
+    @property
+    def strings(self) -> list:
+        out = []
+        for i in range(self.n):
+            ln = lib().or_strindex_get(self.h, i, None, 0)
+            buf = np.zeros(max(ln, 1), np.uint8)
+            lib().or_strindex_get(self.h, i, buf.ctypes.data, ln)
+            out.append(buf[:ln].tobytes())
+        return out
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().or_strindex_free(self.h)
+            self.h = None

@@ -17,6 +17,7 @@
 #include <memory>
 #include <string>
 #include <thread>
+#include <unordered_map>
 #include <vector>
 
 namespace {
@@ -1171,5 +1172,45 @@ void or_gen_highcard(uint64_t seed, int64_t row0, int64_t n, int32_t* a, int64_t
     }
   });
 }
+
+// ---- string GROUP BY keys (consumeBatchStrGroup, exec/aggregate.go:3038) ----
+// strIdx.GetOrInsertRefAt hands out len(h.strGroupStates) to a string it has not
+// seen (aggregate.go:3083-3090), i.e. group indexes in first-appearance order;
+// NULL rows take strNullGroupSlot (aggregate.go:3078), the NULL key here.
+struct StrIndex {
+  std::unordered_map<std::string, int32_t> index;
+  std::vector<std::string> strings;
+};
+
+void* or_strindex_new(void) { return new StrIndex(); }
+
+int64_t or_strindex_map(void* h, const uint32_t* offs, const uint8_t* bytes, const uint64_t* valid, int64_t len,
+                        const uint32_t* sel, int64_t sel_len, int32_t* ids) {
+  StrIndex* x = (StrIndex*)h;
+  const int64_t n = sel ? sel_len : len;
+  for (int64_t i = 0; i < n; ++i) {
+    const int64_t r = sel ? (int64_t)sel[i] : i;
+    if (valid && !((valid[r >> 6] >> (r & 63)) & 1)) { ids[r] = 0; continue; }
+    std::string key((const char*)bytes + offs[r], offs[r + 1] - offs[r]);
+    auto it = x->index.find(key);
+    if (it == x->index.end()) {
+      const int32_t g = (int32_t)x->strings.size();
+      x->strings.push_back(key);
+      it = x->index.emplace(std::move(key), g).first;
+    }
+    ids[r] = it->second;
+  }
+  return (int64_t)x->strings.size();
+}
+
+int64_t or_strindex_get(void* h, int64_t id, uint8_t* out, int64_t cap) {
+  StrIndex* x = (StrIndex*)h;
+  if (id < 0 || id >= (int64_t)x->strings.size()) return -1;
+  const std::string& s = x->strings[(size_t)id];
+  if (out) std::memcpy(out, s.data(), std::min<size_t>(s.size(), (size_t)cap));
+  return (int64_t)s.size();
+}
+
+void or_strindex_free(void* h) { delete (StrIndex*)h; }
 
 }  // extern "C"

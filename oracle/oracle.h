@@ -87,6 +87,19 @@ int64_t or_rle_decode(const uint8_t* data, int64_t len, int32_t bit_width, int64
  * 0, or -1 on a malformed page. */
 int     or_page_decode(const wg_column_chunk* chunk, void* out, uint64_t* valid_words);
 
+/* String GROUP BY keys as consumeBatchStrGroup numbers them
+ * (exec/aggregate.go:3038-3110): each distinct string takes the next group
+ * index at its first appearance, in row (selection) order across batches; a
+ * NULL string is the NULL-key group (ids[row] = 0, its validity kept). map
+ * writes ids[row] for the batch's rows (offsets len + 1 entries) and returns
+ * the distinct strings so far; get copies string `id` into out (at most cap
+ * bytes) and returns its length. */
+void*   or_strindex_new(void);
+int64_t or_strindex_map(void* h, const uint32_t* offsets, const uint8_t* bytes, const uint64_t* valid_words,
+                        int64_t len, const uint32_t* sel, int64_t sel_len, int32_t* ids);
+int64_t or_strindex_get(void* h, int64_t id, uint8_t* out, int64_t cap);
+void    or_strindex_free(void* h);
+
 /* Int128.ToFloat64 (batch/decimal.go:39) for fixture checks. */
 double  or_i128_to_f64(int64_t hi, uint64_t lo, int32_t scale);
 

@@ -111,6 +111,19 @@ GROUPBY = [{
     "expect": {"1": [40.0, 2], "2": [60.0, 2]},
 }]
 
+# ---- string GROUP BY keys (consumeBatchStrGroup, aggregate.go:3038) --------------------------------------
+# batches of (key or None, value); expect: key (None = the NULL group) -> [COUNT(*), SUM(v)]
+STRING_GROUPBY = [
+    {"ref": "internal/engine/exec/aggregate_null_group_test.go:226",
+     "batches": [[["a", 1], [None, 10], ["b", 2], [None, 20]],
+                 [[None, 30], ["a", 3], ["\x01", 100]]],
+     "expect": [["a", 2, 4], ["b", 1, 2], ["\x01", 1, 100], [None, 3, 60]]},
+    # exec_test.go:39 TestHashAggregate with its string keys; SUM(amount) of float64 restated as int64
+    {"ref": "internal/engine/exec/exec_test.go:39",
+     "batches": [[["a", 10], ["b", 20], ["a", 30], ["b", 40]]],
+     "expect": [["a", 2, 40], ["b", 2, 60]]},
+]
+
 # ---- inner join: join_test.go:10 TestHashJoin_Inner, alice=1 bob=2 carol=3 unknown=4 -------------------
 JOINS = [{
     "ref": "internal/engine/exec/join_test.go:10",
@@ -195,6 +208,7 @@ def main() -> None:
                          for r, t, v, n, s, f, e in ACCUMULATORS],
         "decimal": DECIMAL,
         "groupby": GROUPBY,
+        "string_groupby": STRING_GROUPBY,
         "joins": JOINS,
         "packed_layout": PACKED_LAYOUT,
         "extreme_keys": EXTREME_KEYS,

@@ -70,6 +70,21 @@ def test_groupby_known_answer(ctx):
         agg.close()
 
 
+@pytest.mark.parametrize("case", GOLD["string_groupby"], ids=lambda c: c["ref"])
+def test_string_groupby_known_answer(ctx, case):
+    import wadjet_b200 as wg
+    agg = wg.HashAggregate(ctx, [0], [wg.AggColumn(wg.AGG_COUNT, -1), wg.AggColumn(wg.AGG_SUM, 1)])
+    for rows in case["batches"]:
+        agg.consume(wg.Batch([wg.Column.strings([k for k, _ in rows]),
+                              wg.Column(2, np.array([x for _, x in rows], np.int64))]))
+    agg.finalize()
+    out = agg.collect()
+    got = sorted([[out[0][0][i] if out[0][1][i] else None, int(out[1][0][i]), int(out[2][0][i])]
+                  for i in range(len(out[0][0]))], key=lambda r: (r[0] is None, r[0] or ""))
+    assert got == sorted(case["expect"], key=lambda r: (r[0] is None, r[0] or ""))
+    agg.close()
+
+
 def test_join_known_answer(ctx):
     import wadjet_b200 as wg
     for c in GOLD["joins"]:

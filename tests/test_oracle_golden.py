@@ -102,6 +102,34 @@ def test_groupby_known_answer():
         assert got == c["expect"]
 
 
+@pytest.mark.parametrize("case", GOLD["string_groupby"], ids=lambda c: c["ref"])
+def test_string_groupby_known_answer(case):
+    """consumeBatchStrGroup: group indexes by first appearance, NULL its own group
+    (distinct from the one-byte string \x01), accumulated across batches."""
+    idx = ob.StrGroupIndex()
+    agg = ob.Agg([0], [(1, -1, 0), (0, 1, 0)])
+    for rows in case["batches"]:
+        keys = [b"" if k is None else k.encode() for k, _ in rows]
+        valid = np.array([k is not None for k, _ in rows], bool)
+        ids, ok = idx.map(keys, valid)
+        v = np.array([x for _, x in rows], np.int64)
+        agg.consume(ob.HostBatch([(1, ids, ok, 0), (2, v, None, 0)]))
+    e = agg.export()
+    strs = idx.strings
+    got = sorted([[strs[int(e["keys"][0, i])].decode() if e["key_valid"][0, i] else None,
+                   int(e["count"][0, i]), int(e["i64"][1, i])] for i in range(e["count"].shape[1])],
+                 key=lambda r: (r[0] is None, r[0] or ""))
+    want = sorted(case["expect"], key=lambda r: (r[0] is None, r[0] or ""))
+    assert got == want
+    # first-appearance numbering
+    first = []
+    for rows in case["batches"]:
+        for k, _ in rows:
+            if k is not None and k.encode() not in first:
+                first.append(k.encode())
+    assert strs == first
+
+
 def test_join_known_answer():
     for c in GOLD["joins"]:
         j = ob.Join()

@@ -1073,7 +1073,8 @@ static wg_status run_device(const PipelineRun& r) {
   auto fits = [&](int64_t groups, int slots) {
     return slots >= 256 && groups * (blocks_per_sm == 1 ? 4 : 8) <= (int64_t)slots * (blocks_per_sm == 1 ? 3 : 5);
   };
-  const int64_t expect = std::max<int64_t>(a->hint, a->known_groups);
+  // a string dictionary's ids: the groups are at most its strings and the NULL key
+  const int64_t expect = r.str_ids ? strdict_size(a->sdict) + 1 : std::max<int64_t>(a->hint, a->known_groups);
   const bool smem_ok = env_int("WG_AGG_SMEM", 1) != 0 && a->L.key_words == 1 && !any_null_words && !any_dec_minmax &&
                        expect > 0;
   // prefer the kernel's CTAs per SM, then as many float-SUM copies as still
@@ -1092,16 +1093,22 @@ static wg_status run_device(const PipelineRun& r) {
     S = slots_for(blocks_per_sm, 1);
   }
   // dense GROUP BY: the key is a join payload column whose value range is known
-  // and small, so the shared table is indexed by key - min (no hashing, no key
+  // and small, or a small string dictionary's ids, so the shared table is indexed by key - min (no hashing, no key
   // compare, no insert) and holds exactly one slot per possible key
   {
     long long glo = 0, ghi = -1;
     const int kv = ls.P.L.key_vcol[0];
     const int npay = r.join ? join_n_payload(r.join) : 0;
-    const bool cand = smem_ok && env_int("WG_GROUP_DENSE", 1) != 0 && a->L.n_keys == 1 && r.join != nullptr &&
-                      join_type_of(r.join) == WG_JOIN_INNER &&
-                      kv >= ls.P.n_in && kv < ls.P.n_in + npay &&
-                      join_payload_range(r.join, kv - ls.P.n_in, &glo, &ghi) && ghi >= glo && ghi - glo < 16384;
+    bool ranged = false;
+    if (r.join != nullptr && join_type_of(r.join) == WG_JOIN_INNER && kv >= ls.P.n_in && kv < ls.P.n_in + npay)
+      ranged = join_payload_range(r.join, kv - ls.P.n_in, &glo, &ghi);
+    else if (r.str_ids && kv < ls.P.n_in) {  // a string dictionary's ids: [0, its strings)
+      glo = 0;
+      ghi = strdict_size(a->sdict) - 1;
+      ranged = true;
+    }
+    const bool cand = smem_ok && env_int("WG_GROUP_DENSE", 1) != 0 && a->L.n_keys == 1 && ranged && ghi >= glo &&
+                      ghi - glo < 16384;
     bool placed = false;
     for (int t = 0; t < 2 && cand && !placed; ++t) {
       if (t == 1 && (env_bps > 0 || pref_bps == 1)) break;
@@ -1323,8 +1330,7 @@ static wg_status run_device(const PipelineRun& r) {
       WG_CUDA_TRY(cudaMemcpyAsync(a->backup.as<char>() + tb, a->ctr.get(), 64, cudaMemcpyDeviceToDevice, ctx->stream));
       WG_TRY(launch_pipeline(a, ls, n_items));
       int64_t v[2];
-      WG_TRY(read_back_i64(ctx, (const int64_t*)a->ctr.get(), v, 2));
-      WG_TRY(check_device_error(ctx));
+      WG_TRY(read_back_checked(ctx, (const int64_t*)a->ctr.get(), v, 2));
       if ((int32_t)v[1] == 0) {
         a->known_groups = a->upper_groups = v[0];
         return WG_OK;
@@ -2230,7 +2236,7 @@ static wg_status agg_compact(wg_agg* a) {
   ctx->count_launch();
   WG_CUDA_TRY(cudaGetLastError());
   int64_t c = 0;
-  WG_TRY(read_back_i64(ctx, a->cnt.as<int64_t>(), &c, 1));
+  WG_TRY(read_back_checked(ctx, a->cnt.as<int64_t>(), &c, 1));
   a->n_out = c;
   return WG_OK;
 }
@@ -2421,8 +2427,10 @@ wg_status wg_agg_finalize(wg_agg* a, int64_t* n_groups) {
   if (!a->finalized) {
     if (a->hc) WG_TRY(hc_finish(a));
     else if (a->spill) WG_TRY(spill_finish(a));
-    else WG_TRY(agg_compact(a));
+    else WG_TRY(agg_compact(a));  // its read-back checks the device error word
     a->finalized = true;
+    if (n_groups) *n_groups = a->n_out;
+    return a->hc || a->spill ? check_device_error(a->ctx) : WG_OK;
   }
   if (n_groups) *n_groups = a->n_out;
   return check_device_error(a->ctx);
@@ -2557,10 +2565,7 @@ wg_status wg_agg_reset(wg_agg* a) {
   WG_TRY(ensure_device(a->ctx));
   a->finalized = false;
   a->n_out = 0;
-  if (a->sdict) {
-    cudaStreamSynchronize(a->ctx->stream);
-    strdict_reset(a->sdict);  // the schema (and str_keyed) stays resolved
-  }
+  strdict_reset(a->sdict, a->ctx);  // the schema (and str_keyed) stays resolved
   if (!a->resolved) return WG_OK;
   Ctx* ctx = a->ctx;
   if (a->spill) {

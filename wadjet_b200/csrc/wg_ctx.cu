@@ -153,10 +153,31 @@ wg_status read_back_i64(Ctx* ctx, const int64_t* dev, int64_t* out, int n) {
   return WG_OK;
 }
 
+static wg_status device_error_status(Ctx* ctx, int32_t h);
+
 wg_status check_device_error(Ctx* ctx) {
   int32_t h = 0;
   WG_CUDA_TRY(cudaMemcpyAsync(&h, ctx->dev_error, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
   WG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return device_error_status(ctx, h);
+}
+
+wg_status read_back_checked(Ctx* ctx, const int64_t* dev, int64_t* out, int n) {
+  int32_t h = 0;
+  {
+    std::lock_guard<std::mutex> g(ctx->mu);
+    if (n > 0)
+      WG_CUDA_TRY(cudaMemcpyAsync(ctx->host_scalar, dev, sizeof(int64_t) * n, cudaMemcpyDeviceToHost, ctx->stream));
+    int32_t* herr = reinterpret_cast<int32_t*>(ctx->host_scalar + 63);
+    WG_CUDA_TRY(cudaMemcpyAsync(herr, ctx->dev_error, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    WG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    for (int i = 0; i < n; ++i) out[i] = ctx->host_scalar[i];
+    h = *herr;
+  }
+  return device_error_status(ctx, h);
+}
+
+static wg_status device_error_status(Ctx* ctx, int32_t h) {
   if (h == WG_DERR_NONE) return WG_OK;
   WG_CUDA_TRY(cudaMemsetAsync(ctx->dev_error, 0, sizeof(int32_t), ctx->stream));
   switch (h) {

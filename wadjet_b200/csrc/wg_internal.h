@@ -144,6 +144,9 @@ void parallel_copy(void* dst, const void* src, int64_t bytes);
 wg_status ensure_device(Ctx* ctx);           // cudaSetDevice(ctx->device)
 wg_status read_back_i64(Ctx* ctx, const int64_t* dev, int64_t* out, int n);
 wg_status check_device_error(Ctx* ctx);      // reads and clears dev_error
+// read_back_i64 and check_device_error with one wait: n values (n < 63) and
+// the error word, which fails the call when set
+wg_status read_back_checked(Ctx* ctx, const int64_t* dev, int64_t* out, int n);
 
 // Copy a host column/bitmap into a device buffer (synchronous on ctx->stream).
 int64_t elem_size(int32_t type_id);          // 4 / 8 / 16, or 0 when unsupported
@@ -166,7 +169,7 @@ struct StrDict;
 wg_status strdict_map(Ctx* ctx, StrDict** d, const wg_batch_desc* in, int col, bool host, int64_t hint, wg_column* out);
 wg_status strdict_strings(Ctx* ctx, StrDict* d, const int64_t* ids, int64_t n, uint32_t* out_offsets,
                           uint8_t* out_bytes, int64_t bytes_cap, int64_t* need_bytes);
-void strdict_reset(StrDict* d);
+void strdict_reset(StrDict* d, Ctx* ctx);
 void strdict_free(StrDict* d);
 int64_t strdict_size(const StrDict* d);
 

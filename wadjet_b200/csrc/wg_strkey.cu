@@ -24,6 +24,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <vector>
 
@@ -68,23 +69,54 @@ __device__ __forceinline__ U128 str_hash(const uint8_t* p, uint32_t n) {
   return h;
 }
 
-// (1) Find or install each non-NULL item's hash: rowslot[i] = its slot, -1 for
-// a NULL string. ctr[0] counts the slots in use; once it passes `limit` (3/4
-// of the table) ctr[1] is raised and the items still probing stop (rowslot
-// -2), so the host grows the table and runs the pass again; a walk over the
-// whole table raises it too.
-__global__ void str_insert_kernel(StrSrc s, unsigned long long* slots, uint64_t mask, int32_t* rowslot,
-                                  unsigned long long* ctr, unsigned long long limit) {
-  volatile unsigned long long* full = ctr + 1;
+// Distinct-hash sketch of a batch (HyperLogLog, Flajolet, Fusy, Gandouet and
+// Meunier 2007): 2^kSketchBits registers, each the largest rank (leading zeros
+// + 1) of the hashes that fall in it. It sizes the table before the insert
+// pass, so a batch of many new strings does not fill a small table first.
+constexpr int kSketchBits = 10;
+constexpr int kProbeLimit = 4096;  // an insert probing further asks for a larger table
+
+// (1a) Each item's 128-bit hash ({~0, ~0} for a NULL string) and the sketch.
+__global__ void str_hash_kernel(StrSrc s, U128* hashes, uint32_t* sketch) {
+  __shared__ uint32_t reg[1 << kSketchBits];
+  for (int r = threadIdx.x; r < (1 << kSketchBits); r += blockDim.x) reg[r] = 0;
+  __syncthreads();
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < s.n; i += (int64_t)gridDim.x * blockDim.x) {
     const int64_t row = item_row(s, i);
-    if (row_null(s, row)) { rowslot[i] = -1; continue; }
-    if (*full != 0) { rowslot[i] = -2; continue; }
-    const uint32_t b0 = s.offs[row], b1 = s.offs[row + 1];
-    const U128 k = str_hash(s.bytes + b0, b1 - b0);
-    uint64_t idx = k.lo & mask;
+    U128 k;
+    if (row_null(s, row)) {
+      k.lo = kEmpty;
+      k.hi = kEmpty;
+    } else {
+      const uint32_t b0 = s.offs[row];
+      k = str_hash(s.bytes + b0, s.offs[row + 1] - b0);
+      const uint32_t r = (uint32_t)(k.hi >> (64 - kSketchBits));
+      const uint32_t rank = (uint32_t)__clzll((long long)((k.hi << kSketchBits) | (1ULL << (kSketchBits - 1)))) + 1;
+      if (reg[r] < rank) atomicMax(reg + r, rank);
+    }
+    hashes[i] = k;
+  }
+  __syncthreads();
+  for (int r = threadIdx.x; r < (1 << kSketchBits); r += blockDim.x)
+    if (reg[r] != 0) atomicMax(sketch + r, reg[r]);
+}
+
+// (1b) Find or install each non-NULL item's hash: rowslot[i] = its slot, -1 for
+// a NULL string, -2 when the probe passed kProbeLimit slots (ctr[1] is then
+// raised and the host grows the table and runs the pass again). ctr[0] counts
+// the installs, added once per CTA.
+__global__ void str_insert_kernel(const U128* hashes, int64_t n, unsigned long long* slots, uint64_t mask,
+                                  int32_t* rowslot, unsigned long long* ctr) {
+  __shared__ unsigned int installs;
+  if (threadIdx.x == 0) installs = 0;
+  __syncthreads();
+  const uint64_t limit = mask < (uint64_t)kProbeLimit ? mask + 1 : (uint64_t)kProbeLimit;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const U128 k = hashes[i];
+    if (k.lo == kEmpty && k.hi == kEmpty) { rowslot[i] = -1; continue; }
+    uint64_t idx = (k.lo ^ (k.lo >> 32)) & mask;
     int32_t found = -2;
-    for (uint64_t probe = 0; probe <= mask && *full == 0; ++probe) {
+    for (uint64_t probe = 0; probe < limit; ++probe) {
       unsigned long long* sl = slots + idx * 4;
       const U128 cur = read128(sl);
       if (cur.lo == k.lo && cur.hi == k.hi) { found = (int32_t)idx; break; }
@@ -92,7 +124,7 @@ __global__ void str_insert_kernel(StrSrc s, unsigned long long* slots, uint64_t 
         U128 e; e.lo = kEmpty; e.hi = kEmpty;
         const U128 old = cas128((U128*)sl, e, k);
         if (old.lo == e.lo && old.hi == e.hi) {
-          if (atomicAdd(ctr, 1ULL) + 1 > limit) *full = 1;
+          atomicAdd(&installs, 1u);
           found = (int32_t)idx;
           break;
         }
@@ -100,9 +132,11 @@ __global__ void str_insert_kernel(StrSrc s, unsigned long long* slots, uint64_t 
       }
       idx = (idx + 1) & mask;
     }
-    if (found == -2 && *full == 0) *full = 1;  // walked the whole table
+    if (found == -2) ctr[1] = 1;
     rowslot[i] = found;
   }
+  __syncthreads();
+  if (threadIdx.x == 0 && installs != 0) atomicAdd(ctr, (unsigned long long)installs);
 }
 
 // (2) The lowest item of each slot that has no id yet.
@@ -110,7 +144,10 @@ __global__ void str_elect_kernel(int64_t n, const unsigned long long* slots, con
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const int32_t sl = rowslot[i];
     if (sl < 0) continue;
-    if (slots[(int64_t)sl * 4 + 2] == kNoId) atomicMin(rep + sl, (uint32_t)i);
+    // the atomic only when it can lower the slot's candidate: rows of a
+    // frequent string would otherwise all hit one word
+    if (slots[(int64_t)sl * 4 + 2] == kNoId && *(volatile uint32_t*)(rep + sl) > (uint32_t)i)
+      atomicMin(rep + sl, (uint32_t)i);
   }
 }
 
@@ -176,7 +213,7 @@ __global__ void str_rehash_kernel(const unsigned long long* old, uint64_t old_ca
     const unsigned long long* o = old + i * 4;
     if (o[0] == kEmpty && o[1] == kEmpty) continue;
     U128 k; k.lo = o[0]; k.hi = o[1];
-    uint64_t idx = k.lo & mask;
+    uint64_t idx = (k.lo ^ (k.lo >> 32)) & mask;
     for (uint64_t probe = 0; probe <= mask; ++probe) {
       unsigned long long* sl = slots + idx * 4;
       U128 e; e.lo = kEmpty; e.hi = kEmpty;
@@ -221,7 +258,7 @@ struct StrDict {
   uint64_t cap = 0;                 // table slots (a power of two)
   int64_t n_ids = 0, used = 0;      // distinct strings and arena bytes
   int64_t slots_used = 0;           // installed hashes (n_ids after every complete batch)
-  DevBuf rowslot, pack, pre, scan_tmp, gid;           // per-batch scratch
+  DevBuf hashes, sketch, rowslot, pack, pre, scan_tmp, gid;  // per-batch scratch
   DevBuf h_offs, h_bytes, h_valid, h_sel;             // a host batch's string column on the device
   std::vector<unsigned long long> loc_host;           // host copies for wg_agg_key_strings,
   std::vector<uint8_t> arena_host;                    // valid while no batch came since
@@ -265,6 +302,22 @@ wg_status str_table(Ctx* ctx, StrDict* d, uint64_t cap) {
   return WG_OK;
 }
 
+// The sketch's distinct-count estimate: the harmonic-mean estimator with the
+// linear-counting correction for small counts (Flajolet et al. 2007).
+wg_status sketch_estimate(Ctx* ctx, StrDict* d, double* out) {
+  const int m = 1 << kSketchBits;
+  uint32_t reg[1 << kSketchBits];
+  WG_CUDA_TRY(cudaMemcpyAsync(reg, d->sketch.get(), sizeof(reg), cudaMemcpyDeviceToHost, ctx->stream));
+  WG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  double z = 0.0;
+  int zeros = 0;
+  for (int r = 0; r < m; ++r) { z += std::ldexp(1.0, -(int)reg[r]); zeros += reg[r] == 0; }
+  double e = 0.7213 / (1.0 + 1.079 / m) * m * m / z;
+  if (e <= 2.5 * m && zeros > 0) e = m * std::log((double)m / zeros);
+  *out = e;
+  return WG_OK;
+}
+
 uint64_t pow2_at_least(uint64_t v) {
   uint64_t c = 1024;
   while (c < v) c <<= 1;
@@ -275,12 +328,16 @@ uint64_t pow2_at_least(uint64_t v) {
 
 void strdict_free(StrDict* d) { delete d; }
 
-void strdict_reset(StrDict* d) {
+// Forget every string; the buffers (and the table's size) stay for the next query.
+void strdict_reset(StrDict* d, Ctx* ctx) {
   if (!d) return;
-  d->slots.reset(); d->rep.reset(); d->arena.reset(); d->id_loc.reset();
-  d->rowslot.reset(); d->pack.reset(); d->pre.reset(); d->scan_tmp.reset(); d->gid.reset();
-  d->h_offs.reset(); d->h_bytes.reset(); d->h_valid.reset(); d->h_sel.reset();
-  d->cap = 0; d->n_ids = 0; d->used = 0; d->slots_used = 0;
+  if (d->cap > 0) {
+    str_init_slots_kernel<<<str_grid(ctx, (int64_t)d->cap, 256), 256, 0, ctx->stream>>>(d->slots.as<unsigned long long>(),
+                                                                                    d->cap);
+    ctx->count_launch();
+    cudaMemsetAsync(d->rep.get(), 0xFF, (size_t)d->cap * 4, ctx->stream);
+  }
+  d->n_ids = 0; d->used = 0; d->slots_used = 0;
   d->loc_host.clear(); d->arena_host.clear(); d->host_fresh = false;
 }
 
@@ -329,23 +386,34 @@ wg_status strdict_map(Ctx* ctx, StrDict** dp, const wg_batch_desc* in, int col, 
   *out = wg_column{WG_TYPE_INT32, 0, d->gid.get(), s.valid, len};
   if (n == 0) return WG_OK;
 
-  // (1) install the hashes, growing the table whenever it passes 3/4 full
-  const uint64_t want = pow2_at_least(2 * (uint64_t)(d->slots_used + std::min<int64_t>(n, std::max<int64_t>(hint, 1 << 16))));
-  if (d->cap < want) WG_TRY(str_table(ctx, d, want));
+  // (1) hash every item and sketch the batch's distinct strings; size the
+  // table for the strings so far plus the sketch's estimate (load at most 2/3
+  // when the estimate holds), then install the hashes, growing the table and
+  // running the pass again if a probe ran long
+  WG_TRY(d->hashes.ensure(ctx, n * 16));
+  WG_TRY(d->sketch.ensure(ctx, (int64_t(1) << kSketchBits) * 4));
   WG_TRY(d->rowslot.ensure(ctx, n * 4));
   WG_TRY(d->ctr.ensure(ctx, 64));
   unsigned long long* ctr = d->ctr.as<unsigned long long>();
   const unsigned grid = str_grid(ctx, n, 256);
+  WG_CUDA_TRY(cudaMemsetAsync(d->sketch.get(), 0, (size_t(1) << kSketchBits) * 4, ctx->stream));
+  str_hash_kernel<<<grid, 256, 0, ctx->stream>>>(s, d->hashes.as<U128>(), d->sketch.as<uint32_t>());
+  ctx->count_launch();
+  WG_CUDA_TRY(cudaGetLastError());
+  double est = 0.0;
+  WG_TRY(sketch_estimate(ctx, d, &est));
+  const uint64_t want = pow2_at_least((uint64_t)(1.5 * ((double)d->slots_used + std::min<double>((double)n, est * 1.1)) + 64));
+  if (d->cap < want) WG_TRY(str_table(ctx, d, want));
   int64_t cv[4] = {0, 0, 0, 0};
   for (int pass = 0;; ++pass) {
     str_ctr_kernel<<<1, 1, 0, ctx->stream>>>(ctr, (unsigned long long)d->slots_used);
-    str_insert_kernel<<<grid, 256, 0, ctx->stream>>>(s, d->slots.as<unsigned long long>(), d->cap - 1,
-                                                     d->rowslot.as<int32_t>(), ctr, d->cap / 4 * 3);
+    str_insert_kernel<<<grid, 256, 0, ctx->stream>>>(d->hashes.as<U128>(), n, d->slots.as<unsigned long long>(),
+                                                     d->cap - 1, d->rowslot.as<int32_t>(), ctr);
     ctx->count_launch(2);
     WG_CUDA_TRY(cudaGetLastError());
     WG_TRY(read_back_i64(ctx, reinterpret_cast<int64_t*>(ctr), cv, 2));
     if (cv[1] == 0) break;
-    if (pass >= 24 || d->cap >= (1ULL << 31)) return fail(WG_E_NOMEM, "string dictionary table cannot grow");
+    if (pass >= 16 || d->cap >= (1ULL << 31)) return fail(WG_E_NOMEM, "string dictionary table cannot grow");
     d->slots_used = cv[0];  // the installs of the stopped pass stay in the table
     WG_TRY(str_table(ctx, d, std::max<uint64_t>(d->cap * 4, pow2_at_least(2 * (uint64_t)cv[0]))));
   }
@@ -366,7 +434,7 @@ wg_status strdict_map(Ctx* ctx, StrDict** dp, const wg_batch_desc* in, int col, 
   WG_CUDA_TRY(cub::DeviceScan::ExclusiveSum(d->scan_tmp.get(), tmp, d->pack.as<unsigned long long>(),
                                             d->pre.as<unsigned long long>(), (int)n, ctx->stream));
   str_total_kernel<<<1, 1, 0, ctx->stream>>>(d->pre.as<unsigned long long>(), d->pack.as<unsigned long long>(), n, ctr);
-  ctx->count_launch(2);
+  ctx->count_launch(3);  // the scan's two kernels and the total
   WG_CUDA_TRY(cudaGetLastError());
   WG_TRY(read_back_i64(ctx, reinterpret_cast<int64_t*>(ctr), cv, 3));
   const int64_t new_ids = (int64_t)((unsigned long long)cv[2] >> 32);

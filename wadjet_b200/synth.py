@@ -4,6 +4,9 @@
   price DECIMAL(15,2) as Int128, disc float64 U[0,0.1); dim of 2^22 unique keys with grp U[0,1000).
 - ``groupby(n)``   : k int64 U[0,4096), v int64 U[0,1e6), f float64 U[0,1), flag int32 U[0,10).
 - ``highcard(n)``  : a int32, b int64 (~2^26 distinct (a,b)), amt DECIMAL(18,2), x float64 ~N(0,1).
+- ``strgroup(n)``  : a BYTES column of n values drawn uniformly from `distinct` URL-like strings
+  (8-56 lowercase bytes, the first five spelling the string's number in base 26, so all differ),
+  as (offsets uint32, bytes uint8), and v int64 U[0,1e6).
 """
 from __future__ import annotations
 
@@ -89,3 +92,33 @@ def batched_query(ctx, q: int, seed: int = SEED, device: int = 0, rows: int | No
         val = torch.empty(n, dtype=torch.float64, device=dev)
         _check(lib.wg_synth_batched(ctx.h, seed, q, n, card, _p(key), None, _p(val), _p(filt)))
     return key, val, filt, card, thr
+
+
+def strgroup(n: int, distinct: int = 1 << 20, seed: int = SEED, device: int = 0, chunk: int = 1 << 22):
+    """(offsets, bytes, v): see the module docstring. Generated with torch on the device."""
+    dev = torch.device("cuda", device)
+    g = torch.Generator(device=dev)
+    g.manual_seed(seed)
+    lens = torch.randint(8, 57, (distinct,), generator=g, device=dev, dtype=torch.int64)
+    poff = torch.zeros(distinct + 1, dtype=torch.int64, device=dev)
+    poff[1:] = torch.cumsum(lens, 0)
+    pool = torch.randint(97, 123, (int(poff[-1]),), generator=g, device=dev, dtype=torch.int64).to(torch.uint8)
+    ids = torch.arange(distinct, device=dev, dtype=torch.int64)
+    for d in range(5):  # base-26 digits of the string's number
+        pool[poff[:-1] + d] = (97 + (ids // (26 ** d)) % 26).to(torch.uint8)
+    pick = torch.randint(0, distinct, (n,), generator=g, device=dev, dtype=torch.int64)
+    plen = lens[pick]
+    offs64 = torch.zeros(n + 1, dtype=torch.int64, device=dev)
+    offs64[1:] = torch.cumsum(plen, 0)
+    total = int(offs64[-1])
+    if total >= 1 << 32:
+        raise ValueError("strgroup: more than 2^32 bytes")
+    raw = torch.empty(total, dtype=torch.uint8, device=dev)
+    for r0 in range(0, n, chunk):
+        r1 = min(n, r0 + chunk)
+        b0, b1 = int(offs64[r0]), int(offs64[r1])
+        src = torch.repeat_interleave(poff[pick[r0:r1]] - offs64[r0:r1], plen[r0:r1]) + \
+            torch.arange(b0, b1, device=dev, dtype=torch.int64)
+        raw[b0:b1] = pool[src]
+    v = torch.randint(0, 1_000_000, (n,), generator=g, device=dev, dtype=torch.int64)
+    return offs64.to(torch.int32), raw, v
