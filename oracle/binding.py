@@ -375,13 +375,14 @@ class StrGroupIndex:
 
     @property
     def strings(self) -> list:
-        out = []
-        for i in range(self.n):
+        """Every string by its group index (fetched once; later calls only add new ones)."""
+        out = self.__dict__.setdefault("_strings", [])
+        for i in range(len(out), self.n):
             ln = lib().or_strindex_get(self.h, i, None, 0)
             buf = np.zeros(max(ln, 1), np.uint8)
             lib().or_strindex_get(self.h, i, buf.ctypes.data, ln)
             out.append(buf[:ln].tobytes())
-        return out
+        return list(out)
 
     def __del__(self):
         if getattr(self, "h", None):

@@ -89,8 +89,9 @@ def check(ctx, got, want, g, idx):
     assert_groups_equal(got, want, KINDS)
     ok = got["key_valid"][0].astype(bool)
     ids = got["keys"][0][ok]
-    assert sorted(ids.tolist()) == list(range(len(idx.strings)))
-    assert g.key_strings(ids) == [idx.strings[i] for i in ids]
+    strs = idx.strings
+    assert sorted(ids.tolist()) == list(range(len(strs)))
+    assert g.key_strings(ids) == [strs[i] for i in ids]
 
 
 @pytest.mark.parametrize("nulls", [0.0, 0.07])

@@ -9,15 +9,17 @@
 // the string column's validity, so they form the NULL-key group); an export
 // or emit reports ids, and wg_agg_key_strings turns ids back into strings.
 //
-// The dictionary is an open-addressing table of 128-bit key hashes (two
-// independent 64-bit hashes of the bytes and the length) installed with one
-// 16-byte compare-and-swap, plus an arena holding each distinct string once.
-// Per batch: (1) every row finds or installs its hash's slot; (2) the rows of
-// slots installed in this batch elect the lowest row; (3) that row takes the
-// next id and copies its bytes into the arena; (4) every row compares its
-// bytes with its slot's stored string and takes the id. A 128-bit collision
-// between two different strings would make (4) fail, which the call reports
-// instead of merging the groups. No step waits on another thread.
+// The dictionary is an open-addressing table of 128-bit key hashes installed
+// with one 16-byte compare-and-swap, plus an arena holding each distinct
+// string once. Per batch: (1) a hash pass writes every row's hash and sketches
+// the batch's distinct strings, the table is sized from the sketch and every
+// row finds or installs its hash; (2) the rows of slots installed in this batch
+// elect the lowest row; (3) a scan over the elected rows gives each new string
+// its id and arena offset in row order, and its row copies the bytes; (4) every
+// row compares its bytes with its slot's stored string and takes the id. A
+// 128-bit collision between two different strings would make (4) fail, which
+// the call reports instead of merging the groups. No step waits on another
+// thread.
 #include "wg_internal.h"
 #include "wg_device.cuh"
 
@@ -51,22 +53,55 @@ __device__ __forceinline__ bool row_null(const StrSrc& s, int64_t row) {
   return s.valid != nullptr && ((s.valid[row >> 6] >> (row & 63)) & 1ULL) == 0;
 }
 
-// Two independent 64-bit hashes of a string: FNV-1a over the bytes, and a
-// multiply-xorshift mix over the bytes; both fold in the length. Neither word
-// is ~0, so {~0, ~0} stays the empty slot.
+// k (1..8) bytes at p as a little-endian word, zero above them. Only aligned
+// 8-byte words holding at least one of the k bytes are read, so no read leaves
+// the pages the string lies in.
+__device__ __forceinline__ unsigned long long load_bytes8(const uint8_t* p, uint32_t k) {
+  const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+  const unsigned long long* w = reinterpret_cast<const unsigned long long*>(a & ~uintptr_t(7));
+  const uint32_t sh = (uint32_t)(a & 7);
+  unsigned long long v = __ldg(w) >> (sh * 8);
+  if (sh + k > 8) v |= __ldg(w + 1) << ((8 - sh) * 8);
+  return k >= 8 ? v : (v & ((1ULL << (k * 8)) - 1));
+}
+
+// MurmurHash3's 64-bit finalizer (Appleby, public domain).
+__device__ __forceinline__ unsigned long long fmix64(unsigned long long k) {
+  k ^= k >> 33;
+  k *= 0xff51afd7ed558ccdULL;
+  k ^= k >> 33;
+  k *= 0xc4ceb9fe1a85ec53ULL;
+  k ^= k >> 33;
+  return k;
+}
+
+// Two 64-bit hashes of a string, eight bytes a step: a multiply-rotate and a
+// multiply-xorshift chain over the words, each finished with the length and
+// fmix64. Neither word is ~0, so {~0, ~0} stays the empty slot.
 __device__ __forceinline__ U128 str_hash(const uint8_t* p, uint32_t n) {
-  unsigned long long a = 0xcbf29ce484222325ULL, b = 0x9E3779B97F4A7C15ULL ^ (unsigned long long)n;
-  for (uint32_t i = 0; i < n; ++i) {
-    const unsigned long long c = p[i];
-    a = (a ^ c) * 0x100000001b3ULL;
-    b = (b ^ c) * 0xff51afd7ed558ccdULL;
+  unsigned long long a = 0x9E3779B97F4A7C15ULL ^ (unsigned long long)n, b = 0xC2B2AE3D27D4EB4FULL + n;
+  for (uint32_t j = 0; j < n; j += 8) {
+    const unsigned long long c = load_bytes8(p + j, min(8u, n - j));
+    a = (a ^ c) * 0x87C37B91114253D5ULL;
+    a = (a << 31) | (a >> 33);
+    b = (b + c) * 0x4CF5AD432745937FULL;
     b ^= b >> 29;
   }
-  a ^= (unsigned long long)n * 0xc4ceb9fe1a85ec53ULL;
   U128 h;
-  h.lo = a == kEmpty ? kEmpty - 1 : a;
-  h.hi = b == kEmpty ? kEmpty - 1 : b;
+  h.lo = fmix64(a ^ ((unsigned long long)n << 32));
+  h.hi = fmix64(b + a);
+  if (h.lo == kEmpty) h.lo = kEmpty - 1;
+  if (h.hi == kEmpty) h.hi = kEmpty - 1;
   return h;
+}
+
+// The n bytes at p and q are equal (eight at a time).
+__device__ __forceinline__ bool bytes_equal(const uint8_t* p, const uint8_t* q, uint32_t n) {
+  for (uint32_t j = 0; j < n; j += 8) {
+    const uint32_t k = min(8u, n - j);
+    if (load_bytes8(p + j, k) != load_bytes8(q + j, k)) return false;
+  }
+  return true;
 }
 
 // Distinct-hash sketch of a batch (HyperLogLog, Flajolet, Fusy, Gandouet and
@@ -199,9 +234,7 @@ __global__ void str_gid_kernel(StrSrc s, const unsigned long long* slots, const 
     const unsigned long long off = loc & ((1ULL << kLenShift) - 1);
     const uint32_t len = (uint32_t)(loc >> kLenShift);
     const uint32_t b0 = s.offs[row], n = s.offs[row + 1] - b0;
-    bool same = n == len;
-    for (uint32_t k = 0; same && k < n; ++k) same = s.bytes[b0 + k] == arena[off + k];
-    if (!same) set_error(err, WG_DERR_HASH_COLLISION);
+    if (n != len || !bytes_equal(s.bytes + b0, arena + off, n)) set_error(err, WG_DERR_HASH_COLLISION);
     gid[row] = (int32_t)slots[(int64_t)sl * 4 + 2];
   }
 }
