@@ -993,6 +993,13 @@ static wg_status agg_compact(wg_agg* a);
 // Run the fused kernel over a device-resident input with the overflow policy.
 static bool is_str_type(int32_t t) { return t == WG_TYPE_STRING || t == WG_TYPE_BYTES; }
 
+// The batch column holding the aggregate's single string GROUP BY key, or -1.
+static int str_key_col(const wg_agg* a, const wg_batch_desc* in) {
+  if (a->key_cols.size() != 1 || in->ncols < 0 || (in->ncols > 0 && !in->cols)) return -1;
+  const int kc = a->key_cols[0];
+  return kc >= 0 && kc < in->ncols && is_str_type(in->cols[kc].type_id) ? kc : -1;
+}
+
 static wg_status run_device(const PipelineRun& r) {
   wg_agg* a = r.agg;
   Ctx* ctx = a->ctx;
@@ -1002,7 +1009,7 @@ static wg_status run_device(const PipelineRun& r) {
   for (int kc : a->key_cols)
     if (kc >= 0 && kc < r.in->ncols && is_str_type(r.in->cols[kc].type_id))
       return fail(WG_E_UNSUPPORTED, a->key_cols.size() == 1
-                                        ? "a string GROUP BY key is taken by wg_agg_consume / wg_agg_consume_device"
+                                        ? "a string GROUP BY key of a windowed host pipeline run"
                                         : "a string column in a composite GROUP BY key is not on the GPU path");
   if (a->str_keyed >= 0 && a->str_keyed != (r.str_ids ? 1 : 0))
     return fail(WG_E_INVALID, "the GROUP BY column changed between a string and an integer type");
@@ -2260,8 +2267,30 @@ using namespace wg;
 
 namespace wg {
 // Access for the pipeline entry points (wg_pipeline.cu).
+// The aggregate's single string GROUP BY key in column `col` of `in` mapped to
+// its dictionary's ids (*out: the INT32 id column on the device).
+wg_status agg_map_str_key(wg_agg* a, const wg_batch_desc* in, int col, bool host, wg_column* out) {
+  if (a->finalized) return fail(WG_E_STATE, "aggregate already finalized");
+  return strdict_map(a->ctx, &a->sdict, in, col, host, a->hint, out);
+}
+int agg_str_key_col(wg_agg* a, const wg_batch_desc* in) { return str_key_col(a, in); }
+
 wg_status agg_run_device(wg_agg* a, const wg_batch_desc* in, int32_t nf, const wg_predicate* f, wg_join* j, int32_t ne,
-                         const wg_expr* e, bool defer_check) {
+                         const wg_expr* e, bool defer_check, bool str_ids) {
+  // a string key column of a device batch: its ids first, for every row the
+  // fused launch reads (rows its filters or join drop keep their strings in the
+  // dictionary without forming a group)
+  std::vector<wg_column> cols;
+  wg_batch_desc mapped;
+  const int sk = str_ids ? -1 : str_key_col(a, in);
+  if (sk >= 0) {
+    cols.assign(in->cols, in->cols + in->ncols);
+    WG_TRY(agg_map_str_key(a, in, sk, false, &cols[(size_t)sk]));
+    mapped = *in;
+    mapped.cols = cols.data();
+    in = &mapped;
+    str_ids = true;
+  }
   if (j && join_is_grace(j)) {
     // a partitioned build: one pass per group of its partitions, each probe row
     // taking part in the pass of its key's partition
@@ -2269,12 +2298,14 @@ wg_status agg_run_device(wg_agg* a, const wg_batch_desc* in, int32_t nf, const w
       wg_join* pj = nullptr;
       WG_TRY(join_grace_pass(j, g, &pj));
       PipelineRun r{a, in, nf, f, pj, ne, e};
+      r.str_ids = str_ids;
       WG_TRY(run_device(r));
     }
     return WG_OK;
   }
   PipelineRun r{a, in, nf, f, j, ne, e};
   r.defer_check = defer_check;
+  r.str_ids = str_ids;
   return run_device(r);
 }
 Ctx* agg_ctx(wg_agg* a) { return a->ctx; }
@@ -2310,13 +2341,6 @@ wg_status wg_agg_create(wg_ctx* ctx, int32_t n_keys, const int32_t* key_cols, in
   a->hint = group_ndv_hint;
   *out = a;
   return WG_OK;
-}
-
-// The batch column holding the aggregate's single string GROUP BY key, or -1.
-static int str_key_col(const wg_agg* a, const wg_batch_desc* in) {
-  if (a->key_cols.size() != 1 || in->ncols < 0 || (in->ncols > 0 && !in->cols)) return -1;
-  const int kc = a->key_cols[0];
-  return kc >= 0 && kc < in->ncols && is_str_type(in->cols[kc].type_id) ? kc : -1;
 }
 
 wg_status wg_agg_consume_device(wg_agg* a, const wg_batch_desc* in) {

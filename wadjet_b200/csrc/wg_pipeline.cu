@@ -14,8 +14,10 @@
 
 namespace wg {
 wg_status agg_run_device(wg_agg* a, const wg_batch_desc* in, int32_t nf, const wg_predicate* f, wg_join* j, int32_t ne,
-                         const wg_expr* e, bool defer_check = false);
+                         const wg_expr* e, bool defer_check = false, bool str_ids = false);
 Ctx* agg_ctx(wg_agg* a);
+int agg_str_key_col(wg_agg* a, const wg_batch_desc* in);
+wg_status agg_map_str_key(wg_agg* a, const wg_batch_desc* in, int col, bool host, wg_column* out);
 }  // namespace wg
 
 using namespace wg;
@@ -59,11 +61,14 @@ wg_status wg_pipeline_run(wg_ctx* ctx, const wg_pipeline_desc* p) {
   WG_TRY(ensure_device(ctx));
   const wg_batch_desc* in = p->input;
   if (in->ncols < 0 || (in->ncols > 0 && !in->cols)) return fail(WG_E_INVALID, "bad batch descriptor");
-  if (in->sel) {
-    // a selected host batch is staged whole
+  const int sk = agg_str_key_col(p->agg, in);
+  if (in->sel || sk >= 0) {
+    // a selected host batch is staged whole, and so is one grouped by a string
+    // column (its dictionary maps the column before the fused launch)
     StagedBatch sb;
     WG_TRY(stage_batch(ctx, in, &sb));
-    WG_TRY(agg_run_device(p->agg, &sb.desc, p->n_filters, p->filters, p->join, p->n_exprs, p->exprs));
+    if (sk >= 0) WG_TRY(agg_map_str_key(p->agg, in, sk, true, &sb.cols[(size_t)sk]));
+    WG_TRY(agg_run_device(p->agg, &sb.desc, p->n_filters, p->filters, p->join, p->n_exprs, p->exprs, false, sk >= 0));
     WG_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     return WG_OK;
   }

@@ -139,9 +139,10 @@ __global__ void str_hash_kernel(StrSrc s, U128* hashes, uint32_t* sketch) {
 // (1b) Find or install each non-NULL item's hash: rowslot[i] = its slot, -1 for
 // a NULL string, -2 when the probe passed kProbeLimit slots (ctr[1] is then
 // raised and the host grows the table and runs the pass again). ctr[0] counts
-// the installs, added once per CTA.
+// the installs, added once per CTA. (2) The items of a slot with no id yet
+// elect the lowest of them (rep).
 __global__ void str_insert_kernel(const U128* hashes, int64_t n, unsigned long long* slots, uint64_t mask,
-                                  int32_t* rowslot, unsigned long long* ctr) {
+                                  int32_t* rowslot, uint32_t* rep, unsigned long long* ctr) {
   __shared__ unsigned int installs;
   if (threadIdx.x == 0) installs = 0;
   __syncthreads();
@@ -167,75 +168,108 @@ __global__ void str_insert_kernel(const U128* hashes, int64_t n, unsigned long l
       }
       idx = (idx + 1) & mask;
     }
-    if (found == -2) ctr[1] = 1;
+    if (found == -2) {
+      ctr[1] = 1;
+    } else if (slots[(int64_t)found * 4 + 2] == kNoId && *(volatile uint32_t*)(rep + found) > (uint32_t)i) {
+      // a string new in this batch: its lowest item represents it (the atomic
+      // only when it can lower the candidate, so a frequent string's rows do
+      // not all hit one word)
+      atomicMin(rep + found, (uint32_t)i);
+    }
     rowslot[i] = found;
   }
   __syncthreads();
   if (threadIdx.x == 0 && installs != 0) atomicAdd(ctr, (unsigned long long)installs);
 }
 
-// (2) The lowest item of each slot that has no id yet.
-__global__ void str_elect_kernel(int64_t n, const unsigned long long* slots, const int32_t* rowslot, uint32_t* rep) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const int32_t sl = rowslot[i];
-    if (sl < 0) continue;
-    // the atomic only when it can lower the slot's candidate: rows of a
-    // frequent string would otherwise all hit one word
-    if (slots[(int64_t)sl * 4 + 2] == kNoId && *(volatile uint32_t*)(rep + sl) > (uint32_t)i)
-      atomicMin(rep + sl, (uint32_t)i);
-  }
-}
-
-// (3a) Each elected item's (1 id, its length) packed as 1 << 32 | length, so one
-// exclusive scan gives both its id and its arena offset in item order (a
-// batch's bytes stay below 2^32: its offsets are 32-bit).
-__global__ void str_flag_kernel(StrSrc s, const int32_t* rowslot, const uint32_t* rep, unsigned long long* pack) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < s.n; i += (int64_t)gridDim.x * blockDim.x) {
-    const int32_t sl = rowslot[i];
-    unsigned long long v = 0;
-    if (sl >= 0 && rep[sl] == (uint32_t)i) {
-      const int64_t row = item_row(s, i);
-      v = (1ULL << 32) | (unsigned long long)(s.offs[row + 1] - s.offs[row]);
+// (3) Every item checks its bytes: a string new in this batch against its
+// representative item's, an older one against the arena. The representatives
+// append their item index to `list` and their length to ctr[3] (ctr[2] counts
+// them), one atomic pair per warp.
+__global__ void str_collect_kernel(StrSrc s, const unsigned long long* slots, const int32_t* rowslot,
+                                   const uint32_t* rep, const uint8_t* arena, uint32_t* list,
+                                   unsigned long long* ctr, int32_t* err) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x; i0 < s.n; i0 += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = i0 + threadIdx.x;
+    bool mine = false;
+    uint32_t len = 0;
+    if (i < s.n) {
+      const int32_t sl = rowslot[i];
+      if (sl >= 0) {
+        const int64_t row = item_row(s, i);
+        const uint32_t b0 = s.offs[row];
+        len = s.offs[row + 1] - b0;
+        // the table, the representatives and the arena are read-only here
+        const unsigned long long id = __ldg(slots + (int64_t)sl * 4 + 2);
+        bool same = true;
+        if (id == kNoId) {
+          const uint32_t r = __ldg(rep + sl);
+          mine = r == (uint32_t)i;
+          if (!mine) {
+            const int64_t rrow = item_row(s, (int64_t)r);
+            const uint32_t r0 = s.offs[rrow];
+            same = s.offs[rrow + 1] - r0 == len && bytes_equal(s.bytes + b0, s.bytes + r0, len);
+          }
+        } else {
+          const unsigned long long loc = __ldg(slots + (int64_t)sl * 4 + 3);
+          same = (uint32_t)(loc >> kLenShift) == len &&
+                 bytes_equal(s.bytes + b0, arena + (loc & ((1ULL << kLenShift) - 1)), len);
+        }
+        if (!same) set_error(err, WG_DERR_HASH_COLLISION);
+      }
     }
-    pack[i] = v;
+    // every lane of the warp reaches this point once per step of the loop
+    const unsigned m = __ballot_sync(0xFFFFFFFFu, mine);
+    if (m != 0) {
+      const unsigned long long bytes = __reduce_add_sync(0xFFFFFFFFu, mine ? len : 0u);
+      unsigned long long base = 0;
+      const int leader = __ffs(m) - 1;
+      if (lane == leader) {
+        base = atomicAdd(ctr + 2, (unsigned long long)__popc(m));
+        atomicAdd(ctr + 3, bytes);
+      }
+      base = __shfl_sync(0xFFFFFFFFu, base, leader);
+      if (mine) list[base + __popc(m & ((1u << lane) - 1u))] = (uint32_t)i;
+    }
   }
 }
 
-// (3b) The elected item takes its id (first appearance order, as the
-// reference's group indexes) and stores its string.
-__global__ void str_assign_kernel(StrSrc s, unsigned long long* slots, const int32_t* rowslot, uint32_t* rep,
-                                  const unsigned long long* pre, unsigned long long id0, unsigned long long off0,
-                                  uint8_t* arena, unsigned long long* id_loc) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < s.n; i += (int64_t)gridDim.x * blockDim.x) {
+// (4a) The length of each new string, in item order (list sorted).
+__global__ void str_len_kernel(StrSrc s, const uint32_t* list, int64_t k, unsigned long long* lens) {
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < k; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t row = item_row(s, (int64_t)list[t]);
+    lens[t] = s.offs[row + 1] - s.offs[row];
+  }
+}
+
+// (4b) The t-th new string (by first appearance) takes id id0 + t and its
+// bytes go to the arena at off0 + pre[t].
+__global__ void str_assign_kernel(StrSrc s, const uint32_t* list, int64_t k, const unsigned long long* pre,
+                                  unsigned long long* slots, const int32_t* rowslot, uint32_t* rep,
+                                  unsigned long long id0, unsigned long long off0, uint8_t* arena,
+                                  unsigned long long* id_loc) {
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < k; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = (int64_t)list[t];
     const int32_t sl = rowslot[i];
-    if (sl < 0 || rep[sl] != (uint32_t)i) continue;
     const int64_t row = item_row(s, i);
     const uint32_t b0 = s.offs[row], len = s.offs[row + 1] - b0;
-    const unsigned long long id = id0 + (pre[i] >> 32);
-    const unsigned long long off = off0 + (pre[i] & 0xFFFFFFFFULL);
-    for (uint32_t k = 0; k < len; ++k) arena[off + k] = s.bytes[b0 + k];
+    const unsigned long long off = off0 + pre[t];
+    for (uint32_t q = 0; q < len; ++q) arena[off + q] = s.bytes[b0 + q];
     const unsigned long long loc = off | ((unsigned long long)len << kLenShift);
-    id_loc[id] = loc;
+    id_loc[id0 + t] = loc;
     slots[(int64_t)sl * 4 + 3] = loc;
-    slots[(int64_t)sl * 4 + 2] = id;
+    slots[(int64_t)sl * 4 + 2] = id0 + t;
     rep[sl] = kNoRep;
   }
 }
 
-// (4) Every item checks its bytes against its slot's string and takes the id
-// (ids are indexed by row; rows outside the selection are not written).
-__global__ void str_gid_kernel(StrSrc s, const unsigned long long* slots, const int32_t* rowslot, const uint8_t* arena,
-                               int32_t* gid, int32_t* err) {
+// (5) Every item's id (ids are indexed by row; rows outside the selection are
+// not written; a NULL string's row gets 0 under its NULL bit).
+__global__ void str_gid_kernel(StrSrc s, const unsigned long long* slots, const int32_t* rowslot, int32_t* gid) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < s.n; i += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t row = item_row(s, i);
     const int32_t sl = rowslot[i];
-    if (sl < 0) { gid[row] = 0; continue; }
-    const unsigned long long loc = slots[(int64_t)sl * 4 + 3];
-    const unsigned long long off = loc & ((1ULL << kLenShift) - 1);
-    const uint32_t len = (uint32_t)(loc >> kLenShift);
-    const uint32_t b0 = s.offs[row], n = s.offs[row + 1] - b0;
-    if (n != len || !bytes_equal(s.bytes + b0, arena + off, n)) set_error(err, WG_DERR_HASH_COLLISION);
-    gid[row] = (int32_t)slots[(int64_t)sl * 4 + 2];
+    gid[item_row(s, i)] = sl < 0 ? 0 : (int32_t)__ldg(slots + (int64_t)sl * 4 + 2);
   }
 }
 
@@ -270,16 +304,12 @@ __global__ void str_init_slots_kernel(unsigned long long* slots, uint64_t cap) {
   }
 }
 
-// ctr[0] = the slots in use, ctr[1] = 0 (not full)
+// ctr[0] = the slots in use, ctr[1] = 0 (not full), ctr[2..3] = 0 (new strings, their bytes)
 __global__ void str_ctr_kernel(unsigned long long* ctr, unsigned long long used) {
   ctr[0] = used;
   ctr[1] = 0;
-}
-
-// ctr[2] = the scan's total: new ids << 32 | their bytes
-__global__ void str_total_kernel(const unsigned long long* pre, const unsigned long long* pack, int64_t n,
-                                 unsigned long long* ctr) {
-  ctr[2] = pre[n - 1] + pack[n - 1];
+  ctr[2] = 0;
+  ctr[3] = 0;
 }
 
 }  // namespace
@@ -291,7 +321,8 @@ struct StrDict {
   uint64_t cap = 0;                 // table slots (a power of two)
   int64_t n_ids = 0, used = 0;      // distinct strings and arena bytes
   int64_t slots_used = 0;           // installed hashes (n_ids after every complete batch)
-  DevBuf hashes, sketch, rowslot, pack, pre, scan_tmp, gid;  // per-batch scratch
+  DevBuf hashes, sketch, rowslot, list, sorted, pack, pre, scan_tmp, gid;  // per-batch scratch
+  bool dirty = false;               // a batch stopped part way: representatives to clear
   DevBuf h_offs, h_bytes, h_valid, h_sel;             // a host batch's string column on the device
   std::vector<unsigned long long> loc_host;           // host copies for wg_agg_key_strings,
   std::vector<uint8_t> arena_host;                    // valid while no batch came since
@@ -370,7 +401,7 @@ void strdict_reset(StrDict* d, Ctx* ctx) {
     ctx->count_launch();
     cudaMemsetAsync(d->rep.get(), 0xFF, (size_t)d->cap * 4, ctx->stream);
   }
-  d->n_ids = 0; d->used = 0; d->slots_used = 0;
+  d->n_ids = 0; d->used = 0; d->slots_used = 0; d->dirty = false;
   d->loc_host.clear(); d->arena_host.clear(); d->host_fresh = false;
 }
 
@@ -437,11 +468,14 @@ wg_status strdict_map(Ctx* ctx, StrDict** dp, const wg_batch_desc* in, int col, 
   WG_TRY(sketch_estimate(ctx, d, &est));
   const uint64_t want = pow2_at_least((uint64_t)(1.5 * ((double)d->slots_used + std::min<double>((double)n, est * 1.1)) + 64));
   if (d->cap < want) WG_TRY(str_table(ctx, d, want));
+  else if (d->dirty) WG_CUDA_TRY(cudaMemsetAsync(d->rep.get(), 0xFF, (size_t)d->cap * 4, ctx->stream));
+  d->dirty = true;  // until the batch completes
   int64_t cv[4] = {0, 0, 0, 0};
   for (int pass = 0;; ++pass) {
     str_ctr_kernel<<<1, 1, 0, ctx->stream>>>(ctr, (unsigned long long)d->slots_used);
     str_insert_kernel<<<grid, 256, 0, ctx->stream>>>(d->hashes.as<U128>(), n, d->slots.as<unsigned long long>(),
-                                                     d->cap - 1, d->rowslot.as<int32_t>(), ctr);
+                                                     d->cap - 1, d->rowslot.as<int32_t>(), d->rep.as<uint32_t>(),
+                                                     ctr);
     ctx->count_launch(2);
     WG_CUDA_TRY(cudaGetLastError());
     WG_TRY(read_back_i64(ctx, reinterpret_cast<int64_t*>(ctr), cv, 2));
@@ -452,41 +486,57 @@ wg_status strdict_map(Ctx* ctx, StrDict** dp, const wg_batch_desc* in, int col, 
   }
   d->slots_used = cv[0];
 
-  // (2)-(3) ids and arena offsets of the strings new in this batch, in item order
-  WG_TRY(d->pack.ensure(ctx, n * 8));
-  WG_TRY(d->pre.ensure(ctx, n * 8));
-  size_t tmp = 0;
-  WG_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tmp, d->pack.as<unsigned long long>(),
-                                            d->pre.as<unsigned long long>(), (int)n, ctx->stream));
-  WG_TRY(d->scan_tmp.ensure(ctx, std::max<int64_t>((int64_t)tmp, 16)));
-  str_elect_kernel<<<grid, 256, 0, ctx->stream>>>(n, d->slots.as<unsigned long long>(), d->rowslot.as<int32_t>(),
-                                                  d->rep.as<uint32_t>());
-  str_flag_kernel<<<grid, 256, 0, ctx->stream>>>(s, d->rowslot.as<int32_t>(), d->rep.as<uint32_t>(),
-                                                 d->pack.as<unsigned long long>());
-  ctx->count_launch(2);
-  WG_CUDA_TRY(cub::DeviceScan::ExclusiveSum(d->scan_tmp.get(), tmp, d->pack.as<unsigned long long>(),
-                                            d->pre.as<unsigned long long>(), (int)n, ctx->stream));
-  str_total_kernel<<<1, 1, 0, ctx->stream>>>(d->pre.as<unsigned long long>(), d->pack.as<unsigned long long>(), n, ctr);
-  ctx->count_launch(3);  // the scan's two kernels and the total
+  // (3) every item's bytes checked; the new strings' representatives listed
+  // with their total length
+  WG_TRY(d->list.ensure(ctx, std::max<int64_t>(n * 4, 16)));
+  str_collect_kernel<<<grid, 256, 0, ctx->stream>>>(s, d->slots.as<unsigned long long>(), d->rowslot.as<int32_t>(),
+                                                    d->rep.as<uint32_t>(), d->arena.as<uint8_t>(),
+                                                    d->list.as<uint32_t>(), ctr, ctx->dev_error);
+  ctx->count_launch();
   WG_CUDA_TRY(cudaGetLastError());
-  WG_TRY(read_back_i64(ctx, reinterpret_cast<int64_t*>(ctr), cv, 3));
-  const int64_t new_ids = (int64_t)((unsigned long long)cv[2] >> 32);
-  const int64_t new_bytes = (int64_t)((unsigned long long)cv[2] & 0xFFFFFFFFULL);
+  WG_TRY(read_back_checked(ctx, reinterpret_cast<int64_t*>(ctr), cv, 4));
+  const int64_t new_ids = cv[2], new_bytes = cv[3];
   if (d->n_ids + new_ids >= (int64_t)INT32_MAX) return fail(WG_E_UNSUPPORTED, "more than 2^31 - 1 distinct strings");
-  WG_TRY(grow_keep(ctx, d->arena, d->used, std::max<int64_t>(d->used + new_bytes, 16)));
-  WG_TRY(grow_keep(ctx, d->id_loc, d->n_ids * 8, std::max<int64_t>((d->n_ids + new_ids) * 8, 16)));
-  str_assign_kernel<<<grid, 256, 0, ctx->stream>>>(s, d->slots.as<unsigned long long>(), d->rowslot.as<int32_t>(),
-                                                   d->rep.as<uint32_t>(), d->pre.as<unsigned long long>(),
-                                                   (unsigned long long)d->n_ids, (unsigned long long)d->used,
-                                                   d->arena.as<uint8_t>(), d->id_loc.as<unsigned long long>());
-  // (4) every item's id, its bytes checked against the stored string
+  if (new_ids > 0) {
+    // (4) the new strings in first-appearance order (their items sorted), ids
+    // and arena offsets from a scan of their lengths
+    WG_TRY(grow_keep(ctx, d->arena, d->used, std::max<int64_t>(d->used + new_bytes, 16)));
+    WG_TRY(grow_keep(ctx, d->id_loc, d->n_ids * 8, std::max<int64_t>((d->n_ids + new_ids) * 8, 16)));
+    WG_TRY(d->sorted.ensure(ctx, new_ids * 4));
+    WG_TRY(d->pack.ensure(ctx, new_ids * 8));
+    WG_TRY(d->pre.ensure(ctx, new_ids * 8));
+    int bits = 1;
+    while (bits < 32 && (int64_t(1) << bits) < n) ++bits;
+    size_t t1 = 0, t2 = 0;
+    WG_CUDA_TRY(cub::DeviceRadixSort::SortKeys(nullptr, t1, d->list.as<uint32_t>(), d->sorted.as<uint32_t>(),
+                                               (int)new_ids, 0, bits, ctx->stream));
+    WG_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, t2, d->pack.as<unsigned long long>(),
+                                              d->pre.as<unsigned long long>(), (int)new_ids, ctx->stream));
+    WG_TRY(d->scan_tmp.ensure(ctx, std::max<int64_t>((int64_t)std::max(t1, t2), 16)));
+    WG_CUDA_TRY(cub::DeviceRadixSort::SortKeys(d->scan_tmp.get(), t1, d->list.as<uint32_t>(), d->sorted.as<uint32_t>(),
+                                               (int)new_ids, 0, bits, ctx->stream));
+    const unsigned kgrid = str_grid(ctx, new_ids, 256);
+    str_len_kernel<<<kgrid, 256, 0, ctx->stream>>>(s, d->sorted.as<uint32_t>(), new_ids,
+                                                   d->pack.as<unsigned long long>());
+    WG_CUDA_TRY(cub::DeviceScan::ExclusiveSum(d->scan_tmp.get(), t2, d->pack.as<unsigned long long>(),
+                                              d->pre.as<unsigned long long>(), (int)new_ids, ctx->stream));
+    str_assign_kernel<<<kgrid, 256, 0, ctx->stream>>>(s, d->sorted.as<uint32_t>(), new_ids,
+                                                      d->pre.as<unsigned long long>(), d->slots.as<unsigned long long>(),
+                                                      d->rowslot.as<int32_t>(), d->rep.as<uint32_t>(),
+                                                      (unsigned long long)d->n_ids, (unsigned long long)d->used,
+                                                      d->arena.as<uint8_t>(), d->id_loc.as<unsigned long long>());
+    ctx->count_launch(2 + 2 + 2);  // the sort's and the scan's kernels (about two each), lengths, assignment
+    WG_CUDA_TRY(cudaGetLastError());
+  }
+  // (5) every item's id
   str_gid_kernel<<<grid, 256, 0, ctx->stream>>>(s, d->slots.as<unsigned long long>(), d->rowslot.as<int32_t>(),
-                                                d->arena.as<uint8_t>(), d->gid.as<int32_t>(), ctx->dev_error);
-  ctx->count_launch(2);
+                                                d->gid.as<int32_t>());
+  ctx->count_launch();
   WG_CUDA_TRY(cudaGetLastError());
   d->n_ids += new_ids;
   d->used += new_bytes;
-  return check_device_error(ctx);
+  d->dirty = false;
+  return WG_OK;
 }
 
 wg_status strdict_strings(Ctx* ctx, StrDict* d, const int64_t* ids, int64_t n, uint32_t* out_offsets,
