@@ -590,7 +590,7 @@ def run_strgroup(args):
         agg.consume(hbatch)
         got[0] = agg.finalize()
 
-    e2e_ms = _timed_ms(stream, e2e_step, args.e2e_steps, 1)
+    e2e_ms = _timed_ms(stream, e2e_step, args.e2e_steps, 1) if args.e2e_steps > 0 else None
     sample = min(n, 1 << 22)
     cpu = None if args.no_cpu_baseline else {
         "value": cpu_strgroup_sample(h_offs[:sample + 1].astype(np.int64), h_raw, h_v[:sample]), "unit": "rows/s",
@@ -600,8 +600,8 @@ def run_strgroup(args):
                       "bytes": total, "value": n / (ms / 1e3), "unit": "rows/s", "ms_per_step": ms,
                       "hbm_gbs": alg / (ms / 1e3) / 1e9, "frac_of_peak": alg / (ms / 1e3) / 1e9 / peak,
                       "peak_kind": peak_kind_note(kind), "algorithmic_bytes": alg, "gpu_launches": launches,
-                      "e2e": {"value": n / (e2e_ms / 1e3), "unit": "rows/s", "h2d_bytes_per_step": alg,
-                              "d2h_bytes_per_step": 8},
+                      "e2e": None if e2e_ms is None else {"value": n / (e2e_ms / 1e3), "unit": "rows/s",
+                                                          "h2d_bytes_per_step": alg, "d2h_bytes_per_step": 8},
                       "clocks": clocks, "cpu_baseline": cpu}), flush=True)
     agg.close()
     ctx.close()

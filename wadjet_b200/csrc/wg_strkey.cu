@@ -182,13 +182,11 @@ __global__ void str_insert_kernel(const U128* hashes, int64_t n, unsigned long l
   if (threadIdx.x == 0 && installs != 0) atomicAdd(ctr, (unsigned long long)installs);
 }
 
-// (3) Every item checks its bytes: a string new in this batch against its
-// representative item's, an older one against the arena. The representatives
-// append their item index to `list` and their length to ctr[3] (ctr[2] counts
-// them), one atomic pair per warp.
+// (3) The representatives of the strings new in this batch append their item
+// index to `list` and their length to ctr[3] (ctr[2] counts them), one atomic
+// pair per warp.
 __global__ void str_collect_kernel(StrSrc s, const unsigned long long* slots, const int32_t* rowslot,
-                                   const uint32_t* rep, const uint8_t* arena, uint32_t* list,
-                                   unsigned long long* ctr, int32_t* err) {
+                                   const uint32_t* rep, uint32_t* list, unsigned long long* ctr) {
   const int lane = threadIdx.x & 31;
   for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x; i0 < s.n; i0 += (int64_t)gridDim.x * blockDim.x) {
     const int64_t i = i0 + threadIdx.x;
@@ -196,27 +194,11 @@ __global__ void str_collect_kernel(StrSrc s, const unsigned long long* slots, co
     uint32_t len = 0;
     if (i < s.n) {
       const int32_t sl = rowslot[i];
-      if (sl >= 0) {
+      // the table and the representatives are read-only here
+      if (sl >= 0 && __ldg(slots + (int64_t)sl * 4 + 2) == kNoId && __ldg(rep + sl) == (uint32_t)i) {
+        mine = true;
         const int64_t row = item_row(s, i);
-        const uint32_t b0 = s.offs[row];
-        len = s.offs[row + 1] - b0;
-        // the table, the representatives and the arena are read-only here
-        const unsigned long long id = __ldg(slots + (int64_t)sl * 4 + 2);
-        bool same = true;
-        if (id == kNoId) {
-          const uint32_t r = __ldg(rep + sl);
-          mine = r == (uint32_t)i;
-          if (!mine) {
-            const int64_t rrow = item_row(s, (int64_t)r);
-            const uint32_t r0 = s.offs[rrow];
-            same = s.offs[rrow + 1] - r0 == len && bytes_equal(s.bytes + b0, s.bytes + r0, len);
-          }
-        } else {
-          const unsigned long long loc = __ldg(slots + (int64_t)sl * 4 + 3);
-          same = (uint32_t)(loc >> kLenShift) == len &&
-                 bytes_equal(s.bytes + b0, arena + (loc & ((1ULL << kLenShift) - 1)), len);
-        }
-        if (!same) set_error(err, WG_DERR_HASH_COLLISION);
+        len = s.offs[row + 1] - s.offs[row];
       }
     }
     // every lane of the warp reaches this point once per step of the loop
@@ -264,12 +246,21 @@ __global__ void str_assign_kernel(StrSrc s, const uint32_t* list, int64_t k, con
   }
 }
 
-// (5) Every item's id (ids are indexed by row; rows outside the selection are
-// not written; a NULL string's row gets 0 under its NULL bit).
-__global__ void str_gid_kernel(StrSrc s, const unsigned long long* slots, const int32_t* rowslot, int32_t* gid) {
+// (5) Every item checks its bytes against its string's arena copy and takes
+// the id (ids are indexed by row; rows outside the selection are not written;
+// a NULL string's row gets 0 under its NULL bit).
+__global__ void str_gid_kernel(StrSrc s, const unsigned long long* slots, const int32_t* rowslot,
+                               const uint8_t* arena, int32_t* gid, int32_t* err) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < s.n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t row = item_row(s, i);
     const int32_t sl = rowslot[i];
-    gid[item_row(s, i)] = sl < 0 ? 0 : (int32_t)__ldg(slots + (int64_t)sl * 4 + 2);
+    if (sl < 0) { gid[row] = 0; continue; }
+    const unsigned long long loc = __ldg(slots + (int64_t)sl * 4 + 3);
+    const uint32_t len = (uint32_t)(loc >> kLenShift);
+    const uint32_t b0 = s.offs[row], n = s.offs[row + 1] - b0;
+    if (n != len || !bytes_equal(s.bytes + b0, arena + (loc & ((1ULL << kLenShift) - 1)), n))
+      set_error(err, WG_DERR_HASH_COLLISION);
+    gid[row] = (int32_t)__ldg(slots + (int64_t)sl * 4 + 2);
   }
 }
 
@@ -486,15 +477,13 @@ wg_status strdict_map(Ctx* ctx, StrDict** dp, const wg_batch_desc* in, int col, 
   }
   d->slots_used = cv[0];
 
-  // (3) every item's bytes checked; the new strings' representatives listed
-  // with their total length
+  // (3) the new strings' representatives listed with their total length
   WG_TRY(d->list.ensure(ctx, std::max<int64_t>(n * 4, 16)));
   str_collect_kernel<<<grid, 256, 0, ctx->stream>>>(s, d->slots.as<unsigned long long>(), d->rowslot.as<int32_t>(),
-                                                    d->rep.as<uint32_t>(), d->arena.as<uint8_t>(),
-                                                    d->list.as<uint32_t>(), ctr, ctx->dev_error);
+                                                    d->rep.as<uint32_t>(), d->list.as<uint32_t>(), ctr);
   ctx->count_launch();
   WG_CUDA_TRY(cudaGetLastError());
-  WG_TRY(read_back_checked(ctx, reinterpret_cast<int64_t*>(ctr), cv, 4));
+  WG_TRY(read_back_i64(ctx, reinterpret_cast<int64_t*>(ctr), cv, 4));
   const int64_t new_ids = cv[2], new_bytes = cv[3];
   if (d->n_ids + new_ids >= (int64_t)INT32_MAX) return fail(WG_E_UNSUPPORTED, "more than 2^31 - 1 distinct strings");
   if (new_ids > 0) {
@@ -528,15 +517,15 @@ wg_status strdict_map(Ctx* ctx, StrDict** dp, const wg_batch_desc* in, int col, 
     ctx->count_launch(2 + 2 + 2);  // the sort's and the scan's kernels (about two each), lengths, assignment
     WG_CUDA_TRY(cudaGetLastError());
   }
-  // (5) every item's id
+  // (5) every item's bytes checked against its string's arena copy, and its id
   str_gid_kernel<<<grid, 256, 0, ctx->stream>>>(s, d->slots.as<unsigned long long>(), d->rowslot.as<int32_t>(),
-                                                d->gid.as<int32_t>());
+                                                d->arena.as<uint8_t>(), d->gid.as<int32_t>(), ctx->dev_error);
   ctx->count_launch();
   WG_CUDA_TRY(cudaGetLastError());
   d->n_ids += new_ids;
   d->used += new_bytes;
   d->dirty = false;
-  return WG_OK;
+  return check_device_error(ctx);
 }
 
 wg_status strdict_strings(Ctx* ctx, StrDict* d, const int64_t* ids, int64_t n, uint32_t* out_offsets,
