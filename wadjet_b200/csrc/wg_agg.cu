@@ -1397,7 +1397,10 @@ static wg_status run_partitioned(const PipelineRun& r, const wgd::Plan& P0, cons
   wg_agg* a = r.agg;
   Ctx* ctx = a->ctx;
   const int64_t n = P0.n_items;
-  if (env_int("WG_AGG_PARTITION", 1) == 0 || r.join || P0.sel || a->L.key_words == 0 || n < (int64_t(1) << 22))
+  // a string dictionary's ids are dense and its table small per id: the
+  // reorder does not pay for them (2.85 against 3.28 ms at 2^24 rows, 2^20 ids)
+  if (env_int("WG_AGG_PARTITION", 1) == 0 || r.join || r.str_ids || P0.sel || a->L.key_words == 0 ||
+      n < (int64_t(1) << 22))
     return WG_OK;
   for (int j = 0; j < P0.n_in; ++j)
     if (P0.in[j].valid) return WG_OK;

@@ -13,13 +13,14 @@
 // with one 16-byte compare-and-swap, plus an arena holding each distinct
 // string once. Per batch: (1) a hash pass writes every row's hash and sketches
 // the batch's distinct strings, the table is sized from the sketch and every
-// row finds or installs its hash; (2) the rows of slots installed in this batch
-// elect the lowest row; (3) a scan over the elected rows gives each new string
-// its id and arena offset in row order, and its row copies the bytes; (4) every
-// row compares its bytes with its slot's stored string and takes the id. A
-// 128-bit collision between two different strings would make (4) fail, which
-// the call reports instead of merging the groups. No step waits on another
-// thread.
+// row finds or installs its hash, each install listing its slot; (2) in the
+// same pass the rows of a slot with no id yet elect its lowest row; (3) the
+// list, sorted by those rows, gives each new string its id in first-appearance
+// order and (by a scan of the lengths) its arena offset, and the elected row
+// copies the bytes; (4) every row compares its bytes with its string's arena
+// copy and takes the id. A 128-bit collision between two different strings
+// would make (4) fail, which the call reports instead of merging the groups.
+// No step waits on another thread.
 #include "wg_internal.h"
 #include "wg_device.cuh"
 
@@ -104,6 +105,19 @@ __device__ __forceinline__ bool bytes_equal(const uint8_t* p, const uint8_t* q, 
   return true;
 }
 
+// Append `v` for the lanes with `mine` set to list[ctr[2]...], one atomic per
+// warp. Every lane of the warp calls it together.
+__device__ __forceinline__ void warp_append(bool mine, uint32_t v, uint32_t* list, unsigned long long* count) {
+  const unsigned m = __ballot_sync(0xFFFFFFFFu, mine);
+  if (m == 0) return;
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(m) - 1;
+  unsigned long long base = 0;
+  if (lane == leader) base = atomicAdd(count, (unsigned long long)__popc(m));
+  base = __shfl_sync(0xFFFFFFFFu, base, leader);
+  if (mine) list[base + __popc(m & ((1u << lane) - 1u))] = v;
+}
+
 // Distinct-hash sketch of a batch (HyperLogLog, Flajolet, Fusy, Gandouet and
 // Meunier 2007): 2^kSketchBits registers, each the largest rank (leading zeros
 // + 1) of the hashes that fall in it. It sizes the table before the insert
@@ -139,101 +153,90 @@ __global__ void str_hash_kernel(StrSrc s, U128* hashes, uint32_t* sketch) {
 // (1b) Find or install each non-NULL item's hash: rowslot[i] = its slot, -1 for
 // a NULL string, -2 when the probe passed kProbeLimit slots (ctr[1] is then
 // raised and the host grows the table and runs the pass again). ctr[0] counts
-// the installs, added once per CTA. (2) The items of a slot with no id yet
-// elect the lowest of them (rep).
+// the installs (added once per CTA); each install appends its slot to `list`
+// (ctr[2] counts them). (2) The items of a slot with no id yet elect the
+// lowest of them (rep).
 __global__ void str_insert_kernel(const U128* hashes, int64_t n, unsigned long long* slots, uint64_t mask,
-                                  int32_t* rowslot, uint32_t* rep, unsigned long long* ctr) {
+                                  int32_t* rowslot, uint32_t* rep, uint32_t* list, unsigned long long* ctr) {
   __shared__ unsigned int installs;
   if (threadIdx.x == 0) installs = 0;
   __syncthreads();
   const uint64_t limit = mask < (uint64_t)kProbeLimit ? mask + 1 : (uint64_t)kProbeLimit;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const U128 k = hashes[i];
-    if (k.lo == kEmpty && k.hi == kEmpty) { rowslot[i] = -1; continue; }
-    uint64_t idx = (k.lo ^ (k.lo >> 32)) & mask;
-    int32_t found = -2;
-    for (uint64_t probe = 0; probe < limit; ++probe) {
-      unsigned long long* sl = slots + idx * 4;
-      const U128 cur = read128(sl);
-      if (cur.lo == k.lo && cur.hi == k.hi) { found = (int32_t)idx; break; }
-      if (cur.lo == kEmpty || cur.hi == kEmpty) {  // empty, or a key being installed
-        U128 e; e.lo = kEmpty; e.hi = kEmpty;
-        const U128 old = cas128((U128*)sl, e, k);
-        if (old.lo == e.lo && old.hi == e.hi) {
-          atomicAdd(&installs, 1u);
-          found = (int32_t)idx;
-          break;
+  // the loop's trip count is the same for every lane of a warp (warp_append)
+  for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x; i0 < n; i0 += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = i0 + threadIdx.x;
+    bool installed = false;
+    int32_t found = -1;
+    if (i < n) {
+      const U128 k = hashes[i];
+      if (!(k.lo == kEmpty && k.hi == kEmpty)) {
+        uint64_t idx = (k.lo ^ (k.lo >> 32)) & mask;
+        found = -2;
+        for (uint64_t probe = 0; probe < limit; ++probe) {
+          unsigned long long* sl = slots + idx * 4;
+          const U128 cur = read128(sl);
+          if (cur.lo == k.lo && cur.hi == k.hi) { found = (int32_t)idx; break; }
+          if (cur.lo == kEmpty || cur.hi == kEmpty) {  // empty, or a key being installed
+            U128 e; e.lo = kEmpty; e.hi = kEmpty;
+            const U128 old = cas128((U128*)sl, e, k);
+            if (old.lo == e.lo && old.hi == e.hi) {
+              installed = true;
+              found = (int32_t)idx;
+              break;
+            }
+            if (old.lo == k.lo && old.hi == k.hi) { found = (int32_t)idx; break; }
+          }
+          idx = (idx + 1) & mask;
         }
-        if (old.lo == k.lo && old.hi == k.hi) { found = (int32_t)idx; break; }
+        if (found == -2) {
+          ctr[1] = 1;
+        } else if (slots[(int64_t)found * 4 + 2] == kNoId && *(volatile uint32_t*)(rep + found) > (uint32_t)i) {
+          // a string new in this batch: its lowest item represents it (the
+          // atomic only when it can lower the candidate, so a frequent
+          // string's rows do not all hit one word)
+          atomicMin(rep + found, (uint32_t)i);
+        }
       }
-      idx = (idx + 1) & mask;
+      rowslot[i] = found;
     }
-    if (found == -2) {
-      ctr[1] = 1;
-    } else if (slots[(int64_t)found * 4 + 2] == kNoId && *(volatile uint32_t*)(rep + found) > (uint32_t)i) {
-      // a string new in this batch: its lowest item represents it (the atomic
-      // only when it can lower the candidate, so a frequent string's rows do
-      // not all hit one word)
-      atomicMin(rep + found, (uint32_t)i);
-    }
-    rowslot[i] = found;
+    if (installed) atomicAdd(&installs, 1u);
+    warp_append(installed, (uint32_t)found, list, ctr + 2);
   }
   __syncthreads();
   if (threadIdx.x == 0 && installs != 0) atomicAdd(ctr, (unsigned long long)installs);
 }
 
-// (3) The representatives of the strings new in this batch append their item
-// index to `list` and their length to ctr[3] (ctr[2] counts them), one atomic
-// pair per warp.
-__global__ void str_collect_kernel(StrSrc s, const unsigned long long* slots, const int32_t* rowslot,
-                                   const uint32_t* rep, uint32_t* list, unsigned long long* ctr) {
-  const int lane = threadIdx.x & 31;
-  for (int64_t i0 = (int64_t)blockIdx.x * blockDim.x; i0 < s.n; i0 += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t i = i0 + threadIdx.x;
-    bool mine = false;
-    uint32_t len = 0;
-    if (i < s.n) {
-      const int32_t sl = rowslot[i];
-      // the table and the representatives are read-only here
-      if (sl >= 0 && __ldg(slots + (int64_t)sl * 4 + 2) == kNoId && __ldg(rep + sl) == (uint32_t)i) {
-        mine = true;
-        const int64_t row = item_row(s, i);
-        len = s.offs[row + 1] - s.offs[row];
-      }
-    }
-    // every lane of the warp reaches this point once per step of the loop
-    const unsigned m = __ballot_sync(0xFFFFFFFFu, mine);
-    if (m != 0) {
-      const unsigned long long bytes = __reduce_add_sync(0xFFFFFFFFu, mine ? len : 0u);
-      unsigned long long base = 0;
-      const int leader = __ffs(m) - 1;
-      if (lane == leader) {
-        base = atomicAdd(ctr + 2, (unsigned long long)__popc(m));
-        atomicAdd(ctr + 3, bytes);
-      }
-      base = __shfl_sync(0xFFFFFFFFu, base, leader);
-      if (mine) list[base + __popc(m & ((1u << lane) - 1u))] = (uint32_t)i;
-    }
+// (3) Sort keys of the strings new in this batch: the slot above its
+// representative item, so sorting by the low bits gives first-appearance order.
+__global__ void str_key_kernel(const uint32_t* list, int64_t k, const uint32_t* rep, unsigned long long* keys) {
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < k; t += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t sl = list[t];
+    keys[t] = ((unsigned long long)sl << 32) | rep[sl];
   }
 }
 
-// (4a) The length of each new string, in item order (list sorted).
-__global__ void str_len_kernel(StrSrc s, const uint32_t* list, int64_t k, unsigned long long* lens) {
+// The new strings' total length (the last length plus the last offset).
+__global__ void str_bytes_kernel(const unsigned long long* lens, const unsigned long long* pre, int64_t k,
+                                 unsigned long long* ctr) {
+  ctr[3] = lens[k - 1] + pre[k - 1];
+}
+
+// (4a) The length of each new string, in first-appearance order (keys sorted).
+__global__ void str_len_kernel(StrSrc s, const unsigned long long* keys, int64_t k, unsigned long long* lens) {
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < k; t += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t row = item_row(s, (int64_t)list[t]);
+    const int64_t row = item_row(s, (int64_t)(keys[t] & 0xFFFFFFFFULL));
     lens[t] = s.offs[row + 1] - s.offs[row];
   }
 }
 
 // (4b) The t-th new string (by first appearance) takes id id0 + t and its
 // bytes go to the arena at off0 + pre[t].
-__global__ void str_assign_kernel(StrSrc s, const uint32_t* list, int64_t k, const unsigned long long* pre,
-                                  unsigned long long* slots, const int32_t* rowslot, uint32_t* rep,
-                                  unsigned long long id0, unsigned long long off0, uint8_t* arena,
-                                  unsigned long long* id_loc) {
+__global__ void str_assign_kernel(StrSrc s, const unsigned long long* keys, int64_t k, const unsigned long long* pre,
+                                  unsigned long long* slots, uint32_t* rep, unsigned long long id0,
+                                  unsigned long long off0, uint8_t* arena, unsigned long long* id_loc) {
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < k; t += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t i = (int64_t)list[t];
-    const int32_t sl = rowslot[i];
+    const int64_t i = (int64_t)(keys[t] & 0xFFFFFFFFULL);
+    const uint32_t sl = (uint32_t)(keys[t] >> 32);
     const int64_t row = item_row(s, i);
     const uint32_t b0 = s.offs[row], len = s.offs[row + 1] - b0;
     const unsigned long long off = off0 + pre[t];
@@ -265,24 +268,36 @@ __global__ void str_gid_kernel(StrSrc s, const unsigned long long* slots, const 
 }
 
 // The dictionary's slots moved into a larger table.
+// (The table grown between insert passes.) The old slots move to the new
+// table; those installed by the stopped pass (no id yet) are listed again at
+// their new places.
 __global__ void str_rehash_kernel(const unsigned long long* old, uint64_t old_cap, unsigned long long* slots,
-                                  uint64_t mask) {
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < old_cap; i += (uint64_t)gridDim.x * blockDim.x) {
-    const unsigned long long* o = old + i * 4;
-    if (o[0] == kEmpty && o[1] == kEmpty) continue;
-    U128 k; k.lo = o[0]; k.hi = o[1];
-    uint64_t idx = (k.lo ^ (k.lo >> 32)) & mask;
-    for (uint64_t probe = 0; probe <= mask; ++probe) {
-      unsigned long long* sl = slots + idx * 4;
-      U128 e; e.lo = kEmpty; e.hi = kEmpty;
-      const U128 prev = cas128((U128*)sl, e, k);
-      if (prev.lo == e.lo && prev.hi == e.hi) {
-        sl[2] = o[2];
-        sl[3] = o[3];
-        break;
+                                  uint64_t mask, uint32_t* list, unsigned long long* count) {
+  for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x; i0 < old_cap; i0 += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t i = i0 + threadIdx.x;
+    bool pending = false;
+    uint32_t at = 0;
+    if (i < old_cap) {
+      const unsigned long long* o = old + i * 4;
+      if (!(o[0] == kEmpty && o[1] == kEmpty)) {
+        U128 k; k.lo = o[0]; k.hi = o[1];
+        uint64_t idx = (k.lo ^ (k.lo >> 32)) & mask;
+        for (uint64_t probe = 0; probe <= mask; ++probe) {
+          unsigned long long* sl = slots + idx * 4;
+          U128 e; e.lo = kEmpty; e.hi = kEmpty;
+          const U128 prev = cas128((U128*)sl, e, k);
+          if (prev.lo == e.lo && prev.hi == e.hi) {
+            sl[2] = o[2];
+            sl[3] = o[3];
+            pending = o[2] == kNoId;
+            at = (uint32_t)idx;
+            break;
+          }
+          idx = (idx + 1) & mask;
+        }
       }
-      idx = (idx + 1) & mask;
     }
+    warp_append(pending, at, list, count);
   }
 }
 
@@ -313,7 +328,7 @@ struct StrDict {
   int64_t n_ids = 0, used = 0;      // distinct strings and arena bytes
   int64_t slots_used = 0;           // installed hashes (n_ids after every complete batch)
   DevBuf hashes, sketch, rowslot, list, sorted, pack, pre, scan_tmp, gid;  // per-batch scratch
-  bool dirty = false;               // a batch stopped part way: representatives to clear
+  bool dirty = false;               // a batch stopped part way: refused until reset
   DevBuf h_offs, h_bytes, h_valid, h_sel;             // a host batch's string column on the device
   std::vector<unsigned long long> loc_host;           // host copies for wg_agg_key_strings,
   std::vector<uint8_t> arena_host;                    // valid while no batch came since
@@ -347,7 +362,8 @@ wg_status str_table(Ctx* ctx, StrDict* d, uint64_t cap) {
   WG_CUDA_TRY(cudaMemsetAsync(nr.get(), 0xFF, (size_t)cap * 4, ctx->stream));
   if (d->cap > 0) {
     str_rehash_kernel<<<str_grid(ctx, (int64_t)d->cap, 256), 256, 0, ctx->stream>>>(
-        d->slots.as<unsigned long long>(), d->cap, ns.as<unsigned long long>(), cap - 1);
+        d->slots.as<unsigned long long>(), d->cap, ns.as<unsigned long long>(), cap - 1, d->list.as<uint32_t>(),
+        d->ctr.as<unsigned long long>() + 2);
     ctx->count_launch();
   }
   WG_CUDA_TRY(cudaGetLastError());
@@ -409,6 +425,7 @@ wg_status strdict_map(Ctx* ctx, StrDict** dp, const wg_batch_desc* in, int col, 
   if (in->sel && in->sel_len > len) return fail(WG_E_INVALID, "selection longer than the batch");
   if (!*dp) *dp = new StrDict();
   StrDict* d = *dp;
+  if (d->dirty) return fail(WG_E_STATE, "the string dictionary stopped part way through a batch; reset the aggregate");
   d->host_fresh = false;
   const int64_t n = in->sel ? in->sel_len : len;
   StrSrc s{sb->offsets, sb->bytes, c.valid_words, in->sel, n};
@@ -448,6 +465,7 @@ wg_status strdict_map(Ctx* ctx, StrDict** dp, const wg_batch_desc* in, int col, 
   WG_TRY(d->hashes.ensure(ctx, n * 16));
   WG_TRY(d->sketch.ensure(ctx, (int64_t(1) << kSketchBits) * 4));
   WG_TRY(d->rowslot.ensure(ctx, n * 4));
+  WG_TRY(d->list.ensure(ctx, std::max<int64_t>(n * 4, 16)));
   WG_TRY(d->ctr.ensure(ctx, 64));
   unsigned long long* ctr = d->ctr.as<unsigned long long>();
   const unsigned grid = str_grid(ctx, n, 256);
@@ -457,64 +475,70 @@ wg_status strdict_map(Ctx* ctx, StrDict** dp, const wg_batch_desc* in, int col, 
   WG_CUDA_TRY(cudaGetLastError());
   double est = 0.0;
   WG_TRY(sketch_estimate(ctx, d, &est));
+  d->dirty = true;  // until the batch completes
+  str_ctr_kernel<<<1, 1, 0, ctx->stream>>>(ctr, (unsigned long long)d->slots_used);
+  ctx->count_launch();
   const uint64_t want = pow2_at_least((uint64_t)(1.5 * ((double)d->slots_used + std::min<double>((double)n, est * 1.1)) + 64));
   if (d->cap < want) WG_TRY(str_table(ctx, d, want));
-  else if (d->dirty) WG_CUDA_TRY(cudaMemsetAsync(d->rep.get(), 0xFF, (size_t)d->cap * 4, ctx->stream));
-  d->dirty = true;  // until the batch completes
   int64_t cv[4] = {0, 0, 0, 0};
   for (int pass = 0;; ++pass) {
-    str_ctr_kernel<<<1, 1, 0, ctx->stream>>>(ctr, (unsigned long long)d->slots_used);
     str_insert_kernel<<<grid, 256, 0, ctx->stream>>>(d->hashes.as<U128>(), n, d->slots.as<unsigned long long>(),
                                                      d->cap - 1, d->rowslot.as<int32_t>(), d->rep.as<uint32_t>(),
-                                                     ctr);
-    ctx->count_launch(2);
+                                                     d->list.as<uint32_t>(), ctr);
+    ctx->count_launch();
     WG_CUDA_TRY(cudaGetLastError());
-    WG_TRY(read_back_i64(ctx, reinterpret_cast<int64_t*>(ctr), cv, 2));
+    WG_TRY(read_back_i64(ctx, reinterpret_cast<int64_t*>(ctr), cv, 3));
     if (cv[1] == 0) break;
     if (pass >= 16 || d->cap >= (1ULL << 31)) return fail(WG_E_NOMEM, "string dictionary table cannot grow");
-    d->slots_used = cv[0];  // the installs of the stopped pass stay in the table
+    // the installs of the stopped pass stay in the table; the grown table's
+    // rehash lists them again, the next pass lists its own installs
+    d->slots_used = cv[0];
+    str_ctr_kernel<<<1, 1, 0, ctx->stream>>>(ctr, (unsigned long long)d->slots_used);
+    ctx->count_launch();
     WG_TRY(str_table(ctx, d, std::max<uint64_t>(d->cap * 4, pow2_at_least(2 * (uint64_t)cv[0]))));
   }
   d->slots_used = cv[0];
-
-  // (3) the new strings' representatives listed with their total length
-  WG_TRY(d->list.ensure(ctx, std::max<int64_t>(n * 4, 16)));
-  str_collect_kernel<<<grid, 256, 0, ctx->stream>>>(s, d->slots.as<unsigned long long>(), d->rowslot.as<int32_t>(),
-                                                    d->rep.as<uint32_t>(), d->list.as<uint32_t>(), ctr);
-  ctx->count_launch();
-  WG_CUDA_TRY(cudaGetLastError());
-  WG_TRY(read_back_i64(ctx, reinterpret_cast<int64_t*>(ctr), cv, 4));
-  const int64_t new_ids = cv[2], new_bytes = cv[3];
+  const int64_t new_ids = cv[2];
   if (d->n_ids + new_ids >= (int64_t)INT32_MAX) return fail(WG_E_UNSUPPORTED, "more than 2^31 - 1 distinct strings");
+
+  int64_t new_bytes = 0;
   if (new_ids > 0) {
-    // (4) the new strings in first-appearance order (their items sorted), ids
-    // and arena offsets from a scan of their lengths
-    WG_TRY(grow_keep(ctx, d->arena, d->used, std::max<int64_t>(d->used + new_bytes, 16)));
-    WG_TRY(grow_keep(ctx, d->id_loc, d->n_ids * 8, std::max<int64_t>((d->n_ids + new_ids) * 8, 16)));
-    WG_TRY(d->sorted.ensure(ctx, new_ids * 4));
-    WG_TRY(d->pack.ensure(ctx, new_ids * 8));
+    // (3)-(4) the new strings in first-appearance order (sorted by their first
+    // item), ids and arena offsets from a scan of their lengths
+    WG_TRY(d->pack.ensure(ctx, new_ids * 8));     // sort keys, then lengths
+    WG_TRY(d->sorted.ensure(ctx, new_ids * 8));   // sorted keys
     WG_TRY(d->pre.ensure(ctx, new_ids * 8));
     int bits = 1;
     while (bits < 32 && (int64_t(1) << bits) < n) ++bits;
     size_t t1 = 0, t2 = 0;
-    WG_CUDA_TRY(cub::DeviceRadixSort::SortKeys(nullptr, t1, d->list.as<uint32_t>(), d->sorted.as<uint32_t>(),
-                                               (int)new_ids, 0, bits, ctx->stream));
+    WG_CUDA_TRY(cub::DeviceRadixSort::SortKeys(nullptr, t1, d->pack.as<unsigned long long>(),
+                                               d->sorted.as<unsigned long long>(), (int)new_ids, 0, bits, ctx->stream));
     WG_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, t2, d->pack.as<unsigned long long>(),
                                               d->pre.as<unsigned long long>(), (int)new_ids, ctx->stream));
     WG_TRY(d->scan_tmp.ensure(ctx, std::max<int64_t>((int64_t)std::max(t1, t2), 16)));
-    WG_CUDA_TRY(cub::DeviceRadixSort::SortKeys(d->scan_tmp.get(), t1, d->list.as<uint32_t>(), d->sorted.as<uint32_t>(),
-                                               (int)new_ids, 0, bits, ctx->stream));
     const unsigned kgrid = str_grid(ctx, new_ids, 256);
-    str_len_kernel<<<kgrid, 256, 0, ctx->stream>>>(s, d->sorted.as<uint32_t>(), new_ids,
+    str_key_kernel<<<kgrid, 256, 0, ctx->stream>>>(d->list.as<uint32_t>(), new_ids, d->rep.as<uint32_t>(),
+                                                   d->pack.as<unsigned long long>());
+    WG_CUDA_TRY(cub::DeviceRadixSort::SortKeys(d->scan_tmp.get(), t1, d->pack.as<unsigned long long>(),
+                                               d->sorted.as<unsigned long long>(), (int)new_ids, 0, bits, ctx->stream));
+    str_len_kernel<<<kgrid, 256, 0, ctx->stream>>>(s, d->sorted.as<unsigned long long>(), new_ids,
                                                    d->pack.as<unsigned long long>());
     WG_CUDA_TRY(cub::DeviceScan::ExclusiveSum(d->scan_tmp.get(), t2, d->pack.as<unsigned long long>(),
                                               d->pre.as<unsigned long long>(), (int)new_ids, ctx->stream));
-    str_assign_kernel<<<kgrid, 256, 0, ctx->stream>>>(s, d->sorted.as<uint32_t>(), new_ids,
+    str_bytes_kernel<<<1, 1, 0, ctx->stream>>>(d->pack.as<unsigned long long>(), d->pre.as<unsigned long long>(),
+                                               new_ids, ctr);
+    ctx->count_launch(3 + 2 + 2);  // key, lengths, total; the sort's and the scan's kernels (about two each)
+    WG_CUDA_TRY(cudaGetLastError());
+    WG_TRY(read_back_i64(ctx, reinterpret_cast<int64_t*>(ctr), cv, 4));
+    new_bytes = cv[3];
+    WG_TRY(grow_keep(ctx, d->arena, d->used, std::max<int64_t>(d->used + new_bytes, 16)));
+    WG_TRY(grow_keep(ctx, d->id_loc, d->n_ids * 8, std::max<int64_t>((d->n_ids + new_ids) * 8, 16)));
+    str_assign_kernel<<<kgrid, 256, 0, ctx->stream>>>(s, d->sorted.as<unsigned long long>(), new_ids,
                                                       d->pre.as<unsigned long long>(), d->slots.as<unsigned long long>(),
-                                                      d->rowslot.as<int32_t>(), d->rep.as<uint32_t>(),
-                                                      (unsigned long long)d->n_ids, (unsigned long long)d->used,
-                                                      d->arena.as<uint8_t>(), d->id_loc.as<unsigned long long>());
-    ctx->count_launch(2 + 2 + 2);  // the sort's and the scan's kernels (about two each), lengths, assignment
+                                                      d->rep.as<uint32_t>(), (unsigned long long)d->n_ids,
+                                                      (unsigned long long)d->used, d->arena.as<uint8_t>(),
+                                                      d->id_loc.as<unsigned long long>());
+    ctx->count_launch();
     WG_CUDA_TRY(cudaGetLastError());
   }
   // (5) every item's bytes checked against its string's arena copy, and its id
