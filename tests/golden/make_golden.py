@@ -3,9 +3,10 @@ for the filter → hash-join → hash-aggregate path, restated as data.
 
 The reference is Go and cannot run here, so each case below transcribes the
 inputs and the expected outputs of one reference test (cited as file:line in
-the Wadjet tree). String keys in the reference's join/aggregate tests are
-restated as integer keys (the GPU path covers integer-class keys); the
-expected row counts and sums are unchanged by that renaming.
+the Wadjet tree). String keys in the reference's join tests and in the
+integer-key aggregate case are restated as integer keys; the expected row
+counts and sums are unchanged by that renaming. The string GROUP BY cases keep
+their strings.
 
 Run: python tests/golden/make_golden.py
 """
