@@ -110,8 +110,9 @@ def test_host_batches_match_oracle(ctx, nulls):
 
 
 def test_device_batches_grow_the_dictionary(ctx):
-    """Device-resident string columns; 150 000 distinct strings in one batch
-    pass the first table's 3/4 mark, so the dictionary grows mid-batch."""
+    """Device-resident string columns; the second batch brings new strings to a
+    dictionary of about 110 000, so its table is regrown (rehashed) between
+    batches."""
     rng = np.random.default_rng(12)
     batches = []
     for n, nd in [(200_000, 150_000), (50_000, 160_000)]:
