@@ -110,9 +110,8 @@ def test_host_batches_match_oracle(ctx, nulls):
 
 
 def test_device_batches_grow_the_dictionary(ctx):
-    """Device-resident string columns; the second batch brings new strings to a
-    dictionary of about 110 000, so its table is regrown (rehashed) between
-    batches."""
+    """Device-resident string columns over two batches: about 110 000 distinct
+    strings, then about 43 000 new ones added to the same dictionary."""
     rng = np.random.default_rng(12)
     batches = []
     for n, nd in [(200_000, 150_000), (50_000, 160_000)]:
